@@ -1,0 +1,272 @@
+/*
+ * kpolaris_b200.h -- C ABI of the B200-native KPolaris per-pixel GRRT path.
+ *
+ * Every entry point takes plain C structs, pointers and sizes; no C++ or
+ * torch types cross this boundary.  The structs mirror the reference's
+ * parameter objects field for field so that the reference's C++ call sites
+ * (run_riaf_image, run_riaf_multifrequency_image, run_grmhd_image,
+ * run_image_batch_metric) can be forwarded here by a thin host shim
+ * (kpolaris_b200/host/kpolaris_image.hpp).
+ *
+ * Conventions shared by every function:
+ *   - return value: KP_OK (0) on success, a negative kp_status otherwise;
+ *     kp_last_error() returns a human-readable message for the calling
+ *     thread's most recent failure.
+ *   - per-ray failures are not errors: they are reported through the
+ *     per-pixel `reason` codes (kp_termination), identical to the
+ *     reference's TerminationReason (src/common/types.hpp:37-48).
+ *   - image arrays are laid out [nfreq][npix], pixel = j * nx + i, exactly as
+ *     ImageHostData (src/image/result.hpp:9-31) and copy_real_view_2d
+ *     (src/image/driver.hpp:38-49).
+ */
+#ifndef KPOLARIS_B200_H
+#define KPOLARIS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define KP_ABI_VERSION 1
+/* Maximum frequencies that share one geodesic in a single launch
+ * (reference compile-time KPOLARIS_MAX_FREQUENCIES, src/common/types.hpp:5-7). */
+#define KP_MAX_FREQUENCIES 4
+
+typedef enum kp_status {
+    KP_OK = 0,
+    KP_ERR_INVALID = -1,     /* invalid argument (reference: std::invalid_argument) */
+    KP_ERR_OOM = -2,         /* device or host allocation failed */
+    KP_ERR_CUDA = -3,        /* CUDA runtime or launch failure */
+    KP_ERR_TIMEOUT = -4,     /* a bounded device/host wait ran out */
+    KP_ERR_UNSUPPORTED = -5, /* feature/combination not built (reference: std::runtime_error) */
+    KP_ERR_BUSY = -6,        /* admission refused: not enough device memory / slots */
+    KP_ERR_NOT_FOUND = -7,   /* unknown handle or job id */
+    KP_ERR_CANCELLED = -8    /* job was cancelled before completion */
+} kp_status;
+
+/* Reference CoordinateSystem (src/common/types.hpp:51-57). */
+typedef enum kp_coordinate_system {
+    KP_COORD_CARTESIAN_KS = 0,
+    KP_COORD_BOYER_LINDQUIST = 1,
+    KP_COORD_SPHERICAL_KS = 2,
+    KP_COORD_FMKS = 3,
+    KP_COORD_MKS = 4
+} kp_coordinate_system;
+
+/* Reference CameraModel (src/camera/camera.hpp:7-10). */
+typedef enum kp_camera_model {
+    KP_CAMERA_PINHOLE = 0,
+    KP_CAMERA_PARALLEL_PLANE = 1
+} kp_camera_model;
+
+/* Reference TerminationReason (src/common/types.hpp:37-48). */
+typedef enum kp_termination {
+    KP_REASON_NONE = 0,
+    KP_REASON_REACHED_CAMERA = 1,
+    KP_REASON_REACHED_INNER_BOUNDARY = 2,
+    KP_REASON_ESCAPED_DOMAIN = 3,
+    KP_REASON_MAX_STEPS = 4,
+    KP_REASON_INVALID_STATE = 5,
+    KP_REASON_SLOW_LIGHT_TIME_EXHAUSTED = 6,
+    KP_REASON_ADAPTIVE_STEP_UNDERFLOW = 7,
+    KP_REASON_METRIC_TIME_EXHAUSTED = 8,
+    KP_REASON_REACHED_DIRECT_TURN = 9
+} kp_termination;
+
+/* Thermal synchrotron fit selector (src/radiation/thermal_synchrotron.hpp:8-17). */
+typedef enum kp_emission_fit {
+    KP_FIT_PANDYA = 1,
+    KP_FIT_DEXTER = 4
+} kp_emission_fit;
+
+/* Arithmetic used by the image kernels. */
+typedef enum kp_precision {
+    /* FP64 everywhere, IEEE operation order of the reference (bit-exact
+     * termination status and fixed-step counts). */
+    KP_PRECISION_FP64 = 0,
+    /* FP64 geodesic state, step control and near-hole geometry; FP32
+     * coefficients and Stokes transfer with a per-job 2^E scale and
+     * compensated accumulation. */
+    KP_PRECISION_MIXED = 1
+} kp_precision;
+
+/* How rays are scheduled on the device. */
+typedef enum kp_schedule {
+    /* One thread per pixel, one launch per image: the plain form. */
+    KP_SCHEDULE_PER_PIXEL = 0,
+    /* Persistent kernel draining a global ray queue with per-lane refill. */
+    KP_SCHEDULE_PERSISTENT = 1
+} kp_schedule;
+
+/* Geodesic integrator.  The reference image path uses step-doubling RK4
+ * (adaptive_rk4_step, src/geodesic/rk4.hpp:109-161); the Cash-Karp embedded
+ * pair (adaptive_rkf45_endpoint_step, rk4.hpp:164-250) is an added variant. */
+typedef enum kp_integrator {
+    KP_INTEGRATOR_STEP_DOUBLING_RK4 = 0,
+    KP_INTEGRATOR_CASH_KARP = 1
+} kp_integrator;
+
+/* Mirrors CameraParams<double> (src/camera/camera.hpp:12-25). */
+typedef struct kp_camera_params {
+    int nx;
+    int ny;
+    double radius;
+    double inclination; /* radians */
+    double fov;
+    double fov_y;
+    double xspan;
+    double yspan;
+    double x_offset;
+    double y_offset;
+    int model; /* kp_camera_model */
+} kp_camera_params;
+
+/* Mirrors EmissionSelection<double> (src/radiation/emission_selection.hpp:11-19). */
+typedef struct kp_emission_selection {
+    double equatorial_h_over_r;
+    int equatorial_samples;
+    int faraday_rotation;
+} kp_emission_selection;
+
+/* Mirrors PassAParams<double> (src/geodesic/pass_a_core.hpp:10-36). */
+typedef struct kp_pass_a_params {
+    kp_camera_params camera;
+    kp_emission_selection emission_selection;
+    double mass;
+    double spin;
+    double inner_radius;
+    double outer_radius;
+    double step;
+    int max_steps;
+    int adaptive;
+    int direct_only;
+    double adaptive_tolerance;
+    double min_step;
+    double max_step;
+    double max_radiation_step;
+    double max_radiation_depth;
+    double max_absorption_depth;
+    double max_faraday_depth;
+    double fmks_startx1;
+    double fmks_hslope;
+    double fmks_mks_smooth;
+    double fmks_poly_alpha;
+    double fmks_poly_xt;
+    double fmks_poly_norm;
+    int coordinate_system; /* kp_coordinate_system */
+} kp_pass_a_params;
+
+/* Mirrors the thermal fields of RIAFAnalyticRadiationModel<double>
+ * (src/model/riaf.hpp:19-52).  Non-thermal fields are not carried: the
+ * thermal synchrotron fits are the only emission types on this path. */
+typedef struct kp_riaf_model {
+    double nth0;
+    double Te0;
+    double disk_h;
+    double pow_nth;
+    double pow_T;
+    double ne_unit;
+    double te_unit;
+    double b_unit;
+    double freq_cgs;
+    double mbh_solar;
+    double r_min;
+    double r_max;
+    double horizon_buffer;
+    double emission_scale;
+    double absorption_scale;
+    double faraday_scale;
+    double max_pol_frac;
+    double keplerian_factor;
+    double infall_factor;
+    int emission_type; /* kp_emission_fit */
+    double min_frequency_scale;
+    double min_sin_theta;
+    double min_thetae;
+    double min_radius;
+} kp_riaf_model;
+
+/* Caller-owned output buffers (host or device memory, see kp_run_options).
+ * Mirrors ImageHostData (src/image/result.hpp:9-31) without the analysis
+ * fields.  image_* hold nfreq*npix doubles; diagnostics hold npix values. */
+typedef struct kp_image_out {
+    int npix;
+    int nfreq;
+    double* image_i;
+    double* image_q;
+    double* image_u;
+    double* image_v;
+    double* closure_x;
+    double* closure_k;
+    double* final_null;
+    double* frame_error;
+    double* det_r;
+    double* overlap_r11;
+    double* overlap_r12;
+    double* overlap_r21;
+    double* overlap_r22;
+    double* basis_identity_error;
+    double* basis_rotation_angle;
+    int32_t* pass_a_steps;
+    int32_t* steps;
+    int32_t* reason;
+} kp_image_out;
+
+/* Launch-side options that the reference expresses through build flags and
+ * extra driver arguments. */
+typedef struct kp_run_options {
+    int precision;       /* kp_precision */
+    int schedule;        /* kp_schedule */
+    int integrator;      /* kp_integrator */
+    int outputs_on_device; /* 1: kp_image_out pointers are device pointers */
+    int device;          /* CUDA device ordinal */
+    void* stream;        /* cudaStream_t, or NULL for the library's stream */
+    int timing;          /* 1: print "timing <name> <seconds> s" lines like the reference */
+    /* Persistent-schedule tunables; 0 selects the autotuned/default value. */
+    int blocks_per_sm;
+    int threads_per_block;
+} kp_run_options;
+
+/* Fills *opt with defaults: FP64, per-pixel, step-doubling RK4, host
+ * outputs, device 0, library stream. */
+void kp_default_run_options(kp_run_options* opt);
+
+/* Fills *p / *m with the reference's struct defaults
+ * (pass_a_core.hpp:10-36, camera.hpp:12-25, riaf.hpp:19-52). */
+void kp_default_pass_a_params(kp_pass_a_params* p);
+void kp_default_riaf_model(kp_riaf_model* m);
+
+/* Thread-local message describing the most recent failure. */
+const char* kp_last_error(void);
+
+/* ABI version, for the bindings' load-time check. */
+int kp_abi_version(void);
+
+/* Bytes of per-pixel output (15 doubles + 3 int32 = 132 B), the figure the
+ * reference's batch budget uses (src/image/batch_driver.hpp:49). */
+size_t kp_image_output_bytes(int npix, int nfreq);
+
+/*
+ * RIAF image, one or several frequencies sharing one geodesic per pixel.
+ * Replaces run_riaf_image (src/image/riaf.hpp:12-16, nfreq == 1) and
+ * run_riaf_multifrequency_image (src/image/riaf.hpp:32-39, 1..4 frequencies
+ * with step-control list == frequency list).  `frequencies` may be NULL
+ * when nfreq == 1, in which case model->freq_cgs is used.
+ * radiation_substeps is accepted for signature compatibility; the
+ * reference's segment kernels ignore it (pass_b.hpp:526, :1003).
+ */
+int kp_image_riaf(const kp_pass_a_params* params,
+                  const kp_riaf_model* model,
+                  int radiation_substeps,
+                  const double* frequencies,
+                  int nfreq,
+                  const kp_run_options* options,
+                  kp_image_out* out);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* KPOLARIS_B200_H */

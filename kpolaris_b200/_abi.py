@@ -1,0 +1,282 @@
+"""ctypes mirror of include/kpolaris_b200.h (the C ABI of the image path).
+
+Field order and types must match the header exactly; tests/test_abi.py checks
+the struct sizes against the library's own report.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+KP_ABI_VERSION = 1
+KP_MAX_FREQUENCIES = 4
+
+KP_OK = 0
+KP_ERR_INVALID = -1
+KP_ERR_OOM = -2
+KP_ERR_CUDA = -3
+KP_ERR_TIMEOUT = -4
+KP_ERR_UNSUPPORTED = -5
+KP_ERR_BUSY = -6
+KP_ERR_NOT_FOUND = -7
+KP_ERR_CANCELLED = -8
+
+COORD_CARTESIAN_KS = 0
+COORD_BOYER_LINDQUIST = 1
+COORD_SPHERICAL_KS = 2
+COORD_FMKS = 3
+COORD_MKS = 4
+
+CAMERA_PINHOLE = 0
+CAMERA_PARALLEL_PLANE = 1
+
+REASON_NONE = 0
+REASON_REACHED_CAMERA = 1
+REASON_REACHED_INNER_BOUNDARY = 2
+REASON_ESCAPED_DOMAIN = 3
+REASON_MAX_STEPS = 4
+REASON_INVALID_STATE = 5
+REASON_ADAPTIVE_STEP_UNDERFLOW = 7
+
+FIT_PANDYA = 1
+FIT_DEXTER = 4
+
+PRECISION_FP64 = 0
+PRECISION_MIXED = 1
+
+SCHEDULE_PER_PIXEL = 0
+SCHEDULE_PERSISTENT = 1
+
+INTEGRATOR_STEP_DOUBLING_RK4 = 0
+INTEGRATOR_CASH_KARP = 1
+
+
+class CameraParams(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int), ("ny", C.c_int),
+        ("radius", C.c_double), ("inclination", C.c_double),
+        ("fov", C.c_double), ("fov_y", C.c_double),
+        ("xspan", C.c_double), ("yspan", C.c_double),
+        ("x_offset", C.c_double), ("y_offset", C.c_double),
+        ("model", C.c_int),
+    ]
+
+
+class EmissionSelection(C.Structure):
+    _fields_ = [
+        ("equatorial_h_over_r", C.c_double),
+        ("equatorial_samples", C.c_int),
+        ("faraday_rotation", C.c_int),
+    ]
+
+
+class PassAParams(C.Structure):
+    _fields_ = [
+        ("camera", CameraParams),
+        ("emission_selection", EmissionSelection),
+        ("mass", C.c_double), ("spin", C.c_double),
+        ("inner_radius", C.c_double), ("outer_radius", C.c_double),
+        ("step", C.c_double),
+        ("max_steps", C.c_int), ("adaptive", C.c_int), ("direct_only", C.c_int),
+        ("adaptive_tolerance", C.c_double), ("min_step", C.c_double),
+        ("max_step", C.c_double), ("max_radiation_step", C.c_double),
+        ("max_radiation_depth", C.c_double), ("max_absorption_depth", C.c_double),
+        ("max_faraday_depth", C.c_double),
+        ("fmks_startx1", C.c_double), ("fmks_hslope", C.c_double),
+        ("fmks_mks_smooth", C.c_double), ("fmks_poly_alpha", C.c_double),
+        ("fmks_poly_xt", C.c_double), ("fmks_poly_norm", C.c_double),
+        ("coordinate_system", C.c_int),
+    ]
+
+
+class RIAFModel(C.Structure):
+    _fields_ = [
+        ("nth0", C.c_double), ("Te0", C.c_double), ("disk_h", C.c_double),
+        ("pow_nth", C.c_double), ("pow_T", C.c_double),
+        ("ne_unit", C.c_double), ("te_unit", C.c_double), ("b_unit", C.c_double),
+        ("freq_cgs", C.c_double), ("mbh_solar", C.c_double),
+        ("r_min", C.c_double), ("r_max", C.c_double), ("horizon_buffer", C.c_double),
+        ("emission_scale", C.c_double), ("absorption_scale", C.c_double),
+        ("faraday_scale", C.c_double), ("max_pol_frac", C.c_double),
+        ("keplerian_factor", C.c_double), ("infall_factor", C.c_double),
+        ("emission_type", C.c_int),
+        ("min_frequency_scale", C.c_double), ("min_sin_theta", C.c_double),
+        ("min_thetae", C.c_double), ("min_radius", C.c_double),
+    ]
+
+
+_DP = C.POINTER(C.c_double)
+_IP = C.POINTER(C.c_int32)
+
+
+class ImageOut(C.Structure):
+    _fields_ = [
+        ("npix", C.c_int), ("nfreq", C.c_int),
+        ("image_i", _DP), ("image_q", _DP), ("image_u", _DP), ("image_v", _DP),
+        ("closure_x", _DP), ("closure_k", _DP), ("final_null", _DP),
+        ("frame_error", _DP), ("det_r", _DP),
+        ("overlap_r11", _DP), ("overlap_r12", _DP), ("overlap_r21", _DP),
+        ("overlap_r22", _DP), ("basis_identity_error", _DP),
+        ("basis_rotation_angle", _DP),
+        ("pass_a_steps", _IP), ("steps", _IP), ("reason", _IP),
+    ]
+
+
+class RunOptions(C.Structure):
+    _fields_ = [
+        ("precision", C.c_int), ("schedule", C.c_int), ("integrator", C.c_int),
+        ("outputs_on_device", C.c_int), ("device", C.c_int),
+        ("stream", C.c_void_p), ("timing", C.c_int),
+        ("blocks_per_sm", C.c_int), ("threads_per_block", C.c_int),
+    ]
+
+
+IMAGE_FIELDS = ("image_i", "image_q", "image_u", "image_v")
+DIAG_FIELDS = ("closure_x", "closure_k", "final_null", "frame_error", "det_r",
+               "overlap_r11", "overlap_r12", "overlap_r21", "overlap_r22",
+               "basis_identity_error", "basis_rotation_angle")
+INT_FIELDS = ("pass_a_steps", "steps", "reason")
+
+
+@dataclass
+class ImageHostData:
+    """Host result of one image: the fields of the reference's ImageHostData
+    (src/image/result.hpp:9-31) without the analysis block.  image_* arrays are
+    shaped [nfreq, npix]; diagnostics [npix]."""
+
+    npix: int
+    nfreq: int
+    arrays: dict = field(default_factory=dict)
+
+    def __getattr__(self, name):
+        arrays = self.__dict__.get("arrays")
+        if arrays is not None and name in arrays:
+            return arrays[name]
+        raise AttributeError(name)
+
+    @classmethod
+    def allocate(cls, npix: int, nfreq: int) -> "ImageHostData":
+        arrays = {}
+        for name in IMAGE_FIELDS:
+            arrays[name] = np.zeros((nfreq, npix), dtype=np.float64)
+        for name in DIAG_FIELDS:
+            arrays[name] = np.zeros(npix, dtype=np.float64)
+        for name in INT_FIELDS:
+            arrays[name] = np.zeros(npix, dtype=np.int32)
+        return cls(npix=npix, nfreq=nfreq, arrays=arrays)
+
+    def as_struct(self) -> ImageOut:
+        out = ImageOut()
+        out.npix = self.npix
+        out.nfreq = self.nfreq
+        for name in IMAGE_FIELDS + DIAG_FIELDS:
+            setattr(out, name, self.arrays[name].ctypes.data_as(_DP))
+        for name in INT_FIELDS:
+            setattr(out, name, self.arrays[name].ctypes.data_as(_IP))
+        return out
+
+
+def default_camera() -> CameraParams:
+    """CameraParams<double> defaults (src/camera/camera.hpp:12-25)."""
+    c = CameraParams()
+    c.nx, c.ny = 64, 64
+    c.radius = 100.0
+    c.inclination = 1.04719755119659774615
+    c.fov = 10.0
+    c.fov_y = -1.0
+    c.xspan = -1.0
+    c.yspan = -1.0
+    c.x_offset = 0.0
+    c.y_offset = 0.0
+    c.model = CAMERA_PINHOLE
+    return c
+
+
+def default_pass_a_params() -> PassAParams:
+    """PassAParams<double> defaults (src/geodesic/pass_a_core.hpp:10-36)."""
+    p = PassAParams()
+    p.camera = default_camera()
+    p.emission_selection.equatorial_h_over_r = 0.0
+    p.emission_selection.equatorial_samples = 8
+    p.emission_selection.faraday_rotation = 1
+    p.mass = 1.0
+    p.spin = 0.0
+    p.inner_radius = 2.2
+    p.outer_radius = 200.0
+    p.step = 0.05
+    p.max_steps = 4096
+    p.adaptive = 0
+    p.direct_only = 0
+    p.adaptive_tolerance = 1e-7
+    p.min_step = 1e-5
+    p.max_step = 1.0
+    p.max_radiation_step = 1.0
+    p.max_radiation_depth = 1.0
+    p.max_absorption_depth = -1.0
+    p.max_faraday_depth = -1.0
+    p.fmks_startx1 = 0.0
+    p.fmks_hslope = 0.3
+    p.fmks_mks_smooth = 0.5
+    p.fmks_poly_alpha = 14.0
+    p.fmks_poly_xt = 0.82
+    p.fmks_poly_norm = 1.0
+    p.coordinate_system = COORD_CARTESIAN_KS
+    return p
+
+
+def default_riaf_model() -> RIAFModel:
+    """RIAFAnalyticRadiationModel<double> defaults (src/model/riaf.hpp:19-52)."""
+    m = RIAFModel()
+    m.nth0 = 1.0
+    m.Te0 = 1.0
+    m.disk_h = 0.35
+    m.pow_nth = -1.1
+    m.pow_T = -0.84
+    m.ne_unit = 5.0e6
+    m.te_unit = 1.0e11
+    m.b_unit = 30.0
+    m.freq_cgs = 230.0e9
+    m.mbh_solar = 4.3e6
+    m.r_min = 1.0
+    m.r_max = 100.0
+    m.horizon_buffer = 0.1
+    m.emission_scale = 1.0
+    m.absorption_scale = 1.0
+    m.faraday_scale = 1.0
+    m.max_pol_frac = 0.99
+    m.keplerian_factor = 1.0
+    m.infall_factor = 0.0
+    m.emission_type = FIT_PANDYA
+    m.min_frequency_scale = 1e-6
+    m.min_sin_theta = 1e-4
+    m.min_thetae = 1e-3
+    m.min_radius = 1e-6
+    return m
+
+
+def default_run_options() -> RunOptions:
+    o = RunOptions()
+    o.precision = PRECISION_FP64
+    o.schedule = SCHEDULE_PER_PIXEL
+    o.integrator = INTEGRATOR_STEP_DOUBLING_RK4
+    o.outputs_on_device = 0
+    o.device = 0
+    o.stream = None
+    o.timing = 0
+    o.blocks_per_sm = 0
+    o.threads_per_block = 0
+    return o
+
+
+def horizon_radius(mass: float, spin: float) -> float:
+    """KerrSchildInMetric::horizon_radius (kerr_schild_cartesian.hpp:300-302)."""
+    return mass + math.sqrt(max(mass * mass - spin * spin, 0.0))
+
+
+def copy_struct(s):
+    out = type(s)()
+    C.memmove(C.addressof(out), C.addressof(s), C.sizeof(s))
+    return out

@@ -1,0 +1,160 @@
+"""CPU oracles for the KPolaris GRRT image path -- TEST INFRASTRUCTURE ONLY.
+
+Two oracles live here:
+  * port      -- oracle/kp_oracle.c, a C restatement of the reference's path
+                 (libkporacle.so), and
+  * reference -- oracle/_ref/libkpref.so, the reference's own header-only
+                 templates compiled unchanged against oracle/shim
+                 (built from the reference source tree by `make -C oracle ref`).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline / reference
+legs may use this module, and only as the checker or the timed CPU baseline.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+from kpolaris_b200 import _abi
+
+HERE = Path(__file__).resolve().parent
+PORT_SO = HERE / "libkporacle.so"
+REF_SO = HERE / "_ref" / "libkpref.so"
+REFERENCE_SRC = Path(os.environ.get("KPOLARIS_REFERENCE_SRC", "/root/reference/src"))
+
+
+def build(reference: bool = True) -> None:
+    """Compile the port (always) and the reference oracle (when the reference
+    source tree is present; elsewhere the prebuilt _ref/libkpref.so is used)."""
+    subprocess.run(["make", "-s", "-C", str(HERE), "all"], check=True)
+    if reference and REFERENCE_SRC.is_dir():
+        subprocess.run(["make", "-s", "-C", str(HERE), "ref",
+                        f"REFERENCE_SRC={REFERENCE_SRC}"], check=True)
+
+
+_libs: dict = {}
+
+
+def _declare_common(lib, prefix):
+    P = C.POINTER
+    d = C.c_double
+    getattr(lib, prefix + "thermal_coefficients").argtypes = [C.c_int] + [d] * 9 + [P(d)]
+    getattr(lib, prefix + "stokes_step").argtypes = [P(d), P(d), d]
+    getattr(lib, prefix + "riaf_coefficients_cks").argtypes = [d, d, P(_abi.RIAFModel), P(d), P(d)]
+    getattr(lib, prefix + "camera_ray_cks").argtypes = [P(_abi.PassAParams), C.c_int, P(d)]
+    getattr(lib, prefix + "transport_rhs_cks").argtypes = [d, d, P(d), P(d)]
+    getattr(lib, prefix + "last_error").restype = C.c_char_p
+
+
+def port_available() -> bool:
+    return PORT_SO.exists()
+
+
+def ref_available() -> bool:
+    return REF_SO.exists()
+
+
+def lib(kind: str):
+    """kind: 'port' or 'reference'."""
+    if kind in _libs:
+        return _libs[kind]
+    if kind == "port":
+        if not PORT_SO.exists():
+            build(reference=False)
+        L = C.CDLL(str(PORT_SO))
+        L.kpo_image_riaf_range.argtypes = [
+            C.POINTER(_abi.PassAParams), C.POINTER(_abi.RIAFModel), C.c_int,
+            C.POINTER(C.c_double), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+            C.POINTER(_abi.ImageOut)]
+        _declare_common(L, "kpo_")
+    elif kind == "reference":
+        if not REF_SO.exists():
+            build(reference=True)
+        if not REF_SO.exists():
+            raise FileNotFoundError("reference oracle not built (needs the reference source tree)")
+        L = C.CDLL(str(REF_SO))
+        L.kpref_image_riaf_range.argtypes = [
+            C.POINTER(_abi.PassAParams), C.POINTER(_abi.RIAFModel), C.c_int,
+            C.POINTER(C.c_double), C.c_int, C.c_int, C.c_int, C.c_int,
+            C.POINTER(_abi.ImageOut)]
+        _declare_common(L, "kpref_")
+    else:
+        raise ValueError(kind)
+    _libs[kind] = L
+    return L
+
+
+def _prefix(kind):
+    return "kpo_" if kind == "port" else "kpref_"
+
+
+def image_riaf(params, model, freqs, *, kind="port", integrator=0, threads=0,
+               pixel_begin=0, pixel_end=None, out=None) -> _abi.ImageHostData:
+    """Trace a RIAF image (or a pixel range of it) on the CPU."""
+    L = lib(kind)
+    npix = params.camera.nx * params.camera.ny
+    nfreq = len(freqs)
+    if out is None:
+        out = _abi.ImageHostData.allocate(npix, nfreq)
+    if pixel_end is None:
+        pixel_end = npix
+    fa = (C.c_double * nfreq)(*freqs)
+    s = out.as_struct()
+    if kind == "port":
+        rc = L.kpo_image_riaf_range(C.byref(params), C.byref(model), 1, fa, nfreq,
+                                    int(integrator), int(threads), int(pixel_begin),
+                                    int(pixel_end), C.byref(s))
+    else:
+        if integrator != 0:
+            raise ValueError("the reference image path uses step-doubling RK4 only")
+        rc = L.kpref_image_riaf_range(C.byref(params), C.byref(model), 1, fa, nfreq,
+                                      int(threads), int(pixel_begin), int(pixel_end),
+                                      C.byref(s))
+    if rc != 0:
+        raise RuntimeError(getattr(L, _prefix(kind) + "last_error")().decode())
+    return out
+
+
+def thermal_coefficients(fit, nu, ne, thetae, b, theta, sin_theta, cos_theta,
+                         max_pol_frac=0.99, min_sin_theta=1e-4, kind="port"):
+    L = lib(kind)
+    out = (C.c_double * 11)()
+    getattr(L, _prefix(kind) + "thermal_coefficients")(
+        int(fit), nu, ne, thetae, b, theta, sin_theta, cos_theta, max_pol_frac,
+        min_sin_theta, out)
+    return np.array(out[:])
+
+
+def stokes_step(stokes4, coeffs11, dlambda, kind="port"):
+    L = lib(kind)
+    s = (C.c_double * 4)(*stokes4)
+    c = (C.c_double * 11)(*coeffs11)
+    getattr(L, _prefix(kind) + "stokes_step")(s, c, float(dlambda))
+    return np.array(s[:])
+
+
+def riaf_coefficients_cks(mass, spin, model, state16, kind="port"):
+    L = lib(kind)
+    st = (C.c_double * 16)(*state16)
+    out = (C.c_double * 11)()
+    getattr(L, _prefix(kind) + "riaf_coefficients_cks")(mass, spin, C.byref(model), st, out)
+    return np.array(out[:])
+
+
+def camera_ray_cks(params, pixel, kind="port"):
+    L = lib(kind)
+    out = (C.c_double * 16)()
+    getattr(L, _prefix(kind) + "camera_ray_cks")(C.byref(params), int(pixel), out)
+    return np.array(out[:])
+
+
+def transport_rhs_cks(mass, spin, state16, kind="port"):
+    L = lib(kind)
+    st = (C.c_double * 16)(*state16)
+    out = (C.c_double * 16)()
+    getattr(L, _prefix(kind) + "transport_rhs_cks")(mass, spin, st, out)
+    return np.array(out[:])

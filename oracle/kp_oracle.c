@@ -1,0 +1,1686 @@
+/*
+ * kp_oracle.c -- CPU restatement of the reference's per-pixel polarized GRRT
+ * hot path (Cartesian Kerr-Schild metric, pinhole camera, RK4 / step-doubling
+ * RK4 / Cash-Karp, fused pass A + pass B, RIAF plasma, thermal synchrotron
+ * Pandya/Dexter fits, semi-analytic Stokes transfer).
+ *
+ * TEST INFRASTRUCTURE ONLY: the oracle is the parity checker and the CPU
+ * baseline.  The product library never includes or links this file.
+ *
+ * Each function names the reference file:line it restates and keeps that
+ * code's floating-point operation order; with -ffp-contract=off this file
+ * reproduces the reference templates bit for bit (checked in tests against
+ * oracle/_ref/libkpref.so, the reference's own headers built unchanged).
+ */
+#include "kp_oracle.h"
+
+#include <math.h>
+#include <omp.h>
+#include <stdio.h>
+#include <string.h>
+
+#define NDIM 4
+#define TINY 1e-300
+#define LARGE 1e300
+#define PI 3.141592653589793238462643383279502884
+
+typedef struct { double v[4]; } V4;
+typedef struct { double x, y, z; } V3;
+typedef struct { V4 x, k, e1, e2; } TS;
+typedef struct { double I, Q, U, V; } ST;
+typedef struct { double jI, jQ, jU, jV, aI, aQ, aU, aV, rQ, rU, rV; } TC;
+typedef struct { double r11, r12, r21, r22; } OV;
+
+static _Thread_local char g_err[256];
+
+static int fail(const char* m) {
+    snprintf(g_err, sizeof g_err, "%s", m);
+    return KP_ERR_INVALID;
+}
+
+const char* kpo_last_error(void) { return g_err; }
+
+/* ---- common/math.hpp:10-87 ------------------------------------------ */
+static inline double abs_val(double x) { return x < 0.0 ? -x : x; }
+static inline double min_val(double a, double b) { return a < b ? a : b; }
+static inline double max_val(double a, double b) { return a > b ? a : b; }
+static inline double clamp(double x, double lo, double hi) { return min_val(max_val(x, lo), hi); }
+static inline double square(double x) { return x * x; }
+static inline double tol_floor(void) { return 8.0 * 2.220446049250313080847263336181640625e-16; }
+
+static inline double stable_attenuation(double kappa, double dl) { /* math.hpp:65-73 */
+    const double x = kappa * dl;
+    if (x > 700.0) return 0.0;
+    return exp(-x);
+}
+
+static inline double stable_source_factor(double kappa, double dl) { /* math.hpp:75-85 */
+    const double x = kappa * dl;
+    if (abs_val(x) < 1e-6) {
+        return dl * (1.0 - x / 2.0 + x * x / 6.0 - x * x * x / 24.0);
+    }
+    return (1.0 - exp(-x)) / kappa;
+}
+
+/* ---- common/vec.hpp:41-70 -------------------------------------------- */
+static inline double dot3(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static inline V3 cross3(V3 a, V3 b) {
+    V3 o = {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+    return o;
+}
+static inline double norm3(V3 a) {
+    const double scale = max_val(abs_val(a.x), max_val(abs_val(a.y), abs_val(a.z)));
+    if (scale == 0.0) return 0.0;
+    V3 s = {a.x / scale, a.y / scale, a.z / scale};
+    return scale * sqrt(dot3(s, s));
+}
+
+static inline V4 v4(double a, double b, double c, double d) { V4 o = {{a, b, c, d}}; return o; }
+static inline V4 v4_add(V4 a, V4 b) { return v4(a.v[0] + b.v[0], a.v[1] + b.v[1], a.v[2] + b.v[2], a.v[3] + b.v[3]); }
+static inline V4 v4_sub(V4 a, V4 b) { return v4(a.v[0] - b.v[0], a.v[1] - b.v[1], a.v[2] - b.v[2], a.v[3] - b.v[3]); }
+static inline V4 v4_mul(V4 a, double s) { return v4(a.v[0] * s, a.v[1] * s, a.v[2] * s, a.v[3] * s); }
+
+/* geodesic/state.hpp:19-41 */
+static inline TS ts_add(TS a, TS b) { TS o = {v4_add(a.x, b.x), v4_add(a.k, b.k), v4_add(a.e1, b.e1), v4_add(a.e2, b.e2)}; return o; }
+static inline TS ts_mul(TS a, double s) { TS o = {v4_mul(a.x, s), v4_mul(a.k, s), v4_mul(a.e1, s), v4_mul(a.e2, s)}; return o; }
+static inline TS ts_axpy(TS y, double a, TS x) { return ts_add(y, ts_mul(x, a)); }
+
+/* ---- geometry/kerr_schild_cartesian.hpp ------------------------------ */
+typedef struct { double mass, spin; } KS;
+typedef struct {
+    double x, y, z, a, a2, r, r2, sqsum, discr, denom, amp, amp_r;
+    double l[4];
+} KSWork;
+
+static KSWork ks_build_work(const KS* m, const V4* X) { /* :27-51 */
+    KSWork w;
+    w.x = X->v[1];
+    w.y = X->v[2];
+    w.z = X->v[3];
+    w.a = m->spin;
+    w.a2 = m->spin * m->spin;
+    const double radius2 = w.x * w.x + w.y * w.y + w.z * w.z;
+    w.sqsum = radius2 - w.a2;
+    w.discr = sqrt(w.sqsum * w.sqsum + 4.0 * w.a2 * w.z * w.z);
+    w.r2 = 0.5 * (w.sqsum + w.discr);
+    w.r = sqrt(max_val(w.r2, TINY));
+    w.denom = w.r2 * w.r2 + w.a2 * w.z * w.z;
+    w.amp = 2.0 * m->mass * w.r2 * w.r / w.denom;
+    w.amp_r = -2.0 * m->mass * w.r2 * (w.r2 * w.r2 - 3.0 * w.a2 * w.z * w.z) / (w.denom * w.denom);
+    const double r2pa2 = w.r2 + w.a2;
+    w.l[0] = 1.0;
+    w.l[1] = (w.r * w.x + w.a * w.y) / r2pa2;
+    w.l[2] = (w.r * w.y - w.a * w.x) / r2pa2;
+    w.l[3] = w.z / w.r;
+    return w;
+}
+
+static inline double ks_eta(int mu, int nu) { /* :53-58 */
+    if (mu != nu) return 0.0;
+    return mu == 0 ? -1.0 : 1.0;
+}
+
+static inline double ks_gcov(const KS* m, int mu, int nu, const V4* X) { /* :60-63 */
+    const KSWork w = ks_build_work(m, X);
+    return ks_eta(mu, nu) + w.amp * w.l[mu] * w.l[nu];
+}
+
+static inline double ks_gcon(const KS* m, int mu, int nu, const V4* X) { /* :65-70 */
+    const KSWork w = ks_build_work(m, X);
+    const double lmu = (mu == 0 ? -w.l[0] : w.l[mu]);
+    const double lnu = (nu == 0 ? -w.l[0] : w.l[nu]);
+    return ks_eta(mu, nu) - w.amp * lmu * lnu;
+}
+
+static void ks_gcov_matrix(const KS* m, const V4* X, double g[4][4]) { /* :72-79 */
+    const KSWork w = ks_build_work(m, X);
+    for (int mu = 0; mu < NDIM; ++mu)
+        for (int nu = 0; nu < NDIM; ++nu)
+            g[mu][nu] = ks_eta(mu, nu) + w.amp * w.l[mu] * w.l[nu];
+}
+
+static double ks_dot(const KS* m, const V4* X, const V4* u, const V4* v) { /* :92-108 */
+    const KSWork w = ks_build_work(m, X);
+    double eta_dot = 0.0;
+    for (int mu = 0; mu < NDIM; ++mu) eta_dot += ks_eta(mu, mu) * u->v[mu] * v->v[mu];
+    double lu = 0.0, lv = 0.0;
+    for (int mu = 0; mu < NDIM; ++mu) {
+        lu += w.l[mu] * u->v[mu];
+        lv += w.l[mu] * v->v[mu];
+    }
+    return eta_dot + w.amp * lu * lv;
+}
+
+static inline double ks_horizon(const KS* m) { /* :183-185 */
+    return m->mass + sqrt(max_val(m->mass * m->mass - m->spin * m->spin, 0.0));
+}
+
+typedef struct { double amp; double damp[4]; double l[4]; double lcon[4]; double dl[4][4]; } KSConn;
+
+static KSConn ks_conn_work(const KS* m, const V4* X) { /* :198-252 */
+    const KSWork w = ks_build_work(m, X);
+    KSConn c;
+    c.amp = w.amp;
+    for (int mu = 0; mu < NDIM; ++mu) {
+        c.l[mu] = w.l[mu];
+        c.lcon[mu] = (mu == 0 ? -w.l[0] : w.l[mu]);
+        c.damp[mu] = 0.0;
+        for (int a = 0; a < NDIM; ++a) c.dl[mu][a] = 0.0;
+    }
+    const double r2pa2 = w.r2 + w.a2;
+    const double r2pa2_2 = r2pa2 * r2pa2;
+    const double inv_2r = 0.5 / w.r;
+    double dr[4] = {0.0, 0.0, 0.0, 0.0};
+    dr[1] = (w.x + w.sqsum * w.x / w.discr) * inv_2r;
+    dr[2] = (w.y + w.sqsum * w.y / w.discr) * inv_2r;
+    dr[3] = (w.z + (w.sqsum * w.z + 2.0 * w.a2 * w.z) / w.discr) * inv_2r;
+    c.damp[1] = w.amp_r * dr[1];
+    c.damp[2] = w.amp_r * dr[2];
+    c.damp[3] = 6.0 * m->mass * w.r2 * dr[3] / w.denom -
+                w.amp / w.denom * (4.0 * w.r * w.r2 * dr[3] + 2.0 * w.a2 * w.z);
+    c.dl[1][1] = ((w.r + w.x * dr[1]) * r2pa2 - 2.0 * w.r * (w.r * w.x + w.a * w.y) * dr[1]) / r2pa2_2;
+    c.dl[2][1] = ((-w.a + w.y * dr[1]) * r2pa2 - 2.0 * w.r * (w.r * w.y - w.a * w.x) * dr[1]) / r2pa2_2;
+    c.dl[3][1] = -w.z / w.r2 * dr[1];
+    c.dl[1][2] = ((w.a + w.x * dr[2]) * r2pa2 - 2.0 * w.r * (w.r * w.x + w.a * w.y) * dr[2]) / r2pa2_2;
+    c.dl[2][2] = ((w.r + w.y * dr[2]) * r2pa2 - 2.0 * w.r * (w.r * w.y - w.a * w.x) * dr[2]) / r2pa2_2;
+    c.dl[3][2] = -w.z / w.r2 * dr[2];
+    c.dl[1][3] = (w.x * dr[3] * r2pa2 - 2.0 * w.r * (w.r * w.x + w.a * w.y) * dr[3]) / r2pa2_2;
+    c.dl[2][3] = (w.y * dr[3] * r2pa2 - 2.0 * w.r * (w.r * w.y - w.a * w.x) * dr[3]) / r2pa2_2;
+    c.dl[3][3] = (w.r - w.z * dr[3]) / w.r2;
+    return c;
+}
+
+static inline double ks_l_dot(const KSConn* c, const V4* v) { /* :255-262 */
+    double o = 0.0;
+    for (int mu = 0; mu < NDIM; ++mu) o += c->l[mu] * v->v[mu];
+    return o;
+}
+static inline double ks_dl_dot(const KSConn* c, int alpha, const V4* v) { /* :264-272 */
+    double o = 0.0;
+    for (int mu = 0; mu < NDIM; ++mu) o += c->dl[mu][alpha] * v->v[mu];
+    return o;
+}
+static inline double ks_row_dot(const KSConn* c, int alpha, int row, const V4* v) { /* :274-286 */
+    if (alpha == 0) return 0.0;
+    const double lv = ks_l_dot(c, v);
+    const double dlv = ks_dl_dot(c, alpha, v);
+    return c->damp[alpha] * c->l[row] * lv + c->amp * (c->dl[row][alpha] * lv + c->l[row] * dlv);
+}
+static inline double ks_bilinear(const KSConn* c, int alpha, const V4* p, const V4* q) { /* :288-300 */
+    if (alpha == 0) return 0.0;
+    const double lp = ks_l_dot(c, p), lq = ks_l_dot(c, q);
+    const double dlp = ks_dl_dot(c, alpha, p), dlq = ks_dl_dot(c, alpha, q);
+    return c->damp[alpha] * lp * lq + c->amp * (dlp * lq + lp * dlq);
+}
+static V4 ks_contract(const KSConn* c, const V4* p, const V4* q) { /* :302-327 */
+    double t[4];
+    for (int nu = 0; nu < NDIM; ++nu) {
+        double term = 0.0;
+        for (int alpha = 1; alpha < NDIM; ++alpha)
+            term += p->v[alpha] * ks_row_dot(c, alpha, nu, q) + q->v[alpha] * ks_row_dot(c, alpha, nu, p);
+        term -= ks_bilinear(c, nu, p, q);
+        t[nu] = term;
+    }
+    double lt = 0.0;
+    for (int nu = 0; nu < NDIM; ++nu) lt += c->lcon[nu] * t[nu];
+    V4 out;
+    for (int mu = 0; mu < NDIM; ++mu) {
+        const double eta_term = (mu == 0 ? -t[mu] : t[mu]);
+        out.v[mu] = 0.5 * (eta_term - c->amp * c->lcon[mu] * lt);
+    }
+    return out;
+}
+
+static TS ks_rhs(const KS* m, const TS* s) { /* :347-363 */
+    TS d;
+    d.x = s->k;
+    const KSConn c = ks_conn_work(m, &s->x);
+    const V4 ck = ks_contract(&c, &s->k, &s->k);
+    const V4 ce1 = ks_contract(&c, &s->k, &s->e1);
+    const V4 ce2 = ks_contract(&c, &s->k, &s->e2);
+    for (int mu = 0; mu < NDIM; ++mu) {
+        d.k.v[mu] = -ck.v[mu];
+        d.e1.v[mu] = -ce1.v[mu];
+        d.e2.v[mu] = -ce2.v[mu];
+    }
+    return d;
+}
+
+static inline double ks_radius(const KS* m, const V4* x) { /* metric_domain.hpp:159-172 */
+    return ks_build_work(m, x).r;
+}
+
+/* ---- geodesic/rk4.hpp ------------------------------------------------- */
+static TS rk4_from_k1(const KS* m, const TS* s, double h, const TS* k1) { /* :49-59 */
+    const TS a2 = ts_axpy(*s, 0.5 * h, *k1);
+    const TS k2 = ks_rhs(m, &a2);
+    const TS a3 = ts_axpy(*s, 0.5 * h, k2);
+    const TS k3 = ks_rhs(m, &a3);
+    const TS a4 = ts_axpy(*s, h, k3);
+    const TS k4 = ks_rhs(m, &a4);
+    const TS sum = ts_add(ts_add(ts_add(*k1, ts_mul(k2, 2.0)), ts_mul(k3, 2.0)), k4);
+    return ts_add(*s, ts_mul(sum, h / 6.0));
+}
+
+static TS rk4_step(const KS* m, const TS* s, double h) { /* :36-46 */
+    const TS k1 = ks_rhs(m, s);
+    return rk4_from_k1(m, s, h, &k1);
+}
+
+static double state_error_norm(const TS* a, const TS* b) { /* :75-90 */
+    double err = 0.0;
+    for (int mu = 0; mu < NDIM; ++mu) {
+        const double sx = max_val(1.0, max_val(abs_val(a->x.v[mu]), abs_val(b->x.v[mu])));
+        const double sk = max_val(1.0, max_val(abs_val(a->k.v[mu]), abs_val(b->k.v[mu])));
+        const double se1 = max_val(1.0, max_val(abs_val(a->e1.v[mu]), abs_val(b->e1.v[mu])));
+        const double se2 = max_val(1.0, max_val(abs_val(a->e2.v[mu]), abs_val(b->e2.v[mu])));
+        err = max_val(err, abs_val(a->x.v[mu] - b->x.v[mu]) / sx);
+        err = max_val(err, abs_val(a->k.v[mu] - b->k.v[mu]) / sk);
+        err = max_val(err, abs_val(a->e1.v[mu] - b->e1.v[mu]) / se1);
+        err = max_val(err, abs_val(a->e2.v[mu] - b->e2.v[mu]) / se2);
+    }
+    return err;
+}
+
+typedef struct { double tolerance, min_step, max_step; int max_attempts; } ACtl;
+typedef struct { TS state, mid_state; double used_h, next_h, error; int accepted; } AStep;
+
+static AStep adaptive_rk4_step(const KS* m, const TS* state, double requested_h, ACtl ctl) { /* :108-161 */
+    AStep out;
+    double h = min_val(max_val(abs_val(requested_h), ctl.min_step), ctl.max_step);
+    if (requested_h < 0.0) h = -h;
+    double last_err = LARGE;
+    for (int attempt = 0; attempt < ctl.max_attempts; ++attempt) {
+        const TS k1 = ks_rhs(m, state);
+        const TS full = rk4_from_k1(m, state, h, &k1);
+        const TS half = rk4_from_k1(m, state, h * 0.5, &k1);
+        const TS two_half = rk4_step(m, &half, h * 0.5);
+        const double err = state_error_norm(&full, &two_half);
+        last_err = err;
+        const double tol = max_val(ctl.tolerance, tol_floor());
+        if (err <= tol) {
+            double factor = 2.0;
+            if (err > 0.0) {
+                factor = 0.9 * pow(tol / err, 0.2);
+                factor = min_val(2.0, max_val(0.2, factor));
+            }
+            out.state = two_half;
+            out.mid_state = half;
+            out.used_h = h;
+            out.next_h = min_val(ctl.max_step, max_val(ctl.min_step, abs_val(h) * factor));
+            if (requested_h < 0.0) out.next_h = -out.next_h;
+            out.error = err;
+            out.accepted = 1;
+            return out;
+        }
+        if (abs_val(h) <= ctl.min_step * 1.0001) break;
+        double factor = 0.9 * pow(tol / max_val(err, TINY), 0.25);
+        factor = min_val(0.8, max_val(0.1, factor));
+        h *= factor;
+    }
+    const double next_abs = max_val(ctl.min_step, abs_val(h) * 0.5);
+    out.state = *state;
+    out.mid_state = *state;
+    out.used_h = 0.0;
+    out.next_h = requested_h < 0.0 ? -next_abs : next_abs;
+    out.error = last_err;
+    out.accepted = 0;
+    return out;
+}
+
+static TS lincomb(const TS* s, double h, int n, const TS* const* k, const double* c) {
+    /* state + (k1*c1 + k2*c2 + ...) * h, left to right (rk4.hpp:181-213). */
+    TS acc = ts_mul(*k[0], c[0]);
+    for (int i = 1; i < n; ++i) acc = ts_add(acc, ts_mul(*k[i], c[i]));
+    return ts_add(*s, ts_mul(acc, h));
+}
+
+static AStep adaptive_ck_step(const KS* m, const TS* state, double requested_h, ACtl ctl) { /* :163-250 */
+    AStep out;
+    double h = min_val(max_val(abs_val(requested_h), ctl.min_step), ctl.max_step);
+    if (requested_h < 0.0) h = -h;
+    double last_err = LARGE;
+    for (int attempt = 0; attempt < ctl.max_attempts; ++attempt) {
+        const TS k1 = ks_rhs(m, state);
+        const TS s2 = ts_axpy(*state, h * 1.0 / 5.0, k1);
+        const TS k2 = ks_rhs(m, &s2);
+        const TS* a3[] = {&k1, &k2};
+        const double c3[] = {3.0 / 40.0, 9.0 / 40.0};
+        const TS s3 = lincomb(state, h, 2, a3, c3);
+        const TS k3 = ks_rhs(m, &s3);
+        const TS* a4[] = {&k1, &k2, &k3};
+        const double c4[] = {3.0 / 10.0, -9.0 / 10.0, 6.0 / 5.0};
+        const TS s4 = lincomb(state, h, 3, a4, c4);
+        const TS k4 = ks_rhs(m, &s4);
+        const TS* a5[] = {&k1, &k2, &k3, &k4};
+        const double c5[] = {-11.0 / 54.0, 5.0 / 2.0, -70.0 / 27.0, 35.0 / 27.0};
+        const TS s5 = lincomb(state, h, 4, a5, c5);
+        const TS k5 = ks_rhs(m, &s5);
+        const TS* a6[] = {&k1, &k2, &k3, &k4, &k5};
+        const double c6[] = {1631.0 / 55296.0, 175.0 / 512.0, 575.0 / 13824.0, 44275.0 / 110592.0, 253.0 / 4096.0};
+        const TS s6 = lincomb(state, h, 5, a6, c6);
+        const TS k6 = ks_rhs(m, &s6);
+        const TS* a5th[] = {&k1, &k3, &k4, &k6};
+        const double c5th[] = {37.0 / 378.0, 250.0 / 621.0, 125.0 / 594.0, 512.0 / 1771.0};
+        const TS fifth = lincomb(state, h, 4, a5th, c5th);
+        const TS* a4th[] = {&k1, &k3, &k4, &k5, &k6};
+        const double c4th[] = {2825.0 / 27648.0, 18575.0 / 48384.0, 13525.0 / 55296.0, 277.0 / 14336.0, 1.0 / 4.0};
+        const TS fourth = lincomb(state, h, 5, a4th, c4th);
+        const double err = state_error_norm(&fifth, &fourth);
+        last_err = err;
+        const double tol = max_val(ctl.tolerance, tol_floor());
+        if (err <= tol) {
+            double factor = 2.0;
+            if (err > 0.0) {
+                factor = 0.9 * pow(tol / err, 0.2);
+                factor = min_val(2.0, max_val(0.2, factor));
+            }
+            out.state = fifth;
+            out.mid_state = fifth;
+            out.used_h = h;
+            out.next_h = min_val(ctl.max_step, max_val(ctl.min_step, abs_val(h) * factor));
+            if (requested_h < 0.0) out.next_h = -out.next_h;
+            out.error = err;
+            out.accepted = 1;
+            return out;
+        }
+        if (abs_val(h) <= ctl.min_step * 1.0001) break;
+        double factor = 0.9 * pow(tol / max_val(err, TINY), 0.2);
+        factor = min_val(0.8, max_val(0.1, factor));
+        h *= factor;
+    }
+    const double next_abs = max_val(ctl.min_step, abs_val(h) * 0.5);
+    out.state = *state;
+    out.mid_state = *state;
+    out.used_h = 0.0;
+    out.next_h = requested_h < 0.0 ? -next_abs : next_abs;
+    out.error = last_err;
+    out.accepted = 0;
+    return out;
+}
+
+static AStep adaptive_step(int integrator, const KS* m, const TS* s, double h, ACtl ctl) {
+    return integrator == KP_INTEGRATOR_CASH_KARP ? adaptive_ck_step(m, s, h, ctl)
+                                                  : adaptive_rk4_step(m, s, h, ctl);
+}
+
+/* ---- camera/camera.hpp (pinhole, Cartesian KS) ------------------------ */
+static void pixel_offsets(int pixel, const kp_camera_params* cam, double* sx, double* sy) { /* :97-106 */
+    const int i = pixel % cam->nx;
+    const int j = pixel / cam->nx;
+    const double x_extent = cam->xspan > 0.0 ? 2.0 * cam->xspan : cam->fov;
+    const double y_extent = cam->yspan > 0.0 ? 2.0 * cam->yspan
+                          : (cam->xspan > 0.0 ? 2.0 * cam->xspan * (double)cam->ny / (double)cam->nx
+                             : (cam->fov_y > 0.0 ? cam->fov_y : cam->fov));
+    *sx = (((double)i + 0.5) / (double)cam->nx - 0.5) * x_extent + cam->x_offset;
+    *sy = (((double)j + 0.5) / (double)cam->ny - 0.5) * y_extent + cam->y_offset;
+}
+
+static V4 raise_covector(const KS* m, const V4* x, const V4* cov) { /* :240-253 */
+    V4 o;
+    for (int mu = 0; mu < NDIM; ++mu) {
+        double sum = 0.0;
+        for (int nu = 0; nu < NDIM; ++nu) sum += ks_gcon(m, mu, nu, x) * cov->v[nu];
+        o.v[mu] = sum;
+    }
+    return o;
+}
+
+static V4 project_out(const KS* m, const V4* x, V4 a, const V4* b) { /* :255-265 */
+    const double b2 = ks_dot(m, x, b, b);
+    if (abs_val(b2) > TINY) a = v4_sub(a, v4_mul(*b, ks_dot(m, x, &a, b) / b2));
+    return a;
+}
+
+static V4 normalize_basis_vector(const KS* m, const V4* x, V4 v) { /* :267-273 */
+    const double n2 = ks_dot(m, x, &v, &v);
+    const double n = sqrt(max_val(abs_val(n2), TINY));
+    return v4_mul(v, 1.0 / n);
+}
+
+static int levi_civita4(int i, int j, int k, int l) { /* :275-291 */
+    if (i == j || i == k || i == l || j == k || j == l || k == l) return 0;
+    int a[4] = {i, j, k, l};
+    int sign = 1;
+    for (int mm = 0; mm < 4; ++mm)
+        for (int n = mm + 1; n < 4; ++n)
+            if (a[mm] > a[n]) sign = -sign;
+    return sign;
+}
+
+static double tetrad_orientation(const V4* e0, const V4* e1, const V4* e2, const V4* e3) { /* :293-309 */
+    double out = 0.0;
+    for (int i = 0; i < NDIM; ++i)
+        for (int j = 0; j < NDIM; ++j)
+            for (int k = 0; k < NDIM; ++k)
+                for (int l = 0; l < NDIM; ++l)
+                    out += (double)levi_civita4(i, j, k, l) * e0->v[i] * e1->v[j] * e2->v[k] * e3->v[l];
+    return out;
+}
+
+static V4 native_vector_phi0_cks(const KS* m, double v0, double vx1, double vx2, double vphi,
+                                 double radius, double si, double ci) { /* :353-365 */
+    const double vr = radius * vx1;
+    const double vth = PI * vx2;
+    return v4(v0, vr * si + vth * radius * ci - vphi * m->spin * si,
+              vth * m->spin * ci + vphi * radius * si, vr * ci - vth * radius * si);
+}
+
+static V4 ipole_centering_covector_cks(const KS* m, const V4* x) { /* :383-401 */
+    const double xx = x->v[1], yy = x->v[2], zz = x->v[3];
+    const double a2 = m->spin * m->spin;
+    const double radius2 = xx * xx + yy * yy + zz * zz;
+    const double s = radius2 - a2;
+    const double disc = sqrt(max_val(s * s + 4.0 * a2 * zz * zz, TINY));
+    const double r2 = max_val(0.5 * (s + disc), TINY);
+    const double inv_2r2 = 0.5 / r2;
+    const double dx = xx * (1.0 + s / disc) * inv_2r2;
+    const double dy = yy * (1.0 + s / disc) * inv_2r2;
+    const double dz = zz * (1.0 + (s + 2.0 * a2) / disc) * inv_2r2;
+    return v4(1.0, dx, dy, dz);
+}
+
+static V4 normal_observer_velocity(const KS* m, const V4* x) { /* :137-149 */
+    V4 u;
+    for (int mu = 0; mu < NDIM; ++mu) u.v[mu] = -ks_gcon(m, mu, 0, x);
+    const double n2 = ks_dot(m, x, &u, &u);
+    if (n2 < 0.0) u = v4_mul(u, 1.0 / sqrt(-n2));
+    return u;
+}
+
+static V4 normalize_spacelike(const KS* m, const V4* x, V4 e) { /* :219-227 */
+    const double n2 = ks_dot(m, x, &e, &e);
+    if (n2 <= 0.0) return e;
+    return v4_mul(e, 1.0 / sqrt(n2));
+}
+
+static V4 orthogonalize_spacelike(const KS* m, const V4* x, V4 e, const V4* against) { /* :229-237 */
+    const double denom = ks_dot(m, x, against, against);
+    if (abs_val(denom) > TINY) e = v4_sub(e, v4_mul(*against, ks_dot(m, x, &e, against) / denom));
+    return e;
+}
+
+static TS camera_ray_pinhole_cks(const KS* m, int pixel, const kp_camera_params* cam) { /* :485-513 */
+    const double si = sin(cam->inclination);
+    const double ci = cos(cam->inclination);
+    TS st;
+    st.x = v4(0.0, cam->radius * si, m->spin * si, cam->radius * ci); /* :321-324 */
+    /* make_ipole_camera_tetrad :415-453 */
+    V4 e0 = normal_observer_velocity(m, &st.x);
+    const V4 cc = ipole_centering_covector_cks(m, &st.x);
+    V4 e3 = raise_covector(m, &st.x, &cc);
+    V4 e2 = native_vector_phi0_cks(m, 0.0, 0.0, 1.0, 0.0, cam->radius, si, ci);
+    V4 e1 = native_vector_phi0_cks(m, 1.0, 1.0, 1.0, 1.0, cam->radius, si, ci);
+    e0 = normalize_basis_vector(m, &st.x, e0);
+    e3 = project_out(m, &st.x, e3, &e0);
+    e3 = project_out(m, &st.x, e3, &e0);
+    e3 = normalize_basis_vector(m, &st.x, e3);
+    e2 = project_out(m, &st.x, e2, &e0);
+    e2 = project_out(m, &st.x, e2, &e3);
+    e2 = project_out(m, &st.x, e2, &e0);
+    e2 = project_out(m, &st.x, e2, &e3);
+    e2 = normalize_basis_vector(m, &st.x, e2);
+    e1 = project_out(m, &st.x, e1, &e0);
+    e1 = project_out(m, &st.x, e1, &e2);
+    e1 = project_out(m, &st.x, e1, &e3);
+    e1 = project_out(m, &st.x, e1, &e0);
+    e1 = project_out(m, &st.x, e1, &e2);
+    e1 = project_out(m, &st.x, e1, &e3);
+    e1 = normalize_basis_vector(m, &st.x, e1);
+    if (tetrad_orientation(&e0, &e1, &e2, &e3) < 0.0) e1 = v4_mul(e1, -1.0);
+
+    double sx = 0.0, sy = 0.0;
+    pixel_offsets(pixel, cam, &sx, &sy);
+    const double spatial_norm = sqrt(1.0 + sx * sx + sy * sy);
+    const double kt0 = 1.0;
+    const double kt1 = sx / spatial_norm;
+    const double kt2 = sy / spatial_norm;
+    const double kt3 = 1.0 / spatial_norm;
+    const V4 sd = v4_add(v4_add(v4_mul(e1, kt1), v4_mul(e2, kt2)), v4_mul(e3, kt3));
+    st.k = v4_add(v4_mul(e0, kt0), sd);
+    st.e1 = v4_sub(e1, v4_mul(sd, kt1));
+    st.e1 = normalize_spacelike(m, &st.x, st.e1);
+    st.e2 = v4_sub(e2, v4_mul(sd, kt2));
+    st.e2 = orthogonalize_spacelike(m, &st.x, st.e2, &st.e1);
+    st.e2 = normalize_spacelike(m, &st.x, st.e2);
+    return st;
+}
+
+/* ---- radiation/semi_analytic.hpp, frame/stokes_rotation.hpp ----------- */
+static void faraday_rotate(ST* s, const TC* c, double dl) { /* semi_analytic.hpp:10-38 */
+    V3 p = {s->Q, s->U, s->V};
+    const V3 rho = {c->rQ, c->rU, c->rV};
+    const double rho_norm = norm3(rho);
+    if (rho_norm == 0.0 || dl == 0.0) return;
+    const double theta = rho_norm * dl;
+    V3 po;
+    if (abs_val(theta) < 1e-8) {
+        const V3 cr = cross3(rho, p);
+        po.x = p.x + cr.x * dl;
+        po.y = p.y + cr.y * dl;
+        po.z = p.z + cr.z * dl;
+    } else {
+        const double inv = 1.0 / rho_norm;
+        const V3 n = {rho.x * inv, rho.y * inv, rho.z * inv};
+        const double ct = cos(theta);
+        const double st = sin(theta);
+        const double f = dot3(n, p) * (1.0 - ct);
+        const V3 cr = cross3(n, p);
+        po.x = p.x * ct + n.x * f + cr.x * st;
+        po.y = p.y * ct + n.y * f + cr.y * st;
+        po.z = p.z * ct + n.z * f + cr.z * st;
+    }
+    s->Q = po.x;
+    s->U = po.y;
+    s->V = po.z;
+}
+
+static void absorb_emit(ST* s, const TC* c, double dl) { /* semi_analytic.hpp:40-92 */
+    const V3 p = {s->Q, s->U, s->V};
+    const V3 jp = {c->jQ, c->jU, c->jV};
+    const V3 alpha = {c->aQ, c->aU, c->aV};
+    const double an = norm3(alpha);
+    if (an < TINY) {
+        const double e = stable_attenuation(c->aI, dl);
+        const double f = stable_source_factor(c->aI, dl);
+        s->I = e * s->I + f * c->jI;
+        s->Q = e * s->Q + f * c->jQ;
+        s->U = e * s->U + f * c->jU;
+        s->V = e * s->V + f * c->jV;
+        return;
+    }
+    const double inv = 1.0 / an;
+    const V3 n = {alpha.x * inv, alpha.y * inv, alpha.z * inv};
+    const double p_par = dot3(n, p);
+    const V3 p_perp = {p.x - n.x * p_par, p.y - n.y * p_par, p.z - n.z * p_par};
+    const double j_par = dot3(n, jp);
+    const V3 j_perp = {jp.x - n.x * j_par, jp.y - n.y * j_par, jp.z - n.z * j_par};
+    const double s_plus = s->I + p_par;
+    const double s_minus = s->I - p_par;
+    const double j_plus = c->jI + j_par;
+    const double j_minus = c->jI - j_par;
+    const double k_plus = c->aI + an;
+    const double k_minus = c->aI - an;
+    const double sp_out = stable_attenuation(k_plus, dl) * s_plus + stable_source_factor(k_plus, dl) * j_plus;
+    const double sm_out = stable_attenuation(k_minus, dl) * s_minus + stable_source_factor(k_minus, dl) * j_minus;
+    const double e_i = stable_attenuation(c->aI, dl);
+    const double f_i = stable_source_factor(c->aI, dl);
+    const V3 pp_out = {p_perp.x * e_i + j_perp.x * f_i, p_perp.y * e_i + j_perp.y * f_i,
+                       p_perp.z * e_i + j_perp.z * f_i};
+    const double i_out = 0.5 * (sp_out + sm_out);
+    const double ppar_out = 0.5 * (sp_out - sm_out);
+    s->I = i_out;
+    s->Q = n.x * ppar_out + pp_out.x;
+    s->U = n.y * ppar_out + pp_out.y;
+    s->V = n.z * ppar_out + pp_out.z;
+}
+
+static void stokes_step(ST* s, const TC* c, double dl) { /* semi_analytic.hpp:94-100 */
+    faraday_rotate(s, c, 0.5 * dl);
+    absorb_emit(s, c, dl);
+    faraday_rotate(s, c, 0.5 * dl);
+}
+
+static ST to_observer_basis(ST in, const OV* o) { /* stokes_rotation.hpp:39-57 */
+    ST out = in;
+    out.Q = 0.5 * in.Q * (o->r11 * o->r11 - o->r12 * o->r12 - o->r21 * o->r21 + o->r22 * o->r22) +
+            in.U * (o->r11 * o->r12 - o->r21 * o->r22);
+    out.U = in.Q * (o->r11 * o->r21 - o->r12 * o->r22) + in.U * (o->r11 * o->r22 + o->r12 * o->r21);
+    out.V = (o->r11 * o->r22 - o->r12 * o->r21) * in.V;
+    return out;
+}
+
+/* ---- radiation/thermal_synchrotron.hpp -------------------------------- */
+#define EE 4.803204712570263e-10
+#define ME 9.1093837015e-28
+#define CL 2.99792458e10
+#define HPL 6.62607015e-27
+
+static double bessel_i0(double ax) { /* :60-82 */
+    if (ax < 3.75) {
+        double y = ax / 3.75;
+        y *= y;
+        double p = 0.0045813;
+        p = 0.0360768 + y * p;
+        p = 0.2659732 + y * p;
+        p = 1.2067492 + y * p;
+        p = 3.0899424 + y * p;
+        p = 3.5156229 + y * p;
+        return 1.0 + y * p;
+    }
+    double y = 3.75 / ax;
+    double p = 0.00392377;
+    p = -0.01647633 + y * p;
+    p = 0.02635537 + y * p;
+    p = -0.02057706 + y * p;
+    p = 0.00916281 + y * p;
+    p = -0.00157565 + y * p;
+    p = 0.00225319 + y * p;
+    p = 0.01328592 + y * p;
+    p = 0.39894228 + y * p;
+    return exp(ax) / sqrt(ax) * p;
+}
+
+static double bessel_i1(double ax) { /* :84-106 */
+    if (ax < 3.75) {
+        double y = ax / 3.75;
+        y *= y;
+        double p = 0.00032411;
+        p = 0.00301532 + y * p;
+        p = 0.02658733 + y * p;
+        p = 0.15084934 + y * p;
+        p = 0.51498869 + y * p;
+        p = 0.87890594 + y * p;
+        p = 0.5 + y * p;
+        return ax * p;
+    }
+    double y = 3.75 / ax;
+    double p = -0.00420059;
+    p = 0.01787654 + y * p;
+    p = -0.02895312 + y * p;
+    p = 0.02282967 + y * p;
+    p = -0.01031555 + y * p;
+    p = 0.00163801 + y * p;
+    p = -0.00362018 + y * p;
+    p = -0.03988024 + y * p;
+    p = 0.39894228 + y * p;
+    return exp(ax) / sqrt(ax) * p;
+}
+
+static double bessel_k0(double x) { /* :108-132 */
+    if (x <= 0.0) return 1e300;
+    if (x <= 2.0) {
+        double y = x * x * 0.25;
+        double p = 0.00000740;
+        p = 0.00010750 + y * p;
+        p = 0.00262698 + y * p;
+        p = 0.03488590 + y * p;
+        p = 0.23069756 + y * p;
+        p = 0.42278420 + y * p;
+        p = -0.57721566 + y * p;
+        return -log(x * 0.5) * bessel_i0(x) + p;
+    }
+    double y = 2.0 / x;
+    double p = 0.00053208;
+    p = -0.00251540 + y * p;
+    p = 0.00587872 + y * p;
+    p = -0.01062446 + y * p;
+    p = 0.02189568 + y * p;
+    p = -0.07832358 + y * p;
+    p = 1.25331414 + y * p;
+    return exp(-x) / sqrt(x) * p;
+}
+
+static double bessel_k1(double x) { /* :134-158 */
+    if (x <= 0.0) return 1e300;
+    if (x <= 2.0) {
+        double y = x * x * 0.25;
+        double p = -0.00004686;
+        p = -0.00110404 + y * p;
+        p = -0.01919402 + y * p;
+        p = -0.18156897 + y * p;
+        p = -0.67278579 + y * p;
+        p = 0.15443144 + y * p;
+        p = 1.0 + y * p;
+        return log(x * 0.5) * bessel_i1(x) + p / x;
+    }
+    double y = 2.0 / x;
+    double p = -0.00068245;
+    p = 0.00325614 + y * p;
+    p = -0.00780353 + y * p;
+    p = 0.01504268 + y * p;
+    p = -0.03655620 + y * p;
+    p = 0.23498619 + y * p;
+    p = 1.25331414 + y * p;
+    return exp(-x) / sqrt(x) * p;
+}
+
+static void bessel_k012(double x, double* k0, double* k1, double* k2) { /* :214-229 */
+    const double a = bessel_k0(x);
+    const double b = bessel_k1(x);
+    const double c = max_val(a + 2.0 * b / max_val(x, 1e-300), 1e-300);
+    *k0 = a;
+    *k1 = b;
+    *k2 = c;
+}
+
+static double bnu_inv(double nu, double thetae) { /* :233-251 */
+    if (!(thetae > 0.0)) return 0.0;
+    const double x = HPL * nu / (ME * CL * CL * thetae);
+    if (x < 2e-3) {
+        const double denom = x / 24.0 * (24.0 + x * (12.0 + x * (4.0 + x)));
+        return (2.0 * HPL / max_val(denom, TINY)) / (CL * CL);
+    }
+    const double denom = exp(x) - 1.0;
+    return (2.0 * HPL / max_val(denom, TINY)) / (CL * CL);
+}
+
+static double pandya_nu_c(double b) { return EE * b / (2.0 * PI * ME * CL); } /* :314-321 */
+
+static double pandya_x(double nu, double thetae, double b, double sin_theta) { /* :323-329 */
+    const double nu_c = pandya_nu_c(b);
+    const double nu_s = 2.0 / 9.0 * nu_c * sin_theta * thetae * thetae;
+    return max_val(nu / max_val(nu_s, TINY), TINY);
+}
+
+static double pandya_jI(double nu, double ne, double thetae, double b, double st) { /* :331-348 */
+    if (!(thetae > 0.0) || !(ne > 0.0) || !(b > 0.0) || !(st > 0.0)) return 0.0;
+    const double nu_c = pandya_nu_c(b);
+    const double x = pandya_x(nu, thetae, b, st);
+    const double prefactor = ne * EE * EE * nu_c / CL;
+    const double term1 = sqrt(2.0) * PI / 27.0 * st;
+    const double x13 = cbrt(x);
+    const double shape = sqrt(x) + 1.8877486253633869933 * sqrt(x13);
+    const double term2 = shape * shape;
+    return prefactor * term1 * term2 * exp(-x13);
+}
+
+static double pandya_jQ(double nu, double ne, double thetae, double b, double st) { /* :350-370 */
+    if (!(thetae > 0.0) || !(ne > 0.0) || !(b > 0.0) || !(st > 0.0)) return 0.0;
+    const double nu_c = pandya_nu_c(b);
+    const double x = pandya_x(nu, thetae, b, st);
+    const double t2425 = pow(thetae, 24.0 / 25.0);
+    const double prefactor = ne * EE * EE * nu_c / CL;
+    const double term1 = sqrt(2.0) * PI / 27.0 * st;
+    const double term2 = (7.0 * t2425 + 35.0) / (10.0 * t2425 + 75.0);
+    const double x13 = cbrt(x);
+    const double shape = sqrt(x) + term2 * 1.8877486253633869933 * sqrt(x13);
+    const double term3 = shape * shape;
+    return prefactor * term1 * term3 * exp(-x13);
+}
+
+static double pandya_jV(double nu, double ne, double thetae, double b, double st, double ct) { /* :372-395 */
+    if (!(thetae > 0.0) || !(ne > 0.0) || !(b > 0.0) || !(st > 0.0)) return 0.0;
+    const double nu_c = pandya_nu_c(b);
+    const double x = pandya_x(nu, thetae, b, st);
+    const double prefactor = ne * EE * EE * nu_c / CL;
+    const double sin_shift = st * 0.4356824462767121 - ct * 0.9001004421765051;
+    const double term1 = (37.0 - 87.0 * sin_shift) / (100.0 * (thetae + 1.0));
+    const double term2 = pow(1.0 + (pow(thetae, 3.0 / 5.0) / 25.0 + 7.0 / 10.0) * pow(x, 9.0 / 25.0), 5.0 / 3.0);
+    return prefactor * term1 * term2 * exp(-cbrt(x));
+}
+
+static double rho_V_only(double nu, double ne, double thetae, double b, double theta, double min_st) { /* :433-460 */
+    const double st = max_val(sin(theta), min_st);
+    const double omega0 = EE * b / (ME * CL);
+    const double wp2 = 4.0 * PI * ne * EE * EE / ME;
+    const double two_pi_nu = 2.0 * PI * nu;
+    const double x = max_val(thetae * sqrt(max_val(0.0, sqrt(2.0) * st * (1e3 * omega0 / max_val(two_pi_nu, TINY)))), 1e-12);
+    double k0, k1, k2;
+    bessel_k012(1.0 / thetae, &k0, &k1, &k2); /* thermal_bessel_k0k2: same k0, k2 */
+    const double shgm = 1.0 - 0.11 * log(1.0 + 0.035 * x);
+    const double k_ratio = k2 > 0.0 ? k0 / k2 : 1.0;
+    const double fit_factor = k_ratio * shgm;
+    const double safe = max_val(two_pi_nu, TINY);
+    double eps12 = wp2 * omega0;
+    eps12 /= safe;
+    eps12 /= safe;
+    eps12 /= safe;
+    eps12 *= fit_factor * cos(theta);
+    return 2.0 * PI * nu / CL * eps12;
+}
+
+static void rho_QV(double nu, double ne, double thetae, double b, double st, double ct,
+                   double* rhoQ, double* rhoV) { /* :462-506 */
+    const double omega0 = EE * b / (ME * CL);
+    const double wp2 = 4.0 * PI * ne * EE * EE / ME;
+    const double two_pi_nu = 2.0 * PI * nu;
+    const double x = max_val(thetae * sqrt(max_val(0.0, sqrt(2.0) * st * (1e3 * omega0 / max_val(two_pi_nu, TINY)))), 1e-12);
+    double k0, k1, k2;
+    bessel_k012(1.0 / thetae, &k0, &k1, &k2);
+    const double exp_x_47 = exp(-x / 47.2);
+    const double extraterm = (0.011 * exp_x_47 - 369.69342869090815 * pow(x + 1e-16, -8.0 / 3.0)) *
+                             (0.5 + 0.5 * tanh((log(x) - 4.787491742782046) / 0.1));
+    const double jffunc = 2.011 * exp(-pow(x, 1.035) / 4.7) - cos(x / 2.0) * exp(-pow(x, 1.2) / 2.73) -
+                          0.011 * exp_x_47 + extraterm;
+    const double k1_ratio = k2 > 0.0 ? k1 / k2 : 1.0;
+    const double safe = max_val(two_pi_nu, TINY);
+    double eps11m22 = jffunc * wp2 * omega0 * omega0;
+    eps11m22 /= safe;
+    eps11m22 /= safe;
+    eps11m22 /= safe;
+    eps11m22 /= safe;
+    eps11m22 *= (k1_ratio + 6.0 * thetae) * st * st;
+    *rhoQ = PI * nu / CL * eps11m22;
+    const double shgm = 1.0 - 0.11 * log(1.0 + 0.035 * x);
+    const double k0_ratio = k2 > 0.0 ? k0 / k2 : 1.0;
+    const double fit_factor = k0_ratio * shgm;
+    double eps12 = wp2 * omega0;
+    eps12 /= safe;
+    eps12 /= safe;
+    eps12 /= safe;
+    eps12 *= fit_factor * ct;
+    *rhoV = 2.0 * PI * nu / CL * eps12;
+}
+
+typedef struct { double nu, ne, thetae, b, theta, st, ct; } ThermalState;
+typedef struct { int fit; double max_pol_frac, min_sin_theta, emission_scale, absorption_scale, faraday_scale; } ThermalParams;
+
+static TC thermal_coefficients(const ThermalState* s, const ThermalParams* p) { /* :512-627 */
+    TC c;
+    memset(&c, 0, sizeof c);
+    if (!(s->nu > 0.0) || !(s->ne > 0.0) || !(s->thetae > 0.0) || !(s->b > 0.0)) return c;
+    const double nu = max_val(s->nu, 1.0);
+    const double st = max_val(s->st, p->min_sin_theta);
+    double jI = 0.0, jQ = 0.0, jV = 0.0;
+    if (p->fit == KP_FIT_DEXTER) { /* :530-564 */
+        const double nus = 3.0 * EE * s->b * st / (4.0 * PI * ME * CL) * s->thetae * s->thetae + 1.0;
+        const double x = max_val(nu / max_val(nus, TINY), TINY);
+        const double xm13 = 1.0 / cbrt(x);
+        const double exp_shape = exp(-1.8899 / xm13);
+        const double pref = s->ne * EE * EE * nu / (2.0 * sqrt(3.0) * CL * s->thetae * s->thetae);
+        const double i_val = 2.5651 * (1.0 + 1.92 * xm13 + 0.9977 * xm13 * xm13) * exp_shape;
+        const double iq = 2.5651 * (1.0 + 0.93193 * xm13 + 0.499873 * xm13 * xm13) * exp_shape;
+        jI = pref * i_val;
+        jQ = pref * iq;
+        const double stv = st;
+        const double nusv = 3.0 * EE * s->b * stv / (4.0 * PI * ME * CL) * s->thetae * s->thetae + 1.0;
+        const double xv = max_val(nu / max_val(nusv, TINY), TINY);
+        const double xvm13 = 1.0 / cbrt(xv);
+        const double iv = (1.81384 / xv + 3.42319 * xvm13 * xvm13 + 0.0292545 / sqrt(xv) + 2.03773 * xvm13) *
+                          exp(-1.8899 / xvm13);
+        double cft = s->ct;
+        if (abs_val(cft) < 1e-10) cft = cft >= 0.0 ? 1e-10 : -1e-10;
+        const double tan_theta = stv / cft;
+        jV = 2.0 * s->ne * EE * EE * nu /
+             (tan_theta * 3.0 * sqrt(3.0) * CL * s->thetae * s->thetae * s->thetae) * iv;
+    } else {
+        jI = pandya_jI(nu, s->ne, s->thetae, s->b, st);
+        jQ = pandya_jQ(nu, s->ne, s->thetae, s->b, st);
+        jV = pandya_jV(nu, s->ne, s->thetae, s->b, st, s->ct);
+    }
+    const double nusq = nu * nu;
+    double jI_inv = jI / max_val(nusq, TINY);
+    double jQ_inv = jQ / max_val(nusq, TINY);
+    double jV_inv = jV / max_val(nusq, TINY);
+    const double jP_scale = max_val(abs_val(jQ_inv), abs_val(jV_inv));
+    const double jP = jP_scale > 0.0 ? jP_scale * sqrt(square(jQ_inv / jP_scale) + square(jV_inv / jP_scale)) : 0.0;
+    if (jI_inv > 0.0 && jP > 0.0 && jI_inv < jP / max_val(p->max_pol_frac, 1e-30)) {
+        const double scale = jI_inv / jP * p->max_pol_frac;
+        jQ_inv *= scale;
+        jV_inv *= scale;
+    }
+    double aI = 0.0, aQ = 0.0, aV = 0.0;
+    const double b_inv = bnu_inv(nu, s->thetae);
+    if (b_inv > 0.0) {
+        aI = jI_inv / b_inv;
+        aQ = jQ_inv / b_inv;
+        aV = jV_inv / b_inv;
+    }
+    double rQ = 0.0, rV = 0.0;
+    rho_QV(nu, s->ne, s->thetae, s->b, st, s->ct, &rQ, &rV);
+    c.jI = p->emission_scale * jI_inv;
+    c.jQ = p->emission_scale * jQ_inv;
+    c.jV = p->emission_scale * jV_inv;
+    c.aI = p->absorption_scale * aI;
+    c.aQ = p->absorption_scale * aQ;
+    c.aV = p->absorption_scale * aV;
+    c.rQ = p->faraday_scale * (rQ * nu);
+    c.rV = p->faraday_scale * (rV * nu);
+    return c;
+}
+
+/* ---- model/riaf.hpp (Cartesian KS) ------------------------------------ */
+static double density_profile_bl(const kp_riaf_model* m, double r, double th) { /* :54-60 */
+    const double zc = r * cos(th);
+    const double rc = max_val(r * sin(th), m->min_radius);
+    const double h = max_val(m->disk_h, 1e-6);
+    const double vertical = exp(-(zc * zc) / (2.0 * rc * rc * h * h));
+    return m->nth0 * vertical * pow(max_val(r, m->min_radius), m->pow_nth);
+}
+
+static double thetae_profile(const kp_riaf_model* m, double r) { /* :67-74 */
+    const double kbol = 1.380649e-16;
+    const double thetae_unit = m->te_unit * kbol / (ME * CL * CL);
+    return max_val(m->Te0 * pow(max_val(r, m->min_radius), m->pow_T) * thetae_unit, m->min_thetae);
+}
+
+static double riaf_length_unit(const kp_riaf_model* m) { /* :76-81 */
+    const double gnewt = 6.67430e-8;
+    const double msun = 1.98847e33;
+    return gnewt * m->mbh_solar * msun / (CL * CL);
+}
+
+static double riaf_dlambda_scale(const kp_riaf_model* m, double freq) { /* :83-85 */
+    return riaf_length_unit(m) / max_val(freq, 1.0);
+}
+
+static double magnetic_field_cgs(const kp_riaf_model* m, double ne, double r) { /* :87-96 */
+    const double mp = 1.67262192369e-24;
+    const double eps = 0.1;
+    const double b = sqrt(max_val(8.0 * PI * eps * ne * mp * CL * CL / (6.0 * max_val(r, m->min_radius)), 0.0));
+    return max_val(b, 1e-12);
+}
+
+static void bl_coordinates(const V4* x, double spin, double* r, double* th, double* cphi, double* sphi) { /* :98-122 */
+    const double xx = x->v[1], yy = x->v[2], zz = x->v[3];
+    const double a2 = spin * spin;
+    const double radius2 = xx * xx + yy * yy + zz * zz;
+    const double sqsum = radius2 - a2;
+    const double discr = sqrt(sqsum * sqsum + 4.0 * a2 * zz * zz);
+    *r = sqrt(max_val(0.5 * (sqsum + discr), TINY));
+    *th = acos(clamp(zz / max_val(*r, TINY), -1.0, 1.0));
+    const double sinth = max_val(sin(*th), 1e-30);
+    const double denom = max_val(sinth * (*r * *r + a2), TINY);
+    double cp = (*r * xx + spin * yy) / denom;
+    double sp = (*r * yy - spin * xx) / denom;
+    const double normp = sqrt(max_val(cp * cp + sp * sp, TINY));
+    cp /= normp;
+    sp /= normp;
+    *cphi = cp;
+    *sphi = sp;
+}
+
+static void bl_metric(double r, double th, double spin, double gcov[4][4], double gcon[4][4]) { /* :138-164 */
+    const double a = spin;
+    const double a2 = a * a;
+    const double sinth = sin(th);
+    const double sin2 = max_val(sinth * sinth, 1e-30);
+    const double costh = cos(th);
+    const double sigma = r * r + a2 * costh * costh;
+    const double delta = r * r - 2.0 * r + a2;
+    for (int mu = 0; mu < 4; ++mu)
+        for (int nu = 0; nu < 4; ++nu) {
+            gcov[mu][nu] = 0.0;
+            gcon[mu][nu] = 0.0;
+        }
+    gcov[0][0] = -(1.0 - 2.0 * r / sigma);
+    gcov[0][3] = gcov[3][0] = -2.0 * a * r * sin2 / sigma;
+    gcov[1][1] = sigma / max_val(delta, TINY);
+    gcov[2][2] = sigma;
+    gcov[3][3] = (r * r + a2 + 2.0 * a2 * r * sin2 / sigma) * sin2;
+    const double inv_sd = 1.0 / max_val(sigma * delta, TINY);
+    gcon[0][0] = -((r * r + a2) * (r * r + a2) - a2 * delta * sin2) * inv_sd;
+    gcon[0][3] = gcon[3][0] = -2.0 * a * r * inv_sd;
+    gcon[1][1] = delta / sigma;
+    gcon[2][2] = 1.0 / sigma;
+    gcon[3][3] = (delta - a2 * sin2) / max_val(sigma * delta * sin2, TINY);
+}
+
+static double isco_radius(double spin) { /* :166-174 */
+    const double a = spin;
+    const double one = 1.0;
+    const double z1 = one + cbrt(one - a * a) * (cbrt(one + a) + cbrt(one - a));
+    const double z2 = sqrt(3.0 * a * a + z1 * z1);
+    const double sign = a < 0.0 ? -1.0 : 1.0;
+    return 3.0 + z2 - sign * sqrt((3.0 - z1) * (3.0 + z1 + 2.0 * z2));
+}
+
+static double signed_nonzero(double x) { /* :176-182 */
+    if (abs_val(x) > TINY) return x;
+    return x < 0.0 ? -TINY : TINY;
+}
+
+static V4 bl_to_cks_vector(double vt, double vr, double vth, double vphi, double r, double th,
+                           double cphi, double sphi, double spin) { /* :184-204 */
+    const double a = spin;
+    const double delta = max_val(r * r - 2.0 * r + a * a, TINY);
+    const double vt_ks = vt + 2.0 * r / delta * vr;
+    const double vphi_ks = vphi + a / delta * vr;
+    const double sinth = sin(th);
+    const double costh = cos(th);
+    const double dx_dr = cphi * sinth;
+    const double dy_dr = sphi * sinth;
+    const double dz_dr = costh;
+    const double dx_dth = (r * cphi - a * sphi) * costh;
+    const double dy_dth = (r * sphi + a * cphi) * costh;
+    const double dz_dth = -r * sinth;
+    const double dx_dphi = (-r * sphi - a * cphi) * sinth;
+    const double dy_dphi = (r * cphi - a * sphi) * sinth;
+    const double dz_dphi = 0.0;
+    return v4(vt_ks, vr * dx_dr + vth * dx_dth + vphi_ks * dx_dphi,
+              vr * dy_dr + vth * dy_dth + vphi_ks * dy_dphi,
+              vr * dz_dr + vth * dz_dth + vphi_ks * dz_dphi);
+}
+
+static double dot_g(const double g[4][4], const V4* u, const V4* v) { /* :286-296 */
+    double out = 0.0;
+    for (int mu = 0; mu < 4; ++mu)
+        for (int nu = 0; nu < 4; ++nu) out += g[mu][nu] * u->v[mu] * v->v[nu];
+    return out;
+}
+
+static V4 lower_g(const double g[4][4], const V4* v) { /* :298-309 */
+    V4 o;
+    for (int mu = 0; mu < 4; ++mu) {
+        double sum = 0.0;
+        for (int nu = 0; nu < 4; ++nu) sum += g[mu][nu] * v->v[nu];
+        o.v[mu] = sum;
+    }
+    return o;
+}
+
+static V4 fluid_velocity(const kp_riaf_model* md, const KS* m, double r, double th, double cphi,
+                         double sphi, const double mg[4][4]) { /* :206-273 */
+    const double rh = ks_horizon(m);
+    const double risco = isco_radius(m->spin);
+    double gcov[4][4], gcon[4][4];
+    bl_metric(r, th, m->spin, gcov, gcon);
+    double vt = 1.0, vr = 0.0, vth = 0.0, vphi = 0.0;
+    if (r < rh) {
+        vt = 1.0 / sqrt(max_val(-gcon[0][0], TINY));
+    } else if (r < risco) {
+        double gi[4][4], gci[4][4];
+        bl_metric(risco, th, m->spin, gi, gci);
+        const double omega_isco = 1.0 / (risco * sqrt(risco) + m->spin);
+        const double qi = gi[0][0] + 2.0 * omega_isco * gi[0][3] + omega_isco * omega_isco * gi[3][3];
+        const double ut_i = 1.0 / sqrt(max_val(-qi, TINY));
+        const double e = (gi[0][0] + gi[0][3] * omega_isco) * ut_i;
+        const double l = (gi[3][0] + gi[3][3] * omega_isco) * ut_i;
+        const double k_con = gcon[0][0] * e * e + 2.0 * gcon[0][3] * e * l + gcon[3][3] * l * l;
+        const double ur_cov = -sqrt(max_val(-(1.0 + k_con) / max_val(gcon[1][1], TINY), 0.0));
+        const double vr_tmp = gcon[1][1] * ur_cov;
+        const double vt_tmp = gcon[0][0] * e + gcon[0][3] * l;
+        const double vphi_tmp = gcon[3][0] * e + gcon[3][3] * l;
+        const double omega_k = vphi_tmp / max_val(vt_tmp, TINY);
+        const double omega_ff = gcon[0][3] / signed_nonzero(gcon[0][0]);
+        const double omega = omega_k + (1.0 - md->keplerian_factor) * (omega_ff - omega_k);
+        const double ur_ff = -sqrt(max_val(-(1.0 + gcon[0][0]) * gcon[1][1], 0.0));
+        vr = vr_tmp + md->infall_factor * (ur_ff - vr_tmp);
+        const double q = gcov[0][0] + 2.0 * omega * gcov[0][3] + omega * omega * gcov[3][3];
+        vt = sqrt(max_val(-(1.0 + vr * vr * gcov[1][1]) / q, 0.0));
+        vphi = omega * vt;
+    } else {
+        const double r_eff = max_val(r, md->min_radius);
+        const double omega_k = 1.0 / (r_eff * sqrt(r_eff) + m->spin);
+        const double omega_ff = gcon[0][3] / signed_nonzero(gcon[0][0]);
+        const double omega = omega_k + (1.0 - md->keplerian_factor) * (omega_ff - omega_k);
+        vr = md->infall_factor * -sqrt(max_val(-(1.0 + gcon[0][0]) * gcon[1][1], 0.0));
+        const double q = gcov[0][0] + 2.0 * omega * gcov[0][3] + omega * omega * gcov[3][3];
+        vt = sqrt(max_val(-(1.0 + vr * vr * gcov[1][1]) / q, 0.0));
+        vphi = omega * vt;
+    }
+    V4 u = bl_to_cks_vector(vt, vr, vth, vphi, r, th, cphi, sphi, m->spin);
+    const double n2 = dot_g(mg, &u, &u);
+    if (n2 < 0.0) u = v4_mul(u, 1.0 / sqrt(max_val(-n2, TINY)));
+    return u;
+}
+
+static double screen_inner(const double g[4][4], const V4* u, const V4* k, const V4* a, const V4* b) { /* :320-336 */
+    const double uk = dot_g(g, u, k);
+    if (abs_val(uk) <= TINY) return dot_g(g, a, b);
+    const V4 eK = v4_sub(v4_mul(*k, -1.0 / uk), *u);
+    return dot_g(g, a, b) + dot_g(g, u, a) * dot_g(g, u, b) - dot_g(g, &eK, a) * dot_g(g, &eK, b);
+}
+
+static V4 magnetic_unit(const KS* m, const V4* x, const V4* ucon, const double g[4][4]) { /* :350-386 */
+    double r, th, cp, sp;
+    bl_coordinates(x, m->spin, &r, &th, &cp, &sp);
+    V4 bt = bl_to_cks_vector(0.0, 0.0, 0.0, 1.0, r, th, cp, sp, m->spin);
+    const double udotb = dot_g(g, ucon, &bt);
+    V4 bcon = v4_add(bt, v4_mul(*ucon, udotb));
+    double bsq = dot_g(g, &bcon, &bcon);
+    if (!(bsq > 1e-30)) {
+        bt = v4(0.0, 0.0, 0.0, 1.0);
+        const double udz = dot_g(g, ucon, &bt);
+        bcon = v4_add(bt, v4_mul(*ucon, udz));
+        bsq = dot_g(g, &bcon, &bcon);
+    }
+    if (!(bsq > 1e-30)) {
+        bt = v4(0.0, 1.0, 0.0, 0.0);
+        const double udx = dot_g(g, ucon, &bt);
+        bcon = v4_add(bt, v4_mul(*ucon, udx));
+        bsq = dot_g(g, &bcon, &bcon);
+    }
+    if (bsq > 1e-30) bcon = v4_mul(bcon, 1.0 / sqrt(bsq));
+    return bcon;
+}
+
+static TC riaf_coefficients(const kp_riaf_model* md, double freq, const KS* m, const TS* s) { /* :410-549 */
+    TC c;
+    memset(&c, 0, sizeof c);
+    double rc = 0.0, thc = 0.0, cp = 1.0, sp = 0.0;
+    bl_coordinates(&s->x, m->spin, &rc, &thc, &cp, &sp);
+    const double r_bl = max_val(rc, md->min_radius);
+    const double rh = ks_horizon(m);
+    if (r_bl <= rh + md->horizon_buffer || r_bl < md->r_min || r_bl > md->r_max) return c;
+    const double ne_norm = density_profile_bl(md, r_bl, thc);
+    if (!(ne_norm > 0.0)) return c;
+    const double ne_cgs = ne_norm * md->ne_unit;
+    const double thetae = thetae_profile(md, r_bl);
+    const double b_cgs = magnetic_field_cgs(md, ne_cgs, r_bl);
+    double g[4][4];
+    ks_gcov_matrix(m, &s->x, g);
+    const V4 ucon = fluid_velocity(md, m, r_bl, thc, cp, sp, g);
+    const V4 ucov = lower_g(g, &ucon);
+    double uk = 0.0;
+    for (int mu = 0; mu < 4; ++mu) uk += ucov.v[mu] * s->k.v[mu];
+    const double nu_fluid = max_val(abs_val(-uk), md->min_frequency_scale);
+    const V4 bcon = magnetic_unit(m, &s->x, &ucon, g);
+    const V4 bcov = lower_g(g, &bcon);
+    double kdotb = 0.0;
+    for (int mu = 0; mu < 4; ++mu) kdotb += s->k.v[mu] * bcov.v[mu];
+    const double cos_theta = clamp(kdotb / max_val(nu_fluid, 1e-30), -1.0, 1.0);
+    const double sin_theta = max_val(sqrt(max_val(0.0, 1.0 - cos_theta * cos_theta)), md->min_sin_theta);
+    const double theta = acos(clamp(cos_theta, -1.0, 1.0));
+    const double nu = max_val(freq * nu_fluid, 1.0);
+    ThermalParams tp = {md->emission_type == KP_FIT_DEXTER ? KP_FIT_DEXTER : KP_FIT_PANDYA,
+                        md->max_pol_frac, md->min_sin_theta, md->emission_scale,
+                        md->absorption_scale, md->faraday_scale};
+    if (theta <= 0.0 || theta >= PI) {
+        c.rV = md->faraday_scale * rho_V_only(nu, ne_cgs, thetae, b_cgs, theta, md->min_sin_theta) * nu;
+        return c;
+    }
+    ThermalState ts = {nu, ne_cgs, thetae, b_cgs, theta, sin_theta, cos_theta};
+    const TC mc = thermal_coefficients(&ts, &tp);
+    const double b1 = screen_inner(g, &ucon, &s->k, &s->e1, &bcon);
+    const double b2 = screen_inner(g, &ucon, &s->k, &s->e2, &bcon);
+    const double bproj2 = b1 * b1 + b2 * b2;
+    c.jI = mc.jI;
+    c.jV = mc.jV;
+    c.aI = mc.aI;
+    c.aV = mc.aV;
+    c.rV = mc.rV;
+    if (bproj2 > 1e-30) {
+        const double cos2chi = (b2 * b2 - b1 * b1) / bproj2;
+        const double sin2chi = -2.0 * b1 * b2 / bproj2;
+        c.jQ = mc.jQ * cos2chi;
+        c.jU = mc.jQ * sin2chi;
+        c.aQ = mc.aQ * cos2chi;
+        c.aU = mc.aQ * sin2chi;
+        c.rQ = mc.rQ * cos2chi;
+        c.rU = mc.rQ * sin2chi;
+    }
+    return c;
+}
+
+/* ---- geodesic/pass_a_core.hpp, pass_b.hpp ------------------------------ */
+static int finite_state(const TS* s) { /* pass_a_core.hpp:58-71 */
+    for (int mu = 0; mu < NDIM; ++mu) {
+        const double v[4] = {s->x.v[mu], s->k.v[mu], s->e1.v[mu], s->e2.v[mu]};
+        for (int f = 0; f < 4; ++f)
+            if (!(v[f] == v[f]) || abs_val(v[f]) >= LARGE) return 0;
+    }
+    return 1;
+}
+
+static TS surface_path_state(const KS* m, const TS* first, double h, int composed) { /* pass_a_core.hpp:76-87 */
+    if (composed) {
+        const TS half = rk4_step(m, first, h * 0.5);
+        return rk4_step(m, &half, h * 0.5);
+    }
+    return rk4_step(m, first, h);
+}
+
+typedef struct { TS state; double used_h, surface_value; } SurfEvent;
+
+static SurfEvent locate_crossing(const KS* m, const TS* first, const TS* second, double full_h,
+                                 double surface_parameter, int composed) { /* pass_a_core.hpp:94-197 */
+    /* Kerr metrics: the inner and outer surfaces are both radius - parameter. */
+    SurfEvent out;
+    out.state = *first;
+    out.used_h = 0.0;
+    double lo = 0.0, hi = 1.0;
+    double flo = ks_radius(m, &first->x) - surface_parameter;
+    out.surface_value = flo;
+    if (flo == 0.0) return out;
+    if (!finite_state(second)) return out;
+    const TS hs = surface_path_state(m, first, full_h, composed);
+    if (!finite_state(&hs)) return out;
+    double fhi = ks_radius(m, &hs.x) - surface_parameter;
+    if (!(fhi == fhi) || abs_val(fhi) >= LARGE) return out;
+    if (fhi == 0.0) {
+        out.state = hs;
+        out.used_h = full_h;
+        out.surface_value = fhi;
+        return out;
+    }
+    if ((flo > 0.0) == (fhi > 0.0)) return out;
+    int use_secant = 1;
+    for (int iter = 0; iter < 12; ++iter) {
+        const double width = hi - lo;
+        double trial = (lo + hi) * 0.5;
+        const double denom = flo - fhi;
+        if (use_secant && abs_val(denom) > TINY) {
+            const double secant = lo + width * flo / denom;
+            const double guard = width * 0.1;
+            if (secant > lo + guard && secant < hi - guard) trial = secant;
+        }
+        const TS ts = surface_path_state(m, first, full_h * trial, composed);
+        if (!finite_state(&ts)) {
+            hi = trial;
+            use_secant = 0;
+            continue;
+        }
+        const double ft = ks_radius(m, &ts.x) - surface_parameter;
+        if (!(ft == ft) || abs_val(ft) >= LARGE) {
+            hi = trial;
+            use_secant = 0;
+            continue;
+        }
+        if (ft == 0.0) {
+            out.state = ts;
+            out.used_h = full_h * trial;
+            out.surface_value = ft;
+            return out;
+        }
+        if ((flo > 0.0) == (ft > 0.0)) {
+            lo = trial;
+            flo = ft;
+            out.state = ts;
+            out.used_h = full_h * trial;
+            out.surface_value = ft;
+        } else {
+            hi = trial;
+            fhi = ft;
+        }
+    }
+    return out;
+}
+
+static double spatial_distance(const V4* a, const V4* b) { /* pass_b.hpp:32-36 */
+    return sqrt(square(a->v[1] - b->v[1]) + square(a->v[2] - b->v[2]) + square(a->v[3] - b->v[3]));
+}
+
+static double vmaxabsdiff(const V4* a, const V4* b) { /* pass_b.hpp:44-51 */
+    double o = abs_val(a->v[0] - b->v[0]);
+    for (int i = 1; i < NDIM; ++i) o = max_val(o, abs_val(a->v[i] - b->v[i]));
+    return o;
+}
+
+static double max_frame_error(const KS* m, const TS* s) { /* state.hpp:53-76 */
+    const double kn = ks_dot(m, &s->x, &s->k, &s->k);
+    const double e1k = ks_dot(m, &s->x, &s->e1, &s->k);
+    const double e2k = ks_dot(m, &s->x, &s->e2, &s->k);
+    const double e1n = ks_dot(m, &s->x, &s->e1, &s->e1) - 1.0;
+    const double e2n = ks_dot(m, &s->x, &s->e2, &s->e2) - 1.0;
+    const double e12 = ks_dot(m, &s->x, &s->e1, &s->e2);
+    double o = abs_val(kn);
+    o = max_val(o, abs_val(e1k));
+    o = max_val(o, abs_val(e2k));
+    o = max_val(o, abs_val(e1n));
+    o = max_val(o, abs_val(e2n));
+    o = max_val(o, abs_val(e12));
+    return o;
+}
+
+static inline int surface_crossed(double s0, double s1) { /* pass_b.hpp:69-75 */
+    if (s0 == 0.0 || s1 == 0.0) return 1;
+    return (s0 < 0.0 && s1 > 0.0) || (s0 > 0.0 && s1 < 0.0);
+}
+
+static inline double crossing_fraction(double s0, double s1) { /* pass_b.hpp:77-84 */
+    const double denom = s0 - s1;
+    if (abs_val(denom) <= TINY) return 1.0;
+    return min_val(1.0, max_val(0.0, s0 / denom));
+}
+
+static inline double depth_limit(double specific, double legacy) { return specific >= 0.0 ? specific : legacy; }
+
+static int radiation_substep_count(const TC* c, double h, double dls, int requested, double max_rad_step,
+                                   double max_rad_depth, double max_abs_depth, double max_far_depth) { /* pass_b.hpp:147-179 */
+    int nsub = requested > 0 ? requested : 1;
+    const double abs_h = abs_val(h);
+    if (max_rad_step > 0.0)
+        while (abs_h / (double)nsub > max_rad_step && nsub < 4096) nsub *= 2;
+    const double dl = abs_h * abs_val(dls);
+    const double alim = depth_limit(max_abs_depth, max_rad_depth);
+    if (alim > 0.0) {
+        const double depth = (abs_val(c->aI) + sqrt(square(c->aQ) + square(c->aU) + square(c->aV))) * dl;
+        while (depth / (double)nsub > alim && nsub < 4096) nsub *= 2;
+    }
+    const double flim = depth_limit(max_far_depth, max_rad_depth);
+    if (flim > 0.0) {
+        const double depth = sqrt(square(c->rQ) + square(c->rU) + square(c->rV)) * dl;
+        while (depth / (double)nsub > flim && nsub < 4096) nsub *= 2;
+    }
+    return nsub;
+}
+
+typedef struct {
+    ST obs[KP_MAX_FREQUENCIES];
+    OV ov;
+    double closure_x, closure_k, final_null, frame_error;
+    int pass_a_steps, steps, reason;
+} PixelResult;
+
+/* Fused pass A + pass B for one pixel, nfreq channels sharing one geodesic:
+ * trace_pass_b_segment_model_pixel_metric (pass_b.hpp:769-1114) and its
+ * multi-frequency twin (pass_b.hpp:1131-1501), which agree for nfreq == 1. */
+static void trace_pixel(int pixel, const kp_pass_a_params* P, const kp_riaf_model* md,
+                        const double* freqs, int nfreq, int integrator, PixelResult* res) {
+    const KS met = {P->mass, P->spin};
+    const KS* m = &met;
+    memset(res, 0, sizeof *res);
+    res->ov.r11 = 1.0;
+    res->ov.r22 = 1.0;
+    const TS cam = camera_ray_pinhole_cks(m, pixel, &P->camera);
+    TS state = cam;
+    int pa_reason = KP_REASON_MAX_STEPS;
+    int pa_steps = 0;
+    double path_length = 0.0;
+    (void)path_length;
+    ACtl actl = {P->adaptive_tolerance, P->min_step, P->max_step, 10};
+    double h_current = -abs_val(P->step);
+    int entered = 0;
+    int inside = 0;
+    for (int n = 0; n < P->max_steps; ++n) {
+        const double r_bl = ks_radius(m, &state.x);
+        if (!entered) {
+            if (r_bl <= P->outer_radius) {
+                entered = 1;
+                inside = 0;
+            }
+        } else {
+            if (r_bl - P->inner_radius <= 0.0) {
+                pa_reason = KP_REASON_REACHED_INNER_BOUNDARY;
+                break;
+            }
+            if (inside > 0 && r_bl >= P->outer_radius) {
+                pa_reason = KP_REASON_ESCAPED_DOMAIN;
+                break;
+            }
+        }
+        const TS old = state;
+        const double eff_min = abs_val(P->min_step);
+        const double old_r = r_bl;
+        const double old_inner = r_bl - P->inner_radius;
+        double used_h = h_current;
+        TS next;
+        if (P->adaptive) {
+            ACtl tc = actl;
+            tc.min_step = eff_min;
+            if (abs_val(used_h) < tc.min_step) tc.min_step = abs_val(used_h);
+            const AStep st = adaptive_step(integrator, m, &old, used_h, tc);
+            if (!st.accepted) {
+                h_current = st.next_h;
+                if (abs_val(h_current) <= eff_min * 1.0001) {
+                    pa_reason = KP_REASON_ADAPTIVE_STEP_UNDERFLOW;
+                    break;
+                }
+                continue;
+            }
+            next = st.state;
+            used_h = st.used_h;
+            h_current = st.next_h;
+        } else {
+            next = rk4_step(m, &state, used_h);
+        }
+        const double next_r = ks_radius(m, &next.x);
+        const double next_inner = next_r - P->inner_radius;
+        if (!entered && next_r <= P->outer_radius) {
+            entered = 1;
+            inside = 0;
+        } else if (!entered && next_r >= old_r) {
+            state = next;
+            pa_steps += 1;
+            pa_reason = KP_REASON_ESCAPED_DOMAIN;
+            break;
+        }
+        int crossing = KP_REASON_NONE;
+        if (entered && old_inner > 0.0 && next_inner <= 0.0) {
+            crossing = KP_REASON_REACHED_INNER_BOUNDARY;
+        } else if (entered && inside > 0 && old_r < P->outer_radius && next_r >= P->outer_radius) {
+            crossing = KP_REASON_ESCAPED_DOMAIN;
+        }
+        if (crossing != KP_REASON_NONE) {
+            const int inner_event = crossing == KP_REASON_REACHED_INNER_BOUNDARY;
+            const double sp = inner_event ? P->inner_radius : P->outer_radius;
+            const SurfEvent ev = locate_crossing(m, &old, &next, used_h, sp, P->adaptive);
+            next = ev.state;
+            used_h = ev.used_h;
+            state = next;
+            pa_steps += 1;
+            pa_reason = crossing;
+            break;
+        }
+        state = next;
+        pa_steps += 1;
+        if (entered) inside += 1;
+    }
+    res->pass_a_steps = pa_steps;
+    res->reason = pa_reason;
+    if (!entered || (pa_reason != KP_REASON_REACHED_INNER_BOUNDARY && pa_reason != KP_REASON_ESCAPED_DOMAIN)) {
+        res->closure_x = spatial_distance(&state.x, &cam.x);
+        res->closure_k = vmaxabsdiff(&state.k, &cam.k);
+        res->final_null = ks_dot(m, &state.x, &state.k, &state.k);
+        res->frame_error = max_frame_error(m, &state);
+        return;
+    }
+
+    /* pass B */
+    ST stokes[KP_MAX_FREQUENCIES];
+    double dls[KP_MAX_FREQUENCIES];
+    for (int f = 0; f < nfreq; ++f) {
+        stokes[f].I = stokes[f].Q = stokes[f].U = stokes[f].V = 0.0;
+        dls[f] = riaf_dlambda_scale(md, freqs[f]);
+    }
+    int reason = pa_reason;
+    int reached = 0;
+    int steps = 0;
+    h_current = P->step;
+    double cap = P->max_radiation_step > 0.0 ? P->max_radiation_step : P->max_step;
+    while (!reached && steps < P->max_steps) {
+        double h = h_current;
+        const TS old = state;
+        const double eff_min = abs_val(P->min_step);
+        const double start_r = ks_radius(m, &old.x);
+        if (start_r <= P->outer_radius && cap > 0.0) h = min_val(h, cap);
+        TS next, sample;
+        if (P->adaptive) {
+            ACtl tc = actl;
+            tc.min_step = eff_min;
+            const AStep st = adaptive_step(integrator, m, &old, h, tc);
+            if (!st.accepted) {
+                h_current = abs_val(st.next_h);
+                if (h_current <= eff_min * 1.0001) {
+                    reason = KP_REASON_ADAPTIVE_STEP_UNDERFLOW;
+                    break;
+                }
+                continue;
+            }
+            h = abs_val(st.used_h);
+            h_current = abs_val(st.next_h);
+            next = st.state;
+            sample = st.mid_state;
+        } else {
+            next = rk4_step(m, &old, h);
+            sample = next;
+        }
+        const double s0 = ks_radius(m, &old.x) - P->camera.radius;
+        const double s1 = ks_radius(m, &next.x) - P->camera.radius;
+        const int crosses = surface_crossed(s0, s1);
+        if (crosses) {
+            const double frac = crossing_fraction(s0, s1);
+            const double h_cross = h * frac;
+            if (abs_val(h_cross) <= 1e-14) {
+                h = 0.0;
+                next = old;
+                sample = old;
+            } else if (frac < 0.999999999999) {
+                h = h_cross;
+                if (P->adaptive) {
+                    ACtl cc = actl;
+                    cc.min_step = min_val(eff_min, abs_val(h));
+                    cc.max_step = max_val(cc.min_step, abs_val(h));
+                    const AStep cs = adaptive_step(integrator, m, &old, h, cc);
+                    if (!cs.accepted) {
+                        h_current = abs_val(cs.next_h);
+                        continue;
+                    }
+                    h = abs_val(cs.used_h);
+                    next = cs.state;
+                    sample = cs.mid_state;
+                } else {
+                    next = rk4_step(m, &old, h);
+                    sample = next;
+                }
+            }
+        }
+        const double old_r = ks_radius(m, &old.x);
+        const double sample_r = ks_radius(m, &sample.x);
+        const double next_r = ks_radius(m, &next.x);
+        const double local_max_rs =
+            (P->max_radiation_step > 0.0 &&
+             (old_r <= P->outer_radius || sample_r <= P->outer_radius || next_r <= P->outer_radius))
+                ? P->max_radiation_step : 0.0;
+        int required = 1;
+        TC co[KP_MAX_FREQUENCIES];
+        for (int f = 0; f < nfreq; ++f) {
+            memset(&co[f], 0, sizeof co[f]);
+            if (sample_r - P->inner_radius > 0.0 && sample_r < P->outer_radius) {
+                co[f] = riaf_coefficients(md, freqs[f], m, &sample);
+                if (!P->emission_selection.faraday_rotation) co[f].rV = 0.0;
+            }
+            const int cand = radiation_substep_count(&co[f], h, dls[f], 1, local_max_rs, P->max_radiation_depth,
+                                                     P->max_absorption_depth, P->max_faraday_depth);
+            required = cand > required ? cand : required;
+        }
+        if (required > 1 && h > eff_min * 1.0001) {
+            h_current = max_val(eff_min, h / (double)required);
+            cap = h_current;
+            continue;
+        }
+        if (local_max_rs > 0.0 || P->max_radiation_depth > 0.0 || P->max_absorption_depth > 0.0 ||
+            P->max_faraday_depth > 0.0) {
+            int pred = 1;
+            for (int f = 0; f < nfreq; ++f) {
+                const int cand = radiation_substep_count(&co[f], h_current, dls[f], 1, local_max_rs,
+                                                         P->max_radiation_depth, P->max_absorption_depth,
+                                                         P->max_faraday_depth);
+                pred = cand > pred ? cand : pred;
+            }
+            cap = pred > 1 ? max_val(eff_min, h_current / (double)pred) : P->max_step;
+        } else {
+            cap = P->max_step;
+        }
+        if (h > 0.0)
+            for (int f = 0; f < nfreq; ++f) stokes_step(&stokes[f], &co[f], abs_val(h) * dls[f]);
+        state = next;
+        steps += 1;
+        if (crosses) reached = 1;
+    }
+    const double r11 = ks_dot(m, &state.x, &cam.e1, &state.e1);
+    const double r12 = ks_dot(m, &state.x, &cam.e1, &state.e2);
+    const double r21 = ks_dot(m, &state.x, &cam.e2, &state.e1);
+    const double r22 = ks_dot(m, &state.x, &cam.e2, &state.e2);
+    res->ov.r11 = r11;
+    res->ov.r12 = r12;
+    res->ov.r21 = r21;
+    res->ov.r22 = r22;
+    for (int f = 0; f < nfreq; ++f) res->obs[f] = to_observer_basis(stokes[f], &res->ov);
+    res->closure_x = spatial_distance(&state.x, &cam.x);
+    res->closure_k = vmaxabsdiff(&state.k, &cam.k);
+    res->final_null = ks_dot(m, &state.x, &state.k, &state.k);
+    res->frame_error = max_frame_error(m, &state);
+    if (reached) {
+        reason = KP_REASON_REACHED_CAMERA;
+    } else if (reason != KP_REASON_ADAPTIVE_STEP_UNDERFLOW) {
+        reason = KP_REASON_MAX_STEPS;
+    }
+    res->steps = steps;
+    res->reason = reason;
+}
+
+int kpo_image_riaf_range(const kp_pass_a_params* params, const kp_riaf_model* model,
+                         int radiation_substeps, const double* freqs, int nfreq, int integrator,
+                         int threads, int pixel_begin, int pixel_end, kp_image_out* out) {
+    (void)radiation_substeps;
+    if (!params || !model || !out) return fail("null argument");
+    if (nfreq < 1 || nfreq > KP_MAX_FREQUENCIES) return fail("nfreq out of range");
+    if (params->coordinate_system != KP_COORD_CARTESIAN_KS) return fail("oracle restatement covers cartesian_ks only");
+    if (params->camera.model != KP_CAMERA_PINHOLE) return fail("oracle restatement covers the pinhole camera only");
+    if (params->direct_only) return fail("direct_only is not covered by the oracle restatement");
+    if (params->emission_selection.equatorial_h_over_r > 0.0 && params->emission_selection.equatorial_h_over_r < 1.0)
+        return fail("narrow equatorial wedge is not covered by the oracle restatement");
+    const int npix = params->camera.nx * params->camera.ny;
+    if (pixel_begin < 0 || pixel_end > npix || pixel_begin > pixel_end) return fail("pixel range out of bounds");
+    double fr[KP_MAX_FREQUENCIES];
+    for (int f = 0; f < nfreq; ++f) fr[f] = freqs ? freqs[f] : model->freq_cgs;
+    if (threads > 0) omp_set_num_threads(threads);
+#pragma omp parallel for schedule(dynamic)
+    for (int pixel = pixel_begin; pixel < pixel_end; ++pixel) {
+        PixelResult r;
+        trace_pixel(pixel, params, model, fr, nfreq, integrator, &r);
+        for (int f = 0; f < nfreq; ++f) {
+            const size_t idx = (size_t)f * (size_t)npix + (size_t)pixel;
+            out->image_i[idx] = r.obs[f].I;
+            out->image_q[idx] = r.obs[f].Q;
+            out->image_u[idx] = r.obs[f].U;
+            out->image_v[idx] = r.obs[f].V;
+        }
+        out->closure_x[pixel] = r.closure_x;
+        out->closure_k[pixel] = r.closure_k;
+        out->final_null[pixel] = r.final_null;
+        out->frame_error[pixel] = r.frame_error;
+        out->det_r[pixel] = r.ov.r11 * r.ov.r22 - r.ov.r12 * r.ov.r21;
+        out->overlap_r11[pixel] = r.ov.r11;
+        out->overlap_r12[pixel] = r.ov.r12;
+        out->overlap_r21[pixel] = r.ov.r21;
+        out->overlap_r22[pixel] = r.ov.r22;
+        out->basis_identity_error[pixel] = max_val(max_val(abs_val(r.ov.r11 - 1.0), abs_val(r.ov.r22 - 1.0)),
+                                                   max_val(abs_val(r.ov.r12), abs_val(r.ov.r21)));
+        out->basis_rotation_angle[pixel] = atan2(r.ov.r21 - r.ov.r12, r.ov.r11 + r.ov.r22);
+        out->pass_a_steps[pixel] = r.pass_a_steps;
+        out->steps[pixel] = r.steps;
+        out->reason[pixel] = r.reason;
+    }
+    return KP_OK;
+}
+
+int kpo_thermal_coefficients(int fit, double nu, double ne, double thetae, double b_cgs, double theta,
+                             double sin_theta, double cos_theta, double max_pol_frac, double min_sin_theta,
+                             double* out11) {
+    ThermalState s = {nu, ne, thetae, b_cgs, theta, sin_theta, cos_theta};
+    ThermalParams p = {fit, max_pol_frac, min_sin_theta, 1.0, 1.0, 1.0};
+    const TC c = thermal_coefficients(&s, &p);
+    const double v[11] = {c.jI, c.jQ, c.jU, c.jV, c.aI, c.aQ, c.aU, c.aV, c.rQ, c.rU, c.rV};
+    memcpy(out11, v, sizeof v);
+    return KP_OK;
+}
+
+int kpo_stokes_step(double* s4, const double* c11, double dl) {
+    ST s = {s4[0], s4[1], s4[2], s4[3]};
+    TC c = {c11[0], c11[1], c11[2], c11[3], c11[4], c11[5], c11[6], c11[7], c11[8], c11[9], c11[10]};
+    stokes_step(&s, &c, dl);
+    s4[0] = s.I;
+    s4[1] = s.Q;
+    s4[2] = s.U;
+    s4[3] = s.V;
+    return KP_OK;
+}
+
+static TS ts_from(const double* a) {
+    TS s;
+    for (int mu = 0; mu < 4; ++mu) {
+        s.x.v[mu] = a[mu];
+        s.k.v[mu] = a[4 + mu];
+        s.e1.v[mu] = a[8 + mu];
+        s.e2.v[mu] = a[12 + mu];
+    }
+    return s;
+}
+
+static void ts_to(const TS* s, double* a) {
+    for (int mu = 0; mu < 4; ++mu) {
+        a[mu] = s->x.v[mu];
+        a[4 + mu] = s->k.v[mu];
+        a[8 + mu] = s->e1.v[mu];
+        a[12 + mu] = s->e2.v[mu];
+    }
+}
+
+int kpo_riaf_coefficients_cks(double mass, double spin, const kp_riaf_model* model, const double* state16,
+                              double* out11) {
+    const KS m = {mass, spin};
+    const TS s = ts_from(state16);
+    const TC c = riaf_coefficients(model, model->freq_cgs, &m, &s);
+    const double v[11] = {c.jI, c.jQ, c.jU, c.jV, c.aI, c.aQ, c.aU, c.aV, c.rQ, c.rU, c.rV};
+    memcpy(out11, v, sizeof v);
+    return KP_OK;
+}
+
+int kpo_camera_ray_cks(const kp_pass_a_params* params, int pixel, double* state16) {
+    const KS m = {params->mass, params->spin};
+    const TS s = camera_ray_pinhole_cks(&m, pixel, &params->camera);
+    ts_to(&s, state16);
+    return KP_OK;
+}
+
+int kpo_transport_rhs_cks(double mass, double spin, const double* state16, double* d16) {
+    const KS m = {mass, spin};
+    const TS s = ts_from(state16);
+    const TS d = ks_rhs(&m, &s);
+    ts_to(&d, d16);
+    return KP_OK;
+}

@@ -1,0 +1,298 @@
+// Reference-oracle driver: calls the reference's own header-only hot-path
+// templates, compiled unchanged from the reference source tree against the
+// Kokkos stand-in in oracle/shim, and exposes them through a small C ABI so
+// tests and the CPU baseline can run them.  Test infrastructure only: the
+// product library never links this file.
+//
+// The per-pixel loop mirrors the reference's image kernels:
+//   fused single frequency: src/image/driver.hpp:61-113
+//   multi-frequency, one shared geodesic: src/image/multifrequency.hpp:37-76
+// with the OpenMP dynamic schedule of pixel_range_policy (src/image/kernels.hpp:10-20).
+#include <omp.h>
+
+#include <cstring>
+#include <stdexcept>
+
+#include "geodesic/pass_b.hpp"
+#include "geometry/kerr_boyer_lindquist.hpp"
+#include "geometry/kerr_schild_cartesian.hpp"
+#include "model/riaf.hpp"
+
+#include "kpolaris_b200.h"
+
+namespace {
+
+using Real = double;
+
+kpolaris::PassAParams<Real> to_pass_a(const kp_pass_a_params& p) {
+    kpolaris::PassAParams<Real> out;
+    out.camera.nx = p.camera.nx;
+    out.camera.ny = p.camera.ny;
+    out.camera.radius = p.camera.radius;
+    out.camera.inclination = p.camera.inclination;
+    out.camera.fov = p.camera.fov;
+    out.camera.fov_y = p.camera.fov_y;
+    out.camera.xspan = p.camera.xspan;
+    out.camera.yspan = p.camera.yspan;
+    out.camera.x_offset = p.camera.x_offset;
+    out.camera.y_offset = p.camera.y_offset;
+    out.camera.model = static_cast<kpolaris::CameraModel>(p.camera.model);
+    out.emission_selection.equatorial_h_over_r = p.emission_selection.equatorial_h_over_r;
+    out.emission_selection.equatorial_samples = p.emission_selection.equatorial_samples;
+    out.emission_selection.faraday_rotation = p.emission_selection.faraday_rotation;
+    out.mass = p.mass;
+    out.spin = p.spin;
+    out.inner_radius = p.inner_radius;
+    out.outer_radius = p.outer_radius;
+    out.step = p.step;
+    out.max_steps = p.max_steps;
+    out.adaptive = p.adaptive;
+    out.direct_only = p.direct_only;
+    out.adaptive_tolerance = p.adaptive_tolerance;
+    out.min_step = p.min_step;
+    out.max_step = p.max_step;
+    out.max_radiation_step = p.max_radiation_step;
+    out.max_radiation_depth = p.max_radiation_depth;
+    out.max_absorption_depth = p.max_absorption_depth;
+    out.max_faraday_depth = p.max_faraday_depth;
+    out.fmks_startx1 = p.fmks_startx1;
+    out.fmks_hslope = p.fmks_hslope;
+    out.fmks_mks_smooth = p.fmks_mks_smooth;
+    out.fmks_poly_alpha = p.fmks_poly_alpha;
+    out.fmks_poly_xt = p.fmks_poly_xt;
+    out.fmks_poly_norm = p.fmks_poly_norm;
+    out.coordinate_system = static_cast<kpolaris::CoordinateSystem>(p.coordinate_system);
+    return out;
+}
+
+kpolaris::RIAFAnalyticRadiationModel<Real> to_riaf(const kp_riaf_model& m) {
+    kpolaris::RIAFAnalyticRadiationModel<Real> out;
+    out.nth0 = m.nth0;
+    out.Te0 = m.Te0;
+    out.disk_h = m.disk_h;
+    out.pow_nth = m.pow_nth;
+    out.pow_T = m.pow_T;
+    out.ne_unit = m.ne_unit;
+    out.te_unit = m.te_unit;
+    out.b_unit = m.b_unit;
+    out.freq_cgs = m.freq_cgs;
+    out.mbh_solar = m.mbh_solar;
+    out.r_min = m.r_min;
+    out.r_max = m.r_max;
+    out.horizon_buffer = m.horizon_buffer;
+    out.emission_scale = m.emission_scale;
+    out.absorption_scale = m.absorption_scale;
+    out.faraday_scale = m.faraday_scale;
+    out.max_pol_frac = m.max_pol_frac;
+    out.keplerian_factor = m.keplerian_factor;
+    out.infall_factor = m.infall_factor;
+    out.emission_type = m.emission_type;
+    out.min_frequency_scale = m.min_frequency_scale;
+    out.min_sin_theta = m.min_sin_theta;
+    out.min_thetae = m.min_thetae;
+    out.min_radius = m.min_radius;
+    return out;
+}
+
+template<class Overlap>
+void store_common(kp_image_out* out, int pixel, const Overlap& ov, Real closure_x,
+                  Real closure_k, Real final_null, Real frame_error, int pass_a_steps,
+                  int steps, int reason) {
+    out->closure_x[pixel] = closure_x;
+    out->closure_k[pixel] = closure_k;
+    out->final_null[pixel] = final_null;
+    out->frame_error[pixel] = frame_error;
+    out->det_r[pixel] = ov.det();
+    out->overlap_r11[pixel] = ov.r11;
+    out->overlap_r12[pixel] = ov.r12;
+    out->overlap_r21[pixel] = ov.r21;
+    out->overlap_r22[pixel] = ov.r22;
+    out->basis_identity_error[pixel] =
+        kpolaris::max_val(kpolaris::max_val(kpolaris::abs_val(ov.r11 - Real(1)),
+                                            kpolaris::abs_val(ov.r22 - Real(1))),
+                          kpolaris::max_val(kpolaris::abs_val(ov.r12), kpolaris::abs_val(ov.r21)));
+    out->basis_rotation_angle[pixel] = std::atan2(ov.r21 - ov.r12, ov.r11 + ov.r22);
+    out->pass_a_steps[pixel] = pass_a_steps;
+    out->steps[pixel] = steps;
+    out->reason[pixel] = reason;
+}
+
+template<class Metric>
+void run_metric(const kpolaris::PassAParams<Real>& pa,
+                const kpolaris::RIAFAnalyticRadiationModel<Real>& model,
+                int radiation_substeps, const double* freqs, int nfreq,
+                const Metric& metric, int pixel_begin, int pixel_end, kp_image_out* out) {
+    const int npix = pa.camera.nx * pa.camera.ny;
+#pragma omp parallel for schedule(dynamic)
+    for (int pixel = pixel_begin; pixel < pixel_end; ++pixel) {
+        if (nfreq == 1) {
+            auto m = model;
+            if (freqs) m.freq_cgs = freqs[0];
+            const kpolaris::PassBResult<Real> r =
+                kpolaris::trace_pass_b_segment_model_pixel_metric(pixel, pa, m,
+                                                                  radiation_substeps, metric);
+            out->image_i[pixel] = r.observed_stokes.I;
+            out->image_q[pixel] = r.observed_stokes.Q;
+            out->image_u[pixel] = r.observed_stokes.U;
+            out->image_v[pixel] = r.observed_stokes.V;
+            store_common(out, pixel, r.overlap, r.closure_x, r.closure_k, r.final_null,
+                         r.frame_error, r.pass_a.steps, r.steps, static_cast<int>(r.reason));
+        } else {
+            Real local_freqs[KPOLARIS_MAX_FREQUENCIES];
+            kpolaris::Stokes<Real> local_stokes[KPOLARIS_MAX_FREQUENCIES];
+            for (int f = 0; f < nfreq; ++f) local_freqs[f] = freqs[f];
+            const kpolaris::MultiFrequencyPassBResult<Real> r =
+                kpolaris::trace_pass_b_segment_model_multifrequency_pixel_metric(
+                    pixel, pa, model, radiation_substeps, local_freqs, nfreq, local_stokes,
+                    metric);
+            for (int f = 0; f < nfreq; ++f) {
+                const size_t idx = static_cast<size_t>(f) * static_cast<size_t>(npix) + pixel;
+                out->image_i[idx] = local_stokes[f].I;
+                out->image_q[idx] = local_stokes[f].Q;
+                out->image_u[idx] = local_stokes[f].U;
+                out->image_v[idx] = local_stokes[f].V;
+            }
+            store_common(out, pixel, r.overlap, r.closure_x, r.closure_k, r.final_null,
+                         r.frame_error, r.pass_a.steps, r.steps, static_cast<int>(r.reason));
+        }
+    }
+}
+
+thread_local char g_error[512];
+
+int fail(const char* msg) {
+    std::snprintf(g_error, sizeof(g_error), "%s", msg);
+    return KP_ERR_INVALID;
+}
+
+} // namespace
+
+extern "C" {
+
+const char* kpref_last_error(void) { return g_error; }
+
+int kpref_max_frequencies(void) { return KPOLARIS_MAX_FREQUENCIES; }
+
+// Runs pixels [pixel_begin, pixel_end) of a RIAF image with `threads` OpenMP
+// threads (0 = all).  Only the selected pixels of *out are written.
+int kpref_image_riaf_range(const kp_pass_a_params* params, const kp_riaf_model* model,
+                           int radiation_substeps, const double* freqs, int nfreq,
+                           int threads, int pixel_begin, int pixel_end, kp_image_out* out) {
+    if (!params || !model || !out) return fail("null argument");
+    if (nfreq < 1 || nfreq > KPOLARIS_MAX_FREQUENCIES) return fail("nfreq out of range");
+    const int npix = params->camera.nx * params->camera.ny;
+    if (pixel_begin < 0 || pixel_end > npix || pixel_begin > pixel_end)
+        return fail("pixel range out of bounds");
+    if (threads > 0) omp_set_num_threads(threads);
+    const auto pa = to_pass_a(*params);
+    const auto riaf = to_riaf(*model);
+    if (pa.coordinate_system == kpolaris::CoordinateSystem::CartesianKS) {
+        const kpolaris::KerrSchildInMetric<Real> metric(pa.mass, pa.spin);
+        run_metric(pa, riaf, radiation_substeps, freqs, nfreq, metric, pixel_begin, pixel_end, out);
+    } else if (pa.coordinate_system == kpolaris::CoordinateSystem::BoyerLindquist) {
+        const kpolaris::KerrBoyerLindquistMetric<Real> metric(pa.mass, pa.spin);
+        run_metric(pa, riaf, radiation_substeps, freqs, nfreq, metric, pixel_begin, pixel_end, out);
+    } else {
+        return fail("coordinate system not built in the reference oracle");
+    }
+    return KP_OK;
+}
+
+int kpref_image_riaf(const kp_pass_a_params* params, const kp_riaf_model* model,
+                     int radiation_substeps, const double* freqs, int nfreq, int threads,
+                     kp_image_out* out) {
+    if (!params) return fail("null params");
+    return kpref_image_riaf_range(params, model, radiation_substeps, freqs, nfreq, threads, 0,
+                                  params->camera.nx * params->camera.ny, out);
+}
+
+// Thermal synchrotron invariant coefficients in the magnetic basis
+// (thermal_synchrotron_magnetic_basis_coefficients, thermal_synchrotron.hpp:512-627).
+// out = {jI, jQ, jU, jV, aI, aQ, aU, aV, rQ, rU, rV}.
+int kpref_thermal_coefficients(int fit, double nu, double ne, double thetae, double b_cgs,
+                               double theta, double sin_theta, double cos_theta,
+                               double max_pol_frac, double min_sin_theta, double* out11) {
+    kpolaris::LocalThermalSynchrotronState<Real> s;
+    s.nu = nu;
+    s.ne = ne;
+    s.thetae = thetae;
+    s.b_cgs = b_cgs;
+    s.theta = theta;
+    s.sin_theta = sin_theta;
+    s.cos_theta = cos_theta;
+    kpolaris::ThermalSynchrotronParams<Real> p;
+    p.fit = fit;
+    p.max_pol_frac = max_pol_frac;
+    p.min_sin_theta = min_sin_theta;
+    const auto c = kpolaris::thermal_synchrotron_magnetic_basis_coefficients(s, p);
+    const double v[11] = {c.jI, c.jQ, c.jU, c.jV, c.aI, c.aQ, c.aU, c.aV, c.rQ, c.rU, c.rV};
+    std::memcpy(out11, v, sizeof(v));
+    return KP_OK;
+}
+
+// One semi-analytic Strang step (semi_analytic_stokes_step, semi_analytic.hpp:94-100).
+int kpref_stokes_step(double* stokes4, const double* coeffs11, double dlambda) {
+    kpolaris::Stokes<Real> s(stokes4[0], stokes4[1], stokes4[2], stokes4[3]);
+    kpolaris::TransferCoeffs<Real> c;
+    c.jI = coeffs11[0]; c.jQ = coeffs11[1]; c.jU = coeffs11[2]; c.jV = coeffs11[3];
+    c.aI = coeffs11[4]; c.aQ = coeffs11[5]; c.aU = coeffs11[6]; c.aV = coeffs11[7];
+    c.rQ = coeffs11[8]; c.rU = coeffs11[9]; c.rV = coeffs11[10];
+    kpolaris::semi_analytic_stokes_step(s, c, dlambda);
+    stokes4[0] = s.I; stokes4[1] = s.Q; stokes4[2] = s.U; stokes4[3] = s.V;
+    return KP_OK;
+}
+
+// RIAF coefficients at a transport state (RIAFAnalyticRadiationModel::coefficients,
+// riaf.hpp:410-549) in Cartesian KS.  state16 = x[4], k[4], e1[4], e2[4].
+int kpref_riaf_coefficients_cks(double mass, double spin, const kp_riaf_model* model,
+                                const double* state16, double* out11) {
+    const kpolaris::KerrSchildInMetric<Real> metric(mass, spin);
+    const auto riaf = to_riaf(*model);
+    kpolaris::TransportState<Real> s;
+    for (int mu = 0; mu < 4; ++mu) {
+        s.x[mu] = state16[mu];
+        s.k[mu] = state16[4 + mu];
+        s.e1[mu] = state16[8 + mu];
+        s.e2[mu] = state16[12 + mu];
+    }
+    const auto c = riaf.coefficients(metric, s, Real(0.5));
+    const double v[11] = {c.jI, c.jQ, c.jU, c.jV, c.aI, c.aQ, c.aU, c.aV, c.rQ, c.rU, c.rV};
+    std::memcpy(out11, v, sizeof(v));
+    return KP_OK;
+}
+
+// Camera ray for one pixel (initialize_camera_ray, camera.hpp:515-523) in Cartesian KS.
+int kpref_camera_ray_cks(const kp_pass_a_params* params, int pixel, double* state16) {
+    const auto pa = to_pass_a(*params);
+    const kpolaris::KerrSchildInMetric<Real> metric(pa.mass, pa.spin);
+    const auto s = kpolaris::initialize_camera_ray(metric, pixel, pa.camera);
+    for (int mu = 0; mu < 4; ++mu) {
+        state16[mu] = s.x[mu];
+        state16[4 + mu] = s.k[mu];
+        state16[8 + mu] = s.e1[mu];
+        state16[12 + mu] = s.e2[mu];
+    }
+    return KP_OK;
+}
+
+// Geodesic right-hand side (transport_rhs, kerr_schild_cartesian.hpp:348-363).
+int kpref_transport_rhs_cks(double mass, double spin, const double* state16, double* d16) {
+    const kpolaris::KerrSchildInMetric<Real> metric(mass, spin);
+    kpolaris::TransportState<Real> s;
+    for (int mu = 0; mu < 4; ++mu) {
+        s.x[mu] = state16[mu];
+        s.k[mu] = state16[4 + mu];
+        s.e1[mu] = state16[8 + mu];
+        s.e2[mu] = state16[12 + mu];
+    }
+    const auto d = kpolaris::transport_rhs(metric, s);
+    for (int mu = 0; mu < 4; ++mu) {
+        d16[mu] = d.x[mu];
+        d16[4 + mu] = d.k[mu];
+        d16[8 + mu] = d.e1[mu];
+        d16[12 + mu] = d.e2[mu];
+    }
+    return KP_OK;
+}
+
+} // extern "C"
