@@ -244,9 +244,20 @@ const char* kp_last_error(void);
 /* ABI version, for the bindings' load-time check. */
 int kp_abi_version(void);
 
+/* sizeof of the ABI structs, for the bindings' layout check:
+ * 0 kp_camera_params, 1 kp_emission_selection, 2 kp_pass_a_params,
+ * 3 kp_riaf_model, 4 kp_image_out, 5 kp_run_options; 6 is the bytes of
+ * kernel parameters one image launch uploads; 0 for other ids. */
+size_t kp_abi_sizeof(int which);
+
 /* Bytes of per-pixel output (15 doubles + 3 int32 = 132 B), the figure the
  * reference's batch budget uses (src/image/batch_driver.hpp:49). */
 size_t kp_image_output_bytes(int npix, int nfreq);
+
+/* Measured FMA throughput of `device` in TFLOP/s (2 flops per FMA), FP64
+ * (fp64 = 1) or FP32: the pipe roofline the image kernels are reported
+ * against.  No reference counterpart (a measurement helper). */
+int kp_measure_fma_peak(int device, int fp64, double* tflops);
 
 /*
  * RIAF image, one or several frequencies sharing one geodesic per pixel.

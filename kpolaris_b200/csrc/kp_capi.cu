@@ -1,0 +1,483 @@
+// kp_capi.cu -- host side of the C ABI declared in include/kpolaris_b200.h:
+// argument validation with the reference's error semantics, per-image
+// constant resolution, device buffers, launches and copies.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "kp_launch.h"
+#include "kpolaris_b200.h"
+
+namespace {
+
+thread_local char g_error[1024] = "";
+
+}  // namespace
+
+namespace kp {
+
+int set_error(int code, const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(g_error, sizeof(g_error), fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+int cuda_error(cudaError_t e, const char* what) {
+    return set_error(KP_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+// Per-device library state: a non-blocking stream and grow-only output
+// buffers reused across calls.
+struct DeviceState {
+    int initialised = 0;
+    cudaStream_t stream = nullptr;
+    void* out_buf = nullptr;
+    size_t out_bytes = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+static std::mutex g_mutex;
+static DeviceState g_dev[64];
+
+DeviceState* device_state(int device, int* status) {
+    if (device < 0 || device >= 64) {
+        *status = set_error(KP_ERR_INVALID, "device ordinal %d out of range", device);
+        return nullptr;
+    }
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) {
+        *status = cuda_error(e, "cudaSetDevice");
+        return nullptr;
+    }
+    DeviceState& d = g_dev[device];
+    if (!d.initialised) {
+        e = cudaStreamCreateWithFlags(&d.stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) {
+            *status = cuda_error(e, "cudaStreamCreate");
+            return nullptr;
+        }
+        cudaEventCreate(&d.ev0);
+        cudaEventCreate(&d.ev1);
+        d.initialised = 1;
+    }
+    *status = KP_OK;
+    return &d;
+}
+
+void* device_output_buffer(DeviceState* d, size_t bytes, int* status) {
+    if (bytes > d->out_bytes) {
+        if (d->out_buf) cudaFree(d->out_buf);
+        d->out_buf = nullptr;
+        d->out_bytes = 0;
+        cudaError_t e = cudaMalloc(&d->out_buf, bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            *status = set_error(KP_ERR_OOM, "cudaMalloc(%zu bytes) for image outputs: %s", bytes,
+                                cudaGetErrorString(e));
+            return nullptr;
+        }
+        d->out_bytes = bytes;
+    }
+    *status = KP_OK;
+    return d->out_buf;
+}
+
+// Carves a kp_image_out-shaped set of device arrays out of one buffer.
+ImageOutPtrs carve_outputs(void* base, int npix, int nfreq) {
+    char* p = static_cast<char*>(base);
+    auto take_d = [&](size_t n) {
+        double* r = reinterpret_cast<double*>(p);
+        p += ((n * sizeof(double) + 255) / 256) * 256;
+        return r;
+    };
+    auto take_i = [&](size_t n) {
+        int32_t* r = reinterpret_cast<int32_t*>(p);
+        p += ((n * sizeof(int32_t) + 255) / 256) * 256;
+        return r;
+    };
+    const size_t img = size_t(npix) * size_t(nfreq);
+    ImageOutPtrs o;
+    o.image_i = take_d(img);
+    o.image_q = take_d(img);
+    o.image_u = take_d(img);
+    o.image_v = take_d(img);
+    o.closure_x = take_d(npix);
+    o.closure_k = take_d(npix);
+    o.final_null = take_d(npix);
+    o.frame_error = take_d(npix);
+    o.det_r = take_d(npix);
+    o.r11 = take_d(npix);
+    o.r12 = take_d(npix);
+    o.r21 = take_d(npix);
+    o.r22 = take_d(npix);
+    o.basis_identity_error = take_d(npix);
+    o.basis_rotation_angle = take_d(npix);
+    o.pass_a_steps = take_i(npix);
+    o.steps = take_i(npix);
+    o.reason = take_i(npix);
+    return o;
+}
+
+size_t carved_bytes(int npix, int nfreq) {
+    const size_t img = ((size_t(npix) * size_t(nfreq) * 8 + 255) / 256) * 256;
+    const size_t dpix = ((size_t(npix) * 8 + 255) / 256) * 256;
+    const size_t ipix = ((size_t(npix) * 4 + 255) / 256) * 256;
+    return 4 * img + 11 * dpix + 3 * ipix;
+}
+
+ImageOutPtrs from_abi(const kp_image_out* o) {
+    ImageOutPtrs p;
+    p.image_i = o->image_i;
+    p.image_q = o->image_q;
+    p.image_u = o->image_u;
+    p.image_v = o->image_v;
+    p.closure_x = o->closure_x;
+    p.closure_k = o->closure_k;
+    p.final_null = o->final_null;
+    p.frame_error = o->frame_error;
+    p.det_r = o->det_r;
+    p.r11 = o->overlap_r11;
+    p.r12 = o->overlap_r12;
+    p.r21 = o->overlap_r21;
+    p.r22 = o->overlap_r22;
+    p.basis_identity_error = o->basis_identity_error;
+    p.basis_rotation_angle = o->basis_rotation_angle;
+    p.pass_a_steps = o->pass_a_steps;
+    p.steps = o->steps;
+    p.reason = o->reason;
+    return p;
+}
+
+int check_outputs(const kp_image_out* out, int npix, int nfreq) {
+    if (!out) return set_error(KP_ERR_INVALID, "null output struct");
+    if (out->npix != npix || out->nfreq != nfreq)
+        return set_error(KP_ERR_INVALID, "output holds npix=%d nfreq=%d, image needs npix=%d nfreq=%d",
+                         out->npix, out->nfreq, npix, nfreq);
+    const void* ptrs[] = {out->image_i, out->image_q, out->image_u, out->image_v, out->closure_x,
+                          out->closure_k, out->final_null, out->frame_error, out->det_r,
+                          out->overlap_r11, out->overlap_r12, out->overlap_r21, out->overlap_r22,
+                          out->basis_identity_error, out->basis_rotation_angle, out->pass_a_steps,
+                          out->steps, out->reason};
+    for (const void* p : ptrs)
+        if (!p) return set_error(KP_ERR_INVALID, "null output array");
+    return KP_OK;
+}
+
+int copy_outputs_to_host(const ImageOutPtrs& d, const kp_image_out* h, int npix, int nfreq,
+                         cudaStream_t s) {
+    const size_t img = size_t(npix) * size_t(nfreq) * sizeof(double);
+    const size_t dp = size_t(npix) * sizeof(double);
+    const size_t ip = size_t(npix) * sizeof(int32_t);
+    struct Item {
+        void* dst;
+        const void* src;
+        size_t n;
+    } items[] = {
+        {h->image_i, d.image_i, img},          {h->image_q, d.image_q, img},
+        {h->image_u, d.image_u, img},          {h->image_v, d.image_v, img},
+        {h->closure_x, d.closure_x, dp},       {h->closure_k, d.closure_k, dp},
+        {h->final_null, d.final_null, dp},     {h->frame_error, d.frame_error, dp},
+        {h->det_r, d.det_r, dp},               {h->overlap_r11, d.r11, dp},
+        {h->overlap_r12, d.r12, dp},           {h->overlap_r21, d.r21, dp},
+        {h->overlap_r22, d.r22, dp},           {h->basis_identity_error, d.basis_identity_error, dp},
+        {h->basis_rotation_angle, d.basis_rotation_angle, dp},
+        {h->pass_a_steps, d.pass_a_steps, ip}, {h->steps, d.steps, ip},
+        {h->reason, d.reason, ip},
+    };
+    for (const Item& it : items) {
+        cudaError_t e = cudaMemcpyAsync(it.dst, it.src, it.n, cudaMemcpyDeviceToHost, s);
+        if (e != cudaSuccess) return cuda_error(e, "cudaMemcpyAsync(device to host)");
+    }
+    return KP_OK;
+}
+
+// isco_radius (src/model/riaf.hpp:166-174), evaluated on the host with libm.
+double isco_radius(double spin) {
+    const double a = spin;
+    const double one = 1.0;
+    const double z1 = one + std::cbrt(one - a * a) * (std::cbrt(one + a) + std::cbrt(one - a));
+    const double z2 = std::sqrt(3.0 * a * a + z1 * z1);
+    const double sign = a < 0.0 ? -1.0 : 1.0;
+    return 3.0 + z2 - sign * std::sqrt((3.0 - z1) * (3.0 + z1 + 2.0 * z2));
+}
+
+int validate_riaf(const kp_pass_a_params* p, const kp_riaf_model* m, const double* freqs, int nfreq) {
+    if (!p || !m) return set_error(KP_ERR_INVALID, "null params or model");
+    if (p->camera.nx <= 0 || p->camera.ny <= 0 || p->camera.nx > 2147483647 / p->camera.ny)
+        return set_error(KP_ERR_INVALID, "image dimensions must have a positive int-sized product");
+    if (nfreq < 1 || nfreq > KP_MAX_FREQUENCIES)
+        return set_error(KP_ERR_INVALID,
+                         "multifrequency image chunk size must be between 1 and KP_MAX_FREQUENCIES (%d)",
+                         KP_MAX_FREQUENCIES);
+    if (nfreq > 1 && !freqs) return set_error(KP_ERR_INVALID, "null frequency list");
+    switch (p->coordinate_system) {
+    case KP_COORD_CARTESIAN_KS: break;
+    case KP_COORD_BOYER_LINDQUIST:
+        return set_error(KP_ERR_UNSUPPORTED, "RIAF image coordinate backend not built: boyer_lindquist");
+    case KP_COORD_SPHERICAL_KS:
+        return set_error(KP_ERR_UNSUPPORTED, "RIAF image coordinate backend not built: spherical_ks");
+    case KP_COORD_FMKS:
+        return set_error(KP_ERR_UNSUPPORTED, "RIAF image coordinate backend not built: fmks");
+    case KP_COORD_MKS:
+        return set_error(KP_ERR_UNSUPPORTED, "RIAF image coordinate backend not built: mks");
+    default:
+        return set_error(KP_ERR_UNSUPPORTED, "RIAF image coordinate backend not built: unknown");
+    }
+    if (p->camera.model != KP_CAMERA_PINHOLE)
+        return set_error(KP_ERR_UNSUPPORTED, "only the pinhole camera is built for the GPU image path");
+    if (p->direct_only) return set_error(KP_ERR_UNSUPPORTED, "direct_only transport is not built");
+    if (p->emission_selection.equatorial_h_over_r > 0.0 && p->emission_selection.equatorial_h_over_r < 1.0)
+        return set_error(KP_ERR_UNSUPPORTED, "narrow equatorial emission wedge is not built");
+    if (m->emission_type != KP_FIT_PANDYA && m->emission_type != KP_FIT_DEXTER)
+        return set_error(KP_ERR_UNSUPPORTED,
+                         "emission_type %d: only thermal synchrotron (1 Pandya, 4 Dexter) is built",
+                         m->emission_type);
+    if (p->max_steps < 0) return set_error(KP_ERR_INVALID, "max_steps must be non-negative");
+    return KP_OK;
+}
+
+// Resolves one image's launch constants on the host.
+ImageConsts make_consts(const kp_pass_a_params* p, const kp_riaf_model* m, const double* freqs,
+                        int nfreq, int integrator) {
+    ImageConsts c;
+    std::memset(&c, 0, sizeof(c));
+    c.mass = p->mass;
+    c.spin = p->spin;
+    c.horizon = p->mass + std::sqrt(std::max(p->mass * p->mass - p->spin * p->spin, 0.0));
+    c.inner_radius = p->inner_radius;
+    c.outer_radius = p->outer_radius;
+    c.step = p->step;
+    c.min_step_abs = std::fabs(p->min_step);
+    c.max_step = p->max_step;
+    c.tolerance = p->adaptive_tolerance;
+    c.max_radiation_step = p->max_radiation_step;
+    c.max_radiation_depth = p->max_radiation_depth;
+    c.max_absorption_depth = p->max_absorption_depth;
+    c.max_faraday_depth = p->max_faraday_depth;
+    c.max_steps = p->max_steps;
+    c.adaptive = p->adaptive;
+    c.integrator = integrator;
+    c.faraday_rotation = p->emission_selection.faraday_rotation;
+    c.nx = p->camera.nx;
+    c.ny = p->camera.ny;
+    c.cam_radius = p->camera.radius;
+    c.sin_inc = std::sin(p->camera.inclination);
+    c.cos_inc = std::cos(p->camera.inclination);
+    c.fov = p->camera.fov;
+    c.fov_y = p->camera.fov_y;
+    c.xspan = p->camera.xspan;
+    c.yspan = p->camera.yspan;
+    c.x_offset = p->camera.x_offset;
+    c.y_offset = p->camera.y_offset;
+    c.nth0 = m->nth0;
+    c.Te0 = m->Te0;
+    c.disk_h = m->disk_h;
+    c.pow_nth = m->pow_nth;
+    c.pow_T = m->pow_T;
+    c.ne_unit = m->ne_unit;
+    c.r_min = m->r_min;
+    c.r_max = m->r_max;
+    c.horizon_buffer = m->horizon_buffer;
+    c.emission_scale = m->emission_scale;
+    c.absorption_scale = m->absorption_scale;
+    c.faraday_scale = m->faraday_scale;
+    c.max_pol_frac = m->max_pol_frac;
+    c.keplerian_factor = m->keplerian_factor;
+    c.infall_factor = m->infall_factor;
+    c.min_frequency_scale = m->min_frequency_scale;
+    c.min_sin_theta = m->min_sin_theta;
+    c.min_thetae = m->min_thetae;
+    c.min_radius = m->min_radius;
+    {
+        const double kbol = 1.380649e-16, me = 9.1093837015e-28, cl = 2.99792458e10;
+        c.thetae_unit = m->te_unit * kbol / (me * cl * cl);  // riaf.hpp:67-74
+    }
+    c.isco = isco_radius(p->spin);
+    c.fit = m->emission_type == KP_FIT_DEXTER ? 4 : 1;
+    c.nfreq = nfreq;
+    const double gnewt = 6.67430e-8, msun = 1.98847e33, cl = 2.99792458e10;
+    const double length_unit = gnewt * m->mbh_solar * msun / (cl * cl);  // riaf.hpp:76-81
+    for (int f = 0; f < nfreq; ++f) {
+        const double fr = (nfreq == 1 && !freqs) ? m->freq_cgs : freqs[f];
+        c.freq[f] = fr;
+        c.dlambda_scale[f] = length_unit / std::max(fr, 1.0);  // riaf.hpp:83-85
+        c.emission_scale_pow2[f] = 1.0f;
+        c.inv_emission_scale_pow2[f] = 1.0;
+    }
+    return c;
+}
+
+}  // namespace kp
+
+using namespace kp;
+
+extern "C" {
+
+const char* kp_last_error(void) { return g_error; }
+
+int kp_abi_version(void) { return KP_ABI_VERSION; }
+
+size_t kp_abi_sizeof(int which) {
+    switch (which) {
+    case 0: return sizeof(kp_camera_params);
+    case 1: return sizeof(kp_emission_selection);
+    case 2: return sizeof(kp_pass_a_params);
+    case 3: return sizeof(kp_riaf_model);
+    case 4: return sizeof(kp_image_out);
+    case 5: return sizeof(kp_run_options);
+    case 6: return sizeof(ImageConsts) + 5 * sizeof(D4) + sizeof(ImageOutPtrs);
+    default: return 0;
+    }
+}
+
+size_t kp_image_output_bytes(int npix, int nfreq) {
+    return size_t(npix) * (size_t(4 * nfreq + 11) * sizeof(double) + 3 * sizeof(int32_t));
+}
+
+void kp_default_run_options(kp_run_options* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->precision = KP_PRECISION_FP64;
+    o->schedule = KP_SCHEDULE_PER_PIXEL;
+    o->integrator = KP_INTEGRATOR_STEP_DOUBLING_RK4;
+}
+
+void kp_default_pass_a_params(kp_pass_a_params* p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->camera.nx = 64;
+    p->camera.ny = 64;
+    p->camera.radius = 100.0;
+    p->camera.inclination = 1.04719755119659774615;
+    p->camera.fov = 10.0;
+    p->camera.fov_y = -1.0;
+    p->camera.xspan = -1.0;
+    p->camera.yspan = -1.0;
+    p->camera.model = KP_CAMERA_PINHOLE;
+    p->emission_selection.equatorial_h_over_r = 0.0;
+    p->emission_selection.equatorial_samples = 8;
+    p->emission_selection.faraday_rotation = 1;
+    p->mass = 1.0;
+    p->spin = 0.0;
+    p->inner_radius = 2.2;
+    p->outer_radius = 200.0;
+    p->step = 0.05;
+    p->max_steps = 4096;
+    p->adaptive_tolerance = 1e-7;
+    p->min_step = 1e-5;
+    p->max_step = 1.0;
+    p->max_radiation_step = 1.0;
+    p->max_radiation_depth = 1.0;
+    p->max_absorption_depth = -1.0;
+    p->max_faraday_depth = -1.0;
+    p->fmks_hslope = 0.3;
+    p->fmks_mks_smooth = 0.5;
+    p->fmks_poly_alpha = 14.0;
+    p->fmks_poly_xt = 0.82;
+    p->fmks_poly_norm = 1.0;
+    p->coordinate_system = KP_COORD_CARTESIAN_KS;
+}
+
+void kp_default_riaf_model(kp_riaf_model* m) {
+    if (!m) return;
+    std::memset(m, 0, sizeof(*m));
+    m->nth0 = 1.0;
+    m->Te0 = 1.0;
+    m->disk_h = 0.35;
+    m->pow_nth = -1.1;
+    m->pow_T = -0.84;
+    m->ne_unit = 5.0e6;
+    m->te_unit = 1.0e11;
+    m->b_unit = 30.0;
+    m->freq_cgs = 230.0e9;
+    m->mbh_solar = 4.3e6;
+    m->r_min = 1.0;
+    m->r_max = 100.0;
+    m->horizon_buffer = 0.1;
+    m->emission_scale = 1.0;
+    m->absorption_scale = 1.0;
+    m->faraday_scale = 1.0;
+    m->max_pol_frac = 0.99;
+    m->keplerian_factor = 1.0;
+    m->infall_factor = 0.0;
+    m->emission_type = KP_FIT_PANDYA;
+    m->min_frequency_scale = 1e-6;
+    m->min_sin_theta = 1e-4;
+    m->min_thetae = 1e-3;
+    m->min_radius = 1e-6;
+}
+
+int kp_image_riaf(const kp_pass_a_params* params, const kp_riaf_model* model, int radiation_substeps,
+                  const double* frequencies, int nfreq, const kp_run_options* options,
+                  kp_image_out* out) {
+    (void)radiation_substeps;
+    kp_run_options opt;
+    if (options) {
+        opt = *options;
+    } else {
+        kp_default_run_options(&opt);
+    }
+    int st = validate_riaf(params, model, frequencies, nfreq);
+    if (st != KP_OK) return st;
+    const int npix = params->camera.nx * params->camera.ny;
+    st = check_outputs(out, npix, nfreq);
+    if (st != KP_OK) return st;
+    if (opt.integrator != KP_INTEGRATOR_STEP_DOUBLING_RK4 && opt.integrator != KP_INTEGRATOR_CASH_KARP)
+        return set_error(KP_ERR_INVALID, "unknown integrator %d", opt.integrator);
+    if (opt.precision != KP_PRECISION_FP64 && opt.precision != KP_PRECISION_MIXED)
+        return set_error(KP_ERR_INVALID, "unknown precision %d", opt.precision);
+    std::lock_guard<std::mutex> lock(g_mutex);
+    DeviceState* dev = device_state(opt.device, &st);
+    if (!dev) return st;
+    cudaStream_t stream = opt.stream ? static_cast<cudaStream_t>(opt.stream) : dev->stream;
+    const ImageConsts c = make_consts(params, model, frequencies, nfreq, opt.integrator);
+    ImageOutPtrs dptr;
+    if (opt.outputs_on_device) {
+        dptr = from_abi(out);
+    } else {
+        void* buf = device_output_buffer(dev, carved_bytes(npix, nfreq), &st);
+        if (!buf) return st;
+        dptr = carve_outputs(buf, npix, nfreq);
+    }
+    const auto t0 = std::chrono::steady_clock::now();
+    cudaError_t e;
+    if (opt.precision == KP_PRECISION_MIXED || opt.schedule == KP_SCHEDULE_PERSISTENT) {
+        return set_error(KP_ERR_UNSUPPORTED, "mixed precision / persistent schedule not built yet");
+    } else {
+        e = launch_image_fp64(c, dptr, stream);
+    }
+    if (e != cudaSuccess) return cuda_error(e, "image kernel launch");
+    if (opt.timing) {
+        e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) return cuda_error(e, "image kernel");
+        const double s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        std::printf("timing %s %g s\n", nfreq > 1 ? "image_kernel_multifrequency" : "image_kernel_single", s);
+    }
+    if (!opt.outputs_on_device) {
+        const auto t1 = std::chrono::steady_clock::now();
+        st = copy_outputs_to_host(dptr, out, npix, nfreq, stream);
+        if (st != KP_OK) return st;
+        e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) return cuda_error(e, "image kernel / device-to-host copy");
+        if (opt.timing) {
+            const double s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t1).count();
+            std::printf("timing %s %g s\n",
+                        nfreq > 1 ? "image_device_to_host_multifrequency" : "image_device_to_host_single", s);
+        }
+    } else if (!opt.stream) {
+        e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) return cuda_error(e, "image kernel");
+    }
+    return KP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,115 @@
+// kp_common.cuh -- shared device types and per-image launch constants for the
+// B200 GRRT kernels.  Geometry types are FP64; radiation types are templated
+// on the transfer precision R (double for the FP64 path, float for the mixed
+// path).
+#pragma once
+
+#include <cstdint>
+
+#ifndef KP_HD
+#define KP_HD __host__ __device__ __forceinline__
+#endif
+
+namespace kp {
+
+constexpr int kMaxFreq = 4;
+constexpr double kTiny = 1e-300;
+constexpr double kLarge = 1e300;
+constexpr double kPi = 3.141592653589793238462643383279502884;
+// 8 * DBL_EPSILON: adaptive_tolerance_floor (src/common/math.hpp:56-63).
+constexpr double kTolFloor = 8.0 * 2.220446049250313080847263336181640625e-16;
+
+enum Reason : int {
+    kNone = 0,
+    kReachedCamera = 1,
+    kReachedInner = 2,
+    kEscaped = 3,
+    kMaxSteps = 4,
+    kInvalidState = 5,
+    kAdaptiveUnderflow = 7,
+};
+
+template<class T> KP_HD T abs_val(T x) { return x < T(0) ? -x : x; }
+template<class T> KP_HD T min_val(T a, T b) { return a < b ? a : b; }
+template<class T> KP_HD T max_val(T a, T b) { return a > b ? a : b; }
+template<class T> KP_HD T clamp_val(T x, T lo, T hi) { return min_val(max_val(x, lo), hi); }
+template<class T> KP_HD T sq(T x) { return x * x; }
+
+struct D4 {
+    double v[4];
+};
+
+// Ray state: position x, future-directed wavevector k and the transported
+// screen basis e1, e2 (src/geodesic/state.hpp:7-16), 128 bytes.
+struct Ray {
+    D4 x, k, e1, e2;
+};
+
+template<class R>
+struct Stokes4 {
+    R I, Q, U, V;
+};
+
+template<class R>
+struct Coeffs {
+    R jI, jQ, jU, jV, aI, aQ, aU, aV, rQ, rU, rV;
+};
+
+// Everything one image needs on the device, resolved on the host.  Host-side
+// precomputation keeps libm (sin/cos of the inclination, cbrt in the ISCO
+// radius) on the CPU so the device geometry uses only + - * / sqrt and stays
+// bit-identical to the reference's CPU arithmetic.
+struct ImageConsts {
+    // spacetime (Kerr, M = mass)
+    double mass, spin;
+    double horizon;  // KerrSchildInMetric::horizon_radius
+    // integration (PassAParams, src/geodesic/pass_a_core.hpp:10-36)
+    double inner_radius, outer_radius, step;
+    double min_step_abs, max_step, tolerance;
+    double max_radiation_step, max_radiation_depth, max_absorption_depth, max_faraday_depth;
+    int max_steps, adaptive, integrator, faraday_rotation;
+    // pinhole camera (CameraParams, src/camera/camera.hpp:12-25)
+    int nx, ny;
+    double cam_radius, sin_inc, cos_inc;
+    double fov, fov_y, xspan, yspan, x_offset, y_offset;
+    // RIAF plasma (src/model/riaf.hpp:19-52)
+    double nth0, Te0, disk_h, pow_nth, pow_T, ne_unit;
+    double r_min, r_max, horizon_buffer;
+    double emission_scale, absorption_scale, faraday_scale, max_pol_frac;
+    double keplerian_factor, infall_factor;
+    double min_frequency_scale, min_sin_theta, min_thetae, min_radius;
+    double thetae_unit;  // te_unit * k_B / (m_e c^2)
+    double isco;         // isco_radius(spin), riaf.hpp:166-174
+    int fit;             // 1 Pandya, 4 Dexter
+    // frequencies sharing one geodesic
+    int nfreq;
+    double freq[kMaxFreq];
+    double dlambda_scale[kMaxFreq];  // length_unit / max(freq, 1)
+    // mixed path: per-image power-of-two scale applied to j and S
+    float emission_scale_pow2[kMaxFreq];
+    double inv_emission_scale_pow2[kMaxFreq];
+};
+
+// Device pointers of one image's outputs, laid out like ImageHostData.
+struct ImageOutPtrs {
+    double* image_i;
+    double* image_q;
+    double* image_u;
+    double* image_v;
+    double* closure_x;
+    double* closure_k;
+    double* final_null;
+    double* frame_error;
+    double* det_r;
+    double* r11;
+    double* r12;
+    double* r21;
+    double* r22;
+    double* basis_identity_error;
+    double* basis_rotation_angle;
+    int32_t* pass_a_steps;
+    int32_t* steps;
+    int32_t* reason;
+};
+
+}  // namespace kp

@@ -1,0 +1,94 @@
+"""Workload descriptions shared by the golden-fixture generator and the tests."""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from kpolaris_b200 import _abi, configs
+
+# Small image cases the CPU oracle finishes in well under a second each.
+IMAGE_CASES = {
+    # config 1 (fixed-step RK4, h = 1, 2000 steps, depth controls off) at 12^2
+    "riaf_cfg1_12": {"kind": "config1", "n": 12},
+    # config 2 (step-doubling RK4 tol 1e-8, four frequencies, depth 1/1/4) at 8^2
+    "riaf_cfg2_8": {"kind": "config2", "n": 8},
+    # Dexter fit, spin 0.5, inclination 163 deg, non-square 10x7, fixed h = 0.5
+    "riaf_dexter_10x7": {"kind": "custom", "nx": 10, "ny": 7, "spin": 0.5, "inclination_deg": 163.0,
+                         "step": 0.5, "adaptive": 0, "max_steps": 4000, "fit": 4, "xspan": 30.0,
+                         "freqs": [345.0e9]},
+    # close-in camera (r = 30) with rays captured by the hole, adaptive, 2 freqs
+    "riaf_capture_9": {"kind": "custom", "nx": 9, "ny": 9, "spin": 0.99, "inclination_deg": 60.0,
+                       "radius": 30.0, "xspan": 8.0, "step": 0.025, "adaptive": 1,
+                       "max_steps": 100000, "tolerance": 1e-8, "min_step": 1e-10,
+                       "max_step": 2.0, "max_radiation_step": 2.0, "depths": [1.0, 1.0, 4.0],
+                       "freqs": [86.0e9, 230.0e9]},
+    # wide field: corner rays miss the radiating sphere (escaped_domain)
+    "riaf_wide_escape_8": {"kind": "custom", "nx": 8, "ny": 8, "xspan": 150.0, "step": 1.0,
+                           "max_steps": 2000},
+    # step budget too small to reach the sphere (max_steps)
+    "riaf_maxsteps_6": {"kind": "custom", "nx": 6, "ny": 6, "step": 1.0, "max_steps": 600},
+}
+
+
+def build_case(spec: dict):
+    kind = spec["kind"]
+    if kind == "config1":
+        return configs.config1(spec["n"], spec["n"])
+    if kind == "config2":
+        return configs.config2(spec["n"], spec["n"])
+    depths = spec.get("depths", [-1.0, -1.0, -1.0])
+    params = configs.riaf_params(
+        spec["nx"], spec["ny"], spin=spec.get("spin", 0.9375),
+        radius=spec.get("radius", 1000.0), inclination_deg=spec.get("inclination_deg", 17.0),
+        xspan=spec.get("xspan", 80.0), step=spec.get("step", 1.0),
+        adaptive=spec.get("adaptive", 0), max_steps=spec.get("max_steps", 2000),
+        adaptive_tolerance=spec.get("tolerance", 1e-8), min_step=spec.get("min_step", 1e-5),
+        max_step=spec.get("max_step", 1.0), max_radiation_step=spec.get("max_radiation_step", 1.0),
+        max_radiation_depth=depths[0], max_absorption_depth=depths[1], max_faraday_depth=depths[2])
+    model = configs.riaf_model(fit=spec.get("fit", _abi.FIT_PANDYA))
+    return params, model, list(spec.get("freqs", [230.0e9]))
+
+
+def coefficient_points(n: int = 48, seed: int = 7):
+    """(fit, nu, ne, thetae, B, theta, sin, cos) points spanning the RIAF regime."""
+    rng = np.random.default_rng(seed)
+    pts = []
+    for i in range(n):
+        fit = 1 if i % 2 == 0 else 4
+        nu = 10 ** rng.uniform(10.5, 12.5)
+        ne = 10 ** rng.uniform(2.0, 7.0)
+        thetae = 10 ** rng.uniform(-0.5, 2.3)
+        b = 10 ** rng.uniform(-1.0, 2.5)
+        theta = rng.uniform(0.05, math.pi - 0.05)
+        pts.append((fit, nu, ne, thetae, b, theta, math.sin(theta), math.cos(theta)))
+    # the reference's symphony checkpoint state (tests/test_core.cpp:2196-2208)
+    th = math.pi / 3.0
+    pts.append((1, 230.0e9, 1.0, 10.0, 30.0, th, math.sin(th), math.cos(th)))
+    pts.append((4, 230.0e9, 1.0, 10.0, 30.0, th, math.sin(th), math.cos(th)))
+    return pts
+
+
+def transfer_points(n: int = 64, seed: int = 11):
+    """(Stokes, coefficients, dlambda) covering every branch of the Strang step."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        s4 = rng.normal(size=4) * 1e-3
+        s4[0] = abs(s4[0]) + np.linalg.norm(s4[1:])
+        c = np.zeros(11)
+        c[0] = abs(rng.normal())
+        c[1:4] = rng.normal(size=3) * 0.3 * c[0]
+        c[4] = abs(rng.normal()) * 10 ** rng.uniform(-8, 1)
+        c[5:8] = rng.normal(size=3) * 0.3 * c[4]
+        c[8:11] = rng.normal(size=3) * 10 ** rng.uniform(-10, 1)
+        branch = i % 4
+        if branch == 1:
+            c[5:8] = 0.0          # isotropic absorption branch
+        elif branch == 2:
+            c[8:11] *= 1e-9       # small-angle Faraday branch
+        elif branch == 3:
+            c[4] = 800.0          # attenuation cutoff branch (x > 700)
+        dl = 10 ** rng.uniform(-3, 0.5)
+        out.append((s4, c, dl))
+    return out

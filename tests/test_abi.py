@@ -1,0 +1,95 @@
+"""CPU tests of the C-ABI library: it loads, exports every entry point the
+public header declares, agrees with the ctypes mirror on struct layouts, and
+rejects invalid arguments before touching a device (no GPU needed)."""
+from __future__ import annotations
+
+import ctypes as C
+import re
+import subprocess
+from pathlib import Path
+
+import pytest
+
+import kpolaris_b200 as kp
+from kpolaris_b200 import _abi, configs
+
+ROOT = Path(__file__).resolve().parents[1]
+HEADER = ROOT / "include" / "kpolaris_b200.h"
+
+
+def declared_functions():
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(kp_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = kp.library()
+    names = declared_functions()
+    assert "kp_image_riaf" in names
+    for name in names:
+        assert hasattr(lib, name), name
+    out = subprocess.run(["nm", "-D", "--defined-only", str(kp.LIB_PATH)], capture_output=True,
+                         text=True, check=True).stdout
+    exported = set(re.findall(r" T (kp_[a-z0-9_]+)", out))
+    assert set(names) <= exported
+
+
+def test_struct_layouts_match_ctypes_mirror():
+    lib = kp.library()
+    lib.kp_abi_sizeof.restype = C.c_size_t
+    lib.kp_abi_sizeof.argtypes = [C.c_int]
+    mirrors = [_abi.CameraParams, _abi.EmissionSelection, _abi.PassAParams, _abi.RIAFModel,
+               _abi.ImageOut, _abi.RunOptions]
+    for i, s in enumerate(mirrors):
+        assert lib.kp_abi_sizeof(i) == C.sizeof(s), s.__name__
+    assert lib.kp_abi_sizeof(99) == 0
+
+
+def test_defaults_match_reference_struct_defaults():
+    lib = kp.library()
+    p = _abi.PassAParams()
+    lib.kp_default_pass_a_params(C.byref(p))
+    q = _abi.default_pass_a_params()
+    assert bytes(p) == bytes(q)
+    m = _abi.RIAFModel()
+    lib.kp_default_riaf_model(C.byref(m))
+    assert bytes(m) == bytes(_abi.default_riaf_model())
+
+
+def test_output_bytes_match_reference_batch_budget():
+    # 15 doubles + 3 int32 per pixel for one frequency (batch_driver.hpp:49)
+    assert kp.library().kp_image_output_bytes(100, 1) == 132 * 100
+    assert kp.library().kp_image_output_bytes(10, 4) == 10 * (27 * 8 + 12)
+
+
+@pytest.mark.parametrize("mutate,status", [
+    (lambda p, m: setattr(p.camera, "nx", 0), _abi.KP_ERR_INVALID),
+    (lambda p, m: setattr(p, "coordinate_system", _abi.COORD_BOYER_LINDQUIST), _abi.KP_ERR_UNSUPPORTED),
+    (lambda p, m: setattr(p, "coordinate_system", _abi.COORD_FMKS), _abi.KP_ERR_UNSUPPORTED),
+    (lambda p, m: setattr(p, "direct_only", 1), _abi.KP_ERR_UNSUPPORTED),
+    (lambda p, m: setattr(m, "emission_type", 2), _abi.KP_ERR_UNSUPPORTED),
+    (lambda p, m: setattr(p.emission_selection, "equatorial_h_over_r", 0.2), _abi.KP_ERR_UNSUPPORTED),
+])
+def test_invalid_arguments_are_rejected_before_launch(mutate, status):
+    params, model, freqs = configs.config1(4, 4)
+    mutate(params, model)
+    with pytest.raises(kp.KPolarisError) as ei:
+        kp.image_riaf(params, model, freqs, out=_abi.ImageHostData.allocate(16, 1))
+    assert ei.value.status == status
+
+
+def test_frequency_count_limits():
+    params, model, _ = configs.config1(4, 4)
+    with pytest.raises(kp.KPolarisInvalidArgument):
+        kp.run_riaf_multifrequency_image(params, model, 1, [1e11] * 5)
+    with pytest.raises(kp.KPolarisInvalidArgument):
+        kp.run_riaf_multifrequency_image(params, model, 1, [], [])
+    with pytest.raises(kp.KPolarisError):
+        kp.run_riaf_multifrequency_image(params, model, 1, [1e11, 2e11], [1e11])
+
+
+def test_output_shape_mismatch_is_rejected():
+    params, model, freqs = configs.config1(4, 4)
+    with pytest.raises(kp.KPolarisInvalidArgument):
+        kp.image_riaf(params, model, freqs, out=_abi.ImageHostData.allocate(15, 1))
