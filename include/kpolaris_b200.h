@@ -276,6 +276,44 @@ int kp_image_riaf(const kp_pass_a_params* params,
                   const kp_run_options* options,
                   kp_image_out* out);
 
+/* One image of a batch: the arguments of one kp_image_riaf call. */
+typedef struct kp_riaf_job {
+    kp_pass_a_params params;
+    kp_riaf_model model;
+    double frequencies[KP_MAX_FREQUENCIES];
+    int nfreq;
+    int radiation_substeps;
+    kp_image_out out;
+} kp_riaf_job;
+
+/* Per-call counters of kp_batch_riaf (reference ImageBatchTiming,
+ * src/image/batch_driver.hpp:34-40, plus launch facts). */
+typedef struct kp_batch_stats {
+    double kernel_seconds;       /* device time of the launch (CUDA events) */
+    double copy_seconds;         /* device-to-host copies (host outputs only) */
+    long long rays;              /* pixels traced */
+    int launches;                /* kernels launched */
+    int blocks;                  /* CTAs of the persistent launch */
+    int threads_per_block;
+    size_t device_output_bytes;  /* library-owned output scratch used */
+} kp_batch_stats;
+
+/*
+ * A batch of RIAF images traced by ONE persistent launch whose lanes drain a
+ * ray queue spanning every image (continuous refill), so images of any size,
+ * spin, inclination and frequency count share the GPU.  Replaces the
+ * reference's experimental host batching run_image_batch_metric
+ * (src/image/batch_driver.hpp:127-187), which launches one kernel per image
+ * on a few streams.  Every job is validated before anything is launched; an
+ * invalid job fails the whole call (KP_ERR_INVALID / KP_ERR_UNSUPPORTED).
+ * With KP_PRECISION_FP64 each image is bit-identical to the same image
+ * traced alone by kp_image_riaf; KP_PRECISION_MIXED images agree with them
+ * within the mixed-precision tolerance and are also independent of the
+ * batch composition.  `stats` may be NULL.
+ */
+int kp_batch_riaf(const kp_riaf_job* jobs, int njobs, const kp_run_options* options,
+                  kp_batch_stats* stats);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

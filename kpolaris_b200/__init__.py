@@ -8,6 +8,7 @@ fallback: if the library is missing, loading fails loudly.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from pathlib import Path
 
 import numpy as np
@@ -22,7 +23,7 @@ __all__ = [
     "run_riaf_image", "run_riaf_multifrequency_image", "image_riaf",
 ]
 
-LIB_PATH = Path(__file__).resolve().parent / "lib" / "libkpolaris_b200.so"
+LIB_PATH = Path(os.environ.get("KPOLARIS_B200_LIB") or Path(__file__).resolve().parent / "lib" / "libkpolaris_b200.so")
 
 
 class KPolarisError(RuntimeError):
@@ -55,6 +56,11 @@ def library() -> C.CDLL:
     L.kp_image_riaf.argtypes = [C.POINTER(PassAParams), C.POINTER(RIAFModel), C.c_int,
                                 C.POINTER(C.c_double), C.c_int, C.POINTER(RunOptions),
                                 C.POINTER(_abi.ImageOut)]
+    L.kp_batch_riaf.argtypes = [C.POINTER(_abi.RiafJob), C.c_int, C.POINTER(RunOptions),
+                                C.POINTER(_abi.BatchStats)]
+    L.kp_abi_sizeof.restype = C.c_size_t
+    L.kp_abi_sizeof.argtypes = [C.c_int]
+    L.kp_measure_fma_peak.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_double)]
     L.kp_default_run_options.argtypes = [C.POINTER(RunOptions)]
     L.kp_default_pass_a_params.argtypes = [C.POINTER(PassAParams)]
     L.kp_default_riaf_model.argtypes = [C.POINTER(RIAFModel)]
@@ -102,6 +108,41 @@ def image_riaf(params: PassAParams, model: RIAFModel, frequencies=None, *, radia
     check(L.kp_image_riaf(C.byref(params), C.byref(model), int(radiation_substeps), fa, nfreq,
                           C.byref(opt), C.byref(s)))
     return out
+
+
+def batch_riaf(jobs, *, outs=None, precision=_abi.PRECISION_MIXED, stats=None, **options):
+    """Traces a list of RIAF images in one persistent launch (kp_batch_riaf).
+
+    jobs: iterable of (PassAParams, RIAFModel, frequencies).  Returns a list of
+    ImageHostData.  `stats`, if given, is a BatchStats filled by the call."""
+    L = library()
+    jobs = list(jobs)
+    arr = (_abi.RiafJob * max(1, len(jobs)))()
+    results = []
+    for i, (params, model, freqs) in enumerate(jobs):
+        freqs = list(freqs) if freqs is not None else [model.freq_cgs]
+        npix = params.camera.nx * params.camera.ny
+        res = outs[i] if outs is not None else ImageHostData.allocate(npix, len(freqs))
+        results.append(res)
+        j = arr[i]
+        j.params = params
+        j.model = model
+        for f, v in enumerate(freqs[:_abi.KP_MAX_FREQUENCIES]):
+            j.frequencies[f] = v
+        j.nfreq = len(freqs)
+        j.radiation_substeps = 1
+        j.out = res.as_struct()
+    opt = _options(precision=precision, schedule=_abi.SCHEDULE_PERSISTENT, **options)
+    st = stats if stats is not None else _abi.BatchStats()
+    check(L.kp_batch_riaf(arr, len(jobs), C.byref(opt), C.byref(st)))
+    return results
+
+
+def measure_fma_peak(device: int = 0, fp64: bool = True) -> float:
+    """Measured FMA throughput of the device in TFLOP/s (kp_measure_fma_peak)."""
+    out = C.c_double(0.0)
+    check(library().kp_measure_fma_peak(int(device), 1 if fp64 else 0, C.byref(out)))
+    return out.value
 
 
 def run_riaf_image(pass_a: PassAParams, model: RIAFModel, radiation_substeps: int = 1,

@@ -134,6 +134,22 @@ class RunOptions(C.Structure):
     ]
 
 
+class RiafJob(C.Structure):
+    _fields_ = [
+        ("params", PassAParams), ("model", RIAFModel),
+        ("frequencies", C.c_double * KP_MAX_FREQUENCIES), ("nfreq", C.c_int),
+        ("radiation_substeps", C.c_int), ("out", ImageOut),
+    ]
+
+
+class BatchStats(C.Structure):
+    _fields_ = [
+        ("kernel_seconds", C.c_double), ("copy_seconds", C.c_double), ("rays", C.c_longlong),
+        ("launches", C.c_int), ("blocks", C.c_int), ("threads_per_block", C.c_int),
+        ("device_output_bytes", C.c_size_t),
+    ]
+
+
 IMAGE_FIELDS = ("image_i", "image_q", "image_u", "image_v")
 DIAG_FIELDS = ("closure_x", "closure_k", "final_null", "frame_error", "det_r",
                "overlap_r11", "overlap_r12", "overlap_r21", "overlap_r22",

@@ -66,9 +66,6 @@ KP_HD D4 native_vector_phi0_cks(double spin, double v0, double vx1, double vx2, 
 }
 
 // Camera position, tetrad e0..e3 (position-only, identical for every pixel).
-struct CameraFrame {
-    D4 x, e0, e1, e2, e3;
-};
 
 KP_HD CameraFrame camera_frame(const ImageConsts& c) {
     const double mass = c.mass, spin = c.spin;
@@ -129,7 +126,7 @@ KP_HD CameraFrame camera_frame(const ImageConsts& c) {
 }
 
 // initialize_pinhole_camera_ray (camera.hpp:485-513) from a precomputed frame.
-__device__ __noinline__ Ray camera_ray(const ImageConsts& c, const CameraFrame& f, int pixel) {
+static __device__ __noinline__ Ray camera_ray(const ImageConsts& c, const CameraFrame& f, int pixel) {
     const KSMetricPoint w = ks_point(c.mass, c.spin, f.x);
     double sx = 0.0, sy = 0.0;
     pixel_offsets(pixel, c, sx, sy);

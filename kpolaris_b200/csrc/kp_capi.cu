@@ -39,10 +39,17 @@ int cuda_error(cudaError_t e, const char* what) {
 // buffers reused across calls.
 struct DeviceState {
     int initialised = 0;
+    int sms = 0;
     cudaStream_t stream = nullptr;
     void* out_buf = nullptr;
     size_t out_bytes = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // persistent launches
+    JobDesc* d_jobs = nullptr;      // device job table (grow-only)
+    JobDesc* h_jobs = nullptr;      // pinned staging of the job table
+    int jobs_cap = 0;
+    cudaEvent_t staging_free = nullptr;  // last upload from h_jobs has completed
+    unsigned long long* d_queue = nullptr;  // [0] ray-queue head, [1] status word
 };
 
 static std::mutex g_mutex;
@@ -67,6 +74,13 @@ DeviceState* device_state(int device, int* status) {
         }
         cudaEventCreate(&d.ev0);
         cudaEventCreate(&d.ev1);
+        cudaEventCreateWithFlags(&d.staging_free, cudaEventDisableTiming);
+        cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, device);
+        e = cudaMalloc(&d.d_queue, 2 * sizeof(unsigned long long));
+        if (e != cudaSuccess) {
+            *status = cuda_error(e, "cudaMalloc(queue)");
+            return nullptr;
+        }
         d.initialised = 1;
     }
     *status = KP_OK;
@@ -210,6 +224,29 @@ double isco_radius(double spin) {
     return 3.0 + z2 - sign * std::sqrt((3.0 - z1) * (3.0 + z1 + 2.0 * z2));
 }
 
+// Exponent E of the FP32 emission scale 2^E of one frequency (mixed path).
+// The invariant emissivity j ~ n_e e^2 nu_c / (c nu^2) is 1e-38..1e-48 in CGS,
+// below FP32 range; E is chosen so that the emission of one radiation step
+// at a reference plasma point (r = max(r_min, 3), equator, unit shape
+// factor bound 30) is 2^-6.  The transfer equation is linear in (j, S), so
+// the image is exactly rescaled by 2^-E in FP64 at the end.
+int emission_scale_exponent(const kp_pass_a_params* p, const kp_riaf_model* m, double freq, double dls) {
+    const double kPiD = 3.141592653589793, ee = 4.803204712570263e-10, me = 9.1093837015e-28,
+                 cl = 2.99792458e10, mp = 1.67262192369e-24, kbol = 1.380649e-16;
+    const double r_ref = std::max(m->r_min, 3.0);
+    const double ne = std::max(m->ne_unit * m->nth0 * std::pow(r_ref, m->pow_nth), 1e-30);
+    const double b = std::sqrt(8.0 * kPiD * 0.1 * ne * mp * cl * cl / (6.0 * r_ref));
+    const double nu_c = ee * b / (2.0 * kPiD * me * cl);
+    const double j_phys = ne * ee * ee * nu_c / cl * (std::sqrt(2.0) * kPiD / 27.0) * 30.0;
+    const double j_inv = j_phys / std::max(freq * freq, 1.0);
+    const double step = p->max_radiation_step > 0.0 ? p->max_radiation_step : std::max(p->max_step, 1e-3);
+    const double dl = std::max(step * std::fabs(dls), 1e-300);
+    (void)kbol;
+    double e = std::floor(std::log2(std::ldexp(1.0, -6) / std::max(j_inv * dl, 1e-300)));
+    if (!(e == e)) e = 0.0;
+    return int(std::min(120.0, std::max(-120.0, e)));
+}
+
 int validate_riaf(const kp_pass_a_params* p, const kp_riaf_model* m, const double* freqs, int nfreq) {
     if (!p || !m) return set_error(KP_ERR_INVALID, "null params or model");
     if (p->camera.nx <= 0 || p->camera.ny <= 0 || p->camera.nx > 2147483647 / p->camera.ny)
@@ -302,6 +339,7 @@ ImageConsts make_consts(const kp_pass_a_params* p, const kp_riaf_model* m, const
         c.thetae_unit = m->te_unit * kbol / (me * cl * cl);  // riaf.hpp:67-74
     }
     c.isco = isco_radius(p->spin);
+    c.fp32_radius = p->outer_radius + 2.0 * std::fabs(p->max_step);
     c.fit = m->emission_type == KP_FIT_DEXTER ? 4 : 1;
     c.nfreq = nfreq;
     const double gnewt = 6.67430e-8, msun = 1.98847e33, cl = 2.99792458e10;
@@ -310,8 +348,9 @@ ImageConsts make_consts(const kp_pass_a_params* p, const kp_riaf_model* m, const
         const double fr = (nfreq == 1 && !freqs) ? m->freq_cgs : freqs[f];
         c.freq[f] = fr;
         c.dlambda_scale[f] = length_unit / std::max(fr, 1.0);  // riaf.hpp:83-85
-        c.emission_scale_pow2[f] = 1.0f;
-        c.inv_emission_scale_pow2[f] = 1.0;
+        const int e = emission_scale_exponent(p, m, fr, c.dlambda_scale[f]);
+        c.emission_scale_pow2[f] = std::ldexp(1.0f, e);
+        c.inv_emission_scale_pow2[f] = std::ldexp(1.0, -e);
     }
     return c;
 }
@@ -435,6 +474,18 @@ int kp_image_riaf(const kp_pass_a_params* params, const kp_riaf_model* model, in
         return set_error(KP_ERR_INVALID, "unknown integrator %d", opt.integrator);
     if (opt.precision != KP_PRECISION_FP64 && opt.precision != KP_PRECISION_MIXED)
         return set_error(KP_ERR_INVALID, "unknown precision %d", opt.precision);
+    if (opt.precision == KP_PRECISION_MIXED || opt.schedule == KP_SCHEDULE_PERSISTENT) {
+        // the persistent engine: a batch of one
+        kp_riaf_job job;
+        std::memset(&job, 0, sizeof(job));
+        job.params = *params;
+        job.model = *model;
+        for (int f = 0; f < nfreq; ++f) job.frequencies[f] = frequencies ? frequencies[f] : model->freq_cgs;
+        job.nfreq = nfreq;
+        job.radiation_substeps = radiation_substeps;
+        job.out = *out;
+        return kp_batch_riaf(&job, 1, &opt, nullptr);
+    }
     std::lock_guard<std::mutex> lock(g_mutex);
     DeviceState* dev = device_state(opt.device, &st);
     if (!dev) return st;
@@ -449,12 +500,7 @@ int kp_image_riaf(const kp_pass_a_params* params, const kp_riaf_model* model, in
         dptr = carve_outputs(buf, npix, nfreq);
     }
     const auto t0 = std::chrono::steady_clock::now();
-    cudaError_t e;
-    if (opt.precision == KP_PRECISION_MIXED || opt.schedule == KP_SCHEDULE_PERSISTENT) {
-        return set_error(KP_ERR_UNSUPPORTED, "mixed precision / persistent schedule not built yet");
-    } else {
-        e = launch_image_fp64(c, dptr, stream);
-    }
+    cudaError_t e = launch_image_fp64(c, dptr, stream);
     if (e != cudaSuccess) return cuda_error(e, "image kernel launch");
     if (opt.timing) {
         e = cudaStreamSynchronize(stream);
@@ -476,6 +522,169 @@ int kp_image_riaf(const kp_pass_a_params* params, const kp_riaf_model* model, in
     } else if (!opt.stream) {
         e = cudaStreamSynchronize(stream);
         if (e != cudaSuccess) return cuda_error(e, "image kernel");
+    }
+    return KP_OK;
+}
+
+int kp_batch_riaf(const kp_riaf_job* jobs, int njobs, const kp_run_options* options, kp_batch_stats* stats) {
+    kp_run_options opt;
+    if (options) {
+        opt = *options;
+    } else {
+        kp_default_run_options(&opt);
+        opt.schedule = KP_SCHEDULE_PERSISTENT;
+    }
+    if (stats) std::memset(stats, 0, sizeof(*stats));
+    if (njobs < 0 || (njobs > 0 && !jobs)) return set_error(KP_ERR_INVALID, "invalid job list");
+    if (njobs == 0) return KP_OK;
+    if (opt.precision != KP_PRECISION_FP64 && opt.precision != KP_PRECISION_MIXED)
+        return set_error(KP_ERR_INVALID, "unknown precision %d", opt.precision);
+    if (opt.integrator != KP_INTEGRATOR_STEP_DOUBLING_RK4 && opt.integrator != KP_INTEGRATOR_CASH_KARP)
+        return set_error(KP_ERR_INVALID, "unknown integrator %d", opt.integrator);
+    // Validate every job before launching any work (batch_driver.hpp:137-145).
+    long long total = 0;
+    int nf_max = 1;
+    size_t scratch = 0;
+    for (int i = 0; i < njobs; ++i) {
+        const kp_riaf_job& jb = jobs[i];
+        int st = validate_riaf(&jb.params, &jb.model, jb.frequencies, jb.nfreq);
+        if (st != KP_OK) return set_error(st, "job %d: %s", i, g_error);
+        if (jb.radiation_substeps < 1) return set_error(KP_ERR_INVALID, "job %d: batch radiation_substeps must be positive", i);
+        const int npix = jb.params.camera.nx * jb.params.camera.ny;
+        st = check_outputs(&jb.out, npix, jb.nfreq);
+        if (st != KP_OK) return set_error(st, "job %d: %s", i, g_error);
+        total += npix;
+        nf_max = std::max(nf_max, jb.nfreq);
+        scratch += carved_bytes(npix, jb.nfreq);
+    }
+    // The mixed kernel always carries four channels: the same compiled code
+    // traces a ray whatever the other jobs of the batch are.
+    if (opt.precision == KP_PRECISION_MIXED) nf_max = KP_MAX_FREQUENCIES;
+    std::lock_guard<std::mutex> lock(g_mutex);
+    int st = KP_OK;
+    DeviceState* dev = device_state(opt.device, &st);
+    if (!dev) return st;
+    cudaStream_t stream = opt.stream ? static_cast<cudaStream_t>(opt.stream) : dev->stream;
+    // job table storage
+    if (njobs > dev->jobs_cap) {
+        cudaEventSynchronize(dev->staging_free);
+        if (dev->d_jobs) cudaFree(dev->d_jobs);
+        if (dev->h_jobs) cudaFreeHost(dev->h_jobs);
+        dev->d_jobs = nullptr;
+        dev->h_jobs = nullptr;
+        dev->jobs_cap = 0;
+        const int cap = std::max(njobs, 64);
+        cudaError_t e = cudaMalloc(&dev->d_jobs, sizeof(JobDesc) * size_t(cap));
+        if (e != cudaSuccess) return set_error(KP_ERR_OOM, "cudaMalloc(job table): %s", cudaGetErrorString(e));
+        e = cudaMallocHost(&dev->h_jobs, sizeof(JobDesc) * size_t(cap));
+        if (e != cudaSuccess) return set_error(KP_ERR_OOM, "cudaMallocHost(job table): %s", cudaGetErrorString(e));
+        dev->jobs_cap = cap;
+    }
+    void* scratch_base = nullptr;
+    if (!opt.outputs_on_device) {
+        scratch_base = device_output_buffer(dev, scratch, &st);
+        if (!scratch_base) return st;
+    }
+    // the previous upload from the staging table must be complete before it is rewritten
+    cudaEventSynchronize(dev->staging_free);
+    std::vector<ImageOutPtrs> dptrs(static_cast<size_t>(njobs));
+    long long ray = 0;
+    char* carve = static_cast<char*>(scratch_base);
+    for (int i = 0; i < njobs; ++i) {
+        const kp_riaf_job& jb = jobs[i];
+        const int npix = jb.params.camera.nx * jb.params.camera.ny;
+        JobDesc& d = dev->h_jobs[i];
+        std::memset(&d, 0, sizeof(d));
+        d.c = make_consts(&jb.params, &jb.model, jb.frequencies, jb.nfreq, opt.integrator);
+        double fr[5][4];
+        host_camera_frame(d.c, fr);
+        for (int mu = 0; mu < 4; ++mu) {
+            d.frame.x.v[mu] = fr[0][mu];
+            d.frame.e0.v[mu] = fr[1][mu];
+            d.frame.e1.v[mu] = fr[2][mu];
+            d.frame.e2.v[mu] = fr[3][mu];
+            d.frame.e3.v[mu] = fr[4][mu];
+        }
+        if (opt.outputs_on_device) {
+            d.out = from_abi(&jb.out);
+        } else {
+            d.out = carve_outputs(carve, npix, jb.nfreq);
+            carve += carved_bytes(npix, jb.nfreq);
+        }
+        dptrs[size_t(i)] = d.out;
+        d.ray_begin = ray;
+        d.npix = npix;
+        d.precision = opt.precision;
+        ray += npix;
+    }
+    cudaError_t e = cudaMemcpyAsync(dev->d_jobs, dev->h_jobs, sizeof(JobDesc) * size_t(njobs),
+                                    cudaMemcpyHostToDevice, stream);
+    if (e != cudaSuccess) return cuda_error(e, "cudaMemcpyAsync(job table)");
+    cudaEventRecord(dev->staging_free, stream);
+    e = cudaMemsetAsync(dev->d_queue, 0, 2 * sizeof(unsigned long long), stream);
+    if (e != cudaSuccess) return cuda_error(e, "cudaMemsetAsync(queue)");
+    LaunchDesc L;
+    L.jobs = dev->d_jobs;
+    L.njobs = njobs;
+    L.total_rays = total;
+    L.next_ray = dev->d_queue;
+    L.refill = opt.schedule == KP_SCHEDULE_PERSISTENT || opt.precision == KP_PRECISION_MIXED ? 1 : 0;
+    L.r_fp64 = 6.0;
+    L.status = reinterpret_cast<int*>(dev->d_queue + 1);
+    const int threads = opt.threads_per_block > 0 ? opt.threads_per_block : 128;
+    if (threads % 32 != 0 || threads > 1024)
+        return set_error(KP_ERR_INVALID, "threads_per_block must be a multiple of 32 up to 1024");
+    int blocks;
+    if (L.refill) {
+        int per_sm = opt.blocks_per_sm;
+        if (per_sm <= 0) {
+            per_sm = opt.precision == KP_PRECISION_MIXED ? persistent_occupancy_mixed(nf_max, threads)
+                                                         : persistent_occupancy_fp64(nf_max, threads);
+            if (per_sm <= 0) per_sm = 1;
+        }
+        blocks = dev->sms * per_sm;
+        const long long needed = (total + threads - 1) / threads;
+        if (blocks > needed) blocks = int(needed);
+    } else {
+        blocks = int((total + threads - 1) / threads);
+    }
+    cudaEventRecord(dev->ev0, stream);
+    e = opt.precision == KP_PRECISION_MIXED ? launch_persistent_mixed(L, nf_max, blocks, threads, stream)
+                                            : launch_persistent_fp64(L, nf_max, blocks, threads, stream);
+    if (e != cudaSuccess) return cuda_error(e, "persistent image kernel launch");
+    cudaEventRecord(dev->ev1, stream);
+    if (stats) {
+        stats->rays = total;
+        stats->launches = 1;
+        stats->blocks = blocks;
+        stats->threads_per_block = threads;
+        stats->device_output_bytes = opt.outputs_on_device ? 0 : scratch;
+    }
+    const bool must_sync = !opt.outputs_on_device || !opt.stream || stats || opt.timing;
+    if (!must_sync) return KP_OK;
+    e = cudaEventSynchronize(dev->ev1);
+    if (e != cudaSuccess) return cuda_error(e, "persistent image kernel");
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, dev->ev0, dev->ev1);
+    if (stats) stats->kernel_seconds = ms * 1e-3;
+    if (opt.timing) std::printf("timing image_kernel_batch %g s\n", ms * 1e-3);
+    int status_word = 0;
+    e = cudaMemcpy(&status_word, L.status, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_error(e, "status read");
+    if (status_word != 0)
+        return set_error(KP_ERR_TIMEOUT, "a ray exceeded the engine's iteration guard (status %d)", status_word);
+    if (!opt.outputs_on_device) {
+        const auto t1 = std::chrono::steady_clock::now();
+        for (int i = 0; i < njobs; ++i) {
+            st = copy_outputs_to_host(dptrs[size_t(i)], &jobs[i].out, jobs[i].params.camera.nx * jobs[i].params.camera.ny,
+                                      jobs[i].nfreq, stream);
+            if (st != KP_OK) return st;
+        }
+        e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) return cuda_error(e, "device-to-host copy");
+        const double s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t1).count();
+        if (stats) stats->copy_seconds = s;
+        if (opt.timing) std::printf("timing image_device_to_host_batch %g s\n", s);
     }
     return KP_OK;
 }

@@ -80,6 +80,9 @@ struct ImageConsts {
     double min_frequency_scale, min_sin_theta, min_thetae, min_radius;
     double thetae_unit;  // te_unit * k_B / (m_e c^2)
     double isco;         // isco_radius(spin), riaf.hpp:166-174
+    // mixed policy: FP32 connection contraction for RK jobs that start beyond
+    // this radius (outside the radiating sphere by two maximal steps)
+    double fp32_radius;
     int fit;             // 1 Pandya, 4 Dexter
     // frequencies sharing one geodesic
     int nfreq;
@@ -110,6 +113,33 @@ struct ImageOutPtrs {
     int32_t* pass_a_steps;
     int32_t* steps;
     int32_t* reason;
+};
+
+// Camera position and ipole tetrad e0..e3 at phi = 0 (identical for every
+// pixel of an image; evaluated once on the host).
+struct CameraFrame {
+    D4 x, e0, e1, e2, e3;
+};
+
+// One image (job) of a persistent launch.
+struct JobDesc {
+    ImageConsts c;
+    CameraFrame frame;
+    ImageOutPtrs out;
+    long long ray_begin;  // first global ray index of this job
+    int npix;
+    int precision;        // kp_precision of this job
+};
+
+// Device-side launch description (kernel parameter).
+struct LaunchDesc {
+    const JobDesc* jobs;           // device array, ordered by ray_begin
+    int njobs;
+    long long total_rays;
+    unsigned long long* next_ray;  // ray-queue head, zeroed before the launch
+    int refill;                    // 0: lane i traces ray i only (no queue)
+    double r_fp64;                 // mixed policy: FP64 contraction inside this radius
+    int* status;                   // device error word (0 ok)
 };
 
 }  // namespace kp

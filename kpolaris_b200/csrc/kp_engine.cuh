@@ -1,0 +1,248 @@
+// kp_engine.cuh -- persistent ray engine: every lane of a warp holds one ray
+// and advances it through a resumable state machine whose loop iteration is
+// one RK job (a step-doubling attempt, an RK4 step, a composed pair of RK4
+// half steps or a Cash-Karp attempt) started from the lane's current state.
+// Jobs run as a stage loop around ONE right-hand-side site, so lanes of a warp
+// evaluate the RHS together whatever their phase (pass A, surface refinement,
+// pass B, camera crossing).  Finished lanes refill from a global ray queue
+// shared by every image of the launch (warp-aggregated atomics), which removes
+// both the tail of uneven rays and the launch-per-image cost.
+//
+// The control machine restates, as explicit states, the loops of
+// trace_pass_b_segment_model_pixel_metric / _multifrequency_pixel_metric
+// (src/geodesic/pass_b.hpp:769-1114, :1131-1501), adaptive_rk4_step
+// (src/geodesic/rk4.hpp:108-161) and locate_metric_surface_crossing
+// (src/geodesic/pass_a_core.hpp:94-197).  With the FP64 policy every
+// arithmetic operation is the reference's, in its order: results are
+// bit-identical to the per-pixel FP64 kernel.
+#pragma once
+
+#include "kp_camera.cuh"
+#include "kp_integrate.cuh"
+#include "kp_radiation.cuh"
+#include "kp_trace_fp64.cuh"
+#include "kp_geometry_f32.cuh"
+#include "kp_radiation_f32.cuh"
+
+namespace kp {
+
+// One image (job) of a launch.
+enum RkKind : int { kRkSD = 0, kRkRK4 = 1, kRkRK4x2 = 2, kRkCK = 3 };
+
+// Control modes: what the pending RK job's result is for.
+enum Mode : int {
+    kIdle = 0,
+    kAStep = 1,        // pass-A step attempt (adaptive sequence or fixed RK4)
+    kACrossHi = 2,     // crossing search: full-step endpoint with the trial evaluator
+    kACrossTrial = 3,  // crossing search: trial at fraction `trial`
+    kBStep = 4,        // pass-B step attempt
+    kBCamCross = 5,    // pass-B partial step to the camera surface
+    kDone = 6,
+};
+
+// ---------------------------------------------------------------- RHS policy
+// FP64 policy: the reference's arithmetic.
+struct PolicyFP64 {
+    static constexpr bool kMixed = false;
+};
+// Mixed policy: FP32 connection contraction outside r_fp64 when the whole
+// warp is outside it; FP64 state, stage combination and step control.
+struct PolicyMixed {
+    static constexpr bool kMixed = true;
+};
+
+// Radiation side of a policy: FP64 (the reference's arithmetic) or FP32 with
+// the per-frequency 2^E emission scale (kp_radiation_f32.cuh).
+template<class P>
+struct RadTraits;
+
+template<>
+struct RadTraits<PolicyFP64> {
+    using Stokes = Stokes4<double>;
+    using Co = Coeffs<double>;
+    using Sample = RiafSample;
+    __device__ static void zero(Stokes& s) { s = Stokes4<double>{0.0, 0.0, 0.0, 0.0}; }
+    __device__ static Sample sample(const ImageConsts& c, const Ray& r) { return riaf_sample(c, r); }
+    __device__ static Sample none() {
+        Sample s;
+        s.emitting = 0;
+        return s;
+    }
+    __device__ static Co coeffs(const ImageConsts& c, const Sample& p, int f) {
+        return riaf_coefficients(c, p, c.freq[f]);
+    }
+    __device__ static void step(Stokes& s, const Co& co, double h, const ImageConsts& c, int f) {
+        stokes_step(s, co, abs_val(h) * c.dlambda_scale[f]);
+    }
+    __device__ static Stokes4<double> result(const Stokes& s, const ImageConsts&, int) { return s; }
+};
+
+template<>
+struct RadTraits<PolicyMixed> {
+    using Stokes = StokesF;
+    using Co = CoeffsF;
+    using Sample = RiafSampleF;
+    __device__ static void zero(Stokes& s) { s = StokesF{0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f}; }
+    __device__ static Sample sample(const ImageConsts& c, const Ray& r) { return riaf_sample_f(c, r); }
+    __device__ static Sample none() {
+        Sample s;
+        s.emitting = 0;
+        return s;
+    }
+    __device__ static Co coeffs(const ImageConsts& c, const Sample& p, int f) {
+        return riaf_coefficients_f(c, p, float(c.freq[f] * 1e-9), c.emission_scale_pow2[f]);
+    }
+    __device__ static void step(Stokes& s, const Co& co, double h, const ImageConsts& c, int f) {
+        stokes_step_f(s, co, float(abs_val(h) * c.dlambda_scale[f]));
+    }
+    __device__ static Stokes4<double> result(const Stokes& s, const ImageConsts& c, int f) {
+        const double inv = c.inv_emission_scale_pow2[f];
+        return Stokes4<double>{(double(s.I) + double(s.cI)) * inv, (double(s.Q) + double(s.cQ)) * inv,
+                               (double(s.U) + double(s.cU)) * inv, (double(s.V) + double(s.cV)) * inv};
+    }
+};
+
+template<class P>
+__device__ __forceinline__ Ray policy_rhs(double mass, double spin, const Ray& X, bool fp32) {
+    if constexpr (P::kMixed) {
+        if (fp32) return ks_rhs_f32(mass, spin, X);
+    }
+    return ks_rhs(mass, spin, X);
+}
+
+// ---------------------------------------------------------------- RK jobs
+// Runs one RK job from S with signed step h.  Outputs: next (endpoint), mid
+// (sample point: the first half step for SD, the endpoint otherwise) and err
+// (SD / CK only).  The stage arithmetic is the reference's (see file header).
+// Cash-Karp attempt with the reference's stage coefficients (rk4.hpp:171-228).
+template<class P>
+__device__ __noinline__ void ck_job(double mass, double spin, const Ray& S, double h, bool fp32, Ray& next,
+                                    Ray& mid, double& err) {
+    {
+        const Ray k1 = policy_rhs<P>(mass, spin, S, fp32);
+        Ray t;
+        ray_axpy(t, S, h * 1.0 / 5.0, k1);
+        const Ray k2 = policy_rhs<P>(mass, spin, t, fp32);
+        {
+            const Ray* const kk[2] = {&k1, &k2};
+            const double cc[2] = {3.0 / 40.0, 9.0 / 40.0};
+            ray_lincomb<2>(t, S, h, kk, cc);
+        }
+        const Ray k3 = policy_rhs<P>(mass, spin, t, fp32);
+        {
+            const Ray* const kk[3] = {&k1, &k2, &k3};
+            const double cc[3] = {3.0 / 10.0, -9.0 / 10.0, 6.0 / 5.0};
+            ray_lincomb<3>(t, S, h, kk, cc);
+        }
+        const Ray k4 = policy_rhs<P>(mass, spin, t, fp32);
+        {
+            const Ray* const kk[4] = {&k1, &k2, &k3, &k4};
+            const double cc[4] = {-11.0 / 54.0, 5.0 / 2.0, -70.0 / 27.0, 35.0 / 27.0};
+            ray_lincomb<4>(t, S, h, kk, cc);
+        }
+        const Ray k5 = policy_rhs<P>(mass, spin, t, fp32);
+        {
+            const Ray* const kk[5] = {&k1, &k2, &k3, &k4, &k5};
+            const double cc[5] = {1631.0 / 55296.0, 175.0 / 512.0, 575.0 / 13824.0, 44275.0 / 110592.0,
+                                  253.0 / 4096.0};
+            ray_lincomb<5>(t, S, h, kk, cc);
+        }
+        const Ray k6 = policy_rhs<P>(mass, spin, t, fp32);
+        {
+            const Ray* const kk[4] = {&k1, &k3, &k4, &k6};
+            const double cc[4] = {37.0 / 378.0, 250.0 / 621.0, 125.0 / 594.0, 512.0 / 1771.0};
+            ray_lincomb<4>(next, S, h, kk, cc);
+        }
+        Ray fourth;
+        {
+            const Ray* const kk[5] = {&k1, &k3, &k4, &k5, &k6};
+            const double cc[5] = {2825.0 / 27648.0, 18575.0 / 48384.0, 13525.0 / 55296.0, 277.0 / 14336.0,
+                                  1.0 / 4.0};
+            ray_lincomb<5>(fourth, S, h, kk, cc);
+        }
+        err = state_error_norm(next, fourth);
+        mid = next;
+    }
+}
+
+// Step-doubling attempt, RK4 step or composed RK4 pair as a stage loop around
+// one RHS site.  Out of line: the caller's control state is saved once per
+// job and the stage loop has the register file to itself.
+template<class P>
+__device__ __noinline__ void rk_job(int kind, double mass, double spin, const Ray& S, double h, bool fp32,
+                                    Ray& next, Ray& mid, double& err) {
+    if (kind == kRkCK) {
+        ck_job<P>(mass, spin, S, h, fp32, next, mid, err);
+        return;
+    }
+    // Stage schedule (see file header): SD = half chain (4), second half
+    // chain (4), full chain (3); RK4 = 4; RK4x2 = 4 + 4.
+    const int nstage = kind == kRkSD ? 11 : (kind == kRkRK4 ? 4 : 8);
+    const double hs = kind == kRkSD ? h * 0.5 : (kind == kRkRK4x2 ? h * 0.5 : h);  // step of the first chain
+    const double hh_s = 0.5 * hs;
+    const double h6_s = hs / 6.0;
+    const double hh_f = 0.5 * h;
+    const double h6_f = h / 6.0;
+    Ray X = S;   // RHS input
+    Ray A;       // stage accumulator
+    Ray R1;      // SD: k1 of S, then the two-half endpoint
+    Ray R2;      // SD / RK4x2: the first chain's endpoint (half step)
+#pragma unroll 1
+    for (int st = 0; st < nstage; ++st) {
+        const Ray k = policy_rhs<P>(mass, spin, X, fp32);
+        // position of this stage inside its 4-stage RK4 chain
+        const int cs = st < 4 ? st : (st < 8 ? st - 4 : st - 7);
+        const bool full_chain = kind == kRkSD && st >= 8;
+        const bool second_chain = st >= 4 && st < 8;
+        const double hh = full_chain ? hh_f : hh_s;
+        const double hl = full_chain ? h : hs;       // last-stage step of the chain
+        const double h6 = full_chain ? h6_f : h6_s;
+        const Ray& base = second_chain ? R2 : S;
+        if (cs == 0) {
+            A = k;
+            if (st == 0 && kind == kRkSD) R1 = k;
+            ray_axpy(X, base, hh, k);
+        } else if (cs == 1) {
+            ray_acc(A, k, 2.0);
+            ray_axpy(X, base, hh, k);
+        } else if (cs == 2) {
+            ray_acc(A, k, 2.0);
+            ray_axpy(X, base, hl, k);
+        } else {
+            ray_add(A, k);
+            if (st == 3) {
+                if (kind == kRkRK4) {
+                    ray_axpy(next, S, h6, A);
+                } else {
+                    ray_axpy(R2, S, h6, A);  // half step endpoint
+                    X = R2;
+                }
+            } else if (st == 7) {
+                if (kind == kRkRK4x2) {
+                    ray_axpy(next, R2, h6, A);
+                } else {
+                    // two_half = R2 + (hs/6) A; start the full chain from k1 of S
+                    Ray two_half;
+                    ray_axpy(two_half, R2, h6, A);
+                    A = R1;
+                    ray_axpy(X, S, hh_f, R1);
+                    R1 = two_half;
+                    // the full chain's first stage (k1) is already done: advance
+                    // its position counter by running stages 8..10 as cs 1..3.
+                }
+            } else {  // st == 10: full step endpoint
+                Ray full;
+                ray_axpy(full, S, h6_f, A);
+                err = state_error_norm(full, R1);
+                next = R1;
+                mid = R2;
+            }
+        }
+    }
+    if (kind == kRkRK4 || kind == kRkRK4x2) {
+        mid = next;
+        err = 0.0;
+    }
+}
+
+}  // namespace kp

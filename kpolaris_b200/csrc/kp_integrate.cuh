@@ -44,7 +44,7 @@ KP_HD void ray_add(Ray& acc, const Ray& x) {
 
 // rk4_step_from_k1 (rk4.hpp:49-59).  Out of line: one copy of the three
 // inlined right-hand sides serves every RK4 call site.
-__device__ __noinline__ Ray rk4_from_k1(double mass, double spin, const Ray& s, double h, const Ray& k1) {
+static __device__ __noinline__ Ray rk4_from_k1(double mass, double spin, const Ray& s, double h, const Ray& k1) {
     Ray acc = k1;
     Ray tmp;
     const double hh = 0.5 * h;
@@ -100,7 +100,7 @@ struct AdaptiveStep {
 
 // adaptive_rk4_step (rk4.hpp:108-161): one full step against two half steps,
 // at most 10 attempts.  The half-step state is the transfer sample point.
-__device__ __noinline__ void adaptive_rk4(double mass, double spin, const Ray& state,
+static __device__ __noinline__ void adaptive_rk4(double mass, double spin, const Ray& state,
                                              double requested_h, const StepControl& ctl,
                                              AdaptiveStep& out) {
     double h = min_val(max_val(abs_val(requested_h), ctl.min_step), ctl.max_step);
@@ -161,7 +161,7 @@ KP_HD void ray_lincomb(Ray& out, const Ray& s, double h, const Ray* const (&k)[N
 // attempt, the same acceptance rule with a 0.2 shrink exponent; the sample
 // point is the accepted endpoint.  Not used by the reference's image tool;
 // offered as an integrator variant.
-__device__ __noinline__ void adaptive_cash_karp(double mass, double spin, const Ray& state,
+static __device__ __noinline__ void adaptive_cash_karp(double mass, double spin, const Ray& state,
                                                    double requested_h, const StepControl& ctl,
                                                    AdaptiveStep& out) {
     double h = min_val(max_val(abs_val(requested_h), ctl.min_step), ctl.max_step);

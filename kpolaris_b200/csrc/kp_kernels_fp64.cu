@@ -1,11 +1,23 @@
-// kp_kernels_fp64.cu -- the plain FP64 image kernel: one thread per pixel,
-// one launch per image.  This translation unit is compiled with --fmad=false
-// so every double operation rounds exactly as the reference's CPU code does;
-// termination reasons and fixed-step counts are bit-identical to it.
+// kp_kernels_fp64.cu -- FP64 image kernels.  This translation unit is
+// compiled with --fmad=false so every double operation rounds exactly as the
+// reference's CPU code does: termination reasons and fixed-step counts are
+// bit-identical to it.
+//
+//  * image_fp64_per_pixel: the plain form -- one thread per pixel, one launch
+//    per image, the reference's per-pixel code structure.
+//  * persistent_fp64: the persistent engine with the FP64 policy; its
+//    arithmetic is the same, so its results equal the plain kernel's bit for
+//    bit whatever the batch composition.
 #include <cuda_runtime.h>
 
 #include "kp_launch.h"
+#include "kp_persistent.cuh"
 #include "kp_trace_fp64.cuh"
+
+#ifndef KP_PERSISTENT_MIN_BLOCKS
+// resident CTAs of 128 threads per SM the persistent kernel is compiled for
+#define KP_PERSISTENT_MIN_BLOCKS 2
+#endif
 
 namespace kp {
 
@@ -34,7 +46,16 @@ __global__ void __launch_bounds__(128) image_fp64_per_pixel(const ImageConsts c,
     store_diagnostics(out, pixel, o);
 }
 
-CameraFrame host_camera_frame(const ImageConsts& c) { return camera_frame(c); }
+void host_camera_frame(const ImageConsts& c, double frame[5][4]) {
+    const CameraFrame f = camera_frame(c);
+    for (int mu = 0; mu < 4; ++mu) {
+        frame[0][mu] = f.x.v[mu];
+        frame[1][mu] = f.e0.v[mu];
+        frame[2][mu] = f.e1.v[mu];
+        frame[3][mu] = f.e2.v[mu];
+        frame[4][mu] = f.e3.v[mu];
+    }
+}
 
 cudaError_t launch_image_fp64(const ImageConsts& c, const ImageOutPtrs& out, cudaStream_t stream) {
     const CameraFrame frame = camera_frame(c);
@@ -49,6 +70,34 @@ cudaError_t launch_image_fp64(const ImageConsts& c, const ImageOutPtrs& out, cud
     default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
+}
+
+template<int NF>
+__global__ void __launch_bounds__(128, KP_PERSISTENT_MIN_BLOCKS) persistent_fp64(const LaunchDesc L) {
+    persistent_body<PolicyFP64, NF>(L);
+}
+
+cudaError_t launch_persistent_fp64(const LaunchDesc& L, int nf_max, int blocks, int threads,
+                                   cudaStream_t stream) {
+    switch (nf_max) {
+    case 1: persistent_fp64<1><<<blocks, threads, 0, stream>>>(L); break;
+    case 2: persistent_fp64<2><<<blocks, threads, 0, stream>>>(L); break;
+    case 3: persistent_fp64<3><<<blocks, threads, 0, stream>>>(L); break;
+    case 4: persistent_fp64<4><<<blocks, threads, 0, stream>>>(L); break;
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+int persistent_occupancy_fp64(int nf_max, int threads) {
+    int n = 0;
+    switch (nf_max) {
+    case 1: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, persistent_fp64<1>, threads, 0); break;
+    case 2: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, persistent_fp64<2>, threads, 0); break;
+    case 3: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, persistent_fp64<3>, threads, 0); break;
+    default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, persistent_fp64<4>, threads, 0); break;
+    }
+    return n;
 }
 
 }  // namespace kp

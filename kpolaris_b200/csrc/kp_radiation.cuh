@@ -104,7 +104,7 @@ __device__ __forceinline__ void absorb_emit(Stokes4<double>& s, const Coeffs<dou
     s.V = nz * par_out + oz;
 }
 
-__device__ __noinline__ void stokes_step(Stokes4<double>& s, const Coeffs<double>& c, double dl) {
+static __device__ __noinline__ void stokes_step(Stokes4<double>& s, const Coeffs<double>& c, double dl) {
     faraday_rotate(s, c, 0.5 * dl);
     absorb_emit(s, c, dl);
     faraday_rotate(s, c, 0.5 * dl);
@@ -282,7 +282,7 @@ struct ThermalIn {
 
 // Invariant coefficients in the magnetic basis
 // (thermal_synchrotron_magnetic_basis_coefficients_fit, :512-627).
-__device__ __noinline__ Coeffs<double> thermal_coefficients(const ThermalIn& s, const ImageConsts& c) {
+static __device__ __noinline__ Coeffs<double> thermal_coefficients(const ThermalIn& s, const ImageConsts& c) {
     Coeffs<double> o = {};
     if (!(s.nu > 0.0) || !(s.ne > 0.0) || !(s.thetae > 0.0) || !(s.b > 0.0)) return o;
     const double nu = max_val(s.nu, 1.0);
@@ -463,7 +463,7 @@ struct RiafSample {
     int has_chi;
 };
 
-__device__ __noinline__ RiafSample riaf_sample(const ImageConsts& c, const Ray& s) {
+static __device__ __noinline__ RiafSample riaf_sample(const ImageConsts& c, const Ray& s) {
     RiafSample out;
     out.emitting = 0;
     out.on_axis = 0;

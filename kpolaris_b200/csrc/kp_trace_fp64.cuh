@@ -40,7 +40,7 @@ __device__ __forceinline__ Ray surface_path_state(double mass, double spin, cons
 
 // locate_metric_surface_crossing (pass_a_core.hpp:94-197) for the spherical
 // surfaces r = surface_parameter; returns the last point on the original side.
-__device__ __noinline__ void locate_crossing(double mass, double spin, const Ray& first,
+static __device__ __noinline__ void locate_crossing(double mass, double spin, const Ray& first,
                                              const Ray& second, double full_h,
                                              double surface_parameter, int composed,
                                              Ray& out_state, double& out_h) {

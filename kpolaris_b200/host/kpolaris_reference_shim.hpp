@@ -1,0 +1,202 @@
+// kpolaris_reference_shim.hpp -- C++ host shim that gives the reference's
+// image entry points their original signatures on top of the C ABI
+// (include/kpolaris_b200.h), so the reference's callers
+// (tools/kpolaris_model_image.cpp:3416 compute_frequency_image,
+//  :3437 compute_multifrequency_images; examples/grrt_batch_benchmark.cpp;
+//  tests/test_image_batch.cpp) relink unchanged.
+//
+// The shim is templated on the reference's own parameter and result types
+// (PassAParams<double>, RIAFAnalyticRadiationModel<double>, ImageHostData),
+// which it reads field by field; it therefore compiles inside the reference's
+// build without this library depending on the reference's headers.  Errors
+// are rethrown with the reference's exception types: KP_ERR_INVALID as
+// std::invalid_argument, everything else as std::runtime_error.
+#pragma once
+
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "kpolaris_b200.h"
+
+namespace kpolaris_b200 {
+
+inline void throw_on_error(int status) {
+    if (status == KP_OK) return;
+    const std::string msg = kp_last_error();
+    if (status == KP_ERR_INVALID) throw std::invalid_argument(msg);
+    throw std::runtime_error(msg);
+}
+
+// PassAParams<Real> (src/geodesic/pass_a_core.hpp:10-36) -> kp_pass_a_params.
+template<class PassA>
+kp_pass_a_params to_c(const PassA& p) {
+    kp_pass_a_params o;
+    std::memset(&o, 0, sizeof(o));
+    o.camera.nx = p.camera.nx;
+    o.camera.ny = p.camera.ny;
+    o.camera.radius = double(p.camera.radius);
+    o.camera.inclination = double(p.camera.inclination);
+    o.camera.fov = double(p.camera.fov);
+    o.camera.fov_y = double(p.camera.fov_y);
+    o.camera.xspan = double(p.camera.xspan);
+    o.camera.yspan = double(p.camera.yspan);
+    o.camera.x_offset = double(p.camera.x_offset);
+    o.camera.y_offset = double(p.camera.y_offset);
+    o.camera.model = static_cast<int>(p.camera.model);
+    o.emission_selection.equatorial_h_over_r = double(p.emission_selection.equatorial_h_over_r);
+    o.emission_selection.equatorial_samples = p.emission_selection.equatorial_samples;
+    o.emission_selection.faraday_rotation = p.emission_selection.faraday_rotation;
+    o.mass = double(p.mass);
+    o.spin = double(p.spin);
+    o.inner_radius = double(p.inner_radius);
+    o.outer_radius = double(p.outer_radius);
+    o.step = double(p.step);
+    o.max_steps = p.max_steps;
+    o.adaptive = p.adaptive;
+    o.direct_only = p.direct_only;
+    o.adaptive_tolerance = double(p.adaptive_tolerance);
+    o.min_step = double(p.min_step);
+    o.max_step = double(p.max_step);
+    o.max_radiation_step = double(p.max_radiation_step);
+    o.max_radiation_depth = double(p.max_radiation_depth);
+    o.max_absorption_depth = double(p.max_absorption_depth);
+    o.max_faraday_depth = double(p.max_faraday_depth);
+    o.fmks_startx1 = double(p.fmks_startx1);
+    o.fmks_hslope = double(p.fmks_hslope);
+    o.fmks_mks_smooth = double(p.fmks_mks_smooth);
+    o.fmks_poly_alpha = double(p.fmks_poly_alpha);
+    o.fmks_poly_xt = double(p.fmks_poly_xt);
+    o.fmks_poly_norm = double(p.fmks_poly_norm);
+    o.coordinate_system = static_cast<int>(p.coordinate_system);
+    return o;
+}
+
+// RIAFAnalyticRadiationModel<Real> (src/model/riaf.hpp:19-52) -> kp_riaf_model.
+template<class Model>
+kp_riaf_model to_c_riaf(const Model& m) {
+    kp_riaf_model o;
+    std::memset(&o, 0, sizeof(o));
+    o.nth0 = double(m.nth0);
+    o.Te0 = double(m.Te0);
+    o.disk_h = double(m.disk_h);
+    o.pow_nth = double(m.pow_nth);
+    o.pow_T = double(m.pow_T);
+    o.ne_unit = double(m.ne_unit);
+    o.te_unit = double(m.te_unit);
+    o.b_unit = double(m.b_unit);
+    o.freq_cgs = double(m.freq_cgs);
+    o.mbh_solar = double(m.mbh_solar);
+    o.r_min = double(m.r_min);
+    o.r_max = double(m.r_max);
+    o.horizon_buffer = double(m.horizon_buffer);
+    o.emission_scale = double(m.emission_scale);
+    o.absorption_scale = double(m.absorption_scale);
+    o.faraday_scale = double(m.faraday_scale);
+    o.max_pol_frac = double(m.max_pol_frac);
+    o.keplerian_factor = double(m.keplerian_factor);
+    o.infall_factor = double(m.infall_factor);
+    o.emission_type = m.emission_type;
+    o.min_frequency_scale = double(m.min_frequency_scale);
+    o.min_sin_theta = double(m.min_sin_theta);
+    o.min_thetae = double(m.min_thetae);
+    o.min_radius = double(m.min_radius);
+    return o;
+}
+
+// Sizes an ImageHostData (src/image/result.hpp:9-31) and points a
+// kp_image_out at its vectors.
+template<class HostData>
+kp_image_out bind_outputs(HostData& d, int npix, int nfreq) {
+    const size_t img = size_t(npix) * size_t(nfreq);
+    d.npix = npix;
+    d.nfreq = nfreq;
+    d.image_i.assign(img, 0.0);
+    d.image_q.assign(img, 0.0);
+    d.image_u.assign(img, 0.0);
+    d.image_v.assign(img, 0.0);
+    for (auto* v : {&d.closure_x, &d.closure_k, &d.final_null, &d.frame_error, &d.det_r, &d.overlap_r11,
+                    &d.overlap_r12, &d.overlap_r21, &d.overlap_r22, &d.basis_identity_error,
+                    &d.basis_rotation_angle})
+        v->assign(size_t(npix), 0.0);
+    d.pass_a_steps.assign(size_t(npix), 0);
+    d.steps.assign(size_t(npix), 0);
+    d.reason.assign(size_t(npix), 0);
+    d.has_analysis = 0;
+    kp_image_out o;
+    o.npix = npix;
+    o.nfreq = nfreq;
+    o.image_i = d.image_i.data();
+    o.image_q = d.image_q.data();
+    o.image_u = d.image_u.data();
+    o.image_v = d.image_v.data();
+    o.closure_x = d.closure_x.data();
+    o.closure_k = d.closure_k.data();
+    o.final_null = d.final_null.data();
+    o.frame_error = d.frame_error.data();
+    o.det_r = d.det_r.data();
+    o.overlap_r11 = d.overlap_r11.data();
+    o.overlap_r12 = d.overlap_r12.data();
+    o.overlap_r21 = d.overlap_r21.data();
+    o.overlap_r22 = d.overlap_r22.data();
+    o.basis_identity_error = d.basis_identity_error.data();
+    o.basis_rotation_angle = d.basis_rotation_angle.data();
+    o.pass_a_steps = reinterpret_cast<int32_t*>(d.pass_a_steps.data());
+    o.steps = reinterpret_cast<int32_t*>(d.steps.data());
+    o.reason = reinterpret_cast<int32_t*>(d.reason.data());
+    return o;
+}
+
+// Process-wide launch options used by the shim (FP64 bit-exact path by
+// default; set e.g. precision = KP_PRECISION_MIXED to serve the mixed path).
+inline kp_run_options& shim_options() {
+    static kp_run_options o = [] {
+        kp_run_options d;
+        kp_default_run_options(&d);
+        return d;
+    }();
+    return o;
+}
+
+// run_riaf_image (src/image/riaf.hpp:12-16).
+template<class HostData, class PassA, class Model>
+HostData run_riaf_image(const PassA& pass_a, Model model, int radiation_substeps, int timing,
+                        int split_transport) {
+    (void)split_transport;  // one fused launch: identical results to the split pair
+    const kp_pass_a_params p = to_c(pass_a);
+    const kp_riaf_model m = to_c_riaf(model);
+    HostData out;
+    kp_image_out o = bind_outputs(out, p.camera.nx * p.camera.ny, 1);
+    kp_run_options opt = shim_options();
+    opt.timing = timing;
+    const double f = m.freq_cgs;
+    throw_on_error(kp_image_riaf(&p, &m, radiation_substeps, &f, 1, &opt, &o));
+    return out;
+}
+
+// run_riaf_multifrequency_image (src/image/riaf.hpp:32-39).
+template<class HostData, class PassA, class Model>
+HostData run_riaf_multifrequency_image(const PassA& pass_a, Model model, int radiation_substeps,
+                                       const std::vector<double>& frequencies,
+                                       const std::vector<double>& step_control_frequencies,
+                                       int timing, int split_transport) {
+    (void)split_transport;
+    if (step_control_frequencies.empty())
+        throw std::invalid_argument("multifrequency step-control frequency list must not be empty");
+    if (step_control_frequencies != frequencies)
+        throw std::runtime_error("separate step-control frequency sets are not built");
+    const kp_pass_a_params p = to_c(pass_a);
+    const kp_riaf_model m = to_c_riaf(model);
+    HostData out;
+    const int nfreq = int(frequencies.size());
+    if (nfreq < 1 || nfreq > KP_MAX_FREQUENCIES)
+        throw std::invalid_argument("multifrequency image chunk size must be between 1 and KPOLARIS_MAX_FREQUENCIES");
+    kp_image_out o = bind_outputs(out, p.camera.nx * p.camera.ny, nfreq);
+    kp_run_options opt = shim_options();
+    opt.timing = timing;
+    throw_on_error(kp_image_riaf(&p, &m, radiation_substeps, frequencies.data(), nfreq, &opt, &o));
+    return out;
+}
+
+}  // namespace kpolaris_b200
