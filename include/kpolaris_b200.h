@@ -224,7 +224,8 @@ typedef struct kp_run_options {
     int device;          /* CUDA device ordinal */
     void* stream;        /* cudaStream_t, or NULL for the library's stream */
     int timing;          /* 1: print "timing <name> <seconds> s" lines like the reference */
-    /* Persistent-schedule tunables; 0 selects the autotuned/default value. */
+    /* Persistent-schedule tunables; 0 selects the default (occupancy-derived
+     * CTAs per SM; 128 threads per CTA, the only size the kernels take). */
     int blocks_per_sm;
     int threads_per_block;
 } kp_run_options;
@@ -293,23 +294,27 @@ typedef struct kp_batch_stats {
     double copy_seconds;         /* device-to-host copies (host outputs only) */
     long long rays;              /* pixels traced */
     int launches;                /* kernels launched */
-    int blocks;                  /* CTAs of the persistent launch */
+    int blocks;                  /* CTAs of a near-phase launch */
     int threads_per_block;
     size_t device_output_bytes;  /* library-owned output scratch used */
 } kp_batch_stats;
 
 /*
- * A batch of RIAF images traced by ONE persistent launch whose lanes drain a
- * ray queue spanning every image (continuous refill), so images of any size,
- * spin, inclination and frequency count share the GPU.  Replaces the
- * reference's experimental host batching run_image_batch_metric
- * (src/image/batch_driver.hpp:127-187), which launches one kernel per image
- * on a few streams.  Every job is validated before anything is launched; an
- * invalid job fails the whole call (KP_ERR_INVALID / KP_ERR_UNSUPPORTED).
- * With KP_PRECISION_FP64 each image is bit-identical to the same image
- * traced alone by kp_image_riaf; KP_PRECISION_MIXED images agree with them
- * within the mixed-precision tolerance and are also independent of the
- * batch composition.  `stats` may be NULL.
+ * A batch of RIAF images traced by the wavefront engine: persistent far and
+ * near kernels whose lanes drain ray queues spanning every image (continuous
+ * refill), so images of any size, spin, inclination and frequency count
+ * share the GPU.  The far kernel moves rays between the camera and the
+ * radiating sphere (transport only), the near kernel traces the sphere
+ * (surface crossings, radiative transfer); rays migrate between them through
+ * HBM ray records.  Replaces the reference's experimental host batching
+ * run_image_batch_metric (src/image/batch_driver.hpp:127-187), which launches
+ * one kernel per image on a few streams.  Every job is validated before
+ * anything is launched; an invalid job fails the whole call (KP_ERR_INVALID /
+ * KP_ERR_UNSUPPORTED).  With KP_PRECISION_FP64 each image is bit-identical
+ * to the same image traced alone by kp_image_riaf; KP_PRECISION_MIXED images
+ * agree with them within the mixed-precision tolerance and are also
+ * independent of the batch composition.  The call returns when the images
+ * are complete (on options->stream when one is given).  `stats` may be NULL.
  */
 int kp_batch_riaf(const kp_riaf_job* jobs, int njobs, const kp_run_options* options,
                   kp_batch_stats* stats);

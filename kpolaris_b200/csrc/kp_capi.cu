@@ -35,6 +35,21 @@ int cuda_error(cudaError_t e, const char* what) {
     return set_error(KP_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
 }
 
+// Launches of one wavefront batch run in cycles of (far, near-A, near-B)
+// until no ray is left.
+constexpr int kMaxWaveCycles = 24;
+
+// Device-side counters of one batch, zeroed before its first launch.  The
+// queue a phase reads in its g-th launch is generation g of that phase:
+// counts[g][phase] entries of ids[phase][g % 2].  A launch of cycle c pushes
+// a ray for a phase that comes later in the cycle into generation c, for its
+// own or an earlier phase into generation c + 1.
+struct WaveCtrl {
+    unsigned long long heads[kMaxWaveCycles * kPhases];
+    unsigned counts[kMaxWaveCycles + 1][kPhases];
+    int status;
+};
+
 // Per-device library state: a non-blocking stream and grow-only output
 // buffers reused across calls.
 struct DeviceState {
@@ -49,7 +64,11 @@ struct DeviceState {
     JobDesc* h_jobs = nullptr;      // pinned staging of the job table
     int jobs_cap = 0;
     cudaEvent_t staging_free = nullptr;  // last upload from h_jobs has completed
-    unsigned long long* d_queue = nullptr;  // [0] ray-queue head, [1] status word
+    WaveCtrl* d_ctrl = nullptr;     // queue counters and the status word
+    RayRecord* d_pool = nullptr;    // parked ray records, one per ray (grow-only)
+    unsigned* d_ids[kPhases][2] = {};  // id queues per phase, by generation parity
+    long long pool_cap = 0;
+    unsigned* h_left = nullptr;     // pinned: queue counts after a cycle
 };
 
 static std::mutex g_mutex;
@@ -76,9 +95,14 @@ DeviceState* device_state(int device, int* status) {
         cudaEventCreate(&d.ev1);
         cudaEventCreateWithFlags(&d.staging_free, cudaEventDisableTiming);
         cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, device);
-        e = cudaMalloc(&d.d_queue, 2 * sizeof(unsigned long long));
+        e = cudaMalloc(&d.d_ctrl, sizeof(WaveCtrl));
         if (e != cudaSuccess) {
-            *status = cuda_error(e, "cudaMalloc(queue)");
+            *status = cuda_error(e, "cudaMalloc(wave counters)");
+            return nullptr;
+        }
+        e = cudaMallocHost(&d.h_left, sizeof(unsigned) * kPhases);
+        if (e != cudaSuccess) {
+            *status = cuda_error(e, "cudaMallocHost(queue count)");
             return nullptr;
         }
         d.initialised = 1;
@@ -339,7 +363,10 @@ ImageConsts make_consts(const kp_pass_a_params* p, const kp_riaf_model* m, const
         c.thetae_unit = m->te_unit * kbol / (me * cl * cl);  // riaf.hpp:67-74
     }
     c.isco = isco_radius(p->spin);
-    c.fp32_radius = p->outer_radius + 2.0 * std::fabs(p->max_step);
+    // Boundary of the far phase: two of the longest steps either pass can
+    // take (adaptive steps are clamped to max_step, fixed steps are `step`)
+    // beyond the radiating sphere, so no far-phase step reaches the sphere.
+    c.fp32_radius = p->outer_radius + 2.0 * std::max(std::fabs(p->max_step), std::fabs(p->step));
     c.fit = m->emission_type == KP_FIT_DEXTER ? 4 : 1;
     c.nfreq = nfreq;
     const double gnewt = 6.67430e-8, msun = 1.98847e33, cl = 2.99792458e10;
@@ -617,62 +644,114 @@ int kp_batch_riaf(const kp_riaf_job* jobs, int njobs, const kp_run_options* opti
         d.precision = opt.precision;
         ray += npix;
     }
+    // ray records and id queues, grow-only
+    if (total > dev->pool_cap) {
+        cudaStreamSynchronize(stream);
+        cudaFree(dev->d_pool);
+        dev->d_pool = nullptr;
+        for (auto& q : dev->d_ids) {
+            cudaFree(q[0]);
+            cudaFree(q[1]);
+            q[0] = q[1] = nullptr;
+        }
+        dev->pool_cap = 0;
+        cudaError_t e = cudaMalloc(&dev->d_pool, sizeof(RayRecord) * size_t(total));
+        for (auto& q : dev->d_ids)
+            for (auto& b : q)
+                if (e == cudaSuccess) e = cudaMalloc(&b, sizeof(unsigned) * size_t(total));
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return set_error(KP_ERR_OOM, "cudaMalloc(%lld ray records): %s", total, cudaGetErrorString(e));
+        }
+        dev->pool_cap = total;
+    }
     cudaError_t e = cudaMemcpyAsync(dev->d_jobs, dev->h_jobs, sizeof(JobDesc) * size_t(njobs),
                                     cudaMemcpyHostToDevice, stream);
     if (e != cudaSuccess) return cuda_error(e, "cudaMemcpyAsync(job table)");
     cudaEventRecord(dev->staging_free, stream);
-    e = cudaMemsetAsync(dev->d_queue, 0, 2 * sizeof(unsigned long long), stream);
-    if (e != cudaSuccess) return cuda_error(e, "cudaMemsetAsync(queue)");
-    LaunchDesc L;
-    L.jobs = dev->d_jobs;
-    L.njobs = njobs;
-    L.total_rays = total;
-    L.next_ray = dev->d_queue;
-    L.refill = opt.schedule == KP_SCHEDULE_PERSISTENT || opt.precision == KP_PRECISION_MIXED ? 1 : 0;
-    L.r_fp64 = 6.0;
-    L.status = reinterpret_cast<int*>(dev->d_queue + 1);
+    e = cudaMemsetAsync(dev->d_ctrl, 0, sizeof(WaveCtrl), stream);
+    if (e != cudaSuccess) return cuda_error(e, "cudaMemsetAsync(wave counters)");
     const int threads = opt.threads_per_block > 0 ? opt.threads_per_block : 128;
-    if (threads % 32 != 0 || threads > 1024)
-        return set_error(KP_ERR_INVALID, "threads_per_block must be a multiple of 32 up to 1024");
-    int blocks;
-    if (L.refill) {
+    if (threads != 128)
+        return set_error(KP_ERR_INVALID, "threads_per_block must be 128 for the wavefront kernels");
+    const bool mixed = opt.precision == KP_PRECISION_MIXED;
+    int blocks[kPhases];
+    for (int phase = 0; phase < kPhases; ++phase) {
         int per_sm = opt.blocks_per_sm;
         if (per_sm <= 0) {
-            per_sm = opt.precision == KP_PRECISION_MIXED ? persistent_occupancy_mixed(nf_max, threads)
-                                                         : persistent_occupancy_fp64(nf_max, threads);
+            per_sm = mixed ? wave_occupancy_mixed(phase, threads) : wave_occupancy_fp64(phase, nf_max, threads);
             if (per_sm <= 0) per_sm = 1;
         }
-        blocks = dev->sms * per_sm;
+        blocks[phase] = dev->sms * per_sm;
         const long long needed = (total + threads - 1) / threads;
-        if (blocks > needed) blocks = int(needed);
-    } else {
-        blocks = int((total + threads - 1) / threads);
+        if (blocks[phase] > needed) blocks[phase] = int(needed);
     }
+    WaveCtrl* ctrl = dev->d_ctrl;
+    auto launch = [&](int cycle, int phase) -> cudaError_t {
+        WaveDesc W;
+        W.jobs = dev->d_jobs;
+        W.njobs = njobs;
+        W.pool = dev->d_pool;
+        W.fresh_begin = 0;
+        W.fresh_end = cycle == 0 && phase == kPhaseFar ? total : 0;
+        W.in_ids = dev->d_ids[phase][cycle % 2];
+        W.in_count = &ctrl->counts[cycle][phase];
+        W.in_head = &ctrl->heads[cycle * kPhases + phase];
+        for (int q = 0; q < kPhases; ++q) {
+            const int gen = q > phase ? cycle : cycle + 1;
+            W.out_ids[q] = dev->d_ids[q][gen % 2];
+            W.out_count[q] = &ctrl->counts[gen][q];
+        }
+        W.budget = 0;
+        W.status = &ctrl->status;
+        W.job_done = nullptr;
+        return mixed ? launch_wave_mixed(phase, W, blocks[phase], threads, stream)
+                     : launch_wave_fp64(phase, W, nf_max, blocks[phase], threads, stream);
+    };
+    // Rays leave the camera in the far phase, trace the radiating sphere in
+    // near-A then near-B and return in the far phase of the next cycle; a few
+    // graze the boundary and take one more.  After each cycle the host reads
+    // the next generation's queue counts.
     cudaEventRecord(dev->ev0, stream);
-    e = opt.precision == KP_PRECISION_MIXED ? launch_persistent_mixed(L, nf_max, blocks, threads, stream)
-                                            : launch_persistent_fp64(L, nf_max, blocks, threads, stream);
-    if (e != cudaSuccess) return cuda_error(e, "persistent image kernel launch");
+    int launches = 0;
+    int cycle = 0;
+    while (true) {
+        if (cycle >= kMaxWaveCycles)
+            return set_error(KP_ERR_TIMEOUT, "rays still moving between phases after %d launches", launches);
+        for (int phase = 0; phase < kPhases; ++phase) {
+            e = launch(cycle, phase);
+            if (e != cudaSuccess) return cuda_error(e, "wavefront kernel launch");
+            ++launches;
+        }
+        ++cycle;
+        e = cudaMemcpyAsync(dev->h_left, ctrl->counts[cycle], sizeof(unsigned) * kPhases, cudaMemcpyDeviceToHost,
+                            stream);
+        if (e != cudaSuccess) return cuda_error(e, "queue count read");
+        e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) return cuda_error(e, "wavefront kernels");
+        if (dev->h_left[0] == 0 && dev->h_left[1] == 0 && dev->h_left[2] == 0) break;
+    }
     cudaEventRecord(dev->ev1, stream);
     if (stats) {
         stats->rays = total;
-        stats->launches = 1;
-        stats->blocks = blocks;
+        stats->launches = launches;
+        stats->blocks = blocks[kPhaseNearB];
         stats->threads_per_block = threads;
         stats->device_output_bytes = opt.outputs_on_device ? 0 : scratch;
     }
-    const bool must_sync = !opt.outputs_on_device || !opt.stream || stats || opt.timing;
-    if (!must_sync) return KP_OK;
     e = cudaEventSynchronize(dev->ev1);
-    if (e != cudaSuccess) return cuda_error(e, "persistent image kernel");
+    if (e != cudaSuccess) return cuda_error(e, "wavefront kernels");
     float ms = 0.f;
     cudaEventElapsedTime(&ms, dev->ev0, dev->ev1);
     if (stats) stats->kernel_seconds = ms * 1e-3;
     if (opt.timing) std::printf("timing image_kernel_batch %g s\n", ms * 1e-3);
     int status_word = 0;
-    e = cudaMemcpy(&status_word, L.status, sizeof(int), cudaMemcpyDeviceToHost);
+    e = cudaMemcpy(&status_word, &ctrl->status, sizeof(int), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return cuda_error(e, "status read");
+    if (status_word == 2)
+        return set_error(KP_ERR_TIMEOUT, "a lane exceeded the engine's iteration guard");
     if (status_word != 0)
-        return set_error(KP_ERR_TIMEOUT, "a ray exceeded the engine's iteration guard (status %d)", status_word);
+        return set_error(KP_ERR_CUDA, "wavefront engine invariant violated (status %d)", status_word);
     if (!opt.outputs_on_device) {
         const auto t1 = std::chrono::steady_clock::now();
         for (int i = 0; i < njobs; ++i) {

@@ -80,8 +80,8 @@ struct ImageConsts {
     double min_frequency_scale, min_sin_theta, min_thetae, min_radius;
     double thetae_unit;  // te_unit * k_B / (m_e c^2)
     double isco;         // isco_radius(spin), riaf.hpp:166-174
-    // mixed policy: FP32 connection contraction for RK jobs that start beyond
-    // this radius (outside the radiating sphere by two maximal steps)
+    // boundary of the far phase (FP32 contraction under the mixed policy):
+    // outside the radiating sphere by two of the longest steps
     double fp32_radius;
     int fit;             // 1 Pandya, 4 Dexter
     // frequencies sharing one geodesic
@@ -131,15 +131,40 @@ struct JobDesc {
     int precision;        // kp_precision of this job
 };
 
+// Resumable state of one ray between launches (lives in HBM, 448 bytes):
+// the ray, the control state and the Stokes channels (32 bytes per frequency
+// in either precision).  Rays are parked only at the top of the pass-A or
+// pass-B loop, so the crossing search never spans two launches.
+struct alignas(16) RayRecord {
+    Ray S;
+    double st[24];
+    double stokes[4 * kMaxFreq];
+};
+
+// Phases of the wavefront engine (one kernel each).  Far: rays whose loop
+// tops lie beyond ImageConsts::fp32_radius (camera to radiating sphere and
+// back: pure transport).  Near-A: pass A inside (surface-crossing search).
+// Near-B: pass B inside (radiative transfer).  Rays migrate between the
+// phases through id queues.
+enum Phase : int { kPhaseFar = 0, kPhaseNearA = 1, kPhaseNearB = 2, kPhases = 3 };
+
 // Device-side launch description (kernel parameter).
-struct LaunchDesc {
+struct WaveDesc {
     const JobDesc* jobs;           // device array, ordered by ray_begin
     int njobs;
-    long long total_rays;
-    unsigned long long* next_ray;  // ray-queue head, zeroed before the launch
-    int refill;                    // 0: lane i traces ray i only (no queue)
-    double r_fp64;                 // mixed policy: FP64 contraction inside this radius
+    RayRecord* pool;               // indexed by global ray id
+    // input: fresh rays [fresh_begin, fresh_end) first, then in_ids[0, *in_count)
+    long long fresh_begin, fresh_end;
+    const unsigned* in_ids;
+    const unsigned* in_count;
+    unsigned long long* in_head;   // pop counter, zero before the launch
+    // queue of the next launch of each phase (this phase's own entry takes
+    // the rays parked by the iteration budget)
+    unsigned* out_ids[kPhases];
+    unsigned* out_count[kPhases];
+    int budget;                    // RK jobs per lane per launch; 0 = unlimited
     int* status;                   // device error word (0 ok)
+    unsigned* job_done;            // per-job count of finished rays (may be null)
 };
 
 }  // namespace kp

@@ -45,8 +45,9 @@ enum Mode : int {
 struct PolicyFP64 {
     static constexpr bool kMixed = false;
 };
-// Mixed policy: FP32 connection contraction outside r_fp64 when the whole
-// warp is outside it; FP64 state, stage combination and step control.
+// Mixed policy: FP32 connection contraction in the far-phase kernel (rays
+// beyond ImageConsts::fp32_radius), FP64 inside; FP64 state, stage
+// combination and step control everywhere; FP32 radiative transfer.
 struct PolicyMixed {
     static constexpr bool kMixed = true;
 };
@@ -102,12 +103,12 @@ struct RadTraits<PolicyMixed> {
     }
 };
 
-template<class P>
-__device__ __forceinline__ Ray policy_rhs(double mass, double spin, const Ray& X, bool fp32) {
-    if constexpr (P::kMixed) {
-        if (fp32) return ks_rhs_f32(mass, spin, X);
-    }
-    return ks_rhs(mass, spin, X);
+// FP32 is a compile-time choice of the calling kernel, so each kernel holds
+// one contraction body.
+template<class P, bool FP32>
+__device__ __forceinline__ Ray policy_rhs(double mass, double spin, const Ray& X) {
+    if constexpr (P::kMixed && FP32) return ks_rhs_f32(mass, spin, X);
+    else return ks_rhs(mass, spin, X);
 }
 
 // ---------------------------------------------------------------- RK jobs
@@ -115,39 +116,39 @@ __device__ __forceinline__ Ray policy_rhs(double mass, double spin, const Ray& X
 // (sample point: the first half step for SD, the endpoint otherwise) and err
 // (SD / CK only).  The stage arithmetic is the reference's (see file header).
 // Cash-Karp attempt with the reference's stage coefficients (rk4.hpp:171-228).
-template<class P>
-__device__ __noinline__ void ck_job(double mass, double spin, const Ray& S, double h, bool fp32, Ray& next,
+template<class P, bool FP32>
+__device__ __noinline__ void ck_job(double mass, double spin, const Ray& S, double h, Ray& next,
                                     Ray& mid, double& err) {
     {
-        const Ray k1 = policy_rhs<P>(mass, spin, S, fp32);
+        const Ray k1 = policy_rhs<P, FP32>(mass, spin, S);
         Ray t;
         ray_axpy(t, S, h * 1.0 / 5.0, k1);
-        const Ray k2 = policy_rhs<P>(mass, spin, t, fp32);
+        const Ray k2 = policy_rhs<P, FP32>(mass, spin, t);
         {
             const Ray* const kk[2] = {&k1, &k2};
             const double cc[2] = {3.0 / 40.0, 9.0 / 40.0};
             ray_lincomb<2>(t, S, h, kk, cc);
         }
-        const Ray k3 = policy_rhs<P>(mass, spin, t, fp32);
+        const Ray k3 = policy_rhs<P, FP32>(mass, spin, t);
         {
             const Ray* const kk[3] = {&k1, &k2, &k3};
             const double cc[3] = {3.0 / 10.0, -9.0 / 10.0, 6.0 / 5.0};
             ray_lincomb<3>(t, S, h, kk, cc);
         }
-        const Ray k4 = policy_rhs<P>(mass, spin, t, fp32);
+        const Ray k4 = policy_rhs<P, FP32>(mass, spin, t);
         {
             const Ray* const kk[4] = {&k1, &k2, &k3, &k4};
             const double cc[4] = {-11.0 / 54.0, 5.0 / 2.0, -70.0 / 27.0, 35.0 / 27.0};
             ray_lincomb<4>(t, S, h, kk, cc);
         }
-        const Ray k5 = policy_rhs<P>(mass, spin, t, fp32);
+        const Ray k5 = policy_rhs<P, FP32>(mass, spin, t);
         {
             const Ray* const kk[5] = {&k1, &k2, &k3, &k4, &k5};
             const double cc[5] = {1631.0 / 55296.0, 175.0 / 512.0, 575.0 / 13824.0, 44275.0 / 110592.0,
                                   253.0 / 4096.0};
             ray_lincomb<5>(t, S, h, kk, cc);
         }
-        const Ray k6 = policy_rhs<P>(mass, spin, t, fp32);
+        const Ray k6 = policy_rhs<P, FP32>(mass, spin, t);
         {
             const Ray* const kk[4] = {&k1, &k3, &k4, &k6};
             const double cc[4] = {37.0 / 378.0, 250.0 / 621.0, 125.0 / 594.0, 512.0 / 1771.0};
@@ -168,11 +169,11 @@ __device__ __noinline__ void ck_job(double mass, double spin, const Ray& S, doub
 // Step-doubling attempt, RK4 step or composed RK4 pair as a stage loop around
 // one RHS site.  Out of line: the caller's control state is saved once per
 // job and the stage loop has the register file to itself.
-template<class P>
-__device__ __noinline__ void rk_job(int kind, double mass, double spin, const Ray& S, double h, bool fp32,
+template<class P, bool FP32>
+__device__ __noinline__ void rk_job(int kind, double mass, double spin, const Ray& S, double h,
                                     Ray& next, Ray& mid, double& err) {
     if (kind == kRkCK) {
-        ck_job<P>(mass, spin, S, h, fp32, next, mid, err);
+        ck_job<P, FP32>(mass, spin, S, h, next, mid, err);
         return;
     }
     // Stage schedule (see file header): SD = half chain (4), second half
@@ -189,7 +190,7 @@ __device__ __noinline__ void rk_job(int kind, double mass, double spin, const Ra
     Ray R2;      // SD / RK4x2: the first chain's endpoint (half step)
 #pragma unroll 1
     for (int st = 0; st < nstage; ++st) {
-        const Ray k = policy_rhs<P>(mass, spin, X, fp32);
+        const Ray k = policy_rhs<P, FP32>(mass, spin, X);
         // position of this stage inside its 4-stage RK4 chain
         const int cs = st < 4 ? st : (st < 8 ? st - 4 : st - 7);
         const bool full_chain = kind == kRkSD && st >= 8;

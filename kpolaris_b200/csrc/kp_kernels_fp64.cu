@@ -5,18 +5,21 @@
 //
 //  * image_fp64_per_pixel: the plain form -- one thread per pixel, one launch
 //    per image, the reference's per-pixel code structure.
-//  * persistent_fp64: the persistent engine with the FP64 policy; its
-//    arithmetic is the same, so its results equal the plain kernel's bit for
-//    bit whatever the batch composition.
+//  * wave_far_fp64 / wave_near_fp64: the wavefront engine with the FP64
+//    policy; its arithmetic is the same, so its results equal the plain
+//    kernel's bit for bit whatever the batch composition.
 #include <cuda_runtime.h>
 
 #include "kp_launch.h"
 #include "kp_persistent.cuh"
 #include "kp_trace_fp64.cuh"
 
-#ifndef KP_PERSISTENT_MIN_BLOCKS
-// resident CTAs of 128 threads per SM the persistent kernel is compiled for
-#define KP_PERSISTENT_MIN_BLOCKS 2
+// resident CTAs of 128 threads per SM the wavefront kernels are compiled for
+#ifndef KP_FAR_MIN_BLOCKS
+#define KP_FAR_MIN_BLOCKS 2
+#endif
+#ifndef KP_NEAR_MIN_BLOCKS
+#define KP_NEAR_MIN_BLOCKS 2
 #endif
 
 namespace kp {
@@ -72,31 +75,45 @@ cudaError_t launch_image_fp64(const ImageConsts& c, const ImageOutPtrs& out, cud
     return cudaGetLastError();
 }
 
+// The wavefront kernels of the FP64 policy.  NF is 1 for single-frequency
+// launches and 4 otherwise: the per-frequency arithmetic does not depend on
+// NF (the unit is compiled without FMA contraction), so every instantiation
+// traces a ray bit-identically to the plain kernel.
 template<int NF>
-__global__ void __launch_bounds__(128, KP_PERSISTENT_MIN_BLOCKS) persistent_fp64(const LaunchDesc L) {
-    persistent_body<PolicyFP64, NF>(L);
+__global__ void __launch_bounds__(128, KP_FAR_MIN_BLOCKS) wave_far_fp64(const WaveDesc W) {
+    persistent_body<PolicyFP64, NF, kPhaseFar>(W);
 }
 
-cudaError_t launch_persistent_fp64(const LaunchDesc& L, int nf_max, int blocks, int threads,
-                                   cudaStream_t stream) {
-    switch (nf_max) {
-    case 1: persistent_fp64<1><<<blocks, threads, 0, stream>>>(L); break;
-    case 2: persistent_fp64<2><<<blocks, threads, 0, stream>>>(L); break;
-    case 3: persistent_fp64<3><<<blocks, threads, 0, stream>>>(L); break;
-    case 4: persistent_fp64<4><<<blocks, threads, 0, stream>>>(L); break;
-    default: return cudaErrorInvalidValue;
-    }
-    return cudaGetLastError();
+template<int NF>
+__global__ void __launch_bounds__(128, KP_NEAR_MIN_BLOCKS) wave_near_a_fp64(const WaveDesc W) {
+    persistent_body<PolicyFP64, NF, kPhaseNearA>(W);
 }
 
-int persistent_occupancy_fp64(int nf_max, int threads) {
+template<int NF>
+__global__ void __launch_bounds__(128, KP_NEAR_MIN_BLOCKS) wave_near_b_fp64(const WaveDesc W) {
+    persistent_body<PolicyFP64, NF, kPhaseNearB>(W);
+}
+
+template<int NF>
+static const void* wave_kernel_fp64(int phase) {
+    if (phase == kPhaseFar) return reinterpret_cast<const void*>(wave_far_fp64<NF>);
+    if (phase == kPhaseNearA) return reinterpret_cast<const void*>(wave_near_a_fp64<NF>);
+    return reinterpret_cast<const void*>(wave_near_b_fp64<NF>);
+}
+
+cudaError_t launch_wave_fp64(int phase, const WaveDesc& W, int nf_max, int blocks, int threads,
+                             cudaStream_t stream) {
+    if (nf_max < 1 || nf_max > kMaxFreq || phase < 0 || phase >= kPhases) return cudaErrorInvalidValue;
+    const void* fn = nf_max == 1 ? wave_kernel_fp64<1>(phase) : wave_kernel_fp64<kMaxFreq>(phase);
+    void* args[] = {const_cast<WaveDesc*>(&W)};
+    return cudaLaunchKernel(fn, dim3(blocks), dim3(threads), args, 0, stream);
+}
+
+int wave_occupancy_fp64(int phase, int nf_max, int threads) {
+    if (phase < 0 || phase >= kPhases) return 0;
+    const void* fn = nf_max == 1 ? wave_kernel_fp64<1>(phase) : wave_kernel_fp64<kMaxFreq>(phase);
     int n = 0;
-    switch (nf_max) {
-    case 1: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, persistent_fp64<1>, threads, 0); break;
-    case 2: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, persistent_fp64<2>, threads, 0); break;
-    case 3: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, persistent_fp64<3>, threads, 0); break;
-    default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, persistent_fp64<4>, threads, 0); break;
-    }
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, threads, 0);
     return n;
 }
 

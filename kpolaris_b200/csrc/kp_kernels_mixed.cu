@@ -1,44 +1,52 @@
-// kp_kernels_mixed.cu -- the mixed-precision persistent image kernel:
-// FP64 ray state, stage combination and step control; the connection
-// contraction runs in FP32 for warps whose rays are all outside r_fp64
-// (default 4 M), FP64 inside.  Compiled with FMA contraction enabled.
+// kp_kernels_mixed.cu -- the mixed-precision wavefront kernels.  FP64 ray
+// state, stage combination and step control everywhere; the far kernel
+// (rays beyond ImageConsts::fp32_radius) contracts the connection in FP32,
+// the near kernels in FP64; radiative transfer (near-B) in FP32.  Compiled with FMA
+// contraction enabled.  Both always carry four frequency channels, so the
+// same compiled code traces a ray whatever the rest of the batch is.
 #include <cuda_runtime.h>
 
 #include "kp_launch.h"
 #include "kp_persistent.cuh"
 
-#ifndef KP_PERSISTENT_MIN_BLOCKS
-// resident CTAs of 128 threads per SM the persistent kernel is compiled for
-#define KP_PERSISTENT_MIN_BLOCKS 2
+// resident CTAs of 128 threads per SM the wavefront kernels are compiled for
+#ifndef KP_FAR_MIN_BLOCKS
+#define KP_FAR_MIN_BLOCKS 2
+#endif
+#ifndef KP_NEAR_MIN_BLOCKS
+#define KP_NEAR_MIN_BLOCKS 2
 #endif
 
 namespace kp {
 
-template<int NF>
-__global__ void __launch_bounds__(128, KP_PERSISTENT_MIN_BLOCKS) persistent_mixed(const LaunchDesc L) {
-    persistent_body<PolicyMixed, NF>(L);
+__global__ void __launch_bounds__(128, KP_FAR_MIN_BLOCKS) wave_far_mixed(const WaveDesc W) {
+    persistent_body<PolicyMixed, kMaxFreq, kPhaseFar>(W);
 }
 
-cudaError_t launch_persistent_mixed(const LaunchDesc& L, int nf_max, int blocks, int threads,
-                                    cudaStream_t stream) {
-    switch (nf_max) {
-    case 1: persistent_mixed<1><<<blocks, threads, 0, stream>>>(L); break;
-    case 2: persistent_mixed<2><<<blocks, threads, 0, stream>>>(L); break;
-    case 3: persistent_mixed<3><<<blocks, threads, 0, stream>>>(L); break;
-    case 4: persistent_mixed<4><<<blocks, threads, 0, stream>>>(L); break;
-    default: return cudaErrorInvalidValue;
-    }
-    return cudaGetLastError();
+__global__ void __launch_bounds__(128, KP_NEAR_MIN_BLOCKS) wave_near_a_mixed(const WaveDesc W) {
+    persistent_body<PolicyMixed, kMaxFreq, kPhaseNearA>(W);
 }
 
-int persistent_occupancy_mixed(int nf_max, int threads) {
+__global__ void __launch_bounds__(128, KP_NEAR_MIN_BLOCKS) wave_near_b_mixed(const WaveDesc W) {
+    persistent_body<PolicyMixed, kMaxFreq, kPhaseNearB>(W);
+}
+
+static const void* wave_kernel_mixed(int phase) {
+    if (phase == kPhaseFar) return reinterpret_cast<const void*>(wave_far_mixed);
+    if (phase == kPhaseNearA) return reinterpret_cast<const void*>(wave_near_a_mixed);
+    return reinterpret_cast<const void*>(wave_near_b_mixed);
+}
+
+cudaError_t launch_wave_mixed(int phase, const WaveDesc& W, int blocks, int threads, cudaStream_t stream) {
+    if (phase < 0 || phase >= kPhases) return cudaErrorInvalidValue;
+    void* args[] = {const_cast<WaveDesc*>(&W)};
+    return cudaLaunchKernel(wave_kernel_mixed(phase), dim3(blocks), dim3(threads), args, 0, stream);
+}
+
+int wave_occupancy_mixed(int phase, int threads) {
+    if (phase < 0 || phase >= kPhases) return 0;
     int n = 0;
-    switch (nf_max) {
-    case 1: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, persistent_mixed<1>, threads, 0); break;
-    case 2: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, persistent_mixed<2>, threads, 0); break;
-    case 3: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, persistent_mixed<3>, threads, 0); break;
-    default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, persistent_mixed<4>, threads, 0); break;
-    }
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wave_kernel_mixed(phase), threads, 0);
     return n;
 }
 

@@ -1,7 +1,21 @@
-// kp_persistent.cuh -- the persistent image kernel: lanes claim rays from a
-// global queue that spans every job of the launch, advance them one RK job
-// per loop iteration through the pass-A / crossing / pass-B control machine,
-// and write the finished pixel.  See kp_engine.cuh for the design.
+// kp_persistent.cuh -- the wavefront image kernels.  Lanes claim rays from a
+// phase queue (fresh camera rays, then ray ids handed over by other phases),
+// advance them one RK job per loop iteration through the pass-A / crossing /
+// pass-B control machine, and either finish the pixel or park the ray's
+// record in HBM for another phase (or for the next round when an iteration
+// budget is set).  See kp_engine.cuh for the RK jobs.
+//
+// Three phases, one kernel each, so that the lanes of a warp run the same
+// code and each kernel's instruction working set stays small:
+//   far     rays beyond ImageConsts::fp32_radius, pass A and pass B: pure
+//           transport (no surface lies within a step, no plasma is sampled);
+//   near-A  pass A inside: the surface-crossing search, no radiation;
+//   near-B  pass B inside: radiative transfer, Stokes vectors in registers.
+//
+// Parking happens only at the top of the pass-A or pass-B loop, where the
+// whole state is the record: a ray resumed from its record takes exactly the
+// arithmetic it would have taken without parking, so results do not depend on
+// how rays are distributed over launches, lanes or warps.
 #pragma once
 
 #include "kp_engine.cuh"
@@ -10,21 +24,23 @@ namespace kp {
 
 enum : int { kEndA = 7 };
 
+// Control state of one ray (doubles first: 16 doubles + 16 ints, 192 bytes).
 struct LaneState {
-    int job, pixel, mode, in_b;
     // adaptive attempt sequence (rk4.hpp:108-161)
-    int attempt, rk_kind;
     double h_try, req_h, ctl_min, ctl_max;
     // pass A (pass_b.hpp:786-938)
-    int n, entered, inside, pa_steps, reason;
     double h_current, old_r;
     // surface-crossing search (pass_a_core.hpp:94-197)
-    int cross_reason, iter, use_secant;
     double lo, hi, flo, fhi, full_h, surf, trial;
     // pass B (pass_b.hpp:940-1114)
-    int steps, reached;
     double cap, hB, start_r;
+    int job, pixel, mode, in_b;
+    int attempt, rk_kind;
+    int n, entered, inside, pa_steps, reason;
+    int cross_reason, iter, use_secant;
+    int steps, reached;
 };
+static_assert(sizeof(LaneState) <= sizeof(((RayRecord*)nullptr)->st), "LaneState must fit its record slot");
 
 __device__ __forceinline__ void begin_adaptive(LaneState& L, double requested, double min_step,
                                                double max_step) {
@@ -96,161 +112,219 @@ __device__ __forceinline__ void store_stokes_n(const ImageOutPtrs& out, int pixe
     }
 }
 
-template<class P, int NF>
-__device__ __forceinline__ void persistent_body(const LaunchDesc& L) {
+// Warp-aggregated append of the ids of the lanes in `mask` to a queue.
+__device__ __forceinline__ void queue_push(unsigned* ids, unsigned* count, bool push, unsigned id) {
+    const unsigned FULL = 0xffffffffu;
+    const unsigned m = __ballot_sync(FULL, push);
+    if (!m) return;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(m) - 1;
+    unsigned base = 0;
+    if (lane == leader) base = atomicAdd(count, unsigned(__popc(m)));
+    base = __shfl_sync(FULL, base, leader);
+    if (push) ids[base + __popc(m & ((1u << lane) - 1u))] = id;
+}
+
+// Phase that advances a ray from the top of its pass-A or pass-B loop.
+__device__ __forceinline__ int phase_of(const ImageConsts& c, int in_b, double r_bl) {
+    if (r_bl > c.fp32_radius) return kPhaseFar;
+    return in_b ? kPhaseNearB : kPhaseNearA;
+}
+
+template<class P, int NF, int PHASE>
+__device__ __forceinline__ void persistent_body(const WaveDesc& W) {
+    constexpr bool kFar = PHASE == kPhaseFar;
+    constexpr bool kPassA = PHASE != kPhaseNearB;   // pass-A steps run here
+    constexpr bool kPassB = PHASE != kPhaseNearA;   // pass-B steps run here
+    constexpr bool kCross = PHASE == kPhaseNearA;   // surface-crossing search
+    constexpr bool kRad = PHASE == kPhaseNearB;     // radiative transfer (Stokes in registers)
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
+    using RT = RadTraits<P>;
     LaneState st;
     st.mode = kIdle;
     st.job = -1;
     st.rk_kind = -1;
     Ray S;
     Ray best;
-    using RT = RadTraits<P>;
     typename RT::Stokes stokes[NF];
-    int finished = 0;
-    long long my_ray = -1;
-    if (!L.refill) {
-        my_ray = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-        if (my_ray >= L.total_rays) finished = 1;
-    }
+    unsigned my_id = 0;
+    int exhausted = 0;
+    long long lane_jobs = 0;
     const JobDesc* J = nullptr;
-    long long guard = 0;
+    const long long nfresh = W.fresh_end - W.fresh_begin;
+    const long long total_in = nfresh + (long long)(W.in_ids ? *W.in_count : 0u);
 
 #pragma unroll 1
     while (true) {
-        // ------------------------------------------------------------ refill
-        const bool want = !finished && st.mode == kIdle;
-        if (L.refill) {
-            const unsigned need = __ballot_sync(FULL, want);
-            if (need) {
-                unsigned long long base = 0;
-                const int leader = __ffs(need) - 1;
-                if (lane == leader) base = atomicAdd(L.next_ray, (unsigned long long)__popc(need));
-                base = __shfl_sync(FULL, base, leader);
-                if (want) {
-                    my_ray = (long long)(base + __popc(need & ((1u << lane) - 1u)));
-                    if (my_ray >= L.total_rays) finished = 1;
+        // ------------------------------------------------------------ claim
+        const bool want = !exhausted && st.mode == kIdle;
+        const unsigned need = __ballot_sync(FULL, want);
+        if (need) {
+            unsigned long long base = 0;
+            const int leader = __ffs(need) - 1;
+            if (lane == leader) base = atomicAdd(W.in_head, (unsigned long long)__popc(need));
+            base = __shfl_sync(FULL, base, leader);
+            if (want) {
+                const long long k = (long long)(base + __popc(need & ((1u << lane) - 1u)));
+                if (k >= total_in) {
+                    exhausted = 1;
+                } else if (k < nfresh) {
+                    // a fresh camera ray: locate its job and start pass A
+                    const long long id = W.fresh_begin + k;
+                    int lo = 0, hi = W.njobs - 1;
+                    while (lo < hi) {
+                        const int mid = (lo + hi + 1) >> 1;
+                        if (W.jobs[mid].ray_begin <= id) lo = mid; else hi = mid - 1;
+                    }
+                    my_id = unsigned(id);
+                    st.job = lo;
+                    J = &W.jobs[lo];
+                    st.pixel = int(id - J->ray_begin);
+                    S = camera_ray(J->c, J->frame, st.pixel);
+                    st.reason = kMaxSteps;
+                    st.pa_steps = 0;
+                    st.n = 0;
+                    st.entered = 0;
+                    st.inside = 0;
+                    st.in_b = 0;
+                    st.steps = 0;
+                    st.reached = 0;
+                    st.h_current = -abs_val(J->c.step);
+                    st.mode = kAStep;
+                    st.rk_kind = -1;
+                } else {
+                    // a parked ray: resume from its record
+                    my_id = W.in_ids[k - nfresh];
+                    const RayRecord& rec = W.pool[my_id];
+                    S = rec.S;
+                    memcpy(&st, rec.st, sizeof(LaneState));
+                    J = &W.jobs[st.job];
+                    if constexpr (kRad) memcpy(&stokes[0], rec.stokes, sizeof(stokes));
                 }
             }
         }
-        if (!finished && st.mode == kIdle) {
-            int lo = 0, hi = L.njobs - 1;
-            while (lo < hi) {
-                const int mid = (lo + hi + 1) >> 1;
-                if (L.jobs[mid].ray_begin <= my_ray) lo = mid; else hi = mid - 1;
-            }
-            st.job = lo;
-            J = &L.jobs[lo];
-            st.pixel = int(my_ray - J->ray_begin);
-            S = camera_ray(J->c, J->frame, st.pixel);
-            st.reason = kMaxSteps;
-            st.pa_steps = 0;
-            st.n = 0;
-            st.entered = 0;
-            st.inside = 0;
-            st.in_b = 0;
-            st.steps = 0;
-            st.h_current = -abs_val(J->c.step);
-            st.mode = kAStep;
-            st.rk_kind = -1;
-            guard = 0;
-        }
-        const bool active = !finished && st.mode != kIdle;
+        const bool active = st.mode != kIdle;
         if (!__any_sync(FULL, active)) break;
 
         // ---------------------------------------------- control before the job
-        if (active && st.mode == kAStep && st.rk_kind < 0) {
-            // pass-A loop top (pass_b.hpp:793-838)
-            const ImageConsts& c = J->c;
-            if (st.n >= c.max_steps) {
-                st.mode = kEndA;
-            } else {
+        int dest = -1;  // phase the ray is handed to (PHASE itself: next round)
+        if constexpr (kPassA) {
+            if (active && st.mode == kAStep && st.rk_kind < 0) {
+                const ImageConsts& c = J->c;
                 const double r_bl = ks_radius(c.spin, S.x);
-                if (!st.entered) {
-                    if (r_bl <= c.outer_radius) {
-                        st.entered = 1;
-                        st.inside = 0;
+                const int want_phase = phase_of(c, 0, r_bl);
+                if (want_phase != PHASE) {
+                    dest = want_phase;
+                } else if (W.budget > 0 && lane_jobs >= W.budget) {
+                    dest = PHASE;
+                } else if (st.n >= c.max_steps) {
+                    // pass-A loop top (pass_b.hpp:793-838)
+                    st.mode = kEndA;
+                } else {
+                    if (!st.entered) {
+                        if (r_bl <= c.outer_radius) {
+                            st.entered = 1;
+                            st.inside = 0;
+                        }
+                    } else if (r_bl - c.inner_radius <= 0.0) {
+                        st.reason = kReachedInner;
+                        st.mode = kEndA;
+                    } else if (st.inside > 0 && r_bl >= c.outer_radius) {
+                        st.reason = kEscaped;
+                        st.mode = kEndA;
                     }
-                } else if (r_bl - c.inner_radius <= 0.0) {
-                    st.reason = kReachedInner;
-                    st.mode = kEndA;
-                } else if (st.inside > 0 && r_bl >= c.outer_radius) {
-                    st.reason = kEscaped;
-                    st.mode = kEndA;
-                }
-                if (st.mode == kAStep) {
-                    st.old_r = r_bl;
-                    double mn = c.min_step_abs;
-                    if (abs_val(st.h_current) < mn) mn = abs_val(st.h_current);
-                    issue_step(st, c, st.h_current, mn, c.max_step);
+                    if (st.mode == kAStep) {
+                        st.old_r = r_bl;
+                        double mn = c.min_step_abs;
+                        if (abs_val(st.h_current) < mn) mn = abs_val(st.h_current);
+                        issue_step(st, c, st.h_current, mn, c.max_step);
+                    }
                 }
             }
-        }
-        if (active && st.mode == kEndA) {
-            // end of pass A (pass_b.hpp:940-955)
-            const ImageConsts& c = J->c;
-            if (st.entered && (st.reason == kReachedInner || st.reason == kEscaped)) {
-                st.in_b = 1;
-                st.mode = kBStep;
-                st.rk_kind = -1;
-                st.steps = 0;
-                st.reached = 0;
-                st.h_current = c.step;
-                st.cap = c.max_radiation_step > 0.0 ? c.max_radiation_step : c.max_step;
+            if (active && dest < 0 && st.mode == kEndA) {
+                // end of pass A (pass_b.hpp:940-955)
+                const ImageConsts& c = J->c;
+                if (st.entered && (st.reason == kReachedInner || st.reason == kEscaped)) {
+                    st.in_b = 1;
+                    st.mode = kBStep;
+                    st.rk_kind = -1;
+                    st.steps = 0;
+                    st.reached = 0;
+                    st.h_current = c.step;
+                    st.cap = c.max_radiation_step > 0.0 ? c.max_radiation_step : c.max_step;
+                    // pass B starts from zero Stokes, kept in the record until
+                    // the ray reaches the radiating phase
 #pragma unroll
-                for (int f = 0; f < NF; ++f) RT::zero(stokes[f]);
-            } else {
-                st.mode = kDone;
+                    for (int f = 0; f < NF; ++f) RT::zero(stokes[f]);
+                    memcpy(W.pool[my_id].stokes, &stokes[0], sizeof(stokes));
+                } else {
+                    st.mode = kDone;
+                }
             }
         }
-        if (active && st.mode == kBStep && st.rk_kind < 0) {
-            // pass-B loop top (pass_b.hpp:966-981)
+        if (active && dest < 0 && st.mode == kBStep && st.rk_kind < 0) {
             const ImageConsts& c = J->c;
             if (st.reached || st.steps >= c.max_steps) {
                 st.mode = kDone;
             } else {
-                double h = st.h_current;
-                st.start_r = ks_radius(c.spin, S.x);
-                if (st.start_r <= c.outer_radius && st.cap > 0.0) h = min_val(h, st.cap);
-                st.hB = h;
-                issue_step(st, c, h, c.min_step_abs, c.max_step);
+                const double r_bl = ks_radius(c.spin, S.x);
+                const int want_phase = phase_of(c, 1, r_bl);
+                if (want_phase != PHASE) {
+                    dest = want_phase;
+                } else if (W.budget > 0 && lane_jobs >= W.budget) {
+                    dest = PHASE;
+                } else {
+                    // pass-B loop top (pass_b.hpp:966-981)
+                    double h = st.h_current;
+                    st.start_r = r_bl;
+                    if (st.start_r <= c.outer_radius && st.cap > 0.0) h = min_val(h, st.cap);
+                    st.hB = h;
+                    issue_step(st, c, h, c.min_step_abs, c.max_step);
+                }
             }
         }
+        const bool park = dest >= 0;
+        if (park) {
+            RayRecord& rec = W.pool[my_id];
+            rec.S = S;
+            memcpy(rec.st, &st, sizeof(LaneState));
+            if constexpr (kRad) memcpy(rec.stokes, &stokes[0], sizeof(stokes));
+        }
+        // A lane past its budget keeps claiming and parks each claimed ray at
+        // once, so every input ends the launch finished or in a queue.
+#pragma unroll
+        for (int d = 0; d < kPhases; ++d) queue_push(W.out_ids[d], W.out_count[d], dest == d, my_id);
+        if (park) st.mode = kIdle;
 
         // ------------------------------------------------------------ RK job
-        const bool run = active && (st.mode == kAStep || st.mode == kACrossHi || st.mode == kACrossTrial ||
-                                    st.mode == kBStep || st.mode == kBCamCross);
-        // Mixed policy: FP32 contraction only for jobs that start outside the
-        // radiating sphere (by two maximal steps).  Inside it, FP32 noise in
-        // the RHS reaches the step-doubling error estimate at the tolerance
-        // level and reshapes the accepted-step sequence the Faraday-thick
-        // transfer is sensitive to.  The choice depends only on the lane's own
-        // ray, so a ray's result does not depend on its warp-mates.
-        bool fp32 = false;
-        if constexpr (P::kMixed) {
-            fp32 = run && ks_radius(J->c.spin, S.x) > J->c.fp32_radius;
-        }
+        const bool run = !park && (st.mode == kAStep || st.mode == kACrossHi || st.mode == kACrossTrial ||
+                                   st.mode == kBStep || st.mode == kBCamCross);
+        // Mixed policy: FP32 contraction in the far phase only.  Inside the
+        // radiating sphere FP32 noise in the RHS reaches the step-doubling
+        // error estimate at the tolerance level and reshapes the accepted-step
+        // sequence the Faraday-thick transfer is sensitive to.
+        constexpr bool fp32 = P::kMixed && kFar;
         Ray next, mid;
         double err = 0.0;
         if (run) {
             const double mass = J->c.mass, spin = J->c.spin;
-            if (st.mode == kACrossHi || st.mode == kACrossTrial) {
+            if (kCross && (st.mode == kACrossHi || st.mode == kACrossTrial)) {
                 const double hh = st.mode == kACrossHi ? st.full_h : st.full_h * st.trial;
-                rk_job<P>(J->c.adaptive ? kRkRK4x2 : kRkRK4, mass, spin, S, hh, fp32, next, mid, err);
+                rk_job<P, fp32>(J->c.adaptive ? kRkRK4x2 : kRkRK4, mass, spin, S, hh, next, mid, err);
             } else {
-                rk_job<P>(st.rk_kind, mass, spin, S, st.h_try, fp32, next, mid, err);
+                rk_job<P, fp32>(st.rk_kind, mass, spin, S, st.h_try, next, mid, err);
             }
-            if (++guard > (1LL << 28)) {
+            if (++lane_jobs > (1LL << 30)) {
                 st.reason = kInvalidState;
                 st.mode = kDone;
                 st.in_b = 0;
-                atomicExch(L.status, 2);
+                atomicExch(W.status, 2);
             }
         }
 
         // ----------------------------------------------- control after the job
-        if (run && st.mode == kAStep) {
+        if (kPassA && run && st.mode == kAStep) {
             const ImageConsts& c = J->c;
             bool accepted = true;
             double used_h = st.h_try;
@@ -293,19 +367,25 @@ __device__ __forceinline__ void persistent_body(const LaunchDesc& L) {
                         crossing = kEscaped;
                     }
                     if (crossing != kNone) {
-                        st.cross_reason = crossing;
-                        st.surf = crossing == kReachedInner ? c.inner_radius : c.outer_radius;
-                        st.full_h = used_h;
-                        best = S;
-                        st.lo = 0.0;
-                        st.hi = 1.0;
-                        st.flo = ks_radius(c.spin, S.x) - st.surf;
-                        if (st.flo == 0.0 || !finite_ray(next)) {
-                            st.pa_steps += 1;  // the event keeps the first state
-                            st.reason = crossing;
-                            st.mode = kEndA;
+                        if constexpr (kCross) {
+                            st.cross_reason = crossing;
+                            st.surf = crossing == kReachedInner ? c.inner_radius : c.outer_radius;
+                            st.full_h = used_h;
+                            best = S;
+                            st.lo = 0.0;
+                            st.hi = 1.0;
+                            st.flo = ks_radius(c.spin, S.x) - st.surf;
+                            if (st.flo == 0.0 || !finite_ray(next)) {
+                                st.pa_steps += 1;  // the event keeps the first state
+                                st.reason = crossing;
+                                st.mode = kEndA;
+                            } else {
+                                st.mode = kACrossHi;
+                            }
                         } else {
-                            st.mode = kACrossHi;
+                            atomicExch(W.status, 3);  // surfaces lie inside the near phase
+                            st.reason = kInvalidState;
+                            st.mode = kDone;
                         }
                     } else {
                         S = next;
@@ -315,7 +395,7 @@ __device__ __forceinline__ void persistent_body(const LaunchDesc& L) {
                     }
                 }
             }
-        } else if (run && (st.mode == kACrossHi || st.mode == kACrossTrial)) {
+        } else if (kCross && run && (st.mode == kACrossHi || st.mode == kACrossTrial)) {
             const ImageConsts& c = J->c;
             bool finish = false;
             if (st.mode == kACrossHi) {
@@ -372,7 +452,7 @@ __device__ __forceinline__ void persistent_body(const LaunchDesc& L) {
                 st.trial = trial;
                 st.mode = kACrossTrial;
             }
-        } else if (run && (st.mode == kBStep || st.mode == kBCamCross)) {
+        } else if (kPassB && run && (st.mode == kBStep || st.mode == kBCamCross)) {
             const ImageConsts& c = J->c;
             const bool cam = st.mode == kBCamCross;
             bool proceed = true;
@@ -429,15 +509,17 @@ __device__ __forceinline__ void persistent_body(const LaunchDesc& L) {
                         (c.max_radiation_step > 0.0 &&
                          (st.start_r <= c.outer_radius || sample_r <= c.outer_radius || next_r <= c.outer_radius))
                             ? c.max_radiation_step : 0.0;
-                    typename RT::Co co[NF];
-                    typename RT::Sample ps = RT::none();
-                    if (sample_r - c.inner_radius > 0.0 && sample_r < c.outer_radius) ps = RT::sample(c, sample);
-                    int required = 1;
-                    const int nf = c.nfreq;
-#pragma unroll
-                    for (int f = 0; f < NF; ++f) {
-                        co[f] = typename RT::Co{};
-                        if (f < nf) {
+                    if constexpr (kRad) {
+                        // The frequency loops stay rolled: one copy of the
+                        // coefficient and transfer code keeps the kernel's
+                        // instruction working set small.
+                        typename RT::Co co[NF];
+                        typename RT::Sample ps = RT::none();
+                        if (sample_r - c.inner_radius > 0.0 && sample_r < c.outer_radius) ps = RT::sample(c, sample);
+                        int required = 1;
+                        const int nf = c.nfreq < NF ? c.nfreq : NF;
+#pragma unroll 1
+                        for (int f = 0; f < nf; ++f) {
                             co[f] = RT::coeffs(c, ps, f);
                             if (!c.faraday_rotation) co[f].rV = 0.0;
                             const int cand = radiation_substep_count(co[f], h, c.dlambda_scale[f], local_max_rs,
@@ -445,32 +527,41 @@ __device__ __forceinline__ void persistent_body(const LaunchDesc& L) {
                                                                      c.max_faraday_depth);
                             required = cand > required ? cand : required;
                         }
-                    }
-                    if (required > 1 && h > c.min_step_abs * 1.0001) {
-                        st.h_current = max_val(c.min_step_abs, h / double(required));
-                        st.cap = st.h_current;
-                    } else {
-                        if (local_max_rs > 0.0 || c.max_radiation_depth > 0.0 || c.max_absorption_depth > 0.0 ||
-                            c.max_faraday_depth > 0.0) {
-                            int pred = 1;
-#pragma unroll
-                            for (int f = 0; f < NF; ++f) {
-                                if (f < nf) {
+                        if (required > 1 && h > c.min_step_abs * 1.0001) {
+                            st.h_current = max_val(c.min_step_abs, h / double(required));
+                            st.cap = st.h_current;
+                        } else {
+                            if (local_max_rs > 0.0 || c.max_radiation_depth > 0.0 || c.max_absorption_depth > 0.0 ||
+                                c.max_faraday_depth > 0.0) {
+                                int pred = 1;
+#pragma unroll 1
+                                for (int f = 0; f < nf; ++f) {
                                     const int cand = radiation_substep_count(
                                         co[f], st.h_current, c.dlambda_scale[f], local_max_rs,
                                         c.max_radiation_depth, c.max_absorption_depth, c.max_faraday_depth);
                                     pred = cand > pred ? cand : pred;
                                 }
+                                st.cap = pred > 1 ? max_val(c.min_step_abs, st.h_current / double(pred)) : c.max_step;
+                            } else {
+                                st.cap = c.max_step;
                             }
-                            st.cap = pred > 1 ? max_val(c.min_step_abs, st.h_current / double(pred)) : c.max_step;
-                        } else {
-                            st.cap = c.max_step;
+                            if (h > 0.0) {
+#pragma unroll 1
+                                for (int f = 0; f < nf; ++f) RT::step(stokes[f], co[f], h, c, f);
+                            }
+                            S = next;
+                            st.steps += 1;
+                            if (crosses) st.reached = 1;
                         }
-                        if (h > 0.0) {
-#pragma unroll
-                            for (int f = 0; f < NF; ++f)
-                                if (f < nf) RT::step(stokes[f], co[f], h, c, f);
+                    } else {
+                        // Far phase: the sample lies outside the radiating
+                        // sphere, every coefficient is zero and the transfer
+                        // step leaves the Stokes vector unchanged; the step
+                        // cap resolves to max_step (pass_b.hpp:1482-1486).
+                        if (local_max_rs > 0.0 || (sample_r - c.inner_radius > 0.0 && sample_r < c.outer_radius)) {
+                            atomicExch(W.status, 3);
                         }
+                        st.cap = c.max_step;
                         S = next;
                         st.steps += 1;
                         if (crosses) st.reached = 1;
@@ -482,7 +573,7 @@ __device__ __forceinline__ void persistent_body(const LaunchDesc& L) {
         }
 
         // ------------------------------------------------------------ finish
-        if (active && st.mode == kDone) {
+        if (!park && st.mode == kDone) {
             const ImageConsts& c = J->c;
             PixelOut o;
             o.pass_a_steps = st.pa_steps;
@@ -499,14 +590,18 @@ __device__ __forceinline__ void persistent_body(const LaunchDesc& L) {
             const Ray cam = camera_ray(c, J->frame, st.pixel);
             double obs[NF][4];
             Stokes4<double> sd[NF];
+            if constexpr (!kRad) {
+                // only the radiating phase carries the Stokes vector: it is in the record
+                if (st.in_b) memcpy(&stokes[0], W.pool[my_id].stokes, sizeof(stokes));
+            }
 #pragma unroll
             for (int f = 0; f < NF; ++f)
                 sd[f] = st.in_b ? RT::result(stokes[f], c, f) : Stokes4<double>{0.0, 0.0, 0.0, 0.0};
             finish_ray<double, NF>(c, cam, S, st.in_b, sd, o, obs);
             store_stokes_n<NF>(J->out, st.pixel, J->npix, c.nfreq, obs);
             store_diagnostics(J->out, st.pixel, o);
+            if (W.job_done) atomicAdd(&W.job_done[st.job], 1u);
             st.mode = kIdle;
-            if (!L.refill) finished = 1;
         }
     }
 }
