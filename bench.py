@@ -2,16 +2,24 @@
 """Benchmark of the KPolaris-B200 RIAF image path.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--path plain|mixed] [--n 256]
+                    [--path mixed|plain] [--n 256] [--batch 8]
 
-Workload (default): the multi-frequency RIAF configuration -- 256x256 pixels,
+Workload: the multi-frequency RIAF configuration -- 256x256 pixels,
 frequencies {86, 230, 345, 690} GHz sharing one geodesic per pixel, adaptive
 step-doubling RK4 (tolerance 1e-8), Cartesian Kerr-Schild a = 0.9375, observer
 at r = 1000 M, inclination 17 deg.  Inputs are the analytic plasma model
-(synthetic by construction); one step renders one image on every rank.
+(synthetic by construction).
+
+Headline (`--path mixed`, default): one step traces `--batch` images through
+kp_batch_riaf, the mixed-precision wavefront engine (FP64 geodesic state and
+step control, FP32 far-field contraction and FP32 transfer).  The plain FP64
+one-image-per-launch kernel is timed in the same run (`plain_fp64`), and the
+first image of the batch is compared with it (`accuracy_vs_fp64`: total flux
+and image-integrated EVPA per frequency).  `--path plain` makes the plain
+kernel the headline.
 
 Metric: 256^2 images/s (whole job).  `value` is device-timed with outputs in
-HBM; `e2e` goes through the C ABI with host output buffers, launch-parameter
+HBM; `e2e` goes through the public API with host output buffers, job-table
 upload and device-to-host copies inside the timed region.  Multi-GPU runs are
 independent replicas (weak scaling): no collective on the data path.
 """
@@ -30,7 +38,7 @@ from pathlib import Path
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-METRIC = "256^2 images/s (RIAF, 4 frequencies, adaptive RK4)"
+METRIC = "256\u00b2 images/s & p50/p99 latency, mixed batched vs plain FP64, \u22641e-4 flux err"
 UNIT = "images/s"
 FLOP_TABLE = ROOT / "profiles" / "flop_counts.json"
 
@@ -41,8 +49,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--path", default="plain", choices=["plain", "mixed"])
+    ap.add_argument("--path", default="mixed", choices=["plain", "mixed"])
     ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--batch", type=int, default=8, help="images per step of the mixed path")
+    ap.add_argument("--plain-steps", type=int, default=3, help="timed images of the plain FP64 kernel")
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="target CPU time of the bounded CPU-baseline sample")
     return ap.parse_args()
@@ -62,8 +72,9 @@ def workload(n):
     return params, model, freqs
 
 
-def config_dict(n, path, nfreq, world):
-    return {"workload": f"riaf_{n}x{n}_4freq_adaptive_rk4", "pixels": n * n, "nfreq": nfreq,
+def config_dict(n, path, nfreq, world, batch=1):
+    return {"workload": f"riaf_{n}x{n}_4freq_adaptive_rk4", "images_per_step": batch,
+            "pixels": n * n, "nfreq": nfreq,
             "spin": 0.9375, "inclination_deg": 17.0, "r_obs": 1000.0, "tolerance": 1e-8,
             "path": path, "parallelism": f"replicas{world}",
             "l2": "flushed between timed steps (512 MiB write)",
@@ -126,7 +137,7 @@ def reference_arm(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / value,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (analytic RIAF plasma)",
-        "config": config_dict(args.n, "reference CPU (OpenMP dynamic over pixels)", len(freqs), 1),
+        "config": config_dict(args.n, "reference CPU (OpenMP dynamic over pixels)", len(freqs), 1, 1),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
                          "sample": samples[-1]},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -200,15 +211,44 @@ def device_outputs(torch, npix, nfreq, dev):
 
 
 def flop_model(n):
-    """Algorithmic FP64 operation count of one image of this workload, from
-    the committed count of the reference algorithm (oracle/flop_count)."""
+    """Algorithmic operation counts of one image of this workload, from the
+    committed count of the reference algorithm (oracle/flop_count.cpp)."""
     if not FLOP_TABLE.exists():
         return None
     table = json.loads(FLOP_TABLE.read_text())
     return table.get(f"riaf_{n}x{n}_4freq_adaptive_rk4")
 
 
+PHASES = ("far", "near_a", "near_b")
+
+
+def phase_ops(flops, phase, mixed):
+    """(fp64_ops, fp32_ops) of one image in one engine phase.  Mixed policy:
+    the far phase contracts the connection in FP32 and near-B evaluates the
+    plasma and the thermal fits in FP32; the rest is FP64."""
+    ph = flops[f"phase_{phase}"]
+    rhs, other = ph["rhs_ops"], ph["other_ops"]
+    rad = flops["plasma_ops"] + flops["thermal_ops"] if phase == "near_b" else 0
+    if not mixed:
+        return rhs + other + rad, 0
+    if phase == "far":
+        return other, rhs
+    return rhs + other, rad
+
+
+def integrated_stokes(i, q, u):
+    """Total flux and EVPA (degrees) of each frequency of an image."""
+    import numpy as np
+
+    out = []
+    for f in range(i.shape[0]):
+        ti, tq, tu = float(i[f].sum()), float(q[f].sum()), float(u[f].sum())
+        out.append((ti, 0.5 * float(np.degrees(np.arctan2(tu, tq)))))
+    return out
+
+
 def ours_arm(args):
+    import numpy as np
     import torch
 
     import kpolaris_b200 as kp
@@ -229,27 +269,53 @@ def ours_arm(args):
     params, model, freqs = workload(args.n)
     npix = args.n * args.n
     nfreq = len(freqs)
+    mixed = args.path == "mixed"
+    batch = args.batch if mixed else 1
     stream = torch.cuda.current_stream()
-    opt = kp._options(precision=_abi.PRECISION_MIXED if args.path == "mixed" else _abi.PRECISION_FP64,
-                      schedule=_abi.SCHEDULE_PERSISTENT if args.path == "mixed" else _abi.SCHEDULE_PER_PIXEL,
-                      device=local)
-    opt.outputs_on_device = 1
-    opt.stream = C.c_void_p(stream.cuda_stream)
-    outs, keep = device_outputs(torch, npix, nfreq, dev)
-    fa = (C.c_double * nfreq)(*freqs)
     flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
 
-    def step():
-        kp.check(lib.kp_image_riaf(C.byref(params), C.byref(model), 1, fa, nfreq, C.byref(opt),
-                                   C.byref(outs)))
+    # ---- headline path: `batch` images per step through kp_batch_riaf
+    # (mixed, wavefront engine) or one image per launch (plain FP64)
+    opt = kp._options(precision=_abi.PRECISION_MIXED if mixed else _abi.PRECISION_FP64,
+                      schedule=_abi.SCHEDULE_PERSISTENT if mixed else _abi.SCHEDULE_PER_PIXEL, device=local)
+    opt.outputs_on_device = 1
+    opt.stream = C.c_void_p(stream.cuda_stream)
+    outs = [device_outputs(torch, npix, nfreq, dev) for _ in range(batch)]
+    jobs = (_abi.RiafJob * batch)()
+    for b in range(batch):
+        j = jobs[b]
+        j.params = params
+        j.model = model
+        for f, v in enumerate(freqs):
+            j.frequencies[f] = v
+        j.nfreq = nfreq
+        j.radiation_substeps = 1
+        j.out = outs[b][0]
+    fa = (C.c_double * nfreq)(*freqs)
+    stats = _abi.BatchStats()
+    phase_s = [0.0, 0.0, 0.0]
+    launches = [0]
+
+    def step(record=False):
+        if mixed:
+            kp.check(lib.kp_batch_riaf(jobs, batch, C.byref(opt), C.byref(stats)))
+            if record:
+                for k in range(3):
+                    phase_s[k] += stats.phase_seconds[k]
+                launches[0] += stats.launches
+        else:
+            kp.check(lib.kp_image_riaf(C.byref(params), C.byref(model), 1, fa, nfreq, C.byref(opt),
+                                       C.byref(outs[0][0])))
+            if record:
+                launches[0] += 1
 
     for _ in range(max(3, args.warmup)):
         step()
     torch.cuda.synchronize()
-    # roofline denominators measured on this GPU
-    peak = C.c_double(0.0)
-    kp.check(lib.kp_measure_fma_peak(local, 1, C.byref(peak)))
-    fp64_peak = peak.value
+    peak64 = C.c_double(0.0)
+    kp.check(lib.kp_measure_fma_peak(local, 1, C.byref(peak64)))
+    peak32 = C.c_double(0.0)
+    kp.check(lib.kp_measure_fma_peak(local, 0, C.byref(peak32)))
 
     uuid = None
     try:
@@ -268,31 +334,65 @@ def ours_arm(args):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        step()
+        step(record=True)
         e1.record(stream)
         evs.append((e0, e1))
     torch.cuda.synchronize()
     clocks = sampler.stop()
     if pg:
         pg.barrier()
-    kernel_ms = [a.elapsed_time(b) for a, b in evs]
-    ms = sum(kernel_ms) / len(kernel_ms)
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    ms = sum(step_ms) / len(step_ms)
     if pg:
         t = torch.tensor([ms], device=dev)
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         ms = float(t.item())
-    value = world * 1000.0 / ms
+    value = world * batch * 1000.0 / ms
 
-    # e2e: the same image through the public C ABI with host buffers
-    host = _abi.ImageHostData.allocate(npix, nfreq)
-    opt_h = kp._options(precision=opt.precision, schedule=opt.schedule, device=local)
+    # ---- plain FP64 one-image-per-launch kernel, same run, same timing rules
+    plain_out = device_outputs(torch, npix, nfreq, dev)
+    opt_plain = kp._options(precision=_abi.PRECISION_FP64, schedule=_abi.SCHEDULE_PER_PIXEL, device=local)
+    opt_plain.outputs_on_device = 1
+    opt_plain.stream = C.c_void_p(stream.cuda_stream)
+
+    def plain_step():
+        kp.check(lib.kp_image_riaf(C.byref(params), C.byref(model), 1, fa, nfreq, C.byref(opt_plain),
+                                   C.byref(plain_out[0])))
+
+    plain_step()
+    plain_ms = []
+    for _ in range(args.plain_steps):
+        flush.fill_(1.0)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        plain_step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        plain_ms.append(e0.elapsed_time(e1))
+    plain_img_ms = sum(plain_ms) / len(plain_ms)
+
+    # accuracy of the headline path against the FP64 image (first image)
+    img = [t.cpu().numpy() for t in outs[0][1][0]]
+    ref = [t.cpu().numpy() for t in plain_out[1][0]]
+    got_int = integrated_stokes(img[0], img[1], img[2])
+    ref_int = integrated_stokes(ref[0], ref[1], ref[2])
+    flux_err = [abs(g[0] / r[0] - 1.0) if r[0] > 0 else 0.0 for g, r in zip(got_int, ref_int)]
+    evpa_err = [abs((g[1] - r[1] + 90.0) % 180.0 - 90.0) for g, r in zip(got_int, ref_int)]
+    reason_match = float(np.mean(outs[0][1][2][2].cpu().numpy() == plain_out[1][2][2].cpu().numpy()))
+
+    # ---- e2e: the same batch through the public API with host buffers
+    host = [_abi.ImageHostData.allocate(npix, nfreq) for _ in range(batch)]
+    job_list = [(params, model, freqs)] * batch
     e2e_ms = []
     for i in range(args.steps + 1):
         flush.fill_(1.0)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        kp.image_riaf(params, model, freqs, out=host, precision=opt.precision,
-                      schedule=opt.schedule, device=local)
+        if mixed:
+            kp.batch_riaf(job_list, outs=host, precision=_abi.PRECISION_MIXED, device=local)
+        else:
+            kp.image_riaf(params, model, freqs, out=host[0], device=local)
         dt = (time.perf_counter() - t0) * 1000.0
         if i > 0:
             e2e_ms.append(dt)
@@ -301,19 +401,40 @@ def ours_arm(args):
         t = torch.tensor([e2e], device=dev)
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         e2e = float(t.item())
-    d2h = lib.kp_image_output_bytes(npix, nfreq)
-    lib.kp_abi_sizeof.restype = C.c_size_t
-    h2d = int(lib.kp_abi_sizeof(6))
+    d2h = batch * int(lib.kp_image_output_bytes(npix, nfreq))
+    h2d = batch * int(lib.kp_abi_sizeof(6))
 
-    steps_per_image = int(host.pass_a_steps.astype("int64").sum() + host.steps.astype("int64").sum())
+    steps_per_image = int(host[0].pass_a_steps.astype("int64").sum() + host[0].steps.astype("int64").sum())
     flops = flop_model(args.n)
     roof = None
-    if flops:
+    phases = None
+    if flops and mixed and sum(phase_s) > 0:
+        phases = {}
+        for k, name in enumerate(PHASES):
+            f64, f32 = phase_ops(flops, name, mixed)
+            sec = phase_s[k] / args.steps
+            phases[name] = {"ms_per_step": sec * 1e3, "share": phase_s[k] / sum(phase_s),
+                            "fp64_tflops": batch * f64 / sec / 1e12 if sec > 0 else None,
+                            "fp32_tflops": batch * f32 / sec / 1e12 if sec > 0 else None}
+        top = max(range(3), key=lambda k: phase_s[k])
+        name = PHASES[top]
+        f64, f32 = phase_ops(flops, name, mixed)
+        sec = phase_s[top] / args.steps
+        bound64 = f64 / peak64.value >= f32 / peak32.value
+        achieved = batch * (f64 if bound64 else f32) / sec / 1e12
+        peak = peak64.value if bound64 else peak32.value
+        roof = {"bound": "fp64" if bound64 else "fp32", "kernel": f"wave_{name}_mixed",
+                "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                "traffic": None,
+                "peak_source": "measured FMA throughput of this GPU (kp_measure_fma_peak), of measured",
+                "flops_source": "algorithmic op count of the reference algorithm per phase "
+                                "(profiles/flop_counts.json) x images per launch"}
+    elif flops and not mixed:
         achieved = flops["fp64_flops"] / (ms * 1e-3) / 1e12
-        roof = {"bound": "fp64", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
-                "frac": achieved / fp64_peak, "traffic": flops.get("dram_bytes_per_launch"),
-                "peak_source": "measured FP64 FMA throughput on this GPU (kp_measure_fma_peak)",
-                "flops_source": "algorithmic FP64 operation count of the reference algorithm"}
+        roof = {"bound": "fp64", "kernel": "image_fp64_per_pixel", "achieved": achieved,
+                "peak": peak64.value, "unit": "TFLOP/s", "frac": achieved / peak64.value, "traffic": None,
+                "peak_source": "measured FP64 FMA throughput of this GPU (kp_measure_fma_peak), of measured",
+                "flops_source": "algorithmic FP64 op count of the reference algorithm"}
 
     cpu = None
     if rank == 0:
@@ -324,18 +445,27 @@ def ours_arm(args):
         cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
 
     if rank == 0:
+        srt = sorted(step_ms)
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": max(3, args.warmup), "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64" if args.path == "plain" else "f64-geometry/f32-transfer",
-            "data": "synthetic (analytic RIAF plasma)", "config": config_dict(args.n, args.path, nfreq, world),
-            "e2e": {"value": world * 1000.0 / e2e, "unit": UNIT, "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": int(d2h)},
-            "gpu_launches": args.steps,
+            "dtype": "f64-geometry/f32-transfer" if mixed else "f64",
+            "data": "synthetic (analytic RIAF plasma)",
+            "config": config_dict(args.n, args.path, nfreq, world, batch),
+            "e2e": {"value": world * batch * 1000.0 / e2e, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches[0],
+            "plain_fp64": {"images_per_s": world * 1000.0 / plain_img_ms, "ms_per_image": plain_img_ms,
+                           "kernel": "image_fp64_per_pixel (one image per launch)"},
+            "speedup_vs_plain_fp64": value / (world * 1000.0 / plain_img_ms),
+            "accuracy_vs_fp64": {"total_flux_rel_err": flux_err, "evpa_err_deg": evpa_err,
+                                 "reason_agreement": reason_match,
+                                 "frequencies_ghz": [f * 1e-9 for f in freqs]},
+            "step_latency_ms": {"p50": float(np.percentile(srt, 50)), "p99": float(np.percentile(srt, 99))},
             "rays_per_s": value * npix,
             "geodesic_steps_per_s": value * steps_per_image,
-            "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
+            "phases": phases, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
         }
         print(json.dumps(line), flush=True)
     if pg:

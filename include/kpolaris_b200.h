@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define KP_ABI_VERSION 1
+#define KP_ABI_VERSION 2
 /* Maximum frequencies that share one geodesic in a single launch
  * (reference compile-time KPOLARIS_MAX_FREQUENCIES, src/common/types.hpp:5-7). */
 #define KP_MAX_FREQUENCIES 4
@@ -247,8 +247,9 @@ int kp_abi_version(void);
 
 /* sizeof of the ABI structs, for the bindings' layout check:
  * 0 kp_camera_params, 1 kp_emission_selection, 2 kp_pass_a_params,
- * 3 kp_riaf_model, 4 kp_image_out, 5 kp_run_options; 6 is the bytes of
- * kernel parameters one image launch uploads; 0 for other ids. */
+ * 3 kp_riaf_model, 4 kp_image_out, 5 kp_run_options, 7 kp_riaf_job,
+ * 8 kp_batch_stats; 6 is the bytes of the per-image job descriptor an
+ * image uploads to the device; 0 for other ids. */
 size_t kp_abi_sizeof(int which);
 
 /* Bytes of per-pixel output (15 doubles + 3 int32 = 132 B), the figure the
@@ -297,6 +298,11 @@ typedef struct kp_batch_stats {
     int blocks;                  /* CTAs of a near-phase launch */
     int threads_per_block;
     size_t device_output_bytes;  /* library-owned output scratch used */
+    /* Device time per engine phase (0 far, 1 near-A, 2 near-B), summed over
+     * the phase's launches: CUDA events recorded around every launch on the
+     * launching stream. */
+    double phase_seconds[3];
+    int phase_launches[3];
 } kp_batch_stats;
 
 /*

@@ -11,7 +11,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-KP_ABI_VERSION = 1
+KP_ABI_VERSION = 2
 KP_MAX_FREQUENCIES = 4
 
 KP_OK = 0
@@ -147,6 +147,7 @@ class BatchStats(C.Structure):
         ("kernel_seconds", C.c_double), ("copy_seconds", C.c_double), ("rays", C.c_longlong),
         ("launches", C.c_int), ("blocks", C.c_int), ("threads_per_block", C.c_int),
         ("device_output_bytes", C.c_size_t),
+        ("phase_seconds", C.c_double * 3), ("phase_launches", C.c_int * 3),
     ]
 
 

@@ -69,6 +69,7 @@ struct DeviceState {
     unsigned* d_ids[kPhases][2] = {};  // id queues per phase, by generation parity
     long long pool_cap = 0;
     unsigned* h_left = nullptr;     // pinned: queue counts after a cycle
+    cudaEvent_t ev_launch[kMaxWaveCycles * kPhases + 1] = {};  // per-launch timing
 };
 
 static std::mutex g_mutex;
@@ -94,6 +95,7 @@ DeviceState* device_state(int device, int* status) {
         cudaEventCreate(&d.ev0);
         cudaEventCreate(&d.ev1);
         cudaEventCreateWithFlags(&d.staging_free, cudaEventDisableTiming);
+        for (auto& ev : d.ev_launch) cudaEventCreate(&ev);
         cudaDeviceGetAttribute(&d.sms, cudaDevAttrMultiProcessorCount, device);
         e = cudaMalloc(&d.d_ctrl, sizeof(WaveCtrl));
         if (e != cudaSuccess) {
@@ -400,7 +402,9 @@ size_t kp_abi_sizeof(int which) {
     case 3: return sizeof(kp_riaf_model);
     case 4: return sizeof(kp_image_out);
     case 5: return sizeof(kp_run_options);
-    case 6: return sizeof(ImageConsts) + 5 * sizeof(D4) + sizeof(ImageOutPtrs);
+    case 6: return sizeof(JobDesc);
+    case 7: return sizeof(kp_riaf_job);
+    case 8: return sizeof(kp_batch_stats);
     default: return 0;
     }
 }
@@ -719,10 +723,12 @@ int kp_batch_riaf(const kp_riaf_job* jobs, int njobs, const kp_run_options* opti
         if (cycle >= kMaxWaveCycles)
             return set_error(KP_ERR_TIMEOUT, "rays still moving between phases after %d launches", launches);
         for (int phase = 0; phase < kPhases; ++phase) {
+            if (stats) cudaEventRecord(dev->ev_launch[launches], stream);
             e = launch(cycle, phase);
             if (e != cudaSuccess) return cuda_error(e, "wavefront kernel launch");
             ++launches;
         }
+        if (stats) cudaEventRecord(dev->ev_launch[launches], stream);
         ++cycle;
         e = cudaMemcpyAsync(dev->h_left, ctrl->counts[cycle], sizeof(unsigned) * kPhases, cudaMemcpyDeviceToHost,
                             stream);
@@ -743,7 +749,15 @@ int kp_batch_riaf(const kp_riaf_job* jobs, int njobs, const kp_run_options* opti
     if (e != cudaSuccess) return cuda_error(e, "wavefront kernels");
     float ms = 0.f;
     cudaEventElapsedTime(&ms, dev->ev0, dev->ev1);
-    if (stats) stats->kernel_seconds = ms * 1e-3;
+    if (stats) {
+        stats->kernel_seconds = ms * 1e-3;
+        for (int k = 0; k < launches; ++k) {
+            float lms = 0.f;
+            cudaEventElapsedTime(&lms, dev->ev_launch[k], dev->ev_launch[k + 1]);
+            stats->phase_seconds[k % kPhases] += lms * 1e-3;
+            stats->phase_launches[k % kPhases] += 1;
+        }
+    }
     if (opt.timing) std::printf("timing image_kernel_batch %g s\n", ms * 1e-3);
     int status_word = 0;
     e = cudaMemcpy(&status_word, &ctrl->status, sizeof(int), cudaMemcpyDeviceToHost);

@@ -23,6 +23,7 @@ from kpolaris_b200 import _abi
 
 HERE = Path(__file__).resolve().parent
 PORT_SO = HERE / "libkporacle.so"
+ULP_SO = HERE / "libkporacle_ulp.so"
 REF_SO = HERE / "_ref" / "libkpref.so"
 REFERENCE_SRC = Path(os.environ.get("KPOLARIS_REFERENCE_SRC", "/root/reference/src"))
 
@@ -59,13 +60,15 @@ def ref_available() -> bool:
 
 
 def lib(kind: str):
-    """kind: 'port' or 'reference'."""
+    """kind: 'port', 'port_ulp' (the port with every libm result moved by up
+    to +-2 ulp, see set_libm_perturbation) or 'reference'."""
     if kind in _libs:
         return _libs[kind]
-    if kind == "port":
-        if not PORT_SO.exists():
+    if kind in ("port", "port_ulp"):
+        so = PORT_SO if kind == "port" else ULP_SO
+        if not so.exists():
             build(reference=False)
-        L = C.CDLL(str(PORT_SO))
+        L = C.CDLL(str(so))
         L.kpo_image_riaf_range.argtypes = [
             C.POINTER(_abi.PassAParams), C.POINTER(_abi.RIAFModel), C.c_int,
             C.POINTER(C.c_double), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
@@ -88,8 +91,13 @@ def lib(kind: str):
     return L
 
 
+def set_libm_perturbation(seed: int) -> None:
+    """Selects the pseudo-random ulp sequence of the 'port_ulp' oracle."""
+    lib("port_ulp").kpo_set_libm_perturbation(C.c_ulonglong(seed))
+
+
 def _prefix(kind):
-    return "kpo_" if kind == "port" else "kpref_"
+    return "kpref_" if kind == "reference" else "kpo_"
 
 
 def image_riaf(params, model, freqs, *, kind="port", integrator=0, threads=0,
@@ -104,7 +112,7 @@ def image_riaf(params, model, freqs, *, kind="port", integrator=0, threads=0,
         pixel_end = npix
     fa = (C.c_double * nfreq)(*freqs)
     s = out.as_struct()
-    if kind == "port":
+    if kind in ("port", "port_ulp"):
         rc = L.kpo_image_riaf_range(C.byref(params), C.byref(model), 1, fa, nfreq,
                                     int(integrator), int(threads), int(pixel_begin),
                                     int(pixel_end), C.byref(s))

@@ -108,14 +108,34 @@ struct CountingMetric : kpolaris::KerrSchildInMetric<R> {
 };
 static thread_local long long t_rhs = 0;
 
+// Engine phases (kpolaris_b200/csrc/kp_common.cuh): 0 far (Boyer-Lindquist
+// radius beyond fp32_radius), 1 near-A (pass A inside), 2 near-B (pass B
+// inside).  Every RHS call is binned by the radius of its evaluation point;
+// the other integration and transfer ops go to the phase of the latest RHS
+// call.  Pass B is recognised from the pixel's first plasma sample, so the
+// 11 RHS calls of a ray's first pass-B step count as near-A.
+static double g_spin = 0.9375;
+static double g_fp32_radius = 119.0;
+static thread_local int t_in_b = 0;
+static thread_local OpTally t_geom_phase[3];
+static thread_local long long t_rhs_phase[3] = {0, 0, 0};
+
+static double bl_radius(const kpolaris::TransportState<R>& s) {
+    const double x = s.x[1].v, y = s.x[2].v, z = s.x[3].v, a2 = g_spin * g_spin;
+    const double R2 = x * x + y * y + z * z;
+    const double d = R2 - a2;
+    return std::sqrt(0.5 * (d + std::sqrt(d * d + 4.0 * a2 * z * z)));
+}
+
 // Found by argument-dependent lookup from the reference's RK templates; as a
 // non-template exact match it is preferred over the generic transport_rhs.
 kpolaris::TransportState<R> transport_rhs(const CountingMetric& m, const kpolaris::TransportState<R>& s) {
     ++t_rhs;
-    OpTally* saved = g_tally;
+    const int phase = bl_radius(s) > g_fp32_radius ? 0 : (t_in_b ? 2 : 1);
+    ++t_rhs_phase[phase];
     g_tally = nullptr;
     auto d = kpolaris::transport_rhs(static_cast<const kpolaris::KerrSchildInMetric<R>&>(m), s);
-    g_tally = saved;
+    g_tally = &t_geom_phase[phase];
     return d;
 }
 
@@ -133,6 +153,7 @@ struct CountingRIAF : Base {
     template<class Metric>
     kpolaris::TransferCoeffs<R> coefficients(const Metric& metric, const kpolaris::TransportState<R>& state,
                                              R) const {
+        t_in_b = 1;
         double cur[16];
         for (int mu = 0; mu < 4; ++mu) {
             cur[mu] = state.x[mu].v;
@@ -258,9 +279,11 @@ int main(int argc, char** argv) {
     if (cfg == 1) {
         set_common(pa, n, 1.0, 0, 2000, 1e-8, 1e-5, 1.0, 1.0, -1, -1, -1);
         freqs = {230.0e9};
+        g_fp32_radius = 115.0 + 2.0 * 1.0;
     } else {
         set_common(pa, n, 0.025, 1, 400000, 1e-8, 1e-10, 2.0, 2.0, 1, 1, 4);
         freqs = {86.0e9, 230.0e9, 345.0e9, 690.0e9};
+        g_fp32_radius = 115.0 + 2.0 * 2.0;
     }
     CountingRIAF model;
     model.mbh_solar = R(6.5e9);
@@ -270,11 +293,13 @@ int main(int argc, char** argv) {
     model.emission_type = 1;
     const CountingMetric metric(R(1), pa.spin);
     const int npix = n * n;
-    OpTally tot_geom, tot_plasma, tot_thermal;
+    OpTally tot_geom, tot_plasma, tot_thermal, tot_phase[3];
     long long samples = 0, coeff = 0, steps_a = 0, steps_b = 0, rhs = 0;
+    long long rhs_phase[3] = {0, 0, 0};
 #pragma omp parallel reduction(+ : samples, coeff, steps_a, steps_b, rhs)
     {
-        OpTally g;
+        for (auto& t : t_geom_phase) t = OpTally();
+        for (auto& c : t_rhs_phase) c = 0;
         t_plasma = OpTally();
         t_thermal = OpTally();
         t_samples = 0;
@@ -282,7 +307,8 @@ int main(int argc, char** argv) {
         t_rhs = 0;
 #pragma omp for schedule(dynamic)
         for (int pixel = 0; pixel < npix; ++pixel) {
-            g_tally = &g;
+            t_in_b = 0;
+            g_tally = &t_geom_phase[0];
             R f[KPOLARIS_MAX_FREQUENCIES];
             kpolaris::Stokes<R> st[KPOLARIS_MAX_FREQUENCIES];
             for (size_t i = 0; i < freqs.size(); ++i) f[i] = R(freqs[i]);
@@ -298,8 +324,14 @@ int main(int argc, char** argv) {
         coeff += t_coeff;
 #pragma omp critical
         {
-            tot_geom.add += g.add; tot_geom.mul += g.mul; tot_geom.div += g.div;
-            tot_geom.sqrt += g.sqrt; tot_geom.trans += g.trans;
+            for (int ph = 0; ph < 3; ++ph) {
+                const OpTally& g = t_geom_phase[ph];
+                tot_geom.add += g.add; tot_geom.mul += g.mul; tot_geom.div += g.div;
+                tot_geom.sqrt += g.sqrt; tot_geom.trans += g.trans;
+                tot_phase[ph].add += g.add; tot_phase[ph].mul += g.mul; tot_phase[ph].div += g.div;
+                tot_phase[ph].sqrt += g.sqrt; tot_phase[ph].trans += g.trans;
+                rhs_phase[ph] += t_rhs_phase[ph];
+            }
             tot_plasma.add += t_plasma.add; tot_plasma.mul += t_plasma.mul; tot_plasma.div += t_plasma.div;
             tot_plasma.sqrt += t_plasma.sqrt; tot_plasma.trans += t_plasma.trans;
             tot_thermal.add += t_thermal.add; tot_thermal.mul += t_thermal.mul;
@@ -328,6 +360,12 @@ int main(int argc, char** argv) {
     dump("integration_and_transfer", tot_geom, ",");
     dump("plasma", tot_plasma, ",");
     dump("thermal", tot_thermal, ",");
+    std::printf(" \"fp32_radius\": %.17g,\n", g_fp32_radius);
+    const char* names[3] = {"far", "near_a", "near_b"};
+    for (int ph = 0; ph < 3; ++ph) {
+        std::printf(" \"phase_%s\": {\"rhs_calls\": %lld, \"rhs_ops\": %llu, \"other_ops\": %llu},\n", names[ph],
+                    rhs_phase[ph], basic(per_rhs) * (unsigned long long)rhs_phase[ph], basic(tot_phase[ph]));
+    }
     std::printf(" \"fp64_basic_ops\": %llu}\n",
                 basic(rhs_tot) + basic(tot_geom) + basic(tot_plasma) + basic(tot_thermal));
     return 0;

@@ -16,6 +16,51 @@
 
 #include <math.h>
 #include <omp.h>
+#ifdef KPO_PERTURB_LIBM
+/* Built as libkporacle_ulp.so: every libm result of this file is moved by a
+ * pseudo-random whole number of ulps in [-2, 2] (a fixed sequence per pixel
+ * and seed, kpo_set_libm_perturbation), the documented accuracy of the
+ * device's double-precision libm.  The spread of images over seeds measures
+ * how well an image is determined by double precision at all: no libm of
+ * that accuracy, the device's included, can be expected to agree with the
+ * reference more closely.  sqrt is correctly rounded everywhere and is left
+ * alone. */
+static unsigned long long g_perturb_seed = 0;
+static _Thread_local unsigned long long t_rng = 0;
+static double perturb(double r) {
+    if (!(r == r) || r == 0.0 || r - r != 0.0) return r;
+    t_rng ^= t_rng << 13;
+    t_rng ^= t_rng >> 7;
+    t_rng ^= t_rng << 17;
+    const int k = (int)(t_rng % 5ull) - 2;
+    for (int i = 0; i < k; ++i) r = nextafter(r, INFINITY);
+    for (int i = 0; i > k; --i) r = nextafter(r, -INFINITY);
+    return r;
+}
+static void perturb_pixel(int pixel) {
+    t_rng = 0x9E3779B97F4A7C15ull * (unsigned long long)(pixel + 1) + 0xD1B54A32D192ED03ull * (g_perturb_seed + 1);
+    if (!t_rng) t_rng = 1;
+}
+static double p_exp(double x) { return perturb(exp(x)); }
+static double p_log(double x) { return perturb(log(x)); }
+static double p_pow(double x, double y) { return perturb(pow(x, y)); }
+static double p_sin(double x) { return perturb(sin(x)); }
+static double p_cos(double x) { return perturb(cos(x)); }
+static double p_cbrt(double x) { return perturb(cbrt(x)); }
+static double p_acos(double x) { return perturb(acos(x)); }
+static double p_atan2(double y, double x) { return perturb(atan2(y, x)); }
+static double p_tanh(double x) { return perturb(tanh(x)); }
+#define exp p_exp
+#define log p_log
+#define pow p_pow
+#define sin p_sin
+#define cos p_cos
+#define cbrt p_cbrt
+#define acos p_acos
+#define atan2 p_atan2
+#define tanh p_tanh
+void kpo_set_libm_perturbation(unsigned long long seed) { g_perturb_seed = seed; }
+#endif
 #include <stdio.h>
 #include <string.h>
 
@@ -32,6 +77,8 @@ typedef struct { double jI, jQ, jU, jV, aI, aQ, aU, aV, rQ, rU, rV; } TC;
 typedef struct { double r11, r12, r21, r22; } OV;
 
 static _Thread_local char g_err[256];
+
+
 
 static int fail(const char* m) {
     snprintf(g_err, sizeof g_err, "%s", m);
@@ -1590,6 +1637,9 @@ int kpo_image_riaf_range(const kp_pass_a_params* params, const kp_riaf_model* mo
     if (threads > 0) omp_set_num_threads(threads);
 #pragma omp parallel for schedule(dynamic)
     for (int pixel = pixel_begin; pixel < pixel_end; ++pixel) {
+#ifdef KPO_PERTURB_LIBM
+        perturb_pixel(pixel);
+#endif
         PixelResult r;
         trace_pixel(pixel, params, model, fr, nfreq, integrator, &r);
         for (int f = 0; f < nfreq; ++f) {

@@ -92,3 +92,51 @@ def transfer_points(n: int = 64, seed: int = 11):
         dl = 10 ** rng.uniform(-3, 0.5)
         out.append((s4, c, dl))
     return out
+
+
+def libm_conditioning(name, seeds=(1, 2, 3)):
+    """libm_conditioning_of for a golden fixture."""
+    import json
+    from pathlib import Path
+
+    import numpy as np
+
+    fx = np.load(Path(__file__).resolve().parent / "golden" / f"{name}.npz")
+    params, model, freqs = build_case(json.loads(str(fx["spec"])))
+    return libm_conditioning_of(params, model, freqs, fx, seeds)
+
+
+def libm_conditioning_of(params, model, freqs, ref, seeds=(1, 2, 3), integrator=0):
+    """How well double precision determines an image (`ref`: its reference
+    result, a mapping of the output fields): per (channel, frequency) the
+    largest normwise change, per frequency ("flux", f) the relative change
+    of the image-integrated Stokes I, and per path diagnostic the largest
+    absolute change over the rays that reached the camera, when every libm
+    result of the oracle moves by up to +-2 ulp (the device libm's
+    documented accuracy), maximised over a few perturbation seeds.  No libm
+    of that accuracy -- the device's included -- can be expected to agree
+    with the reference more closely on that image."""
+    import numpy as np
+
+    import oracle
+    from kpolaris_b200 import _abi
+
+    ok = ref["reason"] == 1
+    out = {}
+    for seed in seeds:
+        oracle.set_libm_perturbation(seed)
+        res = oracle.image_riaf(params, model, freqs, kind="port_ulp", threads=4, integrator=integrator)
+        for key in _abi.IMAGE_FIELDS:
+            for f in range(ref[key].shape[0]):
+                scale = np.max(np.abs(ref[key][f]))
+                d = np.max(np.abs(res.arrays[key][f] - ref[key][f]))
+                v = d / scale if scale > 0 else d
+                out[(key, f)] = max(out.get((key, f), 0.0), v)
+        for f in range(ref["image_i"].shape[0]):
+            total = ref["image_i"][f].sum()
+            v = abs(res.image_i[f].sum() / total - 1.0) if total > 0 else 0.0
+            out[("flux", f)] = max(out.get(("flux", f), 0.0), v)
+        for key in _abi.DIAG_FIELDS:
+            d = np.abs(res.arrays[key][ok] - ref[key][ok])
+            out[key] = max(out.get(key, 0.0), float(d.max()) if d.size else 0.0)
+    return out

@@ -2,15 +2,22 @@
 
 FP64 bar (stated per result):
   * fixed-step runs: termination reason, pass-A and pass-B step counts
-    bit-exact; Stokes I/Q/U/V within max |gpu - oracle| <= 1e-10 * max |oracle|
-    per channel and frequency (the device's exp/pow/cbrt differ from glibc's in
-    the last ulp, so the radiation side is not bit-equal).
-  * adaptive runs: the step controller evaluates pow(tol/err, 0.2); glibc's pow
-    is itself not correctly rounded (~0.1% of calls), so accepted step
-    sequences can differ by an ulp and the path then moves at the 1e-12 level.
-    Reasons must agree exactly, step counts within +-2 (90% identical), Stokes
-    per channel within 1e-9 * max |oracle|, image-integrated Stokes (total flux)
-    within 1e-10 relative, path diagnostics within 1e-9 absolute.
+    bit-exact.
+  * adaptive runs: the step controller evaluates pow(tol/err, 0.2), so an ulp
+    of libm can change an accepted step; reasons must agree exactly, step
+    counts within +-2 (90% identical).
+  * Stokes I/Q/U/V per channel and frequency: max |gpu - oracle| within
+    max(base, 2 x conditioning) * max |oracle| (base 1e-10 fixed step, 1e-9
+    adaptive); total flux (image-integrated Stokes I) within max(1e-10,
+    2 x conditioning); path diagnostics within max(1e-12 fixed / 1e-9
+    adaptive, 2 x conditioning) absolute.
+  * conditioning (golden_cases.libm_conditioning): how far the oracle itself
+    moves when every libm result is moved by up to +-2 ulp, the device libm's
+    documented accuracy (largest over three perturbation seeds).  It is
+    <= 4e-12 on the well-conditioned cases, so their bar is the base one; on
+    Faraday-thick 86 GHz pixels (riaf_cfg2_8, riaf_capture_9) an ulp of a
+    rotativity becomes a rotation of Q/U of up to 3e-6, and no libm of that
+    accuracy can agree more closely there.
 """
 from __future__ import annotations
 
@@ -22,7 +29,7 @@ import pytest
 
 import kpolaris_b200 as kp
 import oracle
-from golden_cases import IMAGE_CASES, build_case
+from golden_cases import IMAGE_CASES, build_case, libm_conditioning, libm_conditioning_of
 from kpolaris_b200 import _abi, configs
 
 pytestmark = pytest.mark.gpu
@@ -31,6 +38,7 @@ STOKES_RTOL = 1e-10           # fixed step, per channel (normwise)
 STOKES_RTOL_ADAPTIVE = 1e-9   # adaptive, per channel (normwise)
 FLUX_RTOL = 1e-10             # image-integrated Stokes I (total flux), both modes
 DIAG_RTOL = 1e-9
+LIBM_FACTOR = 2.0             # margin over the +-2-ulp libm conditioning
 
 
 def stokes_error(a, b):
@@ -49,7 +57,8 @@ def _get(b, key):
     return b[key] if not hasattr(b, "arrays") else b.arrays[key]
 
 
-def check_fp64(res, ref, fixed: bool):
+def check_fp64(res, ref, fixed: bool, conditioning=None):
+    cond = conditioning or {}
     assert np.array_equal(res.reason, _get(ref, "reason"))
     if fixed:
         assert np.array_equal(res.pass_a_steps, _get(ref, "pass_a_steps"))
@@ -59,21 +68,24 @@ def check_fp64(res, ref, fixed: bool):
         db = np.abs(res.steps.astype(np.int64) - _get(ref, "steps"))
         assert (da <= 2).all() and (db <= 2).all()
         assert np.mean(da == 0) >= 0.9 and np.mean(db == 0) >= 0.9
-    tol = STOKES_RTOL if fixed else STOKES_RTOL_ADAPTIVE
+    base = STOKES_RTOL if fixed else STOKES_RTOL_ADAPTIVE
     for (key, f), e in stokes_error(res, ref).items():
-        assert e <= tol, (key, f, e)
+        tol = max(base, LIBM_FACTOR * cond.get((key, f), 0.0))
+        assert e <= tol, (key, f, e, tol)
     ref_i = _get(ref, "image_i")
     for f in range(ref_i.shape[0]):
         total = ref_i[f].sum()
         if total > 0:
-            assert abs(res.image_i[f].sum() / total - 1.0) <= FLUX_RTOL, ("total flux", f)
+            tol = max(FLUX_RTOL, LIBM_FACTOR * cond.get(("flux", f), 0.0))
+            e = abs(res.image_i[f].sum() / total - 1.0)
+            assert e <= tol, ("total flux", f, e, tol)
     ok = res.reason == 1
     for key in ("closure_x", "closure_k", "final_null", "frame_error", "det_r", "overlap_r11",
                 "overlap_r12", "overlap_r21", "overlap_r22", "basis_rotation_angle"):
         a = res.arrays[key][ok]
         b = _get(ref, key)[ok]
-        atol = 1e-12 if fixed else 1e-9
-        assert np.allclose(a, b, rtol=DIAG_RTOL, atol=atol), key
+        atol = max(1e-12 if fixed else 1e-9, LIBM_FACTOR * cond.get(key, 0.0))
+        assert np.allclose(a, b, rtol=DIAG_RTOL, atol=atol), (key, float(np.max(np.abs(a - b))), atol)
 
 
 @pytest.mark.parametrize("name", sorted(IMAGE_CASES))
@@ -82,7 +94,7 @@ def test_fp64_per_pixel_matches_golden(name):
     spec = json.loads(str(fx["spec"]))
     params, model, freqs = build_case(spec)
     res = kp.image_riaf(params, model, freqs)
-    check_fp64(res, fx, fixed=not params.adaptive)
+    check_fp64(res, fx, fixed=not params.adaptive, conditioning=libm_conditioning(name))
 
 
 def test_fp64_config1_full_size_bit_exact_steps():
@@ -100,7 +112,8 @@ def test_fp64_config2_sample_against_oracle():
     params, model, freqs = configs.config2(24, 24)
     res = kp.image_riaf(params, model, freqs)
     ref = oracle.image_riaf(params, model, freqs, kind="port", threads=0)
-    check_fp64(res, ref, fixed=False)
+    cond = libm_conditioning_of(params, model, freqs, ref.arrays)
+    check_fp64(res, ref, fixed=False, conditioning=cond)
 
 
 def test_fp64_repeat_is_bitwise_identical():
@@ -116,8 +129,9 @@ def test_single_pixel_and_cash_karp_variant():
     params, model, freqs = configs.config2(1, 1)
     res = kp.image_riaf(params, model, freqs)
     ref = oracle.image_riaf(params, model, freqs, kind="port", threads=1)
-    check_fp64(res, ref, fixed=False)
+    check_fp64(res, ref, fixed=False, conditioning=libm_conditioning_of(params, model, freqs, ref.arrays))
     params, model, freqs = configs.config2(8, 8)
     ck = kp.image_riaf(params, model, freqs, integrator=_abi.INTEGRATOR_CASH_KARP)
     ref = oracle.image_riaf(params, model, freqs, kind="port", integrator=1, threads=0)
-    check_fp64(ck, ref, fixed=False)
+    cond = libm_conditioning_of(params, model, freqs, ref.arrays, integrator=1)
+    check_fp64(ck, ref, fixed=False, conditioning=cond)
