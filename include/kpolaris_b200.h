@@ -325,6 +325,31 @@ typedef struct kp_batch_stats {
 int kp_batch_riaf(const kp_riaf_job* jobs, int njobs, const kp_run_options* options,
                   kp_batch_stats* stats);
 
+/* Limits of kp_batch_riaf_noalloc's static device scratch. */
+#define KP_NOALLOC_MAX_RAYS 65536
+#define KP_NOALLOC_MAX_JOBS 16
+
+/*
+ * kp_batch_riaf for callers that must not allocate: the same wavefront
+ * engine and results (bit-identical to kp_batch_riaf with the same options),
+ * but every piece of device scratch lives in one static device array of the
+ * library (31 MB per device), so the call makes no cudaMalloc/cudaFree and
+ * no host allocation.  For callers that run under a fixed device-memory
+ * budget, and for callers that cannot afford cudaFree's device-wide
+ * synchronisation while other streams are busy (a serving loop, a
+ * latency-sensitive pipeline).  Limits: at most KP_NOALLOC_MAX_RAYS pixels
+ * summed over the jobs (one 256x256 image) and KP_NOALLOC_MAX_JOBS jobs;
+ * larger batches fail with KP_ERR_INVALID before anything runs.  Outputs
+ * must be device arrays (options->outputs_on_device = 1); options->stream
+ * (NULL: the legacy default stream) carries the work, and the call returns
+ * when the images are complete.  The scratch is shared: calls on the same
+ * device that overlap in time (from several host threads) race and must be
+ * serialised by the caller.  The first call on a device looks the scratch up
+ * (cudaGetSymbolAddress) and must not happen inside a stream capture.
+ * No counterpart in the reference.
+ */
+int kp_batch_riaf_noalloc(const kp_riaf_job* jobs, int njobs, const kp_run_options* options);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif
