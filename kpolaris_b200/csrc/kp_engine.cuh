@@ -104,10 +104,12 @@ struct RadTraits<PolicyMixed> {
 };
 
 // FP32 is a compile-time choice of the calling kernel, so each kernel holds
-// one contraction body.
+// one contraction body.  The FP64 policy keeps the reference's operation
+// order; the mixed policy uses the factored form (kp_geometry_f32.cuh).
 template<class P, bool FP32>
 __device__ __forceinline__ Ray policy_rhs(double mass, double spin, const Ray& X) {
-    if constexpr (P::kMixed && FP32) return ks_rhs_f32(mass, spin, X);
+    if constexpr (P::kMixed && FP32) return ks_rhs_factored<float>(mass, spin, X);
+    else if constexpr (P::kMixed) return ks_rhs_factored<double>(mass, spin, X);
     else return ks_rhs(mass, spin, X);
 }
 

@@ -141,11 +141,40 @@ KP_HD void bessel_ratios_f(float x, float& r0, float& r1) {
     r1 = k2 > 0.0f ? q / k2 : 1.0f;
 }
 
-// Plasma state at a sample point (FP32).
+// Plasma state at a sample point (FP32), with the frequency-independent
+// factors of the thermal fits (riaf_sample_thermal_f).
 struct RiafSampleF {
     int emitting, on_axis, has_chi;
     float ne, thetae, b, nu_fluid, cos_theta, sin_theta, theta, cos2chi, sin2chi;
+    float r0, r1;   // K0/K2, K1/K2 at 1/Theta_e (Faraday fits)
+    float qterm;    // (7 T^0.96 + 35) / (10 T^0.96 + 75), Pandya jQ
+    float vt1;      // (37 - 87 sin(theta - 0.45)) / (100 (T + 1)), Pandya jV
+    float vt2a;     // T^0.6 / 25 + 0.7, Pandya jV
 };
+
+// x^y for x > 0 as 2^(y log2 x): one LG2 shared by several powers of x.
+KP_HD float pow2_of(float y, float lg2x) {
+#ifdef __CUDA_ARCH__
+    return exp2f(y * lg2x);
+#else
+    return std::exp2(y * lg2x);
+#endif
+}
+
+// Frequency-independent factors of the thermal fits at one sample
+// (thermal_synchrotron.hpp:312-395, 462-506), evaluated once per sample
+// instead of once per frequency.
+KP_HD void riaf_sample_thermal_f(const ImageConsts& c, RiafSampleF& p) {
+    const float te = p.thetae;
+    bessel_ratios_f(1.0f / te, p.r0, p.r1);
+    const float lt = log2f(te);
+    const float t2425 = pow2_of(24.0f / 25.0f, lt);
+    p.qterm = (7.0f * t2425 + 35.0f) / (10.0f * t2425 + 75.0f);
+    const float st = fmaxf(p.sin_theta, float(c.min_sin_theta));
+    const float sin_shift = st * 0.4356824462767121f - p.cos_theta * 0.9001004421765051f;
+    p.vt1 = (37.0f - 87.0f * sin_shift) / (100.0f * (te + 1.0f));
+    p.vt2a = pow2_of(0.6f, lt) / 25.0f + 0.7f;
+}
 
 KP_HD float dot_gf(const float g[4][4], const float* u, const float* v) {
     float out = 0.0f;
@@ -340,6 +369,7 @@ KP_HD RiafSampleF riaf_sample_f(const ImageConsts& c, const Ray& s) {
     out.cos_theta = fminf(fmaxf(kdotb / fmaxf(out.nu_fluid, 1e-30f), -1.0f), 1.0f);
     out.sin_theta = fmaxf(sqrtf(fmaxf(0.0f, 1.0f - out.cos_theta * out.cos_theta)), float(c.min_sin_theta));
     out.theta = acosf(out.cos_theta);
+    riaf_sample_thermal_f(c, out);
     if (out.theta <= 0.0f || out.theta >= f32c::kPi) {
         out.on_axis = 1;
         return out;
@@ -374,8 +404,6 @@ KP_HD CoeffsF riaf_coefficients_f(const ImageConsts& c, const RiafSampleF& p, fl
     // Faraday rotation / conversion (symphony_rho_QV), invariant rho * nu
     float rQ, rV;
     {
-        float r0, r1;
-        bessel_ratios_f(1.0f / te, r0, r1);
         const float omega0 = f32c::kOmega0PerB * b;
         const float wp2 = f32c::kWp2PerNe * ne;
         const float two_pi_nu = 2.0f * f32c::kPi * nu * 1e9f;
@@ -388,22 +416,26 @@ KP_HD CoeffsF riaf_coefficients_f(const ImageConsts& c, const RiafSampleF& p, fl
         float e12 = wp2 * omega0 * inv_w;
         e12 *= inv_w;
         e12 *= inv_w;
-        e12 *= r0 * shgm * cosv;
+        e12 *= p.r0 * shgm * cosv;
         rV = float(2.0 * 3.141592653589793 / f32c::kCL) * (nu * 1e9f) * e12 * (nu * 1e9f);
         if (p.on_axis) {
             o.rV = float(c.faraday_scale) * rV;
             return o;
         }
+        // every power of x from one LG2; 0.5 + 0.5 tanh(z) = 1 / (1 + e^-2z)
+        const float lx = log2f(x);
         const float exp_x_47 = expf(-x / 47.2f);
-        const float extraterm = (0.011f * exp_x_47 - 369.69342869090815f * powf(x + 1e-16f, -8.0f / 3.0f)) *
-                                (0.5f + 0.5f * tanhf((logf(x) - 4.787491742782046f) / 0.1f));
-        const float jffunc = 2.011f * expf(-powf(x, 1.035f) / 4.7f) - cosf(x / 2.0f) * expf(-powf(x, 1.2f) / 2.73f) -
-                             0.011f * exp_x_47 + extraterm;
+        const float z = (lx * 0.6931471805599453f - 4.787491742782046f) / 0.1f;
+        const float sigm = 1.0f / (1.0f + expf(-2.0f * z));
+        const float extraterm = (0.011f * exp_x_47 - 369.69342869090815f * pow2_of(-8.0f / 3.0f, lx)) * sigm;
+        // the cosine term is below 1e-13 of the sum beyond x = 40
+        const float cterm = x < 40.0f ? cosf(x / 2.0f) * expf(-pow2_of(1.2f, lx) / 2.73f) : 0.0f;
+        const float jffunc = 2.011f * expf(-pow2_of(1.035f, lx) / 4.7f) - cterm - 0.011f * exp_x_47 + extraterm;
         float e11 = jffunc * wp2 * omega0 * inv_w;
         e11 *= omega0 * inv_w;
         e11 *= inv_w;
         e11 *= inv_w;
-        e11 *= (r1 + 6.0f * te) * st * st;
+        e11 *= (p.r1 + 6.0f * te) * st * st;
         rQ = float(3.141592653589793 / f32c::kCL) * (nu * 1e9f) * e11 * (nu * 1e9f);
     }
     // emissivities, scaled by 2^E / nu^2 (nu^2 in Hz^2)
@@ -427,19 +459,16 @@ KP_HD CoeffsF riaf_coefficients_f(const ImageConsts& c, const RiafSampleF& p, fl
         const float nu_s = 2.0f / 9.0f * nu_c * st * te * te;
         const float x = fmaxf(nu * 1e9f / fmaxf(nu_s, 1e-30f), 1e-30f);
         const float pref = ne * f32c::kE2OverC * nu_c * f32c::kTerm1 * st;
-        const float x13 = cbrtf(x);
+        const float lx = log2f(x);
+        const float x13 = pow2_of(1.0f / 3.0f, lx);
         const float sqx = sqrtf(x), sqx13 = sqrtf(x13);
         const float ex13 = expf(-x13);
         const float sh = sqx + 1.8877486253633869933f * sqx13;
         jI = pref * (sh * sh) * ex13 * inv_nu2;
-        const float t2425 = powf(te, 24.0f / 25.0f);
-        const float term2 = (7.0f * t2425 + 35.0f) / (10.0f * t2425 + 75.0f);
-        const float shq = sqx + term2 * 1.8877486253633869933f * sqx13;
+        const float shq = sqx + p.qterm * 1.8877486253633869933f * sqx13;
         jQ = pref * (shq * shq) * ex13 * inv_nu2;
-        const float sin_shift = st * 0.4356824462767121f - ct * 0.9001004421765051f;
-        const float vt1 = (37.0f - 87.0f * sin_shift) / (100.0f * (te + 1.0f));
-        const float vt2 = powf(1.0f + (powf(te, 0.6f) / 25.0f + 0.7f) * powf(x, 0.36f), 5.0f / 3.0f);
-        jV = ne * f32c::kE2OverC * nu_c * vt1 * vt2 * ex13 * inv_nu2;
+        const float vt2 = pow2_of(5.0f / 3.0f, log2f(1.0f + p.vt2a * pow2_of(0.36f, lx)));
+        jV = ne * f32c::kE2OverC * nu_c * p.vt1 * vt2 * ex13 * inv_nu2;
     }
     // polarisation cap (thermal_synchrotron.hpp:575-588)
     const float jps = fmaxf(fabsf(jQ), fabsf(jV));
@@ -514,9 +543,14 @@ KP_HD void faraday_rotate_f(StokesF& s, const CoeffsF& c, float dl) {
     } else {
         const float inv = 1.0f / rn;
         const float nx = c.rQ * inv, ny = c.rU * inv, nz = c.rV * inv;
-        float st, ct;
-        kp_sincosf(theta, &st, &ct);
-        const float f = (nx * px + ny * py + nz * pz) * (1.0f - ct);
+        // half-angle forms: 1 - cos(theta) = 2 sin^2(theta/2) keeps its
+        // relative accuracy for small rotations
+        float sh, ch;
+        kp_sincosf(0.5f * theta, &sh, &ch);
+        const float st = 2.0f * sh * ch;
+        const float omc = 2.0f * sh * sh;
+        const float ct = 1.0f - omc;
+        const float f = (nx * px + ny * py + nz * pz) * omc;
         ox = px * ct + nx * f + (ny * pz - nz * py) * st;
         oy = py * ct + ny * f + (nz * px - nx * pz) * st;
         oz = pz * ct + nz * f + (nx * py - ny * px) * st;

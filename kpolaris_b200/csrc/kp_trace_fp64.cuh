@@ -122,6 +122,9 @@ __device__ __forceinline__ double vmaxabsdiff(const D4& a, const D4& b) {
 }
 
 // radiation_substep_count (pass_b.hpp:147-179) with requested_substeps = 1.
+// nsub is a power of two, so q / nsub > lim is exactly q > lim * nsub (both
+// sides are exact scalings): the doubling loops compare against lim * nsub
+// instead of dividing, with the reference's outcomes.
 template<class C>
 __device__ __forceinline__ int radiation_substep_count(const C& co, double h, double dls,
                                                        double max_rad_step, double max_rad_depth,
@@ -129,19 +132,19 @@ __device__ __forceinline__ int radiation_substep_count(const C& co, double h, do
     int nsub = 1;
     const double abs_h = abs_val(h);
     if (max_rad_step > 0.0)
-        while (abs_h / double(nsub) > max_rad_step && nsub < 4096) nsub *= 2;
+        while (abs_h > max_rad_step * double(nsub) && nsub < 4096) nsub *= 2;
     const double dl = abs_h * abs_val(dls);
     const double alim = max_abs_depth >= 0.0 ? max_abs_depth : max_rad_depth;
     if (alim > 0.0) {
         const double aQ = co.aQ, aU = co.aU, aV = co.aV;
         const double depth = (abs_val(double(co.aI)) + sqrt(aQ * aQ + aU * aU + aV * aV)) * dl;
-        while (depth / double(nsub) > alim && nsub < 4096) nsub *= 2;
+        while (depth > alim * double(nsub) && nsub < 4096) nsub *= 2;
     }
     const double flim = max_far_depth >= 0.0 ? max_far_depth : max_rad_depth;
     if (flim > 0.0) {
         const double rQ = co.rQ, rU = co.rU, rV = co.rV;
         const double depth = sqrt(rQ * rQ + rU * rU + rV * rV) * dl;
-        while (depth / double(nsub) > flim && nsub < 4096) nsub *= 2;
+        while (depth > flim * double(nsub) && nsub < 4096) nsub *= 2;
     }
     return nsub;
 }

@@ -34,6 +34,7 @@ int main() {
         p.has_chi = 1;
         p.cos2chi = 1.0f;
         p.sin2chi = 0.0f;
+        kp::riaf_sample_thermal_f(k, p);
         // scale the emission into FP32 range and undo it in double
         const double j0 = ne * 2.3e-19 * 2.8e6 * b / 3e10 / (nu * nu);
         const int e = int(std::floor(std::log2(1.0 / std::max(j0, 1e-300))));
