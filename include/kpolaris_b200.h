@@ -224,8 +224,9 @@ typedef struct kp_run_options {
     int device;          /* CUDA device ordinal */
     void* stream;        /* cudaStream_t, or NULL for the library's stream */
     int timing;          /* 1: print "timing <name> <seconds> s" lines like the reference */
-    /* Persistent-schedule tunables; 0 selects the default (occupancy-derived
-     * CTAs per SM; 128 threads per CTA, the only size the kernels take). */
+    /* Persistent-schedule tunables.  blocks_per_sm: 0 selects the
+     * occupancy-derived CTA count.  threads_per_block must be 0: the kernels
+     * fix it (128 far, 256 near). */
     int blocks_per_sm;
     int threads_per_block;
 } kp_run_options;

@@ -675,19 +675,20 @@ int kp_batch_riaf(const kp_riaf_job* jobs, int njobs, const kp_run_options* opti
     cudaEventRecord(dev->staging_free, stream);
     e = cudaMemsetAsync(dev->d_ctrl, 0, sizeof(WaveCtrl), stream);
     if (e != cudaSuccess) return cuda_error(e, "cudaMemsetAsync(wave counters)");
-    const int threads = opt.threads_per_block > 0 ? opt.threads_per_block : 128;
-    if (threads != 128)
-        return set_error(KP_ERR_INVALID, "threads_per_block must be 128 for the wavefront kernels");
+    if (opt.threads_per_block != 0)
+        return set_error(KP_ERR_INVALID, "threads_per_block is fixed by the wavefront kernels (%d far, %d near): pass 0",
+                         kFarThreads, kNearThreads);
     const bool mixed = opt.precision == KP_PRECISION_MIXED;
     int blocks[kPhases];
     for (int phase = 0; phase < kPhases; ++phase) {
         int per_sm = opt.blocks_per_sm;
         if (per_sm <= 0) {
-            per_sm = mixed ? wave_occupancy_mixed(phase, threads) : wave_occupancy_fp64(phase, nf_max, threads);
+            per_sm = mixed ? wave_occupancy_mixed(phase, wave_threads(phase))
+                           : wave_occupancy_fp64(phase, nf_max, wave_threads(phase));
             if (per_sm <= 0) per_sm = 1;
         }
         blocks[phase] = dev->sms * per_sm;
-        const long long needed = (total + threads - 1) / threads;
+        const long long needed = (total + wave_threads(phase) - 1) / wave_threads(phase);
         if (blocks[phase] > needed) blocks[phase] = int(needed);
     }
     WaveCtrl* ctrl = dev->d_ctrl;
@@ -709,8 +710,8 @@ int kp_batch_riaf(const kp_riaf_job* jobs, int njobs, const kp_run_options* opti
         W.budget = 0;
         W.status = &ctrl->status;
         W.job_done = nullptr;
-        return mixed ? launch_wave_mixed(phase, W, blocks[phase], threads, stream)
-                     : launch_wave_fp64(phase, W, nf_max, blocks[phase], threads, stream);
+        return mixed ? launch_wave_mixed(phase, W, blocks[phase], wave_threads(phase), stream)
+                     : launch_wave_fp64(phase, W, nf_max, blocks[phase], wave_threads(phase), stream);
     };
     // Rays leave the camera in the far phase, trace the radiating sphere in
     // near-A then near-B and return in the far phase of the next cycle; a few
@@ -742,7 +743,7 @@ int kp_batch_riaf(const kp_riaf_job* jobs, int njobs, const kp_run_options* opti
         stats->rays = total;
         stats->launches = launches;
         stats->blocks = blocks[kPhaseNearB];
-        stats->threads_per_block = threads;
+        stats->threads_per_block = kNearThreads;
         stats->device_output_bytes = opt.outputs_on_device ? 0 : scratch;
     }
     e = cudaEventSynchronize(dev->ev1);

@@ -14,12 +14,12 @@
 #include "kp_persistent.cuh"
 #include "kp_trace_fp64.cuh"
 
-// resident CTAs of 128 threads per SM the wavefront kernels are compiled for
+// resident CTAs per SM the wavefront kernels are compiled for
 #ifndef KP_FAR_MIN_BLOCKS
 #define KP_FAR_MIN_BLOCKS 2
 #endif
 #ifndef KP_NEAR_MIN_BLOCKS
-#define KP_NEAR_MIN_BLOCKS 2
+#define KP_NEAR_MIN_BLOCKS 1
 #endif
 
 namespace kp {
@@ -80,17 +80,17 @@ cudaError_t launch_image_fp64(const ImageConsts& c, const ImageOutPtrs& out, cud
 // NF (the unit is compiled without FMA contraction), so every instantiation
 // traces a ray bit-identically to the plain kernel.
 template<int NF>
-__global__ void __launch_bounds__(128, KP_FAR_MIN_BLOCKS) wave_far_fp64(const WaveDesc W) {
+__global__ void __launch_bounds__(kFarThreads, KP_FAR_MIN_BLOCKS) wave_far_fp64(const WaveDesc W) {
     persistent_body<PolicyFP64, NF, kPhaseFar>(W);
 }
 
 template<int NF>
-__global__ void __launch_bounds__(128, KP_NEAR_MIN_BLOCKS) wave_near_a_fp64(const WaveDesc W) {
+__global__ void __launch_bounds__(kNearThreads, KP_NEAR_MIN_BLOCKS) wave_near_a_fp64(const WaveDesc W) {
     persistent_body<PolicyFP64, NF, kPhaseNearA>(W);
 }
 
 template<int NF>
-__global__ void __launch_bounds__(128, KP_NEAR_MIN_BLOCKS) wave_near_b_fp64(const WaveDesc W) {
+__global__ void __launch_bounds__(kNearThreads, KP_NEAR_MIN_BLOCKS) wave_near_b_fp64(const WaveDesc W) {
     persistent_body<PolicyFP64, NF, kPhaseNearB>(W);
 }
 

@@ -9,25 +9,25 @@
 #include "kp_launch.h"
 #include "kp_persistent.cuh"
 
-// resident CTAs of 128 threads per SM the wavefront kernels are compiled for
+// resident CTAs per SM the wavefront kernels are compiled for
 #ifndef KP_FAR_MIN_BLOCKS
 #define KP_FAR_MIN_BLOCKS 2
 #endif
 #ifndef KP_NEAR_MIN_BLOCKS
-#define KP_NEAR_MIN_BLOCKS 2
+#define KP_NEAR_MIN_BLOCKS 1
 #endif
 
 namespace kp {
 
-__global__ void __launch_bounds__(128, KP_FAR_MIN_BLOCKS) wave_far_mixed(const WaveDesc W) {
+__global__ void __launch_bounds__(kFarThreads, KP_FAR_MIN_BLOCKS) wave_far_mixed(const WaveDesc W) {
     persistent_body<PolicyMixed, kMaxFreq, kPhaseFar>(W);
 }
 
-__global__ void __launch_bounds__(128, KP_NEAR_MIN_BLOCKS) wave_near_a_mixed(const WaveDesc W) {
+__global__ void __launch_bounds__(kNearThreads, KP_NEAR_MIN_BLOCKS) wave_near_a_mixed(const WaveDesc W) {
     persistent_body<PolicyMixed, kMaxFreq, kPhaseNearA>(W);
 }
 
-__global__ void __launch_bounds__(128, KP_NEAR_MIN_BLOCKS) wave_near_b_mixed(const WaveDesc W) {
+__global__ void __launch_bounds__(kNearThreads, KP_NEAR_MIN_BLOCKS) wave_near_b_mixed(const WaveDesc W) {
     persistent_body<PolicyMixed, kMaxFreq, kPhaseNearB>(W);
 }
 

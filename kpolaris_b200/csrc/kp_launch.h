@@ -25,4 +25,11 @@ cudaError_t launch_wave_mixed(int phase, const WaveDesc& W, int blocks, int thre
 int wave_occupancy_fp64(int phase, int nf_max, int threads);
 int wave_occupancy_mixed(int phase, int threads);
 
+// Threads per CTA of each phase kernel (its __launch_bounds__): the far
+// kernel runs two CTAs of 128 per SM, the near kernels one CTA of 256, so
+// that every resident warp of an SM steps through the same code region.
+constexpr int kFarThreads = 128;
+constexpr int kNearThreads = 256;
+inline int wave_threads(int phase) { return phase == kPhaseFar ? kFarThreads : kNearThreads; }
+
 }  // namespace kp

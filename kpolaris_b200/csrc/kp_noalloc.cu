@@ -89,8 +89,9 @@ extern "C" int kp_batch_riaf_noalloc(const kp_riaf_job* jobs, int njobs, const k
         return set_error(KP_ERR_INVALID, "unknown precision %d", opt.precision);
     if (opt.integrator != KP_INTEGRATOR_STEP_DOUBLING_RK4 && opt.integrator != KP_INTEGRATOR_CASH_KARP)
         return set_error(KP_ERR_INVALID, "unknown integrator %d", opt.integrator);
-    const int threads = opt.threads_per_block > 0 ? opt.threads_per_block : 128;
-    if (threads != 128) return set_error(KP_ERR_INVALID, "threads_per_block must be 128 for the wavefront kernels");
+    if (opt.threads_per_block != 0)
+        return set_error(KP_ERR_INVALID, "threads_per_block is fixed by the wavefront kernels (%d far, %d near): pass 0",
+                         kFarThreads, kNearThreads);
     long long total = 0;
     int nf_max = 1;
     for (int i = 0; i < njobs; ++i) {
@@ -153,11 +154,12 @@ extern "C" int kp_batch_riaf_noalloc(const kp_riaf_job* jobs, int njobs, const k
     for (int phase = 0; phase < kPhases; ++phase) {
         int per_sm = opt.blocks_per_sm;
         if (per_sm <= 0) {
-            per_sm = mixed ? wave_occupancy_mixed(phase, threads) : wave_occupancy_fp64(phase, nf_max, threads);
+            per_sm = mixed ? wave_occupancy_mixed(phase, wave_threads(phase))
+                           : wave_occupancy_fp64(phase, nf_max, wave_threads(phase));
             if (per_sm <= 0) per_sm = 1;
         }
         blocks[phase] = std::max(1, sms) * per_sm;
-        const long long needed = (total + threads - 1) / threads;
+        const long long needed = (total + wave_threads(phase) - 1) / wave_threads(phase);
         if (blocks[phase] > needed) blocks[phase] = int(needed);
     }
     for (int cycle = 0; cycle < kCycles; ++cycle) {
@@ -179,8 +181,8 @@ extern "C" int kp_batch_riaf_noalloc(const kp_riaf_job* jobs, int njobs, const k
             W.budget = 0;
             W.status = &S->ctrl.status;
             W.job_done = nullptr;
-            e = mixed ? launch_wave_mixed(phase, W, blocks[phase], threads, stream)
-                      : launch_wave_fp64(phase, W, nf_max, blocks[phase], threads, stream);
+            e = mixed ? launch_wave_mixed(phase, W, blocks[phase], wave_threads(phase), stream)
+                      : launch_wave_fp64(phase, W, nf_max, blocks[phase], wave_threads(phase), stream);
             if (e != cudaSuccess) return cuda_error(e, "wavefront kernel launch");
         }
         unsigned left[kPhases] = {0, 0, 0};

@@ -205,7 +205,9 @@ __device__ __forceinline__ void persistent_body(const WaveDesc& W) {
             }
         }
         const bool active = st.mode != kIdle;
-        if (!__any_sync(FULL, active)) break;
+        // The block leaves the loop together, so the barrier below is
+        // reached by every thread of the block in every iteration.
+        if (!__syncthreads_or(active)) break;
 
         // ---------------------------------------------- control before the job
         int dest = -1;  // phase the ray is handed to (PHASE itself: next round)
@@ -322,6 +324,11 @@ __device__ __forceinline__ void persistent_body(const WaveDesc& W) {
                 atomicExch(W.status, 2);
             }
         }
+
+        // The warps of a block finish their RK jobs together and run the
+        // control and radiation code together: one code region at a time
+        // per SM keeps it in the instruction cache.
+        __syncthreads();
 
         // ----------------------------------------------- control after the job
         if (kPassA && run && st.mode == kAStep) {
