@@ -326,6 +326,71 @@ typedef struct kp_batch_stats {
 int kp_batch_riaf(const kp_riaf_job* jobs, int njobs, const kp_run_options* options,
                   kp_batch_stats* stats);
 
+/*
+ * Serving loop.  A server owns one GPU and a device-owner thread that runs
+ * the wavefront engine in bounded ticks: each tick admits waiting jobs whose
+ * HBM footprint fits (ray records + device outputs), seeds their rays, and
+ * runs one (far, near-A, near-B) cycle in which every lane advances at most
+ * `tick_budget` RK jobs before parking its ray.  Jobs that arrive while
+ * others are on the GPU join the next tick, so their work shares launches
+ * with the jobs in flight (continuous batching); a ray resumes from its
+ * record with exactly the arithmetic it would have had, so a job's result is
+ * the same alone and in any mix.  Results are copied into the job's host
+ * buffers (kp_riaf_job.out) when its last ray finishes.  No counterpart in
+ * the reference (closest: run_image_batch_metric, src/image/batch_driver.hpp:127-187).
+ */
+typedef struct kp_server kp_server;
+
+typedef struct kp_server_config {
+    int device;
+    int precision;           /* kp_precision */
+    int integrator;          /* kp_integrator */
+    long long max_rays;      /* ray records resident at once (472 B of HBM each) */
+    size_t output_bytes;     /* device output arena (kp_image_output_bytes per job) */
+    int max_jobs;            /* jobs in flight at once */
+    int tick_budget;         /* RK jobs per lane per launch */
+} kp_server_config;
+
+/* Job states reported by kp_server_poll. */
+typedef enum kp_job_state {
+    KP_JOB_PENDING = 0,      /* waiting for admission */
+    KP_JOB_RUNNING = 1,      /* rays on the device */
+    KP_JOB_DONE = 2,         /* outputs written to the job's buffers */
+    KP_JOB_CANCELLED = 3,
+    KP_JOB_FAILED = 4
+} kp_job_state;
+
+typedef struct kp_server_stats {
+    long long submitted, completed, cancelled, failed;
+    long long ticks;
+    long long max_inflight_rays;  /* peak ray records in use */
+    int max_inflight_jobs;
+    double wall_seconds;          /* since the server was created */
+    double busy_seconds;          /* ticks with work on the device */
+    double latency_p50, latency_p99, latency_max;  /* submit -> done, seconds */
+    double queue_p50;             /* submit -> admission, seconds */
+} kp_server_stats;
+
+/* Defaults: device 0, mixed precision, step-doubling RK4, 4 Mi rays
+ * (2 GB of records), 1 GiB of outputs, 64 jobs, budget 128. */
+void kp_default_server_config(kp_server_config* cfg);
+int kp_server_create(const kp_server_config* cfg, kp_server** out);
+/* Validates the job (as kp_batch_riaf does) and queues it; *ticket names it.
+ * A job whose footprint exceeds the whole server fails with KP_ERR_INVALID.
+ * The job's host output buffers must stay valid until it is done, cancelled
+ * or failed. */
+int kp_server_submit(kp_server* s, const kp_riaf_job* job, unsigned long long* ticket);
+int kp_server_poll(kp_server* s, unsigned long long ticket, int* state);
+/* Waits until the job is done, cancelled or failed, or `timeout_seconds`
+ * pass (KP_ERR_TIMEOUT).  Returns the job's failure status if it failed. */
+int kp_server_wait(kp_server* s, unsigned long long ticket, double timeout_seconds);
+/* A pending job is dropped at once; a running job finishes on the device and
+ * its outputs are not written. */
+int kp_server_cancel(kp_server* s, unsigned long long ticket);
+int kp_server_get_stats(kp_server* s, kp_server_stats* out);
+/* Stops after the jobs in flight finish (pending jobs are cancelled). */
+int kp_server_destroy(kp_server* s);
+
 /* Limits of kp_batch_riaf_noalloc's static device scratch. */
 #define KP_NOALLOC_MAX_RAYS 65536
 #define KP_NOALLOC_MAX_JOBS 16

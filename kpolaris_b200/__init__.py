@@ -20,7 +20,8 @@ from ._abi import (ImageHostData, PassAParams, RIAFModel, RunOptions, default_pa
 __all__ = [
     "ImageHostData", "PassAParams", "RIAFModel", "RunOptions", "KPolarisError",
     "default_pass_a_params", "default_riaf_model", "default_run_options", "library",
-    "run_riaf_image", "run_riaf_multifrequency_image", "image_riaf",
+    "run_riaf_image", "run_riaf_multifrequency_image", "image_riaf", "batch_riaf", "Server",
+    "default_server_config",
 ]
 
 LIB_PATH = Path(os.environ.get("KPOLARIS_B200_LIB") or Path(__file__).resolve().parent / "lib" / "libkpolaris_b200.so")
@@ -64,6 +65,14 @@ def library() -> C.CDLL:
     L.kp_default_run_options.argtypes = [C.POINTER(RunOptions)]
     L.kp_default_pass_a_params.argtypes = [C.POINTER(PassAParams)]
     L.kp_default_riaf_model.argtypes = [C.POINTER(RIAFModel)]
+    L.kp_default_server_config.argtypes = [C.POINTER(_abi.ServerConfig)]
+    L.kp_server_create.argtypes = [C.POINTER(_abi.ServerConfig), C.POINTER(C.c_void_p)]
+    L.kp_server_submit.argtypes = [C.c_void_p, C.POINTER(_abi.RiafJob), C.POINTER(C.c_ulonglong)]
+    L.kp_server_poll.argtypes = [C.c_void_p, C.c_ulonglong, C.POINTER(C.c_int)]
+    L.kp_server_wait.argtypes = [C.c_void_p, C.c_ulonglong, C.c_double]
+    L.kp_server_cancel.argtypes = [C.c_void_p, C.c_ulonglong]
+    L.kp_server_get_stats.argtypes = [C.c_void_p, C.POINTER(_abi.ServerStats)]
+    L.kp_server_destroy.argtypes = [C.c_void_p]
     if L.kp_abi_version() != _abi.KP_ABI_VERSION:
         raise ImportError("libkpolaris_b200.so ABI version mismatch")
     _lib = L
@@ -136,6 +145,84 @@ def batch_riaf(jobs, *, outs=None, precision=_abi.PRECISION_MIXED, stats=None, *
     st = stats if stats is not None else _abi.BatchStats()
     check(L.kp_batch_riaf(arr, len(jobs), C.byref(opt), C.byref(st)))
     return results
+
+
+def default_server_config() -> _abi.ServerConfig:
+    c = _abi.ServerConfig()
+    library().kp_default_server_config(C.byref(c))
+    return c
+
+
+class Server:
+    """The serving loop (kp_server_*): jobs submitted at any time share the
+    GPU in bounded ticks; results land in each job's host buffers.
+
+        with Server(max_rays=1 << 20) as srv:
+            t = srv.submit(params, model, freqs)
+            srv.wait(t)
+            image = srv.result(t)
+    """
+
+    def __init__(self, config: _abi.ServerConfig | None = None, **fields):
+        L = library()
+        cfg = config if config is not None else default_server_config()
+        for k, v in fields.items():
+            setattr(cfg, k, v)
+        h = C.c_void_p()
+        check(L.kp_server_create(C.byref(cfg), C.byref(h)))
+        self._h = h
+        self._keep = {}
+
+    def submit(self, params: PassAParams, model: RIAFModel, frequencies=None, *,
+               out: ImageHostData | None = None) -> int:
+        """Queues one image; returns its ticket.  `out` (allocated if None)
+        receives the result and is kept alive until the job is collected."""
+        freqs = list(frequencies) if frequencies is not None else [model.freq_cgs]
+        npix = params.camera.nx * params.camera.ny
+        res = out if out is not None else ImageHostData.allocate(npix, len(freqs))
+        job = _abi.RiafJob()
+        job.params = params
+        job.model = model
+        for f, v in enumerate(freqs[:_abi.KP_MAX_FREQUENCIES]):
+            job.frequencies[f] = v
+        job.nfreq = len(freqs)
+        job.radiation_substeps = 1
+        job.out = res.as_struct()
+        t = C.c_ulonglong(0)
+        check(library().kp_server_submit(self._h, C.byref(job), C.byref(t)))
+        self._keep[t.value] = res
+        return t.value
+
+    def poll(self, ticket: int) -> int:
+        st = C.c_int(0)
+        check(library().kp_server_poll(self._h, ticket, C.byref(st)))
+        return st.value
+
+    def wait(self, ticket: int, timeout: float = 600.0) -> None:
+        check(library().kp_server_wait(self._h, ticket, float(timeout)))
+
+    def cancel(self, ticket: int) -> None:
+        check(library().kp_server_cancel(self._h, ticket))
+
+    def result(self, ticket: int) -> ImageHostData:
+        """The job's output buffers (complete once wait() returned)."""
+        return self._keep.pop(ticket)
+
+    def stats(self) -> _abi.ServerStats:
+        st = _abi.ServerStats()
+        check(library().kp_server_get_stats(self._h, C.byref(st)))
+        return st
+
+    def close(self) -> None:
+        if self._h:
+            library().kp_server_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 def measure_fma_peak(device: int = 0, fp64: bool = True) -> float:

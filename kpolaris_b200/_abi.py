@@ -151,6 +151,26 @@ class BatchStats(C.Structure):
     ]
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [
+        ("device", C.c_int), ("precision", C.c_int), ("integrator", C.c_int),
+        ("max_rays", C.c_longlong), ("output_bytes", C.c_size_t), ("max_jobs", C.c_int),
+        ("tick_budget", C.c_int),
+    ]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [
+        ("submitted", C.c_longlong), ("completed", C.c_longlong), ("cancelled", C.c_longlong),
+        ("failed", C.c_longlong), ("ticks", C.c_longlong), ("max_inflight_rays", C.c_longlong),
+        ("max_inflight_jobs", C.c_int), ("wall_seconds", C.c_double), ("busy_seconds", C.c_double),
+        ("latency_p50", C.c_double), ("latency_p99", C.c_double), ("latency_max", C.c_double),
+        ("queue_p50", C.c_double),
+    ]
+
+
+JOB_PENDING, JOB_RUNNING, JOB_DONE, JOB_CANCELLED, JOB_FAILED = 0, 1, 2, 3, 4
+
 IMAGE_FIELDS = ("image_i", "image_q", "image_u", "image_v")
 DIAG_FIELDS = ("closure_x", "closure_k", "final_null", "frame_error", "det_r",
                "overlap_r11", "overlap_r12", "overlap_r21", "overlap_r22",

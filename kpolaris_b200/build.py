@@ -32,6 +32,7 @@ UNITS = {
     "kp_kernels_mixed.cu": ["--fmad=true"],
     "kp_capi.cu": ["--fmad=false"],
     "kp_noalloc.cu": ["--fmad=false"],
+    "kp_server.cu": ["--fmad=false"],
     "kp_peak.cu": [],
 }
 

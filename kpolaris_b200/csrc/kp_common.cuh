@@ -148,6 +148,14 @@ struct alignas(16) RayRecord {
 // phases through id queues.
 enum Phase : int { kPhaseFar = 0, kPhaseNearA = 1, kPhaseNearB = 2, kPhases = 3 };
 
+// A newly admitted job of the serving loop: its slot in the job table, the
+// first of its contiguous ray ids and its pixel count.
+struct SeedEntry {
+    int slot;
+    int npix;
+    long long ray_base;
+};
+
 // Device-side launch description (kernel parameter).
 struct WaveDesc {
     const JobDesc* jobs;           // device array, ordered by ray_begin

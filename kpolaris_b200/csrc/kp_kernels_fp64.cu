@@ -109,6 +109,21 @@ cudaError_t launch_wave_fp64(int phase, const WaveDesc& W, int nf_max, int block
     return cudaLaunchKernel(fn, dim3(blocks), dim3(threads), args, 0, stream);
 }
 
+__global__ void __launch_bounds__(128) seed_fp64(const JobDesc* jobs, const SeedEntry* entries,
+                                                const long long* prefix, int nentries, RayRecord* pool,
+                                                unsigned* far_ids, unsigned* far_count) {
+    seed_body(jobs, entries, prefix, nentries, pool, far_ids, far_count);
+}
+
+cudaError_t launch_seed_fp64(const JobDesc* jobs, const SeedEntry* entries, const long long* prefix, int nentries,
+                             long long total, RayRecord* pool, unsigned* far_ids, unsigned* far_count,
+                             cudaStream_t stream) {
+    if (total <= 0) return cudaSuccess;
+    const int grid = int((total + 127) / 128);
+    seed_fp64<<<grid, 128, 0, stream>>>(jobs, entries, prefix, nentries, pool, far_ids, far_count);
+    return cudaGetLastError();
+}
+
 int wave_occupancy_fp64(int phase, int nf_max, int threads) {
     if (phase < 0 || phase >= kPhases) return 0;
     const void* fn = nf_max == 1 ? wave_kernel_fp64<1>(phase) : wave_kernel_fp64<kMaxFreq>(phase);

@@ -43,6 +43,21 @@ cudaError_t launch_wave_mixed(int phase, const WaveDesc& W, int blocks, int thre
     return cudaLaunchKernel(wave_kernel_mixed(phase), dim3(blocks), dim3(threads), args, 0, stream);
 }
 
+__global__ void __launch_bounds__(128) seed_mixed(const JobDesc* jobs, const SeedEntry* entries,
+                                                 const long long* prefix, int nentries, RayRecord* pool,
+                                                 unsigned* far_ids, unsigned* far_count) {
+    seed_body(jobs, entries, prefix, nentries, pool, far_ids, far_count);
+}
+
+cudaError_t launch_seed_mixed(const JobDesc* jobs, const SeedEntry* entries, const long long* prefix, int nentries,
+                              long long total, RayRecord* pool, unsigned* far_ids, unsigned* far_count,
+                              cudaStream_t stream) {
+    if (total <= 0) return cudaSuccess;
+    const int grid = int((total + 127) / 128);
+    seed_mixed<<<grid, 128, 0, stream>>>(jobs, entries, prefix, nentries, pool, far_ids, far_count);
+    return cudaGetLastError();
+}
+
 int wave_occupancy_mixed(int phase, int threads) {
     if (phase < 0 || phase >= kPhases) return 0;
     int n = 0;

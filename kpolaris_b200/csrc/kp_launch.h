@@ -25,6 +25,16 @@ cudaError_t launch_wave_mixed(int phase, const WaveDesc& W, int blocks, int thre
 int wave_occupancy_fp64(int phase, int nf_max, int threads);
 int wave_occupancy_mixed(int phase, int threads);
 
+// Seed kernels of the serving loop (same translation unit, hence the same
+// camera-ray arithmetic, as the policy's phase kernels): initial records of
+// the rays of newly admitted jobs, appended to the far queue.
+cudaError_t launch_seed_fp64(const JobDesc* jobs, const SeedEntry* entries, const long long* prefix, int nentries,
+                             long long total, RayRecord* pool, unsigned* far_ids, unsigned* far_count,
+                             cudaStream_t stream);
+cudaError_t launch_seed_mixed(const JobDesc* jobs, const SeedEntry* entries, const long long* prefix, int nentries,
+                              long long total, RayRecord* pool, unsigned* far_ids, unsigned* far_count,
+                              cudaStream_t stream);
+
 // Threads per CTA of each phase kernel (its __launch_bounds__): the far
 // kernel runs two CTAs of 128 per SM, the near kernels one CTA of 256, so
 // that every resident warp of an SM steps through the same code region.

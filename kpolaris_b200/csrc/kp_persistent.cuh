@@ -125,6 +125,48 @@ __device__ __forceinline__ void queue_push(unsigned* ids, unsigned* count, bool 
     if (push) ids[base + __popc(m & ((1u << lane) - 1u))] = id;
 }
 
+// Initial control state of a camera ray at the top of pass A
+// (pass_b.hpp:786-792).
+__device__ __forceinline__ void start_ray(LaneState& st, Ray& S, const JobDesc* J, int job, int pixel) {
+    memset(&st, 0, sizeof(st));
+    st.job = job;
+    st.pixel = pixel;
+    S = camera_ray(J->c, J->frame, pixel);
+    st.reason = kMaxSteps;
+    st.h_current = -abs_val(J->c.step);
+    st.mode = kAStep;
+    st.rk_kind = -1;
+}
+
+// Seeds the rays of newly admitted jobs: one thread per ray writes the ray's
+// initial record (pass-A loop top) and appends its id to the far queue.
+// entries: (job slot, first ray id, pixel count) with prefix sums of the
+// counts in `prefix` (nentries + 1 values).
+__device__ __forceinline__ void seed_body(const JobDesc* jobs, const SeedEntry* entries, const long long* prefix,
+                                          int nentries, RayRecord* pool, unsigned* far_ids,
+                                          unsigned* far_count) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool live = i < prefix[nentries];
+    unsigned id = 0;
+    if (live) {
+        int lo = 0, hi = nentries - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (prefix[mid] <= i) lo = mid; else hi = mid - 1;
+        }
+        const SeedEntry e = entries[lo];
+        const int pixel = int(i - prefix[lo]);
+        id = unsigned(e.ray_base + pixel);
+        LaneState st;
+        Ray S;
+        start_ray(st, S, &jobs[e.slot], e.slot, pixel);
+        RayRecord& rec = pool[id];
+        rec.S = S;
+        memcpy(rec.st, &st, sizeof(LaneState));
+    }
+    queue_push(far_ids, far_count, live, id);
+}
+
 // Phase that advances a ray from the top of its pass-A or pass-B loop.
 __device__ __forceinline__ int phase_of(const ImageConsts& c, int in_b, double r_bl) {
     if (r_bl > c.fp32_radius) return kPhaseFar;
@@ -159,6 +201,7 @@ __device__ __forceinline__ void persistent_body(const WaveDesc& W) {
     while (true) {
         // ------------------------------------------------------------ claim
         const bool want = !exhausted && st.mode == kIdle;
+        bool forward = false;
         const unsigned need = __ballot_sync(FULL, want);
         if (need) {
             unsigned long long base = 0;
@@ -178,21 +221,12 @@ __device__ __forceinline__ void persistent_body(const WaveDesc& W) {
                         if (W.jobs[mid].ray_begin <= id) lo = mid; else hi = mid - 1;
                     }
                     my_id = unsigned(id);
-                    st.job = lo;
                     J = &W.jobs[lo];
-                    st.pixel = int(id - J->ray_begin);
-                    S = camera_ray(J->c, J->frame, st.pixel);
-                    st.reason = kMaxSteps;
-                    st.pa_steps = 0;
-                    st.n = 0;
-                    st.entered = 0;
-                    st.inside = 0;
-                    st.in_b = 0;
-                    st.steps = 0;
-                    st.reached = 0;
-                    st.h_current = -abs_val(J->c.step);
-                    st.mode = kAStep;
-                    st.rk_kind = -1;
+                    start_ray(st, S, J, lo, int(id - J->ray_begin));
+                } else if (W.budget > 0 && lane_jobs >= W.budget) {
+                    // past the budget: hand the id on untouched (below)
+                    my_id = W.in_ids[k - nfresh];
+                    forward = true;
                 } else {
                     // a parked ray: resume from its record
                     my_id = W.in_ids[k - nfresh];
@@ -204,6 +238,7 @@ __device__ __forceinline__ void persistent_body(const WaveDesc& W) {
                 }
             }
         }
+        queue_push(W.out_ids[PHASE], W.out_count[PHASE], forward, my_id);
         const bool active = st.mode != kIdle;
         // The block leaves the loop together, so the barrier below is
         // reached by every thread of the block in every iteration.
