@@ -41,6 +41,7 @@ sys.path.insert(0, str(ROOT))
 METRIC = "256\u00b2 images/s & p50/p99 latency, mixed batched vs plain FP64, \u22641e-4 flux err"
 UNIT = "images/s"
 FLOP_TABLE = ROOT / "profiles" / "flop_counts.json"
+TRAFFIC_TABLE = ROOT / "profiles" / "ncu_traffic.json"
 
 
 def parse():
@@ -53,6 +54,9 @@ def parse():
     ap.add_argument("--n", type=int, default=256)
     ap.add_argument("--batch", type=int, default=8, help="images per step of the mixed path")
     ap.add_argument("--plain-steps", type=int, default=3, help="timed images of the plain FP64 kernel")
+    ap.add_argument("--serve-requests", type=int, default=48, help="requests of the serving trace (0: skip)")
+    ap.add_argument("--serve-rate", type=float, default=20.0, help="Poisson arrival rate of the trace, 1/s")
+    ap.add_argument("--serve-plain", type=int, default=1, help="replay the trace on the plain FP64 kernel too")
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="target CPU time of the bounded CPU-baseline sample")
     return ap.parse_args()
@@ -247,6 +251,85 @@ def integrated_stokes(i, q, u):
     return out
 
 
+# ---------------------------------------------------------------- serving
+def serving_trace(n_requests, rate, seed=2026):
+    """Seeded Poisson arrivals of RIAF image requests: resolution 64^2, 128^2
+    or 256^2, 1-4 frequencies from {86, 230, 345, 690} GHz, spin U[0, 0.99],
+    inclination U[10, 170] deg, the adaptive 4-frequency controls."""
+    import numpy as np
+
+    from kpolaris_b200 import configs
+
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    trace = []
+    for _ in range(n_requests):
+        t += rng.exponential(1.0 / rate)
+        n = int(rng.choice([64, 128, 256]))
+        nf = int(rng.integers(1, 5))
+        freqs = sorted(rng.choice(configs.CONFIG2_FREQS, size=nf, replace=False).tolist())
+        p = configs.riaf_params(n, n, spin=float(rng.uniform(0.0, 0.99)),
+                                inclination_deg=float(rng.uniform(10.0, 170.0)), step=0.025, adaptive=1,
+                                max_steps=400000, adaptive_tolerance=1e-8, min_step=1e-10, max_step=2.0,
+                                max_radiation_step=2.0, max_radiation_depth=1.0, max_absorption_depth=1.0,
+                                max_faraday_depth=4.0)
+        trace.append((t, p, configs.riaf_model(), freqs))
+    return trace
+
+
+def serve_mixed(trace, device):
+    """Replays the trace against the serving loop in real time."""
+    import kpolaris_b200 as kp
+
+    with kp.Server(device=device, max_rays=1 << 21) as srv:
+        # warm the kernels and the server's buffers
+        w = srv.submit(*trace[0][1:])
+        srv.wait(w, timeout=120.0)
+        srv.result(w)
+        lat = []
+        t0 = time.perf_counter()
+        tickets = []
+        for (t, p, m, f) in trace:
+            delay = t - (time.perf_counter() - t0)
+            if delay > 0:
+                time.sleep(delay)
+            tickets.append((srv.submit(p, m, f), t0 + t))
+        for tk, t_arr in tickets:
+            srv.wait(tk, timeout=300.0)
+        t_end = time.perf_counter()
+        st = srv.stats()
+    # per-request latency from the server's own clock (submit -> done)
+    return {"images_per_s": len(trace) / (t_end - t0), "p50_s": st.latency_p50, "p99_s": st.latency_p99,
+            "max_s": st.latency_max, "queue_p50_s": st.queue_p50,
+            "max_inflight_jobs": st.max_inflight_jobs, "ticks": st.ticks - 1}
+
+
+def serve_plain(trace, device):
+    """The same trace through a FIFO of plain FP64 one-image launches: each
+    request starts when it has arrived and the previous one has finished."""
+    import numpy as np
+
+    import kpolaris_b200 as kp
+
+    kp.image_riaf(*trace[0][1:], device=device)
+    finish = 0.0
+    lat = []
+    busy = 0.0
+    for (t, p, m, f) in trace:
+        t_a = time.perf_counter()
+        kp.image_riaf(p, m, f, device=device)
+        svc = time.perf_counter() - t_a
+        busy += svc
+        finish = max(finish, t) + svc
+        lat.append(finish - t)
+    return {"images_per_s": len(trace) / finish, "p50_s": float(np.percentile(lat, 50)),
+            "p99_s": float(np.percentile(lat, 99)), "max_s": float(max(lat)), "busy_s": busy}
+
+
+def progress(msg):
+    print(f"[bench] {msg}", file=sys.stderr, flush=True)
+
+
 def ours_arm(args):
     import numpy as np
     import torch
@@ -309,9 +392,11 @@ def ours_arm(args):
             if record:
                 launches[0] += 1
 
+    progress("warm-up")
     for _ in range(max(3, args.warmup)):
         step()
     torch.cuda.synchronize()
+    progress("timed steps")
     peak64 = C.c_double(0.0)
     kp.check(lib.kp_measure_fma_peak(local, 1, C.byref(peak64)))
     peak32 = C.c_double(0.0)
@@ -349,6 +434,7 @@ def ours_arm(args):
         ms = float(t.item())
     value = world * batch * 1000.0 / ms
 
+    progress("plain FP64 kernel")
     # ---- plain FP64 one-image-per-launch kernel, same run, same timing rules
     plain_out = device_outputs(torch, npix, nfreq, dev)
     opt_plain = kp._options(precision=_abi.PRECISION_FP64, schedule=_abi.SCHEDULE_PER_PIXEL, device=local)
@@ -381,6 +467,7 @@ def ours_arm(args):
     evpa_err = [abs((g[1] - r[1] + 90.0) % 180.0 - 90.0) for g, r in zip(got_int, ref_int)]
     reason_match = float(np.mean(outs[0][1][2][2].cpu().numpy() == plain_out[1][2][2].cpu().numpy()))
 
+    progress("e2e")
     # ---- e2e: the same batch through the public API with host buffers
     host = [_abi.ImageHostData.allocate(npix, nfreq) for _ in range(batch)]
     job_list = [(params, model, freqs)] * batch
@@ -423,9 +510,13 @@ def ours_arm(args):
         bound64 = f64 / peak64.value >= f32 / peak32.value
         achieved = batch * (f64 if bound64 else f32) / sec / 1e12
         peak = peak64.value if bound64 else peak32.value
+        traffic = None
+        if TRAFFIC_TABLE.exists() and args.n == 256 and batch == 8:
+            t = json.loads(TRAFFIC_TABLE.read_text()).get(f"wave_{name}_mixed")
+            traffic = t["bytes_per_bench_launch"] if t else None
         roof = {"bound": "fp64" if bound64 else "fp32", "kernel": f"wave_{name}_mixed",
                 "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                "traffic": None,
+                "traffic": traffic, "traffic_unit": "bytes per launch (ncu, scaled; see profiles/)",
                 "peak_source": "measured FMA throughput of this GPU (kp_measure_fma_peak), of measured",
                 "flops_source": "algorithmic op count of the reference algorithm per phase "
                                 "(profiles/flop_counts.json) x images per launch"}
@@ -435,6 +526,18 @@ def ours_arm(args):
                 "peak": peak64.value, "unit": "TFLOP/s", "frac": achieved / peak64.value, "traffic": None,
                 "peak_source": "measured FP64 FMA throughput of this GPU (kp_measure_fma_peak), of measured",
                 "flops_source": "algorithmic FP64 op count of the reference algorithm"}
+
+    serving = None
+    if mixed and args.serve_requests > 0:
+        progress("serving trace")
+        trace = serving_trace(args.serve_requests, args.serve_rate)
+        serving = {"workload": "Poisson arrivals of RIAF requests: 64^2/128^2/256^2, 1-4 frequencies, "
+                               "spin U[0,0.99], inclination U[10,170] deg, adaptive RK4",
+                   "requests": len(trace), "rate_per_s": args.serve_rate,
+                   "mixed_batched": serve_mixed(trace, local)}
+        if args.serve_plain:
+            progress("serving trace on the plain FP64 kernel")
+            serving["plain_fp64"] = serve_plain(trace, local)
 
     cpu = None
     if rank == 0:
@@ -463,6 +566,10 @@ def ours_arm(args):
                                  "reason_agreement": reason_match,
                                  "frequencies_ghz": [f * 1e-9 for f in freqs]},
             "step_latency_ms": {"p50": float(np.percentile(srt, 50)), "p99": float(np.percentile(srt, 99))},
+            "latency_ms": ({"p50": serving["mixed_batched"]["p50_s"] * 1e3,
+                            "p99": serving["mixed_batched"]["p99_s"] * 1e3, "source": "serving trace"}
+                           if serving else None),
+            "serving": serving,
             "rays_per_s": value * npix,
             "geodesic_steps_per_s": value * steps_per_image,
             "phases": phases, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,

@@ -388,7 +388,9 @@ int kp_server_wait(kp_server* s, unsigned long long ticket, double timeout_secon
  * its outputs are not written. */
 int kp_server_cancel(kp_server* s, unsigned long long ticket);
 int kp_server_get_stats(kp_server* s, kp_server_stats* out);
-/* Stops after the jobs in flight finish (pending jobs are cancelled). */
+/* Stops after the tick that is running: pending jobs and jobs still in
+ * flight end as cancelled (their outputs are not written), then the
+ * server's device memory is released. */
 int kp_server_destroy(kp_server* s);
 
 /* Limits of kp_batch_riaf_noalloc's static device scratch. */

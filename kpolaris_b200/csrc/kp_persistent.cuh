@@ -241,8 +241,10 @@ __device__ __forceinline__ void persistent_body(const WaveDesc& W) {
         queue_push(W.out_ids[PHASE], W.out_count[PHASE], forward, my_id);
         const bool active = st.mode != kIdle;
         // The block leaves the loop together, so the barrier below is
-        // reached by every thread of the block in every iteration.
-        if (!__syncthreads_or(active)) break;
+        // reached by every thread of the block in every iteration.  A lane
+        // that forwarded an id has more input to claim: it keeps the block
+        // in the loop like an active lane.
+        if (!__syncthreads_or(active || forward)) break;
 
         // ---------------------------------------------- control before the job
         int dest = -1;  // phase the ray is handed to (PHASE itself: next round)

@@ -246,13 +246,23 @@ void worker_main(kp_server* s) {
                 s->cv_work.wait(lock);
             }
             if (s->stop) {
+                // stopping: nothing new is started, and jobs in flight are
+                // abandoned after the tick that was running
                 for (auto& j : s->pending) {
                     j->state = KP_JOB_CANCELLED;
                     ++s->cancelled;
                 }
                 s->pending.clear();
+                for (auto& j : s->slots) {
+                    if (!j) continue;
+                    j->state = KP_JOB_CANCELLED;
+                    ++s->cancelled;
+                    s->rays.release(j->ray_base, j->npix);
+                    s->outs.release(j->out_base, j->out_units);
+                    j = nullptr;
+                }
                 s->cv_done.notify_all();
-                if (!any_inflight) break;
+                break;
             }
             while (!s->pending.empty()) {
                 auto& j = s->pending.front();

@@ -40,7 +40,7 @@ def test_results_same_alone_and_in_the_mix():
         ta = srv.submit(*a)
         tc = srv.submit(*c)
         for x in (tb, ta, tc):
-            srv.wait(x)
+            srv.wait(x, timeout=300.0)
         mixed_a = srv.result(ta)
         srv.result(tb)
         srv.result(tc)
@@ -58,7 +58,7 @@ def test_admission_respects_footprint():
     with kp.Server(max_rays=2 * 32 * 32, tick_budget=64) as srv:
         tickets = [srv.submit(*j) for j in jobs]
         for t in tickets:
-            srv.wait(t)
+            srv.wait(t, timeout=300.0)
         outs = [srv.result(t) for t in tickets]
         st = srv.stats()
     assert st.completed == 6
@@ -67,6 +67,27 @@ def test_admission_respects_footprint():
     ref = kp.batch_riaf(jobs, precision=_abi.PRECISION_MIXED)
     for k in range(6):
         assert_bitwise(outs[k], ref[k], f"job {k}")
+
+
+def test_long_queues_past_the_budget():
+    """More rays than lanes and a small budget: lanes run out of budget with
+    input left and hand it on; every ray must still finish, bit-identically."""
+    jobs = [job(256, spin=0.3 + 0.2 * k, inc=30.0 + 40.0 * k, freqs=[230e9, 345e9]) for k in range(3)]
+    with kp.Server(max_rays=1 << 18, tick_budget=16) as srv:
+        tickets = [srv.submit(*j) for j in jobs]
+        for t in tickets:
+            srv.wait(t, timeout=300.0)
+        outs = [srv.result(t) for t in tickets]
+    ref = kp.batch_riaf(jobs, precision=_abi.PRECISION_MIXED)
+    for k in range(3):
+        assert_bitwise(outs[k], ref[k], f"job {k}")
+
+
+def test_destroy_with_work_in_flight_is_bounded():
+    with kp.Server(max_rays=1 << 17, tick_budget=8) as srv:
+        t = srv.submit(*job(256, freqs=[230e9]))
+        time.sleep(0.05)
+    # leaving the block destroyed the server after one tick; the job ended cancelled
 
 
 def test_cancel_pending_and_running():
