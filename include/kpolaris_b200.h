@@ -327,6 +327,53 @@ int kp_batch_riaf(const kp_riaf_job* jobs, int njobs, const kp_run_options* opti
                   kp_batch_stats* stats);
 
 /*
+ * GRMHD snapshots (config: a grid of primitives in FMKS coordinates).
+ *
+ * kp_grmhd_model holds the scalars of GRMHDGridRadiationModel
+ * (src/model/grmhd_grid.hpp:52-97) this path uses; the grid itself is
+ * uploaded once with kp_grid_upload (primitives as FP32
+ * [8][n1][n2][n3]: rho, u, U1, U2, U3, B1, B2, B3 in code units) and stays
+ * resident until kp_grid_release.  With has_derived_scalars the derived
+ * scalars (n_e, Theta_e, B, sigma, beta per cell; the loaders'
+ * precompute_derived_scalars, src/grmhd/kharma_loader.cpp:261-362) are
+ * computed on the device at upload.  Thermal fits only (emission_type
+ * KP_FIT_PANDYA or KP_FIT_DEXTER); the reference's kappa and power-law
+ * distributions are not built.
+ */
+typedef struct kp_grmhd_model {
+    int n1, n2, n3;
+    double spin, gam;
+    double startx1, startx2, startx3, dx1, dx2, dx3;
+    double r_in, r_out;
+    double hslope, mks_smooth, poly_alpha, poly_xt, poly_norm;
+    double freq_cgs, mbh_solar, M_unit;
+    double trat_small, trat_large, beta_crit, sigma_cut, sigma_cut_high, ne_factor;
+    int emission_type;
+    double emission_scale, absorption_scale, faraday_scale, max_pol_frac;
+    int has_derived_scalars;
+} kp_grmhd_model;
+
+typedef struct kp_grid kp_grid;
+
+/* The struct's default member initialisers (grmhd_grid.hpp:52-97). */
+void kp_default_grmhd_model(kp_grmhd_model* m);
+int kp_grid_upload(const kp_grmhd_model* model, const float* prims, int device, kp_grid** out);
+/* Host copy of the derived scalars, [5][n1][n2][n3] FP64 (KP_ERR_INVALID if
+ * the grid has none). */
+int kp_grid_derived(const kp_grid* grid, double* out);
+int kp_grid_release(kp_grid* grid);
+
+/*
+ * One GRMHD image in FMKS coordinates, 1..KP_MAX_FREQUENCIES frequencies on
+ * one geodesic, through the wavefront engine in FP64.  Replaces
+ * run_grmhd_image (src/image/grmhd.hpp:12-32, src/image/grmhd.cpp:22-59) for
+ * the FMKS backend; params->coordinate_system must be KP_COORD_FMKS and the
+ * grid's spin must be params->spin.
+ */
+int kp_image_grmhd(const kp_pass_a_params* params, const kp_grid* grid, int radiation_substeps,
+                   const double* frequencies, int nfreq, const kp_run_options* options, kp_image_out* out);
+
+/*
  * Serving loop.  A server owns one GPU and a device-owner thread that runs
  * the wavefront engine in bounded ticks: each tick admits waiting jobs whose
  * HBM footprint fits (ray records + device outputs), seeds their rays, and

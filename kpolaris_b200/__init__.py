@@ -21,7 +21,7 @@ __all__ = [
     "ImageHostData", "PassAParams", "RIAFModel", "RunOptions", "KPolarisError",
     "default_pass_a_params", "default_riaf_model", "default_run_options", "library",
     "run_riaf_image", "run_riaf_multifrequency_image", "image_riaf", "batch_riaf", "Server",
-    "default_server_config",
+    "default_server_config", "Grid", "image_grmhd",
 ]
 
 LIB_PATH = Path(os.environ.get("KPOLARIS_B200_LIB") or Path(__file__).resolve().parent / "lib" / "libkpolaris_b200.so")
@@ -66,6 +66,12 @@ def library() -> C.CDLL:
     L.kp_default_pass_a_params.argtypes = [C.POINTER(PassAParams)]
     L.kp_default_riaf_model.argtypes = [C.POINTER(RIAFModel)]
     L.kp_default_server_config.argtypes = [C.POINTER(_abi.ServerConfig)]
+    L.kp_default_grmhd_model.argtypes = [C.POINTER(_abi.GrmhdModel)]
+    L.kp_grid_upload.argtypes = [C.POINTER(_abi.GrmhdModel), C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_void_p)]
+    L.kp_grid_derived.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
+    L.kp_grid_release.argtypes = [C.c_void_p]
+    L.kp_image_grmhd.argtypes = [C.POINTER(PassAParams), C.c_void_p, C.c_int, C.POINTER(C.c_double), C.c_int,
+                                 C.POINTER(RunOptions), C.POINTER(_abi.ImageOut)]
     L.kp_server_create.argtypes = [C.POINTER(_abi.ServerConfig), C.POINTER(C.c_void_p)]
     L.kp_server_submit.argtypes = [C.c_void_p, C.POINTER(_abi.RiafJob), C.POINTER(C.c_ulonglong)]
     L.kp_server_poll.argtypes = [C.c_void_p, C.c_ulonglong, C.POINTER(C.c_int)]
@@ -145,6 +151,58 @@ def batch_riaf(jobs, *, outs=None, precision=_abi.PRECISION_MIXED, stats=None, *
     st = stats if stats is not None else _abi.BatchStats()
     check(L.kp_batch_riaf(arr, len(jobs), C.byref(opt), C.byref(st)))
     return results
+
+
+class Grid:
+    """A GRMHD snapshot resident on a GPU (kp_grid_upload / kp_grid_release).
+    prims: float32 array [8, n1, n2, n3] (rho, u, U1..U3, B1..B3)."""
+
+    def __init__(self, model: _abi.GrmhdModel, prims, device: int = 0):
+        L = library()
+        p = np.ascontiguousarray(prims, dtype=np.float32)
+        if p.shape != (8, model.n1, model.n2, model.n3):
+            raise ValueError(f"prims shape {p.shape} != (8, {model.n1}, {model.n2}, {model.n3})")
+        h = C.c_void_p()
+        check(L.kp_grid_upload(C.byref(model), p.ctypes.data_as(C.POINTER(C.c_float)), int(device), C.byref(h)))
+        self._h = h
+        self.model = model
+        self.device = device
+
+    def derived(self) -> np.ndarray:
+        """Derived scalars [5, n1, n2, n3]: n_e, Theta_e, B (G), sigma, beta."""
+        m = self.model
+        out = np.empty((5, m.n1, m.n2, m.n3), dtype=np.float64)
+        check(library().kp_grid_derived(self._h, out.ctypes.data_as(C.POINTER(C.c_double))))
+        return out
+
+    def release(self) -> None:
+        if self._h:
+            library().kp_grid_release(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.release()
+
+
+def image_grmhd(params: PassAParams, grid: Grid, frequencies=None, *, radiation_substeps=1,
+                out: ImageHostData | None = None, **options) -> ImageHostData:
+    """One GRMHD image in FMKS coordinates (kp_image_grmhd), host outputs.
+    Mirrors run_grmhd_image (src/image/grmhd.hpp:12-32)."""
+    L = library()
+    if frequencies is None:
+        frequencies = [grid.model.freq_cgs]
+    nfreq = len(frequencies)
+    npix = params.camera.nx * params.camera.ny
+    if out is None:
+        out = ImageHostData.allocate(npix, nfreq)
+    fa = (C.c_double * max(nfreq, 1))(*frequencies)
+    s = out.as_struct()
+    opt = _options(device=grid.device, **options)
+    check(L.kp_image_grmhd(C.byref(params), grid._h, int(radiation_substeps), fa, nfreq, C.byref(opt), C.byref(s)))
+    return out
 
 
 def default_server_config() -> _abi.ServerConfig:

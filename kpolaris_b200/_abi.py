@@ -134,6 +134,43 @@ class RunOptions(C.Structure):
     ]
 
 
+class GrmhdModel(C.Structure):
+    _fields_ = [
+        ("n1", C.c_int), ("n2", C.c_int), ("n3", C.c_int),
+        ("spin", C.c_double), ("gam", C.c_double),
+        ("startx1", C.c_double), ("startx2", C.c_double), ("startx3", C.c_double),
+        ("dx1", C.c_double), ("dx2", C.c_double), ("dx3", C.c_double),
+        ("r_in", C.c_double), ("r_out", C.c_double),
+        ("hslope", C.c_double), ("mks_smooth", C.c_double), ("poly_alpha", C.c_double),
+        ("poly_xt", C.c_double), ("poly_norm", C.c_double),
+        ("freq_cgs", C.c_double), ("mbh_solar", C.c_double), ("M_unit", C.c_double),
+        ("trat_small", C.c_double), ("trat_large", C.c_double), ("beta_crit", C.c_double),
+        ("sigma_cut", C.c_double), ("sigma_cut_high", C.c_double), ("ne_factor", C.c_double),
+        ("emission_type", C.c_int),
+        ("emission_scale", C.c_double), ("absorption_scale", C.c_double), ("faraday_scale", C.c_double),
+        ("max_pol_frac", C.c_double),
+        ("has_derived_scalars", C.c_int),
+    ]
+
+
+def default_grmhd_model() -> GrmhdModel:
+    """GRMHDGridRadiationModel<double> defaults (src/model/grmhd_grid.hpp:52-97)."""
+    m = GrmhdModel()
+    m.spin = 0.5
+    m.gam = 4.0 / 3.0
+    m.dx1 = m.dx2 = m.dx3 = 1.0
+    m.r_in, m.r_out = 1.0, 1000.0
+    m.hslope, m.mks_smooth, m.poly_alpha, m.poly_xt, m.poly_norm = 0.3, 0.5, 14.0, 0.82, 1.0
+    m.freq_cgs, m.mbh_solar, m.M_unit = 230.0e9, 6.2e9, 3.0e25
+    m.trat_small, m.trat_large, m.beta_crit = 1.0, 20.0, 1.0
+    m.sigma_cut, m.sigma_cut_high, m.ne_factor = 1.0, -1.0, 1.0
+    m.emission_type = FIT_DEXTER
+    m.emission_scale = m.absorption_scale = m.faraday_scale = 1.0
+    m.max_pol_frac = 0.99
+    m.has_derived_scalars = 1
+    return m
+
+
 class RiafJob(C.Structure):
     _fields_ = [
         ("params", PassAParams), ("model", RIAFModel),

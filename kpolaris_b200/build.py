@@ -30,6 +30,7 @@ COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=o
 UNITS = {
     "kp_kernels_fp64.cu": ["--fmad=false"],
     "kp_kernels_mixed.cu": ["--fmad=true"],
+    "kp_kernels_grmhd.cu": ["--fmad=false"],
     "kp_capi.cu": ["--fmad=false"],
     "kp_noalloc.cu": ["--fmad=false"],
     "kp_server.cu": ["--fmad=false"],

@@ -12,6 +12,9 @@
 #include <mutex>
 #include <vector>
 
+#include "kp_fmks.cuh"
+#include "kp_grmhd.cuh"
+#include "kp_grmhd_setup.h"
 #include "kp_launch.h"
 #include "kpolaris_b200.h"
 
@@ -388,6 +391,188 @@ ImageConsts make_consts(const kp_pass_a_params* p, const kp_riaf_model* m, const
 
 using namespace kp;
 
+// A GRMHD snapshot resident on one device.
+struct kp_grid {
+    int device = 0;
+    kp_grmhd_model model;
+    float* prims = nullptr;     // [8][n1][n2][n3]
+    double* derived = nullptr;  // [5][n1][n2][n3] or null
+};
+
+namespace kp {
+
+GridConsts grid_consts(const kp_grid* g) { return grid_consts_of(g->model, g->prims, g->derived); }
+
+int validate_grmhd_model(const kp_grmhd_model* m) {
+    if (!m) return set_error(KP_ERR_INVALID, "null GRMHD model");
+    if (m->n1 <= 0 || m->n2 <= 0 || m->n3 <= 0 || double(m->n1) * m->n2 * m->n3 > 4.0e9)
+        return set_error(KP_ERR_INVALID, "grid dimensions must be positive (n1 n2 n3 = %d %d %d)", m->n1, m->n2, m->n3);
+    if (!(m->dx1 > 0.0) || !(m->dx2 > 0.0) || !(m->dx3 > 0.0))
+        return set_error(KP_ERR_INVALID, "grid spacings must be positive");
+    if (m->emission_type != KP_FIT_PANDYA && m->emission_type != KP_FIT_DEXTER)
+        return set_error(KP_ERR_UNSUPPORTED,
+                         "emission_type %d: only thermal synchrotron (1 Pandya, 4 Dexter) is built",
+                         m->emission_type);
+    return KP_OK;
+}
+
+ImageConsts make_consts_grmhd(const kp_pass_a_params* p, const kp_grid* g, const double* freqs, int nfreq,
+                              int integrator) {
+    return image_consts_fmks(p, g->model, grid_consts(g), freqs, nfreq, integrator);
+}
+
+}  // namespace kp
+
+// Job table storage for njobs descriptors (device table and pinned staging),
+// grow-only.  The caller holds g_mutex.
+int ensure_job_table(DeviceState* dev, int njobs) {
+    if (njobs <= dev->jobs_cap) return KP_OK;
+    cudaEventSynchronize(dev->staging_free);
+    if (dev->d_jobs) cudaFree(dev->d_jobs);
+    if (dev->h_jobs) cudaFreeHost(dev->h_jobs);
+    dev->d_jobs = nullptr;
+    dev->h_jobs = nullptr;
+    dev->jobs_cap = 0;
+    const int cap = std::max(njobs, 64);
+    cudaError_t e = cudaMalloc(&dev->d_jobs, sizeof(JobDesc) * size_t(cap));
+    if (e != cudaSuccess) return set_error(KP_ERR_OOM, "cudaMalloc(job table): %s", cudaGetErrorString(e));
+    e = cudaMallocHost(&dev->h_jobs, sizeof(JobDesc) * size_t(cap));
+    if (e != cudaSuccess) return set_error(KP_ERR_OOM, "cudaMallocHost(job table): %s", cudaGetErrorString(e));
+    dev->jobs_cap = cap;
+    return KP_OK;
+}
+
+// Runs the wavefront engine over the njobs job descriptors staged in
+// dev->h_jobs (total rays): uploads them, grows the record pool, launches
+// cycles of (far, near-A, near-B) until no ray is left and checks the status
+// word.  The caller holds g_mutex.
+enum : int { kFamilyRiafFP64 = 0, kFamilyRiafMixed = 1, kFamilyGrmhdFP64 = 2 };
+
+int run_wave_jobs(DeviceState* dev, cudaStream_t stream, int njobs, long long total, int family, int nf_max,
+                  const kp_run_options& opt, kp_batch_stats* stats) {
+    // ray records and id queues, grow-only
+    if (total > dev->pool_cap) {
+        cudaStreamSynchronize(stream);
+        cudaFree(dev->d_pool);
+        dev->d_pool = nullptr;
+        for (auto& q : dev->d_ids) {
+            cudaFree(q[0]);
+            cudaFree(q[1]);
+            q[0] = q[1] = nullptr;
+        }
+        dev->pool_cap = 0;
+        cudaError_t e = cudaMalloc(&dev->d_pool, sizeof(RayRecord) * size_t(total));
+        for (auto& q : dev->d_ids)
+            for (auto& b : q)
+                if (e == cudaSuccess) e = cudaMalloc(&b, sizeof(unsigned) * size_t(total));
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return set_error(KP_ERR_OOM, "cudaMalloc(%lld ray records): %s", total, cudaGetErrorString(e));
+        }
+        dev->pool_cap = total;
+    }
+    cudaError_t e = cudaMemcpyAsync(dev->d_jobs, dev->h_jobs, sizeof(JobDesc) * size_t(njobs),
+                                    cudaMemcpyHostToDevice, stream);
+    if (e != cudaSuccess) return cuda_error(e, "cudaMemcpyAsync(job table)");
+    cudaEventRecord(dev->staging_free, stream);
+    e = cudaMemsetAsync(dev->d_ctrl, 0, sizeof(WaveCtrl), stream);
+    if (e != cudaSuccess) return cuda_error(e, "cudaMemsetAsync(wave counters)");
+    if (opt.threads_per_block != 0)
+        return set_error(KP_ERR_INVALID, "threads_per_block is fixed by the wavefront kernels (%d far, %d near): pass 0",
+                         kFarThreads, kNearThreads);
+    const bool mixed = family == kFamilyRiafMixed;
+    int blocks[kPhases];
+    for (int phase = 0; phase < kPhases; ++phase) {
+        int per_sm = opt.blocks_per_sm;
+        if (per_sm <= 0) {
+            per_sm = family == kFamilyGrmhdFP64 ? wave_occupancy_grmhd(phase, nf_max, wave_threads(phase))
+                     : mixed ? wave_occupancy_mixed(phase, wave_threads(phase))
+                             : wave_occupancy_fp64(phase, nf_max, wave_threads(phase));
+            if (per_sm <= 0) per_sm = 1;
+        }
+        blocks[phase] = dev->sms * per_sm;
+        const long long needed = (total + wave_threads(phase) - 1) / wave_threads(phase);
+        if (blocks[phase] > needed) blocks[phase] = int(needed);
+    }
+    WaveCtrl* ctrl = dev->d_ctrl;
+    auto launch = [&](int cycle, int phase) -> cudaError_t {
+        WaveDesc W;
+        W.jobs = dev->d_jobs;
+        W.njobs = njobs;
+        W.pool = dev->d_pool;
+        W.fresh_begin = 0;
+        W.fresh_end = cycle == 0 && phase == kPhaseFar ? total : 0;
+        W.in_ids = dev->d_ids[phase][cycle % 2];
+        W.in_count = &ctrl->counts[cycle][phase];
+        W.in_head = &ctrl->heads[cycle * kPhases + phase];
+        for (int q = 0; q < kPhases; ++q) {
+            const int gen = q > phase ? cycle : cycle + 1;
+            W.out_ids[q] = dev->d_ids[q][gen % 2];
+            W.out_count[q] = &ctrl->counts[gen][q];
+        }
+        W.budget = 0;
+        W.status = &ctrl->status;
+        W.job_done = nullptr;
+        if (family == kFamilyGrmhdFP64) return launch_wave_grmhd(phase, W, nf_max, blocks[phase], wave_threads(phase), stream);
+        return mixed ? launch_wave_mixed(phase, W, blocks[phase], wave_threads(phase), stream)
+                     : launch_wave_fp64(phase, W, nf_max, blocks[phase], wave_threads(phase), stream);
+    };
+    // Rays leave the camera in the far phase, trace the radiating sphere in
+    // near-A then near-B and return in the far phase of the next cycle; a few
+    // graze the boundary and take one more.  After each cycle the host reads
+    // the next generation's queue counts.
+    cudaEventRecord(dev->ev0, stream);
+    int launches = 0;
+    int cycle = 0;
+    while (true) {
+        if (cycle >= kMaxWaveCycles)
+            return set_error(KP_ERR_TIMEOUT, "rays still moving between phases after %d launches", launches);
+        for (int phase = 0; phase < kPhases; ++phase) {
+            if (stats) cudaEventRecord(dev->ev_launch[launches], stream);
+            e = launch(cycle, phase);
+            if (e != cudaSuccess) return cuda_error(e, "wavefront kernel launch");
+            ++launches;
+        }
+        if (stats) cudaEventRecord(dev->ev_launch[launches], stream);
+        ++cycle;
+        e = cudaMemcpyAsync(dev->h_left, ctrl->counts[cycle], sizeof(unsigned) * kPhases, cudaMemcpyDeviceToHost,
+                            stream);
+        if (e != cudaSuccess) return cuda_error(e, "queue count read");
+        e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) return cuda_error(e, "wavefront kernels");
+        if (dev->h_left[0] == 0 && dev->h_left[1] == 0 && dev->h_left[2] == 0) break;
+    }
+    cudaEventRecord(dev->ev1, stream);
+    if (stats) {
+        stats->rays = total;
+        stats->launches = launches;
+        stats->blocks = blocks[kPhaseNearB];
+        stats->threads_per_block = kNearThreads;
+    }
+    e = cudaEventSynchronize(dev->ev1);
+    if (e != cudaSuccess) return cuda_error(e, "wavefront kernels");
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, dev->ev0, dev->ev1);
+    if (stats) {
+        stats->kernel_seconds = ms * 1e-3;
+        for (int k = 0; k < launches; ++k) {
+            float lms = 0.f;
+            cudaEventElapsedTime(&lms, dev->ev_launch[k], dev->ev_launch[k + 1]);
+            stats->phase_seconds[k % kPhases] += lms * 1e-3;
+            stats->phase_launches[k % kPhases] += 1;
+        }
+    }
+    if (opt.timing) std::printf("timing image_kernel_batch %g s\n", ms * 1e-3);
+    int status_word = 0;
+    e = cudaMemcpy(&status_word, &ctrl->status, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_error(e, "status read");
+    if (status_word == 2)
+        return set_error(KP_ERR_TIMEOUT, "a lane exceeded the engine's iteration guard");
+    if (status_word != 0)
+        return set_error(KP_ERR_CUDA, "wavefront engine invariant violated (status %d)", status_word);
+    return KP_OK;
+}
+
 extern "C" {
 
 const char* kp_last_error(void) { return g_error; }
@@ -596,21 +781,8 @@ int kp_batch_riaf(const kp_riaf_job* jobs, int njobs, const kp_run_options* opti
     DeviceState* dev = device_state(opt.device, &st);
     if (!dev) return st;
     cudaStream_t stream = opt.stream ? static_cast<cudaStream_t>(opt.stream) : dev->stream;
-    // job table storage
-    if (njobs > dev->jobs_cap) {
-        cudaEventSynchronize(dev->staging_free);
-        if (dev->d_jobs) cudaFree(dev->d_jobs);
-        if (dev->h_jobs) cudaFreeHost(dev->h_jobs);
-        dev->d_jobs = nullptr;
-        dev->h_jobs = nullptr;
-        dev->jobs_cap = 0;
-        const int cap = std::max(njobs, 64);
-        cudaError_t e = cudaMalloc(&dev->d_jobs, sizeof(JobDesc) * size_t(cap));
-        if (e != cudaSuccess) return set_error(KP_ERR_OOM, "cudaMalloc(job table): %s", cudaGetErrorString(e));
-        e = cudaMallocHost(&dev->h_jobs, sizeof(JobDesc) * size_t(cap));
-        if (e != cudaSuccess) return set_error(KP_ERR_OOM, "cudaMallocHost(job table): %s", cudaGetErrorString(e));
-        dev->jobs_cap = cap;
-    }
+    st = ensure_job_table(dev, njobs);
+    if (st != KP_OK) return st;
     void* scratch_base = nullptr;
     if (!opt.outputs_on_device) {
         scratch_base = device_output_buffer(dev, scratch, &st);
@@ -648,125 +820,10 @@ int kp_batch_riaf(const kp_riaf_job* jobs, int njobs, const kp_run_options* opti
         d.precision = opt.precision;
         ray += npix;
     }
-    // ray records and id queues, grow-only
-    if (total > dev->pool_cap) {
-        cudaStreamSynchronize(stream);
-        cudaFree(dev->d_pool);
-        dev->d_pool = nullptr;
-        for (auto& q : dev->d_ids) {
-            cudaFree(q[0]);
-            cudaFree(q[1]);
-            q[0] = q[1] = nullptr;
-        }
-        dev->pool_cap = 0;
-        cudaError_t e = cudaMalloc(&dev->d_pool, sizeof(RayRecord) * size_t(total));
-        for (auto& q : dev->d_ids)
-            for (auto& b : q)
-                if (e == cudaSuccess) e = cudaMalloc(&b, sizeof(unsigned) * size_t(total));
-        if (e != cudaSuccess) {
-            cudaGetLastError();
-            return set_error(KP_ERR_OOM, "cudaMalloc(%lld ray records): %s", total, cudaGetErrorString(e));
-        }
-        dev->pool_cap = total;
-    }
-    cudaError_t e = cudaMemcpyAsync(dev->d_jobs, dev->h_jobs, sizeof(JobDesc) * size_t(njobs),
-                                    cudaMemcpyHostToDevice, stream);
-    if (e != cudaSuccess) return cuda_error(e, "cudaMemcpyAsync(job table)");
-    cudaEventRecord(dev->staging_free, stream);
-    e = cudaMemsetAsync(dev->d_ctrl, 0, sizeof(WaveCtrl), stream);
-    if (e != cudaSuccess) return cuda_error(e, "cudaMemsetAsync(wave counters)");
-    if (opt.threads_per_block != 0)
-        return set_error(KP_ERR_INVALID, "threads_per_block is fixed by the wavefront kernels (%d far, %d near): pass 0",
-                         kFarThreads, kNearThreads);
-    const bool mixed = opt.precision == KP_PRECISION_MIXED;
-    int blocks[kPhases];
-    for (int phase = 0; phase < kPhases; ++phase) {
-        int per_sm = opt.blocks_per_sm;
-        if (per_sm <= 0) {
-            per_sm = mixed ? wave_occupancy_mixed(phase, wave_threads(phase))
-                           : wave_occupancy_fp64(phase, nf_max, wave_threads(phase));
-            if (per_sm <= 0) per_sm = 1;
-        }
-        blocks[phase] = dev->sms * per_sm;
-        const long long needed = (total + wave_threads(phase) - 1) / wave_threads(phase);
-        if (blocks[phase] > needed) blocks[phase] = int(needed);
-    }
-    WaveCtrl* ctrl = dev->d_ctrl;
-    auto launch = [&](int cycle, int phase) -> cudaError_t {
-        WaveDesc W;
-        W.jobs = dev->d_jobs;
-        W.njobs = njobs;
-        W.pool = dev->d_pool;
-        W.fresh_begin = 0;
-        W.fresh_end = cycle == 0 && phase == kPhaseFar ? total : 0;
-        W.in_ids = dev->d_ids[phase][cycle % 2];
-        W.in_count = &ctrl->counts[cycle][phase];
-        W.in_head = &ctrl->heads[cycle * kPhases + phase];
-        for (int q = 0; q < kPhases; ++q) {
-            const int gen = q > phase ? cycle : cycle + 1;
-            W.out_ids[q] = dev->d_ids[q][gen % 2];
-            W.out_count[q] = &ctrl->counts[gen][q];
-        }
-        W.budget = 0;
-        W.status = &ctrl->status;
-        W.job_done = nullptr;
-        return mixed ? launch_wave_mixed(phase, W, blocks[phase], wave_threads(phase), stream)
-                     : launch_wave_fp64(phase, W, nf_max, blocks[phase], wave_threads(phase), stream);
-    };
-    // Rays leave the camera in the far phase, trace the radiating sphere in
-    // near-A then near-B and return in the far phase of the next cycle; a few
-    // graze the boundary and take one more.  After each cycle the host reads
-    // the next generation's queue counts.
-    cudaEventRecord(dev->ev0, stream);
-    int launches = 0;
-    int cycle = 0;
-    while (true) {
-        if (cycle >= kMaxWaveCycles)
-            return set_error(KP_ERR_TIMEOUT, "rays still moving between phases after %d launches", launches);
-        for (int phase = 0; phase < kPhases; ++phase) {
-            if (stats) cudaEventRecord(dev->ev_launch[launches], stream);
-            e = launch(cycle, phase);
-            if (e != cudaSuccess) return cuda_error(e, "wavefront kernel launch");
-            ++launches;
-        }
-        if (stats) cudaEventRecord(dev->ev_launch[launches], stream);
-        ++cycle;
-        e = cudaMemcpyAsync(dev->h_left, ctrl->counts[cycle], sizeof(unsigned) * kPhases, cudaMemcpyDeviceToHost,
-                            stream);
-        if (e != cudaSuccess) return cuda_error(e, "queue count read");
-        e = cudaStreamSynchronize(stream);
-        if (e != cudaSuccess) return cuda_error(e, "wavefront kernels");
-        if (dev->h_left[0] == 0 && dev->h_left[1] == 0 && dev->h_left[2] == 0) break;
-    }
-    cudaEventRecord(dev->ev1, stream);
-    if (stats) {
-        stats->rays = total;
-        stats->launches = launches;
-        stats->blocks = blocks[kPhaseNearB];
-        stats->threads_per_block = kNearThreads;
-        stats->device_output_bytes = opt.outputs_on_device ? 0 : scratch;
-    }
-    e = cudaEventSynchronize(dev->ev1);
-    if (e != cudaSuccess) return cuda_error(e, "wavefront kernels");
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, dev->ev0, dev->ev1);
-    if (stats) {
-        stats->kernel_seconds = ms * 1e-3;
-        for (int k = 0; k < launches; ++k) {
-            float lms = 0.f;
-            cudaEventElapsedTime(&lms, dev->ev_launch[k], dev->ev_launch[k + 1]);
-            stats->phase_seconds[k % kPhases] += lms * 1e-3;
-            stats->phase_launches[k % kPhases] += 1;
-        }
-    }
-    if (opt.timing) std::printf("timing image_kernel_batch %g s\n", ms * 1e-3);
-    int status_word = 0;
-    e = cudaMemcpy(&status_word, &ctrl->status, sizeof(int), cudaMemcpyDeviceToHost);
-    if (e != cudaSuccess) return cuda_error(e, "status read");
-    if (status_word == 2)
-        return set_error(KP_ERR_TIMEOUT, "a lane exceeded the engine's iteration guard");
-    if (status_word != 0)
-        return set_error(KP_ERR_CUDA, "wavefront engine invariant violated (status %d)", status_word);
+    st = run_wave_jobs(dev, stream, njobs, total, opt.precision == KP_PRECISION_MIXED ? kFamilyRiafMixed : kFamilyRiafFP64,
+                       nf_max, opt, stats);
+    if (st != KP_OK) return st;
+    if (stats) stats->device_output_bytes = opt.outputs_on_device ? 0 : scratch;
     if (!opt.outputs_on_device) {
         const auto t1 = std::chrono::steady_clock::now();
         for (int i = 0; i < njobs; ++i) {
@@ -774,11 +831,159 @@ int kp_batch_riaf(const kp_riaf_job* jobs, int njobs, const kp_run_options* opti
                                       jobs[i].nfreq, stream);
             if (st != KP_OK) return st;
         }
-        e = cudaStreamSynchronize(stream);
+        cudaError_t e = cudaStreamSynchronize(stream);
         if (e != cudaSuccess) return cuda_error(e, "device-to-host copy");
         const double s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t1).count();
         if (stats) stats->copy_seconds = s;
         if (opt.timing) std::printf("timing image_device_to_host_batch %g s\n", s);
+    }
+    return KP_OK;
+}
+
+
+void kp_default_grmhd_model(kp_grmhd_model* m) {
+    if (!m) return;
+    std::memset(m, 0, sizeof(*m));
+    m->spin = 0.5;
+    m->gam = 4.0 / 3.0;
+    m->dx1 = m->dx2 = m->dx3 = 1.0;
+    m->r_in = 1.0;
+    m->r_out = 1000.0;
+    m->hslope = 0.3;
+    m->mks_smooth = 0.5;
+    m->poly_alpha = 14.0;
+    m->poly_xt = 0.82;
+    m->poly_norm = 1.0;
+    m->freq_cgs = 230.0e9;
+    m->mbh_solar = 6.2e9;
+    m->M_unit = 3.0e25;
+    m->trat_small = 1.0;
+    m->trat_large = 20.0;
+    m->beta_crit = 1.0;
+    m->sigma_cut = 1.0;
+    m->sigma_cut_high = -1.0;
+    m->ne_factor = 1.0;
+    m->emission_type = KP_FIT_DEXTER;
+    m->emission_scale = m->absorption_scale = m->faraday_scale = 1.0;
+    m->max_pol_frac = 0.99;
+    m->has_derived_scalars = 1;
+}
+
+int kp_grid_upload(const kp_grmhd_model* model, const float* prims, int device, kp_grid** out) {
+    if (!out) return set_error(KP_ERR_INVALID, "kp_grid_upload: null output handle");
+    *out = nullptr;
+    int st = validate_grmhd_model(model);
+    if (st != KP_OK) return st;
+    if (!prims) return set_error(KP_ERR_INVALID, "kp_grid_upload: null primitives");
+    std::lock_guard<std::mutex> lock(g_mutex);
+    DeviceState* dev = device_state(device, &st);
+    if (!dev) return st;
+    auto* g = new kp_grid();
+    g->device = device;
+    g->model = *model;
+    const size_t ncell = size_t(model->n1) * size_t(model->n2) * size_t(model->n3);
+    cudaError_t e = cudaMalloc(&g->prims, sizeof(float) * 8 * ncell);
+    if (e == cudaSuccess && model->has_derived_scalars) e = cudaMalloc(&g->derived, sizeof(double) * kNumDerived * ncell);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        cudaFree(g->prims);
+        cudaFree(g->derived);
+        delete g;
+        return set_error(KP_ERR_OOM, "grid allocation (%zu cells): %s", ncell, cudaGetErrorString(e));
+    }
+    e = cudaMemcpyAsync(g->prims, prims, sizeof(float) * 8 * ncell, cudaMemcpyHostToDevice, dev->stream);
+    if (e == cudaSuccess && g->derived) e = launch_grid_derived(grid_consts(g), g->derived, dev->sms, dev->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(dev->stream);
+    if (e != cudaSuccess) {
+        cudaFree(g->prims);
+        cudaFree(g->derived);
+        delete g;
+        return cuda_error(e, "grid upload");
+    }
+    *out = g;
+    return KP_OK;
+}
+
+int kp_grid_derived(const kp_grid* g, double* out) {
+    if (!g || !out) return set_error(KP_ERR_INVALID, "kp_grid_derived: null argument");
+    if (!g->derived) return set_error(KP_ERR_INVALID, "the grid has no derived scalars");
+    cudaError_t e = cudaSetDevice(g->device);
+    const size_t ncell = size_t(g->model.n1) * size_t(g->model.n2) * size_t(g->model.n3);
+    if (e == cudaSuccess) e = cudaMemcpy(out, g->derived, sizeof(double) * kNumDerived * ncell, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_error(e, "derived scalar copy");
+    return KP_OK;
+}
+
+int kp_grid_release(kp_grid* g) {
+    if (!g) return KP_OK;
+    cudaSetDevice(g->device);
+    cudaFree(g->prims);
+    cudaFree(g->derived);
+    delete g;
+    return KP_OK;
+}
+
+int kp_image_grmhd(const kp_pass_a_params* params, const kp_grid* grid, int radiation_substeps,
+                   const double* frequencies, int nfreq, const kp_run_options* options, kp_image_out* out) {
+    if (!params || !grid || !out) return set_error(KP_ERR_INVALID, "kp_image_grmhd: null argument");
+    kp_run_options opt;
+    if (options) {
+        opt = *options;
+    } else {
+        kp_default_run_options(&opt);
+    }
+    if (params->coordinate_system != KP_COORD_FMKS)
+        return set_error(KP_ERR_UNSUPPORTED, "GRMHD image coordinate backend not built: only fmks is");
+    if (params->camera.nx <= 0 || params->camera.ny <= 0 || params->camera.nx > 2147483647 / params->camera.ny)
+        return set_error(KP_ERR_INVALID, "image dimensions must have a positive int-sized product");
+    if (nfreq < 1 || nfreq > KP_MAX_FREQUENCIES)
+        return set_error(KP_ERR_INVALID, "multifrequency image chunk size must be between 1 and KP_MAX_FREQUENCIES (%d)",
+                         KP_MAX_FREQUENCIES);
+    if (nfreq > 1 && !frequencies) return set_error(KP_ERR_INVALID, "null frequency list");
+    if (params->camera.model != KP_CAMERA_PINHOLE)
+        return set_error(KP_ERR_UNSUPPORTED, "only the pinhole camera is built for the GPU image path");
+    if (params->direct_only) return set_error(KP_ERR_UNSUPPORTED, "direct_only transport is not built");
+    if (radiation_substeps < 1) return set_error(KP_ERR_INVALID, "radiation_substeps must be positive");
+    if (grid->model.spin != params->spin) return set_error(KP_ERR_INVALID, "grid spin differs from the metric spin");
+    if (opt.precision != KP_PRECISION_FP64)
+        return set_error(KP_ERR_UNSUPPORTED, "GRMHD images are built for KP_PRECISION_FP64 only");
+    if (opt.integrator != KP_INTEGRATOR_STEP_DOUBLING_RK4 && opt.integrator != KP_INTEGRATOR_CASH_KARP)
+        return set_error(KP_ERR_INVALID, "unknown integrator %d", opt.integrator);
+    if (opt.device != grid->device) return set_error(KP_ERR_INVALID, "the grid lives on device %d", grid->device);
+    const int npix = params->camera.nx * params->camera.ny;
+    int st = check_outputs(out, npix, nfreq);
+    if (st != KP_OK) return st;
+    std::lock_guard<std::mutex> lock(g_mutex);
+    DeviceState* dev = device_state(opt.device, &st);
+    if (!dev) return st;
+    cudaStream_t stream = opt.stream ? static_cast<cudaStream_t>(opt.stream) : dev->stream;
+    st = ensure_job_table(dev, 1);
+    if (st != KP_OK) return st;
+    ImageOutPtrs dptr;
+    if (opt.outputs_on_device) {
+        dptr = from_abi(out);
+    } else {
+        void* buf = device_output_buffer(dev, carved_bytes(npix, nfreq), &st);
+        if (!buf) return st;
+        dptr = carve_outputs(buf, npix, nfreq);
+    }
+    cudaEventSynchronize(dev->staging_free);
+    JobDesc& d = dev->h_jobs[0];
+    std::memset(&d, 0, sizeof(d));
+    d.c = make_consts_grmhd(params, grid, frequencies, nfreq, opt.integrator);
+    fmks_camera_frame(d.c.fmks, params->camera.radius, params->camera.inclination, d.frame.x, d.frame.e0,
+                      d.frame.e1, d.frame.e2, d.frame.e3);
+    d.out = dptr;
+    d.ray_begin = 0;
+    d.npix = npix;
+    d.precision = KP_PRECISION_FP64;
+    st = run_wave_jobs(dev, stream, 1, npix, kFamilyGrmhdFP64, nfreq == 1 ? 1 : KP_MAX_FREQUENCIES, opt, nullptr);
+    if (st != KP_OK) return st;
+    if (!opt.outputs_on_device) {
+        st = copy_outputs_to_host(dptr, out, npix, nfreq, stream);
+        if (st != KP_OK) return st;
+        cudaError_t e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) return cuda_error(e, "device-to-host copy");
     }
     return KP_OK;
 }

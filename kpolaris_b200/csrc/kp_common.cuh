@@ -55,6 +55,27 @@ struct Coeffs {
     R jI, jQ, jU, jV, aI, aQ, aU, aV, rQ, rU, rV;
 };
 
+// FMKS coordinate parameters (PassAParams fmks_*, pass_a_core.hpp:29-34, and
+// the grid mapping of GRMHDGridRadiationModel, grmhd_grid.hpp:58-66).
+struct FmksParams {
+    double mass, spin;
+    double startx1, hslope, mks_smooth, poly_alpha, poly_xt, poly_norm;
+};
+
+// A GRMHD snapshot resident on the device (GRMHDGridRadiationModel scalars,
+// grmhd_grid.hpp:52-97, with the unit conversions resolved on the host).
+struct GridConsts {
+    const float* prims;      // [8][n1][n2][n3]: rho, u, U1..U3, B1..B3
+    const double* derived;   // [5][n1][n2][n3]: n_e, Theta_e, B, sigma, beta (or null)
+    int n1, n2, n3, has_derived;
+    double startx1, startx2, startx3, dx1, dx2, dx3;
+    double r_in, r_out, gam;
+    FmksParams map;          // theta(x1, x2) of the grid
+    double rho_unit, b_unit, trat_small, trat_large, beta_crit, sigma_cut, sigma_cut_high, ne_factor;
+};
+
+enum Scene : int { kSceneRiafCks = 0, kSceneGrmhdFmks = 1 };
+
 // Everything one image needs on the device, resolved on the host.  Host-side
 // precomputation keeps libm (sin/cos of the inclination, cbrt in the ISCO
 // radius) on the CPU so the device geometry uses only + - * / sqrt and stays
@@ -91,6 +112,10 @@ struct ImageConsts {
     // mixed path: per-image power-of-two scale applied to j and S
     float emission_scale_pow2[kMaxFreq];
     double inv_emission_scale_pow2[kMaxFreq];
+    // scene: RIAF in Cartesian Kerr-Schild, or a GRMHD grid in FMKS
+    int scene;
+    FmksParams fmks;
+    GridConsts grid;
 };
 
 // Device pointers of one image's outputs, laid out like ImageHostData.

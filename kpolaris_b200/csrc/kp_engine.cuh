@@ -23,6 +23,7 @@
 #include "kp_trace_fp64.cuh"
 #include "kp_geometry_f32.cuh"
 #include "kp_radiation_f32.cuh"
+#include "kp_scene.cuh"
 
 namespace kp {
 
@@ -52,13 +53,13 @@ struct PolicyMixed {
     static constexpr bool kMixed = true;
 };
 
-// Radiation side of a policy: FP64 (the reference's arithmetic) or FP32 with
-// the per-frequency 2^E emission scale (kp_radiation_f32.cuh).
-template<class P>
+// Radiation side of a policy and scene: FP64 (the reference's arithmetic) or
+// FP32 with the per-frequency 2^E emission scale (kp_radiation_f32.cuh).
+template<class P, class S = SceneRiaf>
 struct RadTraits;
 
 template<>
-struct RadTraits<PolicyFP64> {
+struct RadTraits<PolicyFP64, SceneRiaf> {
     using Stokes = Stokes4<double>;
     using Co = Coeffs<double>;
     using Sample = RiafSample;
@@ -79,7 +80,7 @@ struct RadTraits<PolicyFP64> {
 };
 
 template<>
-struct RadTraits<PolicyMixed> {
+struct RadTraits<PolicyMixed, SceneRiaf> {
     using Stokes = StokesF;
     using Co = CoeffsF;
     using Sample = RiafSampleF;
@@ -103,14 +104,35 @@ struct RadTraits<PolicyMixed> {
     }
 };
 
-// FP32 is a compile-time choice of the calling kernel, so each kernel holds
-// one contraction body.  The FP64 policy keeps the reference's operation
-// order; the mixed policy uses the factored form (kp_geometry_f32.cuh).
-template<class P, bool FP32>
-__device__ __forceinline__ Ray policy_rhs(double mass, double spin, const Ray& X) {
-    if constexpr (P::kMixed && FP32) return ks_rhs_factored<float>(mass, spin, X);
-    else if constexpr (P::kMixed) return ks_rhs_factored<double>(mass, spin, X);
-    else return ks_rhs(mass, spin, X);
+// GRMHD grid plasma, FP64 throughout.
+template<>
+struct RadTraits<PolicyFP64, SceneGrmhd> {
+    using Stokes = Stokes4<double>;
+    using Co = Coeffs<double>;
+    using Sample = GrmhdSample;
+    __device__ static void zero(Stokes& s) { s = Stokes4<double>{0.0, 0.0, 0.0, 0.0}; }
+    __device__ static Sample sample(const ImageConsts& c, const Ray& r) { return grmhd_sample(c, r); }
+    __device__ static Sample none() {
+        Sample s;
+        s.emitting = 0;
+        return s;
+    }
+    __device__ static Co coeffs(const ImageConsts& c, const Sample& p, int f) {
+        return grmhd_coefficients(c, p, c.freq[f]);
+    }
+    __device__ static void step(Stokes& s, const Co& co, double h, const ImageConsts& c, int f) {
+        stokes_step(s, co, abs_val(h) * c.dlambda_scale[f]);
+    }
+    __device__ static Stokes4<double> result(const Stokes& s, const ImageConsts&, int) { return s; }
+};
+
+// The scene's transport RHS under a policy; FP32 is a compile-time choice of
+// the calling kernel, so each kernel holds one contraction body.  The FP64
+// policy keeps the reference's operation order; the mixed policy uses the
+// factored form (kp_geometry_f32.cuh).
+template<class P, bool FP32, class S>
+__device__ __forceinline__ Ray policy_rhs(const ImageConsts& c, const Ray& X) {
+    return S::template rhs<P::kMixed, FP32>(c, X);
 }
 
 // ---------------------------------------------------------------- RK jobs
@@ -118,39 +140,39 @@ __device__ __forceinline__ Ray policy_rhs(double mass, double spin, const Ray& X
 // (sample point: the first half step for SD, the endpoint otherwise) and err
 // (SD / CK only).  The stage arithmetic is the reference's (see file header).
 // Cash-Karp attempt with the reference's stage coefficients (rk4.hpp:171-228).
-template<class P, bool FP32>
-__device__ __noinline__ void ck_job(double mass, double spin, const Ray& S, double h, Ray& next,
+template<class P, bool FP32, class SC>
+__device__ __noinline__ void ck_job(const ImageConsts& c, const Ray& S, double h, Ray& next,
                                     Ray& mid, double& err) {
     {
-        const Ray k1 = policy_rhs<P, FP32>(mass, spin, S);
+        const Ray k1 = policy_rhs<P, FP32, SC>(c, S);
         Ray t;
         ray_axpy(t, S, h * 1.0 / 5.0, k1);
-        const Ray k2 = policy_rhs<P, FP32>(mass, spin, t);
+        const Ray k2 = policy_rhs<P, FP32, SC>(c, t);
         {
             const Ray* const kk[2] = {&k1, &k2};
             const double cc[2] = {3.0 / 40.0, 9.0 / 40.0};
             ray_lincomb<2>(t, S, h, kk, cc);
         }
-        const Ray k3 = policy_rhs<P, FP32>(mass, spin, t);
+        const Ray k3 = policy_rhs<P, FP32, SC>(c, t);
         {
             const Ray* const kk[3] = {&k1, &k2, &k3};
             const double cc[3] = {3.0 / 10.0, -9.0 / 10.0, 6.0 / 5.0};
             ray_lincomb<3>(t, S, h, kk, cc);
         }
-        const Ray k4 = policy_rhs<P, FP32>(mass, spin, t);
+        const Ray k4 = policy_rhs<P, FP32, SC>(c, t);
         {
             const Ray* const kk[4] = {&k1, &k2, &k3, &k4};
             const double cc[4] = {-11.0 / 54.0, 5.0 / 2.0, -70.0 / 27.0, 35.0 / 27.0};
             ray_lincomb<4>(t, S, h, kk, cc);
         }
-        const Ray k5 = policy_rhs<P, FP32>(mass, spin, t);
+        const Ray k5 = policy_rhs<P, FP32, SC>(c, t);
         {
             const Ray* const kk[5] = {&k1, &k2, &k3, &k4, &k5};
             const double cc[5] = {1631.0 / 55296.0, 175.0 / 512.0, 575.0 / 13824.0, 44275.0 / 110592.0,
                                   253.0 / 4096.0};
             ray_lincomb<5>(t, S, h, kk, cc);
         }
-        const Ray k6 = policy_rhs<P, FP32>(mass, spin, t);
+        const Ray k6 = policy_rhs<P, FP32, SC>(c, t);
         {
             const Ray* const kk[4] = {&k1, &k3, &k4, &k6};
             const double cc[4] = {37.0 / 378.0, 250.0 / 621.0, 125.0 / 594.0, 512.0 / 1771.0};
@@ -171,11 +193,11 @@ __device__ __noinline__ void ck_job(double mass, double spin, const Ray& S, doub
 // Step-doubling attempt, RK4 step or composed RK4 pair as a stage loop around
 // one RHS site.  Out of line: the caller's control state is saved once per
 // job and the stage loop has the register file to itself.
-template<class P, bool FP32>
-__device__ __noinline__ void rk_job(int kind, double mass, double spin, const Ray& S, double h,
+template<class P, bool FP32, class SC>
+__device__ __noinline__ void rk_job(int kind, const ImageConsts& c, const Ray& S, double h,
                                     Ray& next, Ray& mid, double& err) {
     if (kind == kRkCK) {
-        ck_job<P, FP32>(mass, spin, S, h, next, mid, err);
+        ck_job<P, FP32, SC>(c, S, h, next, mid, err);
         return;
     }
     // Stage schedule (see file header): SD = half chain (4), second half
@@ -192,7 +214,7 @@ __device__ __noinline__ void rk_job(int kind, double mass, double spin, const Ra
     Ray R2;      // SD / RK4x2: the first chain's endpoint (half step)
 #pragma unroll 1
     for (int st = 0; st < nstage; ++st) {
-        const Ray k = policy_rhs<P, FP32>(mass, spin, X);
+        const Ray k = policy_rhs<P, FP32, SC>(c, X);
         // position of this stage inside its 4-stage RK4 chain
         const int cs = st < 4 ? st : (st < 8 ? st - 4 : st - 7);
         const bool full_chain = kind == kRkSD && st >= 8;

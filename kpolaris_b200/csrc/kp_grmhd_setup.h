@@ -1,0 +1,114 @@
+// kp_grmhd_setup.h -- host-side construction of the constants of a GRMHD
+// image: the device view of a grid (GridConsts) with its unit conversions
+// resolved, and the per-image ImageConsts for the FMKS metric.  Shared by the
+// C ABI (kp_capi.cu) and the host-compiled checks of the GRMHD device code.
+//
+// Reference: GRMHDGridRadiationModel unit conversions length_unit_cgs /
+// rho_unit_cgs / b_unit_cgs / dlambda_scale (src/model/grmhd_grid.hpp:140-161),
+// the PassAParams pass controls (src/geodesic/pass_a_core.hpp:10-36).
+#pragma once
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "kp_common.cuh"
+#include "kpolaris_b200.h"
+
+namespace kp {
+
+inline double grmhd_length_unit_cgs(const kp_grmhd_model& m) {
+    const double gnewt = 6.67430e-8, msun = 1.98847e33, cl = 2.99792458e10;
+    return gnewt * m.mbh_solar * msun / (cl * cl);
+}
+
+// Device view of a grid: prims [8][n1][n2][n3] FP32 and derived scalars
+// [5][n1][n2][n3] FP64 (or null) at device addresses.
+inline GridConsts grid_consts_of(const kp_grmhd_model& m, const float* prims, const double* derived) {
+    GridConsts c;
+    std::memset(&c, 0, sizeof(c));
+    c.prims = prims;
+    c.derived = derived;
+    c.n1 = m.n1;
+    c.n2 = m.n2;
+    c.n3 = m.n3;
+    c.has_derived = derived ? 1 : 0;
+    c.startx1 = m.startx1;
+    c.startx2 = m.startx2;
+    c.startx3 = m.startx3;
+    c.dx1 = m.dx1;
+    c.dx2 = m.dx2;
+    c.dx3 = m.dx3;
+    c.r_in = m.r_in;
+    c.r_out = m.r_out;
+    c.gam = m.gam;
+    c.map = FmksParams{1.0, m.spin, m.startx1, m.hslope, m.mks_smooth, m.poly_alpha, m.poly_xt, m.poly_norm};
+    const double L = grmhd_length_unit_cgs(m);
+    const double cl = 2.99792458e10;
+    c.rho_unit = m.M_unit / std::max(L * L * L, 1e-300);
+    c.b_unit = cl * std::sqrt(4.0 * 3.141592653589793238462643383279502884 * c.rho_unit);
+    c.trat_small = m.trat_small;
+    c.trat_large = m.trat_large;
+    c.beta_crit = m.beta_crit;
+    c.sigma_cut = m.sigma_cut;
+    c.sigma_cut_high = m.sigma_cut_high;
+    c.ne_factor = m.ne_factor;
+    return c;
+}
+
+// Constants of one GRMHD image: the pass controls with the FMKS metric and
+// the grid plasma; freqs null means the model's freq_cgs.
+inline ImageConsts image_consts_fmks(const kp_pass_a_params* p, const kp_grmhd_model& m, const GridConsts& grid,
+                                     const double* freqs, int nfreq, int integrator) {
+    ImageConsts c;
+    std::memset(&c, 0, sizeof(c));
+    c.mass = p->mass;
+    c.spin = p->spin;
+    c.horizon = p->mass + std::sqrt(std::max(p->mass * p->mass - p->spin * p->spin, 0.0));
+    c.inner_radius = p->inner_radius;
+    c.outer_radius = p->outer_radius;
+    c.step = p->step;
+    c.min_step_abs = std::fabs(p->min_step);
+    c.max_step = p->max_step;
+    c.tolerance = p->adaptive_tolerance;
+    c.max_radiation_step = p->max_radiation_step;
+    c.max_radiation_depth = p->max_radiation_depth;
+    c.max_absorption_depth = p->max_absorption_depth;
+    c.max_faraday_depth = p->max_faraday_depth;
+    c.max_steps = p->max_steps;
+    c.adaptive = p->adaptive;
+    c.integrator = integrator;
+    c.faraday_rotation = p->emission_selection.faraday_rotation;
+    c.nx = p->camera.nx;
+    c.ny = p->camera.ny;
+    c.cam_radius = p->camera.radius;
+    c.sin_inc = std::sin(p->camera.inclination);
+    c.cos_inc = std::cos(p->camera.inclination);
+    c.fov = p->camera.fov;
+    c.fov_y = p->camera.fov_y;
+    c.xspan = p->camera.xspan;
+    c.yspan = p->camera.yspan;
+    c.x_offset = p->camera.x_offset;
+    c.y_offset = p->camera.y_offset;
+    c.emission_scale = m.emission_scale;
+    c.absorption_scale = m.absorption_scale;
+    c.faraday_scale = m.faraday_scale;
+    c.max_pol_frac = m.max_pol_frac;
+    c.min_sin_theta = 1e-4;  // grmhd_grid.hpp:1149
+    c.fit = m.emission_type == KP_FIT_DEXTER ? 4 : 1;
+    c.fp32_radius = p->outer_radius + 2.0 * std::max(std::fabs(p->max_step), std::fabs(p->step));
+    c.nfreq = nfreq;
+    const double length_unit = grmhd_length_unit_cgs(m);
+    for (int f = 0; f < nfreq; ++f) {
+        const double fr = freqs ? freqs[f] : m.freq_cgs;
+        c.freq[f] = fr;
+        c.dlambda_scale[f] = length_unit / std::max(fr, 1.0);  // grmhd_grid.hpp:159-161
+    }
+    c.scene = kSceneGrmhdFmks;
+    c.fmks = FmksParams{p->mass, p->spin, p->fmks_startx1, p->fmks_hslope, p->fmks_mks_smooth,
+                        p->fmks_poly_alpha, p->fmks_poly_xt, p->fmks_poly_norm};
+    c.grid = grid;
+    return c;
+}
+
+}  // namespace kp

@@ -112,7 +112,7 @@ cudaError_t launch_wave_fp64(int phase, const WaveDesc& W, int nf_max, int block
 __global__ void __launch_bounds__(128) seed_fp64(const JobDesc* jobs, const SeedEntry* entries,
                                                 const long long* prefix, int nentries, RayRecord* pool,
                                                 unsigned* far_ids, unsigned* far_count) {
-    seed_body(jobs, entries, prefix, nentries, pool, far_ids, far_count);
+    seed_body<SceneRiaf>(jobs, entries, prefix, nentries, pool, far_ids, far_count);
 }
 
 cudaError_t launch_seed_fp64(const JobDesc* jobs, const SeedEntry* entries, const long long* prefix, int nentries,

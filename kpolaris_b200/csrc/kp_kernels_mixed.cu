@@ -46,7 +46,7 @@ cudaError_t launch_wave_mixed(int phase, const WaveDesc& W, int blocks, int thre
 __global__ void __launch_bounds__(128) seed_mixed(const JobDesc* jobs, const SeedEntry* entries,
                                                  const long long* prefix, int nentries, RayRecord* pool,
                                                  unsigned* far_ids, unsigned* far_count) {
-    seed_body(jobs, entries, prefix, nentries, pool, far_ids, far_count);
+    seed_body<SceneRiaf>(jobs, entries, prefix, nentries, pool, far_ids, far_count);
 }
 
 cudaError_t launch_seed_mixed(const JobDesc* jobs, const SeedEntry* entries, const long long* prefix, int nentries,

@@ -35,6 +35,17 @@ cudaError_t launch_seed_mixed(const JobDesc* jobs, const SeedEntry* entries, con
                               long long total, RayRecord* pool, unsigned* far_ids, unsigned* far_count,
                               cudaStream_t stream);
 
+// The GRMHD scene (FMKS metric, grid plasma), FP64 policy
+// (kp_kernels_grmhd.cu), its seed kernel and the derived-scalar precompute
+// (derived: [5][n1][n2][n3] device array).
+cudaError_t launch_wave_grmhd(int phase, const WaveDesc& W, int nf_max, int blocks, int threads,
+                              cudaStream_t stream);
+int wave_occupancy_grmhd(int phase, int nf_max, int threads);
+cudaError_t launch_seed_grmhd(const JobDesc* jobs, const SeedEntry* entries, const long long* prefix, int nentries,
+                              long long total, RayRecord* pool, unsigned* far_ids, unsigned* far_count,
+                              cudaStream_t stream);
+cudaError_t launch_grid_derived(const GridConsts& g, double* derived, int sms, cudaStream_t stream);
+
 // Threads per CTA of each phase kernel (its __launch_bounds__): the far
 // kernel runs two CTAs of 128 per SM, the near kernels one CTA of 256, so
 // that every resident warp of an SM steps through the same code region.

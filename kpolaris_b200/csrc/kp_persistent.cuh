@@ -127,11 +127,12 @@ __device__ __forceinline__ void queue_push(unsigned* ids, unsigned* count, bool 
 
 // Initial control state of a camera ray at the top of pass A
 // (pass_b.hpp:786-792).
+template<class SC>
 __device__ __forceinline__ void start_ray(LaneState& st, Ray& S, const JobDesc* J, int job, int pixel) {
     memset(&st, 0, sizeof(st));
     st.job = job;
     st.pixel = pixel;
-    S = camera_ray(J->c, J->frame, pixel);
+    S = SC::camera(J->c, J->frame, pixel);
     st.reason = kMaxSteps;
     st.h_current = -abs_val(J->c.step);
     st.mode = kAStep;
@@ -142,6 +143,7 @@ __device__ __forceinline__ void start_ray(LaneState& st, Ray& S, const JobDesc* 
 // initial record (pass-A loop top) and appends its id to the far queue.
 // entries: (job slot, first ray id, pixel count) with prefix sums of the
 // counts in `prefix` (nentries + 1 values).
+template<class SC>
 __device__ __forceinline__ void seed_body(const JobDesc* jobs, const SeedEntry* entries, const long long* prefix,
                                           int nentries, RayRecord* pool, unsigned* far_ids,
                                           unsigned* far_count) {
@@ -159,7 +161,7 @@ __device__ __forceinline__ void seed_body(const JobDesc* jobs, const SeedEntry* 
         id = unsigned(e.ray_base + pixel);
         LaneState st;
         Ray S;
-        start_ray(st, S, &jobs[e.slot], e.slot, pixel);
+        start_ray<SC>(st, S, &jobs[e.slot], e.slot, pixel);
         RayRecord& rec = pool[id];
         rec.S = S;
         memcpy(rec.st, &st, sizeof(LaneState));
@@ -173,7 +175,7 @@ __device__ __forceinline__ int phase_of(const ImageConsts& c, int in_b, double r
     return in_b ? kPhaseNearB : kPhaseNearA;
 }
 
-template<class P, int NF, int PHASE>
+template<class P, int NF, int PHASE, class SC = SceneRiaf>
 __device__ __forceinline__ void persistent_body(const WaveDesc& W) {
     constexpr bool kFar = PHASE == kPhaseFar;
     constexpr bool kPassA = PHASE != kPhaseNearB;   // pass-A steps run here
@@ -182,7 +184,7 @@ __device__ __forceinline__ void persistent_body(const WaveDesc& W) {
     constexpr bool kRad = PHASE == kPhaseNearB;     // radiative transfer (Stokes in registers)
     const unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
-    using RT = RadTraits<P>;
+    using RT = RadTraits<P, SC>;
     LaneState st;
     st.mode = kIdle;
     st.job = -1;
@@ -222,7 +224,7 @@ __device__ __forceinline__ void persistent_body(const WaveDesc& W) {
                     }
                     my_id = unsigned(id);
                     J = &W.jobs[lo];
-                    start_ray(st, S, J, lo, int(id - J->ray_begin));
+                    start_ray<SC>(st, S, J, lo, int(id - J->ray_begin));
                 } else if (W.budget > 0 && lane_jobs >= W.budget) {
                     // past the budget: hand the id on untouched (below)
                     my_id = W.in_ids[k - nfresh];
@@ -251,7 +253,7 @@ __device__ __forceinline__ void persistent_body(const WaveDesc& W) {
         if constexpr (kPassA) {
             if (active && st.mode == kAStep && st.rk_kind < 0) {
                 const ImageConsts& c = J->c;
-                const double r_bl = ks_radius(c.spin, S.x);
+                const double r_bl = SC::radius(c, S.x);
                 const int want_phase = phase_of(c, 0, r_bl);
                 if (want_phase != PHASE) {
                     dest = want_phase;
@@ -307,7 +309,7 @@ __device__ __forceinline__ void persistent_body(const WaveDesc& W) {
             if (st.reached || st.steps >= c.max_steps) {
                 st.mode = kDone;
             } else {
-                const double r_bl = ks_radius(c.spin, S.x);
+                const double r_bl = SC::radius(c, S.x);
                 const int want_phase = phase_of(c, 1, r_bl);
                 if (want_phase != PHASE) {
                     dest = want_phase;
@@ -347,12 +349,11 @@ __device__ __forceinline__ void persistent_body(const WaveDesc& W) {
         Ray next, mid;
         double err = 0.0;
         if (run) {
-            const double mass = J->c.mass, spin = J->c.spin;
             if (kCross && (st.mode == kACrossHi || st.mode == kACrossTrial)) {
                 const double hh = st.mode == kACrossHi ? st.full_h : st.full_h * st.trial;
-                rk_job<P, fp32>(J->c.adaptive ? kRkRK4x2 : kRkRK4, mass, spin, S, hh, next, mid, err);
+                rk_job<P, fp32, SC>(J->c.adaptive ? kRkRK4x2 : kRkRK4, J->c, S, hh, next, mid, err);
             } else {
-                rk_job<P, fp32>(st.rk_kind, mass, spin, S, st.h_try, next, mid, err);
+                rk_job<P, fp32, SC>(st.rk_kind, J->c, S, st.h_try, next, mid, err);
             }
             if (++lane_jobs > (1LL << 30)) {
                 st.reason = kInvalidState;
@@ -392,7 +393,7 @@ __device__ __forceinline__ void persistent_body(const WaveDesc& W) {
             if (accepted) {
                 // pass_b.hpp:864-937
                 st.rk_kind = -1;
-                const double next_r = ks_radius(c.spin, next.x);
+                const double next_r = SC::radius(c, next.x);
                 const double old_r = st.old_r;
                 if (!st.entered && next_r <= c.outer_radius) {
                     st.entered = 1;
@@ -418,7 +419,7 @@ __device__ __forceinline__ void persistent_body(const WaveDesc& W) {
                             best = S;
                             st.lo = 0.0;
                             st.hi = 1.0;
-                            st.flo = ks_radius(c.spin, S.x) - st.surf;
+                            st.flo = SC::radius(c, S.x) - st.surf;
                             if (st.flo == 0.0 || !finite_ray(next)) {
                                 st.pa_steps += 1;  // the event keeps the first state
                                 st.reason = crossing;
@@ -446,7 +447,7 @@ __device__ __forceinline__ void persistent_body(const WaveDesc& W) {
                 if (!finite_ray(next)) {
                     finish = true;
                 } else {
-                    const double fhi = ks_radius(c.spin, next.x) - st.surf;
+                    const double fhi = SC::radius(c, next.x) - st.surf;
                     if (!(fhi == fhi) || abs_val(fhi) >= kLarge) {
                         finish = true;
                     } else if (fhi == 0.0) {
@@ -461,7 +462,7 @@ __device__ __forceinline__ void persistent_body(const WaveDesc& W) {
                     }
                 }
             } else {
-                const double ft = finite_ray(next) ? ks_radius(c.spin, next.x) - st.surf : 0.0;
+                const double ft = finite_ray(next) ? SC::radius(c, next.x) - st.surf : 0.0;
                 if (!finite_ray(next) || !(ft == ft) || abs_val(ft) >= kLarge) {
                     st.hi = st.trial;
                     st.use_secant = 0;
@@ -525,7 +526,7 @@ __device__ __forceinline__ void persistent_body(const WaveDesc& W) {
                 if (!cam) {
                     // camera surface (pass_b.hpp:999-1028)
                     const double s0 = st.start_r - c.cam_radius;
-                    const double s1 = ks_radius(c.spin, next.x) - c.cam_radius;
+                    const double s1 = SC::radius(c, next.x) - c.cam_radius;
                     crosses = (s0 == 0.0 || s1 == 0.0) ? 1 : ((s0 < 0.0 && s1 > 0.0) || (s0 > 0.0 && s1 < 0.0));
                     if (crosses) {
                         const double denom = s0 - s1;
@@ -547,8 +548,8 @@ __device__ __forceinline__ void persistent_body(const WaveDesc& W) {
                 }
                 if (proceed) {
                     // radiation at the sample point (pass_b.hpp:1414-1496)
-                    const double sample_r = ks_radius(c.spin, sample.x);
-                    const double next_r = ks_radius(c.spin, next.x);
+                    const double sample_r = SC::radius(c, sample.x);
+                    const double next_r = SC::radius(c, next.x);
                     const double local_max_rs =
                         (c.max_radiation_step > 0.0 &&
                          (st.start_r <= c.outer_radius || sample_r <= c.outer_radius || next_r <= c.outer_radius))
@@ -631,7 +632,7 @@ __device__ __forceinline__ void persistent_body(const WaveDesc& W) {
                 }
             }
             o.reason = reason;
-            const Ray cam = camera_ray(c, J->frame, st.pixel);
+            const Ray cam = SC::camera(c, J->frame, st.pixel);
             double obs[NF][4];
             Stokes4<double> sd[NF];
             if constexpr (!kRad) {
@@ -641,7 +642,7 @@ __device__ __forceinline__ void persistent_body(const WaveDesc& W) {
 #pragma unroll
             for (int f = 0; f < NF; ++f)
                 sd[f] = st.in_b ? RT::result(stokes[f], c, f) : Stokes4<double>{0.0, 0.0, 0.0, 0.0};
-            finish_ray<double, NF>(c, cam, S, st.in_b, sd, o, obs);
+            finish_ray_scene<SC, NF>(c, cam, S, st.in_b, sd, o, obs);
             store_stokes_n<NF>(J->out, st.pixel, J->npix, c.nfreq, obs);
             store_diagnostics(J->out, st.pixel, o);
             if (W.job_done) atomicAdd(&W.job_done[st.job], 1u);

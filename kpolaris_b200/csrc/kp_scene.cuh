@@ -1,0 +1,154 @@
+// kp_scene.cuh -- what the wavefront engine needs of a spacetime and its
+// plasma, as compile-time scenes:
+//   SceneRiaf:  Cartesian Kerr-Schild metric, analytic RIAF plasma;
+//   SceneGrmhd: FMKS metric, GRMHD grid plasma.
+// Each scene gives the radial coordinate of the pass logic
+// (metric_domain_radius, src/geodesic/metric_domain.hpp:160-172), the
+// transport right-hand side, the pinhole camera ray, and the metric at a
+// point for the end-of-ray overlaps and diagnostics
+// (src/geodesic/pass_b.hpp:87-98, 1096-1113).
+#pragma once
+
+#include "kp_camera.cuh"
+#include "kp_fmks.cuh"
+#include "kp_geometry_f32.cuh"
+#include "kp_grmhd.cuh"
+#include "kp_trace_fp64.cuh"
+
+#include <type_traits>
+
+namespace kp {
+
+// Mixed policy marker types live in kp_engine.cuh; the scenes only need to
+// know whether FP32 contraction was requested.
+template<bool MIXED, bool FP32>
+__device__ __forceinline__ Ray riaf_rhs(double mass, double spin, const Ray& X) {
+    if constexpr (MIXED && FP32) return ks_rhs_factored<float>(mass, spin, X);
+    else if constexpr (MIXED) return ks_rhs_factored<double>(mass, spin, X);
+    else return ks_rhs(mass, spin, X);
+}
+
+struct SceneRiaf {
+    struct Metric {
+        KSMetricPoint w;
+        __device__ double dot(const D4& u, const D4& v) const { return ks_dot_at(w, u, v); }
+    };
+    __device__ static double radius(const ImageConsts& c, const D4& X) { return ks_radius(c.spin, X); }
+    template<bool MIXED, bool FP32>
+    __device__ static Ray rhs(const ImageConsts& c, const Ray& X) {
+        return riaf_rhs<MIXED, FP32>(c.mass, c.spin, X);
+    }
+    __device__ static Ray camera(const ImageConsts& c, const CameraFrame& f, int pixel) {
+        return camera_ray(c, f, pixel);
+    }
+    __device__ static Metric metric_at(const ImageConsts& c, const D4& X) { return Metric{ks_point(c.mass, c.spin, X)}; }
+};
+
+// initialize_pinhole_camera_ray (camera.hpp:485-513) in FMKS, from the
+// image's precomputed tetrad.
+static __device__ __noinline__ Ray fmks_camera_ray(const ImageConsts& c, const CameraFrame& f, int pixel) {
+    double g[4][4];
+    fmks_gcov(c.fmks, f.x, g);
+    double sx = 0.0, sy = 0.0;
+    pixel_offsets(pixel, c, sx, sy);
+    const double spatial_norm = sqrt(1.0 + sx * sx + sy * sy);
+    const double kt1 = sx / spatial_norm, kt2 = sy / spatial_norm, kt3 = 1.0 / spatial_norm;
+    Ray s;
+    s.x = f.x;
+    D4 sd;
+    for (int i = 0; i < 4; ++i) sd.v[i] = f.e1.v[i] * kt1 + f.e2.v[i] * kt2 + f.e3.v[i] * kt3;
+    for (int i = 0; i < 4; ++i) s.k.v[i] = f.e0.v[i] + sd.v[i];
+    for (int i = 0; i < 4; ++i) s.e1.v[i] = f.e1.v[i] - sd.v[i] * kt1;
+    {
+        const double n2 = dot_gm(g, s.e1, s.e1);
+        if (n2 > 0.0) {
+            const double inv = 1.0 / sqrt(n2);
+            for (int i = 0; i < 4; ++i) s.e1.v[i] *= inv;
+        }
+    }
+    for (int i = 0; i < 4; ++i) s.e2.v[i] = f.e2.v[i] - sd.v[i] * kt2;
+    {
+        const double denom = dot_gm(g, s.e1, s.e1);
+        if (abs_val(denom) > kTiny) {
+            const double k = dot_gm(g, s.e2, s.e1) / denom;
+            for (int i = 0; i < 4; ++i) s.e2.v[i] -= s.e1.v[i] * k;
+        }
+        const double n2 = dot_gm(g, s.e2, s.e2);
+        if (n2 > 0.0) {
+            const double inv = 1.0 / sqrt(n2);
+            for (int i = 0; i < 4; ++i) s.e2.v[i] *= inv;
+        }
+    }
+    return s;
+}
+
+struct SceneGrmhd {
+    struct Metric {
+        double g[4][4];
+        __device__ double dot(const D4& u, const D4& v) const { return dot_gm(g, u, v); }
+    };
+    __device__ static double radius(const ImageConsts&, const D4& X) { return fmks_radius(X); }
+    template<bool MIXED, bool FP32>
+    __device__ static Ray rhs(const ImageConsts& c, const Ray& X) {
+        return fmks_rhs(c.fmks, X);
+    }
+    __device__ static Ray camera(const ImageConsts& c, const CameraFrame& f, int pixel) {
+        return fmks_camera_ray(c, f, pixel);
+    }
+    __device__ static Metric metric_at(const ImageConsts& c, const D4& X) {
+        Metric m;
+        fmks_gcov(c.fmks, X, m.g);
+        return m;
+    }
+};
+
+// End of a ray for any scene: screen overlaps with the camera basis,
+// observer-basis Stokes (stokes_rotation.hpp:39-57) and the closure
+// diagnostics (finish_ray in kp_trace_fp64.cuh for the RIAF plain kernel).
+template<class S, int NF>
+__device__ __forceinline__ void finish_ray_scene(const ImageConsts& c, const Ray& cam, const Ray& state, int passed_b,
+                                                 Stokes4<double> (&stokes)[NF], PixelOut& o,
+                                                 double (&obs)[NF][4]) {
+    if constexpr (std::is_same<S, SceneRiaf>::value) {
+        // the plain kernel's own code, so the FP64 policy stays bit-identical to it
+        finish_ray<double, NF>(c, cam, state, passed_b, stokes, o, obs);
+        return;
+    }
+    const typename S::Metric m = S::metric_at(c, state.x);
+    if (passed_b) {
+        o.r11 = m.dot(cam.e1, state.e1);
+        o.r12 = m.dot(cam.e1, state.e2);
+        o.r21 = m.dot(cam.e2, state.e1);
+        o.r22 = m.dot(cam.e2, state.e2);
+    } else {
+        o.r11 = 1.0;
+        o.r12 = 0.0;
+        o.r21 = 0.0;
+        o.r22 = 1.0;
+    }
+    const double r11 = o.r11, r12 = o.r12, r21 = o.r21, r22 = o.r22;
+#pragma unroll
+    for (int f = 0; f < NF; ++f) {
+        if (passed_b) {
+            const double I = stokes[f].I, Q = stokes[f].Q, U = stokes[f].U, V = stokes[f].V;
+            obs[f][0] = I;
+            obs[f][1] = 0.5 * Q * (r11 * r11 - r12 * r12 - r21 * r21 + r22 * r22) + U * (r11 * r12 - r21 * r22);
+            obs[f][2] = Q * (r11 * r21 - r12 * r22) + U * (r11 * r22 + r12 * r21);
+            obs[f][3] = (r11 * r22 - r12 * r21) * V;
+        } else {
+            obs[f][0] = obs[f][1] = obs[f][2] = obs[f][3] = 0.0;
+        }
+    }
+    o.closure_x = spatial_distance(state.x, cam.x);
+    o.closure_k = vmaxabsdiff(state.k, cam.k);
+    o.final_null = m.dot(state.k, state.k);
+    double fe = abs_val(m.dot(state.k, state.k));
+    fe = max_val(fe, abs_val(m.dot(state.e1, state.k)));
+    fe = max_val(fe, abs_val(m.dot(state.e2, state.k)));
+    fe = max_val(fe, abs_val(m.dot(state.e1, state.e1) - 1.0));
+    fe = max_val(fe, abs_val(m.dot(state.e2, state.e2) - 1.0));
+    fe = max_val(fe, abs_val(m.dot(state.e1, state.e2)));
+    o.frame_error = fe;
+}
+
+}  // namespace kp

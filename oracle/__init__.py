@@ -25,6 +25,7 @@ HERE = Path(__file__).resolve().parent
 PORT_SO = HERE / "libkporacle.so"
 ULP_SO = HERE / "libkporacle_ulp.so"
 REF_SO = HERE / "_ref" / "libkpref.so"
+REF_ULP_SO = HERE / "_ref" / "libkpref_ulp.so"
 REFERENCE_SRC = Path(os.environ.get("KPOLARIS_REFERENCE_SRC", "/root/reference/src"))
 
 
@@ -61,7 +62,8 @@ def ref_available() -> bool:
 
 def lib(kind: str):
     """kind: 'port', 'port_ulp' (the port with every libm result moved by up
-    to +-2 ulp, see set_libm_perturbation) or 'reference'."""
+    to +-2 ulp, see set_libm_perturbation), 'reference' or 'reference_ulp'
+    (the reference's templates with the same perturbation)."""
     if kind in _libs:
         return _libs[kind]
     if kind in ("port", "port_ulp"):
@@ -74,12 +76,13 @@ def lib(kind: str):
             C.POINTER(C.c_double), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
             C.POINTER(_abi.ImageOut)]
         _declare_common(L, "kpo_")
-    elif kind == "reference":
-        if not REF_SO.exists():
+    elif kind in ("reference", "reference_ulp"):
+        so = REF_SO if kind == "reference" else REF_ULP_SO
+        if not so.exists():
             build(reference=True)
-        if not REF_SO.exists():
+        if not so.exists():
             raise FileNotFoundError("reference oracle not built (needs the reference source tree)")
-        L = C.CDLL(str(REF_SO))
+        L = C.CDLL(str(so))
         L.kpref_image_riaf_range.argtypes = [
             C.POINTER(_abi.PassAParams), C.POINTER(_abi.RIAFModel), C.c_int,
             C.POINTER(C.c_double), C.c_int, C.c_int, C.c_int, C.c_int,
@@ -91,9 +94,13 @@ def lib(kind: str):
     return L
 
 
-def set_libm_perturbation(seed: int) -> None:
-    """Selects the pseudo-random ulp sequence of the 'port_ulp' oracle."""
-    lib("port_ulp").kpo_set_libm_perturbation(C.c_ulonglong(seed))
+def set_libm_perturbation(seed: int, kind: str = "port_ulp") -> None:
+    """Selects the pseudo-random ulp sequence of the 'port_ulp' or
+    'reference_ulp' oracle."""
+    if kind == "reference_ulp":
+        lib(kind).kpref_set_libm_perturbation(C.c_ulonglong(seed))
+    else:
+        lib("port_ulp").kpo_set_libm_perturbation(C.c_ulonglong(seed))
 
 
 def _prefix(kind):
@@ -165,4 +172,90 @@ def transport_rhs_cks(mass, spin, state16, kind="port"):
     st = (C.c_double * 16)(*state16)
     out = (C.c_double * 16)()
     getattr(L, _prefix(kind) + "transport_rhs_cks")(mass, spin, st, out)
+    return np.array(out[:])
+
+
+def _declare_grmhd(L):
+    L.kpref_image_grmhd_range.argtypes = [
+        C.POINTER(_abi.PassAParams), C.POINTER(_abi.GrmhdModel), C.POINTER(C.c_double),
+        C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_double), C.c_int, C.c_int, C.c_int, C.c_int,
+        C.POINTER(_abi.ImageOut)]
+    L.kpref_grmhd_derived.argtypes = [C.POINTER(_abi.GrmhdModel), C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    L.kpref_transport_rhs_fmks.argtypes = [C.POINTER(_abi.PassAParams), C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    L.kpref_camera_ray_fmks.argtypes = [C.POINTER(_abi.PassAParams), C.c_int, C.POINTER(C.c_double)]
+    L.kpref_grmhd_coefficients.argtypes = [
+        C.POINTER(_abi.PassAParams), C.POINTER(_abi.GrmhdModel), C.POINTER(C.c_double), C.POINTER(C.c_double),
+        C.POINTER(C.c_double), C.c_double, C.POINTER(C.c_double)]
+
+
+def _dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def grmhd_derived(model, prims):
+    """The reference's derived-scalar precompute over float primitives
+    [8, n1, n2, n3]; returns [5, n1, n2, n3] FP64."""
+    L = lib("reference")
+    _declare_grmhd(L)
+    p = np.ascontiguousarray(prims, dtype=np.float64)
+    out = np.empty((5,) + p.shape[1:], dtype=np.float64)
+    if L.kpref_grmhd_derived(C.byref(model), _dp(p), _dp(out)) != 0:
+        raise RuntimeError(L.kpref_last_error().decode())
+    return out
+
+
+def image_grmhd(params, model, prims, derived, freqs, *, threads=0, pixel_begin=0, pixel_end=None, out=None,
+                kind="reference"):
+    """A GRMHD image (or pixel range) in FMKS with the reference's templates
+    (kind 'reference_ulp': the libm-perturbed build)."""
+    L = lib(kind)
+    _declare_grmhd(L)
+    npix = params.camera.nx * params.camera.ny
+    nfreq = len(freqs)
+    if out is None:
+        out = _abi.ImageHostData.allocate(npix, nfreq)
+    if pixel_end is None:
+        pixel_end = npix
+    p = np.ascontiguousarray(prims, dtype=np.float64)
+    d = None if derived is None else np.ascontiguousarray(derived, dtype=np.float64)
+    fa = (C.c_double * nfreq)(*freqs)
+    s = out.as_struct()
+    rc = L.kpref_image_grmhd_range(C.byref(params), C.byref(model), _dp(p), None if d is None else _dp(d), 1, fa,
+                                   nfreq, int(threads), int(pixel_begin), int(pixel_end), C.byref(s))
+    if rc != 0:
+        raise RuntimeError(L.kpref_last_error().decode())
+    return out
+
+
+def transport_rhs_fmks(params, state16):
+    L = lib("reference")
+    _declare_grmhd(L)
+    st = (C.c_double * 16)(*state16)
+    out = (C.c_double * 16)()
+    if L.kpref_transport_rhs_fmks(C.byref(params), st, out) != 0:
+        raise RuntimeError(L.kpref_last_error().decode())
+    return np.array(out[:])
+
+
+def grmhd_coefficients(params, model, prims, derived, state16, freq):
+    """The reference grid model's 11 transfer coefficients at one FMKS
+    transport state (x, k, e1, e2) and frequency."""
+    L = lib("reference")
+    _declare_grmhd(L)
+    p = np.ascontiguousarray(prims, dtype=np.float64)
+    d = None if derived is None else np.ascontiguousarray(derived, dtype=np.float64)
+    st = (C.c_double * 16)(*state16)
+    out = (C.c_double * 11)()
+    if L.kpref_grmhd_coefficients(C.byref(params), C.byref(model), _dp(p), None if d is None else _dp(d), st,
+                                  float(freq), out) != 0:
+        raise RuntimeError(L.kpref_last_error().decode())
+    return np.array(out[:])
+
+
+def camera_ray_fmks(params, pixel):
+    L = lib("reference")
+    _declare_grmhd(L)
+    out = (C.c_double * 16)()
+    if L.kpref_camera_ray_fmks(C.byref(params), int(pixel), out) != 0:
+        raise RuntimeError(L.kpref_last_error().decode())
     return np.array(out[:])

@@ -15,7 +15,9 @@
 
 #include "geodesic/pass_b.hpp"
 #include "geometry/kerr_boyer_lindquist.hpp"
+#include "geometry/kerr_fmks.hpp"
 #include "geometry/kerr_schild_cartesian.hpp"
+#include "model/grmhd.hpp"
 #include "model/riaf.hpp"
 
 #include "kpolaris_b200.h"
@@ -117,14 +119,17 @@ void store_common(kp_image_out* out, int pixel, const Overlap& ov, Real closure_
     out->reason[pixel] = reason;
 }
 
-template<class Metric>
+template<class Metric, class Model>
 void run_metric(const kpolaris::PassAParams<Real>& pa,
-                const kpolaris::RIAFAnalyticRadiationModel<Real>& model,
+                const Model& model,
                 int radiation_substeps, const double* freqs, int nfreq,
                 const Metric& metric, int pixel_begin, int pixel_end, kp_image_out* out) {
     const int npix = pa.camera.nx * pa.camera.ny;
 #pragma omp parallel for schedule(dynamic)
     for (int pixel = pixel_begin; pixel < pixel_end; ++pixel) {
+#ifdef KPREF_PERTURB_LIBM
+        kpref_ulp::seed_pixel(pixel);
+#endif
         if (nfreq == 1) {
             auto m = model;
             if (freqs) m.freq_cgs = freqs[0];
@@ -158,6 +163,59 @@ void run_metric(const kpolaris::PassAParams<Real>& pa,
     }
 }
 
+// GRMHDGridRadiationModel over host arrays: primitives widened from FP32,
+// derived scalars (if given) as FP64.  Views are non-owning.
+kpolaris::GRMHDGridRadiationModel<Real> to_grmhd(const kp_grmhd_model& m, const double* prims,
+                                                 const double* derived) {
+    kpolaris::GRMHDGridRadiationModel<Real> out;
+    out.n1 = m.n1;
+    out.n2 = m.n2;
+    out.n3 = m.n3;
+    out.spin = m.spin;
+    out.gam = m.gam;
+    out.startx1 = m.startx1;
+    out.startx2 = m.startx2;
+    out.startx3 = m.startx3;
+    out.dx1 = m.dx1;
+    out.dx2 = m.dx2;
+    out.dx3 = m.dx3;
+    out.r_in = m.r_in;
+    out.r_out = m.r_out;
+    out.hslope = m.hslope;
+    out.mks_smooth = m.mks_smooth;
+    out.poly_alpha = m.poly_alpha;
+    out.poly_xt = m.poly_xt;
+    out.poly_norm = m.poly_norm;
+    out.freq_cgs = m.freq_cgs;
+    out.mbh_solar = m.mbh_solar;
+    out.M_unit = m.M_unit;
+    out.trat_small = m.trat_small;
+    out.trat_large = m.trat_large;
+    out.beta_crit = m.beta_crit;
+    out.sigma_cut = m.sigma_cut;
+    out.sigma_cut_high = m.sigma_cut_high;
+    out.ne_factor = m.ne_factor;
+    out.emission_type = m.emission_type;
+    out.emission_scale = m.emission_scale;
+    out.absorption_scale = m.absorption_scale;
+    out.faraday_scale = m.faraday_scale;
+    out.max_pol_frac = m.max_pol_frac;
+    const size_t ncell = size_t(m.n1) * size_t(m.n2) * size_t(m.n3);
+    out.prims = Kokkos::View<Real*>(const_cast<double*>(prims), 8 * ncell);
+    out.has_derived_scalars = derived ? 1 : 0;
+    if (derived) out.derived_scalars = Kokkos::View<Real*>(const_cast<double*>(derived), 5 * ncell);
+    out.data_coordinate_system = static_cast<int>(kpolaris::CoordinateSystem::FMKS);
+    out.radial_coordinate_log = 1;
+    out.native_coordinate_transform = 0;
+    out.precomputed_fluid_state = 0;
+    return out;
+}
+
+kpolaris::KerrFMKSMetric<Real> fmks_metric(const kpolaris::PassAParams<Real>& pa) {
+    return kpolaris::KerrFMKSMetric<Real>(pa.mass, pa.spin, pa.fmks_startx1, pa.fmks_hslope, pa.fmks_mks_smooth,
+                                          pa.fmks_poly_alpha, pa.fmks_poly_xt, pa.fmks_poly_norm);
+}
+
 thread_local char g_error[512];
 
 int fail(const char* msg) {
@@ -172,6 +230,15 @@ extern "C" {
 const char* kpref_last_error(void) { return g_error; }
 
 int kpref_max_frequencies(void) { return KPOLARIS_MAX_FREQUENCIES; }
+
+// Selects the ulp sequence of the libm-perturbed build (no-op otherwise).
+void kpref_set_libm_perturbation(unsigned long long seed) {
+#ifdef KPREF_PERTURB_LIBM
+    kpref_ulp::g_seed = seed;
+#else
+    (void)seed;
+#endif
+}
 
 // Runs pixels [pixel_begin, pixel_end) of a RIAF image with `threads` OpenMP
 // threads (0 = all).  Only the selected pixels of *out are written.
@@ -292,6 +359,136 @@ int kpref_transport_rhs_cks(double mass, double spin, const double* state16, dou
         d16[8 + mu] = d.e1[mu];
         d16[12 + mu] = d.e2[mu];
     }
+    return KP_OK;
+}
+
+// GRMHD image over a pixel range in FMKS with the reference's grid model
+// (run_grmhd_image's FMKS backend, src/image/grmhd.cpp:22-59).
+int kpref_image_grmhd_range(const kp_pass_a_params* params, const kp_grmhd_model* model, const double* prims,
+                            const double* derived, int radiation_substeps, const double* freqs, int nfreq,
+                            int threads, int pixel_begin, int pixel_end, kp_image_out* out) {
+    if (!params || !model || !prims || !out) return fail("null argument");
+    if (nfreq < 1 || nfreq > KPOLARIS_MAX_FREQUENCIES) return fail("nfreq out of range");
+    const int npix = params->camera.nx * params->camera.ny;
+    if (pixel_begin < 0 || pixel_end > npix || pixel_begin > pixel_end) return fail("pixel range out of bounds");
+    if (threads > 0) omp_set_num_threads(threads);
+    const auto pa = to_pass_a(*params);
+    if (pa.coordinate_system != kpolaris::CoordinateSystem::FMKS) return fail("GRMHD oracle is built for FMKS only");
+    auto grmhd = to_grmhd(*model, prims, derived);
+    if (nfreq == 1 && freqs) grmhd.freq_cgs = freqs[0];
+    run_metric(pa, grmhd, radiation_substeps, freqs, nfreq, fmks_metric(pa), pixel_begin, pixel_end, out);
+    return KP_OK;
+}
+
+// The loaders' derived-scalar precompute (kharma_loader.cpp:261-362),
+// restated over the reference model's own helpers (native_fluid_metric,
+// lower_native, rho_unit_cgs, b_unit_cgs).  out: [5][n1][n2][n3].
+int kpref_grmhd_derived(const kp_grmhd_model* model, const double* prims, double* out) {
+    if (!model || !prims || !out) return fail("null argument");
+    const auto m = to_grmhd(*model, prims, nullptr);
+    const Real mp = Real(1.67262171e-24), me = Real(9.1093826e-28), mp_me = mp / me;
+    const Real game = Real(4) / Real(3), gamp = Real(5) / Real(3);
+    const int ncell = m.n1 * m.n2 * m.n3;
+#pragma omp parallel for schedule(static)
+    for (int p = 0; p < ncell; ++p) {
+        const int k = p % m.n3;
+        const int j = (p / m.n3) % m.n2;
+        const int i = p / (m.n2 * m.n3);
+        const Real x1 = m.startx1 + (Real(i) + Real(0.5)) * m.dx1;
+        const Real x2 = m.startx2 + (Real(j) + Real(0.5)) * m.dx2;
+        const Real r = std::exp(x1);
+        const Real th = m.fmks_theta_from_x2(x1, x2);
+        Real gcov[4][4], gcon0[4];
+        m.native_fluid_metric(x1, x2, r, th, gcov, gcon0);
+        const Real rho = m.prim(0, i, j, k), uu = m.prim(1, i, j, k);
+        const kpolaris::Vec4<Real> v(Real(0), m.prim(2, i, j, k), m.prim(3, i, j, k), m.prim(4, i, j, k));
+        Real sn = Real(0);
+        for (int a = 1; a < 4; ++a)
+            for (int b = 1; b < 4; ++b) sn += gcov[a][b] * v[a] * v[b];
+        const Real vfac = std::sqrt(kpolaris::max_val(-Real(1) / gcon0[0] * (Real(1) + kpolaris::abs_val(sn)), Real(0)));
+        kpolaris::Vec4<Real> ucon;
+        ucon[0] = -vfac * gcon0[0];
+        for (int a = 1; a < 4; ++a) ucon[a] = v[a] - vfac * gcon0[a];
+        const kpolaris::Vec4<Real> ucov = m.lower_native(gcov, ucon);
+        const kpolaris::Vec4<Real> B(Real(0), m.prim(5, i, j, k), m.prim(6, i, j, k), m.prim(7, i, j, k));
+        Real udotB = Real(0);
+        for (int a = 1; a < 4; ++a) udotB += ucov[a] * B[a];
+        kpolaris::Vec4<Real> bcon;
+        bcon[0] = udotB;
+        for (int a = 1; a < 4; ++a) bcon[a] = (B[a] + ucon[a] * udotB) / kpolaris::max_val(ucon[0], Real(1e-300));
+        const kpolaris::Vec4<Real> bcov = m.lower_native(gcov, bcon);
+        Real bsq = Real(0);
+        for (int a = 0; a < 4; ++a) bsq += bcon[a] * bcov[a];
+        bsq = kpolaris::max_val(kpolaris::abs_val(bsq), Real(1e-40));
+        const Real beta = (m.gam - Real(1)) * uu / (Real(0.5) * bsq);
+        const Real sigma = bsq / kpolaris::max_val(rho, Real(1e-300));
+        const Real betasq = beta * beta / kpolaris::max_val(m.beta_crit * m.beta_crit, Real(1e-40));
+        const Real trat = (m.trat_large * betasq + m.trat_small) / (Real(1) + betasq);
+        const Real tu = mp_me * (game - Real(1)) * (gamp - Real(1)) / ((gamp - Real(1)) + (game - Real(1)) * trat);
+        const size_t nc = size_t(ncell);
+        out[0 * nc + size_t(p)] = rho * m.rho_unit_cgs() / (mp + me) * m.ne_factor;
+        out[1 * nc + size_t(p)] = kpolaris::max_val(tu * uu / kpolaris::max_val(rho, Real(1e-300)), Real(1e-3));
+        out[2 * nc + size_t(p)] = std::sqrt(bsq) * m.b_unit_cgs();
+        out[3 * nc + size_t(p)] = sigma;
+        out[4 * nc + size_t(p)] = beta;
+    }
+    return KP_OK;
+}
+
+// transport_rhs of KerrFMKSMetric (kerr_fmks.hpp:455-479).
+int kpref_transport_rhs_fmks(const kp_pass_a_params* params, const double* state16, double* d16) {
+    if (!params || !state16 || !d16) return fail("null argument");
+    const auto metric = fmks_metric(to_pass_a(*params));
+    kpolaris::TransportState<Real> s;
+    for (int mu = 0; mu < 4; ++mu) {
+        s.x[mu] = state16[mu];
+        s.k[mu] = state16[4 + mu];
+        s.e1[mu] = state16[8 + mu];
+        s.e2[mu] = state16[12 + mu];
+    }
+    const auto d = kpolaris::transport_rhs(metric, s);
+    for (int mu = 0; mu < 4; ++mu) {
+        d16[mu] = d.x[mu];
+        d16[4 + mu] = d.k[mu];
+        d16[8 + mu] = d.e1[mu];
+        d16[12 + mu] = d.e2[mu];
+    }
+    return KP_OK;
+}
+
+// The FMKS pinhole camera ray of a pixel (camera.hpp:485-513).
+int kpref_camera_ray_fmks(const kp_pass_a_params* params, int pixel, double* state16) {
+    if (!params || !state16) return fail("null argument");
+    const auto pa = to_pass_a(*params);
+    const auto s = kpolaris::initialize_camera_ray(fmks_metric(pa), pixel, pa.camera);
+    for (int mu = 0; mu < 4; ++mu) {
+        state16[mu] = s.x[mu];
+        state16[4 + mu] = s.k[mu];
+        state16[8 + mu] = s.e1[mu];
+        state16[12 + mu] = s.e2[mu];
+    }
+    return KP_OK;
+}
+
+// GRMHD transfer coefficients at a transport state in FMKS
+// (GRMHDGridRadiationModel::coefficients, grmhd_grid.hpp:1091-1240) at the
+// model's freq_cgs = freq.  out11 = jI jQ jU jV aI aQ aU aV rQ rU rV.
+int kpref_grmhd_coefficients(const kp_pass_a_params* params, const kp_grmhd_model* model, const double* prims,
+                             const double* derived, const double* state16, double freq, double* out11) {
+    if (!params || !model || !prims || !state16 || !out11) return fail("null argument");
+    const auto pa = to_pass_a(*params);
+    auto grmhd = to_grmhd(*model, prims, derived);
+    grmhd.freq_cgs = freq;
+    kpolaris::TransportState<Real> s;
+    for (int mu = 0; mu < 4; ++mu) {
+        s.x[mu] = state16[mu];
+        s.k[mu] = state16[4 + mu];
+        s.e1[mu] = state16[8 + mu];
+        s.e2[mu] = state16[12 + mu];
+    }
+    const auto c = grmhd.coefficients(fmks_metric(pa), s, Real(0.5));
+    const double v[11] = {c.jI, c.jQ, c.jU, c.jV, c.aI, c.aQ, c.aU, c.aV, c.rQ, c.rU, c.rV};
+    std::memcpy(out11, v, sizeof(v));
     return KP_OK;
 }
 

@@ -18,22 +18,51 @@
 #define KOKKOS_FUNCTION
 #define KOKKOS_LAMBDA [=]
 
+#ifdef KPREF_PERTURB_LIBM
+// Conditioning probe (the _ref/libkpref_ulp.so build): every transcendental
+// result below is moved by a pseudo-random whole number of ulps in [-2, 2],
+// a fixed sequence per pixel and seed (kpref_perturb_pixel).  sqrt, floor
+// and ceil are correctly rounded everywhere and stay exact.
+namespace kpref_ulp {
+inline unsigned long long g_seed = 0;
+inline thread_local unsigned long long t_rng = 1;
+inline void seed_pixel(int pixel) {
+    t_rng = 0x9E3779B97F4A7C15ull * static_cast<unsigned long long>(pixel + 1) +
+            0xD1B54A32D192ED03ull * (g_seed + 1);
+    if (!t_rng) t_rng = 1;
+}
+template<class T> inline T perturb(T r) {
+    if (!(r == r) || r == T(0) || r - r != T(0)) return r;
+    t_rng ^= t_rng << 13;
+    t_rng ^= t_rng >> 7;
+    t_rng ^= t_rng << 17;
+    const int k = static_cast<int>(t_rng % 5ull) - 2;
+    for (int i = 0; i < k; ++i) r = std::nextafter(r, T(INFINITY));
+    for (int i = 0; i > k; --i) r = std::nextafter(r, -T(INFINITY));
+    return r;
+}
+}  // namespace kpref_ulp
+#define KPREF_P(expr) kpref_ulp::perturb(expr)
+#else
+#define KPREF_P(expr) (expr)
+#endif
+
 namespace Kokkos {
 
 template<class T> inline T sqrt(T x) { return std::sqrt(x); }
-template<class T> inline T cbrt(T x) { return std::cbrt(x); }
-template<class T> inline T exp(T x) { return std::exp(x); }
-template<class T> inline T log(T x) { return std::log(x); }
-template<class T> inline T sin(T x) { return std::sin(x); }
-template<class T> inline T cos(T x) { return std::cos(x); }
-template<class T> inline T tan(T x) { return std::tan(x); }
-template<class T> inline T tanh(T x) { return std::tanh(x); }
-template<class T> inline T acos(T x) { return std::acos(x); }
-template<class T> inline T atan(T x) { return std::atan(x); }
-template<class T> inline T atan2(T y, T x) { return std::atan2(y, x); }
+template<class T> inline T cbrt(T x) { return KPREF_P(std::cbrt(x)); }
+template<class T> inline T exp(T x) { return KPREF_P(std::exp(x)); }
+template<class T> inline T log(T x) { return KPREF_P(std::log(x)); }
+template<class T> inline T sin(T x) { return KPREF_P(std::sin(x)); }
+template<class T> inline T cos(T x) { return KPREF_P(std::cos(x)); }
+template<class T> inline T tan(T x) { return KPREF_P(std::tan(x)); }
+template<class T> inline T tanh(T x) { return KPREF_P(std::tanh(x)); }
+template<class T> inline T acos(T x) { return KPREF_P(std::acos(x)); }
+template<class T> inline T atan(T x) { return KPREF_P(std::atan(x)); }
+template<class T> inline T atan2(T y, T x) { return KPREF_P(std::atan2(y, x)); }
 template<class T> inline T floor(T x) { return std::floor(x); }
 template<class T> inline T ceil(T x) { return std::ceil(x); }
-template<class T, class U> inline auto pow(T x, U y) { return std::pow(x, y); }
+template<class T, class U> inline auto pow(T x, U y) { return KPREF_P(std::pow(x, y)); }
 
 inline void abort(const char* msg) {
     std::fprintf(stderr, "Kokkos::abort: %s\n", msg);

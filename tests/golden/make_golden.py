@@ -8,6 +8,15 @@ Each image fixture stores the workload description (a JSON string that
 tests/golden_cases.py turns back into parameters) and every output array of
 the reference run.  The coefficient fixture stores thermal-synchrotron and
 RIAF coefficients and single Strang transfer steps at seeded points.
+
+Each GRMHD fixture (grmhd_*.npz, tests/golden_cases.py GRMHD_CASES) stores
+the case description, the sha256 of the generated FP32 primitives, the
+reference's derived scalars at 2048 seeded cells plus per-field sums over
+all cells, every output array of the reference image, and the image's +-2-ulp
+libm conditioning measured on the reference's own templates
+(oracle/_ref/libkpref_ulp.so) as parallel arrays cond_keys / cond_vals.
+
+    python tests/golden/make_golden.py --grmhd     # GRMHD fixtures only
 """
 from __future__ import annotations
 
@@ -22,13 +31,40 @@ sys.path.insert(0, str(ROOT))
 sys.path.insert(0, str(ROOT / "tests"))
 
 import oracle  # noqa: E402
-from golden_cases import IMAGE_CASES, build_case, coefficient_points, transfer_points  # noqa: E402
+from golden_cases import (IMAGE_CASES, GRMHD_CASES, build_case, build_grmhd_case,  # noqa: E402
+                          coefficient_points, grmhd_conditioning_of, prims_digest, transfer_points)
 
 OUT = Path(__file__).resolve().parent
 
 
+def cond_key(k) -> str:
+    return f"{k[0]}:{k[1]}" if isinstance(k, tuple) else str(k)
+
+
+def make_grmhd():
+    for name, spec in GRMHD_CASES.items():
+        prims, model, params, freqs = build_grmhd_case(spec)
+        derived = oracle.grmhd_derived(model, prims)
+        rng = np.random.default_rng(20260)
+        ncell = derived.shape[1] * derived.shape[2] * derived.shape[3]
+        cells = np.sort(rng.choice(ncell, size=min(2048, ncell), replace=False))
+        flat = derived.reshape(5, -1)
+        res = oracle.image_grmhd(params, model, prims, derived, freqs, threads=0)
+        cond = grmhd_conditioning_of(params, model, prims, derived, freqs, res.arrays)
+        keys = sorted(cond, key=cond_key)
+        np.savez_compressed(OUT / f"{name}.npz", spec=json.dumps(spec), prims_sha256=prims_digest(prims),
+                            derived_cells=cells, derived_values=flat[:, cells], derived_sums=flat.sum(axis=1),
+                            cond_keys=np.array([cond_key(k) for k in keys]),
+                            cond_vals=np.array([cond[k] for k in keys]), **res.arrays)
+        print(name, np.bincount(res.reason, minlength=8)[:8],
+              {cond_key(k): "%.1e" % cond[k] for k in keys if k[0] in ("flux", "image_i")})
+
+
 def main():
     oracle.build(reference=True)
+    if "--grmhd" in sys.argv[1:]:
+        make_grmhd()
+        return
     for name, spec in IMAGE_CASES.items():
         params, model, freqs = build_case(spec)
         res = oracle.image_riaf(params, model, freqs, kind="reference", threads=0)
@@ -48,6 +84,7 @@ def main():
                         thermal_out=np.array(th_out), transfer_in=np.array(tr_in),
                         transfer_out=np.array(tr_out))
     print("coefficients", len(th_in), len(tr_in))
+    make_grmhd()
 
 
 if __name__ == "__main__":

@@ -121,22 +121,97 @@ def libm_conditioning_of(params, model, freqs, ref, seeds=(1, 2, 3), integrator=
     import oracle
     from kpolaris_b200 import _abi
 
+    def run(seed):
+        oracle.set_libm_perturbation(seed)
+        return oracle.image_riaf(params, model, freqs, kind="port_ulp", threads=4, integrator=integrator)
+
+    return conditioning_over(run, ref, seeds)
+
+
+def conditioning_over(run, ref, seeds):
+    """The spread of `run(seed)` (an ImageHostData) around `ref` as
+    libm_conditioning_of defines it; NaN entries (present in both) are
+    skipped."""
+    import numpy as np
+
+    from kpolaris_b200 import _abi
+
     ok = ref["reason"] == 1
     out = {}
     for seed in seeds:
-        oracle.set_libm_perturbation(seed)
-        res = oracle.image_riaf(params, model, freqs, kind="port_ulp", threads=4, integrator=integrator)
+        res = run(seed)
         for key in _abi.IMAGE_FIELDS:
             for f in range(ref[key].shape[0]):
-                scale = np.max(np.abs(ref[key][f]))
-                d = np.max(np.abs(res.arrays[key][f] - ref[key][f]))
+                scale = np.nanmax(np.abs(ref[key][f]), initial=0.0)
+                diff = np.abs(res.arrays[key][f] - ref[key][f])
+                d = float(np.max(diff[np.isfinite(diff)], initial=0.0))
                 v = d / scale if scale > 0 else d
                 out[(key, f)] = max(out.get((key, f), 0.0), v)
         for f in range(ref["image_i"].shape[0]):
-            total = ref["image_i"][f].sum()
-            v = abs(res.image_i[f].sum() / total - 1.0) if total > 0 else 0.0
+            total = np.nansum(ref["image_i"][f])
+            v = abs(np.nansum(res.image_i[f]) / total - 1.0) if total > 0 else 0.0
             out[("flux", f)] = max(out.get(("flux", f), 0.0), v)
         for key in _abi.DIAG_FIELDS:
             d = np.abs(res.arrays[key][ok] - ref[key][ok])
             out[key] = max(out.get(key, 0.0), float(d.max()) if d.size else 0.0)
     return out
+
+
+# GRMHD cases: a seeded FM torus (kpolaris_b200.synthetic.fm_torus) on a
+# small FMKS grid, imaged in FMKS with the reference's grid model.  Fixtures
+# store the reference outputs and their +-2-ulp libm conditioning (the
+# reference's own templates, built with perturbed libm forwards), so the GPU
+# tests need neither the reference tree nor its build.
+GRMHD_CASES = {
+    # adaptive step-doubling RK4 (tol 1e-8), 230 GHz, i = 163 deg, 16^2
+    "grmhd_adaptive_16": {"grid": [48, 32, 16], "n": 16, "adaptive": 1, "step": 0.025,
+                          "max_steps": 400000, "freqs": [230.0e9]},
+    # fixed-step RK4 h = 0.05: reasons and step counts bit-exact
+    "grmhd_fixed_16": {"grid": [48, 32, 16], "n": 16, "adaptive": 0, "step": 0.05,
+                       "max_steps": 40000, "freqs": [230.0e9]},
+    # four frequencies on one geodesic, non-square 12x10, Pandya fit, R_high 20
+    "grmhd_multifreq_12x10": {"grid": [48, 32, 16], "nx": 12, "ny": 10, "adaptive": 1, "step": 0.025,
+                              "max_steps": 400000, "freqs": [86.0e9, 230.0e9, 345.0e9, 690.0e9],
+                              "fit": 1, "trat_large": 20.0},
+    # edge-on, wider field, coarse fixed step with a step budget some rays
+    # exhaust (max_steps; the reference leaves NaN Q/U/V on some of them)
+    "grmhd_edge_maxsteps_8": {"grid": [48, 32, 16], "n": 8, "inclination_deg": 90.0, "xspan": 30.0,
+                              "adaptive": 0, "step": 0.5, "max_steps": 4000, "freqs": [230.0e9]},
+}
+
+
+def build_grmhd_case(spec: dict):
+    """(prims, model, params, freqs) of a GRMHD case."""
+    from kpolaris_b200 import synthetic
+
+    n1, n2, n3 = spec["grid"]
+    prims, model = synthetic.fm_torus(n1, n2, n3)
+    model.trat_large = spec.get("trat_large", 40.0)
+    model.emission_type = spec.get("fit", _abi.FIT_DEXTER)
+    nx = spec.get("nx", spec.get("n"))
+    ny = spec.get("ny", spec.get("n"))
+    params = synthetic.fmks_pass_a_params(
+        model, nx, ny, inclination_deg=spec.get("inclination_deg", 163.0), xspan=spec.get("xspan", 20.0),
+        adaptive=spec["adaptive"], step=spec["step"], max_steps=spec["max_steps"])
+    return prims, model, params, list(spec["freqs"])
+
+
+def grmhd_conditioning_of(params, model, prims, derived, freqs, ref, seeds=tuple(range(1, 9))):
+    """libm_conditioning_of for a GRMHD image, measured on the reference's
+    own templates with perturbed libm (oracle kind 'reference_ulp'), over
+    eight seeds: the fixtures pay for it once, and the Faraday-thick 86 GHz
+    channels need the larger sample to find their worst case."""
+    import oracle
+
+    def run(seed):
+        oracle.set_libm_perturbation(seed, "reference_ulp")
+        return oracle.image_grmhd(params, model, prims, derived, freqs, threads=0, kind="reference_ulp")
+
+    return conditioning_over(run, ref, seeds)
+
+
+def prims_digest(prims) -> str:
+    """sha256 of the FP32 primitive bytes (generator determinism)."""
+    import hashlib
+
+    return hashlib.sha256(np.ascontiguousarray(prims, dtype=np.float32).tobytes()).hexdigest()

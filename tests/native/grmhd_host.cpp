@@ -1,0 +1,85 @@
+// Host build of the GRMHD/FMKS device code (kpolaris_b200/csrc) as a shared
+// library, so the CPU tests can compare each piece with the reference's own
+// templates point by point: the FMKS transport RHS, the FMKS pinhole camera
+// ray, the per-cell derived-scalar precompute, and the grid plasma sample +
+// transfer coefficients at a transport state.  Arrays use the layouts of the
+// C ABI (prims [8][n1][n2][n3] FP32, derived [5][n1][n2][n3] FP64, transport
+// states x[4] k[4] e1[4] e2[4]).
+#include <cmath>
+#include <cstring>
+#define __host__
+#define __device__
+#define __global__
+#define __forceinline__ inline
+#define __noinline__
+#include "kp_scene.cuh"
+#include "kp_grmhd_setup.h"
+
+namespace {
+
+kp::Ray ray_of(const double* s) {
+    kp::Ray r;
+    for (int m = 0; m < 4; ++m) {
+        r.x.v[m] = s[m];
+        r.k.v[m] = s[4 + m];
+        r.e1.v[m] = s[8 + m];
+        r.e2.v[m] = s[12 + m];
+    }
+    return r;
+}
+
+void store(const kp::Ray& r, double* s) {
+    for (int m = 0; m < 4; ++m) {
+        s[m] = r.x.v[m];
+        s[4 + m] = r.k.v[m];
+        s[8 + m] = r.e1.v[m];
+        s[12 + m] = r.e2.v[m];
+    }
+}
+
+kp::FmksParams fmks_of(const kp_pass_a_params* p) {
+    return kp::FmksParams{p->mass, p->spin, p->fmks_startx1, p->fmks_hslope, p->fmks_mks_smooth,
+                          p->fmks_poly_alpha, p->fmks_poly_xt, p->fmks_poly_norm};
+}
+
+}  // namespace
+
+extern "C" {
+
+void h_fmks_rhs(const kp_pass_a_params* p, const double* s16, double* d16) {
+    store(kp::fmks_rhs(fmks_of(p), ray_of(s16)), d16);
+}
+
+void h_camera_ray_fmks(const kp_pass_a_params* p, int pixel, double* s16) {
+    kp_grmhd_model m;
+    std::memset(&m, 0, sizeof(m));
+    const kp::ImageConsts c = kp::image_consts_fmks(p, m, kp::GridConsts{}, nullptr, 1, 0);
+    kp::CameraFrame f;
+    kp::fmks_camera_frame(c.fmks, p->camera.radius, p->camera.inclination, f.x, f.e0, f.e1, f.e2, f.e3);
+    store(kp::fmks_camera_ray(c, f, pixel), s16);
+}
+
+void h_grmhd_derived(const kp_grmhd_model* m, const float* prims, double* out) {
+    const kp::GridConsts g = kp::grid_consts_of(*m, prims, nullptr);
+    const size_t ncell = size_t(m->n1) * size_t(m->n2) * size_t(m->n3);
+    for (int i = 0; i < m->n1; ++i)
+        for (int j = 0; j < m->n2; ++j)
+            for (int k = 0; k < m->n3; ++k) {
+                double v[kp::kNumDerived];
+                kp::grid_derived_cell(g, i, j, k, v);
+                const size_t cell = (size_t(i) * size_t(m->n2) + size_t(j)) * size_t(m->n3) + size_t(k);
+                for (int q = 0; q < kp::kNumDerived; ++q) out[size_t(q) * ncell + cell] = v[q];
+            }
+}
+
+void h_grmhd_coefficients(const kp_pass_a_params* p, const kp_grmhd_model* m, const float* prims,
+                          const double* derived, const double* s16, double freq, double* out11) {
+    const kp::GridConsts g = kp::grid_consts_of(*m, prims, derived);
+    const kp::ImageConsts c = kp::image_consts_fmks(p, *m, g, &freq, 1, 0);
+    const kp::GrmhdSample smp = kp::grmhd_sample(c, ray_of(s16));
+    const kp::Coeffs<double> o = kp::grmhd_coefficients(c, smp, freq);
+    const double v[11] = {o.jI, o.jQ, o.jU, o.jV, o.aI, o.aQ, o.aU, o.aV, o.rQ, o.rU, o.rV};
+    std::memcpy(out11, v, sizeof(v));
+}
+
+}  // extern "C"
