@@ -446,7 +446,7 @@ int ensure_job_table(DeviceState* dev, int njobs) {
 // dev->h_jobs (total rays): uploads them, grows the record pool, launches
 // cycles of (far, near-A, near-B) until no ray is left and checks the status
 // word.  The caller holds g_mutex.
-enum : int { kFamilyRiafFP64 = 0, kFamilyRiafMixed = 1, kFamilyGrmhdFP64 = 2 };
+enum : int { kFamilyRiafFP64 = 0, kFamilyRiafMixed = 1, kFamilyGrmhdFP64 = 2, kFamilyGrmhdMixed = 3 };
 
 int run_wave_jobs(DeviceState* dev, cudaStream_t stream, int njobs, long long total, int family, int nf_max,
                   const kp_run_options& opt, kp_batch_stats* stats) {
@@ -485,9 +485,10 @@ int run_wave_jobs(DeviceState* dev, cudaStream_t stream, int njobs, long long to
     for (int phase = 0; phase < kPhases; ++phase) {
         int per_sm = opt.blocks_per_sm;
         if (per_sm <= 0) {
-            per_sm = family == kFamilyGrmhdFP64 ? wave_occupancy_grmhd(phase, nf_max, wave_threads(phase))
-                     : mixed ? wave_occupancy_mixed(phase, wave_threads(phase))
-                             : wave_occupancy_fp64(phase, nf_max, wave_threads(phase));
+            per_sm = family == kFamilyGrmhdFP64    ? wave_occupancy_grmhd(phase, nf_max, wave_threads(phase))
+                     : family == kFamilyGrmhdMixed ? wave_occupancy_grmhd_mixed(phase, nf_max, wave_threads(phase))
+                     : mixed                       ? wave_occupancy_mixed(phase, wave_threads(phase))
+                                                   : wave_occupancy_fp64(phase, nf_max, wave_threads(phase));
             if (per_sm <= 0) per_sm = 1;
         }
         blocks[phase] = dev->sms * per_sm;
@@ -514,6 +515,8 @@ int run_wave_jobs(DeviceState* dev, cudaStream_t stream, int njobs, long long to
         W.status = &ctrl->status;
         W.job_done = nullptr;
         if (family == kFamilyGrmhdFP64) return launch_wave_grmhd(phase, W, nf_max, blocks[phase], wave_threads(phase), stream);
+        if (family == kFamilyGrmhdMixed)
+            return launch_wave_grmhd_mixed(phase, W, nf_max, blocks[phase], wave_threads(phase), stream);
         return mixed ? launch_wave_mixed(phase, W, blocks[phase], wave_threads(phase), stream)
                      : launch_wave_fp64(phase, W, nf_max, blocks[phase], wave_threads(phase), stream);
     };
@@ -945,8 +948,8 @@ int kp_image_grmhd(const kp_pass_a_params* params, const kp_grid* grid, int radi
     if (params->direct_only) return set_error(KP_ERR_UNSUPPORTED, "direct_only transport is not built");
     if (radiation_substeps < 1) return set_error(KP_ERR_INVALID, "radiation_substeps must be positive");
     if (grid->model.spin != params->spin) return set_error(KP_ERR_INVALID, "grid spin differs from the metric spin");
-    if (opt.precision != KP_PRECISION_FP64)
-        return set_error(KP_ERR_UNSUPPORTED, "GRMHD images are built for KP_PRECISION_FP64 only");
+    if (opt.precision != KP_PRECISION_FP64 && opt.precision != KP_PRECISION_MIXED)
+        return set_error(KP_ERR_INVALID, "unknown precision %d", opt.precision);
     if (opt.integrator != KP_INTEGRATOR_STEP_DOUBLING_RK4 && opt.integrator != KP_INTEGRATOR_CASH_KARP)
         return set_error(KP_ERR_INVALID, "unknown integrator %d", opt.integrator);
     if (opt.device != grid->device) return set_error(KP_ERR_INVALID, "the grid lives on device %d", grid->device);
@@ -976,8 +979,11 @@ int kp_image_grmhd(const kp_pass_a_params* params, const kp_grid* grid, int radi
     d.out = dptr;
     d.ray_begin = 0;
     d.npix = npix;
-    d.precision = KP_PRECISION_FP64;
-    st = run_wave_jobs(dev, stream, 1, npix, kFamilyGrmhdFP64, nfreq == 1 ? 1 : KP_MAX_FREQUENCIES, opt, nullptr);
+    d.precision = opt.precision;
+    const bool mixed = opt.precision == KP_PRECISION_MIXED;
+    if (mixed) grmhd_emission_scale(params, grid->model, d.c);
+    st = run_wave_jobs(dev, stream, 1, npix, mixed ? kFamilyGrmhdMixed : kFamilyGrmhdFP64,
+                       nfreq == 1 ? 1 : KP_MAX_FREQUENCIES, opt, nullptr);
     if (st != KP_OK) return st;
     if (!opt.outputs_on_device) {
         st = copy_outputs_to_host(dptr, out, npix, nfreq, stream);

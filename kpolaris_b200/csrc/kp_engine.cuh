@@ -126,6 +126,36 @@ struct RadTraits<PolicyFP64, SceneGrmhd> {
     __device__ static Stokes4<double> result(const Stokes& s, const ImageConsts&, int) { return s; }
 };
 
+// GRMHD grid plasma under the mixed policy: the grid gather, the fluid and
+// field four-vectors and the screen angle stay FP64 (grmhd_sample, the
+// reference's fluid_state); the thermal fit per frequency and the Stokes
+// update run in FP32 with the 2^E emission scale and compensated sums, the
+// same code as the mixed RIAF scene.
+__device__ __forceinline__ RiafSampleF grmhd_sample_f(const ImageConsts& c, const Ray& r) {
+    const GrmhdSample p = grmhd_sample(c, r);
+    RiafSampleF o;
+    o.emitting = p.emitting;
+    o.on_axis = 0;
+    o.has_chi = p.has_chi;
+    if (!p.emitting) return o;
+    o.ne = float(p.ne);
+    o.thetae = float(p.thetae);
+    o.b = float(p.b);
+    o.nu_fluid = float(p.nu_scale);
+    o.cos_theta = float(p.ct);
+    o.sin_theta = float(p.st);
+    o.theta = 0.0f;
+    o.cos2chi = float(p.cos2chi);
+    o.sin2chi = float(p.sin2chi);
+    riaf_sample_thermal_f(c, o);
+    return o;
+}
+
+template<>
+struct RadTraits<PolicyMixed, SceneGrmhd> : RadTraits<PolicyMixed, SceneRiaf> {
+    __device__ static Sample sample(const ImageConsts& c, const Ray& r) { return grmhd_sample_f(c, r); }
+};
+
 // The scene's transport RHS under a policy; FP32 is a compile-time choice of
 // the calling kernel, so each kernel holds one contraction body.  The FP64
 // policy keeps the reference's operation order; the mixed policy uses the

@@ -111,4 +111,29 @@ inline ImageConsts image_consts_fmks(const kp_pass_a_params* p, const kp_grmhd_m
     return c;
 }
 
+// FP32 emission scales 2^E of a mixed-precision GRMHD image, one per
+// frequency.  The invariant emissivity j ~ n_e e^2 nu_c / (c nu^2) lies far
+// below FP32 range in CGS; E puts the emission of one radiation step at a
+// reference plasma point (code density 1, code field 0.05, shape factor bound
+// 30) at 2^-6.  The transfer is linear in the emission, so the image is
+// rescaled by 2^-E in FP64 at the end and E changes only rounding.
+inline void grmhd_emission_scale(const kp_pass_a_params* p, const kp_grmhd_model& m, ImageConsts& c) {
+    const double pi = 3.141592653589793, ee = 4.803204712570263e-10, me = 9.1093826e-28, mp = 1.67262171e-24,
+                 cl = 2.99792458e10;
+    const double ne = std::max(c.grid.rho_unit / (mp + me) * m.ne_factor, 1e-30);
+    const double b = 0.05 * c.grid.b_unit;
+    const double nu_c = ee * b / (2.0 * pi * me * cl);
+    const double j_phys = ne * ee * ee * nu_c / cl * (std::sqrt(2.0) * pi / 27.0) * 30.0;
+    const double step = p->max_radiation_step > 0.0 ? p->max_radiation_step : std::max(p->max_step, 1e-3);
+    for (int f = 0; f < c.nfreq; ++f) {
+        const double j_inv = j_phys / std::max(c.freq[f] * c.freq[f], 1.0);
+        const double dl = std::max(step * std::fabs(c.dlambda_scale[f]), 1e-300);
+        double e = std::floor(std::log2(std::ldexp(1.0, -6) / std::max(j_inv * dl, 1e-300)));
+        if (!(e == e)) e = 0.0;
+        const int ei = int(std::min(120.0, std::max(-120.0, e)));
+        c.emission_scale_pow2[f] = std::ldexp(1.0f, ei);
+        c.inv_emission_scale_pow2[f] = std::ldexp(1.0, -ei);
+    }
+}
+
 }  // namespace kp

@@ -41,6 +41,10 @@ cudaError_t launch_seed_mixed(const JobDesc* jobs, const SeedEntry* entries, con
 cudaError_t launch_wave_grmhd(int phase, const WaveDesc& W, int nf_max, int blocks, int threads,
                               cudaStream_t stream);
 int wave_occupancy_grmhd(int phase, int nf_max, int threads);
+// The same scene under the mixed policy (kp_kernels_grmhd_mixed.cu).
+cudaError_t launch_wave_grmhd_mixed(int phase, const WaveDesc& W, int nf_max, int blocks, int threads,
+                                    cudaStream_t stream);
+int wave_occupancy_grmhd_mixed(int phase, int nf_max, int threads);
 cudaError_t launch_seed_grmhd(const JobDesc* jobs, const SeedEntry* entries, const long long* prefix, int nentries,
                               long long total, RayRecord* pool, unsigned* far_ids, unsigned* far_count,
                               cudaStream_t stream);

@@ -138,3 +138,31 @@ def test_grmhd_rejects_invalid_requests():
             kp.image_grmhd(bad, g, freqs)
         with pytest.raises(kp.KPolarisError):
             kp.image_grmhd(synthetic.fmks_pass_a_params(model, 4, 4), g, [230e9] * 5)
+
+
+FLUX_RTOL_MIXED = 1e-4      # total flux (image-integrated Stokes I), mixed vs the reference
+EVPA_TOL_DEG = 0.1          # image-integrated EVPA, mixed vs the reference
+POLFRAC_ATOL = 1e-4         # image-integrated linear / circular polarisation fractions
+
+
+def integrated_pol(arrays, f):
+    i, q, u, v = (np.nansum(arrays[k][f]) for k in ("image_i", "image_q", "image_u", "image_v"))
+    return i, 0.5 * np.degrees(np.arctan2(u, q)), np.hypot(q, u) / i, v / i
+
+
+@pytest.mark.parametrize("name", ["grmhd_adaptive_16", "grmhd_multifreq_12x10", "grmhd_fixed_16"])
+def test_grmhd_mixed_within_budget_of_reference(name):
+    """Mixed policy (FP64 geodesic and grid sample, FP32 fits and transfer)
+    against the reference's FP64 image: total flux within 1e-4, EVPA within
+    0.1 deg, polarisation fractions within 1e-4, reasons 99% identical."""
+    fx, prims, model, params, freqs, _ = load_case(name)
+    with kp.Grid(model, prims) as g:
+        res = kp.image_grmhd(params, g, freqs, precision=_abi.PRECISION_MIXED)
+    assert np.mean(res.reason == fx["reason"]) >= 0.99
+    for f in range(len(freqs)):
+        i_m, e_m, l_m, c_m = integrated_pol(res.arrays, f)
+        i_r, e_r, l_r, c_r = integrated_pol(fx, f)
+        assert abs(i_m / i_r - 1.0) <= FLUX_RTOL_MIXED, (f, i_m / i_r - 1.0)
+        d = abs((e_m - e_r + 90.0) % 180.0 - 90.0)
+        assert d <= EVPA_TOL_DEG, (f, e_m, e_r)
+        assert abs(l_m - l_r) <= POLFRAC_ATOL and abs(c_m - c_r) <= POLFRAC_ATOL, (f, l_m, l_r, c_m, c_r)
