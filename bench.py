@@ -59,6 +59,9 @@ def parse():
     ap.add_argument("--serve-plain", type=int, default=1, help="replay the trace on the plain FP64 kernel too")
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="target CPU time of the bounded CPU-baseline sample")
+    ap.add_argument("--grmhd", type=int, default=1,
+                    help="also time the GRMHD image (288x128x128 FM torus, 512^2, FP64 and mixed)")
+    ap.add_argument("--grmhd-steps", type=int, default=2, help="timed GRMHD images per precision")
     return ap.parse_args()
 
 
@@ -113,6 +116,86 @@ def cpu_sample(params, model, freqs, kind, seconds, threads=0):
     cores = threads if threads > 0 else (os.cpu_count() or 1)
     sample = f"{rows_done} of {ny} rows ({rows_done * nx} pixels, spread over the image), {dt:.2f} s"
     return ips, sample, cores
+
+
+GRMHD_WORKLOAD = ("FMKS GRMHD image: seeded FM torus (a=0.9375, r_in=6, r_max=12, 10% log-normal density "
+                  "noise, one poloidal loop at beta=100, heating 1/r) on 288x128x128 FP32 cells, 512^2 pixels, "
+                  "230 GHz, i=163 deg, R-beta R_high=40, Dexter fit, derived scalars on the device, "
+                  "M87* 6.5e9 Msun, M_unit=1e27 g, adaptive RK4 tol 1e-8")
+
+
+def grmhd_section(args, torch, dev, local, stream, flush, rank):
+    """The GRMHD image (FMKS metric, grid plasma) in FP64 and mixed precision:
+    device time per image with the grid resident and outputs on the device
+    (CUDA events on the launching stream, L2 flushed before each image), the
+    mixed image's error against the FP64 one, and a bounded CPU sample of the
+    reference's own GRMHD path."""
+    import numpy as np
+
+    import kpolaris_b200 as kp
+    from kpolaris_b200 import _abi, synthetic
+
+    n = 512
+    prims, model = synthetic.fm_torus(288, 128, 128)
+    model.trat_large = 40.0
+    params = synthetic.fmks_pass_a_params(model, n, n)
+    freqs = [230.0e9]
+    lib = kp.library()
+    fa = (C.c_double * 1)(*freqs)
+    res = {"workload": GRMHD_WORKLOAD}
+    outs = {}
+    with kp.Grid(model, prims, device=local) as grid:
+        for name, prec in (("fp64", _abi.PRECISION_FP64), ("mixed", _abi.PRECISION_MIXED)):
+            opt = kp._options(precision=prec, device=local)
+            opt.outputs_on_device = 1
+            opt.stream = C.c_void_p(stream.cuda_stream)
+            out = device_outputs(torch, n * n, 1, dev)
+            kp.check(lib.kp_image_grmhd(C.byref(params), grid._h, 1, fa, 1, C.byref(opt), C.byref(out[0])))
+            ms = []
+            for _ in range(max(1, args.grmhd_steps)):
+                flush.fill_(1.0)
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                kp.check(lib.kp_image_grmhd(C.byref(params), grid._h, 1, fa, 1, C.byref(opt), C.byref(out[0])))
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ms.append(e0.elapsed_time(e1))
+            t = sum(ms) / len(ms)
+            img = [x.cpu().numpy()[0] for x in out[1][0]]
+            ints = [x.cpu().numpy() for x in out[1][2]]
+            steps = int(ints[0].astype("int64").sum() + ints[1].astype("int64").sum())
+            outs[name] = (img, ints)
+            res[name] = {"images_per_s": 1000.0 / t, "ms_per_image": t, "rays_per_s": n * n * 1000.0 / t,
+                         "geodesic_steps_per_s": steps * 1000.0 / t,
+                         "flux_jy": synthetic.flux_jy(img[0], freqs[0], 20.0, n, n)}
+    (a, ai), (b, bi) = outs["fp64"], outs["mixed"]
+    ia, ib = integrated_stokes(a[0][None], a[1][None], a[2][None])[0], integrated_stokes(b[0][None], b[1][None], b[2][None])[0]
+    res["mixed_vs_fp64"] = {"total_flux_rel_err": abs(ib[0] / ia[0] - 1.0),
+                            "evpa_err_deg": abs((ib[1] - ia[1] + 90.0) % 180.0 - 90.0),
+                            "reason_agreement": float(np.mean(ai[2] == bi[2]))}
+    res["speedup_mixed_vs_fp64"] = res["mixed"]["images_per_s"] / res["fp64"]["images_per_s"]
+    if rank == 0:
+        import oracle
+
+        if oracle.ref_available():
+            derived = oracle.grmhd_derived(model, prims)
+            host = _abi.ImageHostData.allocate(n * n, 1)
+            rows, t0 = 0, time.perf_counter()
+            order = [j for off in range(16) for j in range(off, n, 16)]
+            for j in order:
+                oracle.image_grmhd(params, model, prims, derived, freqs, threads=0, pixel_begin=j * n,
+                                   pixel_end=(j + 1) * n, out=host)
+                rows += 1
+                if time.perf_counter() - t0 >= args.cpu_seconds:
+                    break
+            dt = time.perf_counter() - t0
+            ips = rows * n / float(n * n) / dt
+            res["cpu_baseline"] = {"value": ips, "unit": "images/s", "cores": os.cpu_count() or 1,
+                                   "kind": "reference",
+                                   "sample": f"{rows} of {n} rows ({rows * n} pixels, spread over the image), "
+                                             f"{dt:.2f} s, FP64, derived scalars precomputed"}
+    return res
 
 
 def reference_arm(args):
@@ -539,6 +622,11 @@ def ours_arm(args):
             progress("serving trace on the plain FP64 kernel")
             serving["plain_fp64"] = serve_plain(trace, local)
 
+    grmhd = None
+    if args.grmhd:
+        progress("GRMHD image")
+        grmhd = grmhd_section(args, torch, dev, local, stream, flush, rank)
+
     cpu = None
     if rank == 0:
         import oracle
@@ -573,6 +661,7 @@ def ours_arm(args):
             "rays_per_s": value * npix,
             "geodesic_steps_per_s": value * steps_per_image,
             "phases": phases, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
+            "grmhd": grmhd,
         }
         print(json.dumps(line), flush=True)
     if pg:
