@@ -365,13 +365,31 @@ int kp_grid_release(kp_grid* grid);
 
 /*
  * One GRMHD image in FMKS coordinates, 1..KP_MAX_FREQUENCIES frequencies on
- * one geodesic, through the wavefront engine in FP64.  Replaces
+ * one geodesic, through the wavefront engine (options->precision FP64, or
+ * MIXED: FP64 geodesic and grid sample, FP32 fits and transfer).  Replaces
  * run_grmhd_image (src/image/grmhd.hpp:12-32, src/image/grmhd.cpp:22-59) for
  * the FMKS backend; params->coordinate_system must be KP_COORD_FMKS and the
  * grid's spin must be params->spin.
  */
 int kp_image_grmhd(const kp_pass_a_params* params, const kp_grid* grid, int radiation_substeps,
                    const double* frequencies, int nfreq, const kp_run_options* options, kp_image_out* out);
+
+/*
+ * One slow-light GRMHD image: nsnap >= 2 resident snapshots of one flow
+ * (uploaded grids sharing one grid shape and coordinate map, times strictly
+ * increasing); a coefficient sample at coordinate time x^0 reads the fluid at
+ * observation_time + x^0, linearly interpolated between the two snapshots
+ * that enclose it (primitives and derived scalars after the spatial gather).
+ * A radiating sample whose time lies outside [times[0], times[nsnap-1]] ends
+ * its ray with KP_REASON_SLOW_LIGHT_TIME_EXHAUSTED.  Replaces
+ * run_slow_light_batch_metric in its default decoupled step mode
+ * (src/image/slow_light_batch_driver.hpp:107-368, window kernel
+ * src/image/slow_light_driver.hpp:1084-1483, finalisation :1560-1760) with
+ * every snapshot resident at once; the geodesics are the fast-light ones.
+ */
+int kp_image_grmhd_slow_light(const kp_pass_a_params* params, const kp_grid* const* snapshots, const double* times,
+                              int nsnap, double observation_time, int radiation_substeps, const double* frequencies,
+                              int nfreq, const kp_run_options* options, kp_image_out* out);
 
 /*
  * Serving loop.  A server owns one GPU and a device-owner thread that runs

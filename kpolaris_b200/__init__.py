@@ -21,7 +21,7 @@ __all__ = [
     "ImageHostData", "PassAParams", "RIAFModel", "RunOptions", "KPolarisError",
     "default_pass_a_params", "default_riaf_model", "default_run_options", "library",
     "run_riaf_image", "run_riaf_multifrequency_image", "image_riaf", "batch_riaf", "Server",
-    "default_server_config", "Grid", "image_grmhd",
+    "default_server_config", "Grid", "image_grmhd", "image_grmhd_slow_light",
 ]
 
 LIB_PATH = Path(os.environ.get("KPOLARIS_B200_LIB") or Path(__file__).resolve().parent / "lib" / "libkpolaris_b200.so")
@@ -72,6 +72,9 @@ def library() -> C.CDLL:
     L.kp_grid_release.argtypes = [C.c_void_p]
     L.kp_image_grmhd.argtypes = [C.POINTER(PassAParams), C.c_void_p, C.c_int, C.POINTER(C.c_double), C.c_int,
                                  C.POINTER(RunOptions), C.POINTER(_abi.ImageOut)]
+    L.kp_image_grmhd_slow_light.argtypes = [
+        C.POINTER(PassAParams), C.POINTER(C.c_void_p), C.POINTER(C.c_double), C.c_int, C.c_double, C.c_int,
+        C.POINTER(C.c_double), C.c_int, C.POINTER(_abi.RunOptions), C.POINTER(_abi.ImageOut)]
     L.kp_server_create.argtypes = [C.POINTER(_abi.ServerConfig), C.POINTER(C.c_void_p)]
     L.kp_server_submit.argtypes = [C.c_void_p, C.POINTER(_abi.RiafJob), C.POINTER(C.c_ulonglong)]
     L.kp_server_poll.argtypes = [C.c_void_p, C.c_ulonglong, C.POINTER(C.c_int)]
@@ -202,6 +205,34 @@ def image_grmhd(params: PassAParams, grid: Grid, frequencies=None, *, radiation_
     s = out.as_struct()
     opt = _options(device=grid.device, **options)
     check(L.kp_image_grmhd(C.byref(params), grid._h, int(radiation_substeps), fa, nfreq, C.byref(opt), C.byref(s)))
+    return out
+
+
+def image_grmhd_slow_light(params: PassAParams, snapshots, times, observation_time: float, frequencies=None, *,
+                           radiation_substeps=1, out: ImageHostData | None = None, **options) -> ImageHostData:
+    """One slow-light GRMHD image (kp_image_grmhd_slow_light): `snapshots`
+    are resident Grid objects of one flow at `times` (strictly increasing);
+    each coefficient sample reads the fluid at observation_time + x^0,
+    interpolated between the enclosing snapshots.  Mirrors the reference's
+    slow-light image driver (src/image/slow_light_batch_driver.hpp) with all
+    snapshots resident."""
+    L = library()
+    grids = list(snapshots)
+    if frequencies is None:
+        frequencies = [grids[0].model.freq_cgs]
+    nfreq = len(frequencies)
+    npix = params.camera.nx * params.camera.ny
+    if out is None:
+        out = ImageHostData.allocate(npix, nfreq)
+    handles = (C.c_void_p * len(grids))(*[g._h.value if isinstance(g._h, C.c_void_p) else g._h for g in grids])
+    ta = (C.c_double * len(grids))(*[float(t) for t in times])
+    if len(times) != len(grids):
+        raise ValueError("one time per snapshot")
+    fa = (C.c_double * max(nfreq, 1))(*frequencies)
+    s = out.as_struct()
+    opt = _options(device=grids[0].device, **options)
+    check(L.kp_image_grmhd_slow_light(C.byref(params), handles, ta, len(grids), float(observation_time),
+                                      int(radiation_substeps), fa, nfreq, C.byref(opt), C.byref(s)))
     return out
 
 

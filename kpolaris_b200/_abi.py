@@ -39,6 +39,7 @@ REASON_REACHED_INNER_BOUNDARY = 2
 REASON_ESCAPED_DOMAIN = 3
 REASON_MAX_STEPS = 4
 REASON_INVALID_STATE = 5
+REASON_SLOW_LIGHT_TIME_EXHAUSTED = 6
 REASON_ADAPTIVE_STEP_UNDERFLOW = 7
 
 FIT_PANDYA = 1

@@ -32,6 +32,8 @@ UNITS = {
     "kp_kernels_mixed.cu": ["--fmad=true"],
     "kp_kernels_grmhd.cu": ["--fmad=false"],
     "kp_kernels_grmhd_mixed.cu": ["--fmad=true"],
+    "kp_kernels_grmhd_slow.cu": ["--fmad=false"],
+    "kp_kernels_grmhd_slow_mixed.cu": ["--fmad=true"],
     "kp_capi.cu": ["--fmad=false"],
     "kp_noalloc.cu": ["--fmad=false"],
     "kp_server.cu": ["--fmad=false"],

@@ -72,6 +72,8 @@ struct DeviceState {
     unsigned* d_ids[kPhases][2] = {};  // id queues per phase, by generation parity
     long long pool_cap = 0;
     unsigned* h_left = nullptr;     // pinned: queue counts after a cycle
+    void* d_series = nullptr;       // slow light: snapshot table and times (grow-only)
+    size_t series_bytes = 0;
     cudaEvent_t ev_launch[kMaxWaveCycles * kPhases + 1] = {};  // per-launch timing
 };
 
@@ -446,7 +448,14 @@ int ensure_job_table(DeviceState* dev, int njobs) {
 // dev->h_jobs (total rays): uploads them, grows the record pool, launches
 // cycles of (far, near-A, near-B) until no ray is left and checks the status
 // word.  The caller holds g_mutex.
-enum : int { kFamilyRiafFP64 = 0, kFamilyRiafMixed = 1, kFamilyGrmhdFP64 = 2, kFamilyGrmhdMixed = 3 };
+enum : int {
+    kFamilyRiafFP64 = 0,
+    kFamilyRiafMixed = 1,
+    kFamilyGrmhdFP64 = 2,
+    kFamilyGrmhdMixed = 3,
+    kFamilyGrmhdSlowFP64 = 4,
+    kFamilyGrmhdSlowMixed = 5
+};
 
 int run_wave_jobs(DeviceState* dev, cudaStream_t stream, int njobs, long long total, int family, int nf_max,
                   const kp_run_options& opt, kp_batch_stats* stats) {
@@ -485,10 +494,13 @@ int run_wave_jobs(DeviceState* dev, cudaStream_t stream, int njobs, long long to
     for (int phase = 0; phase < kPhases; ++phase) {
         int per_sm = opt.blocks_per_sm;
         if (per_sm <= 0) {
-            per_sm = family == kFamilyGrmhdFP64    ? wave_occupancy_grmhd(phase, nf_max, wave_threads(phase))
-                     : family == kFamilyGrmhdMixed ? wave_occupancy_grmhd_mixed(phase, nf_max, wave_threads(phase))
-                     : mixed                       ? wave_occupancy_mixed(phase, wave_threads(phase))
-                                                   : wave_occupancy_fp64(phase, nf_max, wave_threads(phase));
+            const int th = wave_threads(phase);
+            per_sm = family == kFamilyGrmhdFP64        ? wave_occupancy_grmhd(phase, nf_max, th)
+                     : family == kFamilyGrmhdMixed     ? wave_occupancy_grmhd_mixed(phase, nf_max, th)
+                     : family == kFamilyGrmhdSlowFP64  ? wave_occupancy_grmhd_slow(phase, nf_max, th)
+                     : family == kFamilyGrmhdSlowMixed ? wave_occupancy_grmhd_slow_mixed(phase, nf_max, th)
+                     : mixed                           ? wave_occupancy_mixed(phase, th)
+                                                       : wave_occupancy_fp64(phase, nf_max, th);
             if (per_sm <= 0) per_sm = 1;
         }
         blocks[phase] = dev->sms * per_sm;
@@ -517,6 +529,10 @@ int run_wave_jobs(DeviceState* dev, cudaStream_t stream, int njobs, long long to
         if (family == kFamilyGrmhdFP64) return launch_wave_grmhd(phase, W, nf_max, blocks[phase], wave_threads(phase), stream);
         if (family == kFamilyGrmhdMixed)
             return launch_wave_grmhd_mixed(phase, W, nf_max, blocks[phase], wave_threads(phase), stream);
+        if (family == kFamilyGrmhdSlowFP64)
+            return launch_wave_grmhd_slow(phase, W, nf_max, blocks[phase], wave_threads(phase), stream);
+        if (family == kFamilyGrmhdSlowMixed)
+            return launch_wave_grmhd_slow_mixed(phase, W, nf_max, blocks[phase], wave_threads(phase), stream);
         return mixed ? launch_wave_mixed(phase, W, blocks[phase], wave_threads(phase), stream)
                      : launch_wave_fp64(phase, W, nf_max, blocks[phase], wave_threads(phase), stream);
     };
@@ -926,9 +942,28 @@ int kp_grid_release(kp_grid* g) {
     return KP_OK;
 }
 
-int kp_image_grmhd(const kp_pass_a_params* params, const kp_grid* grid, int radiation_substeps,
-                   const double* frequencies, int nfreq, const kp_run_options* options, kp_image_out* out) {
-    if (!params || !grid || !out) return set_error(KP_ERR_INVALID, "kp_image_grmhd: null argument");
+}  // extern "C"
+
+namespace {
+
+// Whether two grids hold the same flow geometry, so one stencil serves both
+// (can_interpolate_fluid_with, src/model/grmhd_grid.hpp:129-139, plus the
+// grid shape this library gathers both snapshots with).
+bool same_grid_geometry(const kp_grmhd_model& a, const kp_grmhd_model& b) {
+    return a.n1 == b.n1 && a.n2 == b.n2 && a.n3 == b.n3 && a.spin == b.spin && a.startx1 == b.startx1 &&
+           a.startx2 == b.startx2 && a.startx3 == b.startx3 && a.dx1 == b.dx1 && a.dx2 == b.dx2 && a.dx3 == b.dx3 &&
+           a.r_in == b.r_in && a.r_out == b.r_out && a.hslope == b.hslope && a.mks_smooth == b.mks_smooth &&
+           a.poly_alpha == b.poly_alpha && a.poly_xt == b.poly_xt && a.poly_norm == b.poly_norm &&
+           a.has_derived_scalars == b.has_derived_scalars;
+}
+
+// One GRMHD image, fast light (nsnap == 0: grids[0] alone) or slow light
+// (nsnap >= 2 resident snapshots at `times`, fluid read at t_obs + x^0).
+int grmhd_image(const kp_pass_a_params* params, const kp_grid* const* grids, const double* times, int nsnap,
+                double t_obs, int radiation_substeps, const double* frequencies, int nfreq,
+                const kp_run_options* options, kp_image_out* out) {
+    const kp_grid* grid = grids ? grids[0] : nullptr;
+    if (!params || !grid || !out) return set_error(KP_ERR_INVALID, "GRMHD image: null argument");
     kp_run_options opt;
     if (options) {
         opt = *options;
@@ -953,6 +988,23 @@ int kp_image_grmhd(const kp_pass_a_params* params, const kp_grid* grid, int radi
     if (opt.integrator != KP_INTEGRATOR_STEP_DOUBLING_RK4 && opt.integrator != KP_INTEGRATOR_CASH_KARP)
         return set_error(KP_ERR_INVALID, "unknown integrator %d", opt.integrator);
     if (opt.device != grid->device) return set_error(KP_ERR_INVALID, "the grid lives on device %d", grid->device);
+    const bool slow = nsnap != 0;
+    if (slow) {
+        if (nsnap < 2) return set_error(KP_ERR_INVALID, "slow-light requires at least two snapshots");
+        if (!times) return set_error(KP_ERR_INVALID, "null snapshot time list");
+        if (!std::isfinite(t_obs)) return set_error(KP_ERR_INVALID, "observation time must be finite");
+        for (int i = 0; i < nsnap; ++i) {
+            if (!grids[i]) return set_error(KP_ERR_INVALID, "null snapshot %d", i);
+            if (grids[i]->device != opt.device)
+                return set_error(KP_ERR_INVALID, "snapshot %d lives on device %d", i, grids[i]->device);
+            if (!same_grid_geometry(grid->model, grids[i]->model))
+                return set_error(KP_ERR_INVALID,
+                                 "slow-light snapshots must share one grid, coordinate map and derived-scalar layout "
+                                 "(snapshot %d differs)", i);
+            if (!std::isfinite(times[i]) || (i > 0 && !(times[i] > times[i - 1])))
+                return set_error(KP_ERR_INVALID, "snapshot times must be finite and strictly increasing");
+        }
+    }
     const int npix = params->camera.nx * params->camera.ny;
     int st = check_outputs(out, npix, nfreq);
     if (st != KP_OK) return st;
@@ -974,6 +1026,37 @@ int kp_image_grmhd(const kp_pass_a_params* params, const kp_grid* grid, int radi
     JobDesc& d = dev->h_jobs[0];
     std::memset(&d, 0, sizeof(d));
     d.c = make_consts_grmhd(params, grid, frequencies, nfreq, opt.integrator);
+    if (slow) {
+        // snapshot table then times, in one grow-only device buffer
+        const size_t table = sizeof(GridConsts) * size_t(nsnap);
+        const size_t bytes = table + sizeof(double) * size_t(nsnap);
+        if (bytes > dev->series_bytes) {
+            cudaStreamSynchronize(stream);
+            cudaFree(dev->d_series);
+            dev->d_series = nullptr;
+            dev->series_bytes = 0;
+            cudaError_t e = cudaMalloc(&dev->d_series, bytes);
+            if (e != cudaSuccess) {
+                cudaGetLastError();
+                return set_error(KP_ERR_OOM, "cudaMalloc(slow-light snapshot table): %s", cudaGetErrorString(e));
+            }
+            dev->series_bytes = bytes;
+        }
+        std::vector<unsigned char> host(bytes);
+        for (int i = 0; i < nsnap; ++i) {
+            const GridConsts g = grid_consts(grids[i]);
+            std::memcpy(host.data() + sizeof(GridConsts) * size_t(i), &g, sizeof(g));
+        }
+        std::memcpy(host.data() + table, times, sizeof(double) * size_t(nsnap));
+        cudaError_t e = cudaMemcpyAsync(dev->d_series, host.data(), bytes, cudaMemcpyHostToDevice, stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) return cuda_error(e, "slow-light snapshot table upload");
+        d.c.scene = kSceneGrmhdFmksSlowLight;
+        d.c.series = static_cast<const GridConsts*>(dev->d_series);
+        d.c.series_times = reinterpret_cast<const double*>(static_cast<unsigned char*>(dev->d_series) + table);
+        d.c.nseries = nsnap;
+        d.c.t_obs = t_obs;
+    }
     fmks_camera_frame(d.c.fmks, params->camera.radius, params->camera.inclination, d.frame.x, d.frame.e0,
                       d.frame.e1, d.frame.e2, d.frame.e3);
     d.out = dptr;
@@ -982,8 +1065,9 @@ int kp_image_grmhd(const kp_pass_a_params* params, const kp_grid* grid, int radi
     d.precision = opt.precision;
     const bool mixed = opt.precision == KP_PRECISION_MIXED;
     if (mixed) grmhd_emission_scale(params, grid->model, d.c);
-    st = run_wave_jobs(dev, stream, 1, npix, mixed ? kFamilyGrmhdMixed : kFamilyGrmhdFP64,
-                       nfreq == 1 ? 1 : KP_MAX_FREQUENCIES, opt, nullptr);
+    const int family = slow ? (mixed ? kFamilyGrmhdSlowMixed : kFamilyGrmhdSlowFP64)
+                            : (mixed ? kFamilyGrmhdMixed : kFamilyGrmhdFP64);
+    st = run_wave_jobs(dev, stream, 1, npix, family, nfreq == 1 ? 1 : KP_MAX_FREQUENCIES, opt, nullptr);
     if (st != KP_OK) return st;
     if (!opt.outputs_on_device) {
         st = copy_outputs_to_host(dptr, out, npix, nfreq, stream);
@@ -992,6 +1076,25 @@ int kp_image_grmhd(const kp_pass_a_params* params, const kp_grid* grid, int radi
         if (e != cudaSuccess) return cuda_error(e, "device-to-host copy");
     }
     return KP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int kp_image_grmhd(const kp_pass_a_params* params, const kp_grid* grid, int radiation_substeps,
+                   const double* frequencies, int nfreq, const kp_run_options* options, kp_image_out* out) {
+    const kp_grid* grids[1] = {grid};
+    return grmhd_image(params, grids, nullptr, 0, 0.0, radiation_substeps, frequencies, nfreq, options, out);
+}
+
+int kp_image_grmhd_slow_light(const kp_pass_a_params* params, const kp_grid* const* snapshots, const double* times,
+                              int nsnap, double observation_time, int radiation_substeps, const double* frequencies,
+                              int nfreq, const kp_run_options* options, kp_image_out* out) {
+    if (!snapshots) return set_error(KP_ERR_INVALID, "kp_image_grmhd_slow_light: null snapshot list");
+    if (nsnap < 2) return set_error(KP_ERR_INVALID, "slow-light requires at least two snapshots");
+    return grmhd_image(params, snapshots, times, nsnap, observation_time, radiation_substeps, frequencies, nfreq,
+                       options, out);
 }
 
 }  // extern "C"

@@ -26,6 +26,7 @@ enum Reason : int {
     kEscaped = 3,
     kMaxSteps = 4,
     kInvalidState = 5,
+    kSlowLightTimeExhausted = 6,
     kAdaptiveUnderflow = 7,
 };
 
@@ -74,7 +75,7 @@ struct GridConsts {
     double rho_unit, b_unit, trat_small, trat_large, beta_crit, sigma_cut, sigma_cut_high, ne_factor;
 };
 
-enum Scene : int { kSceneRiafCks = 0, kSceneGrmhdFmks = 1 };
+enum Scene : int { kSceneRiafCks = 0, kSceneGrmhdFmks = 1, kSceneGrmhdFmksSlowLight = 2 };
 
 // Everything one image needs on the device, resolved on the host.  Host-side
 // precomputation keeps libm (sin/cos of the inclination, cbrt in the ISCO
@@ -116,6 +117,13 @@ struct ImageConsts {
     int scene;
     FmksParams fmks;
     GridConsts grid;
+    // slow light: the resident snapshots of one flow ([nseries] device
+    // tables, times increasing) and the observation time; a sample at
+    // coordinate time x^0 reads the fluid at t_obs + x^0
+    const GridConsts* series;
+    const double* series_times;
+    int nseries;
+    double t_obs;
 };
 
 // Device pointers of one image's outputs, laid out like ImageHostData.

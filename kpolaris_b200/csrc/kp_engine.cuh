@@ -131,8 +131,7 @@ struct RadTraits<PolicyFP64, SceneGrmhd> {
 // reference's fluid_state); the thermal fit per frequency and the Stokes
 // update run in FP32 with the 2^E emission scale and compensated sums, the
 // same code as the mixed RIAF scene.
-__device__ __forceinline__ RiafSampleF grmhd_sample_f(const ImageConsts& c, const Ray& r) {
-    const GrmhdSample p = grmhd_sample(c, r);
+__device__ __forceinline__ RiafSampleF grmhd_sample_to_f(const ImageConsts& c, const GrmhdSample& p) {
     RiafSampleF o;
     o.emitting = p.emitting;
     o.on_axis = 0;
@@ -151,9 +150,29 @@ __device__ __forceinline__ RiafSampleF grmhd_sample_f(const ImageConsts& c, cons
     return o;
 }
 
+__device__ __forceinline__ RiafSampleF grmhd_sample_f(const ImageConsts& c, const Ray& r) {
+    return grmhd_sample_to_f(c, grmhd_sample(c, r));
+}
+
 template<>
 struct RadTraits<PolicyMixed, SceneGrmhd> : RadTraits<PolicyMixed, SceneRiaf> {
     __device__ static Sample sample(const ImageConsts& c, const Ray& r) { return grmhd_sample_f(c, r); }
+};
+
+// Slow light: the grid plasma interpolated in time between the resident
+// snapshots around each sample's fluid time (grmhd_sample_series).
+template<>
+struct RadTraits<PolicyFP64, SceneGrmhdSlow> : RadTraits<PolicyFP64, SceneGrmhd> {
+    __device__ static Sample sample(const ImageConsts& c, const Ray& r) { return grmhd_sample_series(c, r); }
+};
+
+__device__ __forceinline__ RiafSampleF grmhd_series_sample_f(const ImageConsts& c, const Ray& r) {
+    return grmhd_sample_to_f(c, grmhd_sample_series(c, r));
+}
+
+template<>
+struct RadTraits<PolicyMixed, SceneGrmhdSlow> : RadTraits<PolicyMixed, SceneRiaf> {
+    __device__ static Sample sample(const ImageConsts& c, const Ray& r) { return grmhd_series_sample_f(c, r); }
 };
 
 // The scene's transport RHS under a policy; FP32 is a compile-time choice of

@@ -168,13 +168,25 @@ KP_HD double grid_interp(const GridStencil& st, const double* field) {
     return out;
 }
 
+// Linear interpolation in time that keeps the endpoints and static values
+// exact (interpolate_time_value, src/model/time_interpolation.hpp:27-32).
+KP_HD double time_interp(double a, double b, double f) {
+    if (f <= 0.0 || a == b) return a;
+    if (f >= 1.0) return b;
+    return (1.0 - f) * a + f * b;
+}
+
 // Plasma state at a sample point, the frequency-independent part of
-// coefficients (:1091-1240 up to the thermal fit).
-static __device__ __noinline__ GrmhdSample grmhd_sample(const ImageConsts& c, const Ray& s) {
+// coefficients (:1091-1240 up to the thermal fit), from grid g, or with
+// `up` the fluid interpolated in time between g and up at fraction f: every
+// gathered primitive and derived scalar is interpolated after the trilinear
+// gather, the four-vectors are formed from the interpolated primitives
+// (fluid_state with time_upper, :945-962).  The grids share one geometry.
+__device__ __forceinline__ GrmhdSample grmhd_sample_from(const ImageConsts& c, const Ray& s, const GridConsts& g,
+                                                         const GridConsts* up, double f) {
     GrmhdSample out;
     out.emitting = 0;
     out.has_chi = 0;
-    const GridConsts& g = c.grid;
     const double x1 = s.x.v[1], x2 = s.x.v[2], phi = s.x.v[3];
     const double r = exp(x1);
     double th, dth1, dth2;
@@ -183,13 +195,21 @@ static __device__ __noinline__ GrmhdSample grmhd_sample(const ImageConsts& c, co
     GridStencil st;
     if (!grid_stencil(g, x1, x2, phi, st)) return out;
     const size_t ncell = size_t(g.n1) * size_t(g.n2) * size_t(g.n3);
-    const double rho = grid_interp(st, g.prims + 0 * ncell);
-    const double uu = grid_interp(st, g.prims + 1 * ncell);
+    auto prim = [&](size_t v) {
+        const double a = grid_interp(st, g.prims + v * ncell);
+        return up ? time_interp(a, grid_interp(st, up->prims + v * ncell), f) : a;
+    };
+    auto derived = [&](size_t v) {
+        const double a = grid_interp(st, g.derived + v * ncell);
+        return up ? time_interp(a, grid_interp(st, up->derived + v * ncell), f) : a;
+    };
+    const double rho = prim(kPrimRho);
+    const double uu = prim(kPrimU);
     if (!(rho > 0.0 && uu > 0.0)) return out;
     double U[3], B[3];
     for (int i = 0; i < 3; ++i) {
-        U[i] = grid_interp(st, g.prims + size_t(kPrimU1 + i) * ncell);
-        B[i] = grid_interp(st, g.prims + size_t(kPrimB1 + i) * ncell);
+        U[i] = prim(size_t(kPrimU1 + i));
+        B[i] = prim(size_t(kPrimB1 + i));
     }
     double gcov[4][4], gcon0[4];
     grid_native_metric(g, r, th, dth1, dth2, gcov, gcon0);
@@ -197,10 +217,10 @@ static __device__ __noinline__ GrmhdSample grmhd_sample(const ImageConsts& c, co
     const double bsq = grid_four_vectors(gcov, gcon0, U, B, ucon, bcon);
     double ne, thetae, bcgs, sigma;
     if (g.has_derived) {
-        ne = grid_interp(st, g.derived + kDerNe * ncell);
-        thetae = grid_interp(st, g.derived + kDerThetae * ncell);
-        bcgs = grid_interp(st, g.derived + kDerB * ncell);
-        sigma = grid_interp(st, g.derived + kDerSigma * ncell);
+        ne = derived(kDerNe);
+        thetae = derived(kDerThetae);
+        bcgs = derived(kDerB);
+        sigma = derived(kDerSigma);
     } else {
         sigma = bsq / max_val(rho, kTiny);
         const double beta = (g.gam - 1.0) * uu / (0.5 * bsq);
@@ -259,6 +279,39 @@ static __device__ __noinline__ GrmhdSample grmhd_sample(const ImageConsts& c, co
         out.sin2chi = -2.0 * b1 * b2 / bproj2;
     }
     return out;
+}
+
+static __device__ __noinline__ GrmhdSample grmhd_sample(const ImageConsts& c, const Ray& s) {
+    return grmhd_sample_from(c, s, c.grid, nullptr, 0.0);
+}
+
+// Slow light: the snapshot pair whose times enclose t = t_obs + x^0 (binary
+// search, SlowLightResidentWindows::sample_window, slow_light_driver.hpp:
+// 1000-1010) and the clamped fraction (interpolation_fraction, :62-69);
+// at the ends of the pair one snapshot alone (SlowLightTemporalModel::
+// coefficients, :168-176).
+KP_HD double series_time(const ImageConsts& c, const Ray& s) { return c.t_obs + s.x.v[0]; }
+
+KP_HD bool series_holds(const ImageConsts& c, double t) {
+    return t >= c.series_times[0] && t <= c.series_times[c.nseries - 1];
+}
+
+static __device__ __noinline__ GrmhdSample grmhd_sample_series(const ImageConsts& c, const Ray& s) {
+    const double t = series_time(c, s);
+    int lo = 0, hi = c.nseries - 1;
+    while (lo + 1 < hi) {
+        const int mid = lo + (hi - lo) / 2;
+        if (t < c.series_times[mid]) hi = mid;
+        else lo = mid;
+    }
+    const double t0 = c.series_times[lo], t1 = c.series_times[lo + 1];
+    const double denom = t1 - t0;
+    double f = 0.0;
+    if (abs_val(denom) > kTiny) f = (c.t_obs + s.x.v[0] - t0) / denom;
+    f = min_val(1.0, max_val(0.0, f));
+    if (f <= 0.0) return grmhd_sample_from(c, s, c.series[lo], nullptr, 0.0);
+    if (f >= 1.0) return grmhd_sample_from(c, s, c.series[lo + 1], nullptr, 0.0);
+    return grmhd_sample_from(c, s, c.series[lo], &c.series[lo + 1], f);
 }
 
 // Transfer coefficients at one frequency (the thermal fit and the rotation

@@ -514,7 +514,9 @@ __device__ __forceinline__ void persistent_body(const WaveDesc& W) {
                         st.rk_kind = -1;
                         st.mode = kBStep;
                         if (!cam && st.h_current <= c.min_step_abs * 1.0001) {
-                            st.reason = kAdaptiveUnderflow;
+                            // the slow-light window kernel reports max_steps here
+                            // (slow_light_driver.hpp:1172-1177)
+                            st.reason = SC::kSlowLight ? kMaxSteps : kAdaptiveUnderflow;
                             st.mode = kDone;
                         }
                     }
@@ -546,6 +548,7 @@ __device__ __forceinline__ void persistent_body(const WaveDesc& W) {
                         }
                     }
                 }
+                bool stopped = false;
                 if (proceed) {
                     // radiation at the sample point (pass_b.hpp:1414-1496)
                     const double sample_r = SC::radius(c, sample.x);
@@ -560,7 +563,20 @@ __device__ __forceinline__ void persistent_body(const WaveDesc& W) {
                         // instruction working set small.
                         typename RT::Co co[NF];
                         typename RT::Sample ps = RT::none();
-                        if (sample_r - c.inner_radius > 0.0 && sample_r < c.outer_radius) ps = RT::sample(c, sample);
+                        bool radiating = sample_r - c.inner_radius > 0.0 && sample_r < c.outer_radius;
+                        if constexpr (SC::kSlowLight) {
+                            // slow_light_driver.hpp:1295-1304: a radiating sample
+                            // needs its fluid time among the resident snapshots;
+                            // otherwise the ray ends where it stands
+                            radiating = sample_r >= c.inner_radius && sample_r < c.outer_radius;
+                            if (radiating && !SC::time_resident(c, sample)) {
+                                st.reason = kSlowLightTimeExhausted;
+                                st.mode = kDone;
+                                stopped = true;
+                            }
+                        }
+                        if (radiating && !stopped) ps = RT::sample(c, sample);
+                        if (!stopped) {
                         int required = 1;
                         const int nf = c.nfreq < NF ? c.nfreq : NF;
 #pragma unroll 1
@@ -598,6 +614,7 @@ __device__ __forceinline__ void persistent_body(const WaveDesc& W) {
                             st.steps += 1;
                             if (crosses) st.reached = 1;
                         }
+                        }  // !stopped
                     } else {
                         // Far phase: the sample lies outside the radiating
                         // sphere, every coefficient is zero and the transfer
@@ -611,8 +628,10 @@ __device__ __forceinline__ void persistent_body(const WaveDesc& W) {
                         st.steps += 1;
                         if (crosses) st.reached = 1;
                     }
-                    st.mode = kBStep;
-                    st.rk_kind = -1;
+                    if (!stopped) {
+                        st.mode = kBStep;
+                        st.rk_kind = -1;
+                    }
                 }
             }
         }
@@ -627,7 +646,7 @@ __device__ __forceinline__ void persistent_body(const WaveDesc& W) {
             if (st.in_b) {
                 if (st.reached) {
                     reason = kReachedCamera;
-                } else if (reason != kAdaptiveUnderflow) {
+                } else if (reason != kAdaptiveUnderflow && reason != kSlowLightTimeExhausted) {
                     reason = kMaxSteps;
                 }
             }
@@ -645,6 +664,9 @@ __device__ __forceinline__ void persistent_body(const WaveDesc& W) {
             finish_ray_scene<SC, NF>(c, cam, S, st.in_b, sd, o, obs);
             store_stokes_n<NF>(J->out, st.pixel, J->npix, c.nfreq, obs);
             store_diagnostics(J->out, st.pixel, o);
+            if constexpr (SC::kSlowLight) {
+                if (!st.in_b) J->out.basis_identity_error[st.pixel] = 0.0;
+            }
             if (W.job_done) atomicAdd(&W.job_done[st.job], 1u);
             st.mode = kIdle;
         }

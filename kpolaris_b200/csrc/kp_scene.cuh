@@ -29,6 +29,7 @@ __device__ __forceinline__ Ray riaf_rhs(double mass, double spin, const Ray& X) 
 }
 
 struct SceneRiaf {
+    static constexpr bool kSlowLight = false;
     struct Metric {
         KSMetricPoint w;
         __device__ double dot(const D4& u, const D4& v) const { return ks_dot_at(w, u, v); }
@@ -83,6 +84,7 @@ static __device__ __noinline__ Ray fmks_camera_ray(const ImageConsts& c, const C
 }
 
 struct SceneGrmhd {
+    static constexpr bool kSlowLight = false;
     struct Metric {
         double g[4][4];
         __device__ double dot(const D4& u, const D4& v) const { return dot_gm(g, u, v); }
@@ -99,6 +101,17 @@ struct SceneGrmhd {
         Metric m;
         fmks_gcov(c.fmks, X, m.g);
         return m;
+    }
+};
+
+// Slow light on the GRMHD grid: the same FMKS geometry; the plasma of a
+// sample comes from the resident snapshots at t_obs + x^0
+// (ImageConsts::series).  A radiating sample whose time lies outside the
+// resident snapshots ends the ray (slow_light_time_exhausted).
+struct SceneGrmhdSlow : SceneGrmhd {
+    static constexpr bool kSlowLight = true;
+    __device__ static bool time_resident(const ImageConsts& c, const Ray& sample) {
+        return series_holds(c, series_time(c, sample));
     }
 };
 
@@ -120,6 +133,10 @@ __device__ __forceinline__ void finish_ray_scene(const ImageConsts& c, const Ray
         o.r12 = m.dot(cam.e1, state.e2);
         o.r21 = m.dot(cam.e2, state.e1);
         o.r22 = m.dot(cam.e2, state.e2);
+    } else if constexpr (S::kSlowLight) {
+        // a slow-light ray without pass B keeps zero overlaps
+        // (initialize_slow_light_states_metric, slow_light_driver.hpp:393-399)
+        o.r11 = o.r12 = o.r21 = o.r22 = 0.0;
     } else {
         o.r11 = 1.0;
         o.r12 = 0.0;

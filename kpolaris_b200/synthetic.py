@@ -112,12 +112,14 @@ def fm_torus(n1: int = 288, n2: int = 128, n3: int = 128, *, spin: float = 0.937
              r_max: float = 12.0, beta: float = 100.0, perturbation: float = 0.1, seed: int = 2026,
              gam: float = 4.0 / 3.0, kappa: float = 1e-3, r_out: float = 1000.0, hslope: float = 0.3,
              mks_smooth: float = 0.5, poly_alpha: float = 14.0, poly_xt: float = 0.82,
-             heating: float = 1.0, mbh_solar: float = 6.5e9, M_unit: float = 1.0e27):
+             heating: float = 1.0, mbh_solar: float = 6.5e9, M_unit: float = 1.0e27, time: float = 0.0):
     """Seeded FM torus on an n1 x n2 x n3 FMKS grid.  Returns (prims, model):
     prims float32 [8, n1, n2, n3], model a kp_grmhd_model (grid description,
     spin, mbh_solar and M_unit set; the rest at the model defaults).  The
     default M_unit = 1e27 g puts the 230 GHz flux of M87* (6.5e9 Msun,
-    16.8 Mpc) near 1 Jy with R_high = 40."""
+    16.8 Mpc) near 1 Jy with R_high = 40.  `time` (in M) advects the seeded
+    density perturbations with the torus's angular velocity
+    Omega = u^phi / u^t: the snapshot of the same torus `time` later."""
     a = float(spin)
     r_h = 1.0 + math.sqrt(max(0.0, 1.0 - a * a))
     r_grid_in = 0.9 * r_h
@@ -201,6 +203,16 @@ def fm_torus(n1: int = 288, n2: int = 128, n3: int = 128, *, spin: float = 0.937
     # 3-D: seeded log-normal density perturbations inside the torus
     rng = np.random.default_rng(seed)
     noise = np.exp(perturbation * rng.standard_normal((n1, n2, n3)) - 0.5 * perturbation ** 2)
+    if time != 0.0:
+        # the pattern rotates with the fluid: noise(phi) at `time` is the
+        # initial pattern at phi - Omega time (periodic linear interpolation)
+        omega = np.where(inside, uphi / np.where(ut != 0.0, ut, 1.0), 0.0)
+        pos = np.arange(n3)[None, None, :] - (omega * time / dx3)[..., None]
+        k0 = np.floor(pos)
+        frac = pos - k0
+        k0 = k0.astype(np.int64) % n3
+        k1 = (k0 + 1) % n3
+        noise = (1.0 - frac) * np.take_along_axis(noise, k0, axis=2) + frac * np.take_along_axis(noise, k1, axis=2)
     prims = np.empty((8, n1, n2, n3), dtype=np.float32)
     prims[0] = np.where(inside[..., None], rho[..., None] * noise, rho[..., None])
     prims[1] = u[..., None]
@@ -272,3 +284,16 @@ def flux_jy(image_i, frequency: float, xspan: float, nx: int, ny: int, mbh_solar
     d = dsource_pc * 3.085678e18
     omega = (2.0 * xspan * l_unit / nx) * (2.0 * xspan * l_unit / ny) / (d * d)
     return float(np.sum(image_i)) * frequency ** 3 * omega / 1.0e-23
+
+
+def fm_torus_series(n1: int = 288, n2: int = 128, n3: int = 128, *, count: int = 16, dt: float = 10.0,
+                    t0: float = 0.0, **kw):
+    """`count` snapshots of one seeded FM torus at times t0, t0 + dt, ...
+    (fm_torus with `time`): returns (list of prims, model, times)."""
+    prims = []
+    model = None
+    times = [t0 + dt * k for k in range(count)]
+    for t in times:
+        p, model = fm_torus(n1, n2, n3, time=t, **kw)
+        prims.append(p)
+    return prims, model, times

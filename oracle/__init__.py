@@ -183,6 +183,10 @@ def _declare_grmhd(L):
     L.kpref_grmhd_derived.argtypes = [C.POINTER(_abi.GrmhdModel), C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.kpref_transport_rhs_fmks.argtypes = [C.POINTER(_abi.PassAParams), C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.kpref_camera_ray_fmks.argtypes = [C.POINTER(_abi.PassAParams), C.c_int, C.POINTER(C.c_double)]
+    L.kpref_image_grmhd_slow_light_range.argtypes = [
+        C.POINTER(_abi.PassAParams), C.POINTER(_abi.GrmhdModel), C.POINTER(C.POINTER(C.c_double)),
+        C.POINTER(C.POINTER(C.c_double)), C.POINTER(C.c_double), C.c_int, C.c_double, C.POINTER(C.c_double), C.c_int,
+        C.c_int, C.c_int, C.c_int, C.POINTER(_abi.ImageOut)]
     L.kpref_grmhd_coefficients.argtypes = [
         C.POINTER(_abi.PassAParams), C.POINTER(_abi.GrmhdModel), C.POINTER(C.c_double), C.POINTER(C.c_double),
         C.POINTER(C.c_double), C.c_double, C.POINTER(C.c_double)]
@@ -222,6 +226,37 @@ def image_grmhd(params, model, prims, derived, freqs, *, threads=0, pixel_begin=
     s = out.as_struct()
     rc = L.kpref_image_grmhd_range(C.byref(params), C.byref(model), _dp(p), None if d is None else _dp(d), 1, fa,
                                    nfreq, int(threads), int(pixel_begin), int(pixel_end), C.byref(s))
+    if rc != 0:
+        raise RuntimeError(L.kpref_last_error().decode())
+    return out
+
+
+def image_grmhd_slow_light(params, model, prims_list, derived_list, times, observation_time, freqs, *, threads=0,
+                           pixel_begin=0, pixel_end=None, out=None, kind="reference"):
+    """A slow-light GRMHD image (or pixel range): the reference's kernels
+    driven by the restated slow-light ray loop (ref_driver.cpp,
+    slow_light_pixel), every snapshot resident, decoupled step mode."""
+    L = lib(kind)
+    _declare_grmhd(L)
+    npix = params.camera.nx * params.camera.ny
+    nfreq = len(freqs)
+    n = len(prims_list)
+    if out is None:
+        out = _abi.ImageHostData.allocate(npix, nfreq)
+    if pixel_end is None:
+        pixel_end = npix
+    keep = [np.ascontiguousarray(p, dtype=np.float64) for p in prims_list]
+    pa = (C.POINTER(C.c_double) * n)(*[_dp(p) for p in keep])
+    dkeep = None
+    da = None
+    if derived_list is not None:
+        dkeep = [np.ascontiguousarray(d, dtype=np.float64) for d in derived_list]
+        da = (C.POINTER(C.c_double) * n)(*[_dp(d) for d in dkeep])
+    ta = (C.c_double * n)(*[float(t) for t in times])
+    fa = (C.c_double * nfreq)(*freqs)
+    s = out.as_struct()
+    rc = L.kpref_image_grmhd_slow_light_range(C.byref(params), C.byref(model), pa, da, ta, n, float(observation_time),
+                                              fa, nfreq, int(threads), int(pixel_begin), int(pixel_end), C.byref(s))
     if rc != 0:
         raise RuntimeError(L.kpref_last_error().decode())
     return out

@@ -10,7 +10,9 @@
 // with the OpenMP dynamic schedule of pixel_range_policy (src/image/kernels.hpp:10-20).
 #include <omp.h>
 
+#include <cmath>
 #include <cstring>
+#include <vector>
 #include <stdexcept>
 
 #include "geodesic/pass_b.hpp"
@@ -214,6 +216,304 @@ kpolaris::GRMHDGridRadiationModel<Real> to_grmhd(const kp_grmhd_model& m, const 
 kpolaris::KerrFMKSMetric<Real> fmks_metric(const kpolaris::PassAParams<Real>& pa) {
     return kpolaris::KerrFMKSMetric<Real>(pa.mass, pa.spin, pa.fmks_startx1, pa.fmks_hslope, pa.fmks_mks_smooth,
                                           pa.fmks_poly_alpha, pa.fmks_poly_xt, pa.fmks_poly_norm);
+}
+
+// ---- slow light (restated driver loop over the reference's own kernels) ----
+//
+// The reference's slow-light drivers need Kokkos's execution machinery
+// (src/image/slow_light_driver.hpp, slow_light_batch_driver.hpp), which the
+// host shim does not provide, so their per-ray control flow is restated here
+// for one resident block holding every snapshot in the default decoupled step
+// mode; every arithmetic step is a call to the reference's templates
+// (pass A, adaptive_rk4_step / rk4_step, camera crossing, radiation substep
+// counts, the grid model's time-interpolated coefficients, the Strang
+// Stokes step, the observer transform).
+
+// SlowLightTemporalModel::coefficients (slow_light_driver.hpp:162-176) with
+// the pair of snapshots that encloses t = t_obs + x^0 (sample_window,
+// :1000-1010) and interpolation_fraction (:62-69).
+template<class Metric>
+kpolaris::TransferCoeffs<Real> slow_light_coefficients(const Metric& metric,
+                                                        std::vector<kpolaris::GRMHDGridRadiationModel<Real>>& models,
+                                                        const double* times, int nsnap, double t_obs,
+                                                        const kpolaris::TransportState<Real>& s, double freq) {
+    const Real t = t_obs + s.x[0];
+    int lo = 0, hi = nsnap - 1;
+    while (lo + 1 < hi) {
+        const int mid = lo + (hi - lo) / 2;
+        if (t < times[mid]) hi = mid;
+        else lo = mid;
+    }
+    auto& lower = models[size_t(lo)];
+    auto& upper = models[size_t(lo + 1)];
+    lower.freq_cgs = upper.freq_cgs = freq;
+    const Real denom = times[lo + 1] - times[lo];
+    Real f = Real(0);
+    if (kpolaris::abs_val(denom) > kpolaris::tiny_positive<Real>()) f = (t_obs + s.x[0] - times[lo]) / denom;
+    f = kpolaris::min_val(Real(1), kpolaris::max_val(Real(0), f));
+    if (f <= Real(0)) return lower.coefficients(metric, s, Real(0.5));
+    if (f >= Real(1)) return upper.coefficients(metric, s, Real(0.5));
+    return lower.coefficients(metric, s, Real(0.5), {}, &upper, f);
+}
+
+template<class Metric>
+void store_slow_light_end(kp_image_out* out, int npix, int pixel, const Metric& metric,
+                          const kpolaris::TransportState<Real>& camera_state,
+                          const kpolaris::TransportState<Real>& state, const kpolaris::Stokes<Real>* stokes,
+                          int nfreq, int pass_a_steps, int steps, int reason) {
+    const auto overlap = kpolaris::screen_overlap(metric, state.x, camera_state, state);
+    for (int f = 0; f < nfreq; ++f) {
+        const auto observed = kpolaris::transform_to_observer_basis(stokes[f], overlap);
+        const size_t idx = size_t(f) * size_t(npix) + size_t(pixel);
+        out->image_i[idx] = observed.I;
+        out->image_q[idx] = observed.Q;
+        out->image_u[idx] = observed.U;
+        out->image_v[idx] = observed.V;
+    }
+    kpolaris::Vec4<Real> target_k;
+    for (int mu = 0; mu < kpolaris::ndim; ++mu) target_k[mu] = camera_state.k[mu];
+    store_common(out, pixel, overlap, kpolaris::spatial_distance(state.x, camera_state.x),
+                 kpolaris::vector_max_abs_difference(state.k, target_k), metric.dot(state.x, state.k, state.k),
+                 kpolaris::max_frame_error(kpolaris::frame_errors(metric, state)), pass_a_steps, steps, reason);
+}
+
+// advance_slow_light_vacuum_to_camera (slow_light_driver.hpp:1572-1672):
+// an unfinished ray outside the radiating sphere continues in vacuum.
+template<class Metric>
+kpolaris::TerminationReason slow_light_vacuum(const kpolaris::PassAParams<Real>& params, const Metric& metric,
+                                              kpolaris::TransportState<Real>& state, Real& h_current,
+                                              int& local_steps) {
+    using namespace kpolaris;
+    const Real radial_tolerance = Real(1e-8) * max_val(Real(1), abs_val(params.outer_radius));
+    if (radial_coordinate(metric, state.x) < params.outer_radius - radial_tolerance)
+        return TerminationReason::slow_light_time_exhausted;
+    AdaptiveRK4Control<Real> control;
+    control.tolerance = params.adaptive_tolerance;
+    control.min_step = params.min_step;
+    control.max_step = params.max_step;
+    while (local_steps < params.max_steps) {
+        Real h = h_current;
+        const TransportState<Real> old_state = state;
+        TransportState<Real> next_state, sample_state;
+        if (params.adaptive) {
+            const auto proposed = adaptive_rk4_step(metric, old_state, h, control);
+            if (!proposed.accepted) {
+                h_current = abs_val(proposed.next_h);
+                if (h_current <= params.min_step * Real(1.0001)) return TerminationReason::max_steps;
+                continue;
+            }
+            h = abs_val(proposed.used_h);
+            h_current = abs_val(proposed.next_h);
+            next_state = proposed.state;
+            sample_state = proposed.mid_state;
+        } else {
+            next_state = rk4_step(metric, old_state, h);
+            sample_state = next_state;
+        }
+        const Real s0 = camera_surface_value(metric, params.camera, old_state);
+        const Real s1 = camera_surface_value(metric, params.camera, next_state);
+        const int crosses_camera = camera_surface_crossed(s0, s1);
+        if (crosses_camera) {
+            const Real fraction = camera_surface_crossing_fraction(s0, s1);
+            const Real h_cross = h * fraction;
+            if (abs_val(h_cross) <= Real(1e-14)) {
+                h = Real(0);
+                next_state = old_state;
+                sample_state = old_state;
+            } else if (fraction < Real(0.999999999999)) {
+                h = h_cross;
+                if (params.adaptive) {
+                    AdaptiveRK4Control<Real> cc = control;
+                    cc.min_step = min_val(cc.min_step, abs_val(h));
+                    cc.max_step = max_val(cc.min_step, abs_val(h));
+                    const auto crossing_step = adaptive_rk4_step(metric, old_state, h, cc);
+                    if (!crossing_step.accepted) {
+                        h_current = abs_val(crossing_step.next_h);
+                        continue;
+                    }
+                    h = abs_val(crossing_step.used_h);
+                    next_state = crossing_step.state;
+                    sample_state = crossing_step.mid_state;
+                } else {
+                    next_state = rk4_step(metric, old_state, h);
+                    sample_state = next_state;
+                }
+            }
+        }
+        const Real old_radius = radial_coordinate(metric, old_state.x);
+        const Real next_radius = radial_coordinate(metric, next_state.x);
+        const Real sample_radius = radial_coordinate(metric, sample_state.x);
+        if (!std::isfinite(next_radius) || !std::isfinite(sample_radius)) return TerminationReason::max_steps;
+        if (next_radius < old_radius - radial_tolerance || sample_radius < params.outer_radius - radial_tolerance ||
+            next_radius < params.outer_radius - radial_tolerance)
+            return TerminationReason::slow_light_time_exhausted;
+        state = next_state;
+        local_steps += 1;
+        if (crosses_camera) return TerminationReason::reached_camera;
+    }
+    return TerminationReason::max_steps;
+}
+
+// One slow-light pixel: initialize_slow_light_states_metric (:355-458), the
+// window kernel in decoupled mode with one resident block holding every
+// snapshot (:1100-1483), then finalize_slow_light_unfinished_metric
+// (:1674-1760) for a ray left waiting for fluid data.
+template<class Metric>
+void slow_light_pixel(int pixel, const kpolaris::PassAParams<Real>& params, const Metric& metric,
+                      std::vector<kpolaris::GRMHDGridRadiationModel<Real>>& models, const double* times, int nsnap,
+                      double t_obs, const double* freqs, int nfreq, kp_image_out* out) {
+    using namespace kpolaris;
+    const int npix = params.camera.nx * params.camera.ny;
+    const auto endpoint = trace_pass_a_segment_endpoint_pixel_metric(pixel, params, metric);
+    const auto camera_state = initialize_camera_ray(metric, pixel, params.camera);
+    TransportState<Real> state = endpoint.state;
+    Stokes<Real> stokes[KPOLARIS_MAX_FREQUENCIES];
+    for (int f = 0; f < nfreq; ++f) stokes[f] = Stokes<Real>{};
+    if (!endpoint.valid) {
+        for (int f = 0; f < nfreq; ++f) {
+            const size_t idx = size_t(f) * size_t(npix) + size_t(pixel);
+            out->image_i[idx] = out->image_q[idx] = out->image_u[idx] = out->image_v[idx] = 0.0;
+        }
+        out->closure_x[pixel] = spatial_distance(state.x, camera_state.x);
+        out->closure_k[pixel] = vector_max_abs_difference(state.k, camera_state.k);
+        out->final_null[pixel] = metric.dot(state.x, state.k, state.k);
+        out->frame_error[pixel] = max_frame_error(frame_errors(metric, state));
+        out->det_r[pixel] = 0.0;
+        out->overlap_r11[pixel] = out->overlap_r12[pixel] = out->overlap_r21[pixel] = out->overlap_r22[pixel] = 0.0;
+        out->basis_identity_error[pixel] = 0.0;
+        out->basis_rotation_angle[pixel] = 0.0;
+        out->pass_a_steps[pixel] = endpoint.steps;
+        out->steps[pixel] = 0;
+        out->reason[pixel] = static_cast<int>(endpoint.reason);
+        return;
+    }
+    const int screen_orientation = backward_screen_orientation_sign(params.camera);
+    AdaptiveRK4Control<Real> transfer_control;
+    transfer_control.tolerance = params.adaptive_tolerance;
+    transfer_control.min_step = params.min_step;
+    transfer_control.max_step = params.max_step;
+    Real h_current = params.step;
+    Real radiation_step_cap = params.max_radiation_step > Real(0) ? params.max_radiation_step : params.max_step;
+    int local_steps = 0, reached_camera = 0, active = 1, waiting = 0;
+    int reason = static_cast<int>(endpoint.reason);
+    while (!reached_camera && local_steps < params.max_steps) {
+        const Real retry_h = h_current;
+        Real h = h_current;
+        const TransportState<Real> old_state = state;
+        const Real start_r_bl = radial_coordinate(metric, old_state.x);
+        if (start_r_bl <= params.outer_radius && radiation_step_cap > Real(0)) h = min_val(h, radiation_step_cap);
+        TransportState<Real> next_state, sample_state;
+        if (params.adaptive) {
+            const auto proposed = adaptive_rk4_step(metric, old_state, h, transfer_control);
+            if (!proposed.accepted) {
+                h_current = abs_val(proposed.next_h);
+                if (h_current <= params.min_step * Real(1.0001)) {
+                    reason = static_cast<int>(TerminationReason::max_steps);
+                    active = 0;
+                    break;
+                }
+                continue;
+            }
+            h = abs_val(proposed.used_h);
+            h_current = abs_val(proposed.next_h);
+            next_state = proposed.state;
+            sample_state = proposed.mid_state;
+        } else {
+            next_state = rk4_step(metric, old_state, h);
+            sample_state = next_state;
+        }
+        const Real s0 = camera_surface_value(metric, params.camera, old_state);
+        const Real s1 = camera_surface_value(metric, params.camera, next_state);
+        int crosses_camera = camera_surface_crossed(s0, s1);
+        if (crosses_camera) {
+            const Real camera_frac = camera_surface_crossing_fraction(s0, s1);
+            const Real h_cross = h * camera_frac;
+            if (abs_val(h_cross) <= Real(1e-14)) {
+                h = Real(0);
+                next_state = old_state;
+                sample_state = old_state;
+            } else if (camera_frac < Real(0.999999999999)) {
+                h = h_cross;
+                if (params.adaptive) {
+                    AdaptiveRK4Control<Real> cc = transfer_control;
+                    cc.min_step = min_val(cc.min_step, abs_val(h));
+                    cc.max_step = max_val(cc.min_step, abs_val(h));
+                    const auto crossing_step = adaptive_rk4_step(metric, old_state, h, cc);
+                    if (!crossing_step.accepted) {
+                        h_current = abs_val(crossing_step.next_h);
+                        continue;
+                    }
+                    h = abs_val(crossing_step.used_h);
+                    next_state = crossing_step.state;
+                    sample_state = crossing_step.mid_state;
+                } else {
+                    next_state = rk4_step(metric, old_state, h);
+                    sample_state = next_state;
+                }
+            }
+        }
+        const Real old_r_bl = radial_coordinate(metric, old_state.x);
+        const Real sample_r_bl = radial_coordinate(metric, sample_state.x);
+        const Real next_r_bl = radial_coordinate(metric, next_state.x);
+        const int radiation_active = (sample_r_bl >= params.inner_radius && sample_r_bl < params.outer_radius) ? 1 : 0;
+        const Real coefficient_time = t_obs + sample_state.x[0];
+        if (radiation_active && !(coefficient_time >= times[0] && coefficient_time <= times[nsnap - 1])) {
+            waiting = 1;
+            h_current = retry_h;
+            break;
+        }
+        const Real local_max_radiation_step =
+            (params.max_radiation_step > Real(0) &&
+             (old_r_bl <= params.outer_radius || sample_r_bl <= params.outer_radius ||
+              next_r_bl <= params.outer_radius)) ? params.max_radiation_step : Real(0);
+        TransferCoeffs<Real> coeffs[KPOLARIS_MAX_FREQUENCIES]{};
+        Real dlambda_scales[KPOLARIS_MAX_FREQUENCIES];
+        int required_steps = 1, predictive_steps = 1;
+        for (int f = 0; f < nfreq; ++f) {
+            models[0].freq_cgs = freqs[f];
+            dlambda_scales[f] = models[0].dlambda_scale();
+            if (radiation_active) {
+                coeffs[f] = slow_light_coefficients(metric, models, times, nsnap, t_obs, sample_state, freqs[f]);
+                apply_emission_selection(params.emission_selection, metric, sample_state, coeffs[f]);
+                transform_axial_coefficients_to_screen_orientation(coeffs[f], screen_orientation);
+            }
+            const int candidate = radiation_substep_count(coeffs[f], h, dlambda_scales[f], 1, local_max_radiation_step,
+                                                          params.max_radiation_depth, params.max_absorption_depth,
+                                                          params.max_faraday_depth);
+            required_steps = candidate > required_steps ? candidate : required_steps;
+            const int predictive = radiation_substep_count(coeffs[f], h_current, dlambda_scales[f], 1,
+                                                           local_max_radiation_step, params.max_radiation_depth,
+                                                           params.max_absorption_depth, params.max_faraday_depth);
+            predictive_steps = predictive > predictive_steps ? predictive : predictive_steps;
+        }
+        if (required_steps > 1 && h > params.min_step * Real(1.0001)) {
+            h_current = max_val(params.min_step, h / Real(required_steps));
+            radiation_step_cap = h_current;
+            continue;
+        }
+        radiation_step_cap = predictive_steps > 1 ? max_val(params.min_step, h_current / Real(predictive_steps))
+                                                  : params.max_step;
+        if (h > Real(0)) {
+            for (int f = 0; f < nfreq; ++f)
+                semi_analytic_stokes_step(stokes[f], coeffs[f], abs_val(h) * dlambda_scales[f]);
+        }
+        state = next_state;
+        local_steps += 1;
+        if (crosses_camera) reached_camera = 1;
+    }
+    if (reached_camera || local_steps >= params.max_steps || !active) {
+        int r = reason;
+        if (reached_camera) r = static_cast<int>(TerminationReason::reached_camera);
+        else if (r != static_cast<int>(TerminationReason::adaptive_step_underflow))
+            r = static_cast<int>(TerminationReason::max_steps);
+        store_slow_light_end(out, npix, pixel, metric, camera_state, state, stokes, nfreq, endpoint.steps,
+                             local_steps, r);
+        return;
+    }
+    (void)waiting;
+    const auto end_reason = slow_light_vacuum(params, metric, state, h_current, local_steps);
+    store_slow_light_end(out, npix, pixel, metric, camera_state, state, stokes, nfreq, endpoint.steps, local_steps,
+                         static_cast<int>(end_reason));
 }
 
 thread_local char g_error[512];
@@ -489,6 +789,35 @@ int kpref_grmhd_coefficients(const kp_pass_a_params* params, const kp_grmhd_mode
     const auto c = grmhd.coefficients(fmks_metric(pa), s, Real(0.5));
     const double v[11] = {c.jI, c.jQ, c.jU, c.jV, c.aI, c.aQ, c.aU, c.aV, c.rQ, c.rU, c.rV};
     std::memcpy(out11, v, sizeof(v));
+    return KP_OK;
+}
+
+// A slow-light GRMHD image over a pixel range (see slow_light_pixel):
+// nsnap snapshots of one model's grid, prims[k] / derived[k] FP64 arrays.
+int kpref_image_grmhd_slow_light_range(const kp_pass_a_params* params, const kp_grmhd_model* model,
+                                       const double* const* prims, const double* const* derived,
+                                       const double* times, int nsnap, double t_obs, const double* freqs,
+                                       int nfreq, int threads, int pixel_begin, int pixel_end, kp_image_out* out) {
+    if (!params || !model || !prims || !times || !freqs || !out) return fail("null argument");
+    if (nsnap < 2) return fail("slow-light requires at least two snapshots");
+    if (nfreq < 1 || nfreq > KPOLARIS_MAX_FREQUENCIES) return fail("nfreq out of range");
+    const int npix = params->camera.nx * params->camera.ny;
+    if (pixel_begin < 0 || pixel_end > npix || pixel_begin > pixel_end) return fail("pixel range out of bounds");
+    const auto pa = to_pass_a(*params);
+    if (pa.coordinate_system != kpolaris::CoordinateSystem::FMKS) return fail("GRMHD oracle is built for FMKS only");
+    if (pa.emission_selection.narrow_wedge()) return fail("the slow-light oracle has no equatorial wedge");
+    if (threads > 0) omp_set_num_threads(threads);
+    const auto metric = fmks_metric(pa);
+    std::vector<kpolaris::GRMHDGridRadiationModel<Real>> base;
+    for (int k = 0; k < nsnap; ++k) base.push_back(to_grmhd(*model, prims[k], derived ? derived[k] : nullptr));
+#pragma omp parallel for schedule(dynamic)
+    for (int pixel = pixel_begin; pixel < pixel_end; ++pixel) {
+#ifdef KPREF_PERTURB_LIBM
+        kpref_ulp::seed_pixel(pixel);
+#endif
+        auto models = base;
+        slow_light_pixel(pixel, pa, metric, models, times, nsnap, t_obs, freqs, nfreq, out);
+    }
     return KP_OK;
 }
 

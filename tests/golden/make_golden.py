@@ -17,6 +17,12 @@ libm conditioning measured on the reference's own templates
 (oracle/_ref/libkpref_ulp.so) as parallel arrays cond_keys / cond_vals.
 
     python tests/golden/make_golden.py --grmhd     # GRMHD fixtures only
+    python tests/golden/make_golden.py --slow      # slow-light fixtures only
+
+Each slow-light fixture (slow_*.npz, SLOW_CASES) stores the case, the sha256
+of every snapshot's primitives, the reference image arrays (the reference's
+kernels driven by the restated slow-light ray loop of oracle/ref_driver.cpp)
+and their +-2-ulp libm conditioning.
 """
 from __future__ import annotations
 
@@ -31,8 +37,9 @@ sys.path.insert(0, str(ROOT))
 sys.path.insert(0, str(ROOT / "tests"))
 
 import oracle  # noqa: E402
-from golden_cases import (IMAGE_CASES, GRMHD_CASES, build_case, build_grmhd_case,  # noqa: E402
-                          coefficient_points, grmhd_conditioning_of, prims_digest, transfer_points)
+from golden_cases import (IMAGE_CASES, GRMHD_CASES, SLOW_CASES, build_case, build_grmhd_case,  # noqa: E402
+                          build_slow_case, coefficient_points, grmhd_conditioning_of, prims_digest,
+                          slow_conditioning_of, transfer_points)
 
 OUT = Path(__file__).resolve().parent
 
@@ -60,10 +67,28 @@ def make_grmhd():
               {cond_key(k): "%.1e" % cond[k] for k in keys if k[0] in ("flux", "image_i")})
 
 
+def make_slow():
+    for name, spec in SLOW_CASES.items():
+        prims, model, params, freqs, times, t_obs = build_slow_case(spec)
+        derived = [oracle.grmhd_derived(model, p) for p in prims]
+        res = oracle.image_grmhd_slow_light(params, model, prims, derived, times, t_obs, freqs, threads=0)
+        cond = slow_conditioning_of(params, model, prims, derived, times, t_obs, freqs, res.arrays)
+        keys = sorted(cond, key=cond_key)
+        np.savez_compressed(OUT / f"{name}.npz", spec=json.dumps(spec),
+                            prims_sha256=np.array([prims_digest(p) for p in prims]),
+                            cond_keys=np.array([cond_key(k) for k in keys]),
+                            cond_vals=np.array([cond[k] for k in keys]), **res.arrays)
+        print(name, np.bincount(res.reason, minlength=8)[:8],
+              {cond_key(k): "%.1e" % cond[k] for k in keys if k[0] in ("flux", "image_i")})
+
+
 def main():
     oracle.build(reference=True)
     if "--grmhd" in sys.argv[1:]:
         make_grmhd()
+        return
+    if "--slow" in sys.argv[1:]:
+        make_slow()
         return
     for name, spec in IMAGE_CASES.items():
         params, model, freqs = build_case(spec)
@@ -85,6 +110,7 @@ def main():
                         transfer_out=np.array(tr_out))
     print("coefficients", len(th_in), len(tr_in))
     make_grmhd()
+    make_slow()
 
 
 if __name__ == "__main__":

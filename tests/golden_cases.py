@@ -215,3 +215,47 @@ def prims_digest(prims) -> str:
     import hashlib
 
     return hashlib.sha256(np.ascontiguousarray(prims, dtype=np.float32).tobytes()).hexdigest()
+
+
+# Slow-light cases: 16 snapshots of the seeded FM torus 10 M apart
+# (kpolaris_b200.synthetic.fm_torus_series), imaged with the fluid read at
+# t_obs + x^0.  t_obs = 1100 M keeps every radiating sample inside the
+# resident 150 M; 1080 M and 1130 M end some rays early or late with
+# slow_light_time_exhausted.
+SLOW_CASES = {
+    "slow_adaptive_16": {"grid": [48, 32, 16], "n": 16, "adaptive": 1, "step": 0.025, "max_steps": 400000,
+                         "freqs": [230.0e9], "t_obs": 1100.0},
+    "slow_fixed_12": {"grid": [48, 32, 16], "n": 12, "adaptive": 0, "step": 0.05, "max_steps": 40000,
+                      "freqs": [230.0e9], "t_obs": 1100.0},
+    "slow_late_exhausted_12x10": {"grid": [48, 32, 16], "nx": 12, "ny": 10, "adaptive": 1, "step": 0.025,
+                                  "max_steps": 400000, "freqs": [86.0e9, 345.0e9], "t_obs": 1130.0},
+    "slow_early_exhausted_10": {"grid": [48, 32, 16], "n": 10, "adaptive": 1, "step": 0.025, "max_steps": 400000,
+                                "freqs": [230.0e9], "t_obs": 1080.0},
+}
+
+
+def build_slow_case(spec: dict):
+    """(prims list, model, params, freqs, times, t_obs) of a slow-light case."""
+    from kpolaris_b200 import synthetic
+
+    n1, n2, n3 = spec["grid"]
+    prims, model, times = synthetic.fm_torus_series(n1, n2, n3, count=spec.get("count", 16),
+                                                     dt=spec.get("dt", 10.0))
+    model.trat_large = spec.get("trat_large", 40.0)
+    nx = spec.get("nx", spec.get("n"))
+    ny = spec.get("ny", spec.get("n"))
+    params = synthetic.fmks_pass_a_params(model, nx, ny, adaptive=spec["adaptive"], step=spec["step"],
+                                          max_steps=spec["max_steps"])
+    return prims, model, params, list(spec["freqs"]), times, float(spec["t_obs"])
+
+
+def slow_conditioning_of(params, model, prims, derived, times, t_obs, freqs, ref, seeds=tuple(range(1, 9))):
+    """grmhd_conditioning_of for a slow-light image."""
+    import oracle
+
+    def run(seed):
+        oracle.set_libm_perturbation(seed, "reference_ulp")
+        return oracle.image_grmhd_slow_light(params, model, prims, derived, times, t_obs, freqs, threads=0,
+                                             kind="reference_ulp")
+
+    return conditioning_over(run, ref, seeds)
