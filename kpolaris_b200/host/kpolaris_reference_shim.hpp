@@ -8,12 +8,15 @@
 // The shim is templated on the reference's own parameter and result types
 // (PassAParams<double>, RIAFAnalyticRadiationModel<double>, ImageHostData),
 // which it reads field by field; it therefore compiles inside the reference's
-// build without this library depending on the reference's headers.  Errors
+// build without this library depending on the reference's headers.  Include it
+// after the reference's own headers (they bring in Kokkos, whose mirror views
+// the GRMHD entry points use).  Errors
 // are rethrown with the reference's exception types: KP_ERR_INVALID as
 // std::invalid_argument, everything else as std::runtime_error.
 #pragma once
 
 #include <cstring>
+#include <map>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -196,6 +199,141 @@ HostData run_riaf_multifrequency_image(const PassA& pass_a, Model model, int rad
     kp_run_options opt = shim_options();
     opt.timing = timing;
     throw_on_error(kp_image_riaf(&p, &m, radiation_substeps, frequencies.data(), nfreq, &opt, &o));
+    return out;
+}
+
+// GRMHDGridRadiationModel<Real> scalars (src/model/grmhd_grid.hpp:52-97)
+// -> kp_grmhd_model.  Only FMKS data with thermal emission (emission_type 1
+// Pandya or 4 Dexter) is built; the library rejects the rest.
+template<class Model>
+kp_grmhd_model to_c_grmhd(const Model& m) {
+    kp_grmhd_model c;
+    kp_default_grmhd_model(&c);
+    c.n1 = m.n1;
+    c.n2 = m.n2;
+    c.n3 = m.n3;
+    c.spin = double(m.spin);
+    c.gam = double(m.gam);
+    c.startx1 = double(m.startx1);
+    c.startx2 = double(m.startx2);
+    c.startx3 = double(m.startx3);
+    c.dx1 = double(m.dx1);
+    c.dx2 = double(m.dx2);
+    c.dx3 = double(m.dx3);
+    c.r_in = double(m.r_in);
+    c.r_out = double(m.r_out);
+    c.hslope = double(m.hslope);
+    c.mks_smooth = double(m.mks_smooth);
+    c.poly_alpha = double(m.poly_alpha);
+    c.poly_xt = double(m.poly_xt);
+    c.poly_norm = double(m.poly_norm);
+    c.freq_cgs = double(m.freq_cgs);
+    c.mbh_solar = double(m.mbh_solar);
+    c.M_unit = double(m.M_unit);
+    c.trat_small = double(m.trat_small);
+    c.trat_large = double(m.trat_large);
+    c.beta_crit = double(m.beta_crit);
+    c.sigma_cut = double(m.sigma_cut);
+    c.sigma_cut_high = double(m.sigma_cut_high);
+    c.ne_factor = double(m.ne_factor);
+    c.emission_type = m.emission_type;
+    c.emission_scale = double(m.emission_scale);
+    c.absorption_scale = double(m.absorption_scale);
+    c.faraday_scale = double(m.faraday_scale);
+    c.max_pol_frac = double(m.max_pol_frac);
+    c.has_derived_scalars = m.has_derived_scalars;
+    return c;
+}
+
+// A resident grid for a reference model, uploaded on first use and kept per
+// primitive View (the reference's models share their Views by reference
+// counting, so a View's data pointer identifies a snapshot).  The primitives
+// are mirrored to the host (device memory in a CUDA build of the reference)
+// and narrowed to FP32, the layout the library's grids hold.  Call
+// release_grids() when the snapshots go away.
+inline std::map<const void*, kp_grid*>& grid_cache() {
+    static std::map<const void*, kp_grid*> cache;
+    return cache;
+}
+
+inline void release_grids() {
+    for (auto& kv : grid_cache()) kp_grid_release(kv.second);
+    grid_cache().clear();
+}
+
+template<class Model>
+kp_grid* grid_for(const Model& m) {
+    const void* key = m.prims.data();
+    auto it = grid_cache().find(key);
+    if (it != grid_cache().end()) return it->second;
+    auto host = Kokkos::create_mirror_view_and_copy(Kokkos::HostSpace(), m.prims);
+    std::vector<float> prims(host.extent(0));
+    for (size_t i = 0; i < prims.size(); ++i) prims[i] = float(host(i));
+    const kp_grmhd_model c = to_c_grmhd(m);
+    kp_grid* g = nullptr;
+    throw_on_error(kp_grid_upload(&c, prims.data(), shim_options().device, &g));
+    grid_cache()[key] = g;
+    return g;
+}
+
+// run_grmhd_image (src/image/grmhd.hpp:12-18), FMKS backend.
+template<class HostData, class PassA, class Model>
+HostData run_grmhd_image(const PassA& pass_a, Model model, int radiation_substeps, int timing,
+                         int split_transport) {
+    (void)split_transport;
+    const kp_pass_a_params p = to_c(pass_a);
+    kp_grid* g = grid_for(model);
+    HostData out;
+    kp_image_out o = bind_outputs(out, p.camera.nx * p.camera.ny, 1);
+    kp_run_options opt = shim_options();
+    opt.timing = timing;
+    const double f = double(model.freq_cgs);
+    throw_on_error(kp_image_grmhd(&p, g, radiation_substeps, &f, 1, &opt, &o));
+    return out;
+}
+
+// run_grmhd_multifrequency_image (src/image/grmhd.hpp:30-37).
+template<class HostData, class PassA, class Model, class Real>
+HostData run_grmhd_multifrequency_image(const PassA& pass_a, Model model, int radiation_substeps,
+                                        const std::vector<Real>& frequencies,
+                                        const std::vector<Real>& step_control_frequencies, int timing) {
+    if (step_control_frequencies.empty())
+        throw std::invalid_argument("multifrequency step-control frequency list must not be empty");
+    if (step_control_frequencies != frequencies)
+        throw std::runtime_error("separate step-control frequency sets are not built");
+    const int nfreq = int(frequencies.size());
+    if (nfreq < 1 || nfreq > KP_MAX_FREQUENCIES)
+        throw std::invalid_argument("multifrequency image chunk size must be between 1 and KPOLARIS_MAX_FREQUENCIES");
+    const kp_pass_a_params p = to_c(pass_a);
+    kp_grid* g = grid_for(model);
+    HostData out;
+    kp_image_out o = bind_outputs(out, p.camera.nx * p.camera.ny, nfreq);
+    kp_run_options opt = shim_options();
+    opt.timing = timing;
+    std::vector<double> f(frequencies.begin(), frequencies.end());
+    throw_on_error(kp_image_grmhd(&p, g, radiation_substeps, f.data(), nfreq, &opt, &o));
+    return out;
+}
+
+// A slow-light image over resident snapshots (the images
+// run_slow_light_batch_metric produces in its default decoupled step mode,
+// src/image/slow_light_batch_driver.hpp:107-368, for one observation time):
+// `models` are the loaded snapshots at `times`.
+template<class HostData, class PassA, class Model, class Real>
+HostData run_slow_light_image(const PassA& pass_a, const std::vector<Model>& models, const std::vector<Real>& times,
+                              Real observation_time, const std::vector<Real>& frequencies) {
+    if (models.size() != times.size()) throw std::runtime_error("slow-light dump path/time list size mismatch");
+    if (models.size() < 2) throw std::runtime_error("slow-light requires at least two dump time slices");
+    const int nfreq = int(frequencies.size());
+    const kp_pass_a_params p = to_c(pass_a);
+    std::vector<const kp_grid*> grids;
+    for (const auto& m : models) grids.push_back(grid_for(m));
+    std::vector<double> t(times.begin(), times.end()), f(frequencies.begin(), frequencies.end());
+    HostData out;
+    kp_image_out o = bind_outputs(out, p.camera.nx * p.camera.ny, nfreq);
+    kp_run_options opt = shim_options();
+    throw_on_error(kp_image_grmhd_slow_light(&p, grids.data(), t.data(), int(grids.size()), double(observation_time),
+                                             1, f.data(), nfreq, &opt, &o));
     return out;
 }
 
