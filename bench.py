@@ -62,6 +62,8 @@ def parse():
     ap.add_argument("--grmhd", type=int, default=1,
                     help="also time the GRMHD image (288x128x128 FM torus, 512^2, FP64 and mixed)")
     ap.add_argument("--grmhd-steps", type=int, default=2, help="timed GRMHD images per precision")
+    ap.add_argument("--config4", type=int, default=1,
+                    help="also time the uneven 64-image batch (autotuned, graph-captured) and the slow-light job")
     return ap.parse_args()
 
 
@@ -195,6 +197,70 @@ def grmhd_section(args, torch, dev, local, stream, flush, rank):
                                    "kind": "reference",
                                    "sample": f"{rows} of {n} rows ({rows * n} pixels, spread over the image), "
                                              f"{dt:.2f} s, FP64, derived scalars precomputed"}
+    return res
+
+
+def config4_section(local, stream, flush, torch):
+    """The uneven batch: 64 seeded RIAF images (32^2..512^2, spins U[0, 0.99],
+    inclinations U[10, 170] deg, 1-4 frequencies) in one persistent launch,
+    schedule autotuned on a 1/8-resolution sample and the launch loop
+    replayed as a CUDA graph (device time from the library's events, L2
+    flushed first), beside the untuned eager schedule; plus the slow-light
+    job (16 resident snapshots of the torus 10 M apart, 256^2)."""
+    from contextlib import ExitStack
+
+    import kpolaris_b200 as kp
+    from kpolaris_b200 import _abi, configs, synthetic
+
+    jobs = configs.config4_jobs()
+    rays = sum(p.camera.nx * p.camera.ny for p, _, _ in jobs)
+    ray_freqs = sum(p.camera.nx * p.camera.ny * len(f) for p, _, f in jobs)
+    outs = [_abi.ImageHostData.allocate(p.camera.nx * p.camera.ny, len(f)) for p, _, f in jobs]
+    res = {"workload": "64 seeded RIAF images, resolutions {32,64,128,256,512}^2, spin U[0,0.99], "
+                       "inclination U[10,170] deg, 1-4 of {86,230,345,690} GHz, adaptive RK4 tol 1e-8, mixed",
+           "images": len(jobs), "rays": rays, "ray_frequencies": ray_freqs}
+
+    def timed(schedule):
+        st = _abi.BatchStats()
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        kp.batch_riaf(jobs, outs=outs, precision=_abi.PRECISION_MIXED, schedule=schedule, stats=st, device=local)
+        return st.kernel_seconds, st.launches
+
+    timed(_abi.SCHEDULE_PERSISTENT)
+    eager_s, eager_launches = timed(_abi.SCHEDULE_PERSISTENT)
+    tuning = kp.autotune_batch(configs.config4_jobs(scale=8), precision=_abi.PRECISION_MIXED, device=local)
+    timed(_abi.SCHEDULE_GRAPH)
+    graph_s, graph_launches = timed(_abi.SCHEDULE_GRAPH)
+    res["graph_tuned"] = {"seconds": graph_s, "images_per_s": len(jobs) / graph_s, "rays_per_s": rays / graph_s,
+                          "launches": graph_launches}
+    res["persistent_default"] = {"seconds": eager_s, "images_per_s": len(jobs) / eager_s,
+                                 "rays_per_s": rays / eager_s, "launches": eager_launches}
+    res["autotune"] = {"sample": "the same 64 jobs at 1/8 resolution",
+                       "blocks_per_sm": list(tuning.blocks_per_sm), "graph_cycles": tuning.graph_cycles,
+                       "candidates": tuning.candidates, "sample_seconds": tuning.seconds,
+                       "sample_default_seconds": tuning.default_seconds}
+    # slow-light job
+    prims, model, times = synthetic.fm_torus_series(288, 128, 128, count=16, dt=10.0)
+    model.trat_large = 40.0
+    params = synthetic.fmks_pass_a_params(model, 256, 256)
+    with ExitStack() as stack:
+        grids = [stack.enter_context(kp.Grid(model, p, device=local)) for p in prims]
+        out = {}
+        for name, prec in (("fp64", _abi.PRECISION_FP64), ("mixed", _abi.PRECISION_MIXED)):
+            kp.image_grmhd_slow_light(params, grids, times, 1100.0, [230e9], precision=prec,
+                                      schedule=_abi.SCHEDULE_GRAPH, device=local)
+            flush.fill_(1.0)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            img = kp.image_grmhd_slow_light(params, grids, times, 1100.0, [230e9], precision=prec,
+                                            schedule=_abi.SCHEDULE_GRAPH, device=local)
+            dt = time.perf_counter() - t0
+            out[name] = {"seconds_incl_d2h": dt, "flux_jy": synthetic.flux_jy(img.image_i[0], 230e9, 20.0, 256, 256),
+                         "reached_camera": int((img.reason == 1).sum()),
+                         "time_exhausted": int((img.reason == 6).sum())}
+    res["slow_light"] = {"workload": "16 snapshots of the 288x128x128 torus 10 M apart, all resident (5.4 GB), "
+                                     "256^2, 230 GHz, t_obs = 1100 M, graph schedule", **out}
     return res
 
 
@@ -627,6 +693,11 @@ def ours_arm(args):
         progress("GRMHD image")
         grmhd = grmhd_section(args, torch, dev, local, stream, flush, rank)
 
+    config4 = None
+    if args.config4:
+        progress("uneven batch and slow light")
+        config4 = config4_section(local, stream, flush, torch)
+
     cpu = None
     if rank == 0:
         import oracle
@@ -662,6 +733,7 @@ def ours_arm(args):
             "geodesic_steps_per_s": value * steps_per_image,
             "phases": phases, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
             "grmhd": grmhd,
+            "config4": config4,
         }
         print(json.dumps(line), flush=True)
     if pg:

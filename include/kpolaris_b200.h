@@ -6,7 +6,7 @@
  * parameter objects field for field so that the reference's C++ call sites
  * (run_riaf_image, run_riaf_multifrequency_image, run_grmhd_image,
  * run_image_batch_metric) can be forwarded here by a thin host shim
- * (kpolaris_b200/host/kpolaris_image.hpp).
+ * (kpolaris_b200/host/kpolaris_reference_shim.hpp).
  *
  * Conventions shared by every function:
  *   - return value: KP_OK (0) on success, a negative kp_status otherwise;
@@ -97,7 +97,14 @@ typedef enum kp_schedule {
     /* One thread per pixel, one launch per image: the plain form. */
     KP_SCHEDULE_PER_PIXEL = 0,
     /* Persistent kernel draining a global ray queue with per-lane refill. */
-    KP_SCHEDULE_PERSISTENT = 1
+    KP_SCHEDULE_PERSISTENT = 1,
+    /* The persistent engine with its launch loop captured in a CUDA graph:
+     * a fixed number of (far, near-A, near-B) cycles, the counter reset and
+     * the read-back of the remaining queue counts replay as one graph
+     * launch (cached per device and workload shape); rays still moving
+     * after it continue in ordinary launches.  Results are bit-identical to
+     * KP_SCHEDULE_PERSISTENT. */
+    KP_SCHEDULE_GRAPH = 2
 } kp_schedule;
 
 /* Geodesic integrator.  The reference image path uses step-doubling RK4
@@ -457,6 +464,27 @@ int kp_server_get_stats(kp_server* s, kp_server_stats* out);
  * flight end as cancelled (their outputs are not written), then the
  * server's device memory is released. */
 int kp_server_destroy(kp_server* s);
+
+/*
+ * Schedule autotuner for the persistent engine (no counterpart in the
+ * reference, whose launch shape is Kokkos's).  Times candidate schedules --
+ * CTAs per SM of each phase kernel and the number of cycles captured per
+ * graph launch -- on `jobs`, a representative sample of the caller's
+ * workload (e.g. its images at reduced resolution), with the precision of
+ * `options`, and stores the fastest in the device's tuning table: later
+ * persistent and graph launches of that precision with blocks_per_sm == 0
+ * use it.  The sample's outputs are written like kp_batch_riaf's.  Schedule
+ * choices never change results (rays resume bit-exactly from their records).
+ */
+typedef struct kp_tuning {
+    int blocks_per_sm[3];     /* far, near-A, near-B */
+    int graph_cycles;         /* (far, near-A, near-B) cycles per graph launch */
+    double seconds;           /* device time of the sample with the chosen schedule */
+    double default_seconds;   /* device time of the sample with the default schedule */
+    int candidates;           /* schedules timed */
+} kp_tuning;
+
+int kp_autotune_batch(const kp_riaf_job* jobs, int njobs, const kp_run_options* options, kp_tuning* out);
 
 /* Limits of kp_batch_riaf_noalloc's static device scratch. */
 #define KP_NOALLOC_MAX_RAYS 65536

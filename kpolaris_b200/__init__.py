@@ -21,7 +21,7 @@ __all__ = [
     "ImageHostData", "PassAParams", "RIAFModel", "RunOptions", "KPolarisError",
     "default_pass_a_params", "default_riaf_model", "default_run_options", "library",
     "run_riaf_image", "run_riaf_multifrequency_image", "image_riaf", "batch_riaf", "Server",
-    "default_server_config", "Grid", "image_grmhd", "image_grmhd_slow_light",
+    "default_server_config", "Grid", "image_grmhd", "image_grmhd_slow_light", "autotune_batch",
 ]
 
 LIB_PATH = Path(os.environ.get("KPOLARIS_B200_LIB") or Path(__file__).resolve().parent / "lib" / "libkpolaris_b200.so")
@@ -75,6 +75,8 @@ def library() -> C.CDLL:
     L.kp_image_grmhd_slow_light.argtypes = [
         C.POINTER(PassAParams), C.POINTER(C.c_void_p), C.POINTER(C.c_double), C.c_int, C.c_double, C.c_int,
         C.POINTER(C.c_double), C.c_int, C.POINTER(_abi.RunOptions), C.POINTER(_abi.ImageOut)]
+    L.kp_autotune_batch.argtypes = [C.POINTER(_abi.RiafJob), C.c_int, C.POINTER(RunOptions),
+                                    C.POINTER(_abi.Tuning)]
     L.kp_server_create.argtypes = [C.POINTER(_abi.ServerConfig), C.POINTER(C.c_void_p)]
     L.kp_server_submit.argtypes = [C.c_void_p, C.POINTER(_abi.RiafJob), C.POINTER(C.c_ulonglong)]
     L.kp_server_poll.argtypes = [C.c_void_p, C.c_ulonglong, C.POINTER(C.c_int)]
@@ -128,7 +130,8 @@ def image_riaf(params: PassAParams, model: RIAFModel, frequencies=None, *, radia
     return out
 
 
-def batch_riaf(jobs, *, outs=None, precision=_abi.PRECISION_MIXED, stats=None, **options):
+def batch_riaf(jobs, *, outs=None, precision=_abi.PRECISION_MIXED, stats=None, schedule=_abi.SCHEDULE_PERSISTENT,
+               **options):
     """Traces a list of RIAF images in one persistent launch (kp_batch_riaf).
 
     jobs: iterable of (PassAParams, RIAFModel, frequencies).  Returns a list of
@@ -150,10 +153,43 @@ def batch_riaf(jobs, *, outs=None, precision=_abi.PRECISION_MIXED, stats=None, *
         j.nfreq = len(freqs)
         j.radiation_substeps = 1
         j.out = res.as_struct()
-    opt = _options(precision=precision, schedule=_abi.SCHEDULE_PERSISTENT, **options)
+    opt = _options(precision=precision, schedule=schedule, **options)
     st = stats if stats is not None else _abi.BatchStats()
     check(L.kp_batch_riaf(arr, len(jobs), C.byref(opt), C.byref(st)))
     return results
+
+
+def _job_array(jobs, outs=None):
+    jobs = list(jobs)
+    arr = (_abi.RiafJob * max(1, len(jobs)))()
+    results = []
+    for i, (params, model, freqs) in enumerate(jobs):
+        freqs = list(freqs) if freqs is not None else [model.freq_cgs]
+        npix = params.camera.nx * params.camera.ny
+        res = outs[i] if outs is not None else ImageHostData.allocate(npix, len(freqs))
+        results.append(res)
+        j = arr[i]
+        j.params = params
+        j.model = model
+        for f, v in enumerate(freqs[:_abi.KP_MAX_FREQUENCIES]):
+            j.frequencies[f] = v
+        j.nfreq = len(freqs)
+        j.radiation_substeps = 1
+        j.out = res.as_struct()
+    return arr, len(jobs), results
+
+
+def autotune_batch(jobs, *, precision=_abi.PRECISION_MIXED, device=0) -> _abi.Tuning:
+    """kp_autotune_batch: times candidate schedules of the persistent engine
+    (CTAs per SM per phase, cycles per graph launch) on `jobs`, a
+    representative sample of the workload, and makes the fastest the
+    device's default for that precision.  Returns the choice and timings."""
+    L = library()
+    arr, n, _ = _job_array(jobs)
+    opt = _options(precision=precision, schedule=_abi.SCHEDULE_GRAPH, device=device)
+    t = _abi.Tuning()
+    check(L.kp_autotune_batch(arr, n, C.byref(opt), C.byref(t)))
+    return t
 
 
 class Grid:
@@ -203,7 +239,8 @@ def image_grmhd(params: PassAParams, grid: Grid, frequencies=None, *, radiation_
         out = ImageHostData.allocate(npix, nfreq)
     fa = (C.c_double * max(nfreq, 1))(*frequencies)
     s = out.as_struct()
-    opt = _options(device=grid.device, **options)
+    options.setdefault("device", grid.device)
+    opt = _options(**options)
     check(L.kp_image_grmhd(C.byref(params), grid._h, int(radiation_substeps), fa, nfreq, C.byref(opt), C.byref(s)))
     return out
 
@@ -230,7 +267,8 @@ def image_grmhd_slow_light(params: PassAParams, snapshots, times, observation_ti
         raise ValueError("one time per snapshot")
     fa = (C.c_double * max(nfreq, 1))(*frequencies)
     s = out.as_struct()
-    opt = _options(device=grids[0].device, **options)
+    options.setdefault("device", grids[0].device)
+    opt = _options(**options)
     check(L.kp_image_grmhd_slow_light(C.byref(params), handles, ta, len(grids), float(observation_time),
                                       int(radiation_substeps), fa, nfreq, C.byref(opt), C.byref(s)))
     return out

@@ -50,6 +50,7 @@ PRECISION_MIXED = 1
 
 SCHEDULE_PER_PIXEL = 0
 SCHEDULE_PERSISTENT = 1
+SCHEDULE_GRAPH = 2
 
 INTEGRATOR_STEP_DOUBLING_RK4 = 0
 INTEGRATOR_CASH_KARP = 1
@@ -186,6 +187,14 @@ class BatchStats(C.Structure):
         ("launches", C.c_int), ("blocks", C.c_int), ("threads_per_block", C.c_int),
         ("device_output_bytes", C.c_size_t),
         ("phase_seconds", C.c_double * 3), ("phase_launches", C.c_int * 3),
+    ]
+
+
+class Tuning(C.Structure):
+    """kp_tuning: the schedule kp_autotune_batch chose and its timings."""
+    _fields_ = [
+        ("blocks_per_sm", C.c_int * 3), ("graph_cycles", C.c_int), ("seconds", C.c_double),
+        ("default_seconds", C.c_double), ("candidates", C.c_int),
     ]
 
 

@@ -131,3 +131,30 @@ def flux_scale_jy_per_pixel(params: _abi.PassAParams, mbh_solar: float,
     py = width_y * l_unit / params.camera.ny
     solid = px * py / (dsource_cm * dsource_cm)
     return solid / JY_CGS
+
+
+CONFIG4_RESOLUTIONS = (32, 64, 128, 256, 512)
+
+
+def config4_jobs(count: int = 64, seed: int = 2026, scale: int = 1):
+    """The uneven batch: `count` RIAF images with resolutions drawn from
+    {32, 64, 128, 256, 512}^2 (divided by `scale`, at least 8), spins
+    U[0, 0.99], inclinations U[10, 170] deg and 1-4 of the config-2
+    frequencies each (seeded), with config 2's integration and transfer
+    controls.  Returns [(params, model, frequencies)]."""
+    import numpy as np
+
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for _ in range(count):
+        n = max(8, int(rng.choice(CONFIG4_RESOLUTIONS)) // int(scale))
+        spin = float(rng.uniform(0.0, 0.99))
+        inc = float(rng.uniform(10.0, 170.0))
+        nf = int(rng.integers(1, 5))
+        freqs = [CONFIG2_FREQS[i] for i in sorted(rng.choice(4, size=nf, replace=False))]
+        params, model, _ = config2(n, n)
+        params.spin = spin
+        params.inner_radius = reference_horizon(spin) * 1.05
+        params.camera.inclination = inclination_from_degrees(inc)
+        jobs.append((params, model, freqs))
+    return jobs

@@ -41,6 +41,18 @@ int cuda_error(cudaError_t e, const char* what) {
 // Launches of one wavefront batch run in cycles of (far, near-A, near-B)
 // until no ray is left.
 constexpr int kMaxWaveCycles = 24;
+// engine families (scene x policy) of run_wave_jobs
+enum : int {
+    kFamilyRiafFP64 = 0,
+    kFamilyRiafMixed = 1,
+    kFamilyGrmhdFP64 = 2,
+    kFamilyGrmhdMixed = 3,
+    kFamilyGrmhdSlowFP64 = 4,
+    kFamilyGrmhdSlowMixed = 5,
+    kFamilyCount = 6
+};
+constexpr int kDefaultGraphCycles = 3;
+constexpr size_t kGraphCacheSize = 8;
 
 // Device-side counters of one batch, zeroed before its first launch.  The
 // queue a phase reads in its g-th launch is generation g of that phase:
@@ -74,6 +86,23 @@ struct DeviceState {
     unsigned* h_left = nullptr;     // pinned: queue counts after a cycle
     void* d_series = nullptr;       // slow light: snapshot table and times (grow-only)
     size_t series_bytes = 0;
+    // schedule tuning per engine family (kp_autotune_batch): CTAs per SM of
+    // each phase kernel (0: occupancy-derived) and cycles per graph launch
+    int tuned_per_sm[kFamilyCount][kPhases] = {};
+    int tuned_cycles[kFamilyCount] = {};
+    // instantiated launch graphs (KP_SCHEDULE_GRAPH), keyed by everything
+    // they bake in; the oldest is dropped beyond kGraphCacheSize
+    struct GraphEntry {
+        int family, nf_max, njobs, cycles;
+        long long total;
+        int blocks[kPhases];
+        const void* jobs;
+        const void* pool;
+        const void* ctrl;
+        const void* ids[kPhases][2];
+        cudaGraphExec_t exec;
+    };
+    std::vector<GraphEntry> graphs;
     cudaEvent_t ev_launch[kMaxWaveCycles * kPhases + 1] = {};  // per-launch timing
 };
 
@@ -448,15 +477,6 @@ int ensure_job_table(DeviceState* dev, int njobs) {
 // dev->h_jobs (total rays): uploads them, grows the record pool, launches
 // cycles of (far, near-A, near-B) until no ray is left and checks the status
 // word.  The caller holds g_mutex.
-enum : int {
-    kFamilyRiafFP64 = 0,
-    kFamilyRiafMixed = 1,
-    kFamilyGrmhdFP64 = 2,
-    kFamilyGrmhdMixed = 3,
-    kFamilyGrmhdSlowFP64 = 4,
-    kFamilyGrmhdSlowMixed = 5
-};
-
 int run_wave_jobs(DeviceState* dev, cudaStream_t stream, int njobs, long long total, int family, int nf_max,
                   const kp_run_options& opt, kp_batch_stats* stats) {
     // ray records and id queues, grow-only
@@ -484,8 +504,12 @@ int run_wave_jobs(DeviceState* dev, cudaStream_t stream, int njobs, long long to
                                     cudaMemcpyHostToDevice, stream);
     if (e != cudaSuccess) return cuda_error(e, "cudaMemcpyAsync(job table)");
     cudaEventRecord(dev->staging_free, stream);
-    e = cudaMemsetAsync(dev->d_ctrl, 0, sizeof(WaveCtrl), stream);
-    if (e != cudaSuccess) return cuda_error(e, "cudaMemsetAsync(wave counters)");
+    // graphs need a capturable stream: not the legacy default stream
+    const bool graph = opt.schedule == KP_SCHEDULE_GRAPH && stream != nullptr;
+    if (!graph) {
+        e = cudaMemsetAsync(dev->d_ctrl, 0, sizeof(WaveCtrl), stream);
+        if (e != cudaSuccess) return cuda_error(e, "cudaMemsetAsync(wave counters)");
+    }
     if (opt.threads_per_block != 0)
         return set_error(KP_ERR_INVALID, "threads_per_block is fixed by the wavefront kernels (%d far, %d near): pass 0",
                          kFarThreads, kNearThreads);
@@ -493,6 +517,7 @@ int run_wave_jobs(DeviceState* dev, cudaStream_t stream, int njobs, long long to
     int blocks[kPhases];
     for (int phase = 0; phase < kPhases; ++phase) {
         int per_sm = opt.blocks_per_sm;
+        if (per_sm <= 0) per_sm = dev->tuned_per_sm[family][phase];
         if (per_sm <= 0) {
             const int th = wave_threads(phase);
             per_sm = family == kFamilyGrmhdFP64        ? wave_occupancy_grmhd(phase, nf_max, th)
@@ -543,16 +568,79 @@ int run_wave_jobs(DeviceState* dev, cudaStream_t stream, int njobs, long long to
     cudaEventRecord(dev->ev0, stream);
     int launches = 0;
     int cycle = 0;
-    while (true) {
+    if (graph) {
+        // counter reset, `cycles` cycles of launches and the read-back of the
+        // next generation's counts, captured once per workload shape
+        const int cycles = dev->tuned_cycles[family] > 0 ? min_val(dev->tuned_cycles[family], kMaxWaveCycles)
+                                                        : kDefaultGraphCycles;
+        DeviceState::GraphEntry key;
+        std::memset(&key, 0, sizeof(key));
+        key.family = family;
+        key.nf_max = nf_max;
+        key.njobs = njobs;
+        key.cycles = cycles;
+        key.total = total;
+        for (int p = 0; p < kPhases; ++p) {
+            key.blocks[p] = blocks[p];
+            key.ids[p][0] = dev->d_ids[p][0];
+            key.ids[p][1] = dev->d_ids[p][1];
+        }
+        key.jobs = dev->d_jobs;
+        key.pool = dev->d_pool;
+        key.ctrl = dev->d_ctrl;
+        cudaGraphExec_t exec = nullptr;
+        for (const auto& g : dev->graphs) {
+            if (g.family == key.family && g.nf_max == key.nf_max && g.njobs == key.njobs && g.cycles == key.cycles &&
+                g.total == key.total && std::memcmp(g.blocks, key.blocks, sizeof(key.blocks)) == 0 &&
+                g.jobs == key.jobs && g.pool == key.pool && g.ctrl == key.ctrl &&
+                std::memcmp(g.ids, key.ids, sizeof(key.ids)) == 0) {
+                exec = g.exec;
+                break;
+            }
+        }
+        if (!exec) {
+            e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
+            if (e != cudaSuccess) return cuda_error(e, "cudaStreamBeginCapture");
+            cudaError_t ce = cudaMemsetAsync(dev->d_ctrl, 0, sizeof(WaveCtrl), stream);
+            for (int c = 0; c < cycles && ce == cudaSuccess; ++c)
+                for (int phase = 0; phase < kPhases && ce == cudaSuccess; ++phase) ce = launch(c, phase);
+            if (ce == cudaSuccess)
+                ce = cudaMemcpyAsync(dev->h_left, ctrl->counts[cycles], sizeof(unsigned) * kPhases,
+                                     cudaMemcpyDeviceToHost, stream);
+            cudaGraph_t g = nullptr;
+            e = cudaStreamEndCapture(stream, &g);
+            if (ce != cudaSuccess || e != cudaSuccess) {
+                if (g) cudaGraphDestroy(g);
+                cudaGetLastError();
+                return cuda_error(ce != cudaSuccess ? ce : e, "capturing the launch graph");
+            }
+            e = cudaGraphInstantiate(&exec, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) return cuda_error(e, "cudaGraphInstantiate");
+            if (dev->graphs.size() >= kGraphCacheSize) {
+                cudaGraphExecDestroy(dev->graphs.front().exec);
+                dev->graphs.erase(dev->graphs.begin());
+            }
+            key.exec = exec;
+            dev->graphs.push_back(key);
+        }
+        e = cudaGraphLaunch(exec, stream);
+        if (e != cudaSuccess) return cuda_error(e, "cudaGraphLaunch");
+        launches = cycles * kPhases;
+        cycle = cycles;
+        e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) return cuda_error(e, "wavefront graph");
+    }
+    while (!graph || dev->h_left[0] != 0 || dev->h_left[1] != 0 || dev->h_left[2] != 0) {
         if (cycle >= kMaxWaveCycles)
             return set_error(KP_ERR_TIMEOUT, "rays still moving between phases after %d launches", launches);
         for (int phase = 0; phase < kPhases; ++phase) {
-            if (stats) cudaEventRecord(dev->ev_launch[launches], stream);
+            if (stats && !graph) cudaEventRecord(dev->ev_launch[launches], stream);
             e = launch(cycle, phase);
             if (e != cudaSuccess) return cuda_error(e, "wavefront kernel launch");
             ++launches;
         }
-        if (stats) cudaEventRecord(dev->ev_launch[launches], stream);
+        if (stats && !graph) cudaEventRecord(dev->ev_launch[launches], stream);
         ++cycle;
         e = cudaMemcpyAsync(dev->h_left, ctrl->counts[cycle], sizeof(unsigned) * kPhases, cudaMemcpyDeviceToHost,
                             stream);
@@ -574,7 +662,8 @@ int run_wave_jobs(DeviceState* dev, cudaStream_t stream, int njobs, long long to
     cudaEventElapsedTime(&ms, dev->ev0, dev->ev1);
     if (stats) {
         stats->kernel_seconds = ms * 1e-3;
-        for (int k = 0; k < launches; ++k) {
+        // per-launch times need events between launches: eager schedules only
+        for (int k = 0; k < launches && !graph; ++k) {
             float lms = 0.f;
             cudaEventElapsedTime(&lms, dev->ev_launch[k], dev->ev_launch[k + 1]);
             stats->phase_seconds[k % kPhases] += lms * 1e-3;
@@ -609,6 +698,8 @@ size_t kp_abi_sizeof(int which) {
     case 6: return sizeof(JobDesc);
     case 7: return sizeof(kp_riaf_job);
     case 8: return sizeof(kp_batch_stats);
+    case 9: return sizeof(kp_tuning);
+    case 10: return sizeof(kp_grmhd_model);
     default: return 0;
     }
 }
@@ -709,7 +800,7 @@ int kp_image_riaf(const kp_pass_a_params* params, const kp_riaf_model* model, in
         return set_error(KP_ERR_INVALID, "unknown integrator %d", opt.integrator);
     if (opt.precision != KP_PRECISION_FP64 && opt.precision != KP_PRECISION_MIXED)
         return set_error(KP_ERR_INVALID, "unknown precision %d", opt.precision);
-    if (opt.precision == KP_PRECISION_MIXED || opt.schedule == KP_SCHEDULE_PERSISTENT) {
+    if (opt.precision == KP_PRECISION_MIXED || opt.schedule != KP_SCHEDULE_PER_PIXEL) {
         // the persistent engine: a batch of one
         kp_riaf_job job;
         std::memset(&job, 0, sizeof(job));
@@ -856,6 +947,93 @@ int kp_batch_riaf(const kp_riaf_job* jobs, int njobs, const kp_run_options* opti
         if (stats) stats->copy_seconds = s;
         if (opt.timing) std::printf("timing image_device_to_host_batch %g s\n", s);
     }
+    return KP_OK;
+}
+
+int kp_autotune_batch(const kp_riaf_job* jobs, int njobs, const kp_run_options* options, kp_tuning* out) {
+    if (!out) return set_error(KP_ERR_INVALID, "kp_autotune_batch: null result");
+    std::memset(out, 0, sizeof(*out));
+    if (njobs < 1 || !jobs) return set_error(KP_ERR_INVALID, "kp_autotune_batch: empty sample");
+    kp_run_options opt;
+    if (options) {
+        opt = *options;
+    } else {
+        kp_default_run_options(&opt);
+    }
+    if (opt.blocks_per_sm != 0) return set_error(KP_ERR_INVALID, "blocks_per_sm must be 0: the tuner chooses it");
+    if (opt.precision != KP_PRECISION_FP64 && opt.precision != KP_PRECISION_MIXED)
+        return set_error(KP_ERR_INVALID, "unknown precision %d", opt.precision);
+    const int family = opt.precision == KP_PRECISION_MIXED ? kFamilyRiafMixed : kFamilyRiafFP64;
+    int nf_max = 1;
+    for (int i = 0; i < njobs; ++i)
+        if (jobs[i].nfreq > 1) nf_max = KP_MAX_FREQUENCIES;
+    if (opt.precision == KP_PRECISION_MIXED) nf_max = KP_MAX_FREQUENCIES;
+    int limit[kPhases];
+    {
+        std::lock_guard<std::mutex> lock(g_mutex);
+        int st = KP_OK;
+        DeviceState* dev = device_state(opt.device, &st);
+        if (!dev) return st;
+        for (int phase = 0; phase < kPhases; ++phase) {
+            const int th = wave_threads(phase);
+            const int occ = family == kFamilyRiafMixed ? wave_occupancy_mixed(phase, th)
+                                                       : wave_occupancy_fp64(phase, nf_max, th);
+            limit[phase] = occ < 1 ? 1 : (occ > 4 ? 4 : occ);
+        }
+    }
+    auto set_table = [&](const int per_sm[kPhases], int cycles) {
+        std::lock_guard<std::mutex> lock(g_mutex);
+        DeviceState& dev = g_dev[opt.device];
+        for (int p = 0; p < kPhases; ++p) dev.tuned_per_sm[family][p] = per_sm[p];
+        dev.tuned_cycles[family] = cycles;
+    };
+    // device time of the sample under a schedule: the better of two runs
+    auto time_sample = [&](int schedule, double* seconds) -> int {
+        kp_run_options o = opt;
+        o.schedule = schedule;
+        double best = 0.0;
+        for (int rep = 0; rep < 2; ++rep) {
+            kp_batch_stats stats;
+            const int st = kp_batch_riaf(jobs, njobs, &o, &stats);
+            if (st != KP_OK) return st;
+            if (rep == 0 || stats.kernel_seconds < best) best = stats.kernel_seconds;
+        }
+        *seconds = best;
+        return KP_OK;
+    };
+    const int none[kPhases] = {0, 0, 0};
+    set_table(none, 0);
+    double t_default = 0.0;
+    int st = time_sample(KP_SCHEDULE_PERSISTENT, &t_default);
+    if (st != KP_OK) return st;
+    static const int kCycleChoices[] = {2, 3, 4, 6};
+    int best[kPhases] = {0, 0, 0}, best_cycles = 0, n = 0;
+    double t_best = 0.0;
+    for (int far = 1; far <= limit[kPhaseFar]; ++far)
+        for (int na = 1; na <= limit[kPhaseNearA]; ++na)
+            for (int nb = 1; nb <= limit[kPhaseNearB]; ++nb)
+                for (int cycles : kCycleChoices) {
+                    const int cand[kPhases] = {far, na, nb};
+                    set_table(cand, cycles);
+                    double t = 0.0;
+                    st = time_sample(KP_SCHEDULE_GRAPH, &t);
+                    if (st != KP_OK) {
+                        set_table(none, 0);
+                        return st;
+                    }
+                    ++n;
+                    if (n == 1 || t < t_best) {
+                        t_best = t;
+                        best_cycles = cycles;
+                        for (int p = 0; p < kPhases; ++p) best[p] = cand[p];
+                    }
+                }
+    set_table(best, best_cycles);
+    for (int p = 0; p < kPhases; ++p) out->blocks_per_sm[p] = best[p];
+    out->graph_cycles = best_cycles;
+    out->seconds = t_best;
+    out->default_seconds = t_default;
+    out->candidates = n;
     return KP_OK;
 }
 
