@@ -452,6 +452,21 @@ int kp_server_create(const kp_server_config* cfg, kp_server** out);
  * The job's host output buffers must stay valid until it is done, cancelled
  * or failed. */
 int kp_server_submit(kp_server* s, const kp_riaf_job* job, unsigned long long* ticket);
+
+/* A GRMHD image job for the serving loop: the FMKS image of a resident grid
+ * (as kp_image_grmhd).  The grid must live on the server's device; a
+ * kp_grid_release while jobs still use the grid takes effect when the last
+ * of them ends. */
+typedef struct kp_grmhd_job {
+    kp_pass_a_params params;
+    const kp_grid* grid;
+    double frequencies[KP_MAX_FREQUENCIES];
+    int nfreq;
+    int radiation_substeps;
+    kp_image_out out;
+} kp_grmhd_job;
+
+int kp_server_submit_grmhd(kp_server* s, const kp_grmhd_job* job, unsigned long long* ticket);
 int kp_server_poll(kp_server* s, unsigned long long ticket, int* state);
 /* Waits until the job is done, cancelled or failed, or `timeout_seconds`
  * pass (KP_ERR_TIMEOUT).  Returns the job's failure status if it failed. */

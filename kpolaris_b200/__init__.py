@@ -79,6 +79,7 @@ def library() -> C.CDLL:
                                     C.POINTER(_abi.Tuning)]
     L.kp_server_create.argtypes = [C.POINTER(_abi.ServerConfig), C.POINTER(C.c_void_p)]
     L.kp_server_submit.argtypes = [C.c_void_p, C.POINTER(_abi.RiafJob), C.POINTER(C.c_ulonglong)]
+    L.kp_server_submit_grmhd.argtypes = [C.c_void_p, C.POINTER(_abi.GrmhdJob), C.POINTER(C.c_ulonglong)]
     L.kp_server_poll.argtypes = [C.c_void_p, C.c_ulonglong, C.POINTER(C.c_int)]
     L.kp_server_wait.argtypes = [C.c_void_p, C.c_ulonglong, C.c_double]
     L.kp_server_cancel.argtypes = [C.c_void_p, C.c_ulonglong]
@@ -317,6 +318,27 @@ class Server:
         job.out = res.as_struct()
         t = C.c_ulonglong(0)
         check(library().kp_server_submit(self._h, C.byref(job), C.byref(t)))
+        self._keep[t.value] = res
+        return t.value
+
+    def submit_grmhd(self, params: PassAParams, grid: "Grid", frequencies=None, *,
+                     out: ImageHostData | None = None) -> int:
+        """Queues one GRMHD image of a resident grid (kp_server_submit_grmhd);
+        returns its ticket.  The grid stays allocated until the job ends even
+        if it is released meanwhile."""
+        freqs = list(frequencies) if frequencies is not None else [grid.model.freq_cgs]
+        npix = params.camera.nx * params.camera.ny
+        res = out if out is not None else ImageHostData.allocate(npix, len(freqs))
+        job = _abi.GrmhdJob()
+        job.params = params
+        job.grid = grid._h.value
+        for f, v in enumerate(freqs[:_abi.KP_MAX_FREQUENCIES]):
+            job.frequencies[f] = v
+        job.nfreq = len(freqs)
+        job.radiation_substeps = 1
+        job.out = res.as_struct()
+        t = C.c_ulonglong(0)
+        check(library().kp_server_submit_grmhd(self._h, C.byref(job), C.byref(t)))
         self._keep[t.value] = res
         return t.value
 

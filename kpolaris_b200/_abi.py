@@ -181,6 +181,15 @@ class RiafJob(C.Structure):
     ]
 
 
+class GrmhdJob(C.Structure):
+    """kp_grmhd_job: a GRMHD image of a resident grid for the serving loop."""
+    _fields_ = [
+        ("params", PassAParams), ("grid", C.c_void_p),
+        ("frequencies", C.c_double * KP_MAX_FREQUENCIES), ("nfreq", C.c_int),
+        ("radiation_substeps", C.c_int), ("out", ImageOut),
+    ]
+
+
 class BatchStats(C.Structure):
     _fields_ = [
         ("kernel_seconds", C.c_double), ("copy_seconds", C.c_double), ("rays", C.c_longlong),

@@ -422,17 +422,46 @@ ImageConsts make_consts(const kp_pass_a_params* p, const kp_riaf_model* m, const
 
 using namespace kp;
 
-// A GRMHD snapshot resident on one device.
-struct kp_grid {
-    int device = 0;
-    kp_grmhd_model model;
-    float* prims = nullptr;     // [8][n1][n2][n3]
-    double* derived = nullptr;  // [5][n1][n2][n3] or null
-};
-
 namespace kp {
 
 GridConsts grid_consts(const kp_grid* g) { return grid_consts_of(g->model, g->prims, g->derived); }
+
+// Checks of one GRMHD image request before anything is launched (the FMKS
+// backend of run_grmhd_image, src/image/grmhd.cpp:22-59, and this library's
+// limits).
+int validate_grmhd(const kp_pass_a_params* params, const kp_grid* grid, const double* frequencies, int nfreq,
+                   int radiation_substeps, int device) {
+    if (!params || !grid) return set_error(KP_ERR_INVALID, "GRMHD image: null argument");
+    if (grid->released.load()) return set_error(KP_ERR_INVALID, "the grid has been released");
+    if (params->coordinate_system != KP_COORD_FMKS)
+        return set_error(KP_ERR_UNSUPPORTED, "GRMHD image coordinate backend not built: only fmks is");
+    if (params->camera.nx <= 0 || params->camera.ny <= 0 || params->camera.nx > 2147483647 / params->camera.ny)
+        return set_error(KP_ERR_INVALID, "image dimensions must have a positive int-sized product");
+    if (nfreq < 1 || nfreq > KP_MAX_FREQUENCIES)
+        return set_error(KP_ERR_INVALID, "multifrequency image chunk size must be between 1 and KP_MAX_FREQUENCIES (%d)",
+                         KP_MAX_FREQUENCIES);
+    if (nfreq > 1 && !frequencies) return set_error(KP_ERR_INVALID, "null frequency list");
+    if (params->camera.model != KP_CAMERA_PINHOLE)
+        return set_error(KP_ERR_UNSUPPORTED, "only the pinhole camera is built for the GPU image path");
+    if (params->direct_only) return set_error(KP_ERR_UNSUPPORTED, "direct_only transport is not built");
+    if (radiation_substeps < 1) return set_error(KP_ERR_INVALID, "radiation_substeps must be positive");
+    if (grid->model.spin != params->spin) return set_error(KP_ERR_INVALID, "grid spin differs from the metric spin");
+    if (device != grid->device) return set_error(KP_ERR_INVALID, "the grid lives on device %d", grid->device);
+    return KP_OK;
+}
+
+void grid_unref(kp_grid* g, int n) {
+    const int left = n ? g->users.fetch_sub(n) - n : g->users.load();
+    if (left == 0 && g->released.load() && !g->freed.exchange(true)) {
+        int cur = 0;
+        cudaGetDevice(&cur);
+        cudaSetDevice(g->device);
+        cudaFree(g->prims);
+        cudaFree(g->derived);
+        cudaSetDevice(cur);
+        delete g;
+    }
+}
 
 int validate_grmhd_model(const kp_grmhd_model* m) {
     if (!m) return set_error(KP_ERR_INVALID, "null GRMHD model");
@@ -700,6 +729,7 @@ size_t kp_abi_sizeof(int which) {
     case 8: return sizeof(kp_batch_stats);
     case 9: return sizeof(kp_tuning);
     case 10: return sizeof(kp_grmhd_model);
+    case 11: return sizeof(kp_grmhd_job);
     default: return 0;
     }
 }
@@ -1113,10 +1143,10 @@ int kp_grid_derived(const kp_grid* g, double* out) {
 
 int kp_grid_release(kp_grid* g) {
     if (!g) return KP_OK;
-    cudaSetDevice(g->device);
-    cudaFree(g->prims);
-    cudaFree(g->derived);
-    delete g;
+    // a grid that queued or running server jobs still read is freed when
+    // the last of them ends (kp::grid_unref)
+    g->released.store(true);
+    kp::grid_unref(g, 0);
     return KP_OK;
 }
 
@@ -1148,24 +1178,12 @@ int grmhd_image(const kp_pass_a_params* params, const kp_grid* const* grids, con
     } else {
         kp_default_run_options(&opt);
     }
-    if (params->coordinate_system != KP_COORD_FMKS)
-        return set_error(KP_ERR_UNSUPPORTED, "GRMHD image coordinate backend not built: only fmks is");
-    if (params->camera.nx <= 0 || params->camera.ny <= 0 || params->camera.nx > 2147483647 / params->camera.ny)
-        return set_error(KP_ERR_INVALID, "image dimensions must have a positive int-sized product");
-    if (nfreq < 1 || nfreq > KP_MAX_FREQUENCIES)
-        return set_error(KP_ERR_INVALID, "multifrequency image chunk size must be between 1 and KP_MAX_FREQUENCIES (%d)",
-                         KP_MAX_FREQUENCIES);
-    if (nfreq > 1 && !frequencies) return set_error(KP_ERR_INVALID, "null frequency list");
-    if (params->camera.model != KP_CAMERA_PINHOLE)
-        return set_error(KP_ERR_UNSUPPORTED, "only the pinhole camera is built for the GPU image path");
-    if (params->direct_only) return set_error(KP_ERR_UNSUPPORTED, "direct_only transport is not built");
-    if (radiation_substeps < 1) return set_error(KP_ERR_INVALID, "radiation_substeps must be positive");
-    if (grid->model.spin != params->spin) return set_error(KP_ERR_INVALID, "grid spin differs from the metric spin");
+    int vst = kp::validate_grmhd(params, grid, frequencies, nfreq, radiation_substeps, opt.device);
+    if (vst != KP_OK) return vst;
     if (opt.precision != KP_PRECISION_FP64 && opt.precision != KP_PRECISION_MIXED)
         return set_error(KP_ERR_INVALID, "unknown precision %d", opt.precision);
     if (opt.integrator != KP_INTEGRATOR_STEP_DOUBLING_RK4 && opt.integrator != KP_INTEGRATOR_CASH_KARP)
         return set_error(KP_ERR_INVALID, "unknown integrator %d", opt.integrator);
-    if (opt.device != grid->device) return set_error(KP_ERR_INVALID, "the grid lives on device %d", grid->device);
     const bool slow = nsnap != 0;
     if (slow) {
         if (nsnap < 2) return set_error(KP_ERR_INVALID, "slow-light requires at least two snapshots");
@@ -1173,6 +1191,7 @@ int grmhd_image(const kp_pass_a_params* params, const kp_grid* const* grids, con
         if (!std::isfinite(t_obs)) return set_error(KP_ERR_INVALID, "observation time must be finite");
         for (int i = 0; i < nsnap; ++i) {
             if (!grids[i]) return set_error(KP_ERR_INVALID, "null snapshot %d", i);
+            if (grids[i]->released.load()) return set_error(KP_ERR_INVALID, "snapshot %d has been released", i);
             if (grids[i]->device != opt.device)
                 return set_error(KP_ERR_INVALID, "snapshot %d lives on device %d", i, grids[i]->device);
             if (!same_grid_geometry(grid->model, grids[i]->model))
@@ -1245,7 +1264,10 @@ int grmhd_image(const kp_pass_a_params* params, const kp_grid* const* grids, con
     if (mixed) grmhd_emission_scale(params, grid->model, d.c);
     const int family = slow ? (mixed ? kFamilyGrmhdSlowMixed : kFamilyGrmhdSlowFP64)
                             : (mixed ? kFamilyGrmhdMixed : kFamilyGrmhdFP64);
-    st = run_wave_jobs(dev, stream, 1, npix, family, nfreq == 1 ? 1 : KP_MAX_FREQUENCIES, opt, nullptr);
+    // mixed kernels are compiled with FMA contraction: one frequency form
+    // for all mixed work keeps an image bit-identical here and in the server
+    const int nf_form = (mixed || nfreq > 1) ? KP_MAX_FREQUENCIES : 1;
+    st = run_wave_jobs(dev, stream, 1, npix, family, nf_form, opt, nullptr);
     if (st != KP_OK) return st;
     if (!opt.outputs_on_device) {
         st = copy_outputs_to_host(dptr, out, npix, nfreq, stream);

@@ -9,13 +9,33 @@
 #pragma once
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 
 #include "kp_common.cuh"
 #include "kpolaris_b200.h"
 
+// A GRMHD snapshot resident on one device.  `users` counts the server jobs
+// that read it (queued or running); a released grid is freed when the count
+// drops to zero.
+struct kp_grid {
+    int device = 0;
+    kp_grmhd_model model;
+    float* prims = nullptr;     // [8][n1][n2][n3]
+    double* derived = nullptr;  // [5][n1][n2][n3] or null
+    std::atomic<int> users{0};
+    std::atomic<bool> released{false};
+    std::atomic<bool> freed{false};
+};
+
 namespace kp {
+
+inline void grid_ref(kp_grid* g) { g->users.fetch_add(1); }
+
+// Drops `n` users (0: none, just re-checks) and frees the grid once it is
+// released and unused (kp_capi.cu).
+void grid_unref(kp_grid* g, int n);
 
 inline double grmhd_length_unit_cgs(const kp_grmhd_model& m) {
     const double gnewt = 6.67430e-8, msun = 1.98847e33, cl = 2.99792458e10;

@@ -48,4 +48,22 @@ int wave_occupancy_grmhd_mixed(int phase, int nf_max, int threads) {
     return n;
 }
 
+// Initial records of newly admitted GRMHD jobs' rays for the serving loop,
+// compiled with this file's contraction so a served image starts from the
+// same camera rays as kp_image_grmhd's mixed far kernel.
+__global__ void __launch_bounds__(128) seed_grmhd_mixed(const JobDesc* jobs, const SeedEntry* entries,
+                                                       const long long* prefix, int nentries, RayRecord* pool,
+                                                       unsigned* far_ids, unsigned* far_count) {
+    seed_body<SceneGrmhd>(jobs, entries, prefix, nentries, pool, far_ids, far_count);
+}
+
+cudaError_t launch_seed_grmhd_mixed(const JobDesc* jobs, const SeedEntry* entries, const long long* prefix,
+                                    int nentries, long long total, RayRecord* pool, unsigned* far_ids,
+                                    unsigned* far_count, cudaStream_t stream) {
+    if (total <= 0) return cudaSuccess;
+    const int grid = int((total + 127) / 128);
+    seed_grmhd_mixed<<<grid, 128, 0, stream>>>(jobs, entries, prefix, nentries, pool, far_ids, far_count);
+    return cudaGetLastError();
+}
+
 }  // namespace kp

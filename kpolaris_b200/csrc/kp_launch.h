@@ -45,6 +45,9 @@ int wave_occupancy_grmhd(int phase, int nf_max, int threads);
 cudaError_t launch_wave_grmhd_mixed(int phase, const WaveDesc& W, int nf_max, int blocks, int threads,
                                     cudaStream_t stream);
 int wave_occupancy_grmhd_mixed(int phase, int nf_max, int threads);
+cudaError_t launch_seed_grmhd_mixed(const JobDesc* jobs, const SeedEntry* entries, const long long* prefix,
+                                    int nentries, long long total, RayRecord* pool, unsigned* far_ids,
+                                    unsigned* far_count, cudaStream_t stream);
 // Slow-light GRMHD (kp_kernels_grmhd_slow.cu, kp_kernels_grmhd_slow_mixed.cu).
 cudaError_t launch_wave_grmhd_slow(int phase, const WaveDesc& W, int nf_max, int blocks, int threads,
                                    cudaStream_t stream);

@@ -23,6 +23,8 @@
 #include <unordered_map>
 #include <vector>
 
+#include "kp_fmks.cuh"
+#include "kp_grmhd_setup.h"
 #include "kp_launch.h"
 #include "kp_range_alloc.h"
 #include "kpolaris_b200.h"
@@ -33,6 +35,8 @@ int set_error(int code, const char* fmt, ...);
 int cuda_error(cudaError_t e, const char* what);
 int check_outputs(const kp_image_out* out, int npix, int nfreq);
 int validate_riaf(const kp_pass_a_params* p, const kp_riaf_model* m, const double* freqs, int nfreq);
+int validate_grmhd(const kp_pass_a_params* params, const kp_grid* grid, const double* frequencies, int nfreq,
+                   int radiation_substeps, int device);
 ImageConsts make_consts(const kp_pass_a_params* p, const kp_riaf_model* m, const double* freqs, int nfreq,
                         int integrator);
 ImageOutPtrs carve_outputs(void* base, int npix, int nfreq);
@@ -44,9 +48,17 @@ namespace {
 using Clock = std::chrono::steady_clock;
 constexpr long long kOutUnit = 256;  // bytes per output-arena unit
 
+// Scenes the server traces; each has its own phase queues.
+enum : int { kServeRiaf = 0, kServeGrmhd = 1, kServeScenes = 2 };
+
 struct ServerJob {
     unsigned long long ticket = 0;
-    kp_riaf_job req;
+    int scene = kServeRiaf;
+    kp_riaf_job req;        // RIAF jobs
+    kp_grmhd_job greq;      // GRMHD jobs
+    kp_grid* grid = nullptr;  // held (grid_ref) until the job ends
+    int nfreq = 1;
+    kp_image_out out;
     int state = KP_JOB_PENDING;
     int status = KP_OK;
     bool cancel = false;
@@ -94,9 +106,10 @@ struct kp_server {
     // device state (worker thread only)
     cudaStream_t stream = nullptr;
     RayRecord* pool = nullptr;
-    unsigned* ids[kPhases][2] = {};
-    unsigned* counts = nullptr;            // [2][kPhases]
-    unsigned long long* heads = nullptr;   // [kPhases]
+    unsigned* ids[kServeScenes][kPhases][2] = {};
+    unsigned* counts[kServeScenes] = {};           // per scene [2][kPhases]
+    unsigned long long* heads[kServeScenes] = {};  // per scene [kPhases]
+    long long scene_cycle[kServeScenes] = {};      // generation parity of each scene's queues
     int* status = nullptr;
     unsigned* done = nullptr;              // [max_jobs]
     JobDesc* d_jobs = nullptr;
@@ -114,21 +127,32 @@ struct kp_server {
 
 namespace {
 
-int footprint_units(const kp_riaf_job& j, long long* rays, long long* out_units) {
-    const long long npix = (long long)j.params.camera.nx * j.params.camera.ny;
+int footprint_units(const kp_pass_a_params& params, int nfreq, long long* rays, long long* out_units) {
+    const long long npix = (long long)params.camera.nx * params.camera.ny;
     *rays = npix;
-    *out_units = (long long)((carved_bytes(int(npix), j.nfreq) + kOutUnit - 1) / kOutUnit);
+    *out_units = (long long)((carved_bytes(int(npix), nfreq) + kOutUnit - 1) / kOutUnit);
     return KP_OK;
+}
+
+// A job leaves the server (done, cancelled, failed or abandoned): drop its
+// hold on the grid.  Callers hold s->mu or own the job alone.
+void end_job(ServerJob& j) {
+    if (j.grid) {
+        grid_unref(j.grid, 1);
+        j.grid = nullptr;
+    }
 }
 
 void release_device(kp_server* s) {
     cudaFree(s->pool);
-    for (auto& q : s->ids) {
-        cudaFree(q[0]);
-        cudaFree(q[1]);
+    for (int sc = 0; sc < kServeScenes; ++sc) {
+        for (auto& q : s->ids[sc]) {
+            cudaFree(q[0]);
+            cudaFree(q[1]);
+        }
+        cudaFree(s->counts[sc]);
+        cudaFree(s->heads[sc]);
     }
-    cudaFree(s->counts);
-    cudaFree(s->heads);
     cudaFree(s->status);
     cudaFree(s->done);
     cudaFree(s->d_jobs);
@@ -153,26 +177,30 @@ int allocate_device(kp_server* s) {
         if (e == cudaSuccess) e = cudaMalloc(p, n);
     };
     dev((void**)&s->pool, sizeof(RayRecord) * size_t(c.max_rays));
-    for (auto& q : s->ids)
-        for (auto& b : q) dev((void**)&b, sizeof(unsigned) * size_t(c.max_rays));
-    dev((void**)&s->counts, sizeof(unsigned) * 2 * kPhases);
-    dev((void**)&s->heads, sizeof(unsigned long long) * kPhases);
+    for (int sc = 0; sc < kServeScenes; ++sc) {
+        for (auto& q : s->ids[sc])
+            for (auto& b : q) dev((void**)&b, sizeof(unsigned) * size_t(c.max_rays));
+        dev((void**)&s->counts[sc], sizeof(unsigned) * 2 * kPhases);
+        dev((void**)&s->heads[sc], sizeof(unsigned long long) * kPhases);
+    }
     dev((void**)&s->status, sizeof(int));
     dev((void**)&s->done, sizeof(unsigned) * size_t(c.max_jobs));
     dev((void**)&s->d_jobs, sizeof(JobDesc) * size_t(c.max_jobs));
     dev((void**)&s->d_seed, sizeof(SeedEntry) * size_t(c.max_jobs));
-    dev((void**)&s->d_prefix, sizeof(long long) * size_t(c.max_jobs + 1));
+    dev((void**)&s->d_prefix, sizeof(long long) * size_t(c.max_jobs + kServeScenes));
     dev(&s->out_arena, c.output_bytes);
     if (e == cudaSuccess) e = cudaMallocHost((void**)&s->h_jobs, sizeof(JobDesc) * size_t(c.max_jobs));
     if (e == cudaSuccess) e = cudaMallocHost((void**)&s->h_seed, sizeof(SeedEntry) * size_t(c.max_jobs));
-    if (e == cudaSuccess) e = cudaMallocHost((void**)&s->h_prefix, sizeof(long long) * size_t(c.max_jobs + 1));
+    if (e == cudaSuccess) e = cudaMallocHost((void**)&s->h_prefix, sizeof(long long) * size_t(c.max_jobs + kServeScenes));
     if (e == cudaSuccess) e = cudaMallocHost((void**)&s->h_done, sizeof(unsigned) * size_t(c.max_jobs));
     if (e == cudaSuccess) e = cudaMallocHost((void**)&s->h_status, sizeof(int));
     if (e != cudaSuccess) {
         cudaGetLastError();
         return set_error(KP_ERR_OOM, "server allocation: %s", cudaGetErrorString(e));
     }
-    e = cudaMemset(s->counts, 0, sizeof(unsigned) * 2 * kPhases);
+    e = cudaSuccess;
+    for (int sc = 0; sc < kServeScenes && e == cudaSuccess; ++sc)
+        e = cudaMemset(s->counts[sc], 0, sizeof(unsigned) * 2 * kPhases);
     if (e == cudaSuccess) e = cudaMemset(s->status, 0, sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(s->done, 0, sizeof(unsigned) * size_t(c.max_jobs));
     if (e != cudaSuccess) return cuda_error(e, "server initialisation");
@@ -185,15 +213,25 @@ int allocate_device(kp_server* s) {
 JobDesc job_desc(const kp_server* s, const ServerJob& j) {
     JobDesc d;
     std::memset(&d, 0, sizeof(d));
-    d.c = make_consts(&j.req.params, &j.req.model, j.req.frequencies, j.req.nfreq, s->cfg.integrator);
-    double fr[5][4];
-    host_camera_frame(d.c, fr);
-    for (int mu = 0; mu < 4; ++mu) {
-        d.frame.x.v[mu] = fr[0][mu];
-        d.frame.e0.v[mu] = fr[1][mu];
-        d.frame.e1.v[mu] = fr[2][mu];
-        d.frame.e2.v[mu] = fr[3][mu];
-        d.frame.e3.v[mu] = fr[4][mu];
+    if (j.scene == kServeGrmhd) {
+        const kp_grmhd_job& g = j.greq;
+        d.c = image_consts_fmks(&g.params, j.grid->model,
+                                grid_consts_of(j.grid->model, j.grid->prims, j.grid->derived), g.frequencies, g.nfreq,
+                                s->cfg.integrator);
+        fmks_camera_frame(d.c.fmks, g.params.camera.radius, g.params.camera.inclination, d.frame.x, d.frame.e0,
+                          d.frame.e1, d.frame.e2, d.frame.e3);
+        if (s->cfg.precision == KP_PRECISION_MIXED) grmhd_emission_scale(&g.params, j.grid->model, d.c);
+    } else {
+        d.c = make_consts(&j.req.params, &j.req.model, j.req.frequencies, j.req.nfreq, s->cfg.integrator);
+        double fr[5][4];
+        host_camera_frame(d.c, fr);
+        for (int mu = 0; mu < 4; ++mu) {
+            d.frame.x.v[mu] = fr[0][mu];
+            d.frame.e0.v[mu] = fr[1][mu];
+            d.frame.e1.v[mu] = fr[2][mu];
+            d.frame.e2.v[mu] = fr[3][mu];
+            d.frame.e3.v[mu] = fr[4][mu];
+        }
     }
     d.out = j.dout;
     d.ray_begin = j.ray_base;
@@ -210,12 +248,14 @@ void fail_inflight(kp_server* s, int status) {
         j->state = KP_JOB_FAILED;
         j->status = status;
         ++s->failed;
+        end_job(*j);
         j = nullptr;
     }
     for (auto& j : s->pending) {
         j->state = KP_JOB_FAILED;
         j->status = status;
         ++s->failed;
+        end_job(*j);
     }
     s->pending.clear();
     s->stop = true;
@@ -228,12 +268,14 @@ void worker_main(kp_server* s) {
     const int nf_max = KP_MAX_FREQUENCIES;  // one compiled form for every job
     int sms = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, s->cfg.device);
-    int blocks[kPhases];
+    int blocks[kServeScenes][kPhases];
     for (int p = 0; p < kPhases; ++p) {
-        const int per_sm = mixed ? wave_occupancy_mixed(p, wave_threads(p)) : wave_occupancy_fp64(p, nf_max, wave_threads(p));
-        blocks[p] = std::max(1, sms) * std::max(1, per_sm);
+        const int th = wave_threads(p);
+        const int riaf = mixed ? wave_occupancy_mixed(p, th) : wave_occupancy_fp64(p, nf_max, th);
+        const int grmhd = mixed ? wave_occupancy_grmhd_mixed(p, nf_max, th) : wave_occupancy_grmhd(p, nf_max, th);
+        blocks[kServeRiaf][p] = std::max(1, sms) * std::max(1, riaf);
+        blocks[kServeGrmhd][p] = std::max(1, sms) * std::max(1, grmhd);
     }
-    long long cycle = 0;
     while (true) {
         // ---- admission (FIFO; the head of the queue waits for room)
         std::vector<std::shared_ptr<ServerJob>> admitted;
@@ -251,6 +293,7 @@ void worker_main(kp_server* s) {
                 for (auto& j : s->pending) {
                     j->state = KP_JOB_CANCELLED;
                     ++s->cancelled;
+                    end_job(*j);
                 }
                 s->pending.clear();
                 for (auto& j : s->slots) {
@@ -259,6 +302,7 @@ void worker_main(kp_server* s) {
                     ++s->cancelled;
                     s->rays.release(j->ray_base, j->npix);
                     s->outs.release(j->out_base, j->out_units);
+                    end_job(*j);
                     j = nullptr;
                 }
                 s->cv_done.notify_all();
@@ -269,7 +313,7 @@ void worker_main(kp_server* s) {
                 auto slot_it = std::find(s->slots.begin(), s->slots.end(), nullptr);
                 if (slot_it == s->slots.end()) break;
                 long long nr = 0, nu = 0;
-                footprint_units(j->req, &nr, &nu);
+                footprint_units(j->scene == kServeGrmhd ? j->greq.params : j->req.params, j->nfreq, &nr, &nu);
                 const long long rb = s->rays.alloc(nr);
                 if (rb < 0) break;
                 const long long ob = s->outs.alloc(nu);
@@ -282,7 +326,7 @@ void worker_main(kp_server* s) {
                 j->ray_base = rb;
                 j->out_base = ob;
                 j->out_units = nu;
-                j->dout = carve_outputs(static_cast<char*>(s->out_arena) + ob * kOutUnit, int(nr), j->req.nfreq);
+                j->dout = carve_outputs(static_cast<char*>(s->out_arena) + ob * kOutUnit, int(nr), j->nfreq);
                 j->state = KP_JOB_RUNNING;
                 j->t_admit = Clock::now();
                 *slot_it = j;
@@ -302,59 +346,92 @@ void worker_main(kp_server* s) {
         }
         const auto t_tick = Clock::now();
         cudaError_t e = cudaSuccess;
-        // ---- upload the new jobs and seed their rays
-        long long seeded = 0;
-        int nseed = 0;
-        for (const auto& j : admitted) {
-            s->h_jobs[j->slot] = job_desc(s, *j);
-            if (e == cudaSuccess)
-                e = cudaMemcpyAsync(s->d_jobs + j->slot, s->h_jobs + j->slot, sizeof(JobDesc), cudaMemcpyHostToDevice,
-                                    s->stream);
-            if (e == cudaSuccess) e = cudaMemsetAsync(s->done + j->slot, 0, sizeof(unsigned), s->stream);
-            s->h_seed[nseed] = SeedEntry{j->slot, int(j->npix), j->ray_base};
-            s->h_prefix[nseed] = seeded;
-            seeded += j->npix;
-            ++nseed;
+        // ---- upload the new jobs; seed their rays per scene (disjoint
+        // ranges of the pinned staging, so no copy in flight is overwritten)
+        int scene_jobs[kServeScenes] = {0, 0};
+        {
+            std::lock_guard<std::mutex> lock(s->mu);
+            for (const auto& j : s->slots)
+                if (j) ++scene_jobs[j->scene];
         }
-        s->h_prefix[nseed] = seeded;
-        const int cur = int(cycle % 2), nxt = int((cycle + 1) % 2);
-        unsigned* cnt = s->counts;
-        if (e == cudaSuccess) e = cudaMemsetAsync(cnt + nxt * kPhases, 0, sizeof(unsigned) * kPhases, s->stream);
-        if (e == cudaSuccess) e = cudaMemsetAsync(s->heads, 0, sizeof(unsigned long long) * kPhases, s->stream);
+        int seed_first[kServeScenes] = {0, 0}, seed_count[kServeScenes] = {0, 0};
+        long long seeded[kServeScenes] = {0, 0};
+        int nseed = 0;
+        for (int sc = 0; sc < kServeScenes; ++sc) {
+            seed_first[sc] = nseed;
+            for (const auto& j : admitted) {
+                if (j->scene != sc) continue;
+                s->h_jobs[j->slot] = job_desc(s, *j);
+                if (e == cudaSuccess)
+                    e = cudaMemcpyAsync(s->d_jobs + j->slot, s->h_jobs + j->slot, sizeof(JobDesc),
+                                        cudaMemcpyHostToDevice, s->stream);
+                if (e == cudaSuccess) e = cudaMemsetAsync(s->done + j->slot, 0, sizeof(unsigned), s->stream);
+                s->h_seed[nseed] = SeedEntry{j->slot, int(j->npix), j->ray_base};
+                s->h_prefix[nseed + sc] = seeded[sc];
+                seeded[sc] += j->npix;
+                ++nseed;
+                ++seed_count[sc];
+            }
+            s->h_prefix[nseed + sc] = seeded[sc];
+        }
         if (nseed > 0) {
             if (e == cudaSuccess)
                 e = cudaMemcpyAsync(s->d_seed, s->h_seed, sizeof(SeedEntry) * size_t(nseed), cudaMemcpyHostToDevice,
                                     s->stream);
             if (e == cudaSuccess)
-                e = cudaMemcpyAsync(s->d_prefix, s->h_prefix, sizeof(long long) * size_t(nseed + 1),
+                e = cudaMemcpyAsync(s->d_prefix, s->h_prefix, sizeof(long long) * size_t(nseed + kServeScenes),
                                     cudaMemcpyHostToDevice, s->stream);
-            if (e == cudaSuccess)
-                e = mixed ? launch_seed_mixed(s->d_jobs, s->d_seed, s->d_prefix, nseed, seeded, s->pool,
-                                              s->ids[kPhaseFar][cur], cnt + cur * kPhases + kPhaseFar, s->stream)
-                          : launch_seed_fp64(s->d_jobs, s->d_seed, s->d_prefix, nseed, seeded, s->pool,
-                                             s->ids[kPhaseFar][cur], cnt + cur * kPhases + kPhaseFar, s->stream);
         }
-        // ---- one cycle of the three phases
-        for (int p = 0; p < kPhases && e == cudaSuccess; ++p) {
-            WaveDesc W;
-            W.jobs = s->d_jobs;
-            W.njobs = s->cfg.max_jobs;
-            W.pool = s->pool;
-            W.fresh_begin = 0;
-            W.fresh_end = 0;
-            W.in_ids = s->ids[p][cur];
-            W.in_count = cnt + cur * kPhases + p;
-            W.in_head = s->heads + p;
-            for (int q = 0; q < kPhases; ++q) {
-                const int g = q > p ? cur : nxt;
-                W.out_ids[q] = s->ids[q][g];
-                W.out_count[q] = cnt + g * kPhases + q;
+        // ---- one cycle of the three phases for each scene with jobs in flight;
+        // each scene's queues alternate with its own tick count
+        for (int sc = 0; sc < kServeScenes && e == cudaSuccess; ++sc) {
+            if (scene_jobs[sc] == 0) continue;
+            const long long cycle = s->scene_cycle[sc];
+            const int cur = int(cycle % 2), nxt = int((cycle + 1) % 2);
+            unsigned* cnt = s->counts[sc];
+            if (e == cudaSuccess) e = cudaMemsetAsync(cnt + nxt * kPhases, 0, sizeof(unsigned) * kPhases, s->stream);
+            if (e == cudaSuccess) e = cudaMemsetAsync(s->heads[sc], 0, sizeof(unsigned long long) * kPhases, s->stream);
+            if (seed_count[sc] > 0 && e == cudaSuccess) {
+                const SeedEntry* ents = s->d_seed + seed_first[sc];
+                const long long* pre = s->d_prefix + seed_first[sc] + sc;
+                if (sc == kServeGrmhd)
+                    e = (mixed ? launch_seed_grmhd_mixed : launch_seed_grmhd)(
+                        s->d_jobs, ents, pre, seed_count[sc], seeded[sc], s->pool, s->ids[sc][kPhaseFar][cur],
+                        cnt + cur * kPhases + kPhaseFar, s->stream);
+                else if (mixed)
+                    e = launch_seed_mixed(s->d_jobs, ents, pre, seed_count[sc], seeded[sc], s->pool,
+                                          s->ids[sc][kPhaseFar][cur], cnt + cur * kPhases + kPhaseFar, s->stream);
+                else
+                    e = launch_seed_fp64(s->d_jobs, ents, pre, seed_count[sc], seeded[sc], s->pool,
+                                         s->ids[sc][kPhaseFar][cur], cnt + cur * kPhases + kPhaseFar, s->stream);
             }
-            W.budget = s->cfg.tick_budget;
-            W.status = s->status;
-            W.job_done = s->done;
-            e = mixed ? launch_wave_mixed(p, W, blocks[p], wave_threads(p), s->stream)
-                      : launch_wave_fp64(p, W, nf_max, blocks[p], wave_threads(p), s->stream);
+            for (int p = 0; p < kPhases && e == cudaSuccess; ++p) {
+                WaveDesc W;
+                W.jobs = s->d_jobs;
+                W.njobs = s->cfg.max_jobs;
+                W.pool = s->pool;
+                W.fresh_begin = 0;
+                W.fresh_end = 0;
+                W.in_ids = s->ids[sc][p][cur];
+                W.in_count = cnt + cur * kPhases + p;
+                W.in_head = s->heads[sc] + p;
+                for (int q = 0; q < kPhases; ++q) {
+                    const int g = q > p ? cur : nxt;
+                    W.out_ids[q] = s->ids[sc][q][g];
+                    W.out_count[q] = cnt + g * kPhases + q;
+                }
+                W.budget = s->cfg.tick_budget;
+                W.status = s->status;
+                W.job_done = s->done;
+                const int b = blocks[sc][p], th = wave_threads(p);
+                if (sc == kServeGrmhd)
+                    e = mixed ? launch_wave_grmhd_mixed(p, W, nf_max, b, th, s->stream)
+                              : launch_wave_grmhd(p, W, nf_max, b, th, s->stream);
+                else
+                    e = mixed ? launch_wave_mixed(p, W, b, th, s->stream)
+                              : launch_wave_fp64(p, W, nf_max, b, th, s->stream);
+            }
+            s->scene_cycle[sc] = cycle + 1;
         }
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(s->h_done, s->done, sizeof(unsigned) * size_t(s->cfg.max_jobs),
@@ -362,7 +439,6 @@ void worker_main(kp_server* s) {
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(s->h_status, s->status, sizeof(int), cudaMemcpyDeviceToHost, s->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
-        ++cycle;
         if (e != cudaSuccess) {
             fail_inflight(s, cuda_error(e, "serving tick"));
             break;
@@ -381,7 +457,7 @@ void worker_main(kp_server* s) {
         }
         for (const auto& j : finished) {
             if (!j->cancel) {
-                int st = copy_outputs_to_host(j->dout, &j->req.out, int(j->npix), j->req.nfreq, s->stream);
+                int st = copy_outputs_to_host(j->dout, &j->out, int(j->npix), j->nfreq, s->stream);
                 if (st == KP_OK) {
                     e = cudaStreamSynchronize(s->stream);
                     if (e != cudaSuccess) st = cuda_error(e, "result copy");
@@ -396,6 +472,7 @@ void worker_main(kp_server* s) {
                 s->slots[size_t(j->slot)] = nullptr;
                 s->rays.release(j->ray_base, j->npix);
                 s->outs.release(j->out_base, j->out_units);
+                end_job(*j);
                 j->t_done = now;
                 if (j->cancel) {
                     j->state = KP_JOB_CANCELLED;
@@ -463,21 +540,11 @@ int kp_server_create(const kp_server_config* cfg, kp_server** out) {
     return KP_OK;
 }
 
-int kp_server_submit(kp_server* s, const kp_riaf_job* job, unsigned long long* ticket) {
-    if (!s || !job || !ticket) return set_error(KP_ERR_INVALID, "kp_server_submit: null argument");
-    int st = validate_riaf(&job->params, &job->model, job->frequencies, job->nfreq);
-    if (st != KP_OK) return st;
-    if (job->radiation_substeps < 1) return set_error(KP_ERR_INVALID, "radiation_substeps must be positive");
-    const int npix = job->params.camera.nx * job->params.camera.ny;
-    st = check_outputs(&job->out, npix, job->nfreq);
-    if (st != KP_OK) return st;
-    long long nr = 0, nu = 0;
-    footprint_units(*job, &nr, &nu);
-    if (nr > s->cfg.max_rays || nu * kOutUnit > (long long)s->cfg.output_bytes)
-        return set_error(KP_ERR_INVALID, "job footprint (%lld rays, %lld output bytes) exceeds the server's capacity",
-                         nr, nu * kOutUnit);
-    auto j = std::make_shared<ServerJob>();
-    j->req = *job;
+}  // extern "C"
+
+namespace {
+
+int enqueue(kp_server* s, const std::shared_ptr<ServerJob>& j, unsigned long long* ticket) {
     j->t_submit = Clock::now();
     {
         std::lock_guard<std::mutex> lock(s->mu);
@@ -490,6 +557,56 @@ int kp_server_submit(kp_server* s, const kp_riaf_job* job, unsigned long long* t
     s->cv_work.notify_one();
     *ticket = j->ticket;
     return KP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int kp_server_submit(kp_server* s, const kp_riaf_job* job, unsigned long long* ticket) {
+    if (!s || !job || !ticket) return set_error(KP_ERR_INVALID, "kp_server_submit: null argument");
+    int st = validate_riaf(&job->params, &job->model, job->frequencies, job->nfreq);
+    if (st != KP_OK) return st;
+    if (job->radiation_substeps < 1) return set_error(KP_ERR_INVALID, "radiation_substeps must be positive");
+    const int npix = job->params.camera.nx * job->params.camera.ny;
+    st = check_outputs(&job->out, npix, job->nfreq);
+    if (st != KP_OK) return st;
+    long long nr = 0, nu = 0;
+    footprint_units(job->params, job->nfreq, &nr, &nu);
+    if (nr > s->cfg.max_rays || nu * kOutUnit > (long long)s->cfg.output_bytes)
+        return set_error(KP_ERR_INVALID, "job footprint (%lld rays, %lld output bytes) exceeds the server's capacity",
+                         nr, nu * kOutUnit);
+    auto j = std::make_shared<ServerJob>();
+    j->scene = kServeRiaf;
+    j->req = *job;
+    j->nfreq = job->nfreq;
+    j->out = job->out;
+    return enqueue(s, j, ticket);
+}
+
+int kp_server_submit_grmhd(kp_server* s, const kp_grmhd_job* job, unsigned long long* ticket) {
+    if (!s || !job || !ticket || !job->grid) return set_error(KP_ERR_INVALID, "kp_server_submit_grmhd: null argument");
+    int st = validate_grmhd(&job->params, job->grid, job->frequencies, job->nfreq, job->radiation_substeps,
+                            s->cfg.device);
+    if (st != KP_OK) return st;
+    const int npix = job->params.camera.nx * job->params.camera.ny;
+    st = check_outputs(&job->out, npix, job->nfreq);
+    if (st != KP_OK) return st;
+    long long nr = 0, nu = 0;
+    footprint_units(job->params, job->nfreq, &nr, &nu);
+    if (nr > s->cfg.max_rays || nu * kOutUnit > (long long)s->cfg.output_bytes)
+        return set_error(KP_ERR_INVALID, "job footprint (%lld rays, %lld output bytes) exceeds the server's capacity",
+                         nr, nu * kOutUnit);
+    auto j = std::make_shared<ServerJob>();
+    j->scene = kServeGrmhd;
+    j->greq = *job;
+    j->nfreq = job->nfreq;
+    j->out = job->out;
+    j->grid = const_cast<kp_grid*>(job->grid);
+    grid_ref(j->grid);
+    st = enqueue(s, j, ticket);
+    if (st != KP_OK) end_job(*j);
+    return st;
 }
 
 int kp_server_poll(kp_server* s, unsigned long long ticket, int* state) {
@@ -525,6 +642,7 @@ int kp_server_cancel(kp_server* s, unsigned long long ticket) {
         s->pending.erase(std::find(s->pending.begin(), s->pending.end(), j));
         j->state = KP_JOB_CANCELLED;
         ++s->cancelled;
+        end_job(*j);
         s->cv_done.notify_all();
     } else if (j->state == KP_JOB_RUNNING) {
         j->cancel = true;

@@ -47,6 +47,7 @@ def test_struct_layouts_match_ctypes_mirror():
     assert lib.kp_abi_sizeof(8) == C.sizeof(_abi.BatchStats)
     assert lib.kp_abi_sizeof(9) == C.sizeof(_abi.Tuning)
     assert lib.kp_abi_sizeof(10) == C.sizeof(_abi.GrmhdModel)
+    assert lib.kp_abi_sizeof(11) == C.sizeof(_abi.GrmhdJob)
     assert lib.kp_abi_sizeof(6) > 0
     assert lib.kp_abi_sizeof(99) == 0
 
