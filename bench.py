@@ -62,6 +62,12 @@ def parse():
     ap.add_argument("--grmhd", type=int, default=1,
                     help="also time the GRMHD image (288x128x128 FM torus, 512^2, FP64 and mixed)")
     ap.add_argument("--grmhd-steps", type=int, default=2, help="timed GRMHD images per precision")
+    ap.add_argument("--grmhd-only", action="store_true",
+                    help="profiling entry: only trace GRMHD images (--grmhd-grid, --grmhd-n, --grmhd-precision, "
+                         "--grmhd-steps images) and print their times; no JSON line")
+    ap.add_argument("--grmhd-grid", type=int, nargs=3, default=[288, 128, 128])
+    ap.add_argument("--grmhd-n", type=int, default=512)
+    ap.add_argument("--grmhd-precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--config4", type=int, default=1,
                     help="also time the uneven 64-image batch (autotuned, graph-captured) and the slow-light job")
     return ap.parse_args()
@@ -401,15 +407,19 @@ def integrated_stokes(i, q, u):
 
 
 # ---------------------------------------------------------------- serving
-def serving_trace(n_requests, rate, seed=2026):
-    """Seeded Poisson arrivals of RIAF image requests: resolution 64^2, 128^2
-    or 256^2, 1-4 frequencies from {86, 230, 345, 690} GHz, spin U[0, 0.99],
-    inclination U[10, 170] deg, the adaptive 4-frequency controls."""
+def serving_trace(n_requests, rate, seed=2026, grmhd_fraction=0.25, ngrids=4):
+    """Seeded Poisson arrivals of image requests: resolution 64^2, 128^2 or
+    256^2, 1-4 frequencies from {86, 230, 345, 690} GHz, inclination
+    U[10, 170] deg, the adaptive 4-frequency controls; a fraction of them
+    GRMHD images of one of `ngrids` resident torus grids, the rest RIAF
+    images with spin U[0, 0.99].  Entries: (t, kind, params, model or grid
+    index, frequencies)."""
     import numpy as np
 
-    from kpolaris_b200 import configs
+    from kpolaris_b200 import configs, synthetic
 
     rng = np.random.default_rng(seed)
+    _, gmodel = synthetic.fm_torus(8, 8, 8)
     t = 0.0
     trace = []
     for _ in range(n_requests):
@@ -417,56 +427,90 @@ def serving_trace(n_requests, rate, seed=2026):
         n = int(rng.choice([64, 128, 256]))
         nf = int(rng.integers(1, 5))
         freqs = sorted(rng.choice(configs.CONFIG2_FREQS, size=nf, replace=False).tolist())
-        p = configs.riaf_params(n, n, spin=float(rng.uniform(0.0, 0.99)),
-                                inclination_deg=float(rng.uniform(10.0, 170.0)), step=0.025, adaptive=1,
-                                max_steps=400000, adaptive_tolerance=1e-8, min_step=1e-10, max_step=2.0,
-                                max_radiation_step=2.0, max_radiation_depth=1.0, max_absorption_depth=1.0,
-                                max_faraday_depth=4.0)
-        trace.append((t, p, configs.riaf_model(), freqs))
+        inc = float(rng.uniform(10.0, 170.0))
+        if rng.uniform() < grmhd_fraction:
+            p = synthetic.fmks_pass_a_params(gmodel, n, n, inclination_deg=inc)
+            trace.append((t, "grmhd", p, int(rng.integers(0, ngrids)), freqs))
+            continue
+        p = configs.riaf_params(n, n, spin=float(rng.uniform(0.0, 0.99)), inclination_deg=inc, step=0.025,
+                                adaptive=1, max_steps=400000, adaptive_tolerance=1e-8, min_step=1e-10,
+                                max_step=2.0, max_radiation_step=2.0, max_radiation_depth=1.0,
+                                max_absorption_depth=1.0, max_faraday_depth=4.0)
+        trace.append((t, "riaf", p, configs.riaf_model(), freqs))
     return trace
 
 
-def serve_mixed(trace, device):
+def serving_grids(device, ngrids=4):
+    """The resident grids of the serving trace: 288x128x128 tori, seeds
+    2026 + k, R_high = 40."""
+    import kpolaris_b200 as kp
+    from kpolaris_b200 import synthetic
+
+    grids = []
+    for k in range(ngrids):
+        prims, model = synthetic.fm_torus(288, 128, 128, seed=2026 + k)
+        model.trat_large = 40.0
+        grids.append(kp.Grid(model, prims, device=device))
+    return grids
+
+
+def serve_mixed(trace, grids, device):
     """Replays the trace against the serving loop in real time."""
     import kpolaris_b200 as kp
 
+    def submit(srv, kind, p, m, f):
+        return srv.submit_grmhd(p, grids[m], f) if kind == "grmhd" else srv.submit(p, m, f)
+
     with kp.Server(device=device, max_rays=1 << 21) as srv:
-        # warm the kernels and the server's buffers
-        w = srv.submit(*trace[0][1:])
-        srv.wait(w, timeout=120.0)
-        srv.result(w)
-        lat = []
+        # warm the kernels and the server's buffers with one request of each kind
+        for kind in ("riaf", "grmhd"):
+            first = next((e for e in trace if e[1] == kind), None)
+            if first:
+                w = submit(srv, *first[1:])
+                srv.wait(w, timeout=120.0)
+                srv.result(w)
+        base = srv.stats()
         t0 = time.perf_counter()
         tickets = []
-        for (t, p, m, f) in trace:
+        for (t, kind, p, m, f) in trace:
             delay = t - (time.perf_counter() - t0)
             if delay > 0:
                 time.sleep(delay)
-            tickets.append((srv.submit(p, m, f), t0 + t))
-        for tk, t_arr in tickets:
+            tickets.append(submit(srv, kind, p, m, f))
+        for tk in tickets:
             srv.wait(tk, timeout=300.0)
         t_end = time.perf_counter()
         st = srv.stats()
     # per-request latency from the server's own clock (submit -> done)
     return {"images_per_s": len(trace) / (t_end - t0), "p50_s": st.latency_p50, "p99_s": st.latency_p99,
             "max_s": st.latency_max, "queue_p50_s": st.queue_p50,
-            "max_inflight_jobs": st.max_inflight_jobs, "ticks": st.ticks - 1}
+            "max_inflight_jobs": st.max_inflight_jobs, "ticks": st.ticks - base.ticks}
 
 
-def serve_plain(trace, device):
-    """The same trace through a FIFO of plain FP64 one-image launches: each
-    request starts when it has arrived and the previous one has finished."""
+def serve_plain(trace, grids, device):
+    """The same trace through a FIFO of plain FP64 launches: each request
+    starts when it has arrived and the previous one has finished (RIAF: the
+    one-image-per-launch kernel; GRMHD: one FP64 image per call)."""
     import numpy as np
 
     import kpolaris_b200 as kp
 
-    kp.image_riaf(*trace[0][1:], device=device)
+    def run(kind, p, m, f):
+        if kind == "grmhd":
+            kp.image_grmhd(p, grids[m], f, device=device)
+        else:
+            kp.image_riaf(p, m, f, device=device)
+
+    for kind in ("riaf", "grmhd"):
+        first = next((e for e in trace if e[1] == kind), None)
+        if first:
+            run(*first[1:])
     finish = 0.0
     lat = []
     busy = 0.0
-    for (t, p, m, f) in trace:
+    for (t, kind, p, m, f) in trace:
         t_a = time.perf_counter()
-        kp.image_riaf(p, m, f, device=device)
+        run(kind, p, m, f)
         svc = time.perf_counter() - t_a
         busy += svc
         finish = max(finish, t) + svc
@@ -680,13 +724,20 @@ def ours_arm(args):
     if mixed and args.serve_requests > 0:
         progress("serving trace")
         trace = serving_trace(args.serve_requests, args.serve_rate)
-        serving = {"workload": "Poisson arrivals of RIAF requests: 64^2/128^2/256^2, 1-4 frequencies, "
-                               "spin U[0,0.99], inclination U[10,170] deg, adaptive RK4",
-                   "requests": len(trace), "rate_per_s": args.serve_rate,
-                   "mixed_batched": serve_mixed(trace, local)}
-        if args.serve_plain:
-            progress("serving trace on the plain FP64 kernel")
-            serving["plain_fp64"] = serve_plain(trace, local)
+        grids = serving_grids(local)
+        try:
+            serving = {"workload": "Poisson arrivals: 3/4 RIAF images (spin U[0,0.99]), 1/4 GRMHD images of one of "
+                                   "4 resident 288x128x128 tori; 64^2/128^2/256^2, 1-4 frequencies, inclination "
+                                   "U[10,170] deg, adaptive RK4",
+                       "requests": len(trace), "grmhd_requests": sum(1 for e in trace if e[1] == "grmhd"),
+                       "rate_per_s": args.serve_rate,
+                       "mixed_batched": serve_mixed(trace, grids, local)}
+            if args.serve_plain:
+                progress("serving trace on the plain FP64 path")
+                serving["plain_fp64"] = serve_plain(trace, grids, local)
+        finally:
+            for g in grids:
+                g.release()
 
     grmhd = None
     if args.grmhd:
@@ -742,8 +793,30 @@ def ours_arm(args):
     return 0
 
 
+def grmhd_only(args):
+    """Profiling entry: GRMHD images of the seeded torus, nothing else."""
+    import kpolaris_b200 as kp
+    from kpolaris_b200 import _abi, synthetic
+
+    n1, n2, n3 = args.grmhd_grid
+    prims, model = synthetic.fm_torus(n1, n2, n3)
+    model.trat_large = 40.0
+    prec = _abi.PRECISION_MIXED if args.grmhd_precision == "mixed" else _abi.PRECISION_FP64
+    params = synthetic.fmks_pass_a_params(model, args.grmhd_n, args.grmhd_n)
+    with kp.Grid(model, prims) as g:
+        for _ in range(max(1, args.grmhd_steps)):
+            t0 = time.perf_counter()
+            r = kp.image_grmhd(params, g, [230e9], precision=prec)
+            print(f"grmhd {n1}x{n2}x{n3} {args.grmhd_n}^2 {args.grmhd_precision}: "
+                  f"{time.perf_counter() - t0:.3f} s, steps A {int(r.pass_a_steps.sum())} B {int(r.steps.sum())}",
+                  flush=True)
+    return 0
+
+
 def main():
     args = parse()
+    if args.grmhd_only:
+        return grmhd_only(args)
     if args.impl == "reference":
         return reference_arm(args)
     return ours_arm(args)
