@@ -481,6 +481,42 @@ int kp_server_get_stats(kp_server* s, kp_server_stats* out);
 int kp_server_destroy(kp_server* s);
 
 /*
+ * Output packing of one frequency (host arrays), in the convention of the
+ * reference's image tool: pack_transport_frequency_image
+ * (tools/kpolaris_model_image.cpp:2561-2800) with output_qu_sign
+ * (tools/kpolaris_evpa.hpp:15-17).  Pixels whose ray did not reach the
+ * camera are zero; Q and U change sign for the N EVPA convention
+ * (evpa_north = 1), not for W; S_nu = S_inv * frequency^3; total_steps =
+ * pass_a_steps + steps.  Any output array may be NULL.  The sums run over
+ * returned pixels in pixel order; flux_jy = sum * frequency^3 *
+ * intensity_to_flux_jy_per_pixel (flux_density_jy, :589-595), NaN when that
+ * scale is not positive.
+ */
+typedef struct kp_packed_image {
+    double* i_inv;
+    double* q_inv;
+    double* u_inv;
+    double* v_inv;
+    double* i_nu;
+    double* q_nu;
+    double* u_nu;
+    double* v_nu;
+    int32_t* total_steps;
+    int returned;        /* out: pixels whose ray reached the camera */
+    double sum_inv[4];   /* out: sums of I, Q, U, V (invariant, output convention) */
+    double flux_jy[4];   /* out: the sums as flux densities in Jy */
+} kp_packed_image;
+
+int kp_pack_image(const kp_image_out* data, int freq_index, double frequency, int evpa_north,
+                  double intensity_to_flux_jy_per_pixel, kp_packed_image* out);
+
+/* Pixel solid angle / 1 Jy (compute_flux_scale, tools/kpolaris_model_image.cpp:
+ * 551-587): image widths in M, source distance in pc; NaN unless every input
+ * is positive. */
+double kp_flux_scale_jy_per_pixel(double mbh_solar, double dsource_pc, double image_width_x, double image_width_y,
+                                  int nx, int ny);
+
+/*
  * Schedule autotuner for the persistent engine (no counterpart in the
  * reference, whose launch shape is Kokkos's).  Times candidate schedules --
  * CTAs per SM of each phase kernel and the number of cycles captured per

@@ -75,6 +75,10 @@ def library() -> C.CDLL:
     L.kp_image_grmhd_slow_light.argtypes = [
         C.POINTER(PassAParams), C.POINTER(C.c_void_p), C.POINTER(C.c_double), C.c_int, C.c_double, C.c_int,
         C.POINTER(C.c_double), C.c_int, C.POINTER(_abi.RunOptions), C.POINTER(_abi.ImageOut)]
+    L.kp_pack_image.argtypes = [C.POINTER(_abi.ImageOut), C.c_int, C.c_double, C.c_int, C.c_double,
+                                C.POINTER(_abi.PackedImage)]
+    L.kp_flux_scale_jy_per_pixel.restype = C.c_double
+    L.kp_flux_scale_jy_per_pixel.argtypes = [C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int]
     L.kp_autotune_batch.argtypes = [C.POINTER(_abi.RiafJob), C.c_int, C.POINTER(RunOptions),
                                     C.POINTER(_abi.Tuning)]
     L.kp_server_create.argtypes = [C.POINTER(_abi.ServerConfig), C.POINTER(C.c_void_p)]
@@ -178,6 +182,38 @@ def _job_array(jobs, outs=None):
         j.radiation_substeps = 1
         j.out = res.as_struct()
     return arr, len(jobs), results
+
+
+def flux_scale_jy_per_pixel(mbh_solar: float, dsource_pc: float, image_width_x: float, image_width_y: float,
+                            nx: int, ny: int) -> float:
+    """kp_flux_scale_jy_per_pixel: pixel solid angle / 1 Jy (NaN if undefined)."""
+    return library().kp_flux_scale_jy_per_pixel(float(mbh_solar), float(dsource_pc), float(image_width_x),
+                                                float(image_width_y), int(nx), int(ny))
+
+
+def pack_image(result: ImageHostData, freq_index: int, frequency: float, *, evpa_0: str = "N",
+               flux_scale: float = float("nan")) -> dict:
+    """kp_pack_image: one frequency of `result` in the image tool's output
+    convention (pack_transport_frequency_image).  Returns the I/Q/U/V
+    invariant and S_nu arrays, total_steps, the returned-pixel count, the
+    invariant sums and the fluxes in Jy (NaN without `flux_scale`)."""
+    if evpa_0 not in ("N", "n", "W", "w"):
+        raise ValueError("evpa_0 must be N or W")
+    npix = result.npix
+    arr = {k: np.zeros(npix) for k in ("i_inv", "q_inv", "u_inv", "v_inv", "i_nu", "q_nu", "u_nu", "v_nu")}
+    steps = np.zeros(npix, dtype=np.int32)
+    pk = _abi.PackedImage()
+    for k, a in arr.items():
+        setattr(pk, k, a.ctypes.data_as(C.POINTER(C.c_double)))
+    pk.total_steps = steps.ctypes.data_as(C.POINTER(C.c_int32))
+    s = result.as_struct()
+    check(library().kp_pack_image(C.byref(s), int(freq_index), float(frequency), int(evpa_0 in ("N", "n")),
+                                  float(flux_scale), C.byref(pk)))
+    arr["total_steps"] = steps
+    arr["returned"] = pk.returned
+    arr["sum_inv"] = np.array(pk.sum_inv[:])
+    arr["flux_jy"] = np.array(pk.flux_jy[:])
+    return arr
 
 
 def autotune_batch(jobs, *, precision=_abi.PRECISION_MIXED, device=0) -> _abi.Tuning:

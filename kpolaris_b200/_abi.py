@@ -181,6 +181,14 @@ class RiafJob(C.Structure):
     ]
 
 
+class PackedImage(C.Structure):
+    """kp_packed_image: one frequency in the image tool's output convention."""
+    _fields_ = [(name, C.POINTER(C.c_double)) for name in
+                ("i_inv", "q_inv", "u_inv", "v_inv", "i_nu", "q_nu", "u_nu", "v_nu")] + [
+        ("total_steps", C.POINTER(C.c_int32)), ("returned", C.c_int), ("sum_inv", C.c_double * 4),
+        ("flux_jy", C.c_double * 4)]
+
+
 class GrmhdJob(C.Structure):
     """kp_grmhd_job: a GRMHD image of a resident grid for the serving loop."""
     _fields_ = [

@@ -9,6 +9,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <limits>
 #include <mutex>
 #include <vector>
 
@@ -978,6 +979,65 @@ int kp_batch_riaf(const kp_riaf_job* jobs, int njobs, const kp_run_options* opti
         if (opt.timing) std::printf("timing image_device_to_host_batch %g s\n", s);
     }
     return KP_OK;
+}
+
+int kp_pack_image(const kp_image_out* data, int freq_index, double frequency, int evpa_north,
+                  double intensity_to_flux_jy_per_pixel, kp_packed_image* out) {
+    if (!data || !out) return set_error(KP_ERR_INVALID, "kp_pack_image: null argument");
+    if (freq_index < 0 || freq_index >= data->nfreq)
+        return set_error(KP_ERR_INVALID, "frequency index %d outside [0, %d)", freq_index, data->nfreq);
+    if (!data->image_i || !data->image_q || !data->image_u || !data->image_v || !data->reason)
+        return set_error(KP_ERR_INVALID, "kp_pack_image: image arrays and reason are required");
+    const int npix = data->npix;
+    const size_t off = size_t(freq_index) * size_t(npix);
+    const double sign = evpa_north ? -1.0 : 1.0;
+    const double nu3 = frequency * frequency * frequency;
+    double sum[4] = {0.0, 0.0, 0.0, 0.0};
+    int returned = 0;
+    for (int p = 0; p < npix; ++p) {
+        const bool reached = data->reason[p] == KP_REASON_REACHED_CAMERA;
+        const double i = reached ? data->image_i[off + size_t(p)] : 0.0;
+        const double q = reached ? sign * data->image_q[off + size_t(p)] : 0.0;
+        const double u = reached ? sign * data->image_u[off + size_t(p)] : 0.0;
+        const double v = reached ? data->image_v[off + size_t(p)] : 0.0;
+        if (out->i_inv) out->i_inv[p] = i;
+        if (out->q_inv) out->q_inv[p] = q;
+        if (out->u_inv) out->u_inv[p] = u;
+        if (out->v_inv) out->v_inv[p] = v;
+        if (out->i_nu) out->i_nu[p] = i * nu3;
+        if (out->q_nu) out->q_nu[p] = q * nu3;
+        if (out->u_nu) out->u_nu[p] = u * nu3;
+        if (out->v_nu) out->v_nu[p] = v * nu3;
+        if (out->total_steps && data->pass_a_steps && data->steps)
+            out->total_steps[p] = data->pass_a_steps[p] + data->steps[p];
+        if (reached) {
+            ++returned;
+            sum[0] += i;
+            sum[1] += q;
+            sum[2] += u;
+            sum[3] += v;
+        }
+    }
+    out->returned = returned;
+    const bool valid = intensity_to_flux_jy_per_pixel > 0.0 && std::isfinite(intensity_to_flux_jy_per_pixel);
+    for (int k = 0; k < 4; ++k) {
+        out->sum_inv[k] = sum[k];
+        out->flux_jy[k] = valid ? sum[k] * frequency * frequency * frequency * intensity_to_flux_jy_per_pixel
+                                : std::numeric_limits<double>::quiet_NaN();
+    }
+    return KP_OK;
+}
+
+double kp_flux_scale_jy_per_pixel(double mbh_solar, double dsource_pc, double image_width_x, double image_width_y,
+                                  int nx, int ny) {
+    const double gnewt = 6.6742e-8, msun = 1.989e33, cl = 2.99792458e10, pc_cgs = 3.085678e18, jy_cgs = 1.0e-23;
+    const double l_unit = gnewt * mbh_solar * msun / (cl * cl);
+    const double dsource = dsource_pc * pc_cgs;
+    if (!(dsource_pc > 0.0 && image_width_x > 0.0 && image_width_y > 0.0 && nx > 0 && ny > 0 && mbh_solar > 0.0))
+        return std::numeric_limits<double>::quiet_NaN();
+    const double px = image_width_x * l_unit / double(nx);
+    const double py = image_width_y * l_unit / double(ny);
+    return px * py / (dsource * dsource) / jy_cgs;
 }
 
 int kp_autotune_batch(const kp_riaf_job* jobs, int njobs, const kp_run_options* options, kp_tuning* out) {
