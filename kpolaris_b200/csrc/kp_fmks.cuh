@@ -274,6 +274,82 @@ KP_HD Ray fmks_rhs(const FmksParams& m, const Ray& s) {
     return d;
 }
 
+// The same right-hand side in factored form, for the mixed policy: the
+// spherical Kerr-Schild derivatives have only seven distinct nonzero
+// entries per direction (d/dr g: rows 0 and 1 coincide, A(q0 + q1) + B q3;
+// d/dtheta g likewise with two different (0,3)/(1,3) entries), the inverse
+// metric five, and the three divisions by rho^2, r and dtheta/dx2 become
+// reciprocals.  Same algebra as fmks_rhs, regrouped: agrees to rounding.
+KP_HD Ray fmks_rhs_factored(const FmksParams& m, const Ray& s) {
+    const FmksTheta t = fmks_theta(m, s.x.v[1], s.x.v[2]);
+    const double a = m.spin, M = m.mass, r = t.r;
+    double sn, cs;
+    sincos(t.th, &sn, &cs);
+    const double a2 = a * a, s2 = sn * sn, safe_s2 = max_val(s2, kTiny);
+    const double rho2 = r * r + a2 * cs * cs;
+    const double inv_rho2 = 1.0 / rho2;
+    const double inv_rho4 = inv_rho2 * inv_rho2;
+    const double f = 2.0 * M * r * inv_rho2;
+    const double delta = r * r - 2.0 * M * r + a2;
+    // inverse metric: g00, g01 = g10, g11, g13 = g31, g22, g33
+    const double G00 = -(1.0 + f), G01 = f, G11 = delta * inv_rho2, G13 = a * inv_rho2, G22 = inv_rho2;
+    const double G33 = inv_rho2 / safe_s2;
+    // d/dr g and d/dtheta g
+    const double drho_dth = -2.0 * a2 * sn * cs, ds2_dth = 2.0 * sn * cs;
+    const double df_dr = 2.0 * M * (rho2 - 2.0 * r * r) * inv_rho4;
+    const double df_dth = -2.0 * M * r * drho_dth * inv_rho4;
+    const double A = df_dr, B = -a * s2 * df_dr, C = 2.0 * r;
+    const double Dr = s2 * (2.0 * r + a2 * s2 * df_dr);
+    const double E = df_dth, F0 = -a * (s2 * df_dth + ds2_dth * f), F1 = -a * (ds2_dth * (1.0 + f) + s2 * df_dth);
+    const double Gt = drho_dth;
+    const double bracket = rho2 + a2 * s2 * (1.0 + f);
+    const double Ht = ds2_dth * bracket + s2 * (drho_dth + a2 * (ds2_dth * (1.0 + f) + s2 * df_dth));
+    const double inv_r = 1.0 / r, inv_dth2 = 1.0 / t.dth2;
+    struct V {
+        double v0, v1, v2, v3;
+    };
+    auto to_sph = [&](const D4& q) { return V{q.v[0], r * q.v[1], t.dth1 * q.v[1] + t.dth2 * q.v[2], q.v[3]}; };
+    auto drow = [&](const V& q, V& rr, V& rt) {
+        const double sig = q.v0 + q.v1;
+        rr = V{A * sig + B * q.v3, A * sig + B * q.v3, C * q.v2, B * sig + Dr * q.v3};
+        rt = V{E * sig + F0 * q.v3, E * sig + F1 * q.v3, Gt * q.v2, F0 * q.v0 + F1 * q.v1 + Ht * q.v3};
+    };
+    const V ks = to_sph(s.k);
+    V rk, tk;
+    drow(ks, rk, tk);
+    auto contract = [&](const D4& qn) {
+        const V q = to_sph(qn);
+        V rr, rt;
+        drow(q, rr, rt);
+        const double d1 = ks.v0 * rr.v0 + ks.v1 * rr.v1 + ks.v2 * rr.v2 + ks.v3 * rr.v3;
+        const double d2 = ks.v0 * rt.v0 + ks.v1 * rt.v1 + ks.v2 * rt.v2 + ks.v3 * rt.v3;
+        const double t0 = ks.v1 * rr.v0 + q.v1 * rk.v0 + ks.v2 * rt.v0 + q.v2 * tk.v0;
+        const double t1 = ks.v1 * rr.v1 + q.v1 * rk.v1 + ks.v2 * rt.v1 + q.v2 * tk.v1 - d1;
+        const double t2 = ks.v1 * rr.v2 + q.v1 * rk.v2 + ks.v2 * rt.v2 + q.v2 * tk.v2 - d2;
+        const double t3 = ks.v1 * rr.v3 + q.v1 * rk.v3 + ks.v2 * rt.v3 + q.v2 * tk.v3;
+        const double h0 = 0.5 * (G00 * t0 + G01 * t1);
+        double h1 = 0.5 * (G01 * t0 + G11 * t1 + G13 * t3);
+        double h2 = 0.5 * (G22 * t2);
+        const double h3 = 0.5 * (G13 * t1 + G33 * t3);
+        h1 += r * s.k.v[1] * qn.v[1];
+        h2 += t.d2th11 * s.k.v[1] * qn.v[1] + t.d2th12 * (s.k.v[1] * qn.v[2] + s.k.v[2] * qn.v[1]) +
+              t.d2th22 * s.k.v[2] * qn.v[2];
+        const double h1r = h1 * inv_r;
+        D4 out;
+        out.v[0] = -h0;
+        out.v[1] = -h1r;
+        out.v[2] = -((h2 - t.dth1 * h1r) * inv_dth2);
+        out.v[3] = -h3;
+        return out;
+    };
+    Ray d;
+    d.x = s.k;
+    d.k = contract(s.k);
+    d.e1 = contract(s.e1);
+    d.e2 = contract(s.e2);
+    return d;
+}
+
 // Camera at phi = 0 and its ipole tetrad in FMKS (camera.hpp:302-456): the
 // normal observer, the raised centering covector (1, 1, 0, 0), and the native
 // trial vectors (0, 0, 1, 0), (1, 1, 1, 1), made orthonormal by Gram-Schmidt.

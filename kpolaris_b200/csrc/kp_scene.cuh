@@ -90,9 +90,15 @@ struct SceneGrmhd {
         __device__ double dot(const D4& u, const D4& v) const { return dot_gm(g, u, v); }
     };
     __device__ static double radius(const ImageConsts&, const D4& X) { return fmks_radius(X); }
+    // FP64 everywhere (an FP32 FMKS connection puts its rounding noise into
+    // the step-doubling error norm); the mixed policy uses the factored form
     template<bool MIXED, bool FP32>
     __device__ static Ray rhs(const ImageConsts& c, const Ray& X) {
-        return fmks_rhs(c.fmks, X);
+        if constexpr (MIXED) {
+            return fmks_rhs_factored(c.fmks, X);
+        } else {
+            return fmks_rhs(c.fmks, X);
+        }
     }
     __device__ static Ray camera(const ImageConsts& c, const CameraFrame& f, int pixel) {
         return fmks_camera_ray(c, f, pixel);

@@ -50,6 +50,10 @@ void h_fmks_rhs(const kp_pass_a_params* p, const double* s16, double* d16) {
     store(kp::fmks_rhs(fmks_of(p), ray_of(s16)), d16);
 }
 
+void h_fmks_rhs_factored(const kp_pass_a_params* p, const double* s16, double* d16) {
+    store(kp::fmks_rhs_factored(fmks_of(p), ray_of(s16)), d16);
+}
+
 void h_camera_ray_fmks(const kp_pass_a_params* p, int pixel, double* s16) {
     kp_grmhd_model m;
     std::memset(&m, 0, sizeof(m));

@@ -46,6 +46,7 @@ def host(tmp_path_factory):
     L = C.CDLL(str(so))
     P, d = C.POINTER, C.c_double
     L.h_fmks_rhs.argtypes = [P(_abi.PassAParams), P(d), P(d)]
+    L.h_fmks_rhs_factored.argtypes = [P(_abi.PassAParams), P(d), P(d)]
     L.h_camera_ray_fmks.argtypes = [P(_abi.PassAParams), C.c_int, P(d)]
     L.h_grmhd_derived.argtypes = [P(_abi.GrmhdModel), P(C.c_float), P(d)]
     L.h_grmhd_coefficients.argtypes = [P(_abi.PassAParams), P(_abi.GrmhdModel), P(C.c_float), P(d), P(d), d, P(d)]
@@ -142,6 +143,26 @@ def test_host_fmks_rhs_matches_reference(host, case):
             scale = np.max(np.abs(want[4 * v:4 * v + 4]))
             if scale > 0:
                 worst = max(worst, np.max(np.abs(got[4 * v:4 * v + 4] - want[4 * v:4 * v + 4])) / scale)
+    assert worst <= 1e-12, worst
+
+
+@needs_reference
+def test_host_factored_fmks_rhs_matches_reference(host, case):
+    """The mixed policy's factored FMKS RHS (kp_fmks.cuh fmks_rhs_factored):
+    the same algebra regrouped, within 1e-12 normwise per vector of the
+    reference's transport_rhs, from the horizon out to the camera."""
+    _, _, model, params, _ = case
+    worst = 0.0
+    for lo, hi in ((1.6, 6.0), (2.5, 40.0), (40.0, 1000.0)):
+        for s in seeded_states(model, 300, 13, r_lo=lo, r_hi=hi):
+            want = oracle.transport_rhs_fmks(params, s)
+            got = np.empty(16)
+            host.h_fmks_rhs_factored(C.byref(params), _dp(np.ascontiguousarray(s)), _dp(got))
+            assert np.array_equal(got[:4], s[4:8])
+            for v in range(1, 4):
+                scale = np.max(np.abs(want[4 * v:4 * v + 4]))
+                if scale > 0:
+                    worst = max(worst, np.max(np.abs(got[4 * v:4 * v + 4] - want[4 * v:4 * v + 4])) / scale)
     assert worst <= 1e-12, worst
 
 
