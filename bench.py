@@ -80,6 +80,18 @@ def dist_env():
     return rank, world, local
 
 
+def max_over_ranks(value, pg=None, device=None):
+    """The largest `value` over all ranks (replica timing takes the slowest
+    rank); the identity without a process group."""
+    if pg is None:
+        return float(value)
+    import torch
+
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
 def workload(n):
     from kpolaris_b200 import configs
 
@@ -620,11 +632,7 @@ def ours_arm(args):
     if pg:
         pg.barrier()
     step_ms = [a.elapsed_time(b) for a, b in evs]
-    ms = sum(step_ms) / len(step_ms)
-    if pg:
-        t = torch.tensor([ms], device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(sum(step_ms) / len(step_ms), pg, dev)
     value = world * batch * 1000.0 / ms
 
     progress("plain FP64 kernel")
@@ -676,11 +684,7 @@ def ours_arm(args):
         dt = (time.perf_counter() - t0) * 1000.0
         if i > 0:
             e2e_ms.append(dt)
-    e2e = sum(e2e_ms) / len(e2e_ms)
-    if pg:
-        t = torch.tensor([e2e], device=dev)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e = float(t.item())
+    e2e = max_over_ranks(sum(e2e_ms) / len(e2e_ms), pg, dev)
     d2h = batch * int(lib.kp_image_output_bytes(npix, nfreq))
     h2d = batch * int(lib.kp_abi_sizeof(6))
 
@@ -720,8 +724,10 @@ def ours_arm(args):
                 "peak_source": "measured FP64 FMA throughput of this GPU (kp_measure_fma_peak), of measured",
                 "flops_source": "algorithmic FP64 op count of the reference algorithm"}
 
+    # the serving trace, config 3 and config 4 are single-GPU measurements:
+    # they run at N = 1 only, so replica runs time the headline alone
     serving = None
-    if mixed and args.serve_requests > 0:
+    if mixed and args.serve_requests > 0 and world == 1:
         progress("serving trace")
         trace = serving_trace(args.serve_requests, args.serve_rate)
         grids = serving_grids(local)
@@ -740,12 +746,12 @@ def ours_arm(args):
                 g.release()
 
     grmhd = None
-    if args.grmhd:
+    if args.grmhd and world == 1:
         progress("GRMHD image")
         grmhd = grmhd_section(args, torch, dev, local, stream, flush, rank)
 
     config4 = None
-    if args.config4:
+    if args.config4 and world == 1:
         progress("uneven batch and slow light")
         config4 = config4_section(local, stream, flush, torch)
 
