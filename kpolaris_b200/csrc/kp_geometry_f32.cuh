@@ -23,13 +23,36 @@
 
 namespace kp {
 
+// sqrt(v) with its reciprocal, and 1/v: FP64 as written; FP32 (the far
+// field, where the contraction's own cancellation already limits it to
+// ~3e-5) from one hardware reciprocal square root or reciprocal each, a few
+// ulp instead of the correctly rounded IEEE sequences.
 template<class T>
-KP_HD T kp_sqrt_t(T v) {
-    return sqrt(v);
+KP_HD void kp_sqrt_pair(T v, T& sq, T& inv) {
+    sq = sqrt(v);
+    inv = T(1) / sq;
 }
 template<>
-KP_HD float kp_sqrt_t<float>(float v) {
-    return sqrtf(v);
+KP_HD void kp_sqrt_pair<float>(float v, float& sq, float& inv) {
+#ifdef __CUDA_ARCH__
+    inv = rsqrtf(v);
+    sq = v * inv;
+#else
+    sq = sqrtf(v);
+    inv = 1.0f / sq;
+#endif
+}
+template<class T>
+KP_HD T kp_recip(T v) {
+    return T(1) / v;
+}
+template<>
+KP_HD float kp_recip<float>(float v) {
+#ifdef __CUDA_ARCH__
+    return __fdividef(1.0f, v);
+#else
+    return 1.0f / v;
+#endif
 }
 
 template<class T>
@@ -38,13 +61,13 @@ KP_HD Ray ks_rhs_factored(double mass_d, double spin_d, const Ray& s) {
     const T x = T(s.x.v[1]), y = T(s.x.v[2]), z = T(s.x.v[3]);
     const T a2 = a * a;
     const T sqsum = x * x + y * y + z * z - a2;
-    const T discr = kp_sqrt_t<T>(sqsum * sqsum + T(4) * a2 * z * z);
+    T discr, inv_discr;
+    kp_sqrt_pair<T>(sqsum * sqsum + T(4) * a2 * z * z, discr, inv_discr);
     const T r2 = T(0.5) * (sqsum + discr);
-    const T r = kp_sqrt_t<T>(r2 > T(1e-30) ? r2 : T(1e-30));
-    const T inv_r = T(1) / r;
-    const T inv_denom = T(1) / (r2 * r2 + a2 * z * z);
-    const T inv_rp = T(1) / (r2 + a2);
-    const T inv_discr = T(1) / discr;
+    T r, inv_r;
+    kp_sqrt_pair<T>(r2 > T(1e-30) ? r2 : T(1e-30), r, inv_r);
+    const T inv_denom = kp_recip<T>(r2 * r2 + a2 * z * z);
+    const T inv_rp = kp_recip<T>(r2 + a2);
     const T amp = T(2) * M * r2 * r * inv_denom;
     const T amp_r = T(-2) * M * r2 * (r2 * r2 - T(3) * a2 * z * z) * (inv_denom * inv_denom);
     const T l1 = (r * x + a * y) * inv_rp;
