@@ -29,11 +29,11 @@ COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=o
 # translation unit -> extra flags
 UNITS = {
     "kp_kernels_fp64.cu": ["--fmad=false"],
-    "kp_kernels_mixed.cu": ["--fmad=true"],
+    "kp_kernels_mixed.cu": ["--fmad=true", "--use_fast_math"],
     "kp_kernels_grmhd.cu": ["--fmad=false"],
-    "kp_kernels_grmhd_mixed.cu": ["--fmad=true"],
+    "kp_kernels_grmhd_mixed.cu": ["--fmad=true", "--use_fast_math"],
     "kp_kernels_grmhd_slow.cu": ["--fmad=false"],
-    "kp_kernels_grmhd_slow_mixed.cu": ["--fmad=true"],
+    "kp_kernels_grmhd_slow_mixed.cu": ["--fmad=true", "--use_fast_math"],
     "kp_capi.cu": ["--fmad=false"],
     "kp_noalloc.cu": ["--fmad=false"],
     "kp_server.cu": ["--fmad=false"],

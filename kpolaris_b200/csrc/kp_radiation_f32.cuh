@@ -70,6 +70,21 @@ KP_HD void kp_sincosf(float x, float* s, float* c) {
 #endif
 }
 
+// sin and cos of an angle that is usually small: below |x| = 0.5 from their
+// Taylor series to the x^9 / x^8 terms (truncation < 1e-11, under FP32
+// rounding), keeping full relative accuracy where a hardware sine's absolute
+// error would not; above it the library (or hardware) form.
+KP_HD void kp_sincos_small(float x, float* s, float* c) {
+    if (fabsf(x) < 0.5f) {
+        const float x2 = x * x;
+        *s = x * (1.0f - x2 * (1.0f / 6.0f) * (1.0f - x2 * (1.0f / 20.0f) * (1.0f - x2 * (1.0f / 42.0f) *
+                                                                                     (1.0f - x2 * (1.0f / 72.0f)))));
+        *c = 1.0f - x2 * 0.5f * (1.0f - x2 * (1.0f / 12.0f) * (1.0f - x2 * (1.0f / 30.0f) * (1.0f - x2 * (1.0f / 56.0f))));
+        return;
+    }
+    kp_sincosf(x, s, c);
+}
+
 struct StokesF {
     float I, Q, U, V;     // scaled by 2^E
     float cI, cQ, cU, cV; // compensation terms
@@ -546,7 +561,7 @@ KP_HD void faraday_rotate_f(StokesF& s, const CoeffsF& c, float dl) {
         // half-angle forms: 1 - cos(theta) = 2 sin^2(theta/2) keeps its
         // relative accuracy for small rotations
         float sh, ch;
-        kp_sincosf(0.5f * theta, &sh, &ch);
+        kp_sincos_small(0.5f * theta, &sh, &ch);
         const float st = 2.0f * sh * ch;
         const float omc = 2.0f * sh * sh;
         const float ct = 1.0f - omc;
