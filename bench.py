@@ -710,10 +710,11 @@ def ours_arm(args):
         traffic = None
         if TRAFFIC_TABLE.exists() and args.n == 256 and batch == 8:
             t = json.loads(TRAFFIC_TABLE.read_text()).get(f"wave_{name}_mixed")
-            traffic = t["bytes_per_bench_launch"] if t else None
+            traffic = t["bytes_per_bench_step"] if t else None
         roof = {"bound": "fp64" if bound64 else "fp32", "kernel": f"wave_{name}_mixed",
                 "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                "traffic": traffic, "traffic_unit": "bytes per launch (ncu, scaled; see profiles/)",
+                "traffic": traffic,
+                "traffic_unit": "DRAM bytes of the phase's launches in one step (ncu, scaled by rays; see profiles/)",
                 "peak_source": "measured FMA throughput of this GPU (kp_measure_fma_peak), of measured",
                 "flops_source": "algorithmic op count of the reference algorithm per phase "
                                 "(profiles/flop_counts.json) x images per launch"}
