@@ -35,6 +35,7 @@ UNITS = {
     "kp_kernels_grmhd_slow.cu": ["--fmad=false"],
     "kp_kernels_grmhd_slow_mixed.cu": ["--fmad=true", "--use_fast_math"],
     "kp_capi.cu": ["--fmad=false"],
+    "kp_reorder.cu": ["--fmad=false"],
     "kp_noalloc.cu": ["--fmad=false"],
     "kp_server.cu": ["--fmad=false"],
     "kp_peak.cu": [],

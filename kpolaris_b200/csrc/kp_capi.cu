@@ -85,6 +85,8 @@ struct DeviceState {
     unsigned* d_ids[kPhases][2] = {};  // id queues per phase, by generation parity
     long long pool_cap = 0;
     unsigned* h_left = nullptr;     // pinned: queue counts after a cycle
+    unsigned* d_sorted = nullptr;   // near-B queue in longest-first order (pool_cap)
+    unsigned* d_lpt = nullptr;      // its bucket counters (2 x 256)
     void* d_series = nullptr;       // slow light: snapshot table and times (grow-only)
     size_t series_bytes = 0;
     // schedule tuning per engine family (kp_autotune_batch): CTAs per SM of
@@ -519,11 +521,15 @@ int run_wave_jobs(DeviceState* dev, cudaStream_t stream, int njobs, long long to
             cudaFree(q[1]);
             q[0] = q[1] = nullptr;
         }
+        cudaFree(dev->d_sorted);
+        dev->d_sorted = nullptr;
         dev->pool_cap = 0;
         cudaError_t e = cudaMalloc(&dev->d_pool, sizeof(RayRecord) * size_t(total));
         for (auto& q : dev->d_ids)
             for (auto& b : q)
                 if (e == cudaSuccess) e = cudaMalloc(&b, sizeof(unsigned) * size_t(total));
+        if (e == cudaSuccess) e = cudaMalloc(&dev->d_sorted, sizeof(unsigned) * size_t(total));
+        if (e == cudaSuccess && !dev->d_lpt) e = cudaMalloc(&dev->d_lpt, sizeof(unsigned) * 512);
         if (e != cudaSuccess) {
             cudaGetLastError();
             return set_error(KP_ERR_OOM, "cudaMalloc(%lld ray records): %s", total, cudaGetErrorString(e));
@@ -581,6 +587,13 @@ int run_wave_jobs(DeviceState* dev, cudaStream_t stream, int njobs, long long to
         W.budget = 0;
         W.status = &ctrl->status;
         W.job_done = nullptr;
+        if (phase == kPhaseNearB) {
+            // longest rays first (kp_reorder.cu): shortens the tail of the launch
+            const cudaError_t le = launch_lpt_order(W.in_ids, W.in_count, dev->d_pool, dev->d_lpt, dev->d_sorted,
+                                                    dev->sms, stream);
+            if (le != cudaSuccess) return le;
+            W.in_ids = dev->d_sorted;
+        }
         if (family == kFamilyGrmhdFP64) return launch_wave_grmhd(phase, W, nf_max, blocks[phase], wave_threads(phase), stream);
         if (family == kFamilyGrmhdMixed)
             return launch_wave_grmhd_mixed(phase, W, nf_max, blocks[phase], wave_threads(phase), stream);

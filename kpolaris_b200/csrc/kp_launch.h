@@ -48,6 +48,11 @@ int wave_occupancy_grmhd_mixed(int phase, int nf_max, int threads);
 cudaError_t launch_seed_grmhd_mixed(const JobDesc* jobs, const SeedEntry* entries, const long long* prefix,
                                     int nentries, long long total, RayRecord* pool, unsigned* far_ids,
                                     unsigned* far_count, cudaStream_t stream);
+// Longest-first order of a near-B queue (kp_reorder.cu): `count` ids from
+// `ids` into `out`, grouped by pass-A steps, most first; `scratch` holds 512
+// unsigned counters.
+cudaError_t launch_lpt_order(const unsigned* ids, const unsigned* count, const RayRecord* pool, unsigned* scratch,
+                             unsigned* out, int sms, cudaStream_t stream);
 // Slow-light GRMHD (kp_kernels_grmhd_slow.cu, kp_kernels_grmhd_slow_mixed.cu).
 cudaError_t launch_wave_grmhd_slow(int phase, const WaveDesc& W, int nf_max, int blocks, int threads,
                                    cudaStream_t stream);
