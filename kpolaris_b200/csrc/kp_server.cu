@@ -110,6 +110,8 @@ struct kp_server {
     unsigned* counts[kServeScenes] = {};           // per scene [2][kPhases]
     unsigned long long* heads[kServeScenes] = {};  // per scene [kPhases]
     long long scene_cycle[kServeScenes] = {};      // generation parity of each scene's queues
+    unsigned* sorted = nullptr;                    // near-B queue in longest-first order (max_rays)
+    unsigned* lpt = nullptr;                       // its bucket counters (512)
     int* status = nullptr;
     unsigned* done = nullptr;              // [max_jobs]
     JobDesc* d_jobs = nullptr;
@@ -145,6 +147,8 @@ void end_job(ServerJob& j) {
 
 void release_device(kp_server* s) {
     cudaFree(s->pool);
+    cudaFree(s->sorted);
+    cudaFree(s->lpt);
     for (int sc = 0; sc < kServeScenes; ++sc) {
         for (auto& q : s->ids[sc]) {
             cudaFree(q[0]);
@@ -177,6 +181,8 @@ int allocate_device(kp_server* s) {
         if (e == cudaSuccess) e = cudaMalloc(p, n);
     };
     dev((void**)&s->pool, sizeof(RayRecord) * size_t(c.max_rays));
+    dev((void**)&s->sorted, sizeof(unsigned) * size_t(c.max_rays));
+    dev((void**)&s->lpt, sizeof(unsigned) * 512);
     for (int sc = 0; sc < kServeScenes; ++sc) {
         for (auto& q : s->ids[sc])
             for (auto& b : q) dev((void**)&b, sizeof(unsigned) * size_t(c.max_rays));
@@ -423,6 +429,12 @@ void worker_main(kp_server* s) {
                 W.budget = s->cfg.tick_budget;
                 W.status = s->status;
                 W.job_done = s->done;
+                if (p == kPhaseNearB) {
+                    // longest rays first (kp_reorder.cu)
+                    e = launch_lpt_order(W.in_ids, W.in_count, s->pool, s->lpt, s->sorted, sms, s->stream);
+                    if (e != cudaSuccess) break;
+                    W.in_ids = s->sorted;
+                }
                 const int b = blocks[sc][p], th = wave_threads(p);
                 if (sc == kServeGrmhd)
                     e = mixed ? launch_wave_grmhd_mixed(p, W, nf_max, b, th, s->stream)
