@@ -340,7 +340,9 @@ int kp_batch_riaf(const kp_riaf_job* jobs, int njobs, const kp_run_options* opti
  * (src/model/grmhd_grid.hpp:52-97) this path uses; the grid itself is
  * uploaded once with kp_grid_upload (primitives as FP32
  * [8][n1][n2][n3]: rho, u, U1, U2, U3, B1, B2, B3 in code units) and stays
- * resident until kp_grid_release.  With has_derived_scalars the derived
+ * resident until kp_grid_release; on the device it is stored cell-major
+ * (8 floats per cell, 16-byte aligned) so each trilinear corner is two
+ * vector loads.  With has_derived_scalars the derived
  * scalars (n_e, Theta_e, B, sigma, beta per cell; the loaders'
  * precompute_derived_scalars, src/grmhd/kharma_loader.cpp:261-362) are
  * computed on the device at upload.  Thermal fits only (emission_type

@@ -1182,18 +1182,25 @@ int kp_grid_upload(const kp_grmhd_model* model, const float* prims, int device, 
     g->device = device;
     g->model = *model;
     const size_t ncell = size_t(model->n1) * size_t(model->n2) * size_t(model->n3);
-    cudaError_t e = cudaMalloc(&g->prims, sizeof(float) * 8 * ncell);
-    if (e == cudaSuccess && model->has_derived_scalars) e = cudaMalloc(&g->derived, sizeof(double) * kNumDerived * ncell);
+    // cell-major device layout (kPrimStride floats, kDerStride doubles per
+    // cell), filled from the reference layout through a staging buffer
+    float* staging = nullptr;
+    cudaError_t e = cudaMalloc(&g->prims, sizeof(float) * kPrimStride * ncell);
+    if (e == cudaSuccess) e = cudaMalloc(&staging, sizeof(float) * 8 * ncell);
+    if (e == cudaSuccess && model->has_derived_scalars) e = cudaMalloc(&g->derived, sizeof(double) * kDerStride * ncell);
     if (e != cudaSuccess) {
         cudaGetLastError();
         cudaFree(g->prims);
         cudaFree(g->derived);
+        cudaFree(staging);
         delete g;
         return set_error(KP_ERR_OOM, "grid allocation (%zu cells): %s", ncell, cudaGetErrorString(e));
     }
-    e = cudaMemcpyAsync(g->prims, prims, sizeof(float) * 8 * ncell, cudaMemcpyHostToDevice, dev->stream);
+    e = cudaMemcpyAsync(staging, prims, sizeof(float) * 8 * ncell, cudaMemcpyHostToDevice, dev->stream);
+    if (e == cudaSuccess) e = launch_grid_to_cells(staging, g->prims, (long long)ncell, dev->sms, dev->stream);
     if (e == cudaSuccess && g->derived) e = launch_grid_derived(grid_consts(g), g->derived, dev->sms, dev->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(dev->stream);
+    cudaFree(staging);
     if (e != cudaSuccess) {
         cudaFree(g->prims);
         cudaFree(g->derived);
@@ -1209,8 +1216,12 @@ int kp_grid_derived(const kp_grid* g, double* out) {
     if (!g->derived) return set_error(KP_ERR_INVALID, "the grid has no derived scalars");
     cudaError_t e = cudaSetDevice(g->device);
     const size_t ncell = size_t(g->model.n1) * size_t(g->model.n2) * size_t(g->model.n3);
-    if (e == cudaSuccess) e = cudaMemcpy(out, g->derived, sizeof(double) * kNumDerived * ncell, cudaMemcpyDeviceToHost);
+    std::vector<double> cells(ncell * kDerStride);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(cells.data(), g->derived, sizeof(double) * kDerStride * ncell, cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return cuda_error(e, "derived scalar copy");
+    for (size_t p = 0; p < ncell; ++p)
+        for (int v = 0; v < kNumDerived; ++v) out[size_t(v) * ncell + p] = cells[p * kDerStride + size_t(v)];
     return KP_OK;
 }
 

@@ -65,9 +65,15 @@ struct FmksParams {
 
 // A GRMHD snapshot resident on the device (GRMHDGridRadiationModel scalars,
 // grmhd_grid.hpp:52-97, with the unit conversions resolved on the host).
+// Device layout of a grid: cell-major, so the eight corners of a trilinear
+// stencil read whole 32-byte cells (primitives) and 48-byte cells (derived
+// scalars) with 16-byte vector loads.
+constexpr int kPrimStride = 8;  // floats per cell: rho, u, U1..U3, B1..B3
+constexpr int kDerStride = 6;   // doubles per cell: n_e, Theta_e, B, sigma, beta, pad
+
 struct GridConsts {
-    const float* prims;      // [8][n1][n2][n3]: rho, u, U1..U3, B1..B3
-    const double* derived;   // [5][n1][n2][n3]: n_e, Theta_e, B, sigma, beta (or null)
+    const float* prims;      // [n1][n2][n3][kPrimStride]
+    const double* derived;   // [n1][n2][n3][kDerStride] (or null)
     int n1, n2, n3, has_derived;
     double startx1, startx2, startx3, dx1, dx2, dx3;
     double r_in, r_out, gam;

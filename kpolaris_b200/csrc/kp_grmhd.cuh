@@ -156,16 +156,42 @@ KP_HD bool grid_stencil(const GridConsts& g, double x1, double x2, double phi, G
     return true;
 }
 
-KP_HD double grid_interp(const GridStencil& st, const float* field) {
-    double out = 0.0;
-    for (int n = 0; n < 8; ++n) out += st.w[n] * double(field[st.cell[n]]);
-    return out;
+// The eight primitives at a point: each corner is one 32-byte cell (two
+// 16-byte loads); every field accumulates over the corners in stencil order.
+KP_HD void grid_gather_prims(const GridStencil& st, const float* prims, double out[kPrimStride]) {
+    for (int v = 0; v < kPrimStride; ++v) out[v] = 0.0;
+    for (int n = 0; n < 8; ++n) {
+        const float* c = prims + st.cell[n] * kPrimStride;
+        float val[kPrimStride];
+#ifdef __CUDA_ARCH__
+        const float4 a = __ldg(reinterpret_cast<const float4*>(c));
+        const float4 b = __ldg(reinterpret_cast<const float4*>(c) + 1);
+        val[0] = a.x; val[1] = a.y; val[2] = a.z; val[3] = a.w;
+        val[4] = b.x; val[5] = b.y; val[6] = b.z; val[7] = b.w;
+#else
+        for (int v = 0; v < kPrimStride; ++v) val[v] = c[v];
+#endif
+        for (int v = 0; v < kPrimStride; ++v) out[v] += st.w[n] * double(val[v]);
+    }
 }
 
-KP_HD double grid_interp(const GridStencil& st, const double* field) {
-    double out = 0.0;
-    for (int n = 0; n < 8; ++n) out += st.w[n] * field[st.cell[n]];
-    return out;
+// The five derived scalars at a point: each corner is one 48-byte cell
+// (three 16-byte loads).
+KP_HD void grid_gather_derived(const GridStencil& st, const double* derived, double out[kNumDerived]) {
+    for (int v = 0; v < kNumDerived; ++v) out[v] = 0.0;
+    for (int n = 0; n < 8; ++n) {
+        const double* c = derived + st.cell[n] * kDerStride;
+        double val[kDerStride];
+#ifdef __CUDA_ARCH__
+        const double2 a = __ldg(reinterpret_cast<const double2*>(c));
+        const double2 b = __ldg(reinterpret_cast<const double2*>(c) + 1);
+        const double2 d = __ldg(reinterpret_cast<const double2*>(c) + 2);
+        val[0] = a.x; val[1] = a.y; val[2] = b.x; val[3] = b.y; val[4] = d.x; val[5] = d.y;
+#else
+        for (int v = 0; v < kDerStride; ++v) val[v] = c[v];
+#endif
+        for (int v = 0; v < kNumDerived; ++v) out[v] += st.w[n] * val[v];
+    }
 }
 
 // Linear interpolation in time that keeps the endpoints and static values
@@ -194,22 +220,20 @@ __device__ __forceinline__ GrmhdSample grmhd_sample_from(const ImageConsts& c, c
     if (!(r >= g.r_in && r < g.r_out)) return out;
     GridStencil st;
     if (!grid_stencil(g, x1, x2, phi, st)) return out;
-    const size_t ncell = size_t(g.n1) * size_t(g.n2) * size_t(g.n3);
-    auto prim = [&](size_t v) {
-        const double a = grid_interp(st, g.prims + v * ncell);
-        return up ? time_interp(a, grid_interp(st, up->prims + v * ncell), f) : a;
-    };
-    auto derived = [&](size_t v) {
-        const double a = grid_interp(st, g.derived + v * ncell);
-        return up ? time_interp(a, grid_interp(st, up->derived + v * ncell), f) : a;
-    };
-    const double rho = prim(kPrimRho);
-    const double uu = prim(kPrimU);
+    double P[kPrimStride];
+    grid_gather_prims(st, g.prims, P);
+    if (up) {
+        double Pu[kPrimStride];
+        grid_gather_prims(st, up->prims, Pu);
+        for (int v = 0; v < kPrimStride; ++v) P[v] = time_interp(P[v], Pu[v], f);
+    }
+    const double rho = P[kPrimRho];
+    const double uu = P[kPrimU];
     if (!(rho > 0.0 && uu > 0.0)) return out;
     double U[3], B[3];
     for (int i = 0; i < 3; ++i) {
-        U[i] = prim(size_t(kPrimU1 + i));
-        B[i] = prim(size_t(kPrimB1 + i));
+        U[i] = P[kPrimU1 + i];
+        B[i] = P[kPrimB1 + i];
     }
     double gcov[4][4], gcon0[4];
     grid_native_metric(g, r, th, dth1, dth2, gcov, gcon0);
@@ -217,10 +241,17 @@ __device__ __forceinline__ GrmhdSample grmhd_sample_from(const ImageConsts& c, c
     const double bsq = grid_four_vectors(gcov, gcon0, U, B, ucon, bcon);
     double ne, thetae, bcgs, sigma;
     if (g.has_derived) {
-        ne = derived(kDerNe);
-        thetae = derived(kDerThetae);
-        bcgs = derived(kDerB);
-        sigma = derived(kDerSigma);
+        double D[kNumDerived];
+        grid_gather_derived(st, g.derived, D);
+        if (up) {
+            double Du[kNumDerived];
+            grid_gather_derived(st, up->derived, Du);
+            for (int v = 0; v < kNumDerived; ++v) D[v] = time_interp(D[v], Du[v], f);
+        }
+        ne = D[kDerNe];
+        thetae = D[kDerThetae];
+        bcgs = D[kDerB];
+        sigma = D[kDerSigma];
     } else {
         sigma = bsq / max_val(rho, kTiny);
         const double beta = (g.gam - 1.0) * uu / (0.5 * bsq);
@@ -341,8 +372,8 @@ __device__ __forceinline__ Coeffs<double> grmhd_coefficients(const ImageConsts& 
 // Derived scalars of one cell (precompute_derived_scalars): n_e, Theta_e,
 // B in gauss, sigma, beta from the cell-centre primitives.
 KP_HD void grid_derived_cell(const GridConsts& g, int i, int j, int k, double out[kNumDerived]) {
-    const size_t ncell = size_t(g.n1) * size_t(g.n2) * size_t(g.n3);
     const size_t cell = (size_t(i) * size_t(g.n2) + size_t(j)) * size_t(g.n3) + size_t(k);
+    const float* pc = g.prims + cell * kPrimStride;
     const double x1 = g.startx1 + (double(i) + 0.5) * g.dx1;
     const double x2 = g.startx2 + (double(j) + 0.5) * g.dx2;
     const double r = exp(x1);
@@ -350,12 +381,12 @@ KP_HD void grid_derived_cell(const GridConsts& g, int i, int j, int k, double ou
     grid_theta(g, x1, x2, th, dth1, dth2);
     double gcov[4][4], gcon0[4];
     grid_native_metric(g, r, th, dth1, dth2, gcov, gcon0);
-    const double rho = g.prims[0 * ncell + cell];
-    const double uu = g.prims[1 * ncell + cell];
+    const double rho = pc[kPrimRho];
+    const double uu = pc[kPrimU];
     double U[3], B[3];
     for (int n = 0; n < 3; ++n) {
-        U[n] = g.prims[size_t(kPrimU1 + n) * ncell + cell];
-        B[n] = g.prims[size_t(kPrimB1 + n) * ncell + cell];
+        U[n] = pc[kPrimU1 + n];
+        B[n] = pc[kPrimB1 + n];
     }
     double ucon[4], bcon[4];
     const double bsq = grid_four_vectors(gcov, gcon0, U, B, ucon, bcon);

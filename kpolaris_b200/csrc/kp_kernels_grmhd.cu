@@ -63,7 +63,8 @@ cudaError_t launch_seed_grmhd(const JobDesc* jobs, const SeedEntry* entries, con
 }
 
 // One thread per cell, consecutive threads along phi (the innermost index):
-// the eight primitive loads and five stores of a warp are contiguous.
+// a warp reads 32 consecutive 32-byte primitive cells and writes 32
+// consecutive 48-byte derived cells.
 __global__ void __launch_bounds__(256) grid_derived_kernel(const GridConsts g, double* derived) {
     const long long ncell = (long long)g.n1 * g.n2 * g.n3;
     for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < ncell;
@@ -73,8 +74,33 @@ __global__ void __launch_bounds__(256) grid_derived_kernel(const GridConsts g, d
         const int i = int(p / ((long long)g.n2 * g.n3));
         double out[kNumDerived];
         grid_derived_cell(g, i, j, k, out);
-        for (int v = 0; v < kNumDerived; ++v) derived[(size_t)v * (size_t)ncell + (size_t)p] = out[v];
+        double* c = derived + (size_t)p * kDerStride;
+        for (int v = 0; v < kNumDerived; ++v) c[v] = out[v];
+        for (int v = kNumDerived; v < kDerStride; ++v) c[v] = 0.0;
     }
+}
+
+// Reference layout [8][ncell] -> cell-major [ncell][8]: thread p reads field
+// v of cell p (coalesced over p for each v) and writes its cell as two
+// 16-byte stores.
+__global__ void __launch_bounds__(256) grid_to_cells_kernel(const float* soa, float* cells, long long ncell) {
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < ncell;
+         p += (long long)gridDim.x * blockDim.x) {
+        float v[kPrimStride];
+        for (int f = 0; f < kPrimStride; ++f) v[f] = soa[(size_t)f * (size_t)ncell + (size_t)p];
+        float4* c = reinterpret_cast<float4*>(cells + (size_t)p * kPrimStride);
+        c[0] = make_float4(v[0], v[1], v[2], v[3]);
+        c[1] = make_float4(v[4], v[5], v[6], v[7]);
+    }
+}
+
+cudaError_t launch_grid_to_cells(const float* soa, float* cells, long long ncell, int sms, cudaStream_t stream) {
+    long long blocks = (ncell + 255) / 256;
+    const long long cap = (long long)sms * 8;
+    if (blocks > cap) blocks = cap;
+    if (blocks < 1) blocks = 1;
+    grid_to_cells_kernel<<<int(blocks), 256, 0, stream>>>(soa, cells, ncell);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_grid_derived(const GridConsts& g, double* derived, int sms, cudaStream_t stream) {

@@ -63,6 +63,8 @@ int wave_occupancy_grmhd_slow_mixed(int phase, int nf_max, int threads);
 cudaError_t launch_seed_grmhd(const JobDesc* jobs, const SeedEntry* entries, const long long* prefix, int nentries,
                               long long total, RayRecord* pool, unsigned* far_ids, unsigned* far_count,
                               cudaStream_t stream);
+// Reference-layout primitives [8][ncell] into the cell-major device grid.
+cudaError_t launch_grid_to_cells(const float* soa, float* cells, long long ncell, int sms, cudaStream_t stream);
 cudaError_t launch_grid_derived(const GridConsts& g, double* derived, int sms, cudaStream_t stream);
 
 // Threads per CTA of each phase kernel (its __launch_bounds__): the far

@@ -7,6 +7,7 @@
 // states x[4] k[4] e1[4] e2[4]).
 #include <cmath>
 #include <cstring>
+#include <vector>
 #define __host__
 #define __device__
 #define __global__
@@ -16,6 +17,23 @@
 #include "kp_grmhd_setup.h"
 
 namespace {
+
+// the library stores grids cell-major; these turn the C-ABI layouts into it
+std::vector<float> prim_cells(const kp_grmhd_model* m, const float* prims) {
+    const size_t ncell = size_t(m->n1) * size_t(m->n2) * size_t(m->n3);
+    std::vector<float> cells(ncell * kp::kPrimStride);
+    for (size_t p = 0; p < ncell; ++p)
+        for (int f = 0; f < 8; ++f) cells[p * kp::kPrimStride + size_t(f)] = prims[size_t(f) * ncell + p];
+    return cells;
+}
+
+std::vector<double> derived_cells(const kp_grmhd_model* m, const double* derived) {
+    const size_t ncell = size_t(m->n1) * size_t(m->n2) * size_t(m->n3);
+    std::vector<double> cells(ncell * kp::kDerStride, 0.0);
+    for (size_t p = 0; p < ncell; ++p)
+        for (int v = 0; v < kp::kNumDerived; ++v) cells[p * kp::kDerStride + size_t(v)] = derived[size_t(v) * ncell + p];
+    return cells;
+}
 
 kp::Ray ray_of(const double* s) {
     kp::Ray r;
@@ -64,7 +82,8 @@ void h_camera_ray_fmks(const kp_pass_a_params* p, int pixel, double* s16) {
 }
 
 void h_grmhd_derived(const kp_grmhd_model* m, const float* prims, double* out) {
-    const kp::GridConsts g = kp::grid_consts_of(*m, prims, nullptr);
+    const std::vector<float> pc = prim_cells(m, prims);
+    const kp::GridConsts g = kp::grid_consts_of(*m, pc.data(), nullptr);
     const size_t ncell = size_t(m->n1) * size_t(m->n2) * size_t(m->n3);
     for (int i = 0; i < m->n1; ++i)
         for (int j = 0; j < m->n2; ++j)
@@ -78,7 +97,9 @@ void h_grmhd_derived(const kp_grmhd_model* m, const float* prims, double* out) {
 
 void h_grmhd_coefficients(const kp_pass_a_params* p, const kp_grmhd_model* m, const float* prims,
                           const double* derived, const double* s16, double freq, double* out11) {
-    const kp::GridConsts g = kp::grid_consts_of(*m, prims, derived);
+    const std::vector<float> pc = prim_cells(m, prims);
+    const std::vector<double> dc = derived ? derived_cells(m, derived) : std::vector<double>();
+    const kp::GridConsts g = kp::grid_consts_of(*m, pc.data(), derived ? dc.data() : nullptr);
     const kp::ImageConsts c = kp::image_consts_fmks(p, *m, g, &freq, 1, 0);
     const kp::GrmhdSample smp = kp::grmhd_sample(c, ray_of(s16));
     const kp::Coeffs<double> o = kp::grmhd_coefficients(c, smp, freq);
