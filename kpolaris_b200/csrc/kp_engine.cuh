@@ -234,9 +234,131 @@ __device__ __noinline__ void ck_job(const ImageConsts& c, const Ray& S, double h
                                   1.0 / 4.0};
             ray_lincomb<5>(fourth, S, h, kk, cc);
         }
-        err = state_error_norm(next, fourth);
+        err = control_error(next, fourth, max_val(c.tolerance, kTolFloor));
         mid = next;
     }
+}
+
+// Far-field RK chains of the mixed policy (Kerr-Schild scene).  Beyond the
+// radiating sphere the transports change the ray by ~M/r^2 per unit step, so
+// their FP32 rounding is far below the step-doubling tolerance; the state,
+// the position derivative (= k) and every chain endpoint stay FP64.  What
+// only feeds the FP32 contraction or sums FP32 derivatives is carried in
+// FP32: the stage inputs x, k, e1, e2 (formed from the chain base's FP32
+// copy) and the accumulator of dk, de1, de2.  Per stage that leaves four
+// FP32->FP64 conversions and eight FP64 FMAs (k of the next stage input, the
+// position accumulator) around the contraction, where converting FP64 stage
+// states took 28 conversions and 48 FP64 operations.  Stage order,
+// coefficients and the k1 reuse of step doubling are the reference's
+// (rk4.hpp:37-59, 108-161).
+struct ChainF {
+    float x[3];      // x^1..x^3 of the stage input
+    float q[3][4];   // k, e1, e2 of the stage input
+};
+
+__device__ __forceinline__ void chain_base_f(const Ray& B, ChainF& b) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i) b.x[i] = float(B.x.v[i + 1]);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        b.q[0][i] = float(B.k.v[i]);
+        b.q[1][i] = float(B.e1.v[i]);
+        b.q[2][i] = float(B.e2.v[i]);
+    }
+}
+
+// One RK4 chain of step hc from B.  k1 holds the RHS of B when use_k1 is set,
+// and receives it when save_k1 is set.
+__device__ __forceinline__ void far_chain_f(const ImageConsts& c, const Ray& B, double hc, bool use_k1,
+                                            bool save_k1, float (&k1)[3][4], Ray& end) {
+    const float M = float(c.mass), a = float(c.spin);
+    ChainF b;
+    chain_base_f(B, b);
+    ChainF X = b;
+    D4 Xk = B.k;   // k of the stage input, FP64: the position derivative
+    D4 Ax;         // position accumulator, FP64
+    float Aq[3][4];
+    const double hh = 0.5 * hc;
+#pragma unroll 1
+    for (int st = 0; st < 4; ++st) {
+        float kq[3][4];
+        if (st == 0 && use_k1) {
+#pragma unroll
+            for (int w = 0; w < 3; ++w)
+#pragma unroll
+                for (int i = 0; i < 4; ++i) kq[w][i] = k1[w][i];
+        } else {
+            ks_transport_factored<float>(M, a, X.x[0], X.x[1], X.x[2], X.q, kq);
+        }
+        if (st == 0 && save_k1) {
+#pragma unroll
+            for (int w = 0; w < 3; ++w)
+#pragma unroll
+                for (int i = 0; i < 4; ++i) k1[w][i] = kq[w][i];
+        }
+        // acc = ((k1 + 2 k2) + 2 k3) + k4
+        if (st == 0) {
+            Ax = Xk;
+#pragma unroll
+            for (int w = 0; w < 3; ++w)
+#pragma unroll
+                for (int i = 0; i < 4; ++i) Aq[w][i] = kq[w][i];
+        } else {
+            const double wd = st == 3 ? 1.0 : 2.0;
+            const float wf = st == 3 ? 1.0f : 2.0f;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) Ax.v[i] = Ax.v[i] + Xk.v[i] * wd;
+#pragma unroll
+            for (int w = 0; w < 3; ++w)
+#pragma unroll
+                for (int i = 0; i < 4; ++i) Aq[w][i] = Aq[w][i] + kq[w][i] * wf;
+        }
+        if (st < 3) {
+            // next stage input B + cc * (this stage's derivative)
+            const double cc = st < 2 ? hh : hc;
+            const float cf = float(cc);
+#pragma unroll
+            for (int i = 0; i < 3; ++i) X.x[i] = b.x[i] + X.q[0][i + 1] * cf;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) Xk.v[i] = B.k.v[i] + double(kq[0][i]) * cc;
+#pragma unroll
+            for (int w = 0; w < 3; ++w)
+#pragma unroll
+                for (int i = 0; i < 4; ++i) X.q[w][i] = b.q[w][i] + kq[w][i] * cf;
+        }
+    }
+    const double h6 = hc / 6.0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        end.x.v[i] = B.x.v[i] + Ax.v[i] * h6;
+        end.k.v[i] = B.k.v[i] + double(Aq[0][i]) * h6;
+        end.e1.v[i] = B.e1.v[i] + double(Aq[1][i]) * h6;
+        end.e2.v[i] = B.e2.v[i] + double(Aq[2][i]) * h6;
+    }
+}
+
+// Step-doubling attempt (half, half, full reusing k1), RK4 step or composed
+// RK4 pair from far_chain_f; outputs as rk_job's.
+__device__ __forceinline__ void far_job_f(int kind, const ImageConsts& c, const Ray& S, double h, Ray& next,
+                                          Ray& mid, double& err) {
+    float k1[3][4];
+    Ray R2;
+    const int nchain = kind == kRkRK4 ? 1 : (kind == kRkRK4x2 ? 2 : 3);
+    err = 0.0;
+#pragma unroll 1
+    for (int ch = 0; ch < nchain; ++ch) {
+        const double hc = (kind == kRkRK4 || ch == 2) ? h : 0.5 * h;
+        Ray E;
+        far_chain_f(c, ch == 1 ? R2 : S, hc, ch == 2, ch == 0 && kind == kRkSD, k1, E);
+        if (ch == 0 && kind != kRkRK4) {
+            R2 = E;
+        } else if (ch < 2) {
+            next = E;
+        } else {
+            err = control_error(E, next, max_val(c.tolerance, kTolFloor));
+        }
+    }
+    mid = kind == kRkSD ? R2 : next;
 }
 
 // Step-doubling attempt, RK4 step or composed RK4 pair as a stage loop around
@@ -247,6 +369,10 @@ __device__ __noinline__ void rk_job(int kind, const ImageConsts& c, const Ray& S
                                     Ray& next, Ray& mid, double& err) {
     if (kind == kRkCK) {
         ck_job<P, FP32, SC>(c, S, h, next, mid, err);
+        return;
+    }
+    if constexpr (FP32 && std::is_same_v<SC, SceneRiaf>) {
+        far_job_f(kind, c, S, h, next, mid, err);
         return;
     }
     // Stage schedule (see file header): SD = half chain (4), second half
@@ -307,7 +433,7 @@ __device__ __noinline__ void rk_job(int kind, const ImageConsts& c, const Ray& S
             } else {  // st == 10: full step endpoint
                 Ray full;
                 ray_axpy(full, S, h6_f, A);
-                err = state_error_norm(full, R1);
+                err = control_error(full, R1, max_val(c.tolerance, kTolFloor));
                 next = R1;
                 mid = R2;
             }

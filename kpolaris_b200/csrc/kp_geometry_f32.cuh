@@ -1,7 +1,8 @@
 // kp_geometry_f32.cuh -- the Kerr-Schild transport right-hand side of the
 // mixed-precision policy, in a factored form templated on the arithmetic
-// type: FP32 in the far field, FP64 inside the radiating sphere.  Inputs and
-// outputs stay FP64 Rays.
+// type: FP32 in the far field, FP64 inside the radiating sphere.  The core
+// (ks_transport_factored) works on T values; ks_rhs_factored wraps it for
+// FP64 Rays.
 //
 // Same algebra as ks_rhs in kp_geometry.cuh (the reference's specialised
 // transport_rhs, src/geometry/kerr_schild_cartesian.hpp:194-363), regrouped:
@@ -55,10 +56,10 @@ KP_HD float kp_recip<float>(float v) {
 #endif
 }
 
+// The transports of q[0] = k, q[1] = e1, q[2] = e2 at spatial position
+// (x, y, z): out[w] = dq[w]/dlambda = -Gamma(k, q[w]).
 template<class T>
-KP_HD Ray ks_rhs_factored(double mass_d, double spin_d, const Ray& s) {
-    const T M = T(mass_d), a = T(spin_d);
-    const T x = T(s.x.v[1]), y = T(s.x.v[2]), z = T(s.x.v[3]);
+KP_HD void ks_transport_factored(T M, T a, T x, T y, T z, const T (&q)[3][4], T (&out)[3][4]) {
     const T a2 = a * a;
     const T sqsum = x * x + y * y + z * z - a2;
     T discr, inv_discr;
@@ -92,7 +93,7 @@ KP_HD Ray ks_rhs_factored(double mass_d, double spin_d, const Ray& s) {
     const T dl23 = (y - c2) * dr3 * inv_rp;
     const T dl33 = (r - z * dr3) * (inv_r * inv_r);
 
-    const T k0 = T(s.k.v[0]), k1 = T(s.k.v[1]), k2 = T(s.k.v[2]), k3 = T(s.k.v[3]);
+    const T k0 = q[0][0], k1 = q[0][1], k2 = q[0][2], k3 = q[0][3];
     const T lk = k0 + l1 * k1 + l2 * k2 + l3 * k3;
     const T Mk1 = dl11 * k1 + dl12 * k2 + dl13 * k3;
     const T Mk2 = dl21 * k1 + dl22 * k2 + dl23 * k3;
@@ -102,12 +103,9 @@ KP_HD Ray ks_rhs_factored(double mass_d, double spin_d, const Ray& s) {
     const T dlk3 = dl13 * k1 + dl23 * k2 + dl33 * k3;
     const T Dk = d1 * k1 + d2 * k2 + d3 * k3;
 
-    Ray d;
-    d.x = s.k;
 #pragma unroll
     for (int which = 0; which < 3; ++which) {
-        const D4& src = which == 0 ? s.k : (which == 1 ? s.e1 : s.e2);
-        const T q0 = T(src.v[0]), q1 = T(src.v[1]), q2 = T(src.v[2]), q3 = T(src.v[3]);
+        const T q0 = q[which][0], q1 = q[which][1], q2 = q[which][2], q3 = q[which][3];
         const T lq = q0 + l1 * q1 + l2 * q2 + l3 * q3;
         const T Mq1 = dl11 * q1 + dl12 * q2 + dl13 * q3;
         const T Mq2 = dl21 * q1 + dl22 * q2 + dl23 * q3;
@@ -126,11 +124,30 @@ KP_HD Ray ks_rhs_factored(double mass_d, double spin_d, const Ray& s) {
         const T t3 = l3 * common + amp * (lq * Mk3 + lk * Mq3) - (d3 * lklq + amp * (dlk3 * lq + lk * dlq3));
         const T lt = -t0 + l1 * t1 + l2 * t2 + l3 * t3;
         const T al = amp * lt;
-        D4& dst = which == 0 ? d.k : (which == 1 ? d.e1 : d.e2);
-        dst.v[0] = -double(T(0.5) * (-t0 + al));
-        dst.v[1] = -double(T(0.5) * (t1 - l1 * al));
-        dst.v[2] = -double(T(0.5) * (t2 - l2 * al));
-        dst.v[3] = -double(T(0.5) * (t3 - l3 * al));
+        out[which][0] = -(T(0.5) * (-t0 + al));
+        out[which][1] = -(T(0.5) * (t1 - l1 * al));
+        out[which][2] = -(T(0.5) * (t2 - l2 * al));
+        out[which][3] = -(T(0.5) * (t3 - l3 * al));
+    }
+}
+
+template<class T>
+KP_HD Ray ks_rhs_factored(double mass_d, double spin_d, const Ray& s) {
+    T q[3][4], o[3][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        q[0][i] = T(s.k.v[i]);
+        q[1][i] = T(s.e1.v[i]);
+        q[2][i] = T(s.e2.v[i]);
+    }
+    ks_transport_factored<T>(T(mass_d), T(spin_d), T(s.x.v[1]), T(s.x.v[2]), T(s.x.v[3]), q, o);
+    Ray d;
+    d.x = s.k;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        d.k.v[i] = double(o[0][i]);
+        d.e1.v[i] = double(o[1][i]);
+        d.e2.v[i] = double(o[2][i]);
     }
     return d;
 }

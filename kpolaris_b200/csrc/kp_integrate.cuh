@@ -86,6 +86,30 @@ KP_HD double state_error_norm(const Ray& a, const Ray& b) {
     return err;
 }
 
+// The error the step control acts on.  The control needs the norm exactly
+// only above tol/64: at or below it the attempt is accepted and the growth
+// factor 0.9 (tol/err)^0.2 >= 2.07 clamps to 2 (rk4.hpp:130-142).  Every
+// scale of the norm is >= 1, so max |a - b| bounds it from above; when that
+// bound is at most tol/64 it stands in for the norm with the same accept
+// decision and the same next step, and the sixteen divisions are skipped.
+// A NaN difference fails the comparison and takes the exact norm.
+KP_HD double control_error(const Ray& a, const Ray& b, double tol) {
+    const double lim = tol * (1.0 / 64.0);
+    bool small = true;
+    double m = 0.0;
+#pragma unroll
+    for (int mu = 0; mu < 4; ++mu) {
+        const double d[4] = {abs_val(a.x.v[mu] - b.x.v[mu]), abs_val(a.k.v[mu] - b.k.v[mu]),
+                             abs_val(a.e1.v[mu] - b.e1.v[mu]), abs_val(a.e2.v[mu] - b.e2.v[mu])};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            small = small && d[i] <= lim;
+            m = max_val(m, d[i]);
+        }
+    }
+    return small ? m : state_error_norm(a, b);
+}
+
 struct StepControl {
     double tolerance, min_step, max_step;
 };

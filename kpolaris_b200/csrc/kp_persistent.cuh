@@ -53,11 +53,13 @@ __device__ __forceinline__ void begin_adaptive(LaneState& L, double requested, d
     L.attempt = 0;
 }
 
-// Step growth after an accepted attempt (rk4.hpp:130-142).
+// Step growth after an accepted attempt (rk4.hpp:130-142).  With
+// tol >= 64 err the factor 0.9 (tol/err)^0.2 is at least 2.07 and clamps to
+// 2, so pow is evaluated only below that ratio (same result).
 __device__ __forceinline__ double accepted_next_h(double h, double err, double tol, double min_step,
                                                   double max_step, double requested) {
     double factor = 2.0;
-    if (err > 0.0) {
+    if (err > 0.0 && !(tol >= 64.0 * err)) {
         factor = 0.9 * pow(tol / err, 0.2);
         factor = min_val(2.0, max_val(0.2, factor));
     }
