@@ -11,7 +11,7 @@
 
 // resident CTAs per SM the wavefront kernels are compiled for
 #ifndef KP_FAR_MIN_BLOCKS
-#define KP_FAR_MIN_BLOCKS 2
+#define KP_FAR_MIN_BLOCKS 3
 #endif
 #ifndef KP_NEAR_MIN_BLOCKS
 #define KP_NEAR_MIN_BLOCKS 1
