@@ -4,6 +4,9 @@ flags: the FP64 kernels are compiled with --fmad=false (reference rounding),
 the mixed-precision kernels with FMA contraction enabled.
 
     python -m kpolaris_b200.build [--force] [-j N]
+
+It also builds the command-line image tool kpolaris_b200/bin/kp_model_image
+(host C++, kpolaris_b200/host/) against that library.
 """
 from __future__ import annotations
 
@@ -21,6 +24,8 @@ CSRC = PKG / "csrc"
 INCLUDE = ROOT / "include"
 BUILD = PKG / "_build"
 LIB = PKG / "lib" / "libkpolaris_b200.so"
+HOST = PKG / "host"
+TOOL = PKG / "bin" / "kp_model_image"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=off",
@@ -96,7 +101,28 @@ def build(force: bool = False, jobs: int = 4, verbose: bool = False) -> Path:
         if res.returncode != 0:
             sys.stderr.write(res.stdout + res.stderr)
             raise RuntimeError("link failed")
+    build_tool(force=force, verbose=verbose)
     return LIB
+
+
+def build_tool(force: bool = False, verbose: bool = False) -> Path:
+    """The image tool: host C++ over the C ABI, found next to the library
+    through its run path."""
+    TOOL.parent.mkdir(parents=True, exist_ok=True)
+    src = HOST / "kp_model_image.cpp"
+    deps = [src, HOST / "kpolaris_image_options.hpp", INCLUDE / "kpolaris_b200.h", LIB]
+    if not force and not _stale(TOOL, deps):
+        return TOOL
+    cxx = shutil.which("g++") or "g++"
+    cmd = [cxx, "-std=c++17", "-O2", "-Wall", f"-I{INCLUDE}", f"-I{HOST}", str(src), f"-L{LIB.parent}",
+           "-lkpolaris_b200", "-Wl,-rpath,$ORIGIN/../lib", "-o", str(TOOL)]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        sys.stderr.write(res.stdout + res.stderr)
+        raise RuntimeError("kp_model_image build failed")
+    return TOOL
 
 
 def main(argv=None):

@@ -1,0 +1,252 @@
+// kp_model_image -- command-line image tool for the RIAF image path, the
+// counterpart of the reference's kpolaris_model_image for model=riaf
+// (tools/kpolaris_model_image.cpp:4908-4960 main, :3909-4260 run_model,
+// :2561-2800 output packing, :4136-4245 CSV output).
+//
+//   kp_model_image --parameter_file=run.par [--key=value ...]
+//
+// Reads the reference's parameter files and overrides
+// (kpolaris_image_options.hpp), traces the image through the C ABI
+// (kp_image_riaf, frequencies in chunks of at most KP_MAX_FREQUENCIES),
+// packs each frequency with kp_pack_image, writes the CSV image format and
+// <output>.params, and prints the tool's summary lines.  HDF5 output is not
+// built (format=hdf5, or output=*.h5 with format=auto, is an error).
+//
+// Extra keys: kp_precision=fp64|mixed, kp_schedule=auto|per_pixel|
+// persistent|graph (auto: per-pixel kernel for fp64, wavefront engine for
+// mixed), kp_device=N, kp_print_resolved=1 (print the resolved settings and
+// exit, no GPU), kp_dry_run=1 (resolve and write <output>.params, no GPU).
+#include <algorithm>
+#include <chrono>
+#include <cstdint>
+#include <cstdio>
+#include <fstream>
+#include <iostream>
+#include <limits>
+#include <string>
+#include <vector>
+
+#include "kpolaris_image_options.hpp"
+
+namespace {
+
+struct HostImage {
+    std::vector<double> i, q, u, v;
+    std::vector<double> diag[11];
+    std::vector<int32_t> pass_a_steps, steps, reason;
+
+    HostImage(int npix, int nfreq)
+        : i(size_t(npix) * nfreq), q(i.size()), u(i.size()), v(i.size()), pass_a_steps(npix), steps(npix),
+          reason(npix) {
+        for (auto& d : diag) d.assign(size_t(npix), 0.0);
+    }
+    kp_image_out view(int npix, int nfreq) {
+        kp_image_out o;
+        o.npix = npix;
+        o.nfreq = nfreq;
+        o.image_i = i.data();
+        o.image_q = q.data();
+        o.image_u = u.data();
+        o.image_v = v.data();
+        double** d[11] = {&o.closure_x, &o.closure_k, &o.final_null, &o.frame_error, &o.det_r, &o.overlap_r11,
+                          &o.overlap_r12, &o.overlap_r21, &o.overlap_r22, &o.basis_identity_error,
+                          &o.basis_rotation_angle};
+        for (int k = 0; k < 11; ++k) *d[k] = diag[k].data();
+        o.pass_a_steps = pass_a_steps.data();
+        o.steps = steps.data();
+        o.reason = reason.data();
+        return o;
+    }
+};
+
+struct PackedFrequency {
+    double frequency = 0.0;
+    std::vector<double> inv[4], nu[4];
+    std::vector<int32_t> total_steps;
+    kp_packed_image p{};
+};
+
+void check(int rc, const char* what) {
+    if (rc != KP_OK) throw std::runtime_error(std::string(what) + ": " + kp_last_error());
+}
+
+double seconds_since(std::chrono::steady_clock::time_point t0) {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+void report_timing(const kpb::ImageOptions& o, const char* name, double s) {
+    if (o.timing) std::cout << "timing " << name << " " << s << " s\n";
+}
+
+int run(const std::vector<std::string>& args) {
+    const auto t_start = std::chrono::steady_clock::now();
+    kpb::ImageOptions opt = kpb::parse_options(args);
+    kpb::finalize_options(opt);
+    if (opt.kp_print_resolved) {
+        kpb::print_resolved(std::cout, opt);
+        return 0;
+    }
+    const std::vector<double> freqs = kpb::build_frequency_grid(opt);
+    const kp_pass_a_params pass_a = kpb::to_pass_a(opt);
+    const bool hdf5 = opt.output_format == "hdf5" ||
+                      (opt.output_format == "auto" && opt.output.size() >= 3 &&
+                       opt.output.compare(opt.output.size() - 3, 3, ".h5") == 0);
+    if (opt.output_format != "auto" && opt.output_format != "hdf5" && opt.output_format != "csv")
+        throw std::runtime_error("unknown output format: " + opt.output_format);
+    if (hdf5)
+        throw std::runtime_error("HDF5 image output is not built in this library: use format=csv "
+                                 "(or an output path not ending in .h5)");
+    const std::string params_path = kpb::effective_parameter_path(opt);
+    kpb::write_effective_parameters(params_path, opt, pass_a, freqs);
+    if (opt.kp_dry_run) {
+        std::cout << "parameters " << params_path << "\n";
+        return 0;
+    }
+
+    kp_run_options ro;
+    kp_default_run_options(&ro);
+    ro.device = opt.kp_device;
+    ro.timing = opt.timing;
+    ro.precision = opt.kp_precision == "mixed" ? KP_PRECISION_MIXED : KP_PRECISION_FP64;
+    if (opt.kp_schedule == "per_pixel") ro.schedule = KP_SCHEDULE_PER_PIXEL;
+    else if (opt.kp_schedule == "persistent") ro.schedule = KP_SCHEDULE_PERSISTENT;
+    else if (opt.kp_schedule == "graph") ro.schedule = KP_SCHEDULE_GRAPH;
+    else ro.schedule = ro.precision == KP_PRECISION_MIXED ? KP_SCHEDULE_PERSISTENT : KP_SCHEDULE_PER_PIXEL;
+
+    const int npix = opt.nx * opt.ny;
+    const int chunk = kpb::effective_chunk_size(opt, freqs.size());
+    const kpb::FluxScale fs = kpb::flux_scale_of(opt);
+    const double jy = fs.valid ? fs.jy_per_pixel : -1.0;
+    std::vector<PackedFrequency> packed(freqs.size());
+    HostImage first_chunk(npix, 1);
+    const auto t_transport = std::chrono::steady_clock::now();
+    for (size_t c0 = 0; c0 < freqs.size(); c0 += size_t(chunk)) {
+        const int nf = int(std::min(freqs.size() - c0, size_t(chunk)));
+        HostImage img(npix, nf);
+        kp_image_out out = img.view(npix, nf);
+        const kp_riaf_model model = kpb::to_riaf_model(opt, freqs[c0]);
+        check(kp_image_riaf(&pass_a, &model, opt.radiation_substeps, freqs.data() + c0, nf, &ro, &out),
+              "kp_image_riaf");
+        for (int f = 0; f < nf; ++f) {
+            PackedFrequency& pf = packed[c0 + size_t(f)];
+            pf.frequency = freqs[c0 + size_t(f)];
+            for (int k = 0; k < 4; ++k) {
+                pf.inv[k].assign(size_t(npix), 0.0);
+                pf.nu[k].assign(size_t(npix), 0.0);
+            }
+            pf.total_steps.assign(size_t(npix), 0);
+            pf.p.i_inv = pf.inv[0].data();
+            pf.p.q_inv = pf.inv[1].data();
+            pf.p.u_inv = pf.inv[2].data();
+            pf.p.v_inv = pf.inv[3].data();
+            pf.p.i_nu = pf.nu[0].data();
+            pf.p.q_nu = pf.nu[1].data();
+            pf.p.u_nu = pf.nu[2].data();
+            pf.p.v_nu = pf.nu[3].data();
+            pf.p.total_steps = pf.total_steps.data();
+            check(kp_pack_image(&out, f, pf.frequency, opt.evpa_0 == "N", jy, &pf.p), "kp_pack_image");
+        }
+        if (c0 == 0) {
+            // one geodesic per pixel: the diagnostics of every chunk match
+            for (int k = 0; k < 11; ++k) first_chunk.diag[k].swap(img.diag[k]);
+            first_chunk.pass_a_steps.swap(img.pass_a_steps);
+            first_chunk.steps.swap(img.steps);
+            first_chunk.reason.swap(img.reason);
+        }
+    }
+    report_timing(opt, "image_transport", seconds_since(t_transport));
+
+    const auto t_output = std::chrono::steady_clock::now();
+    const bool multi = freqs.size() > 1;
+    {
+        std::ofstream out(opt.output);
+        if (!out) throw std::runtime_error("failed to open output: " + opt.output);
+        out.precision(17);
+        out << "# code,KPolaris-B200\n# code_abi_version," << kp_abi_version() << "\n";
+        out << "# model," << opt.model << "\n# parameter_file," << opt.parameter_file << "\n";
+        out << "# effective_parameter_file," << params_path << "\n";
+        out << "# nx," << opt.nx << "\n# ny," << opt.ny << "\n# camera," << opt.camera << "\n";
+        out << "# coordinate," << opt.coordinate << "\n# metric," << kpb::metric_name_of(opt.coordinate) << "\n";
+        out << "# stokes_convention,camera_frame\n# polarization_basis,camera_screen\n";
+        out << "# inner_radius," << opt.inner_radius << "\n# outer_radius," << opt.outer_radius << "\n";
+        const kp_riaf_model m = kpb::to_riaf_model(opt, freqs.front());
+        out << "# riaf_r_min," << m.r_min << "\n# riaf_r_max," << m.r_max << "\n# riaf_nth0," << m.nth0
+            << "\n# riaf_Te0," << m.Te0 << "\n# riaf_disk_h," << m.disk_h << "\n# riaf_pow_nth," << m.pow_nth
+            << "\n# riaf_pow_T," << m.pow_T << "\n# riaf_ne_unit," << m.ne_unit << "\n# riaf_te_unit," << m.te_unit
+            << "\n# riaf_mbh_solar," << m.mbh_solar << "\n# riaf_keplerian_factor," << m.keplerian_factor
+            << "\n# riaf_infall_factor," << m.infall_factor << "\n# emission_type," << m.emission_type
+            << "\n# emission_fit," << kpb::emission_fit_name(m.emission_type) << "\n";
+        // riaf.hpp:76-85: length unit over the frequency
+        const double l_unit = 6.67430e-8 * m.mbh_solar * 1.98847e33 / (2.99792458e10 * 2.99792458e10);
+        out << "# dlambda_scale," << l_unit / std::max(m.freq_cgs, 1.0) << "\n";
+        if (multi) out << "freq_index,frequency_hz,";
+        out << "ix,iy,I_inv,Q_inv,U_inv,V_inv,I_nu,Q_nu,U_nu,V_nu,reason,pass_a_steps,pass_b_steps,total_steps,"
+               "closure_x,closure_k,final_null,frame_error,det_r,overlap_r11,overlap_r12,overlap_r21,overlap_r22,"
+               "basis_identity_error,basis_rotation_angle\n";
+        for (size_t fi = 0; fi < packed.size(); ++fi) {
+            const PackedFrequency& pf = packed[fi];
+            for (int p = 0; p < npix; ++p) {
+                if (multi) out << fi << ',' << pf.frequency << ',';
+                out << p % opt.nx << ',' << p / opt.nx;
+                for (int k = 0; k < 4; ++k) out << ',' << pf.inv[k][size_t(p)];
+                for (int k = 0; k < 4; ++k) out << ',' << pf.nu[k][size_t(p)];
+                out << ',' << first_chunk.reason[size_t(p)] << ',' << first_chunk.pass_a_steps[size_t(p)] << ','
+                    << first_chunk.steps[size_t(p)] << ',' << pf.total_steps[size_t(p)];
+                for (int k = 0; k < 11; ++k) out << ',' << first_chunk.diag[k][size_t(p)];
+                out << '\n';
+            }
+        }
+        if (!out) throw std::runtime_error("failed writing output: " + opt.output);
+    }
+    report_timing(opt, "image_output", seconds_since(t_output));
+    report_timing(opt, "image_run_model_total", seconds_since(t_start));
+
+    std::cout.precision(17);
+    std::cout << "KPolaris-B200 model image output\nmodel " << opt.model << "\nformat csv\n";
+    std::cout << "output " << opt.output << "\n";
+    if (!params_path.empty()) std::cout << "parameters " << params_path << "\n";
+    std::cout << "pixels " << npix << "\nfrequencies " << freqs.size() << "\n";
+    std::cout << "intensity_to_flux_jy_per_pixel "
+              << (fs.valid ? fs.jy_per_pixel : std::numeric_limits<double>::quiet_NaN()) << "\n";
+    long long sa = 0, sb = 0;
+    int ma = 0, mb = 0, mt = 0;
+    for (int p = 0; p < npix; ++p) {
+        sa += first_chunk.pass_a_steps[size_t(p)];
+        sb += first_chunk.steps[size_t(p)];
+        ma = std::max(ma, int(first_chunk.pass_a_steps[size_t(p)]));
+        mb = std::max(mb, int(first_chunk.steps[size_t(p)]));
+        mt = std::max(mt, int(first_chunk.pass_a_steps[size_t(p)] + first_chunk.steps[size_t(p)]));
+    }
+    for (size_t fi = 0; fi < packed.size(); ++fi) {
+        const PackedFrequency& pf = packed[fi];
+        std::cout << "freq_index " << fi << "\nfrequency_hz " << pf.frequency << "\nreturned " << pf.p.returned << "\n";
+        std::cout << "mean_pass_a_steps " << double(sa) / npix << "\nmean_pass_b_steps " << double(sb) / npix
+                  << "\nmean_total_steps " << double(sa + sb) / npix << "\n";
+        std::cout << "max_pass_a_steps " << ma << "\nmax_pass_b_steps " << mb << "\nmax_total_steps " << mt << "\n";
+        const char* names[4] = {"I", "Q", "U", "V"};
+        for (int k = 0; k < 4; ++k) std::cout << names[k] << "_inv " << pf.p.sum_inv[k] << "\n";
+        for (int k = 0; k < 4; ++k) std::cout << "flux_" << names[k] << "_Jy " << pf.p.flux_jy[k] << "\n";
+    }
+    return 0;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+    std::vector<std::string> args;
+    for (int i = 1; i < argc; ++i) {
+        const std::string a(argv[i]);
+        if (a == "--help" || a == "-h") {
+            std::cout << "usage: kp_model_image --parameter_file=FILE.par [--key=value ...]\n"
+                         "RIAF images through the KPolaris-B200 C ABI; CSV output and <output>.params.\n";
+            return 0;
+        }
+        args.push_back(a);
+    }
+    try {
+        return run(args);
+    } catch (const std::exception& e) {
+        std::cerr << "error: " << e.what() << "\n";
+        return 1;
+    }
+}

@@ -109,6 +109,10 @@ private:
     std::size_t n_ = 0;
 };
 
+// Runtime lifetime: the host shim has nothing to start or stop.
+inline bool is_initialized() { return true; }
+inline void finalize() {}
+
 // Host views already live in host memory: the mirror is the view itself.
 template<class Space, class V>
 inline V create_mirror_view_and_copy(const Space&, const V& v) {

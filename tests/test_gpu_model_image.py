@@ -1,0 +1,135 @@
+"""kp_model_image end to end on the GPU: a parameter file in, the CSV image
+format out (tools/kpolaris_model_image.cpp:4136-4245, rows as written by
+pack_transport_frequency_image, :2561-2800).  The tool's numbers must be the
+library's own: every CSV value (printed at 17 digits, so exact) equals the
+same image traced through the Python API and packed with kp_pack_image,
+including a five-frequency run split into chunks of KP_MAX_FREQUENCIES; the
+summary's fluxes equal the packed sums times the flux scale; and the FP64
+steps and reasons equal the oracle's.
+"""
+from __future__ import annotations
+
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import kpolaris_b200 as kp
+import oracle
+from kpolaris_b200 import configs
+
+ROOT = Path(__file__).resolve().parents[1]
+TOOL = ROOT / "kpolaris_b200" / "bin" / "kp_model_image"
+
+FREQS = [86.0e9, 230.0e9, 345.0e9, 690.0e9, 1.0e12]
+
+PAR = """
+# config-2 controls on a small image, five frequencies
+model=riaf
+coordinate=cartesian_ks
+camera=pinhole
+nx=16
+ny=12
+radius=1000
+inclination_deg=17
+xspan=80
+spin=0.9375
+freq_list=86e9,230e9,345e9,690e9,1e12
+adaptive=1
+adaptive_tolerance=1e-8
+step=0.025
+min_step=1e-10
+max_step=2
+max_steps=400000
+max_radiation_step=2
+max_radiation_depth=1
+max_absorption_depth=1
+max_faraday_depth=4
+riaf_mbh_solar=6.5e9
+riaf_ne_unit=4e6
+riaf_te_unit=1.5e11
+riaf_disk_h=0.3
+riaf_pow_nth=-1.1
+riaf_pow_T=-0.84
+riaf_r_min=1
+riaf_r_max=100
+dsource=16.8e6
+emission_fit=symphony
+evpa_0=N
+format=csv
+"""
+
+
+def _read_csv(path):
+    rows = [line for line in Path(path).read_text().splitlines() if not line.startswith("#")]
+    header = rows[0].split(",")
+    data = np.array([[float(x) for x in r.split(",")] for r in rows[1:]])
+    return header, data
+
+
+@pytest.mark.gpu
+def test_tool_csv_equals_library(tmp_path):
+    assert TOOL.exists(), "kp_model_image not built"
+    par = tmp_path / "run.par"
+    par.write_text(PAR)
+    out = tmp_path / "img.csv"
+    r = subprocess.run([str(TOOL), f"--parameter_file={par}", f"--output={out}"], capture_output=True, text=True,
+                       timeout=600)
+    assert r.returncode == 0, r.stderr
+    header, data = _read_csv(out)
+    assert header[:4] == ["freq_index", "frequency_hz", "ix", "iy"]
+    col = {h: i for i, h in enumerate(header)}
+
+    params = configs.riaf_params(16, 12, step=0.025, adaptive=1, max_steps=400000, adaptive_tolerance=1e-8,
+                                 min_step=1e-10, max_step=2.0, max_radiation_step=2.0, max_radiation_depth=1.0,
+                                 max_absorption_depth=1.0, max_faraday_depth=4.0)
+    jy = configs.flux_scale_jy_per_pixel(params, 6.5e9, 16.8e6)
+    npix = 16 * 12
+    summary = r.stdout.split("\n")
+    fluxes = [float(line.split()[1]) for line in summary if line.startswith("flux_I_Jy ")]
+    assert len(fluxes) == len(FREQS)
+    chunks = [FREQS[:4], FREQS[4:]]
+    fi = 0
+    for chunk in chunks:
+        res = kp.image_riaf(params, configs.riaf_model(freq=chunk[0]), chunk)
+        for f, freq in enumerate(chunk):
+            pk = kp.pack_image(res, f, freq, evpa_0="N", flux_scale=jy)
+            rows = data[data[:, col["freq_index"]] == fi]
+            assert rows.shape[0] == npix
+            assert np.all(rows[:, col["frequency_hz"]] == freq)
+            assert np.array_equal(rows[:, col["ix"]], np.arange(npix) % 16)
+            assert np.array_equal(rows[:, col["iy"]], np.arange(npix) // 16)
+            for name, key in (("I_inv", "i_inv"), ("Q_inv", "q_inv"), ("U_inv", "u_inv"), ("V_inv", "v_inv"),
+                              ("I_nu", "i_nu"), ("Q_nu", "q_nu"), ("U_nu", "u_nu"), ("V_nu", "v_nu")):
+                assert np.array_equal(rows[:, col[name]], pk[key]), (fi, name)
+            assert np.array_equal(rows[:, col["total_steps"]], pk["total_steps"])
+            assert fluxes[fi] == pk["flux_jy"][0] or (np.isnan(fluxes[fi]) and np.isnan(pk["flux_jy"][0]))
+            fi += 1
+    # one geodesic per pixel: the first chunk's steps and reasons, against the oracle
+    first = kp.image_riaf(params, configs.riaf_model(freq=FREQS[0]), FREQS[:4])
+    ref = oracle.image_riaf(params, configs.riaf_model(freq=FREQS[0]), FREQS[:4], kind="port", threads=0)
+    rows = data[data[:, col["freq_index"]] == 0]
+    assert np.array_equal(rows[:, col["reason"]], first.reason)
+    assert np.array_equal(rows[:, col["reason"]], ref.reason)
+    assert np.array_equal(rows[:, col["pass_a_steps"]], ref.pass_a_steps)
+    assert np.array_equal(rows[:, col["pass_b_steps"]], ref.steps)
+    params_file = Path(str(out) + ".params")
+    assert params_file.exists() and "derived_freq_list=86000000000,230000000000" in params_file.read_text()
+
+
+@pytest.mark.gpu
+def test_tool_mixed_precision_within_budget(tmp_path):
+    """kp_precision=mixed runs the wavefront engine: total flux within 1e-4 of the FP64 run."""
+    assert TOOL.exists(), "kp_model_image not built"
+    par = tmp_path / "run.par"
+    par.write_text(PAR.replace("freq_list=86e9,230e9,345e9,690e9,1e12", "freq_list=86e9,230e9,345e9,690e9"))
+    fluxes = {}
+    for prec in ("fp64", "mixed"):
+        out = tmp_path / f"img_{prec}.csv"
+        r = subprocess.run([str(TOOL), f"--parameter_file={par}", f"--output={out}", f"--kp_precision={prec}"],
+                           capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr
+        fluxes[prec] = [float(line.split()[1]) for line in r.stdout.splitlines() if line.startswith("flux_I_Jy ")]
+    for a, b in zip(fluxes["fp64"], fluxes["mixed"]):
+        assert abs(b / a - 1.0) <= 1e-4, (a, b)
