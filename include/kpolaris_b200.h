@@ -526,12 +526,16 @@ double kp_flux_scale_jy_per_pixel(double mbh_solar, double dsource_pc, double im
  * workload (e.g. its images at reduced resolution), with the precision of
  * `options`, and stores the fastest in the device's tuning table: later
  * persistent and graph launches of that precision with blocks_per_sm == 0
- * use it.  The sample's outputs are written like kp_batch_riaf's.  Schedule
- * choices never change results (rays resume bit-exactly from their records).
+ * use it.  A candidate is adopted only when it beats the default eager
+ * schedule (KP_SCHEDULE_PERSISTENT, occupancy-derived CTAs) by at least 2%
+ * on the sample; otherwise the table keeps the defaults, blocks_per_sm and
+ * graph_cycles come back 0, and the caller should keep the eager schedule.
+ * The sample's outputs are written like kp_batch_riaf's.  Schedule choices
+ * never change results (rays resume bit-exactly from their records).
  */
 typedef struct kp_tuning {
     int blocks_per_sm[3];     /* far, near-A, near-B */
-    int graph_cycles;         /* (far, near-A, near-B) cycles per graph launch */
+    int graph_cycles;         /* (far, near-A, near-B) cycles per graph launch; 0: keep the eager schedule */
     double seconds;           /* device time of the sample with the chosen schedule */
     double default_seconds;   /* device time of the sample with the default schedule */
     int candidates;           /* schedules timed */

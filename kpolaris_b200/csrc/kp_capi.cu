@@ -1131,6 +1131,15 @@ int kp_autotune_batch(const kp_riaf_job* jobs, int njobs, const kp_run_options* 
                         for (int p = 0; p < kPhases; ++p) best[p] = cand[p];
                     }
                 }
+    // A candidate replaces the default only by a margin above the sample's
+    // run-to-run noise (about 1%): a small sample favours whatever shortens
+    // its own tail, which the full workload need not share.
+    constexpr double kAdoptMargin = 0.02;
+    if (!(t_best < t_default * (1.0 - kAdoptMargin))) {
+        for (int p = 0; p < kPhases; ++p) best[p] = 0;
+        best_cycles = 0;
+        t_best = t_default;
+    }
     set_table(best, best_cycles);
     for (int p = 0; p < kPhases; ++p) out->blocks_per_sm[p] = best[p];
     out->graph_cycles = best_cycles;

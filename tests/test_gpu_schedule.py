@@ -4,8 +4,9 @@ Bars: a batch traced with KP_SCHEDULE_GRAPH is bit-identical, in every output
 array, to the same batch on the eager persistent schedule (FP64 and mixed,
 uneven image sizes, 1-4 frequencies), also when the graph is replayed from
 the cache and when rays outlive the captured cycles; GRMHD images likewise.
-kp_autotune_batch picks a schedule within the occupancy limits, reports the
-timings it compared, and leaves results bit-identical.
+kp_autotune_batch picks a schedule within the occupancy limits (or keeps the
+defaults when no candidate beats them by its 2% margin), reports the timings
+it compared, and leaves results bit-identical.
 """
 from __future__ import annotations
 
@@ -72,9 +73,14 @@ def test_autotuner_picks_a_valid_schedule_and_keeps_results(uneven):
     before = kp.batch_riaf(uneven, precision=_abi.PRECISION_MIXED)
     t = kp.autotune_batch(configs.config4_jobs(count=8, seed=11, scale=16), precision=_abi.PRECISION_MIXED)
     assert t.candidates >= 4
-    assert 1 <= t.blocks_per_sm[0] <= 4 and 1 <= t.blocks_per_sm[1] <= 4 and 1 <= t.blocks_per_sm[2] <= 4
-    assert t.graph_cycles in (2, 3, 4, 6)
     assert 0.0 < t.seconds and 0.0 < t.default_seconds
+    if t.graph_cycles == 0:
+        # no candidate beat the default by the adoption margin: defaults kept
+        assert list(t.blocks_per_sm) == [0, 0, 0] and t.seconds == t.default_seconds
+    else:
+        assert 1 <= t.blocks_per_sm[0] <= 4 and 1 <= t.blocks_per_sm[1] <= 4 and 1 <= t.blocks_per_sm[2] <= 4
+        assert t.graph_cycles in (2, 3, 4, 6)
+        assert t.seconds < 0.98 * t.default_seconds
     after = kp.batch_riaf(uneven, precision=_abi.PRECISION_MIXED, schedule=_abi.SCHEDULE_GRAPH)
     for i, (a, b) in enumerate(zip(before, after)):
         same(a, b, ("tuned", i))
