@@ -256,7 +256,7 @@ int kp_abi_version(void);
 /* sizeof of the ABI structs, for the bindings' layout check:
  * 0 kp_camera_params, 1 kp_emission_selection, 2 kp_pass_a_params,
  * 3 kp_riaf_model, 4 kp_image_out, 5 kp_run_options, 7 kp_riaf_job,
- * 8 kp_batch_stats; 6 is the bytes of the per-image job descriptor an
+ * 8 kp_batch_stats, 12 kp_analysis_config, 13 kp_analysis_out; 6 is the bytes of the per-image job descriptor an
  * image uploads to the device; 0 for other ids. */
 size_t kp_abi_sizeof(int which);
 
@@ -285,6 +285,97 @@ int kp_image_riaf(const kp_pass_a_params* params,
                   int nfreq,
                   const kp_run_options* options,
                   kp_image_out* out);
+
+/*
+ * Analysis mode (the reference's analysis_mode=1 image path,
+ * src/image/analysis_driver.hpp): the FP64 per-pixel image with
+ * line-of-sight diagnostics accumulated along pass B.  Single frequency;
+ * the source-partition response channels (analysis_response) are not built.
+ * kp_analysis_config mirrors AnalysisConfig (:16-23).
+ */
+#define KP_MAX_ANALYSIS_RADIAL_BINS 24
+
+typedef struct kp_analysis_config {
+    int radial_bins;            /* 1..KP_MAX_ANALYSIS_RADIAL_BINS (16) */
+    double radial_min;          /* inner edge of the logarithmic bins (2 M) */
+    double radial_max;          /* outer edge (100 M) */
+    double formation_fraction;  /* central fraction of the formation quantiles, in (0, 1) (0.9) */
+} kp_analysis_config;
+
+void kp_default_analysis_config(kp_analysis_config* cfg);
+
+/* Per-pixel analysis arrays, the analysis fields of ImageHostData
+ * (src/image/result.hpp:35-92): scalars hold npix values; the radial_*
+ * arrays hold radial_bins * npix values, bin-major.  Host or device memory
+ * as kp_run_options::outputs_on_device says; none may be NULL. */
+typedef struct kp_analysis_out {
+    double* radiating_path_length;
+    double* emission_weight;
+    double* emission_weighted_radius;
+    double* emission_weighted_optical_depth_to_camera;
+    double* absorption_depth;
+    double* absorption_operator_depth;
+    double* faraday_rotation_depth;
+    double* faraday_conversion_depth;
+    double* faraday_operator_depth;
+    double* dominant_emission_radius;
+    int32_t* dominant_emission_region;
+    double* dominant_ne_cgs;
+    double* dominant_thetae;
+    double* dominant_b_cgs;
+    double* dominant_beta;
+    double* dominant_sigma;
+    double* emission_weighted_ne_cgs;
+    double* emission_weighted_thetae;
+    double* emission_weighted_b_cgs;
+    double* emission_weighted_beta;
+    double* emission_weighted_sigma;
+    double* photon_ring_winding_estimate;
+    int32_t* radiation_substeps;
+    double* radial_stokes_i_contribution;
+    double* radial_stokes_q_contribution;
+    double* radial_stokes_u_contribution;
+    double* radial_stokes_v_contribution;
+    double* radial_absorption_depth;
+    double* radial_faraday_rotation_depth;
+    double* radial_faraday_conversion_depth;
+    double* radial_faraday_operator_depth;
+    double* observer_weighted_radius_i;
+    double* observer_weighted_radius_linear;
+    double* observer_weighted_radius_circular;
+    double* intensity_formation_radius_low;
+    double* intensity_formation_radius_median;
+    double* intensity_formation_radius_high;
+    double* linear_formation_radius_low;
+    double* linear_formation_radius_median;
+    double* linear_formation_radius_high;
+    double* circular_formation_radius_low;
+    double* circular_formation_radius_median;
+    double* circular_formation_radius_high;
+    double* los_linear_coherence;
+    double* los_circular_coherence;
+    double* contribution_closure_max_abs;
+    double* contribution_closure_relative_l1;
+    double* foreground_absorption_depth;
+    double* foreground_faraday_rotation_depth;
+    double* foreground_faraday_conversion_depth;
+    double* foreground_faraday_operator_depth;
+    double* foreground_faraday_operator_fraction;
+} kp_analysis_out;
+
+/*
+ * One analysis-mode RIAF image at model->freq_cgs.  Replaces the per-pixel
+ * body of the reference's analysis image driver
+ * (trace_pass_b_segment_model_analysis_pixel_metric,
+ * src/image/analysis_driver.hpp:623-636, called per pixel by its analysis
+ * image kernels).  `out` takes the image and diagnostics (nfreq = 1) as for
+ * kp_image_riaf; `analysis` the arrays above.  FP64 only
+ * (options->precision must be KP_PRECISION_FP64; the schedule is ignored:
+ * one thread per pixel), step-doubling RK4 only, min_step > 0.
+ */
+int kp_image_riaf_analysis(const kp_pass_a_params* params, const kp_riaf_model* model, int radiation_substeps,
+                           const kp_analysis_config* config, const kp_run_options* options, kp_image_out* out,
+                           kp_analysis_out* analysis);
 
 /* One image of a batch: the arguments of one kp_image_riaf call. */
 typedef struct kp_riaf_job {

@@ -81,6 +81,10 @@ def library() -> C.CDLL:
     L.kp_flux_scale_jy_per_pixel.argtypes = [C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int]
     L.kp_autotune_batch.argtypes = [C.POINTER(_abi.RiafJob), C.c_int, C.POINTER(RunOptions),
                                     C.POINTER(_abi.Tuning)]
+    L.kp_default_analysis_config.argtypes = [C.POINTER(_abi.AnalysisConfig)]
+    L.kp_image_riaf_analysis.argtypes = [C.POINTER(PassAParams), C.POINTER(RIAFModel), C.c_int,
+                                         C.POINTER(_abi.AnalysisConfig), C.POINTER(RunOptions),
+                                         C.POINTER(_abi.ImageOut), C.POINTER(_abi.AnalysisOut)]
     L.kp_server_create.argtypes = [C.POINTER(_abi.ServerConfig), C.POINTER(C.c_void_p)]
     L.kp_server_submit.argtypes = [C.c_void_p, C.POINTER(_abi.RiafJob), C.POINTER(C.c_ulonglong)]
     L.kp_server_submit_grmhd.argtypes = [C.c_void_p, C.POINTER(_abi.GrmhdJob), C.POINTER(C.c_ulonglong)]
@@ -182,6 +186,24 @@ def _job_array(jobs, outs=None):
         j.radiation_substeps = 1
         j.out = res.as_struct()
     return arr, len(jobs), results
+
+
+def image_riaf_analysis(params: PassAParams, model: RIAFModel, config: _abi.AnalysisConfig | None = None, *,
+                        radiation_substeps=1, **options):
+    """kp_image_riaf_analysis: one single-frequency FP64 RIAF image (at
+    model.freq_cgs) with the analysis-mode line-of-sight diagnostics.
+    Returns (ImageHostData, AnalysisHostData)."""
+    L = library()
+    if config is None:
+        config = _abi.default_analysis_config()
+    npix = params.camera.nx * params.camera.ny
+    out = ImageHostData.allocate(npix, 1)
+    an = _abi.AnalysisHostData.allocate(npix, int(config.radial_bins))
+    s, a = out.as_struct(), an.as_struct()
+    opt = _options(**options)
+    check(L.kp_image_riaf_analysis(C.byref(params), C.byref(model), int(radiation_substeps), C.byref(config),
+                                   C.byref(opt), C.byref(s), C.byref(a)))
+    return out, an
 
 
 def flux_scale_jy_per_pixel(mbh_solar: float, dsource_pc: float, image_width_x: float, image_width_y: float,

@@ -280,6 +280,79 @@ class ImageHostData:
         return out
 
 
+MAX_ANALYSIS_RADIAL_BINS = 24
+
+
+class AnalysisConfig(C.Structure):
+    """kp_analysis_config (AnalysisConfig, src/image/analysis_driver.hpp:16-23)."""
+    _fields_ = [("radial_bins", C.c_int), ("radial_min", C.c_double), ("radial_max", C.c_double),
+                ("formation_fraction", C.c_double)]
+
+
+def default_analysis_config(radial_bins: int = 16, radial_min: float = 2.0, radial_max: float = 100.0,
+                            formation_fraction: float = 0.9) -> AnalysisConfig:
+    return AnalysisConfig(int(radial_bins), float(radial_min), float(radial_max), float(formation_fraction))
+
+
+# kp_analysis_out, in order: per-pixel scalars, then the bin-major radial
+# arrays, then the observer-weighted results (src/image/result.hpp:35-92)
+ANALYSIS_SCALARS_A = ["radiating_path_length", "emission_weight", "emission_weighted_radius",
+                      "emission_weighted_optical_depth_to_camera", "absorption_depth", "absorption_operator_depth",
+                      "faraday_rotation_depth", "faraday_conversion_depth", "faraday_operator_depth",
+                      "dominant_emission_radius", "dominant_emission_region", "dominant_ne_cgs", "dominant_thetae",
+                      "dominant_b_cgs", "dominant_beta", "dominant_sigma", "emission_weighted_ne_cgs",
+                      "emission_weighted_thetae", "emission_weighted_b_cgs", "emission_weighted_beta",
+                      "emission_weighted_sigma", "photon_ring_winding_estimate", "radiation_substeps"]
+ANALYSIS_RADIAL = ["radial_stokes_i_contribution", "radial_stokes_q_contribution", "radial_stokes_u_contribution",
+                   "radial_stokes_v_contribution", "radial_absorption_depth", "radial_faraday_rotation_depth",
+                   "radial_faraday_conversion_depth", "radial_faraday_operator_depth"]
+ANALYSIS_SCALARS_B = ["observer_weighted_radius_i", "observer_weighted_radius_linear",
+                      "observer_weighted_radius_circular", "intensity_formation_radius_low",
+                      "intensity_formation_radius_median", "intensity_formation_radius_high",
+                      "linear_formation_radius_low", "linear_formation_radius_median", "linear_formation_radius_high",
+                      "circular_formation_radius_low", "circular_formation_radius_median",
+                      "circular_formation_radius_high", "los_linear_coherence", "los_circular_coherence",
+                      "contribution_closure_max_abs", "contribution_closure_relative_l1",
+                      "foreground_absorption_depth", "foreground_faraday_rotation_depth",
+                      "foreground_faraday_conversion_depth", "foreground_faraday_operator_depth",
+                      "foreground_faraday_operator_fraction"]
+ANALYSIS_FIELDS = ANALYSIS_SCALARS_A + ANALYSIS_RADIAL + ANALYSIS_SCALARS_B
+ANALYSIS_INT_FIELDS = ("dominant_emission_region", "radiation_substeps")
+
+
+class AnalysisOut(C.Structure):
+    _fields_ = [(n, _IP if n in ANALYSIS_INT_FIELDS else _DP) for n in ANALYSIS_FIELDS]
+
+
+@dataclass
+class AnalysisHostData:
+    """Host analysis arrays of one image: scalars [npix], radial_* [bins, npix]."""
+
+    npix: int
+    radial_bins: int
+    arrays: dict = field(default_factory=dict)
+
+    def __getattr__(self, name):
+        arrays = self.__dict__.get("arrays")
+        if arrays is not None and name in arrays:
+            return arrays[name]
+        raise AttributeError(name)
+
+    @classmethod
+    def allocate(cls, npix: int, radial_bins: int) -> "AnalysisHostData":
+        arrays = {}
+        for name in ANALYSIS_FIELDS:
+            shape = (radial_bins, npix) if name in ANALYSIS_RADIAL else (npix,)
+            arrays[name] = np.zeros(shape, dtype=np.int32 if name in ANALYSIS_INT_FIELDS else np.float64)
+        return cls(npix=npix, radial_bins=radial_bins, arrays=arrays)
+
+    def as_struct(self) -> AnalysisOut:
+        out = AnalysisOut()
+        for name in ANALYSIS_FIELDS:
+            setattr(out, name, self.arrays[name].ctypes.data_as(_IP if name in ANALYSIS_INT_FIELDS else _DP))
+        return out
+
+
 def default_camera() -> CameraParams:
     """CameraParams<double> defaults (src/camera/camera.hpp:12-25)."""
     c = CameraParams()

@@ -744,6 +744,8 @@ size_t kp_abi_sizeof(int which) {
     case 9: return sizeof(kp_tuning);
     case 10: return sizeof(kp_grmhd_model);
     case 11: return sizeof(kp_grmhd_job);
+    case 12: return sizeof(kp_analysis_config);
+    case 13: return sizeof(kp_analysis_out);
     default: return 0;
     }
 }
@@ -894,6 +896,114 @@ int kp_image_riaf(const kp_pass_a_params* params, const kp_riaf_model* model, in
         if (e != cudaSuccess) return cuda_error(e, "image kernel");
     }
     return KP_OK;
+}
+
+void kp_default_analysis_config(kp_analysis_config* cfg) {
+    if (!cfg) return;
+    cfg->radial_bins = 16;  // AnalysisConfig defaults (analysis_driver.hpp:16-23)
+    cfg->radial_min = 2.0;
+    cfg->radial_max = 100.0;
+    cfg->formation_fraction = 0.9;
+}
+
+int kp_image_riaf_analysis(const kp_pass_a_params* params, const kp_riaf_model* model, int radiation_substeps,
+                           const kp_analysis_config* config, const kp_run_options* options, kp_image_out* out,
+                           kp_analysis_out* analysis) {
+    (void)radiation_substeps;
+    kp_run_options opt;
+    if (options) {
+        opt = *options;
+    } else {
+        kp_default_run_options(&opt);
+    }
+    int st = validate_riaf(params, model, nullptr, 1);
+    if (st != KP_OK) return st;
+    if (!config || !analysis) return set_error(KP_ERR_INVALID, "null analysis config or outputs");
+    // validate_options (tools/kpolaris_model_image_options.cpp:265-284)
+    if (config->radial_bins < 1 || config->radial_bins > KP_MAX_ANALYSIS_RADIAL_BINS)
+        return set_error(KP_ERR_INVALID, "analysis radial_bins must lie in [1, %d]", KP_MAX_ANALYSIS_RADIAL_BINS);
+    if ((config->radial_min > 0.0 && !std::isfinite(config->radial_min)) ||
+        (config->radial_max > 0.0 && !std::isfinite(config->radial_max)))
+        return set_error(KP_ERR_INVALID, "analysis radial bounds must be finite when specified");
+    if (config->radial_min > 0.0 && config->radial_max > 0.0 && !(config->radial_max > config->radial_min))
+        return set_error(KP_ERR_INVALID, "analysis radial_max must exceed radial_min");
+    if (!std::isfinite(config->formation_fraction) || !(config->formation_fraction > 0.0) ||
+        !(config->formation_fraction < 1.0))
+        return set_error(KP_ERR_INVALID, "analysis formation_fraction must lie strictly between 0 and 1");
+    if (opt.precision != KP_PRECISION_FP64)
+        return set_error(KP_ERR_UNSUPPORTED, "analysis mode runs in FP64 only");
+    if (opt.integrator != KP_INTEGRATOR_STEP_DOUBLING_RK4)
+        return set_error(KP_ERR_UNSUPPORTED, "analysis mode uses step-doubling RK4 only");
+    if (!(params->min_step > 0.0)) return set_error(KP_ERR_INVALID, "analysis mode needs min_step > 0");
+    const int npix = params->camera.nx * params->camera.ny;
+    st = check_outputs(out, npix, 1);
+    if (st != KP_OK) return st;
+    // kp_analysis_out and AnalysisPtrs list the same arrays in the same order
+    constexpr int kArrays = int(sizeof(kp_analysis_out) / sizeof(void*));
+    static_assert(sizeof(kp_analysis_out) == sizeof(AnalysisPtrs), "analysis array lists differ");
+    static_assert(kArrays == 52, "analysis array count");
+    auto is_int = [](int i) { return i == 10 || i == 22; };
+    auto is_radial = [](int i) { return i >= 23 && i < 31; };
+    void* host[kArrays];
+    std::memcpy(host, analysis, sizeof(host));
+    for (int i = 0; i < kArrays; ++i)
+        if (!host[i]) return set_error(KP_ERR_INVALID, "analysis output array %d is NULL", i);
+    const int bins = config->radial_bins;
+    auto bytes_of = [&](int i) {
+        return size_t(is_radial(i) ? bins : 1) * size_t(npix) * (is_int(i) ? sizeof(int32_t) : sizeof(double));
+    };
+
+    std::lock_guard<std::mutex> lock(g_mutex);
+    DeviceState* dev = device_state(opt.device, &st);
+    if (!dev) return st;
+    cudaStream_t stream = opt.stream ? static_cast<cudaStream_t>(opt.stream) : dev->stream;
+    const ImageConsts c = make_consts(params, model, nullptr, 1, opt.integrator);
+    const AnalysisConsts k{bins, config->radial_min, config->radial_max, config->formation_fraction};
+    ImageOutPtrs dptr;
+    void* dev_arrays[kArrays];
+    void* analysis_buf = nullptr;
+    if (opt.outputs_on_device) {
+        dptr = from_abi(out);
+        std::memcpy(dev_arrays, host, sizeof(dev_arrays));
+    } else {
+        void* buf = device_output_buffer(dev, carved_bytes(npix, 1), &st);
+        if (!buf) return st;
+        dptr = carve_outputs(buf, npix, 1);
+        size_t total = 0;
+        for (int i = 0; i < kArrays; ++i) total += (bytes_of(i) + 255) / 256 * 256;
+        cudaError_t e = cudaMalloc(&analysis_buf, total);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return set_error(KP_ERR_OOM, "cudaMalloc(%zu bytes) for analysis outputs: %s", total,
+                             cudaGetErrorString(e));
+        }
+        char* p = static_cast<char*>(analysis_buf);
+        for (int i = 0; i < kArrays; ++i) {
+            dev_arrays[i] = p;
+            p += (bytes_of(i) + 255) / 256 * 256;
+        }
+    }
+    AnalysisPtrs an;
+    std::memcpy(&an, dev_arrays, sizeof(an));
+    const auto t0 = std::chrono::steady_clock::now();
+    cudaError_t e = launch_image_fp64_analysis(c, k, dptr, an, stream);
+    if (e == cudaSuccess && opt.timing) {
+        e = cudaStreamSynchronize(stream);
+        if (e == cudaSuccess)
+            std::printf("timing image_kernel_analysis %g s\n",
+                        std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count());
+    }
+    if (e == cudaSuccess && !opt.outputs_on_device) {
+        st = copy_outputs_to_host(dptr, out, npix, 1, stream);
+        for (int i = 0; st == KP_OK && e == cudaSuccess && i < kArrays; ++i)
+            e = cudaMemcpyAsync(host[i], dev_arrays[i], bytes_of(i), cudaMemcpyDeviceToHost, stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    } else if (e == cudaSuccess && !opt.stream) {
+        e = cudaStreamSynchronize(stream);
+    }
+    if (analysis_buf) cudaFree(analysis_buf);
+    if (e != cudaSuccess) return cuda_error(e, "analysis image");
+    return st;
 }
 
 int kp_batch_riaf(const kp_riaf_job* jobs, int njobs, const kp_run_options* options, kp_batch_stats* stats) {

@@ -10,6 +10,74 @@ namespace kp {
 
 // Plain FP64 kernel, one thread per pixel, one image (kp_kernels_fp64.cu).
 cudaError_t launch_image_fp64(const ImageConsts& c, const ImageOutPtrs& out, cudaStream_t stream);
+// Analysis mode: the per-pixel FP64 image with the line-of-sight
+// diagnostics (one frequency; radial_bins in 1..24).
+constexpr int kMaxRadialBins = 24;  // KPOLARIS_MAX_ANALYSIS_RADIAL_BINS
+
+struct AnalysisConsts {
+    int radial_bins;
+    double radial_min, radial_max, formation_fraction;
+};
+
+// Device arrays of the analysis outputs: scalars [npix]; radial arrays
+// [radial_bins][npix].
+struct AnalysisPtrs {
+    double* radiating_path_length;
+    double* emission_weight;
+    double* emission_weighted_radius;
+    double* emission_weighted_optical_depth_to_camera;
+    double* absorption_depth;
+    double* absorption_operator_depth;
+    double* faraday_rotation_depth;
+    double* faraday_conversion_depth;
+    double* faraday_operator_depth;
+    double* dominant_emission_radius;
+    int32_t* dominant_emission_region;
+    double* dominant_ne_cgs;
+    double* dominant_thetae;
+    double* dominant_b_cgs;
+    double* dominant_beta;
+    double* dominant_sigma;
+    double* emission_weighted_ne_cgs;
+    double* emission_weighted_thetae;
+    double* emission_weighted_b_cgs;
+    double* emission_weighted_beta;
+    double* emission_weighted_sigma;
+    double* photon_ring_winding_estimate;
+    int32_t* radiation_substeps;
+    double* radial_stokes_i;
+    double* radial_stokes_q;
+    double* radial_stokes_u;
+    double* radial_stokes_v;
+    double* radial_absorption_depth;
+    double* radial_faraday_rotation_depth;
+    double* radial_faraday_conversion_depth;
+    double* radial_faraday_operator_depth;
+    double* observer_weighted_radius_i;
+    double* observer_weighted_radius_linear;
+    double* observer_weighted_radius_circular;
+    double* intensity_formation_radius_low;
+    double* intensity_formation_radius_median;
+    double* intensity_formation_radius_high;
+    double* linear_formation_radius_low;
+    double* linear_formation_radius_median;
+    double* linear_formation_radius_high;
+    double* circular_formation_radius_low;
+    double* circular_formation_radius_median;
+    double* circular_formation_radius_high;
+    double* los_linear_coherence;
+    double* los_circular_coherence;
+    double* contribution_closure_max_abs;
+    double* contribution_closure_relative_l1;
+    double* foreground_absorption_depth;
+    double* foreground_faraday_rotation_depth;
+    double* foreground_faraday_conversion_depth;
+    double* foreground_faraday_operator_depth;
+    double* foreground_faraday_operator_fraction;
+};
+
+cudaError_t launch_image_fp64_analysis(const ImageConsts& c, const AnalysisConsts& k, const ImageOutPtrs& out,
+                                       const AnalysisPtrs& an, cudaStream_t stream);
 
 // Camera tetrad of an image, evaluated on the host (bit-identical to the
 // reference's CPU evaluation).

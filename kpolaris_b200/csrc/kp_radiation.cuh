@@ -463,48 +463,68 @@ struct RiafSample {
     int has_chi;
 };
 
+// Boyer-Lindquist r, theta and the azimuth's cosine and sine of a
+// Cartesian Kerr-Schild position (bl_coordinates, riaf.hpp:98-122).
+struct BlCoords {
+    double rc, th, sin_th, cos_th, cphi, sphi;
+};
+
+__device__ __forceinline__ BlCoords riaf_bl_coords(double spin, const D4& x) {
+    BlCoords q;
+    const double xx = x.v[1], yy = x.v[2], zz = x.v[3];
+    const double a2 = spin * spin;
+    const double radius2 = xx * xx + yy * yy + zz * zz;
+    const double sqsum = radius2 - a2;
+    const double discr = sqrt(sqsum * sqsum + 4.0 * a2 * zz * zz);
+    q.rc = sqrt(max_val(0.5 * (sqsum + discr), kTiny));
+    q.th = acos(clamp_val(zz / max_val(q.rc, kTiny), -1.0, 1.0));
+    sincos(q.th, &q.sin_th, &q.cos_th);
+    const double sinth_f = max_val(q.sin_th, 1e-30);
+    const double denom = max_val(sinth_f * (q.rc * q.rc + a2), kTiny);
+    q.cphi = (q.rc * xx + spin * yy) / denom;
+    q.sphi = (q.rc * yy - spin * xx) / denom;
+    const double normp = sqrt(max_val(q.cphi * q.cphi + q.sphi * q.sphi, kTiny));
+    q.cphi /= normp;
+    q.sphi /= normp;
+    return q;
+}
+
+// n_e, Theta_e and B of the plasma at BL (r, theta): density_profile_bl
+// (riaf.hpp:54-60), thetae_profile (:67-74), magnetic_field_cgs (:87-96)
+// at r_bl = max(r, min_radius).  Returns 0 outside the emitting region.
+__device__ __forceinline__ int riaf_plasma(const ImageConsts& c, const BlCoords& q, double& r_bl, double& ne,
+                                           double& thetae, double& b) {
+    r_bl = max_val(q.rc, c.min_radius);
+    if (r_bl <= c.horizon + c.horizon_buffer || r_bl < c.r_min || r_bl > c.r_max) return 0;
+    double ne_norm;
+    {
+        const double zc = r_bl * q.cos_th;
+        const double rcyl = max_val(r_bl * q.sin_th, c.min_radius);
+        const double h = max_val(c.disk_h, 1e-6);
+        const double vertical = exp(-(zc * zc) / (2.0 * rcyl * rcyl * h * h));
+        ne_norm = c.nth0 * vertical * pow(max_val(r_bl, c.min_radius), c.pow_nth);
+    }
+    if (!(ne_norm > 0.0)) return 0;
+    ne = ne_norm * c.ne_unit;
+    thetae = max_val(c.Te0 * pow(max_val(r_bl, c.min_radius), c.pow_T) * c.thetae_unit, c.min_thetae);
+    {
+        const double bb = sqrt(max_val(8.0 * kPi * 0.1 * ne * kMP * kCL * kCL / (6.0 * max_val(r_bl, c.min_radius)), 0.0));
+        b = max_val(bb, 1e-12);
+    }
+    return 1;
+}
+
 static __device__ __noinline__ RiafSample riaf_sample(const ImageConsts& c, const Ray& s) {
     RiafSample out;
     out.emitting = 0;
     out.on_axis = 0;
     out.has_chi = 0;
     const double spin = c.spin;
-    // bl_coordinates (riaf.hpp:98-122)
-    const double xx = s.x.v[1], yy = s.x.v[2], zz = s.x.v[3];
-    const double a2 = spin * spin;
-    const double radius2 = xx * xx + yy * yy + zz * zz;
-    const double sqsum = radius2 - a2;
-    const double discr = sqrt(sqsum * sqsum + 4.0 * a2 * zz * zz);
-    const double rc = sqrt(max_val(0.5 * (sqsum + discr), kTiny));
-    const double th = acos(clamp_val(zz / max_val(rc, kTiny), -1.0, 1.0));
-    double sin_th, cos_th;
-    sincos(th, &sin_th, &cos_th);
-    const double sinth_f = max_val(sin_th, 1e-30);
-    const double denom = max_val(sinth_f * (rc * rc + a2), kTiny);
-    double cphi = (rc * xx + spin * yy) / denom;
-    double sphi = (rc * yy - spin * xx) / denom;
-    const double normp = sqrt(max_val(cphi * cphi + sphi * sphi, kTiny));
-    cphi /= normp;
-    sphi /= normp;
-    const double r_bl = max_val(rc, c.min_radius);
-    if (r_bl <= c.horizon + c.horizon_buffer || r_bl < c.r_min || r_bl > c.r_max) return out;
-    // density_profile_bl (riaf.hpp:54-60)
-    double ne_norm;
-    {
-        const double zc = r_bl * cos_th;
-        const double rcyl = max_val(r_bl * sin_th, c.min_radius);
-        const double h = max_val(c.disk_h, 1e-6);
-        const double vertical = exp(-(zc * zc) / (2.0 * rcyl * rcyl * h * h));
-        ne_norm = c.nth0 * vertical * pow(max_val(r_bl, c.min_radius), c.pow_nth);
-    }
-    if (!(ne_norm > 0.0)) return out;
+    const BlCoords q = riaf_bl_coords(spin, s.x);
+    const double rc = q.rc, th = q.th, sin_th = q.sin_th, cos_th = q.cos_th, cphi = q.cphi, sphi = q.sphi;
+    double r_bl;
+    if (!riaf_plasma(c, q, r_bl, out.ne, out.thetae, out.b)) return out;
     out.emitting = 1;
-    out.ne = ne_norm * c.ne_unit;
-    out.thetae = max_val(c.Te0 * pow(max_val(r_bl, c.min_radius), c.pow_T) * c.thetae_unit, c.min_thetae);
-    {
-        const double bb = sqrt(max_val(8.0 * kPi * 0.1 * out.ne * kMP * kCL * kCL / (6.0 * max_val(r_bl, c.min_radius)), 0.0));
-        out.b = max_val(bb, 1e-12);
-    }
     double g[4][4];
     ks_gcov_matrix(c.mass, spin, s.x, g);
     // fluid_four_velocity_from_bl_coords (riaf.hpp:206-273) at r = r_bl

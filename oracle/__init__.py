@@ -87,6 +87,9 @@ def lib(kind: str):
             C.POINTER(_abi.PassAParams), C.POINTER(_abi.RIAFModel), C.c_int,
             C.POINTER(C.c_double), C.c_int, C.c_int, C.c_int, C.c_int,
             C.POINTER(_abi.ImageOut)]
+        L.kpref_image_riaf_analysis_range.argtypes = [
+            C.POINTER(_abi.PassAParams), C.POINTER(_abi.RIAFModel), C.POINTER(_abi.AnalysisConfig), C.c_int,
+            C.c_int, C.c_int, C.POINTER(_abi.ImageOut), C.POINTER(_abi.AnalysisOut)]
         _declare_common(L, "kpref_")
     else:
         raise ValueError(kind)
@@ -132,6 +135,31 @@ def image_riaf(params, model, freqs, *, kind="port", integrator=0, threads=0,
     if rc != 0:
         raise RuntimeError(getattr(L, _prefix(kind) + "last_error")().decode())
     return out
+
+
+def image_riaf_analysis(params, model, config=None, *, kind="reference", threads=0, pixel_begin=0,
+                        pixel_end=None, out=None, analysis=None):
+    """Analysis-mode RIAF image (or a pixel range of it) through the
+    reference's own per-pixel analysis function (kind 'reference' or
+    'reference_ulp'), single frequency at model.freq_cgs."""
+    if kind not in ("reference", "reference_ulp"):
+        raise ValueError("the analysis oracle is the reference's own code")
+    L = lib(kind)
+    if config is None:
+        config = _abi.default_analysis_config()
+    npix = params.camera.nx * params.camera.ny
+    if out is None:
+        out = _abi.ImageHostData.allocate(npix, 1)
+    if analysis is None:
+        analysis = _abi.AnalysisHostData.allocate(npix, int(config.radial_bins))
+    if pixel_end is None:
+        pixel_end = npix
+    s, a = out.as_struct(), analysis.as_struct()
+    rc = L.kpref_image_riaf_analysis_range(C.byref(params), C.byref(model), C.byref(config), int(threads),
+                                           int(pixel_begin), int(pixel_end), C.byref(s), C.byref(a))
+    if rc != 0:
+        raise RuntimeError(L.kpref_last_error().decode())
+    return out, analysis
 
 
 def thermal_coefficients(fit, nu, ne, thetae, b, theta, sin_theta, cos_theta,

@@ -16,6 +16,7 @@
 #include <stdexcept>
 
 #include "geodesic/pass_b.hpp"
+#include "image/analysis_driver.hpp"
 #include "geometry/kerr_boyer_lindquist.hpp"
 #include "geometry/kerr_fmks.hpp"
 #include "geometry/kerr_schild_cartesian.hpp"
@@ -561,6 +562,103 @@ int kpref_image_riaf_range(const kp_pass_a_params* params, const kp_riaf_model* 
         run_metric(pa, riaf, radiation_substeps, freqs, nfreq, metric, pixel_begin, pixel_end, out);
     } else {
         return fail("coordinate system not built in the reference oracle");
+    }
+    return KP_OK;
+}
+
+// Analysis mode: pixels [pixel_begin, pixel_end) of a single-frequency RIAF
+// image through the reference's per-pixel analysis function
+// (trace_pass_b_segment_model_analysis_pixel_metric,
+// src/image/analysis_driver.hpp:623-636; response channels off), written as
+// the analysis image driver writes them (:820-880).
+int kpref_image_riaf_analysis_range(const kp_pass_a_params* params, const kp_riaf_model* model,
+                                    const kp_analysis_config* config, int threads, int pixel_begin,
+                                    int pixel_end, kp_image_out* out, kp_analysis_out* an) {
+    if (!params || !model || !config || !out || !an) return fail("null argument");
+    const int npix = params->camera.nx * params->camera.ny;
+    if (pixel_begin < 0 || pixel_end > npix || pixel_begin > pixel_end) return fail("pixel range out of bounds");
+    if (config->radial_bins < 1 || config->radial_bins > KPOLARIS_MAX_ANALYSIS_RADIAL_BINS)
+        return fail("radial_bins out of range");
+    if (threads > 0) omp_set_num_threads(threads);
+    const auto pa = to_pass_a(*params);
+    const auto riaf = to_riaf(*model);
+    if (pa.coordinate_system != kpolaris::CoordinateSystem::CartesianKS) return fail("analysis oracle: CKS only");
+    kpolaris::AnalysisConfig<Real> cfg;
+    cfg.radial_bins = config->radial_bins;
+    cfg.radial_min = config->radial_min;
+    cfg.radial_max = config->radial_max;
+    cfg.formation_fraction = config->formation_fraction;
+    const kpolaris::KerrSchildInMetric<Real> metric(pa.mass, pa.spin);
+#pragma omp parallel for schedule(dynamic)
+    for (int pixel = pixel_begin; pixel < pixel_end; ++pixel) {
+#ifdef KPREF_PERTURB_LIBM
+        kpref_ulp::seed_pixel(pixel);
+#endif
+        const kpolaris::PassBAnalysisResult<Real> r =
+            kpolaris::trace_pass_b_segment_model_analysis_pixel_metric(pixel, pa, cfg, riaf, 1, metric);
+        const auto& t = r.transport;
+        const auto& d = r.analysis;
+        out->image_i[pixel] = t.observed_stokes.I;
+        out->image_q[pixel] = t.observed_stokes.Q;
+        out->image_u[pixel] = t.observed_stokes.U;
+        out->image_v[pixel] = t.observed_stokes.V;
+        store_common(out, pixel, t.overlap, t.closure_x, t.closure_k, t.final_null, t.frame_error, t.pass_a.steps,
+                     t.steps, static_cast<int>(t.reason));
+        an->radiating_path_length[pixel] = d.radiating_path_length;
+        an->emission_weight[pixel] = d.emission_weight;
+        an->emission_weighted_radius[pixel] = d.emission_weighted_radius;
+        an->emission_weighted_optical_depth_to_camera[pixel] = d.emission_weighted_optical_depth_to_camera;
+        an->absorption_depth[pixel] = d.absorption_depth;
+        an->absorption_operator_depth[pixel] = d.absorption_operator_depth;
+        an->faraday_rotation_depth[pixel] = d.faraday_rotation_depth;
+        an->faraday_conversion_depth[pixel] = d.faraday_conversion_depth;
+        an->faraday_operator_depth[pixel] = d.faraday_operator_depth;
+        an->dominant_emission_radius[pixel] = d.dominant_emission_radius;
+        an->dominant_emission_region[pixel] = d.dominant_emission_region;
+        an->dominant_ne_cgs[pixel] = d.dominant_ne_cgs;
+        an->dominant_thetae[pixel] = d.dominant_thetae;
+        an->dominant_b_cgs[pixel] = d.dominant_b_cgs;
+        an->dominant_beta[pixel] = d.dominant_beta;
+        an->dominant_sigma[pixel] = d.dominant_sigma;
+        an->emission_weighted_ne_cgs[pixel] = d.emission_weighted_ne_cgs;
+        an->emission_weighted_thetae[pixel] = d.emission_weighted_thetae;
+        an->emission_weighted_b_cgs[pixel] = d.emission_weighted_b_cgs;
+        an->emission_weighted_beta[pixel] = d.emission_weighted_beta;
+        an->emission_weighted_sigma[pixel] = d.emission_weighted_sigma;
+        an->photon_ring_winding_estimate[pixel] = d.photon_ring_winding_estimate;
+        an->radiation_substeps[pixel] = d.radiation_substeps;
+        for (int b = 0; b < cfg.radial_bins; ++b) {
+            const size_t i = size_t(b) * size_t(npix) + size_t(pixel);
+            an->radial_stokes_i_contribution[i] = r.observer_radial_stokes[b].I;
+            an->radial_stokes_q_contribution[i] = r.observer_radial_stokes[b].Q;
+            an->radial_stokes_u_contribution[i] = r.observer_radial_stokes[b].U;
+            an->radial_stokes_v_contribution[i] = r.observer_radial_stokes[b].V;
+            an->radial_absorption_depth[i] = d.radial_absorption_depth[b];
+            an->radial_faraday_rotation_depth[i] = d.radial_faraday_rotation_depth[b];
+            an->radial_faraday_conversion_depth[i] = d.radial_faraday_conversion_depth[b];
+            an->radial_faraday_operator_depth[i] = d.radial_faraday_operator_depth[b];
+        }
+        an->observer_weighted_radius_i[pixel] = d.observer_weighted_radius_i;
+        an->observer_weighted_radius_linear[pixel] = d.observer_weighted_radius_linear;
+        an->observer_weighted_radius_circular[pixel] = d.observer_weighted_radius_circular;
+        an->intensity_formation_radius_low[pixel] = d.intensity_formation_radius_low;
+        an->intensity_formation_radius_median[pixel] = d.intensity_formation_radius_median;
+        an->intensity_formation_radius_high[pixel] = d.intensity_formation_radius_high;
+        an->linear_formation_radius_low[pixel] = d.linear_formation_radius_low;
+        an->linear_formation_radius_median[pixel] = d.linear_formation_radius_median;
+        an->linear_formation_radius_high[pixel] = d.linear_formation_radius_high;
+        an->circular_formation_radius_low[pixel] = d.circular_formation_radius_low;
+        an->circular_formation_radius_median[pixel] = d.circular_formation_radius_median;
+        an->circular_formation_radius_high[pixel] = d.circular_formation_radius_high;
+        an->los_linear_coherence[pixel] = d.los_linear_coherence;
+        an->los_circular_coherence[pixel] = d.los_circular_coherence;
+        an->contribution_closure_max_abs[pixel] = d.contribution_closure_max_abs;
+        an->contribution_closure_relative_l1[pixel] = d.contribution_closure_relative_l1;
+        an->foreground_absorption_depth[pixel] = d.foreground_absorption_depth;
+        an->foreground_faraday_rotation_depth[pixel] = d.foreground_faraday_rotation_depth;
+        an->foreground_faraday_conversion_depth[pixel] = d.foreground_faraday_conversion_depth;
+        an->foreground_faraday_operator_depth[pixel] = d.foreground_faraday_operator_depth;
+        an->foreground_faraday_operator_fraction[pixel] = d.foreground_faraday_operator_fraction;
     }
     return KP_OK;
 }

@@ -1,11 +1,15 @@
 // Minimal host-only stand-in for <Kokkos_Core.hpp>, used ONLY to compile the
 // reference's header-only hot-path templates (src/common, src/geometry,
-// src/camera, src/geodesic, src/radiation, src/frame, src/model) on the CPU
-// as the parity oracle.  It provides exactly what those headers use:
-// KOKKOS_INLINE_FUNCTION, the Kokkos:: math forwards and a reference-counted
-// host View<T*>.  Test infrastructure; never linked into the product.
+// src/camera, src/geodesic, src/radiation, src/frame, src/model, and the
+// image drivers of src/image and src/diagnostics) on the CPU as the parity
+// oracle.  It provides what those headers use: KOKKOS_INLINE_FUNCTION, the
+// Kokkos:: math forwards, reference-counted host Views of rank 1 and 2, and a
+// serial stand-in for the execution API (parallel_for over a RangePolicy in
+// index order, fence, deep_copy, Timer).  Test infrastructure; never linked
+// into the product.
 #pragma once
 
+#include <chrono>
 #include <cmath>
 #include <cstddef>
 #include <cstdio>
@@ -112,6 +116,80 @@ private:
 // Runtime lifetime: the host shim has nothing to start or stop.
 inline bool is_initialized() { return true; }
 inline void finalize() {}
+
+// Host View of rank 2 (the image drivers' [nfreq][npix] arrays).
+template<class T, class... Props>
+class View<T**, Props...> {
+public:
+    using value_type = T;
+    using non_const_value_type = std::remove_const_t<T>;
+    View() = default;
+    View(const std::string&, std::size_t n0, std::size_t n1)
+        : storage_(std::shared_ptr<non_const_value_type[]>(new non_const_value_type[n0 * n1]())),
+          ptr_(storage_.get()), n0_(n0), n1_(n1) {}
+    T& operator()(std::size_t i, std::size_t j) const { return ptr_[i * n1_ + j]; }
+    std::size_t extent(int d) const { return d == 0 ? n0_ : n1_; }
+    std::size_t span() const { return n0_ * n1_; }
+    std::size_t size() const { return n0_ * n1_; }
+    T* data() const { return ptr_; }
+
+private:
+    std::shared_ptr<non_const_value_type[]> storage_;
+    T* ptr_ = nullptr;
+    std::size_t n0_ = 0, n1_ = 0;
+};
+
+// Execution: one serial host space.  The image drivers' parallel_for loops
+// run in index order on the calling thread.
+struct OpenMP {};
+using DefaultExecutionSpace = OpenMP;
+using DefaultHostExecutionSpace = OpenMP;
+struct Unmanaged {};
+struct Dynamic {};
+struct Static {};
+template<class T> struct Schedule {};
+template<class T> struct IndexType {};
+
+template<class... Args>
+struct RangePolicy {
+    long long begin = 0, end = 0;
+    RangePolicy(long long b, long long e) : begin(b), end(e) {}
+    template<class Space>
+    RangePolicy(const Space&, long long b, long long e) : begin(b), end(e) {}
+};
+
+template<class... Args, class F>
+inline void parallel_for(const RangePolicy<Args...>& policy, const F& f) {
+    for (long long i = policy.begin; i < policy.end; ++i) f(static_cast<int>(i));
+}
+template<class... Args, class F>
+inline void parallel_for(const std::string&, const RangePolicy<Args...>& policy, const F& f) {
+    parallel_for(policy, f);
+}
+template<class F>
+inline void parallel_for(const std::string&, long long n, const F& f) {
+    for (long long i = 0; i < n; ++i) f(static_cast<int>(i));
+}
+template<class F>
+inline void parallel_for(long long n, const F& f) {
+    for (long long i = 0; i < n; ++i) f(static_cast<int>(i));
+}
+
+inline void fence() {}
+inline void fence(const std::string&) {}
+
+template<class A, class B>
+inline void deep_copy(const A& dst, const B& src) {
+    for (std::size_t i = 0; i < src.span(); ++i) dst.data()[i] = src.data()[i];
+}
+
+struct Timer {
+    std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+    double seconds() const {
+        return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+    void reset() { t0 = std::chrono::steady_clock::now(); }
+};
 
 // Host views already live in host memory: the mirror is the view itself.
 template<class Space, class V>

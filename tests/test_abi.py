@@ -48,6 +48,8 @@ def test_struct_layouts_match_ctypes_mirror():
     assert lib.kp_abi_sizeof(9) == C.sizeof(_abi.Tuning)
     assert lib.kp_abi_sizeof(10) == C.sizeof(_abi.GrmhdModel)
     assert lib.kp_abi_sizeof(11) == C.sizeof(_abi.GrmhdJob)
+    assert lib.kp_abi_sizeof(12) == C.sizeof(_abi.AnalysisConfig)
+    assert lib.kp_abi_sizeof(13) == C.sizeof(_abi.AnalysisOut)
     assert lib.kp_abi_sizeof(6) > 0
     assert lib.kp_abi_sizeof(99) == 0
 
