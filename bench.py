@@ -70,6 +70,8 @@ def parse():
     ap.add_argument("--grmhd-precision", default="mixed", choices=["fp64", "mixed"])
     ap.add_argument("--config4", type=int, default=1,
                     help="also time the uneven 64-image batch (autotuned, graph-captured) and the slow-light job")
+    ap.add_argument("--analysis", type=int, default=1,
+                    help="also time an analysis-mode image (kp_image_riaf_analysis) beside the plain FP64 image")
     return ap.parse_args()
 
 
@@ -215,6 +217,57 @@ def grmhd_section(args, torch, dev, local, stream, flush, rank):
                                    "kind": "reference",
                                    "sample": f"{rows} of {n} rows ({rows * n} pixels, spread over the image), "
                                              f"{dt:.2f} s, FP64, derived scalars precomputed"}
+    return res
+
+
+def analysis_section(args, local, flush, torch, rank):
+    """Analysis mode: one 256^2 single-frequency (230 GHz) RIAF image with the
+    line-of-sight diagnostics (16 radial bins), config-2 controls, through
+    kp_image_riaf_analysis with host outputs (device time plus the copies of
+    the image and 52 analysis arrays), beside the plain FP64 image of the
+    same frequency; the reference's own analysis code on a bounded CPU
+    sample of the same image."""
+    import kpolaris_b200 as kp
+    from kpolaris_b200 import _abi, configs
+
+    n = 256
+    params, model, _ = configs.config2(n, n)
+    cfg = _abi.default_analysis_config()
+    kp.image_riaf_analysis(params, model, cfg, device=local)
+    times, plain = [], []
+    for _ in range(2):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        kp.image_riaf_analysis(params, model, cfg, device=local)
+        times.append(time.perf_counter() - t0)
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        kp.image_riaf(params, model, [model.freq_cgs], device=local)
+        plain.append(time.perf_counter() - t0)
+    res = {"workload": "RIAF 256^2, 230 GHz, config-2 controls (adaptive RK4 tol 1e-8), analysis mode with "
+                       "16 logarithmic radial bins 2-100 M, FP64 per-pixel kernel",
+           "seconds_incl_d2h": min(times), "images_per_s": 1.0 / min(times),
+           "plain_fp64_seconds_incl_d2h": min(plain)}
+    if rank == 0:
+        import oracle
+
+        if oracle.ref_available():
+            host = _abi.ImageHostData.allocate(n * n, 1)
+            an = _abi.AnalysisHostData.allocate(n * n, int(cfg.radial_bins))
+            rows, t0 = 0, time.perf_counter()
+            for j in [j for off in range(16) for j in range(off, n, 16)]:
+                oracle.image_riaf_analysis(params, model, cfg, threads=0, pixel_begin=j * n,
+                                           pixel_end=(j + 1) * n, out=host, analysis=an)
+                rows += 1
+                if time.perf_counter() - t0 >= min(args.cpu_seconds, 6.0):
+                    break
+            dt = time.perf_counter() - t0
+            res["cpu_baseline"] = {"value": rows / float(n) / dt, "unit": "images/s", "cores": os.cpu_count() or 1,
+                                   "kind": "reference",
+                                   "sample": f"{rows} of {n} rows ({rows * n} pixels, spread over the image), "
+                                             f"{dt:.2f} s, FP64"}
     return res
 
 
@@ -759,6 +812,11 @@ def ours_arm(args):
         progress("uneven batch and slow light")
         config4 = config4_section(local, stream, flush, torch)
 
+    analysis = None
+    if args.analysis and world == 1:
+        progress("analysis-mode image")
+        analysis = analysis_section(args, local, flush, torch, rank)
+
     cpu = None
     if rank == 0:
         import oracle
@@ -795,6 +853,7 @@ def ours_arm(args):
             "phases": phases, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
             "grmhd": grmhd,
             "config4": config4,
+            "analysis": analysis,
         }
         print(json.dumps(line), flush=True)
     if pg:
