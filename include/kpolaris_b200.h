@@ -642,7 +642,7 @@ int kp_autotune_batch(const kp_riaf_job* jobs, int njobs, const kp_run_options* 
  * kp_batch_riaf for callers that must not allocate: the same wavefront
  * engine and results (bit-identical to kp_batch_riaf with the same options),
  * but every piece of device scratch lives in one static device array of the
- * library (31 MB per device), so the call makes no cudaMalloc/cudaFree and
+ * library (32 MB per device), so the call makes no cudaMalloc/cudaFree and
  * no host allocation.  For callers that run under a fixed device-memory
  * budget, and for callers that cannot afford cudaFree's device-wide
  * synchronisation while other streams are busy (a serving loop, a

@@ -170,13 +170,13 @@ struct JobDesc {
     int precision;        // kp_precision of this job
 };
 
-// Resumable state of one ray between launches (lives in HBM, 448 bytes):
+// Resumable state of one ray between launches (lives in HBM, 464 bytes):
 // the ray, the control state and the Stokes channels (32 bytes per frequency
 // in either precision).  Rays are parked only at the top of the pass-A or
 // pass-B loop, so the crossing search never spans two launches.
 struct alignas(16) RayRecord {
     Ray S;
-    double st[24];
+    double st[26];
     double stokes[4 * kMaxFreq];
 };
 

@@ -175,6 +175,11 @@ struct RadTraits<PolicyMixed, SceneGrmhdSlow> : RadTraits<PolicyMixed, SceneRiaf
     __device__ static Sample sample(const ImageConsts& c, const Ray& r) { return grmhd_series_sample_f(c, r); }
 };
 
+// A far-phase chart scene radiates nothing; its Stokes types are its
+// record scene's.
+template<class P, class B>
+struct RadTraits<P, SceneFarCks<B>> : RadTraits<P, B> {};
+
 // The scene's transport RHS under a policy; FP32 is a compile-time choice of
 // the calling kernel, so each kernel holds one contraction body.  The FP64
 // policy keeps the reference's operation order; the mixed policy uses the
@@ -371,9 +376,11 @@ __device__ __noinline__ void rk_job(int kind, const ImageConsts& c, const Ray& S
         ck_job<P, FP32, SC>(c, S, h, next, mid, err);
         return;
     }
-    if constexpr (FP32 && std::is_same_v<SC, SceneRiaf>) {
-        far_job_f(kind, c, S, h, next, mid, err);
-        return;
+    if constexpr (FP32 && SC::kCksRhs) {
+        if (SC::chart_active(c)) {
+            far_job_f(kind, c, S, h, next, mid, err);
+            return;
+        }
     }
     // Stage schedule (see file header): SD = half chain (4), second half
     // chain (4), full chain (3); RK4 = 4; RK4x2 = 4 + 4.

@@ -12,7 +12,7 @@ namespace kp {
 
 template<int NF>
 __global__ void __launch_bounds__(kFarThreads, 2) wave_far_grmhd_mixed(const WaveDesc W) {
-    persistent_body<PolicyMixed, NF, kPhaseFar, SceneGrmhd>(W);
+    persistent_body<PolicyMixed, NF, kPhaseFar, SceneFarCks<SceneGrmhd>>(W);
 }
 
 template<int NF>

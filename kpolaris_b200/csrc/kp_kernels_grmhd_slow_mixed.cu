@@ -10,7 +10,7 @@ namespace kp {
 
 template<int NF>
 __global__ void __launch_bounds__(kFarThreads, 2) wave_far_grmhd_slow_mixed(const WaveDesc W) {
-    persistent_body<PolicyMixed, NF, kPhaseFar, SceneGrmhdSlow>(W);
+    persistent_body<PolicyMixed, NF, kPhaseFar, SceneFarCks<SceneGrmhdSlow>>(W);
 }
 
 template<int NF>

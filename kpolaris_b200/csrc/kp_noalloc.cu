@@ -47,7 +47,7 @@ NoAllocScratch* g_scratch_ptr[64] = {};
 }  // namespace
 }  // namespace kp
 
-// The scratch of every call on a device (31 MB: 448-byte records and six id
+// The scratch of every call on a device (32 MB: 464-byte records and six id
 // queues for KP_NOALLOC_MAX_RAYS rays, a job table of KP_NOALLOC_MAX_JOBS
 // descriptors, the counters).  Reserved when this unit's module loads, and
 // shared by every call on the device: calls that overlap in time race.

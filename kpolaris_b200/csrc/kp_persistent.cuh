@@ -24,7 +24,7 @@ namespace kp {
 
 enum : int { kEndA = 7 };
 
-// Control state of one ray (doubles first: 16 doubles + 16 ints, 192 bytes).
+// Control state of one ray (doubles first: 17 doubles + 17 ints, 208 bytes).
 struct LaneState {
     // adaptive attempt sequence (rk4.hpp:108-161)
     double h_try, req_h, ctl_min, ctl_max;
@@ -34,11 +34,16 @@ struct LaneState {
     double lo, hi, flo, fhi, full_h, surf, trial;
     // pass B (pass_b.hpp:940-1114)
     double cap, hB, start_r;
+    // far-phase chart scenes: the FMKS azimuth the ray entered the far
+    // phase with, and whether S (here and in a record parked for the far
+    // phase itself) holds the far phase's chart
+    double x3_ref;
     int job, pixel, mode, in_b;
     int attempt, rk_kind;
     int n, entered, inside, pa_steps, reason;
     int cross_reason, iter, use_secant;
     int steps, reached;
+    int chart;
 };
 static_assert(sizeof(LaneState) <= sizeof(((RayRecord*)nullptr)->st), "LaneState must fit its record slot");
 
@@ -177,6 +182,17 @@ __device__ __forceinline__ int phase_of(const ImageConsts& c, int in_b, double r
     return in_b ? kPhaseNearB : kPhaseNearA;
 }
 
+// The scene a ray is finished in: a far-phase chart scene hands the ray
+// back to the scene its records use.
+template<class SC>
+struct RecordScene {
+    using type = SC;
+};
+template<class B>
+struct RecordScene<SceneFarCks<B>> {
+    using type = B;
+};
+
 template<class P, int NF, int PHASE, class SC = SceneRiaf>
 __device__ __forceinline__ void persistent_body(const WaveDesc& W) {
     constexpr bool kFar = PHASE == kPhaseFar;
@@ -227,6 +243,13 @@ __device__ __forceinline__ void persistent_body(const WaveDesc& W) {
                     my_id = unsigned(id);
                     J = &W.jobs[lo];
                     start_ray<SC>(st, S, J, lo, int(id - J->ray_begin));
+                    if constexpr (SC::kFarChart) {
+                        if (SC::chart_active(J->c)) {
+                            st.x3_ref = S.x.v[3];
+                            S = SC::to_phase(J->c, S);
+                            st.chart = 1;
+                        }
+                    }
                 } else if (W.budget > 0 && lane_jobs >= W.budget) {
                     // past the budget: hand the id on untouched (below)
                     my_id = W.in_ids[k - nfresh];
@@ -238,6 +261,14 @@ __device__ __forceinline__ void persistent_body(const WaveDesc& W) {
                     S = rec.S;
                     memcpy(&st, rec.st, sizeof(LaneState));
                     J = &W.jobs[st.job];
+                    if constexpr (SC::kFarChart) {
+                        // a record parked for this phase already holds its chart
+                        if (!st.chart && SC::chart_active(J->c)) {
+                            st.x3_ref = S.x.v[3];
+                            S = SC::to_phase(J->c, S);
+                            st.chart = 1;
+                        }
+                    }
                     if constexpr (kRad) memcpy(&stokes[0], rec.stokes, sizeof(stokes));
                 }
             }
@@ -330,7 +361,19 @@ __device__ __forceinline__ void persistent_body(const WaveDesc& W) {
         const bool park = dest >= 0;
         if (park) {
             RayRecord& rec = W.pool[my_id];
-            rec.S = S;
+            if constexpr (SC::kFarChart) {
+                // leaving the phase: back to the records' chart; parked for
+                // this phase (a tick budget): kept as is, so the ray resumes
+                // bit for bit as if it had not been parked
+                if (st.chart && dest != PHASE) {
+                    rec.S = SC::to_record(J->c, S, st.x3_ref);
+                    st.chart = 0;
+                } else {
+                    rec.S = S;
+                }
+            } else {
+                rec.S = S;
+            }
             memcpy(rec.st, &st, sizeof(LaneState));
             if constexpr (kRad) memcpy(rec.stokes, &stokes[0], sizeof(stokes));
         }
@@ -663,7 +706,12 @@ __device__ __forceinline__ void persistent_body(const WaveDesc& W) {
 #pragma unroll
             for (int f = 0; f < NF; ++f)
                 sd[f] = st.in_b ? RT::result(stokes[f], c, f) : Stokes4<double>{0.0, 0.0, 0.0, 0.0};
-            finish_ray_scene<SC, NF>(c, cam, S, st.in_b, sd, o, obs);
+            if constexpr (SC::kFarChart) {
+                const Ray S_rec = st.chart ? SC::to_record(c, S, st.x3_ref) : S;
+                finish_ray_scene<typename RecordScene<SC>::type, NF>(c, cam, S_rec, st.in_b, sd, o, obs);
+            } else {
+                finish_ray_scene<SC, NF>(c, cam, S, st.in_b, sd, o, obs);
+            }
             store_stokes_n<NF>(J->out, st.pixel, J->npix, c.nfreq, obs);
             store_diagnostics(J->out, st.pixel, o);
             if constexpr (SC::kSlowLight) {

@@ -10,6 +10,7 @@
 #pragma once
 
 #include "kp_camera.cuh"
+#include "kp_chart.cuh"
 #include "kp_fmks.cuh"
 #include "kp_geometry_f32.cuh"
 #include "kp_grmhd.cuh"
@@ -30,6 +31,9 @@ __device__ __forceinline__ Ray riaf_rhs(double mass, double spin, const Ray& X) 
 
 struct SceneRiaf {
     static constexpr bool kSlowLight = false;
+    static constexpr bool kCksRhs = true;     // transport is the Cartesian Kerr-Schild RHS
+    static constexpr bool kFarChart = false;  // records and integration share one chart
+    __device__ static bool chart_active(const ImageConsts&) { return true; }
     struct Metric {
         KSMetricPoint w;
         __device__ double dot(const D4& u, const D4& v) const { return ks_dot_at(w, u, v); }
@@ -85,6 +89,9 @@ static __device__ __noinline__ Ray fmks_camera_ray(const ImageConsts& c, const C
 
 struct SceneGrmhd {
     static constexpr bool kSlowLight = false;
+    static constexpr bool kCksRhs = false;
+    static constexpr bool kFarChart = false;
+    __device__ static bool chart_active(const ImageConsts&) { return false; }
     struct Metric {
         double g[4][4];
         __device__ double dot(const D4& u, const D4& v) const { return dot_gm(g, u, v); }
@@ -118,6 +125,38 @@ struct SceneGrmhdSlow : SceneGrmhd {
     static constexpr bool kSlowLight = true;
     __device__ static bool time_resident(const ImageConsts& c, const Ray& sample) {
         return series_holds(c, series_time(c, sample));
+    }
+};
+
+// A GRMHD scene as the mixed policy's far kernel runs it: beyond the
+// radiating sphere no plasma is sampled, so the ray is integrated in
+// Cartesian Kerr-Schild (the RIAF scene's FP32 stage chains, with the
+// policy's step control) and converted at the phase boundary
+// (kp_chart.cuh).  Records, cameras and the end of a ray stay in FMKS:
+// to_phase converts a claimed ray, to_record converts it back before it is
+// parked or finished.  Phase decisions use the radius its record will hold.
+//
+// Only step-doubling images change chart: with adaptive steps the far
+// field's truncation error stays under the tolerance in either chart, while
+// a fixed step's error depends on the chart it is taken in.  Fixed-step and
+// Cash-Karp images keep FMKS in the same kernel (chart_active false: the
+// base scene's radius and RHS, no conversion).
+template<class Base>
+struct SceneFarCks : Base {
+    static constexpr bool kCksRhs = true;
+    static constexpr bool kFarChart = true;
+    __device__ static bool chart_active(const ImageConsts& c) { return c.adaptive && c.integrator != 1; }
+    __device__ static double radius(const ImageConsts& c, const D4& X) {
+        return chart_active(c) ? cks_record_radius(c.spin, X) : Base::radius(c, X);
+    }
+    // reached only with the chart inactive (the active chart runs far_job_f)
+    template<bool MIXED, bool FP32>
+    __device__ static Ray rhs(const ImageConsts& c, const Ray& X) {
+        return Base::template rhs<MIXED, false>(c, X);
+    }
+    __device__ static Ray to_phase(const ImageConsts& c, const Ray& S) { return fmks_to_cks(c.fmks, c.spin, S); }
+    __device__ static Ray to_record(const ImageConsts& c, const Ray& S, double x3_ref) {
+        return cks_to_fmks(c.fmks, c.spin, S, x3_ref);
     }
 };
 

@@ -64,6 +64,33 @@ kp::FmksParams fmks_of(const kp_pass_a_params* p) {
 
 extern "C" {
 
+// The far phase's change of chart (kp_chart.cuh) and the two metrics' dot
+// products, for the round-trip and invariance checks.
+void h_fmks_to_cks(const kp_pass_a_params* p, const double* s16, double* o16) {
+    store(kp::fmks_to_cks(fmks_of(p), p->spin, ray_of(s16)), o16);
+}
+
+void h_cks_to_fmks(const kp_pass_a_params* p, const double* s16, double x3_ref, double* o16) {
+    store(kp::cks_to_fmks(fmks_of(p), p->spin, ray_of(s16), x3_ref), o16);
+}
+
+double h_cks_record_radius(double spin, const double* x4) {
+    kp::D4 x{{x4[0], x4[1], x4[2], x4[3]}};
+    return kp::cks_record_radius(spin, x);
+}
+
+double h_dot_fmks(const kp_pass_a_params* p, const double* x4, const double* u4, const double* v4) {
+    kp::D4 x{{x4[0], x4[1], x4[2], x4[3]}}, u{{u4[0], u4[1], u4[2], u4[3]}}, v{{v4[0], v4[1], v4[2], v4[3]}};
+    double g[4][4];
+    kp::fmks_gcov(fmks_of(p), x, g);
+    return kp::dot_gm(g, u, v);
+}
+
+double h_dot_cks(double spin, const double* x4, const double* u4, const double* v4) {
+    kp::D4 x{{x4[0], x4[1], x4[2], x4[3]}}, u{{u4[0], u4[1], u4[2], u4[3]}}, v{{v4[0], v4[1], v4[2], v4[3]}};
+    return kp::ks_dot_at(kp::ks_point(1.0, spin, x), u, v);
+}
+
 void h_fmks_rhs(const kp_pass_a_params* p, const double* s16, double* d16) {
     store(kp::fmks_rhs(fmks_of(p), ray_of(s16)), d16);
 }

@@ -50,6 +50,14 @@ def host(tmp_path_factory):
     L.h_camera_ray_fmks.argtypes = [P(_abi.PassAParams), C.c_int, P(d)]
     L.h_grmhd_derived.argtypes = [P(_abi.GrmhdModel), P(C.c_float), P(d)]
     L.h_grmhd_coefficients.argtypes = [P(_abi.PassAParams), P(_abi.GrmhdModel), P(C.c_float), P(d), P(d), d, P(d)]
+    L.h_fmks_to_cks.argtypes = [P(_abi.PassAParams), P(d), P(d)]
+    L.h_cks_to_fmks.argtypes = [P(_abi.PassAParams), P(d), d, P(d)]
+    L.h_cks_record_radius.argtypes = [d, P(d)]
+    L.h_cks_record_radius.restype = d
+    L.h_dot_fmks.argtypes = [P(_abi.PassAParams), P(d), P(d), P(d)]
+    L.h_dot_fmks.restype = d
+    L.h_dot_cks.argtypes = [d, P(d), P(d), P(d)]
+    L.h_dot_cks.restype = d
     return L
 
 
@@ -210,3 +218,35 @@ def test_host_grid_coefficients_match_reference(host, case, fit):
                 err = np.max(np.abs(got[lo:hi] - want[lo:hi]))
                 assert err <= 1e-11 * scale or (scale == 0 and err == 0), (i, use_derived, lo, got, want)
     assert emitting > 50
+
+
+def test_far_phase_chart_round_trip(host, case):
+    """The mixed far phase integrates GRMHD rays in Cartesian Kerr-Schild
+    (kp_chart.cuh): FMKS -> CKS -> FMKS returns the state to rounding, every
+    metric dot product of x, k, e1, e2 is the same in both charts, the
+    azimuth is unwrapped against the entry value, and the far kernel's phase
+    radius equals exp(x1) of the record it writes."""
+    fx, prims, model, params, freqs = case
+    for s in seeded_states(model, 64, 31, r_lo=55.0, r_hi=1000.0):
+        s = np.array(s, dtype=np.float64)
+        for turns in (0.0, 2.0, -1.0):  # FMKS azimuths beyond [0, 2 pi) stay continuous
+            s_in = s.copy()
+            s_in[3] += turns * 2.0 * math.pi
+            cks = np.zeros(16)
+            host.h_fmks_to_cks(C.byref(params), _dp(s_in), _dp(cks))
+            back = np.zeros(16)
+            host.h_cks_to_fmks(C.byref(params), _dp(cks), s_in[3], _dp(back))
+            assert np.allclose(back[:4], s_in[:4], rtol=1e-12, atol=1e-12), (s_in[:4], back[:4])
+            for a in range(1, 4):
+                v, w = s_in[4 * a:4 * a + 4], back[4 * a:4 * a + 4]
+                assert np.max(np.abs(v - w)) <= 1e-10 * max(1.0, np.max(np.abs(v))), (a, v, w)
+            pairs = [(1, 1), (1, 2), (2, 2), (1, 3), (3, 3), (2, 3)]
+            for a, b in pairs:
+                fm = host.h_dot_fmks(C.byref(params), _dp(s_in[:4]), _dp(s_in[4 * a:4 * a + 4]),
+                                     _dp(s_in[4 * b:4 * b + 4]))
+                ck = host.h_dot_cks(params.spin, _dp(cks[:4]), _dp(cks[4 * a:4 * a + 4]), _dp(cks[4 * b:4 * b + 4]))
+                # metric components grow as r^2: the bar scales with the terms of the sum
+                terms = math.exp(2.0 * s_in[1]) * max(1.0, np.max(np.abs(s_in[4 * a:4 * a + 4]))) * \
+                    max(1.0, np.max(np.abs(s_in[4 * b:4 * b + 4])))
+                assert abs(fm - ck) <= 1e-14 * terms + 1e-13 * abs(fm), (a, b, fm, ck, terms)
+            assert host.h_cks_record_radius(params.spin, _dp(cks[:4])) == math.exp(back[1])
