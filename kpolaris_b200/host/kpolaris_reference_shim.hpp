@@ -15,6 +15,7 @@
 // std::invalid_argument, everything else as std::runtime_error.
 #pragma once
 
+#include <cmath>
 #include <cstring>
 #include <map>
 #include <stdexcept>
@@ -175,6 +176,117 @@ HostData run_riaf_image(const PassA& pass_a, Model model, int radiation_substeps
     opt.timing = timing;
     const double f = m.freq_cgs;
     throw_on_error(kp_image_riaf(&p, &m, radiation_substeps, &f, 1, &opt, &o));
+    return out;
+}
+
+// run_riaf_analysis_image (src/image/riaf.hpp:22-28, src/image/riaf.cpp:48-75):
+// the image plus the analysis block of ImageHostData (src/image/result.hpp:
+// 35-92), with the radial-bin edges and centres the reference's analysis
+// driver records (src/image/analysis_driver.hpp:1060-1076).  The response
+// channels (analysis_config.response) are not built.
+template<class HostData, class PassA, class AnalysisCfg, class Model>
+HostData run_riaf_analysis_image(const PassA& pass_a, const AnalysisCfg& analysis_config, Model model,
+                                 int radiation_substeps, int timing, int split_transport) {
+    (void)split_transport;
+    if (analysis_config.response.enabled())
+        throw std::runtime_error("analysis response channels (analysis_partition) are not built");
+    const kp_pass_a_params p = to_c(pass_a);
+    const kp_riaf_model m = to_c_riaf(model);
+    const int npix = p.camera.nx * p.camera.ny;
+    const int bins = analysis_config.radial_bins;
+    if (bins < 1 || bins > KP_MAX_ANALYSIS_RADIAL_BINS)
+        throw std::invalid_argument("analysis_radial_bins must lie in [1, KPOLARIS_MAX_ANALYSIS_RADIAL_BINS]");
+    HostData out;
+    kp_image_out o = bind_outputs(out, npix, 1);
+    kp_analysis_out a;
+    auto scalar = [&](auto& v) {
+        v.assign(size_t(npix), 0);
+        return v.data();
+    };
+    auto radial = [&](auto& v) {
+        v.assign(size_t(bins) * size_t(npix), 0);
+        return v.data();
+    };
+    auto as_i32 = [](int* q) { return reinterpret_cast<int32_t*>(q); };
+    static_assert(sizeof(int) == sizeof(int32_t), "int arrays are passed as int32");
+    a.radiating_path_length = scalar(out.radiating_path_length);
+    a.emission_weight = scalar(out.emission_weight);
+    a.emission_weighted_radius = scalar(out.emission_weighted_radius);
+    a.emission_weighted_optical_depth_to_camera = scalar(out.emission_weighted_optical_depth_to_camera);
+    a.absorption_depth = scalar(out.absorption_depth);
+    a.absorption_operator_depth = scalar(out.absorption_operator_depth);
+    a.faraday_rotation_depth = scalar(out.faraday_rotation_depth);
+    a.faraday_conversion_depth = scalar(out.faraday_conversion_depth);
+    a.faraday_operator_depth = scalar(out.faraday_operator_depth);
+    a.dominant_emission_radius = scalar(out.dominant_emission_radius);
+    a.dominant_emission_region = as_i32(scalar(out.dominant_emission_region));
+    a.dominant_ne_cgs = scalar(out.dominant_ne_cgs);
+    a.dominant_thetae = scalar(out.dominant_thetae);
+    a.dominant_b_cgs = scalar(out.dominant_b_cgs);
+    a.dominant_beta = scalar(out.dominant_beta);
+    a.dominant_sigma = scalar(out.dominant_sigma);
+    a.emission_weighted_ne_cgs = scalar(out.emission_weighted_ne_cgs);
+    a.emission_weighted_thetae = scalar(out.emission_weighted_thetae);
+    a.emission_weighted_b_cgs = scalar(out.emission_weighted_b_cgs);
+    a.emission_weighted_beta = scalar(out.emission_weighted_beta);
+    a.emission_weighted_sigma = scalar(out.emission_weighted_sigma);
+    a.photon_ring_winding_estimate = scalar(out.photon_ring_winding_estimate);
+    a.radiation_substeps = as_i32(scalar(out.radiation_substeps));
+    a.radial_stokes_i_contribution = radial(out.radial_stokes_i_contribution);
+    a.radial_stokes_q_contribution = radial(out.radial_stokes_q_contribution);
+    a.radial_stokes_u_contribution = radial(out.radial_stokes_u_contribution);
+    a.radial_stokes_v_contribution = radial(out.radial_stokes_v_contribution);
+    a.radial_absorption_depth = radial(out.radial_absorption_depth);
+    a.radial_faraday_rotation_depth = radial(out.radial_faraday_rotation_depth);
+    a.radial_faraday_conversion_depth = radial(out.radial_faraday_conversion_depth);
+    a.radial_faraday_operator_depth = radial(out.radial_faraday_operator_depth);
+    a.observer_weighted_radius_i = scalar(out.observer_weighted_radius_i);
+    a.observer_weighted_radius_linear = scalar(out.observer_weighted_radius_linear);
+    a.observer_weighted_radius_circular = scalar(out.observer_weighted_radius_circular);
+    a.intensity_formation_radius_low = scalar(out.intensity_formation_radius_low);
+    a.intensity_formation_radius_median = scalar(out.intensity_formation_radius_median);
+    a.intensity_formation_radius_high = scalar(out.intensity_formation_radius_high);
+    a.linear_formation_radius_low = scalar(out.linear_formation_radius_low);
+    a.linear_formation_radius_median = scalar(out.linear_formation_radius_median);
+    a.linear_formation_radius_high = scalar(out.linear_formation_radius_high);
+    a.circular_formation_radius_low = scalar(out.circular_formation_radius_low);
+    a.circular_formation_radius_median = scalar(out.circular_formation_radius_median);
+    a.circular_formation_radius_high = scalar(out.circular_formation_radius_high);
+    a.los_linear_coherence = scalar(out.los_linear_coherence);
+    a.los_circular_coherence = scalar(out.los_circular_coherence);
+    a.contribution_closure_max_abs = scalar(out.contribution_closure_max_abs);
+    a.contribution_closure_relative_l1 = scalar(out.contribution_closure_relative_l1);
+    a.foreground_absorption_depth = scalar(out.foreground_absorption_depth);
+    a.foreground_faraday_rotation_depth = scalar(out.foreground_faraday_rotation_depth);
+    a.foreground_faraday_conversion_depth = scalar(out.foreground_faraday_conversion_depth);
+    a.foreground_faraday_operator_depth = scalar(out.foreground_faraday_operator_depth);
+    a.foreground_faraday_operator_fraction = scalar(out.foreground_faraday_operator_fraction);
+    kp_analysis_config c;
+    c.radial_bins = bins;
+    c.radial_min = analysis_config.radial_min;
+    c.radial_max = analysis_config.radial_max;
+    c.formation_fraction = analysis_config.formation_fraction;
+    kp_run_options opt = shim_options();
+    opt.timing = timing;
+    throw_on_error(kp_image_riaf_analysis(&p, &m, radiation_substeps, &c, &opt, &o, &a));
+    out.has_analysis = 1;
+    out.response_config = analysis_config.response;
+    out.analysis_radial_bins = bins;
+    out.analysis_radial_min = analysis_config.radial_min;
+    out.analysis_radial_max = analysis_config.radial_max;
+    out.analysis_formation_fraction = analysis_config.formation_fraction;
+    out.analysis_radial_bin_edges.assign(size_t(bins) + 1, 0.0);
+    out.analysis_radial_bin_centers.assign(size_t(bins), 0.0);
+    const double lo = std::log(analysis_config.radial_min), hi = std::log(analysis_config.radial_max);
+    for (int b = 0; b <= bins; ++b) {
+        out.analysis_radial_bin_edges[size_t(b)] = std::exp(lo + double(b) / double(bins) * (hi - lo));
+        if (b < bins) {
+            const bool valid = analysis_config.radial_max > analysis_config.radial_min &&
+                               analysis_config.radial_min > 0.0;
+            out.analysis_radial_bin_centers[size_t(b)] =
+                valid ? std::exp(lo + (double(b) + 0.5) / double(bins) * (hi - lo)) : 0.0;
+        }
+    }
     return out;
 }
 

@@ -4,6 +4,7 @@
 // the reference's build would.  Linked against the library, it runs no GPU
 // work: main only checks that each instantiation exists.
 #include "geodesic/pass_a_core.hpp"
+#include "image/analysis_driver.hpp"
 #include "image/result.hpp"
 #include "model/grmhd.hpp"
 #include "model/riaf.hpp"
@@ -15,6 +16,9 @@ using Riaf = kpolaris::RIAFAnalyticRadiationModel<double>;
 using Grmhd = kpolaris::GRMHDGridRadiationModel<double>;
 
 template ImageHostData kpolaris_b200::run_riaf_image<ImageHostData, PassA, Riaf>(const PassA&, Riaf, int, int, int);
+template ImageHostData kpolaris_b200::run_riaf_analysis_image<ImageHostData, PassA,
+                                                               kpolaris::AnalysisConfig<double>, Riaf>(
+    const PassA&, const kpolaris::AnalysisConfig<double>&, Riaf, int, int, int);
 template ImageHostData kpolaris_b200::run_riaf_multifrequency_image<ImageHostData, PassA, Riaf>(
     const PassA&, Riaf, int, const std::vector<double>&, const std::vector<double>&, int, int);
 template ImageHostData kpolaris_b200::run_grmhd_image<ImageHostData, PassA, Grmhd>(const PassA&, Grmhd, int, int, int);
