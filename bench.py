@@ -19,7 +19,7 @@ and image-integrated EVPA per frequency).  `--path plain` makes the plain
 kernel the headline.
 
 Metric: 256^2 images/s (whole job).  `value` is device-timed with outputs in
-HBM; `e2e` goes through the public API with host output buffers, job-table
+HBM; `e2e` goes through the public API with pinned host output buffers, job-table
 upload and device-to-host copies inside the timed region.  Multi-GPU runs are
 independent replicas (weak scaling): no collective on the data path.
 """
@@ -725,8 +725,22 @@ def ours_arm(args):
     reason_match = float(np.mean(outs[0][1][2][2].cpu().numpy() == plain_out[1][2][2].cpu().numpy()))
 
     progress("e2e")
-    # ---- e2e: the same batch through the public API with host buffers
-    host = [_abi.ImageHostData.allocate(npix, nfreq) for _ in range(batch)]
+    # ---- e2e: the same batch through the public API with host buffers in
+    # pinned memory (the library copies each output array device-to-host)
+    pinned = []
+
+    def pinned_host_data():
+        arrays = {}
+        shapes = [(name, (nfreq, npix), torch.float64) for name in _abi.IMAGE_FIELDS]
+        shapes += [(name, (npix,), torch.float64) for name in _abi.DIAG_FIELDS]
+        shapes += [(name, (npix,), torch.int32) for name in _abi.INT_FIELDS]
+        for name, shape, dt in shapes:
+            t = torch.zeros(shape, dtype=dt, pin_memory=True)
+            pinned.append(t)
+            arrays[name] = t.numpy()
+        return _abi.ImageHostData(npix=npix, nfreq=nfreq, arrays=arrays)
+
+    host = [pinned_host_data() for _ in range(batch)]
     job_list = [(params, model, freqs)] * batch
     e2e_ms = []
     for i in range(args.steps + 1):
