@@ -310,6 +310,12 @@ def config4_section(local, stream, flush, torch):
                     "images_per_s": len(jobs) / tuned_s, "rays_per_s": rays / tuned_s, "launches": tuned_launches}
     res["persistent_default"] = {"seconds": eager_s, "images_per_s": len(jobs) / eager_s,
                                  "rays_per_s": rays / eager_s, "launches": eager_launches}
+    if tuning.graph_cycles == 0:
+        # the launch loop as a CUDA graph (default CTAs and cycles), as config 4 names it
+        timed(_abi.SCHEDULE_GRAPH)
+        graph_s, graph_launches = timed(_abi.SCHEDULE_GRAPH)
+        res["graph_default"] = {"seconds": graph_s, "images_per_s": len(jobs) / graph_s,
+                                "rays_per_s": rays / graph_s, "launches": graph_launches}
     res["autotune"] = {"sample": "the same 64 jobs at 1/4 resolution",
                        "blocks_per_sm": list(tuning.blocks_per_sm), "graph_cycles": tuning.graph_cycles,
                        "candidates": tuning.candidates, "sample_seconds": tuning.seconds,
