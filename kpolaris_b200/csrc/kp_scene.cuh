@@ -154,8 +154,12 @@ struct SceneFarCks : Base {
     __device__ static Ray rhs(const ImageConsts& c, const Ray& X) {
         return Base::template rhs<MIXED, false>(c, X);
     }
-    __device__ static Ray to_phase(const ImageConsts& c, const Ray& S) { return fmks_to_cks(c.fmks, c.spin, S); }
-    __device__ static Ray to_record(const ImageConsts& c, const Ray& S, double x3_ref) {
+    // out of line: conversions happen a few times per ray, and inlined at
+    // each claim, park and finish site they crowd the kernel's registers
+    static __device__ __noinline__ Ray to_phase(const ImageConsts& c, const Ray& S) {
+        return fmks_to_cks(c.fmks, c.spin, S);
+    }
+    static __device__ __noinline__ Ray to_record(const ImageConsts& c, const Ray& S, double x3_ref) {
         return cks_to_fmks(c.fmks, c.spin, S, x3_ref);
     }
 };
