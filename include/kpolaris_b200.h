@@ -648,7 +648,10 @@ int kp_autotune_batch(const kp_riaf_job* jobs, int njobs, const kp_run_options* 
  * synchronisation while other streams are busy (a serving loop, a
  * latency-sensitive pipeline).  Limits: at most KP_NOALLOC_MAX_RAYS pixels
  * summed over the jobs (one 256x256 image) and KP_NOALLOC_MAX_JOBS jobs;
- * larger batches fail with KP_ERR_INVALID before anything runs.  Outputs
+ * larger batches fail with KP_ERR_INVALID before anything runs.  Like
+ * kp_batch_riaf, a batch whose rays still move between the phase kernels
+ * after 24 launch cycles of (far, near-A, near-B) ends with KP_ERR_TIMEOUT
+ * (a 256x256 image takes 2 to 4).  Outputs
  * must be device arrays (options->outputs_on_device = 1); options->stream
  * (NULL: the legacy default stream) carries the work, and the call returns
  * when the images are complete.  The scratch is shared: calls on the same

@@ -35,13 +35,19 @@ int set_error(int code, const char* fmt, ...) {
     return code;
 }
 
+// Prefixes the current error message with the index of the job it concerns
+// (the message is copied first: it is the buffer being formatted into).
+int job_error(int code, int job) {
+    char msg[sizeof(g_error)];
+    std::memcpy(msg, g_error, sizeof(msg));
+    msg[sizeof(msg) - 1] = '\0';
+    return set_error(code, "job %d: %s", job, msg);
+}
+
 int cuda_error(cudaError_t e, const char* what) {
     return set_error(KP_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
 }
 
-// Launches of one wavefront batch run in cycles of (far, near-A, near-B)
-// until no ray is left.
-constexpr int kMaxWaveCycles = 24;
 // engine families (scene x policy) of run_wave_jobs
 enum : int {
     kFamilyRiafFP64 = 0,
@@ -103,6 +109,8 @@ struct DeviceState {
         const void* pool;
         const void* ctrl;
         const void* ids[kPhases][2];
+        const void* sorted;
+        const void* lpt;
         cudaGraphExec_t exec;
     };
     std::vector<GraphEntry> graphs;
@@ -486,11 +494,21 @@ ImageConsts make_consts_grmhd(const kp_pass_a_params* p, const kp_grid* g, const
 
 }  // namespace kp
 
+// Destroys every cached launch graph of a device.  A graph bakes in the
+// addresses of the job table, the ray records, the id queues and the
+// longest-first buffers: it must not outlive any of them, so every
+// reallocation of those buffers calls this first.  The caller holds g_mutex.
+void drop_graphs(DeviceState* dev) {
+    for (auto& g : dev->graphs) cudaGraphExecDestroy(g.exec);
+    dev->graphs.clear();
+}
+
 // Job table storage for njobs descriptors (device table and pinned staging),
 // grow-only.  The caller holds g_mutex.
 int ensure_job_table(DeviceState* dev, int njobs) {
     if (njobs <= dev->jobs_cap) return KP_OK;
     cudaEventSynchronize(dev->staging_free);
+    drop_graphs(dev);
     if (dev->d_jobs) cudaFree(dev->d_jobs);
     if (dev->h_jobs) cudaFreeHost(dev->h_jobs);
     dev->d_jobs = nullptr;
@@ -514,6 +532,7 @@ int run_wave_jobs(DeviceState* dev, cudaStream_t stream, int njobs, long long to
     // ray records and id queues, grow-only
     if (total > dev->pool_cap) {
         cudaStreamSynchronize(stream);
+        drop_graphs(dev);
         cudaFree(dev->d_pool);
         dev->d_pool = nullptr;
         for (auto& q : dev->d_ids) {
@@ -631,12 +650,14 @@ int run_wave_jobs(DeviceState* dev, cudaStream_t stream, int njobs, long long to
         key.jobs = dev->d_jobs;
         key.pool = dev->d_pool;
         key.ctrl = dev->d_ctrl;
+        key.sorted = dev->d_sorted;
+        key.lpt = dev->d_lpt;
         cudaGraphExec_t exec = nullptr;
         for (const auto& g : dev->graphs) {
             if (g.family == key.family && g.nf_max == key.nf_max && g.njobs == key.njobs && g.cycles == key.cycles &&
                 g.total == key.total && std::memcmp(g.blocks, key.blocks, sizeof(key.blocks)) == 0 &&
-                g.jobs == key.jobs && g.pool == key.pool && g.ctrl == key.ctrl &&
-                std::memcmp(g.ids, key.ids, sizeof(key.ids)) == 0) {
+                g.jobs == key.jobs && g.pool == key.pool && g.ctrl == key.ctrl && g.sorted == key.sorted &&
+                g.lpt == key.lpt && std::memcmp(g.ids, key.ids, sizeof(key.ids)) == 0) {
                 exec = g.exec;
                 break;
             }
@@ -1028,11 +1049,11 @@ int kp_batch_riaf(const kp_riaf_job* jobs, int njobs, const kp_run_options* opti
     for (int i = 0; i < njobs; ++i) {
         const kp_riaf_job& jb = jobs[i];
         int st = validate_riaf(&jb.params, &jb.model, jb.frequencies, jb.nfreq);
-        if (st != KP_OK) return set_error(st, "job %d: %s", i, g_error);
+        if (st != KP_OK) return job_error(st, i);
         if (jb.radiation_substeps < 1) return set_error(KP_ERR_INVALID, "job %d: batch radiation_substeps must be positive", i);
         const int npix = jb.params.camera.nx * jb.params.camera.ny;
         st = check_outputs(&jb.out, npix, jb.nfreq);
-        if (st != KP_OK) return set_error(st, "job %d: %s", i, g_error);
+        if (st != KP_OK) return job_error(st, i);
         total += npix;
         nf_max = std::max(nf_max, jb.nfreq);
         scratch += carved_bytes(npix, jb.nfreq);

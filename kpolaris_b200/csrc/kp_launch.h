@@ -135,6 +135,12 @@ cudaError_t launch_seed_grmhd(const JobDesc* jobs, const SeedEntry* entries, con
 cudaError_t launch_grid_to_cells(const float* soa, float* cells, long long ncell, int sms, cudaStream_t stream);
 cudaError_t launch_grid_derived(const GridConsts& g, double* derived, int sms, cudaStream_t stream);
 
+// Launches of one wavefront batch run in cycles of (far, near-A, near-B)
+// until no ray is left; a batch whose rays still move between phases after
+// this many cycles ends with KP_ERR_TIMEOUT (a 256x256 image takes 2 cycles,
+// rays grazing the radiating sphere a few more).
+constexpr int kMaxWaveCycles = 24;
+
 // Threads per CTA of each phase kernel (its __launch_bounds__): the far
 // kernel runs two CTAs of 128 per SM, the near kernels one CTA of 256, so
 // that every resident warp of an SM steps through the same code region.

@@ -17,6 +17,7 @@ namespace kp {
 // Helpers of the C-ABI unit (kp_capi.cu).
 int set_error(int code, const char* fmt, ...);
 int cuda_error(cudaError_t e, const char* what);
+int job_error(int code, int job);
 ImageOutPtrs from_abi(const kp_image_out* o);
 int check_outputs(const kp_image_out* out, int npix, int nfreq);
 int validate_riaf(const kp_pass_a_params* p, const kp_riaf_model* m, const double* freqs, int nfreq);
@@ -25,12 +26,10 @@ ImageConsts make_consts(const kp_pass_a_params* p, const kp_riaf_model* m, const
 
 namespace {
 
-constexpr int kCycles = 24;  // launch cycles of (far, near-A, near-B) before giving up
-
 // Counters of one call, laid out as the batch engine expects them.
 struct NoAllocCtrl {
-    unsigned long long heads[kCycles * kPhases];
-    unsigned counts[kCycles + 1][kPhases];
+    unsigned long long heads[kMaxWaveCycles * kPhases];
+    unsigned counts[kMaxWaveCycles + 1][kPhases];
     int status;
 };
 
@@ -38,6 +37,8 @@ struct NoAllocScratch {
     NoAllocCtrl ctrl;
     JobDesc jobs[KP_NOALLOC_MAX_JOBS];
     unsigned ids[kPhases][2][KP_NOALLOC_MAX_RAYS];
+    unsigned sorted[KP_NOALLOC_MAX_RAYS];  // near-B queue in longest-first order
+    unsigned lpt[512];                     // its bucket counters
     RayRecord pool[KP_NOALLOC_MAX_RAYS];
 };
 
@@ -47,7 +48,7 @@ NoAllocScratch* g_scratch_ptr[64] = {};
 }  // namespace
 }  // namespace kp
 
-// The scratch of every call on a device (32 MB: 464-byte records and six id
+// The scratch of every call on a device (32 MB: 464-byte records and seven id
 // queues for KP_NOALLOC_MAX_RAYS rays, a job table of KP_NOALLOC_MAX_JOBS
 // descriptors, the counters).  Reserved when this unit's module loads, and
 // shared by every call on the device: calls that overlap in time race.
@@ -97,12 +98,12 @@ extern "C" int kp_batch_riaf_noalloc(const kp_riaf_job* jobs, int njobs, const k
     for (int i = 0; i < njobs; ++i) {
         const kp_riaf_job& jb = jobs[i];
         int st = validate_riaf(&jb.params, &jb.model, jb.frequencies, jb.nfreq);
-        if (st != KP_OK) return st;
+        if (st != KP_OK) return job_error(st, i);
         if (jb.radiation_substeps < 1)
             return set_error(KP_ERR_INVALID, "job %d: batch radiation_substeps must be positive", i);
         const int npix = jb.params.camera.nx * jb.params.camera.ny;
         st = check_outputs(&jb.out, npix, jb.nfreq);
-        if (st != KP_OK) return st;
+        if (st != KP_OK) return job_error(st, i);
         total += npix;
         nf_max = std::max(nf_max, jb.nfreq);
     }
@@ -162,7 +163,7 @@ extern "C" int kp_batch_riaf_noalloc(const kp_riaf_job* jobs, int njobs, const k
         const long long needed = (total + wave_threads(phase) - 1) / wave_threads(phase);
         if (blocks[phase] > needed) blocks[phase] = int(needed);
     }
-    for (int cycle = 0; cycle < kCycles; ++cycle) {
+    for (int cycle = 0; cycle < kMaxWaveCycles; ++cycle) {
         for (int phase = 0; phase < kPhases; ++phase) {
             WaveDesc W;
             W.jobs = S->jobs;
@@ -181,6 +182,12 @@ extern "C" int kp_batch_riaf_noalloc(const kp_riaf_job* jobs, int njobs, const k
             W.budget = 0;
             W.status = &S->ctrl.status;
             W.job_done = nullptr;
+            if (phase == kPhaseNearB) {
+                // longest rays first, as kp_batch_riaf orders its near-B queue
+                e = launch_lpt_order(W.in_ids, W.in_count, S->pool, S->lpt, S->sorted, std::max(1, sms), stream);
+                if (e != cudaSuccess) return cuda_error(e, "near-B queue order");
+                W.in_ids = S->sorted;
+            }
             e = mixed ? launch_wave_mixed(phase, W, blocks[phase], wave_threads(phase), stream)
                       : launch_wave_fp64(phase, W, nf_max, blocks[phase], wave_threads(phase), stream);
             if (e != cudaSuccess) return cuda_error(e, "wavefront kernel launch");
@@ -200,5 +207,5 @@ extern "C" int kp_batch_riaf_noalloc(const kp_riaf_job* jobs, int njobs, const k
             return KP_OK;
         }
     }
-    return set_error(KP_ERR_TIMEOUT, "rays still moving between phases after %d launches", kCycles * kPhases);
+    return set_error(KP_ERR_TIMEOUT, "rays still moving between phases after %d launches", kMaxWaveCycles * kPhases);
 }

@@ -26,16 +26,38 @@ PORT_SO = HERE / "libkporacle.so"
 ULP_SO = HERE / "libkporacle_ulp.so"
 REF_SO = HERE / "_ref" / "libkpref.so"
 REF_ULP_SO = HERE / "_ref" / "libkpref_ulp.so"
-REFERENCE_SRC = Path(os.environ.get("KPOLARIS_REFERENCE_SRC", "/root/reference/src"))
+
+
+def _make_vars() -> list:
+    """REFERENCE_SRC for the oracle Makefile when KPOLARIS_REFERENCE_SRC is
+    set; otherwise the Makefile's own default location applies."""
+    src = os.environ.get("KPOLARIS_REFERENCE_SRC")
+    return [f"REFERENCE_SRC={src}"] if src else []
+
+
+def reference_source():
+    """The reference source tree (its src/ directory) the oracle Makefile
+    builds from, or None where it is absent."""
+    r = subprocess.run(["make", "-s", "--no-print-directory", "-C", str(HERE), "print-reference-src"] + _make_vars(),
+                       stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+    p = Path(r.stdout.strip()) if r.returncode == 0 and r.stdout.strip() else None
+    return p if p is not None and p.is_dir() else None
 
 
 def build(reference: bool = True) -> None:
     """Compile the port (always) and the reference oracle (when the reference
-    source tree is present; elsewhere the prebuilt _ref/libkpref.so is used)."""
+    source tree is present; elsewhere the prebuilt _ref files are used)."""
     subprocess.run(["make", "-s", "-C", str(HERE), "all"], check=True)
-    if reference and REFERENCE_SRC.is_dir():
-        subprocess.run(["make", "-s", "-C", str(HERE), "ref",
-                        f"REFERENCE_SRC={REFERENCE_SRC}"], check=True)
+    if reference:
+        subprocess.run(["make", "-s", "-C", str(HERE), "ref-if-present"] + _make_vars(), check=True)
+
+
+def make_ref_target(target: str) -> bool:
+    """Builds one oracle/_ref target from the reference source; False when
+    the source tree is absent or the build fails."""
+    r = subprocess.run(["make", "-s", "-C", str(HERE), target] + _make_vars(),
+                       stdout=subprocess.PIPE, stderr=subprocess.STDOUT)
+    return r.returncode == 0
 
 
 _libs: dict = {}

@@ -17,12 +17,12 @@ import oracle
 ROOT = Path(__file__).resolve().parents[1]
 
 
-@pytest.mark.skipif(not oracle.REFERENCE_SRC.is_dir(), reason="reference source tree not present")
+@pytest.mark.skipif(oracle.reference_source() is None, reason="reference source tree not present")
 def test_host_shim_compiles_links_and_converts(tmp_path):
     exe = tmp_path / "shim_compile"
     lib = ROOT / "kpolaris_b200" / "lib"
     subprocess.run(["g++", "-std=c++20", "-O0", "-fopenmp", "-DKPOLARIS_MAX_FREQUENCIES=4",
-                    f"-I{ROOT / 'oracle' / 'shim'}", f"-I{oracle.REFERENCE_SRC}", f"-I{ROOT / 'include'}",
+                    f"-I{ROOT / 'oracle' / 'shim'}", f"-I{oracle.reference_source()}", f"-I{ROOT / 'include'}",
                     f"-I{ROOT}", "-o", str(exe), str(ROOT / "tests" / "native" / "shim_compile.cpp"),
                     f"-L{lib}", "-lkpolaris_b200", f"-Wl,-rpath,{lib}"], check=True)
     subprocess.run([str(exe)], check=True)

@@ -143,9 +143,10 @@ def exes():
             pytest.skip("library not built")
         kbuild.build_tool()
     if not REF.exists():
-        if not Path("/root/reference/tools").is_dir():
+        import oracle
+
+        if not oracle.make_ref_target("_ref/kpref_options"):
             pytest.skip("oracle/_ref/kpref_options not built and the reference source is absent")
-        subprocess.run(["make", "-s", "-C", str(ROOT / "oracle"), "_ref/kpref_options"], check=True)
     return TOOL, REF
 
 
