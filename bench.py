@@ -57,6 +57,10 @@ def parse():
     ap.add_argument("--serve-requests", type=int, default=48, help="requests of the serving trace (0: skip)")
     ap.add_argument("--serve-rate", type=float, default=20.0, help="Poisson arrival rate of the trace, 1/s")
     ap.add_argument("--serve-plain", type=int, default=1, help="replay the trace on the plain FP64 kernel too")
+    ap.add_argument("--ref-row-stride", type=int, default=8,
+                    help="reference arm: every N-th image row is traced per step")
+    ap.add_argument("--fp64-batched-steps", type=int, default=2,
+                    help="timed steps of the FP64 policy of the batched engine (0: skip)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0,
                     help="target CPU time of the bounded CPU-baseline sample")
     ap.add_argument("--grmhd", type=int, default=1,
@@ -111,6 +115,48 @@ def config_dict(n, path, nfreq, world, batch=1):
 
 
 # ---------------------------------------------------------------- CPU legs
+CPU = {"cores": os.cpu_count() or 1, "logical": os.cpu_count() or 1, "pinning": "none"}
+
+
+def physical_core_first(available, topology_root=Path("/sys/devices/system/cpu")):
+    """The allowed logical CPUs ordered one per physical core first, SMT
+    siblings after (the reference's CPU benchmark policy,
+    scripts/benchmark_image_scaling.py:41-53)."""
+    groups = {}
+    for cpu in sorted(available):
+        base = topology_root / f"cpu{cpu}" / "topology"
+        try:
+            core = (int((base / "physical_package_id").read_text()), int((base / "core_id").read_text()))
+        except (OSError, ValueError):
+            core = ("unknown", cpu)
+        groups.setdefault(core, []).append(cpu)
+    width = max(map(len, groups.values()), default=0)
+    return [cpus[i] for i in range(width) for cpus in groups.values() if i < len(cpus)], len(groups)
+
+
+def pin_physical_cores():
+    """Pins this process to one logical CPU per physical core and sets the
+    OpenMP environment of the CPU oracles (OMP_NUM_THREADS = physical cores,
+    spread over those CPUs), as the reference's benchmark does for its
+    OpenMP backend.  Must run before the oracle libraries load."""
+    try:
+        available = os.sched_getaffinity(0)
+    except AttributeError:
+        return
+    order, ncores = physical_core_first(available)
+    chosen = order[:ncores]
+    try:
+        os.sched_setaffinity(0, chosen)
+    except OSError:
+        return
+    os.environ["OMP_NUM_THREADS"] = str(ncores)
+    os.environ["OMP_PROC_BIND"] = "spread"
+    os.environ["OMP_PLACES"] = "threads"
+    CPU.update(cores=ncores, logical=len(available),
+               pinning=f"physical-core-first: {ncores} threads on CPUs {chosen[0]}..{chosen[-1]} "
+                       f"({ncores} physical cores, {len(available)} logical CPUs allowed), OMP_PROC_BIND=spread")
+
+
 def cpu_sample(params, model, freqs, kind, seconds, threads=0):
     """Times the CPU oracle on evenly spaced image rows until `seconds` of
     wall time are spent (at least one row); returns (images/s, sample text,
@@ -135,7 +181,7 @@ def cpu_sample(params, model, freqs, kind, seconds, threads=0):
     dt = time.perf_counter() - t0
     frac = rows_done * nx / float(nx * ny)
     ips = frac / dt
-    cores = threads if threads > 0 else (os.cpu_count() or 1)
+    cores = threads if threads > 0 else CPU["cores"]
     sample = f"{rows_done} of {ny} rows ({rows_done * nx} pixels, spread over the image), {dt:.2f} s"
     return ips, sample, cores
 
@@ -344,36 +390,64 @@ def config4_section(local, stream, flush, torch):
     return res
 
 
+def reference_rows(ny, stride=8):
+    """The image rows one reference-arm step traces: every `stride`-th row,
+    offset to the middle of its band, the same rows every step."""
+    return list(range(stride // 2, ny, stride))
+
+
 def reference_arm(args):
+    """The reference's own CPU implementation of the path (oracle/_ref: its
+    hot-path templates, OpenMP dynamic over pixels, all physical cores).
+    Each step traces a fixed sample of the benchmark image -- the same
+    `--ref-row-stride`-spaced rows every step -- and is timed by wall clock;
+    ms_per_step is that time, value the image fraction traced per second."""
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
     import oracle
+    from kpolaris_b200 import _abi
 
     params, model, freqs = workload(args.n)
     kind = "reference" if oracle.ref_available() else "port"
-    if kind == "reference":
-        oracle.lib("reference")
+    nx, ny = params.camera.nx, params.camera.ny
+    rows = reference_rows(ny, args.ref_row_stride)
+    out = _abi.ImageHostData.allocate(nx * ny, len(freqs))
+    import numpy as np
+
+    pixels = np.concatenate([np.arange(j * nx, (j + 1) * nx) for j in rows]).astype(np.int32)
+
+    def step():
+        t0 = time.perf_counter()
+        if kind == "reference":
+            # one dynamic loop over every pixel of the sample
+            oracle.image_riaf_pixels(params, model, freqs, pixels, threads=0, out=out)
+        else:
+            for j in rows:
+                oracle.image_riaf(params, model, freqs, kind=kind, threads=0, pixel_begin=j * nx,
+                                  pixel_end=(j + 1) * nx, out=out)
+        return time.perf_counter() - t0
+
     for _ in range(max(0, args.warmup)):
-        cpu_sample(params, model, freqs, kind, seconds=0.0)
-    vals = []
-    samples = []
-    per = max(2.0, args.cpu_seconds / max(1, args.steps))
-    cores = os.cpu_count() or 1
-    for _ in range(args.steps):
-        v, s, cores = cpu_sample(params, model, freqs, kind, seconds=per)
-        vals.append(v)
-        samples.append(s)
-    value = statistics.median(vals)
+        step()
+    step_s = [step() for _ in range(args.steps)]
+    mean_s = sum(step_s) / len(step_s)
+    frac = len(rows) / float(ny)
+    value = frac / mean_s
+    sample = (f"{len(rows)} of {ny} rows per step (every {args.ref_row_stride}th, from row {rows[0]}; "
+              f"{len(rows) * nx} pixels = {frac:.4f} image) in one OpenMP dynamic loop, the same rows every "
+              f"step, wall clock; "
+              f"{CPU['pinning']}")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 / value,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": mean_s * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (analytic RIAF plasma)",
-        "config": config_dict(args.n, "reference CPU (OpenMP dynamic over pixels)", len(freqs), 1, 1),
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
-                         "sample": samples[-1]},
+        "config": {**config_dict(args.n, "reference CPU (OpenMP dynamic over pixels)", len(freqs), 1, 1),
+                   "images_per_step": frac, "l2": "n/a (CPU)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": CPU["cores"], "kind": kind, "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "step_s": {"min": min(step_s), "max": max(step_s)},
     }
     print(json.dumps(line), flush=True)
     return 0
@@ -730,6 +804,35 @@ def ours_arm(args):
     evpa_err = [abs((g[1] - r[1] + 90.0) % 180.0 - 90.0) for g, r in zip(got_int, ref_int)]
     reason_match = float(np.mean(outs[0][1][2][2].cpu().numpy() == plain_out[1][2][2].cpu().numpy()))
 
+    # ---- the FP64 policy of the same batched engine on the same step: splits
+    # the speed-up over the plain kernel into engine and precision
+    fp64_batched = None
+    if mixed and args.fp64_batched_steps > 0:
+        progress("FP64 policy of the batched engine")
+        opt64 = kp._options(precision=_abi.PRECISION_FP64, schedule=_abi.SCHEDULE_PERSISTENT, device=local)
+        opt64.outputs_on_device = 1
+        opt64.stream = C.c_void_p(stream.cuda_stream)
+        stats64 = _abi.BatchStats()
+        kp.check(lib.kp_batch_riaf(jobs, batch, C.byref(opt64), C.byref(stats64)))
+        torch.cuda.synchronize()
+        b64_ms = []
+        for _ in range(args.fp64_batched_steps):
+            flush.fill_(1.0)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            kp.check(lib.kp_batch_riaf(jobs, batch, C.byref(opt64), C.byref(stats64)))
+            e1.record(stream)
+            torch.cuda.synchronize()
+            b64_ms.append(e0.elapsed_time(e1))
+        b64 = sum(b64_ms) / len(b64_ms)
+        same = all(torch.equal(a, b) for a, b in zip(outs[0][1][0], plain_out[1][0]))
+        fp64_batched = {"images_per_s": world * batch * 1000.0 / b64, "ms_per_step": b64, "images_per_step": batch,
+                        "steps": args.fp64_batched_steps,
+                        "stokes_bit_identical_to_plain": bool(same),
+                        "path": "kp_batch_riaf, FP64 policy (wavefront engine, the reference's arithmetic)"}
+
+
     progress("e2e")
     # ---- e2e: the same batch through the public API with host buffers in
     # pinned memory (the library copies each output array device-to-host)
@@ -843,7 +946,7 @@ def ours_arm(args):
 
         kind = "reference" if oracle.ref_available() else "port"
         v, sample, cores = cpu_sample(params, model, freqs, kind, seconds=args.cpu_seconds)
-        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": f"{sample}; {CPU['pinning']}"}
 
     if rank == 0:
         srt = sorted(step_ms)
@@ -857,24 +960,33 @@ def ours_arm(args):
             "e2e": {"value": world * batch * 1000.0 / e2e, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": launches[0],
-            "plain_fp64": {"images_per_s": world * 1000.0 / plain_img_ms, "ms_per_image": plain_img_ms,
-                           "kernel": "image_fp64_per_pixel (one image per launch)"},
-            "speedup_vs_plain_fp64": value / (world * 1000.0 / plain_img_ms),
-            "accuracy_vs_fp64": {"total_flux_rel_err": flux_err, "evpa_err_deg": evpa_err,
-                                 "reason_agreement": reason_match,
-                                 "frequencies_ghz": [f * 1e-9 for f in freqs]},
+            "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
+            # the secondary workloads (bulky) before the north-star numbers,
+            # which close the line
+            "serving": serving,
+            "grmhd": grmhd,
+            "config4": config4,
+            "analysis": analysis,
+            "phases": phases,
+            "rays_per_s": value * npix,
+            "geodesic_steps_per_s": value * steps_per_image,
             "step_latency_ms": {"p50": float(np.percentile(srt, 50)), "p99": float(np.percentile(srt, 99))},
             "latency_ms": ({"p50": serving["mixed_batched"]["p50_s"] * 1e3,
                             "p99": serving["mixed_batched"]["p99_s"] * 1e3, "source": "serving trace"}
                            if serving else None),
-            "serving": serving,
-            "rays_per_s": value * npix,
-            "geodesic_steps_per_s": value * steps_per_image,
-            "phases": phases, "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
-            "grmhd": grmhd,
-            "config4": config4,
-            "analysis": analysis,
+            "accuracy_vs_fp64": {"total_flux_rel_err": flux_err, "evpa_err_deg": evpa_err,
+                                 "reason_agreement": reason_match,
+                                 "frequencies_ghz": [f * 1e-9 for f in freqs]},
+            "plain_fp64": {"images_per_s": world * 1000.0 / plain_img_ms, "ms_per_image": plain_img_ms,
+                           "kernel": "image_fp64_per_pixel (one image per launch)"},
+            "fp64_batched": fp64_batched,
+            "speedup_vs_plain_fp64": value / (world * 1000.0 / plain_img_ms),
         }
+        if fp64_batched:
+            # engine gain (FP64 batched / plain) x precision gain (mixed / FP64 batched)
+            line["speedup_split"] = {
+                "engine": fp64_batched["images_per_s"] / (world * 1000.0 / plain_img_ms),
+                "precision": value / fp64_batched["images_per_s"]}
         print(json.dumps(line), flush=True)
     if pg:
         pg.barrier()
@@ -904,6 +1016,7 @@ def grmhd_only(args):
 
 def main():
     args = parse()
+    pin_physical_cores()
     if args.grmhd_only:
         return grmhd_only(args)
     if args.impl == "reference":

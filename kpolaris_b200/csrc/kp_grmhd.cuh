@@ -327,8 +327,8 @@ KP_HD bool series_holds(const ImageConsts& c, double t) {
     return t >= c.series_times[0] && t <= c.series_times[c.nseries - 1];
 }
 
-static __device__ __noinline__ GrmhdSample grmhd_sample_series(const ImageConsts& c, const Ray& s) {
-    const double t = series_time(c, s);
+KP_HD int series_bracket(const ImageConsts& c, double x0, double& f) {
+    const double t = c.t_obs + x0;
     int lo = 0, hi = c.nseries - 1;
     while (lo + 1 < hi) {
         const int mid = lo + (hi - lo) / 2;
@@ -337,9 +337,15 @@ static __device__ __noinline__ GrmhdSample grmhd_sample_series(const ImageConsts
     }
     const double t0 = c.series_times[lo], t1 = c.series_times[lo + 1];
     const double denom = t1 - t0;
-    double f = 0.0;
-    if (abs_val(denom) > kTiny) f = (c.t_obs + s.x.v[0] - t0) / denom;
+    f = 0.0;
+    if (abs_val(denom) > kTiny) f = (c.t_obs + x0 - t0) / denom;
     f = min_val(1.0, max_val(0.0, f));
+    return lo;
+}
+
+static __device__ __noinline__ GrmhdSample grmhd_sample_series(const ImageConsts& c, const Ray& s) {
+    double f;
+    const int lo = series_bracket(c, s.x.v[0], f);
     if (f <= 0.0) return grmhd_sample_from(c, s, c.series[lo], nullptr, 0.0);
     if (f >= 1.0) return grmhd_sample_from(c, s, c.series[lo + 1], nullptr, 0.0);
     return grmhd_sample_from(c, s, c.series[lo], &c.series[lo + 1], f);

@@ -159,6 +159,29 @@ def image_riaf(params, model, freqs, *, kind="port", integrator=0, threads=0,
     return out
 
 
+def image_riaf_pixels(params, model, freqs, pixels, *, kind="reference", threads=0, out=None):
+    """The listed pixels of a RIAF image through the reference's templates
+    in one OpenMP dynamic loop (outputs at their image positions)."""
+    if kind not in ("reference", "reference_ulp"):
+        raise ValueError("pixel lists run through the reference oracle")
+    L = lib(kind)
+    L.kpref_image_riaf_pixels.argtypes = [
+        C.POINTER(_abi.PassAParams), C.POINTER(_abi.RIAFModel), C.c_int, C.POINTER(C.c_double), C.c_int,
+        C.c_int, C.POINTER(C.c_int), C.c_int, C.POINTER(_abi.ImageOut)]
+    npix = params.camera.nx * params.camera.ny
+    nfreq = len(freqs)
+    if out is None:
+        out = _abi.ImageHostData.allocate(npix, nfreq)
+    px = np.ascontiguousarray(pixels, dtype=np.int32)
+    fa = (C.c_double * nfreq)(*freqs)
+    s = out.as_struct()
+    rc = L.kpref_image_riaf_pixels(C.byref(params), C.byref(model), 1, fa, nfreq, int(threads),
+                                   px.ctypes.data_as(C.POINTER(C.c_int)), len(px), C.byref(s))
+    if rc != 0:
+        raise RuntimeError(L.kpref_last_error().decode())
+    return out
+
+
 def image_riaf_analysis(params, model, config=None, *, kind="reference", threads=0, pixel_begin=0,
                         pixel_end=None, out=None, analysis=None):
     """Analysis-mode RIAF image (or a pixel range of it) through the
@@ -223,6 +246,48 @@ def transport_rhs_cks(mass, spin, state16, kind="port"):
     out = (C.c_double * 16)()
     getattr(L, _prefix(kind) + "transport_rhs_cks")(mass, spin, st, out)
     return np.array(out[:])
+
+
+def adaptive_step_cks(integrator, mass, spin, state16, h, tolerance, min_step, max_step, max_attempts=10,
+                      kind="port"):
+    """One adaptive attempt sequence on the Cartesian Kerr-Schild metric:
+    integrator 0 step doubling (adaptive_rk4_step), 1 Cash-Karp
+    (adaptive_rkf45_endpoint_step).  Returns (accepted, state16, mid16,
+    used_h, next_h, error)."""
+    L = lib(kind)
+    fn = getattr(L, _prefix(kind) + "adaptive_step_cks")
+    fn.argtypes = [C.c_int, C.c_double, C.c_double, C.POINTER(C.c_double), C.c_double, C.c_double, C.c_double,
+                   C.c_double, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    st = (C.c_double * 16)(*state16)
+    out = (C.c_double * 32)()
+    sc = (C.c_double * 3)()
+    acc = fn(int(integrator), float(mass), float(spin), st, float(h), float(tolerance), float(min_step),
+             float(max_step), int(max_attempts), out, sc)
+    o = np.array(out[:])
+    return int(acc), o[:16], o[16:], sc[0], sc[1], sc[2]
+
+
+def slow_light_sampling(times, t_obs, x0, a, b, kind="reference"):
+    """The reference's slow-light time sampling for sample coordinate times
+    x0: (snapshot window, clamped fraction, interpolate_time_value(a, b, f))
+    per sample (ref_driver.cpp kpref_slow_light_sampling)."""
+    L = lib(kind)
+    fn = L.kpref_slow_light_sampling
+    P = C.POINTER
+    fn.argtypes = [P(C.c_double), C.c_int, C.c_double, P(C.c_double), P(C.c_double), P(C.c_double), C.c_int,
+                   P(C.c_int), P(C.c_double), P(C.c_double)]
+    t = np.ascontiguousarray(times, dtype=np.float64)
+    x = np.ascontiguousarray(x0, dtype=np.float64)
+    aa = np.ascontiguousarray(a, dtype=np.float64)
+    bb = np.ascontiguousarray(b, dtype=np.float64)
+    n = len(x)
+    w = np.zeros(n, dtype=np.int32)
+    f = np.zeros(n)
+    v = np.zeros(n)
+    rc = fn(_dp(t), len(t), float(t_obs), _dp(x), _dp(aa), _dp(bb), n, w.ctypes.data_as(P(C.c_int)), _dp(f), _dp(v))
+    if rc != 0:
+        raise RuntimeError(L.kpref_last_error().decode())
+    return w, f, v
 
 
 def _declare_grmhd(L):

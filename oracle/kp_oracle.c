@@ -1734,3 +1734,26 @@ int kpo_transport_rhs_cks(double mass, double spin, const double* state16, doubl
     ts_to(&d, d16);
     return KP_OK;
 }
+
+/* One adaptive attempt sequence from state16 with signed step requested_h:
+ * step doubling (adaptive_rk4_step, rk4.hpp:108-161) or Cash-Karp
+ * (adaptive_rkf45_endpoint_step, rk4.hpp:164-250).  out16x2: the state and
+ * the mid state; scalars: used_h, next_h, error; returns accepted. */
+int kpo_adaptive_step_cks(int integrator, double mass, double spin, const double* state16, double requested_h,
+                          double tolerance, double min_step, double max_step, int max_attempts,
+                          double* out32, double* scalars3) {
+    const KS m = {mass, spin};
+    const TS s = ts_from(state16);
+    ACtl ctl;
+    ctl.tolerance = tolerance;
+    ctl.min_step = min_step;
+    ctl.max_step = max_step;
+    ctl.max_attempts = max_attempts;
+    const AStep r = adaptive_step(integrator, &m, &s, requested_h, ctl);
+    ts_to(&r.state, out32);
+    ts_to(&r.mid_state, out32 + 16);
+    scalars3[0] = r.used_h;
+    scalars3[1] = r.next_h;
+    scalars3[2] = r.error;
+    return r.accepted;
+}

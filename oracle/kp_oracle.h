@@ -34,6 +34,9 @@ int kpo_riaf_coefficients_cks(double mass, double spin, const kp_riaf_model* mod
                               const double* state16, double* out11);
 int kpo_camera_ray_cks(const kp_pass_a_params* params, int pixel, double* state16);
 int kpo_transport_rhs_cks(double mass, double spin, const double* state16, double* d16);
+int kpo_adaptive_step_cks(int integrator, double mass, double spin, const double* state16, double requested_h,
+                          double tolerance, double min_step, double max_step, int max_attempts,
+                          double* out32, double* scalars3);
 const char* kpo_last_error(void);
 
 #ifdef __cplusplus

@@ -17,6 +17,7 @@
 
 #include "geodesic/pass_b.hpp"
 #include "image/analysis_driver.hpp"
+#include "image/slow_light_driver.hpp"
 #include "geometry/kerr_boyer_lindquist.hpp"
 #include "geometry/kerr_fmks.hpp"
 #include "geometry/kerr_schild_cartesian.hpp"
@@ -126,10 +127,12 @@ template<class Metric, class Model>
 void run_metric(const kpolaris::PassAParams<Real>& pa,
                 const Model& model,
                 int radiation_substeps, const double* freqs, int nfreq,
-                const Metric& metric, int pixel_begin, int pixel_end, kp_image_out* out) {
+                const Metric& metric, int pixel_begin, int pixel_end, kp_image_out* out,
+                const int* pixel_list = nullptr) {
     const int npix = pa.camera.nx * pa.camera.ny;
 #pragma omp parallel for schedule(dynamic)
-    for (int pixel = pixel_begin; pixel < pixel_end; ++pixel) {
+    for (int slot = pixel_begin; slot < pixel_end; ++slot) {
+        const int pixel = pixel_list ? pixel_list[slot] : slot;
 #ifdef KPREF_PERTURB_LIBM
         kpref_ulp::seed_pixel(pixel);
 #endif
@@ -566,6 +569,32 @@ int kpref_image_riaf_range(const kp_pass_a_params* params, const kp_riaf_model* 
     return KP_OK;
 }
 
+// The pixels pixel_list[0, n) of a RIAF image in one OpenMP dynamic loop
+// (the benchmark's bounded sample of spread-out rows, without a barrier per
+// row); outputs at their image positions.
+int kpref_image_riaf_pixels(const kp_pass_a_params* params, const kp_riaf_model* model, int radiation_substeps,
+                            const double* freqs, int nfreq, int threads, const int* pixel_list, int n,
+                            kp_image_out* out) {
+    if (!params || !model || !out || (n > 0 && !pixel_list)) return fail("null argument");
+    if (nfreq < 1 || nfreq > KPOLARIS_MAX_FREQUENCIES) return fail("nfreq out of range");
+    const int npix = params->camera.nx * params->camera.ny;
+    for (int i = 0; i < n; ++i)
+        if (pixel_list[i] < 0 || pixel_list[i] >= npix) return fail("pixel index out of bounds");
+    if (threads > 0) omp_set_num_threads(threads);
+    const auto pa = to_pass_a(*params);
+    const auto riaf = to_riaf(*model);
+    if (pa.coordinate_system == kpolaris::CoordinateSystem::CartesianKS) {
+        const kpolaris::KerrSchildInMetric<Real> metric(pa.mass, pa.spin);
+        run_metric(pa, riaf, radiation_substeps, freqs, nfreq, metric, 0, n, out, pixel_list);
+    } else if (pa.coordinate_system == kpolaris::CoordinateSystem::BoyerLindquist) {
+        const kpolaris::KerrBoyerLindquistMetric<Real> metric(pa.mass, pa.spin);
+        run_metric(pa, riaf, radiation_substeps, freqs, nfreq, metric, 0, n, out, pixel_list);
+    } else {
+        return fail("coordinate system not built in the reference oracle");
+    }
+    return KP_OK;
+}
+
 // Analysis mode: pixels [pixel_begin, pixel_end) of a single-frequency RIAF
 // image through the reference's per-pixel analysis function
 // (trace_pass_b_segment_model_analysis_pixel_metric,
@@ -756,6 +785,79 @@ int kpref_transport_rhs_cks(double mass, double spin, const double* state16, dou
         d16[4 + mu] = d.k[mu];
         d16[8 + mu] = d.e1[mu];
         d16[12 + mu] = d.e2[mu];
+    }
+    return KP_OK;
+}
+
+// One adaptive attempt sequence with the reference's own steppers
+// (adaptive_rk4_step, rk4.hpp:108-161, and adaptive_rkf45_endpoint_step,
+// rk4.hpp:164-250) on the Cartesian Kerr-Schild metric.  out32: the state and
+// the mid state; scalars3: used_h, next_h, error; returns accepted.
+int kpref_adaptive_step_cks(int integrator, double mass, double spin, const double* state16, double requested_h,
+                            double tolerance, double min_step, double max_step, int max_attempts,
+                            double* out32, double* scalars3) {
+    const kpolaris::KerrSchildInMetric<Real> metric(mass, spin);
+    kpolaris::TransportState<Real> s;
+    for (int mu = 0; mu < 4; ++mu) {
+        s.x[mu] = state16[mu];
+        s.k[mu] = state16[4 + mu];
+        s.e1[mu] = state16[8 + mu];
+        s.e2[mu] = state16[12 + mu];
+    }
+    kpolaris::AdaptiveRK4Control<Real> ctl;
+    ctl.tolerance = tolerance;
+    ctl.min_step = min_step;
+    ctl.max_step = max_step;
+    ctl.max_attempts = max_attempts;
+    const auto r = integrator == KP_INTEGRATOR_CASH_KARP
+                       ? kpolaris::adaptive_rkf45_endpoint_step(metric, s, requested_h, ctl)
+                       : kpolaris::adaptive_rk4_step(metric, s, requested_h, ctl);
+    for (int mu = 0; mu < 4; ++mu) {
+        out32[mu] = r.state.x[mu];
+        out32[4 + mu] = r.state.k[mu];
+        out32[8 + mu] = r.state.e1[mu];
+        out32[12 + mu] = r.state.e2[mu];
+        out32[16 + mu] = r.mid_state.x[mu];
+        out32[20 + mu] = r.mid_state.k[mu];
+        out32[24 + mu] = r.mid_state.e1[mu];
+        out32[28 + mu] = r.mid_state.e2[mu];
+    }
+    scalars3[0] = r.used_h;
+    scalars3[1] = r.next_h;
+    scalars3[2] = r.error;
+    return r.accepted;
+}
+
+// Slow-light time sampling with the reference's own code: for each sample
+// coordinate time x0[i], the resident snapshot pair a decoupled window
+// kernel reads (SlowLightResidentWindows::sample_window,
+// slow_light_driver.hpp:1002-1013, at coefficient_time = t_obs + x^0, :1298),
+// the clamped fraction of the pair's temporal model
+// (SlowLightTemporalModel::interpolation_fraction, :62-69, built by
+// SlowLightResidentWindows::model, :1019-1026) and interpolate_time_value
+// (model/time_interpolation.hpp:27-32) of (a[i], b[i]) at that fraction.
+int kpref_slow_light_sampling(const double* times, int nsnap, double t_obs, const double* x0, const double* a,
+                              const double* b, int n, int* window, double* fraction, double* value) {
+    using Model = kpolaris::GRMHDGridRadiationModel<Real>;
+    if (nsnap < 2) return fail("slow-light sampling needs at least two snapshots");
+    kpolaris_image_detail::SlowLightResidentWindows<Kokkos::DefaultExecutionSpace, Real, Model> w;
+    w.models = Kokkos::View<Model*, Kokkos::DefaultExecutionSpace>("models", std::size_t(nsnap));
+    w.times = Kokkos::View<Real*, Kokkos::DefaultExecutionSpace>("times", std::size_t(nsnap));
+    for (int k = 0; k < nsnap; ++k) w.times(k) = times[k];
+    w.observer_time = t_obs;
+    w.first = 0;
+    w.last = nsnap - 1;
+    w.step_mode = kpolaris::SlowLightStepMode::decoupled;
+    w.interpolation = kpolaris::SlowLightInterpolation::fluid;
+    for (int i = 0; i < n; ++i) {
+        kpolaris::TransportState<Real> s{};
+        s.x[0] = x0[i];
+        const Real coefficient_time = w.observation_time() + s.x[0];
+        const int k = w.sample_window(coefficient_time, 0);
+        const auto temporal = w.model(k);
+        window[i] = k;
+        fraction[i] = temporal.interpolation_fraction(s);
+        value[i] = kpolaris::interpolate_time_value(a[i], b[i], fraction[i]);
     }
     return KP_OK;
 }

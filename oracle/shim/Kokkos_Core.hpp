@@ -4,8 +4,8 @@
 // image drivers of src/image and src/diagnostics) on the CPU as the parity
 // oracle.  It provides what those headers use: KOKKOS_INLINE_FUNCTION, the
 // Kokkos:: math forwards, reference-counted host Views of rank 1 and 2, and a
-// serial stand-in for the execution API (parallel_for over a RangePolicy in
-// index order, fence, deep_copy, Timer).  Test infrastructure; never linked
+// serial stand-in for the execution API (parallel_for and parallel_reduce over
+// a RangePolicy in index order, fence, deep_copy, mirrors, Timer).  Test infrastructure; never linked
 // into the product.
 #pragma once
 
@@ -67,6 +67,8 @@ template<class T> inline T atan2(T y, T x) { return KPREF_P(std::atan2(y, x)); }
 template<class T> inline T floor(T x) { return std::floor(x); }
 template<class T> inline T ceil(T x) { return std::ceil(x); }
 template<class T, class U> inline auto pow(T x, U y) { return KPREF_P(std::pow(x, y)); }
+template<class T> inline bool isfinite(T x) { return std::isfinite(x); }
+template<class T> inline bool isnan(T x) { return std::isnan(x); }
 
 inline void abort(const char* msg) {
     std::fprintf(stderr, "Kokkos::abort: %s\n", msg);
@@ -195,6 +197,26 @@ struct Timer {
 template<class Space, class V>
 inline V create_mirror_view_and_copy(const Space&, const V& v) {
     return v;
+}
+template<class V>
+inline V create_mirror_view(const V& v) {
+    return v;
+}
+
+// Serial sum reduction (the slow-light driver's active-ray count).
+template<class... Args, class F, class T>
+inline void parallel_reduce(const std::string&, const RangePolicy<Args...>& policy, const F& f, T& result) {
+    T acc = T();
+    for (long long i = policy.begin; i < policy.end; ++i) f(static_cast<int>(i), acc);
+    result = acc;
+}
+template<class... Args, class F, class T>
+inline void parallel_reduce(const RangePolicy<Args...>& policy, const F& f, T& result) {
+    parallel_reduce(std::string(), policy, f, result);
+}
+template<class F, class T>
+inline void parallel_reduce(const std::string& name, long long n, const F& f, T& result) {
+    parallel_reduce(name, RangePolicy<>(0, n), f, result);
 }
 
 } // namespace Kokkos

@@ -18,6 +18,25 @@ libm conditioning measured on the reference's own templates
 
     python tests/golden/make_golden.py --grmhd     # GRMHD fixtures only
     python tests/golden/make_golden.py --slow      # slow-light fixtures only
+    python tests/golden/make_golden.py --steps     # adaptive step fixture only
+    python tests/golden/make_golden.py --sampling  # slow-light sampling fixture only
+
+The slow-light sampling fixture (slow_sampling.npz) stores 16 distinct,
+unevenly spaced snapshot times, two observation times, seeded sample
+coordinate times x0 (random over and beyond the resident range, exactly at
+each snapshot time and one ulp either side of it) and value pairs (a, b),
+and the reference's snapshot window, interpolation fraction and
+interpolated value for each (SlowLightResidentWindows::sample_window,
+SlowLightTemporalModel::interpolation_fraction, interpolate_time_value).
+
+The adaptive step fixture (adaptive_steps.npz) stores seeded transport
+states taken along camera rays (the reference's own step-doubling stepper
+carries each ray inward from r = 1000 M, every 14th state kept, every
+one inside r = 30 M, 3000 of them drawn), a signed
+requested step, a tolerance, a step floor and an attempt limit for each, and the reference's results of
+one adaptive attempt sequence with step doubling (adaptive_rk4_step) and
+with Cash-Karp (adaptive_rkf45_endpoint_step): accepted flag, state, mid
+state, used_h, next_h, error.
 
 Each slow-light fixture (slow_*.npz, SLOW_CASES) stores the case, the sha256
 of every snapshot's primitives, the reference image arrays (the reference's
@@ -82,8 +101,96 @@ def make_slow():
               {cond_key(k): "%.1e" % cond[k] for k in keys if k[0] in ("flux", "image_i")})
 
 
+def make_steps():
+    from kpolaris_b200 import configs
+
+    params, _, _ = configs.config2(48, 48)
+    mass, spin = params.mass, params.spin
+    rng = np.random.default_rng(4051)
+    states = []
+    # wide-field rays (most escape) and rays aimed at the hole (captured or
+    # skimming the photon ring)
+    rays = [(0.5, int(p)) for p in rng.choice(48 * 48, size=16, replace=False)]
+    rays += [(0.03, int(p)) for p in rng.choice(48 * 48, size=40, replace=False)]
+    for fov, pixel in rays:
+        params.camera.fov = fov
+        s16 = oracle.camera_ray_cks(params, pixel, kind="reference")
+        h = -0.5
+        for n in range(2400):
+            acc, nxt, _, used, h, _ = oracle.adaptive_step_cks(0, mass, spin, s16, h, 1e-8, 1e-10, 2.0,
+                                                               kind="reference")
+            if not acc or not np.all(np.isfinite(nxt)):
+                break
+            r2 = nxt[1] ** 2 + nxt[2] ** 2 + nxt[3] ** 2
+            if n % 14 == 0 or r2 < 30.0 ** 2:
+                states.append(nxt)
+            s16 = nxt
+            if r2 < 1.2 ** 2 or r2 > 1100.0 ** 2:
+                break
+    states = np.array(states)
+    states = states[np.sort(rng.choice(len(states), size=min(3000, len(states)), replace=False))]
+    n = len(states)
+    h = rng.choice([-1.0, 1.0], size=n) * 10.0 ** rng.uniform(-3.0, 0.7, size=n)
+    tol = rng.choice([1e-6, 1e-8, 1e-10, 1e-12], size=n)
+    # long steps at tight tolerances inside r = 30 M: rejected attempts
+    r = np.sqrt(np.sum(states[:, 1:4] ** 2, axis=1))
+    hard = (r < 30.0) & (rng.uniform(size=n) < 0.5)
+    h = np.where(hard, np.sign(h) * 2.0, h)
+    tol = np.where(hard, rng.choice([1e-10, 1e-12, 1e-14], size=n), tol)
+    # a quarter of the items give up early: few attempts, or a floor the
+    # shrinking step reaches (the exhausted-sequence branch)
+    max_attempts = np.where(rng.uniform(size=n) < 0.25, rng.integers(1, 3, size=n), 10).astype(np.int32)
+    min_step = np.where(rng.uniform(size=n) < 0.15, 0.2, 1e-10)
+    out = {}
+    for integ, tag in ((0, "sd"), (1, "ck")):
+        acc, st, mid, sc = [], [], [], []
+        for i in range(n):
+            a, s16, m16, used, nxt, err = oracle.adaptive_step_cks(integ, mass, spin, states[i], h[i], tol[i],
+                                                                  min_step[i], 2.0, int(max_attempts[i]),
+                                                                  kind="reference")
+            acc.append(a)
+            st.append(s16)
+            mid.append(m16)
+            sc.append([used, nxt, err])
+        out[f"{tag}_accepted"] = np.array(acc, dtype=np.int32)
+        out[f"{tag}_state"] = np.array(st)
+        out[f"{tag}_mid"] = np.array(mid)
+        out[f"{tag}_scalars"] = np.array(sc)
+    np.savez_compressed(OUT / "adaptive_steps.npz", mass=mass, spin=spin, states=states, h=h, tol=tol,
+                        min_step=min_step, max_step=2.0, max_attempts=max_attempts, **out)
+    for tag in ("sd", "ck"):
+        clamp = np.minimum(np.maximum(np.abs(h), min_step), 2.0)
+        shrunk = (out[f"{tag}_accepted"] == 1) & (np.abs(out[f"{tag}_scalars"][:, 0]) < clamp)
+        print("adaptive_steps", tag, n, "states; accepted", int(out[f"{tag}_accepted"].sum()),
+              "after a rejection", int(shrunk.sum()), "exhausted", int((out[f"{tag}_accepted"] == 0).sum()))
+
+
+def make_sampling():
+    rng = np.random.default_rng(7001)
+    times = np.cumsum(np.concatenate([[40.0], rng.uniform(4.0, 16.0, size=15)]))
+    times[7] = times[6] + 1e-3  # two snapshots close together
+    cases = {}
+    for tag, t_obs in (("obs0", 0.0), ("obs1", 1234.5)):
+        x_rand = rng.uniform(times[0] - t_obs - 25.0, times[-1] - t_obs + 25.0, size=2000)
+        exact = times - t_obs
+        x0 = np.concatenate([x_rand, exact, np.nextafter(exact, -np.inf), np.nextafter(exact, np.inf)])
+        a = rng.normal(size=len(x0)) * 10.0 ** rng.uniform(-3, 3, size=len(x0))
+        b = np.where(rng.uniform(size=len(x0)) < 0.1, a, a * (1.0 + rng.normal(size=len(x0)) * 0.2))
+        w, f, v = oracle.slow_light_sampling(times, t_obs, x0, a, b)
+        cases.update({f"{tag}_t_obs": t_obs, f"{tag}_x0": x0, f"{tag}_a": a, f"{tag}_b": b, f"{tag}_window": w,
+                      f"{tag}_fraction": f, f"{tag}_value": v})
+        print("slow_sampling", tag, len(x0), "samples; fractions in (0, 1):", int(((f > 0) & (f < 1)).sum()))
+    np.savez_compressed(OUT / "slow_sampling.npz", times=times, **cases)
+
+
 def main():
     oracle.build(reference=True)
+    if "--sampling" in sys.argv[1:]:
+        make_sampling()
+        return
+    if "--steps" in sys.argv[1:]:
+        make_steps()
+        return
     if "--grmhd" in sys.argv[1:]:
         make_grmhd()
         return
@@ -111,6 +218,8 @@ def main():
     print("coefficients", len(th_in), len(tr_in))
     make_grmhd()
     make_slow()
+    make_steps()
+    make_sampling()
 
 
 if __name__ == "__main__":

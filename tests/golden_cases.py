@@ -106,7 +106,7 @@ def libm_conditioning(name, seeds=(1, 2, 3)):
     return libm_conditioning_of(params, model, freqs, fx, seeds)
 
 
-def libm_conditioning_of(params, model, freqs, ref, seeds=(1, 2, 3), integrator=0):
+def libm_conditioning_of(params, model, freqs, ref, seeds=(1, 2, 3), integrator=0, threads=4):
     """How well double precision determines an image (`ref`: its reference
     result, a mapping of the output fields): per (channel, frequency) the
     largest normwise change, per frequency ("flux", f) the relative change
@@ -123,7 +123,7 @@ def libm_conditioning_of(params, model, freqs, ref, seeds=(1, 2, 3), integrator=
 
     def run(seed):
         oracle.set_libm_perturbation(seed)
-        return oracle.image_riaf(params, model, freqs, kind="port_ulp", threads=4, integrator=integrator)
+        return oracle.image_riaf(params, model, freqs, kind="port_ulp", threads=threads, integrator=integrator)
 
     return conditioning_over(run, ref, seeds)
 
