@@ -47,8 +47,8 @@ struct LaneState {
 };
 static_assert(sizeof(LaneState) <= sizeof(((RayRecord*)nullptr)->st), "LaneState must fit its record slot");
 
-__device__ __forceinline__ void begin_adaptive(LaneState& L, double requested, double min_step,
-                                               double max_step) {
+template<class LS>
+__device__ __forceinline__ void begin_adaptive(LS& L, double requested, double min_step, double max_step) {
     L.req_h = requested;
     L.ctl_min = min_step;
     L.ctl_max = max_step;
@@ -76,7 +76,8 @@ __device__ __forceinline__ double accepted_next_h(double h, double err, double t
 // A rejected attempt: shrink and retry, or give up (rk4.hpp:143-160).
 // Returns 1 when the sequence is exhausted; L.h_current then holds the
 // signed next_h of the failed sequence.
-__device__ __forceinline__ int rejected_attempt(LaneState& L, double err, double tol) {
+template<class LS>
+__device__ __forceinline__ int rejected_attempt(LS& L, double err, double tol) {
     L.attempt += 1;
     int exhausted = L.attempt >= 10;
     if (abs_val(L.h_try) <= L.ctl_min * 1.0001) {
@@ -93,8 +94,8 @@ __device__ __forceinline__ int rejected_attempt(LaneState& L, double err, double
     return exhausted;
 }
 
-__device__ __forceinline__ void issue_step(LaneState& L, const ImageConsts& c, double h, double min_step,
-                                           double max_step) {
+template<class LS>
+__device__ __forceinline__ void issue_step(LS& L, const ImageConsts& c, double h, double min_step, double max_step) {
     if (c.adaptive) {
         begin_adaptive(L, h, min_step, max_step);
         L.rk_kind = c.integrator == 1 ? kRkCK : kRkSD;
