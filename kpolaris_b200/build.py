@@ -38,6 +38,8 @@ UNITS = {
     "kp_kernels_grmhd.cu": ["--fmad=false"],
     "kp_kernels_grmhd_mixed.cu": ["--fmad=true", "--use_fast_math"],
     "kp_kernels_grmhd_slow.cu": ["--fmad=false"],
+    "kp_kernels_bl.cu": ["--fmad=false"],
+    "kp_kernels_bl_mixed.cu": ["--fmad=true", "--use_fast_math"],
     "kp_kernels_grmhd_slow_mixed.cu": ["--fmad=true", "--use_fast_math"],
     "kp_capi.cu": ["--fmad=false"],
     "kp_reorder.cu": ["--fmad=false"],

@@ -56,7 +56,9 @@ enum : int {
     kFamilyGrmhdMixed = 3,
     kFamilyGrmhdSlowFP64 = 4,
     kFamilyGrmhdSlowMixed = 5,
-    kFamilyCount = 6
+    kFamilyRiafBLFP64 = 6,
+    kFamilyRiafBLMixed = 7,
+    kFamilyCount = 8
 };
 constexpr int kDefaultGraphCycles = 3;
 constexpr size_t kGraphCacheSize = 8;
@@ -329,8 +331,7 @@ int validate_riaf(const kp_pass_a_params* p, const kp_riaf_model* m, const doubl
     if (nfreq > 1 && !freqs) return set_error(KP_ERR_INVALID, "null frequency list");
     switch (p->coordinate_system) {
     case KP_COORD_CARTESIAN_KS: break;
-    case KP_COORD_BOYER_LINDQUIST:
-        return set_error(KP_ERR_UNSUPPORTED, "RIAF image coordinate backend not built: boyer_lindquist");
+    case KP_COORD_BOYER_LINDQUIST: break;
     case KP_COORD_SPHERICAL_KS:
         return set_error(KP_ERR_UNSUPPORTED, "RIAF image coordinate backend not built: spherical_ks");
     case KP_COORD_FMKS:
@@ -378,6 +379,8 @@ ImageConsts make_consts(const kp_pass_a_params* p, const kp_riaf_model* m, const
     c.nx = p->camera.nx;
     c.ny = p->camera.ny;
     c.cam_radius = p->camera.radius;
+    c.inclination = p->camera.inclination;
+    c.scene = p->coordinate_system == KP_COORD_BOYER_LINDQUIST ? kSceneRiafBL : kSceneRiafCks;
     c.sin_inc = std::sin(p->camera.inclination);
     c.cos_inc = std::cos(p->camera.inclination);
     c.fov = p->camera.fov;
@@ -579,6 +582,8 @@ int run_wave_jobs(DeviceState* dev, cudaStream_t stream, int njobs, long long to
                      : family == kFamilyGrmhdMixed     ? wave_occupancy_grmhd_mixed(phase, nf_max, th)
                      : family == kFamilyGrmhdSlowFP64  ? wave_occupancy_grmhd_slow(phase, nf_max, th)
                      : family == kFamilyGrmhdSlowMixed ? wave_occupancy_grmhd_slow_mixed(phase, nf_max, th)
+                     : family == kFamilyRiafBLFP64     ? wave_occupancy_bl(phase, nf_max, th)
+                     : family == kFamilyRiafBLMixed    ? wave_occupancy_bl_mixed(phase, nf_max, th)
                      : mixed                           ? wave_occupancy_mixed(phase, th)
                                                        : wave_occupancy_fp64(phase, nf_max, th);
             if (per_sm <= 0) per_sm = 1;
@@ -618,6 +623,9 @@ int run_wave_jobs(DeviceState* dev, cudaStream_t stream, int njobs, long long to
             return launch_wave_grmhd_mixed(phase, W, nf_max, blocks[phase], wave_threads(phase), stream);
         if (family == kFamilyGrmhdSlowFP64)
             return launch_wave_grmhd_slow(phase, W, nf_max, blocks[phase], wave_threads(phase), stream);
+        if (family == kFamilyRiafBLFP64) return launch_wave_bl(phase, W, nf_max, blocks[phase], wave_threads(phase), stream);
+        if (family == kFamilyRiafBLMixed)
+            return launch_wave_bl_mixed(phase, W, nf_max, blocks[phase], wave_threads(phase), stream);
         if (family == kFamilyGrmhdSlowMixed)
             return launch_wave_grmhd_slow_mixed(phase, W, nf_max, blocks[phase], wave_threads(phase), stream);
         return mixed ? launch_wave_mixed(phase, W, blocks[phase], wave_threads(phase), stream)
@@ -867,8 +875,10 @@ int kp_image_riaf(const kp_pass_a_params* params, const kp_riaf_model* model, in
         return set_error(KP_ERR_INVALID, "unknown integrator %d", opt.integrator);
     if (opt.precision != KP_PRECISION_FP64 && opt.precision != KP_PRECISION_MIXED)
         return set_error(KP_ERR_INVALID, "unknown precision %d", opt.precision);
-    if (opt.precision == KP_PRECISION_MIXED || opt.schedule != KP_SCHEDULE_PER_PIXEL) {
-        // the persistent engine: a batch of one
+    if (opt.precision == KP_PRECISION_MIXED || opt.schedule != KP_SCHEDULE_PER_PIXEL ||
+        params->coordinate_system != KP_COORD_CARTESIAN_KS) {
+        // the persistent engine: a batch of one (the plain per-pixel kernel
+        // is the Cartesian Kerr-Schild form)
         kp_riaf_job job;
         std::memset(&job, 0, sizeof(job));
         job.params = *params;
@@ -938,6 +948,8 @@ int kp_image_riaf_analysis(const kp_pass_a_params* params, const kp_riaf_model* 
         kp_default_run_options(&opt);
     }
     int st = validate_riaf(params, model, nullptr, 1);
+    if (st == KP_OK && params->coordinate_system != KP_COORD_CARTESIAN_KS)
+        return set_error(KP_ERR_UNSUPPORTED, "analysis-mode image coordinate backend not built: boyer_lindquist");
     if (st != KP_OK) return st;
     if (!config || !analysis) return set_error(KP_ERR_INVALID, "null analysis config or outputs");
     // validate_options (tools/kpolaris_model_image_options.cpp:265-284)
@@ -1050,6 +1062,9 @@ int kp_batch_riaf(const kp_riaf_job* jobs, int njobs, const kp_run_options* opti
         const kp_riaf_job& jb = jobs[i];
         int st = validate_riaf(&jb.params, &jb.model, jb.frequencies, jb.nfreq);
         if (st != KP_OK) return job_error(st, i);
+        // one metric per batch, as run_image_batch_metric<Metric> has
+        if (jb.params.coordinate_system != jobs[0].params.coordinate_system)
+            return set_error(KP_ERR_UNSUPPORTED, "job %d: the jobs of a batch must share one coordinate system", i);
         if (jb.radiation_substeps < 1) return set_error(KP_ERR_INVALID, "job %d: batch radiation_substeps must be positive", i);
         const int npix = jb.params.camera.nx * jb.params.camera.ny;
         st = check_outputs(&jb.out, npix, jb.nfreq);
@@ -1058,9 +1073,13 @@ int kp_batch_riaf(const kp_riaf_job* jobs, int njobs, const kp_run_options* opti
         nf_max = std::max(nf_max, jb.nfreq);
         scratch += carved_bytes(npix, jb.nfreq);
     }
-    // The mixed kernel always carries four channels: the same compiled code
-    // traces a ray whatever the other jobs of the batch are.
-    if (opt.precision == KP_PRECISION_MIXED) nf_max = KP_MAX_FREQUENCIES;
+    const bool bl = jobs[0].params.coordinate_system == KP_COORD_BOYER_LINDQUIST;
+    const bool mixed_policy = opt.precision == KP_PRECISION_MIXED;
+    const int family = bl ? (mixed_policy ? kFamilyRiafBLMixed : kFamilyRiafBLFP64)
+                          : (mixed_policy ? kFamilyRiafMixed : kFamilyRiafFP64);
+    // The mixed Kerr-Schild kernel always carries four channels: the same
+    // compiled code traces a ray whatever the other jobs of the batch are.
+    if (family == kFamilyRiafMixed) nf_max = KP_MAX_FREQUENCIES;
     std::lock_guard<std::mutex> lock(g_mutex);
     int st = KP_OK;
     DeviceState* dev = device_state(opt.device, &st);
@@ -1105,8 +1124,7 @@ int kp_batch_riaf(const kp_riaf_job* jobs, int njobs, const kp_run_options* opti
         d.precision = opt.precision;
         ray += npix;
     }
-    st = run_wave_jobs(dev, stream, njobs, total, opt.precision == KP_PRECISION_MIXED ? kFamilyRiafMixed : kFamilyRiafFP64,
-                       nf_max, opt, stats);
+    st = run_wave_jobs(dev, stream, njobs, total, family, nf_max, opt, stats);
     if (st != KP_OK) return st;
     if (stats) stats->device_output_bytes = opt.outputs_on_device ? 0 : scratch;
     if (!opt.outputs_on_device) {
@@ -1197,11 +1215,13 @@ int kp_autotune_batch(const kp_riaf_job* jobs, int njobs, const kp_run_options* 
     if (opt.blocks_per_sm != 0) return set_error(KP_ERR_INVALID, "blocks_per_sm must be 0: the tuner chooses it");
     if (opt.precision != KP_PRECISION_FP64 && opt.precision != KP_PRECISION_MIXED)
         return set_error(KP_ERR_INVALID, "unknown precision %d", opt.precision);
-    const int family = opt.precision == KP_PRECISION_MIXED ? kFamilyRiafMixed : kFamilyRiafFP64;
+    const bool bl = jobs[0].params.coordinate_system == KP_COORD_BOYER_LINDQUIST;
+    const int family = bl ? (opt.precision == KP_PRECISION_MIXED ? kFamilyRiafBLMixed : kFamilyRiafBLFP64)
+                          : (opt.precision == KP_PRECISION_MIXED ? kFamilyRiafMixed : kFamilyRiafFP64);
     int nf_max = 1;
     for (int i = 0; i < njobs; ++i)
         if (jobs[i].nfreq > 1) nf_max = KP_MAX_FREQUENCIES;
-    if (opt.precision == KP_PRECISION_MIXED) nf_max = KP_MAX_FREQUENCIES;
+    if (family == kFamilyRiafMixed) nf_max = KP_MAX_FREQUENCIES;
     int limit[kPhases];
     {
         std::lock_guard<std::mutex> lock(g_mutex);
@@ -1210,8 +1230,10 @@ int kp_autotune_batch(const kp_riaf_job* jobs, int njobs, const kp_run_options* 
         if (!dev) return st;
         for (int phase = 0; phase < kPhases; ++phase) {
             const int th = wave_threads(phase);
-            const int occ = family == kFamilyRiafMixed ? wave_occupancy_mixed(phase, th)
-                                                       : wave_occupancy_fp64(phase, nf_max, th);
+            const int occ = family == kFamilyRiafMixed     ? wave_occupancy_mixed(phase, th)
+                            : family == kFamilyRiafBLFP64  ? wave_occupancy_bl(phase, nf_max, th)
+                            : family == kFamilyRiafBLMixed ? wave_occupancy_bl_mixed(phase, nf_max, th)
+                                                           : wave_occupancy_fp64(phase, nf_max, th);
             limit[phase] = occ < 1 ? 1 : (occ > 4 ? 4 : occ);
         }
     }

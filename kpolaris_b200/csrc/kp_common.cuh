@@ -81,7 +81,7 @@ struct GridConsts {
     double rho_unit, b_unit, trat_small, trat_large, beta_crit, sigma_cut, sigma_cut_high, ne_factor;
 };
 
-enum Scene : int { kSceneRiafCks = 0, kSceneGrmhdFmks = 1, kSceneGrmhdFmksSlowLight = 2 };
+enum Scene : int { kSceneRiafCks = 0, kSceneGrmhdFmks = 1, kSceneGrmhdFmksSlowLight = 2, kSceneRiafBL = 3 };
 
 // Everything one image needs on the device, resolved on the host.  Host-side
 // precomputation keeps libm (sin/cos of the inclination, cbrt in the ISCO
@@ -99,6 +99,7 @@ struct ImageConsts {
     // pinhole camera (CameraParams, src/camera/camera.hpp:12-25)
     int nx, ny;
     double cam_radius, sin_inc, cos_inc;
+    double inclination;  // the camera's theta in Boyer-Lindquist scenes
     double fov, fov_y, xspan, yspan, x_offset, y_offset;
     // RIAF plasma (src/model/riaf.hpp:19-52)
     double nth0, Te0, disk_h, pow_nth, pow_T, ne_unit;

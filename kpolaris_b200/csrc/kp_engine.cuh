@@ -175,6 +175,40 @@ struct RadTraits<PolicyMixed, SceneGrmhdSlow> : RadTraits<PolicyMixed, SceneRiaf
     __device__ static Sample sample(const ImageConsts& c, const Ray& r) { return grmhd_series_sample_f(c, r); }
 };
 
+// The RIAF in Boyer-Lindquist coordinates: the same plasma model, sampled
+// in the ray's own BL components (riaf_sample_t<true>); under the mixed
+// policy the FP64 sample feeds the FP32 fits and transfer.
+template<>
+struct RadTraits<PolicyFP64, SceneRiafBL> : RadTraits<PolicyFP64, SceneRiaf> {
+    __device__ static Sample sample(const ImageConsts& c, const Ray& r) { return riaf_sample_t<true>(c, r); }
+};
+
+__device__ __forceinline__ RiafSampleF riaf_sample_to_f(const ImageConsts& c, const RiafSample& p) {
+    RiafSampleF o;
+    o.emitting = p.emitting;
+    o.on_axis = p.on_axis;
+    o.has_chi = p.has_chi;
+    if (!p.emitting) return o;
+    o.ne = float(p.ne);
+    o.thetae = float(p.thetae);
+    o.b = float(p.b);
+    o.nu_fluid = float(p.nu_fluid);
+    o.cos_theta = float(p.cos_theta);
+    o.sin_theta = float(p.sin_theta);
+    o.theta = float(p.theta);
+    o.cos2chi = float(p.cos2chi);
+    o.sin2chi = float(p.sin2chi);
+    riaf_sample_thermal_f(c, o);
+    return o;
+}
+
+template<>
+struct RadTraits<PolicyMixed, SceneRiafBL> : RadTraits<PolicyMixed, SceneRiaf> {
+    __device__ static Sample sample(const ImageConsts& c, const Ray& r) {
+        return riaf_sample_to_f(c, riaf_sample_t<true>(c, r));
+    }
+};
+
 // A far-phase chart scene radiates nothing; its Stokes types are its
 // record scene's.
 template<class P, class B>

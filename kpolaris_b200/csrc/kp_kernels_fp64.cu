@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include "kp_analysis.cuh"
+#include "kp_bl.cuh"
 #include "kp_launch.h"
 #include "kp_persistent.cuh"
 #include "kp_trace_fp64.cuh"
@@ -148,7 +149,12 @@ cudaError_t launch_image_fp64_analysis(const ImageConsts& c, const AnalysisConst
 }
 
 void host_camera_frame(const ImageConsts& c, double frame[5][4]) {
-    const CameraFrame f = camera_frame(c);
+    CameraFrame f;
+    if (c.scene == kSceneRiafBL) {
+        bl_camera_frame(c.mass, c.spin, c.cam_radius, c.inclination, f.x, f.e0, f.e1, f.e2, f.e3);
+    } else {
+        f = camera_frame(c);
+    }
     for (int mu = 0; mu < 4; ++mu) {
         frame[0][mu] = f.x.v[mu];
         frame[1][mu] = f.e0.v[mu];

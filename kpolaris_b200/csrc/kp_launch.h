@@ -80,7 +80,8 @@ cudaError_t launch_image_fp64_analysis(const ImageConsts& c, const AnalysisConst
                                        const AnalysisPtrs& an, cudaStream_t stream);
 
 // Camera tetrad of an image, evaluated on the host (bit-identical to the
-// reference's CPU evaluation).
+// reference's CPU evaluation): Cartesian Kerr-Schild, or Boyer-Lindquist for
+// a kSceneRiafBL image.
 void host_camera_frame(const ImageConsts& c, double frame[5][4]);
 
 // Wavefront engine: one launch of `phase` (kPhaseFar / kPhaseNear) over the
@@ -116,6 +117,13 @@ int wave_occupancy_grmhd_mixed(int phase, int nf_max, int threads);
 cudaError_t launch_seed_grmhd_mixed(const JobDesc* jobs, const SeedEntry* entries, const long long* prefix,
                                     int nentries, long long total, RayRecord* pool, unsigned* far_ids,
                                     unsigned* far_count, cudaStream_t stream);
+// The RIAF in Boyer-Lindquist coordinates, FP64 policy (kp_kernels_bl.cu)
+// and mixed policy (kp_kernels_bl_mixed.cu).
+cudaError_t launch_wave_bl(int phase, const WaveDesc& W, int nf_max, int blocks, int threads, cudaStream_t stream);
+int wave_occupancy_bl(int phase, int nf_max, int threads);
+cudaError_t launch_wave_bl_mixed(int phase, const WaveDesc& W, int nf_max, int blocks, int threads,
+                                 cudaStream_t stream);
+int wave_occupancy_bl_mixed(int phase, int nf_max, int threads);
 // Longest-first order of a near-B queue (kp_reorder.cu): `count` ids from
 // `ids` into `out`, grouped by pass-A steps, most first; `scratch` holds 512
 // unsigned counters.

@@ -99,6 +99,8 @@ extern "C" int kp_batch_riaf_noalloc(const kp_riaf_job* jobs, int njobs, const k
         const kp_riaf_job& jb = jobs[i];
         int st = validate_riaf(&jb.params, &jb.model, jb.frequencies, jb.nfreq);
         if (st != KP_OK) return job_error(st, i);
+        if (jb.params.coordinate_system != KP_COORD_CARTESIAN_KS)
+            return set_error(KP_ERR_UNSUPPORTED, "job %d: kp_batch_riaf_noalloc traces Cartesian Kerr-Schild images only", i);
         if (jb.radiation_substeps < 1)
             return set_error(KP_ERR_INVALID, "job %d: batch radiation_substeps must be positive", i);
         const int npix = jb.params.camera.nx * jb.params.camera.ny;

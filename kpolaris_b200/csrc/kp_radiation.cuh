@@ -9,6 +9,7 @@
 // forms) re-expressed here.
 #pragma once
 
+#include "kp_bl.cuh"
 #include "kp_geometry.cuh"
 
 namespace kp {
@@ -514,19 +515,39 @@ __device__ __forceinline__ int riaf_plasma(const ImageConsts& c, const BlCoords&
     return 1;
 }
 
-static __device__ __noinline__ RiafSample riaf_sample(const ImageConsts& c, const Ray& s) {
+// The plasma state of a sample point, in either chart of the RIAF scenes
+// (kBL: the ray is in Boyer-Lindquist coordinates, where the model's BL
+// quantities are the ray's own components; otherwise Cartesian Kerr-Schild,
+// converted with bl_to_cks -- bl_coordinates_for_metric and the
+// coordinate_system branches of riaf.hpp:124-137, 255-268, 350-364).
+template<bool kBL>
+static __device__ __noinline__ RiafSample riaf_sample_t(const ImageConsts& c, const Ray& s) {
     RiafSample out;
     out.emitting = 0;
     out.on_axis = 0;
     out.has_chi = 0;
     const double spin = c.spin;
-    const BlCoords q = riaf_bl_coords(spin, s.x);
+    BlCoords q;
+    if constexpr (kBL) {
+        q.rc = s.x.v[1];
+        q.th = s.x.v[2];
+        q.sin_th = sin(q.th);
+        q.cos_th = cos(q.th);
+        q.cphi = cos(s.x.v[3]);
+        q.sphi = sin(s.x.v[3]);
+    } else {
+        q = riaf_bl_coords(spin, s.x);
+    }
     const double rc = q.rc, th = q.th, sin_th = q.sin_th, cos_th = q.cos_th, cphi = q.cphi, sphi = q.sphi;
     double r_bl;
     if (!riaf_plasma(c, q, r_bl, out.ne, out.thetae, out.b)) return out;
     out.emitting = 1;
     double g[4][4];
-    ks_gcov_matrix(c.mass, spin, s.x, g);
+    if constexpr (kBL) {
+        bl_gcov_matrix(c.mass, spin, s.x, g);
+    } else {
+        ks_gcov_matrix(c.mass, spin, s.x, g);
+    }
     // fluid_four_velocity_from_bl_coords (riaf.hpp:206-273) at r = r_bl
     D4 ucon;
     {
@@ -568,7 +589,11 @@ static __device__ __noinline__ RiafSample riaf_sample(const ImageConsts& c, cons
             vt = sqrt(max_val(-(1.0 + vr * vr * gcov[1][1]) / q, 0.0));
             vphi = omega * vt;
         }
-        ucon = bl_to_cks(vt, vr, 0.0, vphi, r, sin_th, cos_th, cphi, sphi, spin);
+        if constexpr (kBL) {
+            ucon = d4(vt, vr, 0.0, vphi);
+        } else {
+            ucon = bl_to_cks(vt, vr, 0.0, vphi, r, sin_th, cos_th, cphi, sphi, spin);
+        }
         const double n2 = dot_g(g, ucon, ucon);
         if (n2 < 0.0) ucon = d4_scale(ucon, 1.0 / sqrt(max_val(-n2, kTiny)));
     }
@@ -581,7 +606,7 @@ static __device__ __noinline__ RiafSample riaf_sample(const ImageConsts& c, cons
     // at the raw BL radius rc of the sample.
     D4 bcon;
     {
-        D4 bt = bl_to_cks(0.0, 0.0, 0.0, 1.0, rc, sin_th, cos_th, cphi, sphi, spin);
+        D4 bt = kBL ? d4(0.0, 0.0, 0.0, 1.0) : bl_to_cks(0.0, 0.0, 0.0, 1.0, rc, sin_th, cos_th, cphi, sphi, spin);
         double udotb = dot_g(g, ucon, bt);
         for (int i = 0; i < 4; ++i) bcon.v[i] = bt.v[i] + ucon.v[i] * udotb;
         double bsq = dot_g(g, bcon, bcon);
@@ -619,6 +644,10 @@ static __device__ __noinline__ RiafSample riaf_sample(const ImageConsts& c, cons
         out.sin2chi = -2.0 * b1 * b2 / bproj2;
     }
     return out;
+}
+
+static __device__ __forceinline__ RiafSample riaf_sample(const ImageConsts& c, const Ray& s) {
+    return riaf_sample_t<false>(c, s);
 }
 
 // RIAFAnalyticRadiationModel::coefficients for one frequency (riaf.hpp:410-549).

@@ -9,6 +9,7 @@
 // (src/geodesic/pass_b.hpp:87-98, 1096-1113).
 #pragma once
 
+#include "kp_bl.cuh"
 #include "kp_camera.cuh"
 #include "kp_chart.cuh"
 #include "kp_fmks.cuh"
@@ -47,6 +48,67 @@ struct SceneRiaf {
         return camera_ray(c, f, pixel);
     }
     __device__ static Metric metric_at(const ImageConsts& c, const D4& X) { return Metric{ks_point(c.mass, c.spin, X)}; }
+};
+
+// initialize_pinhole_camera_ray (camera.hpp:485-513) in Boyer-Lindquist
+// coordinates, from the image's precomputed tetrad (normalize_spacelike and
+// orthogonalize_spacelike, camera.hpp:207-228).
+static __device__ __noinline__ Ray bl_camera_ray(const ImageConsts& c, const CameraFrame& f, int pixel) {
+    const BLMetricPoint w = bl_point(c.mass, c.spin, f.x);
+    double sx = 0.0, sy = 0.0;
+    pixel_offsets(pixel, c, sx, sy);
+    const double spatial_norm = sqrt(1.0 + sx * sx + sy * sy);
+    const double kt1 = sx / spatial_norm;
+    const double kt2 = sy / spatial_norm;
+    const double kt3 = 1.0 / spatial_norm;
+    D4 sd;
+    for (int mu = 0; mu < 4; ++mu)
+        sd.v[mu] = f.e1.v[mu] * kt1 + f.e2.v[mu] * kt2 + f.e3.v[mu] * kt3;
+    Ray s;
+    s.x = f.x;
+    for (int mu = 0; mu < 4; ++mu) s.k.v[mu] = f.e0.v[mu] * 1.0 + sd.v[mu];
+    D4 e1 = d4_sub_scaled(f.e1, sd, kt1);
+    {
+        const double n2 = bl_dot_at(w, e1, e1);
+        if (!(n2 <= 0.0)) e1 = d4_scale(e1, 1.0 / sqrt(n2));
+    }
+    D4 e2 = d4_sub_scaled(f.e2, sd, kt2);
+    {
+        const double denom = bl_dot_at(w, e1, e1);
+        if (abs_val(denom) > kTiny) e2 = d4_sub_scaled(e2, e1, bl_dot_at(w, e2, e1) / denom);
+        const double n2 = bl_dot_at(w, e2, e2);
+        if (!(n2 <= 0.0)) e2 = d4_scale(e2, 1.0 / sqrt(n2));
+    }
+    s.e1 = e1;
+    s.e2 = e2;
+    return s;
+}
+
+// The analytic RIAF in Boyer-Lindquist coordinates (the reference's RIAF
+// backend, src/image/riaf.cpp:21-45, over KerrBoyerLindquistMetric): radius
+// x^1 (metric_domain_radius, src/geodesic/metric_domain.hpp:160-172), the
+// specialised BL transport in FP64 under both policies, the camera from the
+// host's BL tetrad.
+struct SceneRiafBL {
+    static constexpr bool kSlowLight = false;
+    static constexpr bool kCksRhs = false;
+    static constexpr bool kFarChart = false;
+    __device__ static bool chart_active(const ImageConsts&) { return false; }
+    struct Metric {
+        BLMetricPoint p;
+        __device__ double dot(const D4& u, const D4& v) const { return bl_dot_at(p, u, v); }
+    };
+    __device__ static double radius(const ImageConsts&, const D4& X) { return X.v[1]; }
+    template<bool MIXED, bool FP32>
+    __device__ static Ray rhs(const ImageConsts& c, const Ray& X) {
+        return bl_rhs(c.mass, c.spin, X);
+    }
+    __device__ static Ray camera(const ImageConsts& c, const CameraFrame& f, int pixel) {
+        return bl_camera_ray(c, f, pixel);
+    }
+    __device__ static Metric metric_at(const ImageConsts& c, const D4& X) {
+        return Metric{bl_point(c.mass, c.spin, X)};
+    }
 };
 
 // initialize_pinhole_camera_ray (camera.hpp:485-513) in FMKS, from the

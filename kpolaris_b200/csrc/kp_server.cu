@@ -579,6 +579,8 @@ int kp_server_submit(kp_server* s, const kp_riaf_job* job, unsigned long long* t
     if (!s || !job || !ticket) return set_error(KP_ERR_INVALID, "kp_server_submit: null argument");
     int st = validate_riaf(&job->params, &job->model, job->frequencies, job->nfreq);
     if (st != KP_OK) return st;
+    if (job->params.coordinate_system != KP_COORD_CARTESIAN_KS)
+        return set_error(KP_ERR_UNSUPPORTED, "the serving loop traces Cartesian Kerr-Schild RIAF images only");
     if (job->radiation_substeps < 1) return set_error(KP_ERR_INVALID, "radiation_substeps must be positive");
     const int npix = job->params.camera.nx * job->params.camera.ny;
     st = check_outputs(&job->out, npix, job->nfreq);

@@ -769,6 +769,52 @@ int kpref_camera_ray_cks(const kp_pass_a_params* params, int pixel, double* stat
     return KP_OK;
 }
 
+// The same three pieces over KerrBoyerLindquistMetric (the reference's RIAF
+// backend): RIAF coefficients at a BL transport state, the pinhole camera
+// ray, and the BL transport RHS (kerr_boyer_lindquist.hpp:306-322).
+static kpolaris::TransportState<Real> state_of(const double* state16) {
+    kpolaris::TransportState<Real> s;
+    for (int mu = 0; mu < 4; ++mu) {
+        s.x[mu] = state16[mu];
+        s.k[mu] = state16[4 + mu];
+        s.e1[mu] = state16[8 + mu];
+        s.e2[mu] = state16[12 + mu];
+    }
+    return s;
+}
+
+static void put_state(const kpolaris::TransportState<Real>& s, double* state16) {
+    for (int mu = 0; mu < 4; ++mu) {
+        state16[mu] = s.x[mu];
+        state16[4 + mu] = s.k[mu];
+        state16[8 + mu] = s.e1[mu];
+        state16[12 + mu] = s.e2[mu];
+    }
+}
+
+int kpref_riaf_coefficients_bl(double mass, double spin, const kp_riaf_model* model, const double* state16,
+                               double* out11) {
+    const kpolaris::KerrBoyerLindquistMetric<Real> metric(mass, spin);
+    const auto riaf = to_riaf(*model);
+    const auto c = riaf.coefficients(metric, state_of(state16), Real(0.5));
+    const double v[11] = {c.jI, c.jQ, c.jU, c.jV, c.aI, c.aQ, c.aU, c.aV, c.rQ, c.rU, c.rV};
+    std::memcpy(out11, v, sizeof(v));
+    return KP_OK;
+}
+
+int kpref_camera_ray_bl(const kp_pass_a_params* params, int pixel, double* state16) {
+    const auto pa = to_pass_a(*params);
+    const kpolaris::KerrBoyerLindquistMetric<Real> metric(pa.mass, pa.spin);
+    put_state(kpolaris::initialize_camera_ray(metric, pixel, pa.camera), state16);
+    return KP_OK;
+}
+
+int kpref_transport_rhs_bl(double mass, double spin, const double* state16, double* d16) {
+    const kpolaris::KerrBoyerLindquistMetric<Real> metric(mass, spin);
+    put_state(kpolaris::transport_rhs(metric, state_of(state16)), d16);
+    return KP_OK;
+}
+
 // Geodesic right-hand side (transport_rhs, kerr_schild_cartesian.hpp:348-363).
 int kpref_transport_rhs_cks(double mass, double spin, const double* state16, double* d16) {
     const kpolaris::KerrSchildInMetric<Real> metric(mass, spin);

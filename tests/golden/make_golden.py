@@ -20,6 +20,11 @@ libm conditioning measured on the reference's own templates
     python tests/golden/make_golden.py --slow      # slow-light fixtures only
     python tests/golden/make_golden.py --steps     # adaptive step fixture only
     python tests/golden/make_golden.py --sampling  # slow-light sampling fixture only
+    python tests/golden/make_golden.py --bl        # Boyer-Lindquist RIAF fixtures only
+
+Each Boyer-Lindquist fixture (riaf_bl_*.npz, BL_CASES) stores the case, every
+output array of the reference's image over KerrBoyerLindquistMetric, and the
+image's +-2-ulp libm conditioning on the reference's own templates.
 
 The slow-light sampling fixture (slow_sampling.npz) stores 16 distinct,
 unevenly spaced snapshot times, two observation times, seeded sample
@@ -56,7 +61,8 @@ sys.path.insert(0, str(ROOT))
 sys.path.insert(0, str(ROOT / "tests"))
 
 import oracle  # noqa: E402
-from golden_cases import (IMAGE_CASES, GRMHD_CASES, SLOW_CASES, build_case, build_grmhd_case,  # noqa: E402
+from golden_cases import (BL_CASES, IMAGE_CASES, GRMHD_CASES, SLOW_CASES, bl_conditioning_of, build_bl_case,  # noqa: E402
+                          build_case, build_grmhd_case,
                           build_slow_case, coefficient_points, grmhd_conditioning_of, prims_digest,
                           slow_conditioning_of, transfer_points)
 
@@ -165,6 +171,19 @@ def make_steps():
               "after a rejection", int(shrunk.sum()), "exhausted", int((out[f"{tag}_accepted"] == 0).sum()))
 
 
+def make_bl():
+    for name, spec in BL_CASES.items():
+        params, model, freqs = build_bl_case(spec)
+        res = oracle.image_riaf(params, model, freqs, kind="reference", threads=0)
+        cond = bl_conditioning_of(params, model, freqs, res.arrays)
+        keys = sorted(cond, key=cond_key)
+        np.savez_compressed(OUT / f"{name}.npz", spec=json.dumps(spec),
+                            cond_keys=np.array([cond_key(k) for k in keys]),
+                            cond_vals=np.array([cond[k] for k in keys]), **res.arrays)
+        print(name, np.bincount(res.reason, minlength=8)[:8],
+              {cond_key(k): "%.1e" % cond[k] for k in keys if k[0] in ("flux", "image_i")})
+
+
 def make_sampling():
     rng = np.random.default_rng(7001)
     times = np.cumsum(np.concatenate([[40.0], rng.uniform(4.0, 16.0, size=15)]))
@@ -187,6 +206,9 @@ def main():
     oracle.build(reference=True)
     if "--sampling" in sys.argv[1:]:
         make_sampling()
+        return
+    if "--bl" in sys.argv[1:]:
+        make_bl()
         return
     if "--steps" in sys.argv[1:]:
         make_steps()
@@ -220,6 +242,7 @@ def main():
     make_slow()
     make_steps()
     make_sampling()
+    make_bl()
 
 
 if __name__ == "__main__":

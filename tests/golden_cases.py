@@ -259,3 +259,44 @@ def slow_conditioning_of(params, model, prims, derived, times, t_obs, freqs, ref
                                              kind="reference_ulp")
 
     return conditioning_over(run, ref, seeds)
+
+
+# The RIAF in Boyer-Lindquist coordinates (the reference's RIAF backend,
+# src/image/riaf.cpp:21-45): image cases whose oracle is the reference's own
+# templates over KerrBoyerLindquistMetric (the C restatement covers the
+# Cartesian Kerr-Schild chart only).
+BL_CASES = {
+    # config-1 controls (fixed RK4, h = 1) at 12^2
+    "riaf_bl_cfg1_12": {"kind": "config1", "n": 12, "coordinate": "bl"},
+    # config-2 controls (adaptive tol 1e-8, four frequencies, depth 1/1/4) at 8^2
+    "riaf_bl_cfg2_8": {"kind": "config2", "n": 8, "coordinate": "bl"},
+    # camera at r = 100, i = 30 deg, a field of +-12 M: the shadow, the
+    # photon ring and captured rays (which end in adaptive step underflow at
+    # the BL horizon's coordinate singularity), adaptive, two frequencies
+    "riaf_bl_near_9": {"kind": "custom", "nx": 9, "ny": 9, "spin": 0.9375, "inclination_deg": 30.0,
+                       "radius": 100.0, "xspan": 12.0, "step": 0.025, "adaptive": 1,
+                       "max_steps": 100000, "tolerance": 1e-8, "min_step": 1e-10,
+                       "max_step": 2.0, "max_radiation_step": 2.0, "depths": [1.0, 1.0, 4.0],
+                       "freqs": [86.0e9, 230.0e9], "coordinate": "bl"},
+    # wide field at i = 163 deg: escaping corner rays, rays past the pole
+    "riaf_bl_wide_10x7": {"kind": "custom", "nx": 10, "ny": 7, "inclination_deg": 163.0, "xspan": 150.0,
+                          "step": 1.0, "max_steps": 2000, "fit": 4, "freqs": [345.0e9], "coordinate": "bl"},
+}
+
+
+def build_bl_case(spec: dict):
+    params, model, freqs = build_case(spec)
+    params.coordinate_system = _abi.COORD_BOYER_LINDQUIST
+    return params, model, freqs
+
+
+def bl_conditioning_of(params, model, freqs, ref, seeds=tuple(range(1, 9))):
+    """libm_conditioning_of for a BL image, measured on the reference's own
+    templates with perturbed libm (oracle kind 'reference_ulp')."""
+    import oracle
+
+    def run(seed):
+        oracle.set_libm_perturbation(seed, "reference_ulp")
+        return oracle.image_riaf(params, model, freqs, kind="reference_ulp", threads=0)
+
+    return conditioning_over(run, ref, seeds)

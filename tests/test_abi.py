@@ -73,7 +73,7 @@ def test_output_bytes_match_reference_batch_budget():
 
 @pytest.mark.parametrize("mutate,status", [
     (lambda p, m: setattr(p.camera, "nx", 0), _abi.KP_ERR_INVALID),
-    (lambda p, m: setattr(p, "coordinate_system", _abi.COORD_BOYER_LINDQUIST), _abi.KP_ERR_UNSUPPORTED),
+    (lambda p, m: setattr(p, "coordinate_system", _abi.COORD_SPHERICAL_KS), _abi.KP_ERR_UNSUPPORTED),
     (lambda p, m: setattr(p, "coordinate_system", _abi.COORD_FMKS), _abi.KP_ERR_UNSUPPORTED),
     (lambda p, m: setattr(p, "direct_only", 1), _abi.KP_ERR_UNSUPPORTED),
     (lambda p, m: setattr(m, "emission_type", 2), _abi.KP_ERR_UNSUPPORTED),
