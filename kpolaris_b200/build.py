@@ -112,7 +112,8 @@ def build_tool(force: bool = False, verbose: bool = False) -> Path:
     through its run path."""
     TOOL.parent.mkdir(parents=True, exist_ok=True)
     src = HOST / "kp_model_image.cpp"
-    deps = [src, HOST / "kpolaris_image_options.hpp", INCLUDE / "kpolaris_b200.h", LIB]
+    deps = [src, HOST / "kpolaris_image_options.hpp", HOST / "kp_image_h5.hpp", HOST / "kp_hdf5.hpp",
+            INCLUDE / "kpolaris_b200.h", LIB]
     if not force and not _stale(TOOL, deps):
         return TOOL
     cxx = shutil.which("g++") or "g++"

@@ -8,9 +8,10 @@
 // Reads the reference's parameter files and overrides
 // (kpolaris_image_options.hpp), traces the image through the C ABI
 // (kp_image_riaf, frequencies in chunks of at most KP_MAX_FREQUENCIES),
-// packs each frequency with kp_pack_image, writes the CSV image format and
-// <output>.params, and prints the tool's summary lines.  HDF5 output is not
-// built (format=hdf5, or output=*.h5 with format=auto, is an error).
+// packs each frequency with kp_pack_image, writes the image -- the
+// kpolaris_image v1 HDF5 layout (kp_image_h5.hpp) for format=hdf5 or an
+// output ending in .h5 with format=auto, else the CSV image format -- and
+// <output>.params, and prints the tool's summary lines.
 //
 // Extra keys: kp_precision=fp64|mixed, kp_schedule=auto|per_pixel|
 // persistent|graph (auto: per-pixel kernel for fp64, wavefront engine for
@@ -26,6 +27,7 @@
 #include <string>
 #include <vector>
 
+#include "kp_image_h5.hpp"
 #include "kpolaris_image_options.hpp"
 
 namespace {
@@ -93,13 +95,10 @@ int run(const std::vector<std::string>& args) {
                        opt.output.compare(opt.output.size() - 3, 3, ".h5") == 0);
     if (opt.output_format != "auto" && opt.output_format != "hdf5" && opt.output_format != "csv")
         throw std::runtime_error("unknown output format: " + opt.output_format);
-    if (hdf5)
-        throw std::runtime_error("HDF5 image output is not built in this library: use format=csv "
-                                 "(or an output path not ending in .h5)");
     const std::string params_path = kpb::effective_parameter_path(opt);
     kpb::write_effective_parameters(params_path, opt, pass_a, freqs);
     if (opt.kp_dry_run) {
-        std::cout << "parameters " << params_path << "\n";
+        std::cout << "format " << (hdf5 ? "hdf5" : "csv") << "\nparameters " << params_path << "\n";
         return 0;
     }
 
@@ -158,7 +157,27 @@ int run(const std::vector<std::string>& args) {
 
     const auto t_output = std::chrono::steady_clock::now();
     const bool multi = freqs.size() > 1;
-    {
+    if (hdf5) {
+        std::vector<kpb::H5Frequency> h5f(packed.size());
+        for (size_t fi = 0; fi < packed.size(); ++fi) {
+            const PackedFrequency& pf = packed[fi];
+            kpb::H5Frequency& f = h5f[fi];
+            f.frequency = pf.frequency;
+            for (int k = 0; k < 4; ++k) {
+                f.inv[k] = pf.inv[k].data();
+                f.nu[k] = pf.nu[k].data();
+                f.sum_inv[k] = pf.p.sum_inv[k];
+                f.flux_jy[k] = pf.p.flux_jy[k];
+            }
+        }
+        kpb::H5Diagnostics dg;
+        dg.reason = first_chunk.reason.data();
+        dg.pass_a_steps = first_chunk.pass_a_steps.data();
+        dg.steps = first_chunk.steps.data();
+        dg.total_steps = packed.front().total_steps.data();
+        for (int k = 0; k < 11; ++k) dg.diag[k] = first_chunk.diag[k].data();
+        kpb::write_image_h5(opt.output, opt, params_path, pass_a, freqs, h5f, dg, fs);
+    } else {
         std::ofstream out(opt.output);
         if (!out) throw std::runtime_error("failed to open output: " + opt.output);
         out.precision(17);
@@ -202,7 +221,8 @@ int run(const std::vector<std::string>& args) {
     report_timing(opt, "image_run_model_total", seconds_since(t_start));
 
     std::cout.precision(17);
-    std::cout << "KPolaris-B200 model image output\nmodel " << opt.model << "\nformat csv\n";
+    std::cout << "KPolaris-B200 model image output\nmodel " << opt.model << "\nformat " << (hdf5 ? "hdf5" : "csv")
+              << "\n";
     std::cout << "output " << opt.output << "\n";
     if (!params_path.empty()) std::cout << "parameters " << params_path << "\n";
     std::cout << "pixels " << npix << "\nfrequencies " << freqs.size() << "\n";

@@ -21,10 +21,18 @@ libm conditioning measured on the reference's own templates
     python tests/golden/make_golden.py --steps     # adaptive step fixture only
     python tests/golden/make_golden.py --sampling  # slow-light sampling fixture only
     python tests/golden/make_golden.py --bl        # Boyer-Lindquist RIAF fixtures only
+    python tests/golden/make_golden.py --recommended  # riaf_recommended.par replay fixture only
 
 Each Boyer-Lindquist fixture (riaf_bl_*.npz, BL_CASES) stores the case, every
 output array of the reference's image over KerrBoyerLindquistMetric, and the
 image's +-2-ulp libm conditioning on the reference's own templates.
+
+The replay fixture (riaf_recommended.npz) stores the settings of the
+reference's params/riaf_recommended.par in file order (comment and blank lines
+dropped: the GPU box has no copy of the reference tree), the reference's
+image at a 32 x 32 lattice of its 256 x 256 pixels (golden_cases.
+recommended_pixels(8); arrays hold those pixels only) and that sample's
++-2-ulp libm conditioning on the reference's own templates.
 
 The slow-light sampling fixture (slow_sampling.npz) stores 16 distinct,
 unevenly spaced snapshot times, two observation times, seeded sample
@@ -61,8 +69,9 @@ sys.path.insert(0, str(ROOT))
 sys.path.insert(0, str(ROOT / "tests"))
 
 import oracle  # noqa: E402
-from golden_cases import (BL_CASES, IMAGE_CASES, GRMHD_CASES, SLOW_CASES, bl_conditioning_of, build_bl_case,  # noqa: E402
-                          build_case, build_grmhd_case,
+from golden_cases import (BL_CASES, IMAGE_CASES, GRMHD_CASES, RECOMMENDED_PAR, SLOW_CASES,  # noqa: E402
+                          bl_conditioning_of, build_bl_case, build_case, build_grmhd_case, conditioning_over,
+                          recommended_case, recommended_pixels,
                           build_slow_case, coefficient_points, grmhd_conditioning_of, prims_digest,
                           slow_conditioning_of, transfer_points)
 
@@ -184,6 +193,34 @@ def make_bl():
               {cond_key(k): "%.1e" % cond[k] for k in keys if k[0] in ("flux", "image_i")})
 
 
+def make_recommended():
+    src = oracle.reference_source()
+    if src is None:
+        raise SystemExit("the reference source tree is needed to read its parameter file")
+    text = (src.parent / "params" / RECOMMENDED_PAR).read_text()
+    lines = [ln.strip() for ln in text.splitlines() if ln.strip() and not ln.strip().startswith("#")]
+    params, model, freqs = recommended_case()
+    px = recommended_pixels(8)
+
+    def run(kind):
+        return oracle.image_riaf_pixels(params, model, freqs, px, kind=kind, threads=0)
+
+    ref = run("reference")
+
+    def perturbed(seed):
+        oracle.set_libm_perturbation(seed, "reference_ulp")
+        return run("reference_ulp")
+
+    cond = conditioning_over(perturbed, ref.arrays, tuple(range(1, 9)))
+    keys = sorted(cond, key=cond_key)
+    np.savez_compressed(OUT / "riaf_recommended.npz", par_lines=np.array(lines), pixels=px,
+                        cond_keys=np.array([cond_key(k) for k in keys]),
+                        cond_vals=np.array([cond[k] for k in keys]),
+                        **{k: v[..., px] for k, v in ref.arrays.items()})
+    print("riaf_recommended", len(lines), "settings;", np.bincount(ref.reason[px], minlength=8)[:8],
+          {cond_key(k): "%.1e" % cond[k] for k in keys if k[0] in ("flux", "image_i") or k in ("pass_a_steps", "steps")})
+
+
 def make_sampling():
     rng = np.random.default_rng(7001)
     times = np.cumsum(np.concatenate([[40.0], rng.uniform(4.0, 16.0, size=15)]))
@@ -209,6 +246,9 @@ def main():
         return
     if "--bl" in sys.argv[1:]:
         make_bl()
+        return
+    if "--recommended" in sys.argv[1:]:
+        make_recommended()
         return
     if "--steps" in sys.argv[1:]:
         make_steps()
@@ -243,6 +283,7 @@ def main():
     make_steps()
     make_sampling()
     make_bl()
+    make_recommended()
 
 
 if __name__ == "__main__":

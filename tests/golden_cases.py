@@ -154,6 +154,10 @@ def conditioning_over(run, ref, seeds):
         for key in _abi.DIAG_FIELDS:
             d = np.abs(res.arrays[key][ok] - ref[key][ok])
             out[key] = max(out.get(key, 0.0), float(d.max()) if d.size else 0.0)
+        # step counts: the largest change of any pixel's count
+        for key in ("pass_a_steps", "steps"):
+            d = np.abs(res.arrays[key].astype(np.int64) - ref[key].astype(np.int64))
+            out[key] = max(out.get(key, 0.0), float(d.max()) if d.size else 0.0)
     return out
 
 
@@ -300,3 +304,30 @@ def bl_conditioning_of(params, model, freqs, ref, seeds=tuple(range(1, 9))):
         return oracle.image_riaf(params, model, freqs, kind="reference_ulp", threads=0)
 
     return conditioning_over(run, ref, seeds)
+
+
+# params/riaf_recommended.par of the reference: its settings in file order
+# (comments and blank lines dropped), the image kp_model_image replays.
+RECOMMENDED_PAR = "riaf_recommended.par"
+
+
+def recommended_case():
+    """The parameters kp_model_image resolves from riaf_recommended.par
+    (pinhole, Boyer-Lindquist, 256^2, r = 1000 M, i = 85 deg, fov 0.08 read
+    after xspan, a = 0.9375, adaptive 1e-10, 230 GHz, the Sgr A*-like RIAF
+    plasma with the symphony fit)."""
+    params = configs.riaf_params(256, 256, spin=0.9375, radius=1000.0, inclination_deg=85.0, xspan=40.0,
+                                 step=0.025, adaptive=1, max_steps=400000, adaptive_tolerance=1e-10,
+                                 min_step=1e-10, max_step=2.0, max_radiation_step=2.0, max_radiation_depth=1.0,
+                                 max_absorption_depth=1.0, max_faraday_depth=4.0,
+                                 coordinate=_abi.COORD_BOYER_LINDQUIST)
+    model = configs.riaf_model(freq=230.0e9, mbh_solar=4.3e6, ne_unit=5.0e6, te_unit=1.0e11, disk_h=0.35,
+                               fit=_abi.FIT_PANDYA)
+    return params, model, [230.0e9]
+
+
+def recommended_pixels(step: int = 16):
+    """A (256/step)^2 lattice of the 256^2 image, pixel = iy * 256 + ix with
+    ix, iy = step/2 + step k."""
+    c = np.arange(step // 2, 256, step)
+    return (c[:, None] * 256 + c[None, :]).ravel().astype(np.int32)

@@ -133,3 +133,51 @@ def test_tool_mixed_precision_within_budget(tmp_path):
         fluxes[prec] = [float(line.split()[1]) for line in r.stdout.splitlines() if line.startswith("flux_I_Jy ")]
     for a, b in zip(fluxes["fp64"], fluxes["mixed"]):
         assert abs(b / a - 1.0) <= 1e-4, (a, b)
+
+
+@pytest.mark.gpu
+def test_tool_replays_riaf_recommended_par(tmp_path):
+    """The reference's params/riaf_recommended.par, every setting as the file
+    gives it (Boyer-Lindquist, 256^2, adaptive 1e-10, format=hdf5,
+    output=riaf_recommended.h5, parameter_output=auto), through kp_model_image:
+    the HDF5 image (read by tests/hdf5_subset.py) equals the library's own
+    image of the same parameters packed with kp_pack_image, and its 32 x 32
+    pixel lattice matches the reference's templates under the FP64 bars of
+    tests/test_gpu_parity.py with the sample's +-2-ulp libm conditioning."""
+    import hdf5_subset as h5
+    from golden_cases import recommended_case
+    from test_gpu_parity import check_fp64
+    from kpolaris_b200 import _abi
+
+    assert TOOL.exists(), "kp_model_image not built"
+    fx = np.load(ROOT / "tests" / "golden" / "riaf_recommended.npz")
+    par = tmp_path / "riaf_recommended.par"
+    par.write_text("\n".join(str(x) for x in fx["par_lines"]) + "\n")
+    r = subprocess.run([str(TOOL), f"--parameter_file={par}"], cwd=tmp_path, capture_output=True, text=True,
+                       timeout=1200)
+    assert r.returncode == 0, r.stderr
+    out = tmp_path / "riaf_recommended.h5"
+    assert out.exists() and (tmp_path / "riaf_recommended.h5.params").exists()
+    f = h5.read(out)
+    assert f.attrs["schema"] == "kpolaris_image" and f.attrs["coordinate"] == "boyer_lindquist"
+    assert (f.attrs["nx"], f.attrs["ny"], f.attrs["nfreq"]) == (256, 256, 1)
+
+    params, model, freqs = recommended_case()
+    res = kp.image_riaf(params, model, freqs)
+    pk = kp.pack_image(res, 0, freqs[0], evpa_0="N")
+    g = f["frame_0/freq_0"]
+    for name, key in (("I_inv", "i_inv"), ("Q_inv", "q_inv"), ("U_inv", "u_inv"), ("V_inv", "v_inv"),
+                      ("I", "i_nu"), ("Q", "q_nu"), ("U", "u_nu"), ("V", "v_nu")):
+        assert np.array_equal(g[name].value.ravel(), pk[key]), name
+    dg = f["frame_0/diagnostics"]
+    assert np.array_equal(dg["reason"].value.ravel(), res.reason)
+    assert np.array_equal(dg["pass_a_steps"].value.ravel(), res.pass_a_steps)
+    assert np.array_equal(dg["steps"].value.ravel(), res.steps)
+
+    px = fx["pixels"]
+    sample = _abi.ImageHostData(npix=len(px), nfreq=1, arrays={k: v[..., px] for k, v in res.arrays.items()})
+    cond = {}
+    for k, v in zip(fx["cond_keys"], fx["cond_vals"]):
+        key, _, fr = str(k).partition(":")
+        cond[(key, int(fr)) if fr else key] = float(v)
+    check_fp64(sample, fx, fixed=False, conditioning=cond)

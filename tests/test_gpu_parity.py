@@ -5,7 +5,8 @@ FP64 bar (stated per result):
     bit-exact.
   * adaptive runs: the step controller evaluates pow(tol/err, 0.2), so an ulp
     of libm can change an accepted step; reasons must agree exactly, step
-    counts within +-2 (90% identical).
+    counts within +-2 (or within the reference's own step-count spread under
+    the +-2-ulp probe, where a fixture records it) and 90% identical.
   * Stokes I/Q/U/V per channel and frequency: max |gpu - oracle| within
     max(base, 2 x conditioning) * max |oracle| (base 1e-10 fixed step, 1e-9
     adaptive); total flux (image-integrated Stokes I) within max(1e-10,
@@ -66,7 +67,9 @@ def check_fp64(res, ref, fixed: bool, conditioning=None):
     else:
         da = np.abs(res.pass_a_steps.astype(np.int64) - _get(ref, "pass_a_steps"))
         db = np.abs(res.steps.astype(np.int64) - _get(ref, "steps"))
-        assert (da <= 2).all() and (db <= 2).all()
+        # +-2, or the reference's own step-count spread under +-2-ulp libm
+        assert (da <= max(2.0, cond.get("pass_a_steps", 0.0))).all(), int(da.max())
+        assert (db <= max(2.0, cond.get("steps", 0.0))).all(), int(db.max())
         assert np.mean(da == 0) >= 0.9 and np.mean(db == 0) >= 0.9
     base = STOKES_RTOL if fixed else STOKES_RTOL_ADAPTIVE
     for (key, f), e in stokes_error(res, ref).items():

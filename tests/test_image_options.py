@@ -270,7 +270,17 @@ def test_frequency_grid_and_chunks(exes, par_dir):
     assert int(lines["effective_multifrequency_chunk_size"]) == 2
 
 
-def test_hdf5_output_is_refused(exes, tmp_path):
+def test_output_format_selection(exes, tmp_path):
+    """format=hdf5, or format=auto with an output ending in .h5, selects the
+    HDF5 image (tools/kpolaris_model_image.cpp:4112-4117); an unknown format
+    is refused before any work."""
     tool, _ = exes
-    r = _run(tool, [f"--output={tmp_path / 'x.h5'}"])
-    assert r.returncode != 0 and "HDF5" in r.stderr
+    r = _run(tool, [f"--output={tmp_path / 'x.h5'}", "--kp_dry_run=1"])
+    assert r.returncode == 0, r.stderr
+    assert "format hdf5" in r.stdout
+    r = _run(tool, [f"--output={tmp_path / 'x.csv'}", "--kp_dry_run=1"])
+    assert r.returncode == 0 and "format csv" in r.stdout, r.stderr
+    r = _run(tool, [f"--output={tmp_path / 'x.csv'}", "--format=hdf5", "--kp_dry_run=1"])
+    assert r.returncode == 0 and "format hdf5" in r.stdout, r.stderr
+    r = _run(tool, [f"--output={tmp_path / 'x.out'}", "--format=fits"])
+    assert r.returncode != 0 and "unknown output format" in r.stderr
