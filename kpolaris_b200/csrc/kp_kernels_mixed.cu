@@ -6,16 +6,12 @@
 // same compiled code traces a ray whatever the rest of the batch is.
 #include <cuda_runtime.h>
 
-#include <cstdlib>
-#include <cstring>
-
-#include "kp_far.cuh"
 #include "kp_launch.h"
 #include "kp_persistent.cuh"
 
 // resident CTAs per SM the wavefront kernels are compiled for
 #ifndef KP_FAR_MIN_BLOCKS
-#define KP_FAR_MIN_BLOCKS 4
+#define KP_FAR_MIN_BLOCKS 3
 #endif
 #ifndef KP_NEAR_MIN_BLOCKS
 #define KP_NEAR_MIN_BLOCKS 1
@@ -23,45 +19,9 @@
 
 namespace kp {
 
-// The far phase: the stage-loop kernel of kp_far.cuh (dynamic shared memory
-// kFarSmemBytes per CTA).
 __global__ void __launch_bounds__(kFarThreads, KP_FAR_MIN_BLOCKS) wave_far_mixed(const WaveDesc W) {
-    far_body<SceneRiaf, kMaxFreq, false>(W);
-}
-
-__global__ void __launch_bounds__(kFarThreads, KP_FAR_MIN_BLOCKS) wave_far_mixed_exact(const WaveDesc W) {
-    far_body<SceneRiaf, kMaxFreq, true>(W);
-}
-
-__global__ void __launch_bounds__(kFarThreads, 3) wave_far_mixed_mb3(const WaveDesc W) {
-    far_body<SceneRiaf, kMaxFreq, false>(W);
-}
-
-__global__ void __launch_bounds__(kFarThreads, 3) wave_far_mixed_generic(const WaveDesc W) {
     persistent_body<PolicyMixed, kMaxFreq, kPhaseFar>(W);
 }
-
-// development switch between the far kernels (KP_FAR_KERNEL=fast|exact|fast3;
-// default: the generic persistent body)
-static int far_variant() {
-    static int v = -1;
-    if (v < 0) {
-        const char* e = std::getenv("KP_FAR_KERNEL");
-        v = (e && !std::strcmp(e, "fast")) ? 0 : (e && !std::strcmp(e, "exact")) ? 1
-            : (e && !std::strcmp(e, "fast3")) ? 3 : 2;
-    }
-    return v;
-}
-
-static const void* far_kernel() {
-    const int v = far_variant();
-    return v == 2 ? reinterpret_cast<const void*>(wave_far_mixed_generic)
-           : v == 1 ? reinterpret_cast<const void*>(wave_far_mixed_exact)
-           : v == 3 ? reinterpret_cast<const void*>(wave_far_mixed_mb3)
-                    : reinterpret_cast<const void*>(wave_far_mixed);
-}
-
-static size_t far_smem() { return far_variant() == 2 ? 0 : kFarSmemBytes; }
 
 __global__ void __launch_bounds__(kNearThreads, KP_NEAR_MIN_BLOCKS) wave_near_a_mixed(const WaveDesc W) {
     persistent_body<PolicyMixed, kMaxFreq, kPhaseNearA>(W);
@@ -72,23 +32,15 @@ __global__ void __launch_bounds__(kNearThreads, KP_NEAR_MIN_BLOCKS) wave_near_b_
 }
 
 static const void* wave_kernel_mixed(int phase) {
-    if (phase == kPhaseFar) return far_kernel();
+    if (phase == kPhaseFar) return reinterpret_cast<const void*>(wave_far_mixed);
     if (phase == kPhaseNearA) return reinterpret_cast<const void*>(wave_near_a_mixed);
     return reinterpret_cast<const void*>(wave_near_b_mixed);
-}
-
-static size_t wave_smem_mixed(int phase) {
-    if (phase != kPhaseFar) return 0;
-    const size_t bytes = far_smem();
-    if (bytes > 0) cudaFuncSetAttribute(far_kernel(), cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes));
-    return bytes;
 }
 
 cudaError_t launch_wave_mixed(int phase, const WaveDesc& W, int blocks, int threads, cudaStream_t stream) {
     if (phase < 0 || phase >= kPhases) return cudaErrorInvalidValue;
     void* args[] = {const_cast<WaveDesc*>(&W)};
-    const size_t smem = wave_smem_mixed(phase);
-    return cudaLaunchKernel(wave_kernel_mixed(phase), dim3(blocks), dim3(threads), args, smem, stream);
+    return cudaLaunchKernel(wave_kernel_mixed(phase), dim3(blocks), dim3(threads), args, 0, stream);
 }
 
 __global__ void __launch_bounds__(128) seed_mixed(const JobDesc* jobs, const SeedEntry* entries,
@@ -109,8 +61,7 @@ cudaError_t launch_seed_mixed(const JobDesc* jobs, const SeedEntry* entries, con
 int wave_occupancy_mixed(int phase, int threads) {
     if (phase < 0 || phase >= kPhases) return 0;
     int n = 0;
-    const size_t smem = wave_smem_mixed(phase);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wave_kernel_mixed(phase), threads, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, wave_kernel_mixed(phase), threads, 0);
     return n;
 }
 
