@@ -43,7 +43,9 @@ typedef enum kp_status {
     KP_ERR_UNSUPPORTED = -5, /* feature/combination not built (reference: std::runtime_error) */
     KP_ERR_BUSY = -6,        /* admission refused: not enough device memory / slots */
     KP_ERR_NOT_FOUND = -7,   /* unknown handle or job id */
-    KP_ERR_CANCELLED = -8    /* job was cancelled before completion */
+    KP_ERR_CANCELLED = -8,   /* job was cancelled before completion */
+    KP_ERR_IO = -9           /* input file missing, unreadable or malformed (reference: std::runtime_error
+                                from its loaders and H5::Exception from the HDF5 library) */
 } kp_status;
 
 /* Reference CoordinateSystem (src/common/types.hpp:51-57). */
@@ -256,7 +258,8 @@ int kp_abi_version(void);
 /* sizeof of the ABI structs, for the bindings' layout check:
  * 0 kp_camera_params, 1 kp_emission_selection, 2 kp_pass_a_params,
  * 3 kp_riaf_model, 4 kp_image_out, 5 kp_run_options, 7 kp_riaf_job,
- * 8 kp_batch_stats, 12 kp_analysis_config, 13 kp_analysis_out; 6 is the bytes of the per-image job descriptor an
+ * 8 kp_batch_stats, 9 kp_tuning, 10 kp_grmhd_model, 11 kp_grmhd_job, 12 kp_analysis_config,
+ * 13 kp_analysis_out, 14 kp_iharm_options; 6 is the bytes of the per-image job descriptor an
  * image uploads to the device; 0 for other ids. */
 size_t kp_abi_sizeof(int which);
 
@@ -462,6 +465,36 @@ int kp_grid_upload(const kp_grmhd_model* model, const float* prims, int device, 
  * the grid has none). */
 int kp_grid_derived(const kp_grid* grid, double* out);
 int kp_grid_release(kp_grid* grid);
+
+/*
+ * iharm GRMHD dumps (HDF5 files written by the HDF5 library: header
+ * datasets, /header/geom/{fmks,mmks}, /prims [n1][n2][n3][>=8]).
+ * kp_iharm_options holds the fields of IHARMLoadOptions
+ * (src/grmhd/iharm_loader.hpp:10-44) this path uses; the defaults are the
+ * reference's.  kp_iharm_read replaces the reading half of
+ * load_iharm_model_from_hdf5 (src/grmhd/iharm_loader.cpp:254-370): it fills
+ * `model` from the header and the options, applies the reference's checks
+ * with its messages, and with `prims` non-NULL writes the first eight
+ * primitives as FP32 [8][n1][n2][n3] (capacity in floats; KP_ERR_INVALID if
+ * short).  With `prims` NULL only the header is read (no device needed).
+ * kp_grid_load_iharm is kp_iharm_read followed by kp_grid_upload (the
+ * derived-scalar precompute of :402-520 runs on the device at upload).
+ * kp_iharm_dump_time replaces read_iharm_dump_time (:240-252).  File and
+ * format errors return KP_ERR_IO.
+ */
+typedef struct kp_iharm_options {
+    double freq_cgs, M_unit, mbh_solar;
+    double trat_small, trat_large, beta_crit, sigma_cut, sigma_cut_high;
+    int emission_type;
+    int interpolate_derived_scalars;
+} kp_iharm_options;
+
+void kp_default_iharm_options(kp_iharm_options* o);
+int kp_iharm_read(const char* path, const kp_iharm_options* options, kp_grmhd_model* model, float* prims,
+                  size_t capacity);
+int kp_grid_load_iharm(const char* path, const kp_iharm_options* options, int device, kp_grmhd_model* model,
+                       kp_grid** out);
+int kp_iharm_dump_time(const char* path, double* t);
 
 /*
  * One GRMHD image in FMKS coordinates, 1..KP_MAX_FREQUENCIES frequencies on

@@ -70,6 +70,12 @@ def library() -> C.CDLL:
     L.kp_grid_upload.argtypes = [C.POINTER(_abi.GrmhdModel), C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_void_p)]
     L.kp_grid_derived.argtypes = [C.c_void_p, C.POINTER(C.c_double)]
     L.kp_grid_release.argtypes = [C.c_void_p]
+    L.kp_default_iharm_options.argtypes = [C.POINTER(_abi.IharmOptions)]
+    L.kp_iharm_read.argtypes = [C.c_char_p, C.POINTER(_abi.IharmOptions), C.POINTER(_abi.GrmhdModel),
+                                C.POINTER(C.c_float), C.c_size_t]
+    L.kp_grid_load_iharm.argtypes = [C.c_char_p, C.POINTER(_abi.IharmOptions), C.c_int,
+                                     C.POINTER(_abi.GrmhdModel), C.POINTER(C.c_void_p)]
+    L.kp_iharm_dump_time.argtypes = [C.c_char_p, C.POINTER(C.c_double)]
     L.kp_image_grmhd.argtypes = [C.POINTER(PassAParams), C.c_void_p, C.c_int, C.POINTER(C.c_double), C.c_int,
                                  C.POINTER(RunOptions), C.POINTER(_abi.ImageOut)]
     L.kp_image_grmhd_slow_light.argtypes = [
@@ -283,6 +289,50 @@ class Grid:
 
     def __exit__(self, *exc):
         self.release()
+
+
+def default_iharm_options(**overrides) -> _abi.IharmOptions:
+    """kp_default_iharm_options (IHARMLoadOptions defaults,
+    src/grmhd/iharm_loader.hpp:10-44), with keyword overrides."""
+    o = _abi.IharmOptions()
+    library().kp_default_iharm_options(C.byref(o))
+    for k, v in overrides.items():
+        setattr(o, k, v)
+    return o
+
+
+def iharm_read(path, options: _abi.IharmOptions | None = None, *, header_only: bool = False):
+    """kp_iharm_read: (model, prims [8, n1, n2, n3] float32, or None with
+    header_only) from an iharm HDF5 dump, on the host."""
+    L = library()
+    o = options if options is not None else default_iharm_options()
+    m = _abi.GrmhdModel()
+    check(L.kp_iharm_read(str(path).encode(), C.byref(o), C.byref(m), None, 0))
+    if header_only:
+        return m, None
+    prims = np.empty((8, m.n1, m.n2, m.n3), dtype=np.float32)
+    check(L.kp_iharm_read(str(path).encode(), C.byref(o), C.byref(m),
+                          prims.ctypes.data_as(C.POINTER(C.c_float)), prims.size))
+    return m, prims
+
+
+def iharm_dump_time(path) -> float:
+    """kp_iharm_dump_time: /t, else /header/t."""
+    t = C.c_double()
+    check(library().kp_iharm_dump_time(str(path).encode(), C.byref(t)))
+    return t.value
+
+
+def grid_load_iharm(path, options: _abi.IharmOptions | None = None, device: int = 0) -> "Grid":
+    """kp_grid_load_iharm: an iharm dump read and uploaded as a resident Grid."""
+    L = library()
+    o = options if options is not None else default_iharm_options()
+    m = _abi.GrmhdModel()
+    h = C.c_void_p()
+    check(L.kp_grid_load_iharm(str(path).encode(), C.byref(o), int(device), C.byref(m), C.byref(h)))
+    g = Grid.__new__(Grid)
+    g._h, g.model, g.device = h, m, device
+    return g
 
 
 def image_grmhd(params: PassAParams, grid: Grid, frequencies=None, *, radiation_substeps=1,

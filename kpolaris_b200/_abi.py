@@ -23,6 +23,7 @@ KP_ERR_UNSUPPORTED = -5
 KP_ERR_BUSY = -6
 KP_ERR_NOT_FOUND = -7
 KP_ERR_CANCELLED = -8
+KP_ERR_IO = -9
 
 COORD_CARTESIAN_KS = 0
 COORD_BOYER_LINDQUIST = 1
@@ -152,6 +153,16 @@ class GrmhdModel(C.Structure):
         ("emission_scale", C.c_double), ("absorption_scale", C.c_double), ("faraday_scale", C.c_double),
         ("max_pol_frac", C.c_double),
         ("has_derived_scalars", C.c_int),
+    ]
+
+
+class IharmOptions(C.Structure):
+    """kp_iharm_options: the IHARMLoadOptions fields the iharm reader uses."""
+    _fields_ = [
+        ("freq_cgs", C.c_double), ("M_unit", C.c_double), ("mbh_solar", C.c_double),
+        ("trat_small", C.c_double), ("trat_large", C.c_double), ("beta_crit", C.c_double),
+        ("sigma_cut", C.c_double), ("sigma_cut_high", C.c_double),
+        ("emission_type", C.c_int), ("interpolate_derived_scalars", C.c_int),
     ]
 
 

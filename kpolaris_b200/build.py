@@ -46,6 +46,7 @@ UNITS = {
     "kp_noalloc.cu": ["--fmad=false"],
     "kp_server.cu": ["--fmad=false"],
     "kp_peak.cu": [],
+    "kp_io.cu": [f"-I{HOST}"],
 }
 
 
@@ -55,7 +56,8 @@ def nvcc() -> str:
 
 
 def _headers():
-    return list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + [INCLUDE / "kpolaris_b200.h"]
+    return (list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + list(HOST.glob("*.hpp")) +
+            [INCLUDE / "kpolaris_b200.h"])
 
 
 def _stale(target: Path, deps) -> bool:
@@ -96,7 +98,7 @@ def build(force: bool = False, jobs: int = 4, verbose: bool = False) -> Path:
         with ThreadPoolExecutor(max_workers=max(1, jobs)) as ex:
             list(ex.map(lambda uf: _compile(uf[0], uf[1], verbose), todo))
     if force or todo or _stale(LIB, objs):
-        cmd = [nvcc(), *ARCH, "-shared", "-o", str(LIB), *map(str, objs)]
+        cmd = [nvcc(), *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lz"]
         if verbose:
             print(" ".join(cmd), flush=True)
         res = subprocess.run(cmd, capture_output=True, text=True)

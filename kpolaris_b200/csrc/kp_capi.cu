@@ -775,6 +775,7 @@ size_t kp_abi_sizeof(int which) {
     case 11: return sizeof(kp_grmhd_job);
     case 12: return sizeof(kp_analysis_config);
     case 13: return sizeof(kp_analysis_out);
+    case 14: return sizeof(kp_iharm_options);
     default: return 0;
     }
 }

@@ -50,6 +50,7 @@ def test_struct_layouts_match_ctypes_mirror():
     assert lib.kp_abi_sizeof(11) == C.sizeof(_abi.GrmhdJob)
     assert lib.kp_abi_sizeof(12) == C.sizeof(_abi.AnalysisConfig)
     assert lib.kp_abi_sizeof(13) == C.sizeof(_abi.AnalysisOut)
+    assert lib.kp_abi_sizeof(14) == C.sizeof(_abi.IharmOptions)
     assert lib.kp_abi_sizeof(6) > 0
     assert lib.kp_abi_sizeof(99) == 0
 
