@@ -33,6 +33,9 @@ extern "C" {
 /* Maximum frequencies that share one geodesic in a single launch
  * (reference compile-time KPOLARIS_MAX_FREQUENCIES, src/common/types.hpp:5-7). */
 #define KP_MAX_FREQUENCIES 4
+/* Longest step-control frequency list of kp_image_riaf_step_control and
+ * kp_image_grmhd_step_control. */
+#define KP_MAX_CONTROL_FREQUENCIES 64
 
 typedef enum kp_status {
     KP_OK = 0,
@@ -290,6 +293,25 @@ int kp_image_riaf(const kp_pass_a_params* params,
                   kp_image_out* out);
 
 /*
+ * RIAF image of 1..4 frequencies whose pass-B step control (the radiation
+ * substep counts and the predictive step cap) takes the largest count over a
+ * separate step-control frequency list, so that every chunk of a longer
+ * frequency list follows one geodesic.  Replaces
+ * run_riaf_multifrequency_image with step_control_frequencies
+ * (src/image/riaf.cpp:79-105 -> run_multifrequency_image_metric_with_step_control,
+ * src/image/multifrequency.hpp:152-236; per-pixel loop
+ * trace_pass_b_segment_model_multifrequency_control_pixel_metric,
+ * src/geodesic/pass_b.hpp:1505-1895) as the image tool calls it for each
+ * chunk of its frequency grid (tools/kpolaris_model_image.cpp:3432-3446).
+ * A control list equal to the frequency list (same length and values, the
+ * reference's test) is the plain kp_image_riaf.  1 <= ncontrol <=
+ * KP_MAX_CONTROL_FREQUENCIES; every control frequency finite and positive.
+ */
+int kp_image_riaf_step_control(const kp_pass_a_params* params, const kp_riaf_model* model, int radiation_substeps,
+                               const double* frequencies, int nfreq, const double* control_frequencies,
+                               int ncontrol, const kp_run_options* options, kp_image_out* out);
+
+/*
  * Analysis mode (the reference's analysis_mode=1 image path,
  * src/image/analysis_driver.hpp): the FP64 per-pixel image with
  * line-of-sight diagnostics accumulated along pass B.  Single frequency;
@@ -506,6 +528,13 @@ int kp_iharm_dump_time(const char* path, double* t);
  */
 int kp_image_grmhd(const kp_pass_a_params* params, const kp_grid* grid, int radiation_substeps,
                    const double* frequencies, int nfreq, const kp_run_options* options, kp_image_out* out);
+
+/* kp_image_grmhd with a separate step-control frequency list, as
+ * kp_image_riaf_step_control (the GRMHD backends' multi-frequency images,
+ * src/image/grmhd.cpp:131-170, with step_control_frequencies). */
+int kp_image_grmhd_step_control(const kp_pass_a_params* params, const kp_grid* grid, int radiation_substeps,
+                                const double* frequencies, int nfreq, const double* control_frequencies,
+                                int ncontrol, const kp_run_options* options, kp_image_out* out);
 
 /*
  * One slow-light GRMHD image: nsnap >= 2 resident snapshots of one flow

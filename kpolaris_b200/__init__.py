@@ -78,6 +78,12 @@ def library() -> C.CDLL:
     L.kp_iharm_dump_time.argtypes = [C.c_char_p, C.POINTER(C.c_double)]
     L.kp_image_grmhd.argtypes = [C.POINTER(PassAParams), C.c_void_p, C.c_int, C.POINTER(C.c_double), C.c_int,
                                  C.POINTER(RunOptions), C.POINTER(_abi.ImageOut)]
+    L.kp_image_riaf_step_control.argtypes = [C.POINTER(PassAParams), C.POINTER(RIAFModel), C.c_int,
+                                             C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_double), C.c_int,
+                                             C.POINTER(RunOptions), C.POINTER(_abi.ImageOut)]
+    L.kp_image_grmhd_step_control.argtypes = [C.POINTER(PassAParams), C.c_void_p, C.c_int, C.POINTER(C.c_double),
+                                              C.c_int, C.POINTER(C.c_double), C.c_int, C.POINTER(RunOptions),
+                                              C.POINTER(_abi.ImageOut)]
     L.kp_image_grmhd_slow_light.argtypes = [
         C.POINTER(PassAParams), C.POINTER(C.c_void_p), C.POINTER(C.c_double), C.c_int, C.c_double, C.c_int,
         C.POINTER(C.c_double), C.c_int, C.POINTER(_abi.RunOptions), C.POINTER(_abi.ImageOut)]
@@ -128,8 +134,10 @@ def _options(precision=_abi.PRECISION_FP64, schedule=_abi.SCHEDULE_PER_PIXEL,
 
 
 def image_riaf(params: PassAParams, model: RIAFModel, frequencies=None, *, radiation_substeps=1,
-               out: ImageHostData | None = None, **options) -> ImageHostData:
-    """One RIAF image with 1..4 frequencies sharing each pixel's geodesic, host outputs."""
+               out: ImageHostData | None = None, control_frequencies=None, **options) -> ImageHostData:
+    """One RIAF image with 1..4 frequencies sharing each pixel's geodesic,
+    host outputs.  With `control_frequencies` the pass-B step control takes
+    its substep counts over that list (kp_image_riaf_step_control)."""
     L = library()
     if frequencies is None:
         frequencies = [model.freq_cgs]
@@ -140,8 +148,13 @@ def image_riaf(params: PassAParams, model: RIAFModel, frequencies=None, *, radia
     fa = (C.c_double * max(nfreq, 1))(*frequencies)
     s = out.as_struct()
     opt = _options(**options)
-    check(L.kp_image_riaf(C.byref(params), C.byref(model), int(radiation_substeps), fa, nfreq,
-                          C.byref(opt), C.byref(s)))
+    if control_frequencies is None:
+        check(L.kp_image_riaf(C.byref(params), C.byref(model), int(radiation_substeps), fa, nfreq,
+                              C.byref(opt), C.byref(s)))
+    else:
+        ca = (C.c_double * max(len(control_frequencies), 1))(*control_frequencies)
+        check(L.kp_image_riaf_step_control(C.byref(params), C.byref(model), int(radiation_substeps), fa, nfreq,
+                                           ca, len(control_frequencies), C.byref(opt), C.byref(s)))
     return out
 
 
@@ -336,9 +349,10 @@ def grid_load_iharm(path, options: _abi.IharmOptions | None = None, device: int 
 
 
 def image_grmhd(params: PassAParams, grid: Grid, frequencies=None, *, radiation_substeps=1,
-                out: ImageHostData | None = None, **options) -> ImageHostData:
+                out: ImageHostData | None = None, control_frequencies=None, **options) -> ImageHostData:
     """One GRMHD image in FMKS coordinates (kp_image_grmhd), host outputs.
-    Mirrors run_grmhd_image (src/image/grmhd.hpp:12-32)."""
+    Mirrors run_grmhd_image (src/image/grmhd.hpp:12-32); with
+    `control_frequencies`, kp_image_grmhd_step_control."""
     L = library()
     if frequencies is None:
         frequencies = [grid.model.freq_cgs]
@@ -350,7 +364,13 @@ def image_grmhd(params: PassAParams, grid: Grid, frequencies=None, *, radiation_
     s = out.as_struct()
     options.setdefault("device", grid.device)
     opt = _options(**options)
-    check(L.kp_image_grmhd(C.byref(params), grid._h, int(radiation_substeps), fa, nfreq, C.byref(opt), C.byref(s)))
+    if control_frequencies is None:
+        check(L.kp_image_grmhd(C.byref(params), grid._h, int(radiation_substeps), fa, nfreq, C.byref(opt),
+                               C.byref(s)))
+    else:
+        ca = (C.c_double * max(len(control_frequencies), 1))(*control_frequencies)
+        check(L.kp_image_grmhd_step_control(C.byref(params), grid._h, int(radiation_substeps), fa, nfreq, ca,
+                                            len(control_frequencies), C.byref(opt), C.byref(s)))
     return out
 
 

@@ -354,6 +354,12 @@ int validate_riaf(const kp_pass_a_params* p, const kp_riaf_model* m, const doubl
     return KP_OK;
 }
 
+// GM/c^2 in cm of the RIAF model's mass (riaf.hpp:76-81).
+double riaf_length_unit(const kp_riaf_model* m) {
+    const double gnewt = 6.67430e-8, msun = 1.98847e33, cl = 2.99792458e10;
+    return gnewt * m->mbh_solar * msun / (cl * cl);
+}
+
 // Resolves one image's launch constants on the host.
 ImageConsts make_consts(const kp_pass_a_params* p, const kp_riaf_model* m, const double* freqs,
                         int nfreq, int integrator) {
@@ -419,8 +425,7 @@ ImageConsts make_consts(const kp_pass_a_params* p, const kp_riaf_model* m, const
     c.fp32_radius = p->outer_radius + 2.0 * std::max(std::fabs(p->max_step), std::fabs(p->step));
     c.fit = m->emission_type == KP_FIT_DEXTER ? 4 : 1;
     c.nfreq = nfreq;
-    const double gnewt = 6.67430e-8, msun = 1.98847e33, cl = 2.99792458e10;
-    const double length_unit = gnewt * m->mbh_solar * msun / (cl * cl);  // riaf.hpp:76-81
+    const double length_unit = riaf_length_unit(m);
     for (int f = 0; f < nfreq; ++f) {
         const double fr = (nfreq == 1 && !freqs) ? m->freq_cgs : freqs[f];
         c.freq[f] = fr;
@@ -493,6 +498,43 @@ int validate_grmhd_model(const kp_grmhd_model* m) {
 ImageConsts make_consts_grmhd(const kp_pass_a_params* p, const kp_grid* g, const double* freqs, int nfreq,
                               int integrator) {
     return image_consts_fmks(p, g->model, grid_consts(g), freqs, nfreq, integrator);
+}
+
+// A step-control frequency list is separate from the image's frequencies
+// when its length or any value differs
+// (run_multifrequency_image_metric_with_step_control,
+// src/image/multifrequency.hpp:174-182); only then is it applied.
+int validate_control(const double* ctl, int nctl) {
+    if (nctl < 1 || !ctl) return set_error(KP_ERR_INVALID, "multifrequency step-control frequency list must not be empty");
+    if (nctl > KP_MAX_CONTROL_FREQUENCIES)
+        return set_error(KP_ERR_INVALID, "step-control frequency list longer than KP_MAX_CONTROL_FREQUENCIES (%d)",
+                         KP_MAX_CONTROL_FREQUENCIES);
+    for (int g = 0; g < nctl; ++g)
+        if (!std::isfinite(ctl[g]) || !(ctl[g] > 0.0))
+            return set_error(KP_ERR_INVALID, "step-control frequency %d must be finite and positive", g);
+    return KP_OK;
+}
+
+bool separate_control(const double* freqs, int nfreq, double single_freq, const double* ctl, int nctl) {
+    if (nctl != nfreq) return true;
+    for (int f = 0; f < nfreq; ++f) {
+        const double fr = (nfreq == 1 && !freqs) ? single_freq : freqs[f];
+        if (fr != ctl[f]) return true;
+    }
+    return false;
+}
+
+// The control list's frequencies, dlambda scales (length unit / frequency)
+// and, for the FP32 fits, 2^E emission scales.
+void apply_control_riaf(ImageConsts& c, const kp_pass_a_params* p, const kp_riaf_model* m, const double* ctl,
+                        int nctl) {
+    const double length_unit = riaf_length_unit(m);
+    c.nctl = nctl;
+    for (int g = 0; g < nctl; ++g) {
+        c.ctl_freq[g] = ctl[g];
+        c.ctl_dlambda_scale[g] = length_unit / std::max(ctl[g], 1.0);
+        c.ctl_emission_scale_pow2[g] = std::ldexp(1.0f, emission_scale_exponent(p, m, ctl[g], c.ctl_dlambda_scale[g]));
+    }
 }
 
 }  // namespace kp
@@ -857,9 +899,13 @@ void kp_default_riaf_model(kp_riaf_model* m) {
     m->min_radius = 1e-6;
 }
 
-int kp_image_riaf(const kp_pass_a_params* params, const kp_riaf_model* model, int radiation_substeps,
-                  const double* frequencies, int nfreq, const kp_run_options* options,
-                  kp_image_out* out) {
+static int batch_riaf_impl(const kp_riaf_job* jobs, int njobs, const kp_run_options* options, kp_batch_stats* stats,
+                           const double* ctl, int nctl);
+
+// kp_image_riaf with an optional separate step-control list (nctl > 0).
+static int image_riaf_impl(const kp_pass_a_params* params, const kp_riaf_model* model, int radiation_substeps,
+                           const double* frequencies, int nfreq, const kp_run_options* options, kp_image_out* out,
+                           const double* ctl, int nctl) {
     (void)radiation_substeps;
     kp_run_options opt;
     if (options) {
@@ -888,13 +934,14 @@ int kp_image_riaf(const kp_pass_a_params* params, const kp_riaf_model* model, in
         job.nfreq = nfreq;
         job.radiation_substeps = radiation_substeps;
         job.out = *out;
-        return kp_batch_riaf(&job, 1, &opt, nullptr);
+        return batch_riaf_impl(&job, 1, &opt, nullptr, ctl, nctl);
     }
     std::lock_guard<std::mutex> lock(g_mutex);
     DeviceState* dev = device_state(opt.device, &st);
     if (!dev) return st;
     cudaStream_t stream = opt.stream ? static_cast<cudaStream_t>(opt.stream) : dev->stream;
-    const ImageConsts c = make_consts(params, model, frequencies, nfreq, opt.integrator);
+    ImageConsts c = make_consts(params, model, frequencies, nfreq, opt.integrator);
+    if (nctl > 0) apply_control_riaf(c, params, model, ctl, nctl);
     ImageOutPtrs dptr;
     if (opt.outputs_on_device) {
         dptr = from_abi(out);
@@ -928,6 +975,24 @@ int kp_image_riaf(const kp_pass_a_params* params, const kp_riaf_model* model, in
         if (e != cudaSuccess) return cuda_error(e, "image kernel");
     }
     return KP_OK;
+}
+
+int kp_image_riaf(const kp_pass_a_params* params, const kp_riaf_model* model, int radiation_substeps,
+                  const double* frequencies, int nfreq, const kp_run_options* options, kp_image_out* out) {
+    return image_riaf_impl(params, model, radiation_substeps, frequencies, nfreq, options, out, nullptr, 0);
+}
+
+int kp_image_riaf_step_control(const kp_pass_a_params* params, const kp_riaf_model* model, int radiation_substeps,
+                               const double* frequencies, int nfreq, const double* control_frequencies,
+                               int ncontrol, const kp_run_options* options, kp_image_out* out) {
+    int st = validate_control(control_frequencies, ncontrol);
+    if (st != KP_OK) return st;
+    st = validate_riaf(params, model, frequencies, nfreq);
+    if (st != KP_OK) return st;
+    if (!separate_control(frequencies, nfreq, model->freq_cgs, control_frequencies, ncontrol))
+        return image_riaf_impl(params, model, radiation_substeps, frequencies, nfreq, options, out, nullptr, 0);
+    return image_riaf_impl(params, model, radiation_substeps, frequencies, nfreq, options, out, control_frequencies,
+                           ncontrol);
 }
 
 void kp_default_analysis_config(kp_analysis_config* cfg) {
@@ -1041,6 +1106,12 @@ int kp_image_riaf_analysis(const kp_pass_a_params* params, const kp_riaf_model* 
 }
 
 int kp_batch_riaf(const kp_riaf_job* jobs, int njobs, const kp_run_options* options, kp_batch_stats* stats) {
+    return batch_riaf_impl(jobs, njobs, options, stats, nullptr, 0);
+}
+
+// kp_batch_riaf; a step-control list (nctl > 0) applies to every job.
+static int batch_riaf_impl(const kp_riaf_job* jobs, int njobs, const kp_run_options* options, kp_batch_stats* stats,
+                           const double* ctl, int nctl) {
     kp_run_options opt;
     if (options) {
         opt = *options;
@@ -1104,6 +1175,7 @@ int kp_batch_riaf(const kp_riaf_job* jobs, int njobs, const kp_run_options* opti
         JobDesc& d = dev->h_jobs[i];
         std::memset(&d, 0, sizeof(d));
         d.c = make_consts(&jb.params, &jb.model, jb.frequencies, jb.nfreq, opt.integrator);
+        if (nctl > 0) apply_control_riaf(d.c, &jb.params, &jb.model, ctl, nctl);
         double fr[5][4];
         host_camera_frame(d.c, fr);
         for (int mu = 0; mu < 4; ++mu) {
@@ -1416,7 +1488,7 @@ bool same_grid_geometry(const kp_grmhd_model& a, const kp_grmhd_model& b) {
 // (nsnap >= 2 resident snapshots at `times`, fluid read at t_obs + x^0).
 int grmhd_image(const kp_pass_a_params* params, const kp_grid* const* grids, const double* times, int nsnap,
                 double t_obs, int radiation_substeps, const double* frequencies, int nfreq,
-                const kp_run_options* options, kp_image_out* out) {
+                const kp_run_options* options, kp_image_out* out, const double* ctl = nullptr, int nctl = 0) {
     const kp_grid* grid = grids ? grids[0] : nullptr;
     if (!params || !grid || !out) return set_error(KP_ERR_INVALID, "GRMHD image: null argument");
     kp_run_options opt;
@@ -1509,6 +1581,7 @@ int grmhd_image(const kp_pass_a_params* params, const kp_grid* const* grids, con
     d.precision = opt.precision;
     const bool mixed = opt.precision == KP_PRECISION_MIXED;
     if (mixed) grmhd_emission_scale(params, grid->model, d.c);
+    if (nctl > 0) grmhd_apply_control(params, grid->model, d.c, ctl, nctl);
     const int family = slow ? (mixed ? kFamilyGrmhdSlowMixed : kFamilyGrmhdSlowFP64)
                             : (mixed ? kFamilyGrmhdMixed : kFamilyGrmhdFP64);
     // mixed kernels are compiled with FMA contraction: one frequency form
@@ -1533,6 +1606,19 @@ int kp_image_grmhd(const kp_pass_a_params* params, const kp_grid* grid, int radi
                    const double* frequencies, int nfreq, const kp_run_options* options, kp_image_out* out) {
     const kp_grid* grids[1] = {grid};
     return grmhd_image(params, grids, nullptr, 0, 0.0, radiation_substeps, frequencies, nfreq, options, out);
+}
+
+int kp_image_grmhd_step_control(const kp_pass_a_params* params, const kp_grid* grid, int radiation_substeps,
+                                const double* frequencies, int nfreq, const double* control_frequencies,
+                                int ncontrol, const kp_run_options* options, kp_image_out* out) {
+    const int st = validate_control(control_frequencies, ncontrol);
+    if (st != KP_OK) return st;
+    if (!grid) return set_error(KP_ERR_INVALID, "GRMHD image: null argument");
+    if (nfreq > 1 && !frequencies) return set_error(KP_ERR_INVALID, "null frequency list");
+    const kp_grid* grids[1] = {grid};
+    const bool separate = separate_control(frequencies, nfreq, grid->model.freq_cgs, control_frequencies, ncontrol);
+    return grmhd_image(params, grids, nullptr, 0, 0.0, radiation_substeps, frequencies, nfreq, options, out,
+                       separate ? control_frequencies : nullptr, separate ? ncontrol : 0);
 }
 
 int kp_image_grmhd_slow_light(const kp_pass_a_params* params, const kp_grid* const* snapshots, const double* times,

@@ -6,6 +6,8 @@
 
 #include <cstdint>
 
+#include "kpolaris_b200.h"
+
 #ifndef KP_HD
 #define KP_HD __host__ __device__ __forceinline__
 #endif
@@ -13,6 +15,7 @@
 namespace kp {
 
 constexpr int kMaxFreq = 4;
+constexpr int kMaxControl = KP_MAX_CONTROL_FREQUENCIES;
 constexpr double kTiny = 1e-300;
 constexpr double kLarge = 1e300;
 constexpr double kPi = 3.141592653589793238462643383279502884;
@@ -120,6 +123,13 @@ struct ImageConsts {
     // mixed path: per-image power-of-two scale applied to j and S
     float emission_scale_pow2[kMaxFreq];
     double inv_emission_scale_pow2[kMaxFreq];
+    // separate step-control frequency list (pass_b.hpp:1505-1895): with
+    // nctl > 0 the pass-B substep counts take the largest count over these
+    // frequencies instead of over freq[]; nctl == 0 is the fused form
+    int nctl;
+    double ctl_freq[kMaxControl];
+    double ctl_dlambda_scale[kMaxControl];
+    float ctl_emission_scale_pow2[kMaxControl];
     // scene: RIAF in Cartesian Kerr-Schild, or a GRMHD grid in FMKS
     int scene;
     FmksParams fmks;

@@ -73,6 +73,9 @@ struct RadTraits<PolicyFP64, SceneRiaf> {
     __device__ static Co coeffs(const ImageConsts& c, const Sample& p, int f) {
         return riaf_coefficients(c, p, c.freq[f]);
     }
+    __device__ static Co coeffs_ctl(const ImageConsts& c, const Sample& p, int g) {
+        return riaf_coefficients(c, p, c.ctl_freq[g]);
+    }
     __device__ static void step(Stokes& s, const Co& co, double h, const ImageConsts& c, int f) {
         stokes_step(s, co, abs_val(h) * c.dlambda_scale[f]);
     }
@@ -93,6 +96,9 @@ struct RadTraits<PolicyMixed, SceneRiaf> {
     }
     __device__ static Co coeffs(const ImageConsts& c, const Sample& p, int f) {
         return riaf_coefficients_f(c, p, float(c.freq[f] * 1e-9), c.emission_scale_pow2[f]);
+    }
+    __device__ static Co coeffs_ctl(const ImageConsts& c, const Sample& p, int g) {
+        return riaf_coefficients_f(c, p, float(c.ctl_freq[g] * 1e-9), c.ctl_emission_scale_pow2[g]);
     }
     __device__ static void step(Stokes& s, const Co& co, double h, const ImageConsts& c, int f) {
         stokes_step_f(s, co, float(abs_val(h) * c.dlambda_scale[f]));
@@ -119,6 +125,9 @@ struct RadTraits<PolicyFP64, SceneGrmhd> {
     }
     __device__ static Co coeffs(const ImageConsts& c, const Sample& p, int f) {
         return grmhd_coefficients(c, p, c.freq[f]);
+    }
+    __device__ static Co coeffs_ctl(const ImageConsts& c, const Sample& p, int g) {
+        return grmhd_coefficients(c, p, c.ctl_freq[g]);
     }
     __device__ static void step(Stokes& s, const Co& co, double h, const ImageConsts& c, int f) {
         stokes_step(s, co, abs_val(h) * c.dlambda_scale[f]);

@@ -137,7 +137,8 @@ inline ImageConsts image_consts_fmks(const kp_pass_a_params* p, const kp_grmhd_m
 // reference plasma point (code density 1, code field 0.05, shape factor bound
 // 30) at 2^-6.  The transfer is linear in the emission, so the image is
 // rescaled by 2^-E in FP64 at the end and E changes only rounding.
-inline void grmhd_emission_scale(const kp_pass_a_params* p, const kp_grmhd_model& m, ImageConsts& c) {
+inline int grmhd_emission_exponent(const kp_pass_a_params* p, const kp_grmhd_model& m, const ImageConsts& c,
+                                   double freq, double dls) {
     const double pi = 3.141592653589793, ee = 4.803204712570263e-10, me = 9.1093826e-28, mp = 1.67262171e-24,
                  cl = 2.99792458e10;
     const double ne = std::max(c.grid.rho_unit / (mp + me) * m.ne_factor, 1e-30);
@@ -145,14 +146,31 @@ inline void grmhd_emission_scale(const kp_pass_a_params* p, const kp_grmhd_model
     const double nu_c = ee * b / (2.0 * pi * me * cl);
     const double j_phys = ne * ee * ee * nu_c / cl * (std::sqrt(2.0) * pi / 27.0) * 30.0;
     const double step = p->max_radiation_step > 0.0 ? p->max_radiation_step : std::max(p->max_step, 1e-3);
+    const double j_inv = j_phys / std::max(freq * freq, 1.0);
+    const double dl = std::max(step * std::fabs(dls), 1e-300);
+    double e = std::floor(std::log2(std::ldexp(1.0, -6) / std::max(j_inv * dl, 1e-300)));
+    if (!(e == e)) e = 0.0;
+    return int(std::min(120.0, std::max(-120.0, e)));
+}
+
+inline void grmhd_emission_scale(const kp_pass_a_params* p, const kp_grmhd_model& m, ImageConsts& c) {
     for (int f = 0; f < c.nfreq; ++f) {
-        const double j_inv = j_phys / std::max(c.freq[f] * c.freq[f], 1.0);
-        const double dl = std::max(step * std::fabs(c.dlambda_scale[f]), 1e-300);
-        double e = std::floor(std::log2(std::ldexp(1.0, -6) / std::max(j_inv * dl, 1e-300)));
-        if (!(e == e)) e = 0.0;
-        const int ei = int(std::min(120.0, std::max(-120.0, e)));
+        const int ei = grmhd_emission_exponent(p, m, c, c.freq[f], c.dlambda_scale[f]);
         c.emission_scale_pow2[f] = std::ldexp(1.0f, ei);
         c.inv_emission_scale_pow2[f] = std::ldexp(1.0, -ei);
+    }
+}
+
+// A separate step-control list of a GRMHD image (the control frequencies,
+// their dlambda scales and FP32 emission scales).
+inline void grmhd_apply_control(const kp_pass_a_params* p, const kp_grmhd_model& m, ImageConsts& c,
+                                const double* ctl, int nctl) {
+    const double length_unit = grmhd_length_unit_cgs(m);
+    c.nctl = nctl;
+    for (int g = 0; g < nctl; ++g) {
+        c.ctl_freq[g] = ctl[g];
+        c.ctl_dlambda_scale[g] = length_unit / std::max(ctl[g], 1.0);
+        c.ctl_emission_scale_pow2[g] = std::ldexp(1.0f, grmhd_emission_exponent(p, m, c, ctl[g], c.ctl_dlambda_scale[g]));
     }
 }
 

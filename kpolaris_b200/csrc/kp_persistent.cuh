@@ -623,16 +623,37 @@ __device__ __forceinline__ void persistent_body(const WaveDesc& W) {
                         }
                         if (radiating && !stopped) ps = RT::sample(c, sample);
                         if (!stopped) {
-                        int required = 1;
                         const int nf = c.nfreq < NF ? c.nfreq : NF;
 #pragma unroll 1
                         for (int f = 0; f < nf; ++f) {
                             co[f] = RT::coeffs(c, ps, f);
                             if (!c.faraday_rotation) co[f].rV = 0.0;
-                            const int cand = radiation_substep_count(co[f], h, c.dlambda_scale[f], local_max_rs,
-                                                                     c.max_radiation_depth, c.max_absorption_depth,
-                                                                     c.max_faraday_depth);
+                        }
+                        // Substep counts at h (required) and at h_current
+                        // (predictive) in one pass: neither test changes h or
+                        // h_current.  Over the image's frequencies, or over a
+                        // separate step-control list (pass_b.hpp:1787-1833).
+                        int required = 1, pred = 1;
+                        const bool fused = c.nctl == 0;
+#pragma unroll 1
+                        for (int g = 0; g < (fused ? nf : c.nctl); ++g) {
+                            typename RT::Co cg;
+                            double dls;
+                            if (fused) {
+                                cg = co[g];
+                                dls = c.dlambda_scale[g];
+                            } else {
+                                cg = RT::coeffs_ctl(c, ps, g);
+                                if (!c.faraday_rotation) cg.rV = 0.0;
+                                dls = c.ctl_dlambda_scale[g];
+                            }
+                            const int cand = radiation_substep_count(cg, h, dls, local_max_rs, c.max_radiation_depth,
+                                                                     c.max_absorption_depth, c.max_faraday_depth);
                             required = cand > required ? cand : required;
+                            const int pc = radiation_substep_count(cg, st.h_current, dls, local_max_rs,
+                                                                   c.max_radiation_depth, c.max_absorption_depth,
+                                                                   c.max_faraday_depth);
+                            pred = pc > pred ? pc : pred;
                         }
                         if (required > 1 && h > c.min_step_abs * 1.0001) {
                             st.h_current = max_val(c.min_step_abs, h / double(required));
@@ -640,14 +661,6 @@ __device__ __forceinline__ void persistent_body(const WaveDesc& W) {
                         } else {
                             if (local_max_rs > 0.0 || c.max_radiation_depth > 0.0 || c.max_absorption_depth > 0.0 ||
                                 c.max_faraday_depth > 0.0) {
-                                int pred = 1;
-#pragma unroll 1
-                                for (int f = 0; f < nf; ++f) {
-                                    const int cand = radiation_substep_count(
-                                        co[f], st.h_current, c.dlambda_scale[f], local_max_rs,
-                                        c.max_radiation_depth, c.max_absorption_depth, c.max_faraday_depth);
-                                    pred = cand > pred ? cand : pred;
-                                }
                                 st.cap = pred > 1 ? max_val(c.min_step_abs, st.h_current / double(pred)) : c.max_step;
                             } else {
                                 st.cap = c.max_step;

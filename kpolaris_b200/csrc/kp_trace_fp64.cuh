@@ -331,15 +331,42 @@ __device__ __forceinline__ void trace_pass_b_fp64(const ImageConsts& c, Ray& sta
         RiafSample ps;
         ps.emitting = 0;
         if (inside) ps = riaf_sample(c, sample);
-        int required = 1;
 #pragma unroll
         for (int f = 0; f < NF; ++f) {
             co[f] = riaf_coefficients(c, ps, c.freq[f]);
             if (!c.faraday_rotation) co[f].rV = 0.0;
-            const int cand = radiation_substep_count(co[f], h, c.dlambda_scale[f], local_max_rs,
-                                                     c.max_radiation_depth, c.max_absorption_depth,
-                                                     c.max_faraday_depth);
-            required = cand > required ? cand : required;
+        }
+        // Substep counts at h (required) and at h_current (predictive) in
+        // one pass: neither test changes h or h_current.  Over the image's
+        // frequencies, or over a separate step-control list
+        // (pass_b.hpp:1787-1833).
+        int required = 1, pred = 1;
+        if (c.nctl == 0) {
+#pragma unroll
+            for (int f = 0; f < NF; ++f) {
+                const int cand = radiation_substep_count(co[f], h, c.dlambda_scale[f], local_max_rs,
+                                                         c.max_radiation_depth, c.max_absorption_depth,
+                                                         c.max_faraday_depth);
+                required = cand > required ? cand : required;
+                const int pc = radiation_substep_count(co[f], h_current, c.dlambda_scale[f], local_max_rs,
+                                                       c.max_radiation_depth, c.max_absorption_depth,
+                                                       c.max_faraday_depth);
+                pred = pc > pred ? pc : pred;
+            }
+        } else {
+#pragma unroll 1
+            for (int g = 0; g < c.nctl; ++g) {
+                Coeffs<double> cg = riaf_coefficients(c, ps, c.ctl_freq[g]);
+                if (!c.faraday_rotation) cg.rV = 0.0;
+                const int cand = radiation_substep_count(cg, h, c.ctl_dlambda_scale[g], local_max_rs,
+                                                         c.max_radiation_depth, c.max_absorption_depth,
+                                                         c.max_faraday_depth);
+                required = cand > required ? cand : required;
+                const int pc = radiation_substep_count(cg, h_current, c.ctl_dlambda_scale[g], local_max_rs,
+                                                       c.max_radiation_depth, c.max_absorption_depth,
+                                                       c.max_faraday_depth);
+                pred = pc > pred ? pc : pred;
+            }
         }
         if (required > 1 && h > eff_min * 1.0001) {
             h_current = max_val(eff_min, h / double(required));
@@ -348,14 +375,6 @@ __device__ __forceinline__ void trace_pass_b_fp64(const ImageConsts& c, Ray& sta
         }
         if (local_max_rs > 0.0 || c.max_radiation_depth > 0.0 || c.max_absorption_depth > 0.0 ||
             c.max_faraday_depth > 0.0) {
-            int pred = 1;
-#pragma unroll
-            for (int f = 0; f < NF; ++f) {
-                const int cand = radiation_substep_count(co[f], h_current, c.dlambda_scale[f], local_max_rs,
-                                                         c.max_radiation_depth, c.max_absorption_depth,
-                                                         c.max_faraday_depth);
-                pred = cand > pred ? cand : pred;
-            }
             cap = pred > 1 ? max_val(eff_min, h_current / double(pred)) : c.max_step;
         } else {
             cap = c.max_step;

@@ -159,6 +159,33 @@ def image_riaf(params, model, freqs, *, kind="port", integrator=0, threads=0,
     return out
 
 
+def image_riaf_control(params, model, freqs, control, *, kind="reference", threads=0, pixel_begin=0,
+                       pixel_end=None, out=None) -> _abi.ImageHostData:
+    """A RIAF image (or pixel range) whose pass-B step control runs over the
+    separate frequency list `control`, through the reference's control
+    variant (kind 'reference' or 'reference_ulp')."""
+    if kind not in ("reference", "reference_ulp"):
+        raise ValueError("the step-control variant runs through the reference oracle")
+    L = lib(kind)
+    L.kpref_image_riaf_control_range.argtypes = [
+        C.POINTER(_abi.PassAParams), C.POINTER(_abi.RIAFModel), C.c_int, C.POINTER(C.c_double), C.c_int,
+        C.POINTER(C.c_double), C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(_abi.ImageOut)]
+    npix = params.camera.nx * params.camera.ny
+    nfreq = len(freqs)
+    if out is None:
+        out = _abi.ImageHostData.allocate(npix, nfreq)
+    if pixel_end is None:
+        pixel_end = npix
+    fa = (C.c_double * nfreq)(*freqs)
+    ca = (C.c_double * len(control))(*control)
+    s = out.as_struct()
+    rc = L.kpref_image_riaf_control_range(C.byref(params), C.byref(model), 1, fa, nfreq, ca, len(control),
+                                          int(threads), int(pixel_begin), int(pixel_end), C.byref(s))
+    if rc != 0:
+        raise RuntimeError(L.kpref_last_error().decode())
+    return out
+
+
 def image_riaf_pixels(params, model, freqs, pixels, *, kind="reference", threads=0, out=None):
     """The listed pixels of a RIAF image through the reference's templates
     in one OpenMP dynamic loop (outputs at their image positions)."""
@@ -319,6 +346,30 @@ def grmhd_derived(model, prims):
     p = np.ascontiguousarray(prims, dtype=np.float64)
     out = np.empty((5,) + p.shape[1:], dtype=np.float64)
     if L.kpref_grmhd_derived(C.byref(model), _dp(p), _dp(out)) != 0:
+        raise RuntimeError(L.kpref_last_error().decode())
+    return out
+
+
+def image_grmhd_control(params, model, prims, derived, freqs, control, *, threads=0, out=None, kind="reference"):
+    """A GRMHD image in FMKS whose pass-B step control runs over the separate
+    frequency list `control` (the reference's control variant)."""
+    L = lib(kind)
+    L.kpref_image_grmhd_control_range.argtypes = [
+        C.POINTER(_abi.PassAParams), C.POINTER(_abi.GrmhdModel), C.POINTER(C.c_double), C.POINTER(C.c_double),
+        C.c_int, C.POINTER(C.c_double), C.c_int, C.POINTER(C.c_double), C.c_int, C.c_int, C.c_int, C.c_int,
+        C.POINTER(_abi.ImageOut)]
+    npix = params.camera.nx * params.camera.ny
+    nfreq = len(freqs)
+    if out is None:
+        out = _abi.ImageHostData.allocate(npix, nfreq)
+    p = np.ascontiguousarray(prims, dtype=np.float64)
+    d = None if derived is None else np.ascontiguousarray(derived, dtype=np.float64)
+    fa = (C.c_double * nfreq)(*freqs)
+    ca = (C.c_double * len(control))(*control)
+    s = out.as_struct()
+    rc = L.kpref_image_grmhd_control_range(C.byref(params), C.byref(model), _dp(p), None if d is None else _dp(d), 1,
+                                           fa, nfreq, ca, len(control), int(threads), 0, npix, C.byref(s))
+    if rc != 0:
         raise RuntimeError(L.kpref_last_error().decode())
     return out
 

@@ -123,12 +123,16 @@ void store_common(kp_image_out* out, int pixel, const Overlap& ov, Real closure_
     out->reason[pixel] = reason;
 }
 
+// With a step-control list (nctl > 0) every pixel runs the reference's
+// control variant (trace_pass_b_segment_model_multifrequency_control_pixel_metric,
+// pass_b.hpp:1505-1895), as run_multifrequency_image_metric_with_step_control
+// does for a separate list (multifrequency.hpp:174-228).
 template<class Metric, class Model>
 void run_metric(const kpolaris::PassAParams<Real>& pa,
                 const Model& model,
                 int radiation_substeps, const double* freqs, int nfreq,
                 const Metric& metric, int pixel_begin, int pixel_end, kp_image_out* out,
-                const int* pixel_list = nullptr) {
+                const int* pixel_list = nullptr, const double* ctl = nullptr, int nctl = 0) {
     const int npix = pa.camera.nx * pa.camera.ny;
 #pragma omp parallel for schedule(dynamic)
     for (int slot = pixel_begin; slot < pixel_end; ++slot) {
@@ -136,7 +140,25 @@ void run_metric(const kpolaris::PassAParams<Real>& pa,
 #ifdef KPREF_PERTURB_LIBM
         kpref_ulp::seed_pixel(pixel);
 #endif
-        if (nfreq == 1) {
+        if (nctl > 0) {
+            Real local_freqs[KPOLARIS_MAX_FREQUENCIES];
+            kpolaris::Stokes<Real> local_stokes[KPOLARIS_MAX_FREQUENCIES];
+            for (int f = 0; f < nfreq; ++f) local_freqs[f] = freqs[f];
+            std::vector<Real> local_ctl(ctl, ctl + nctl);
+            const kpolaris::MultiFrequencyPassBResult<Real> r =
+                kpolaris::trace_pass_b_segment_model_multifrequency_control_pixel_metric(
+                    pixel, pa, model, radiation_substeps, local_freqs, nfreq, local_ctl.data(), nctl, local_stokes,
+                    metric);
+            for (int f = 0; f < nfreq; ++f) {
+                const size_t idx = static_cast<size_t>(f) * static_cast<size_t>(npix) + pixel;
+                out->image_i[idx] = local_stokes[f].I;
+                out->image_q[idx] = local_stokes[f].Q;
+                out->image_u[idx] = local_stokes[f].U;
+                out->image_v[idx] = local_stokes[f].V;
+            }
+            store_common(out, pixel, r.overlap, r.closure_x, r.closure_k, r.final_null,
+                         r.frame_error, r.pass_a.steps, r.steps, static_cast<int>(r.reason));
+        } else if (nfreq == 1) {
             auto m = model;
             if (freqs) m.freq_cgs = freqs[0];
             const kpolaris::PassBResult<Real> r =
@@ -569,6 +591,34 @@ int kpref_image_riaf_range(const kp_pass_a_params* params, const kp_riaf_model* 
     return KP_OK;
 }
 
+// Pixels [pixel_begin, pixel_end) of a RIAF image whose pass-B step control
+// runs over a separate step-control frequency list.
+int kpref_image_riaf_control_range(const kp_pass_a_params* params, const kp_riaf_model* model,
+                                   int radiation_substeps, const double* freqs, int nfreq, const double* ctl,
+                                   int nctl, int threads, int pixel_begin, int pixel_end, kp_image_out* out) {
+    if (!params || !model || !out || !freqs || !ctl) return fail("null argument");
+    if (nfreq < 1 || nfreq > KPOLARIS_MAX_FREQUENCIES) return fail("nfreq out of range");
+    if (nctl < 1) return fail("empty step-control list");
+    const int npix = params->camera.nx * params->camera.ny;
+    if (pixel_begin < 0 || pixel_end > npix || pixel_begin > pixel_end)
+        return fail("pixel range out of bounds");
+    if (threads > 0) omp_set_num_threads(threads);
+    const auto pa = to_pass_a(*params);
+    const auto riaf = to_riaf(*model);
+    if (pa.coordinate_system == kpolaris::CoordinateSystem::CartesianKS) {
+        const kpolaris::KerrSchildInMetric<Real> metric(pa.mass, pa.spin);
+        run_metric(pa, riaf, radiation_substeps, freqs, nfreq, metric, pixel_begin, pixel_end, out, nullptr, ctl,
+                   nctl);
+    } else if (pa.coordinate_system == kpolaris::CoordinateSystem::BoyerLindquist) {
+        const kpolaris::KerrBoyerLindquistMetric<Real> metric(pa.mass, pa.spin);
+        run_metric(pa, riaf, radiation_substeps, freqs, nfreq, metric, pixel_begin, pixel_end, out, nullptr, ctl,
+                   nctl);
+    } else {
+        return fail("coordinate system not built in the reference oracle");
+    }
+    return KP_OK;
+}
+
 // The pixels pixel_list[0, n) of a RIAF image in one OpenMP dynamic loop
 // (the benchmark's bounded sample of spread-out rows, without a barrier per
 // row); outputs at their image positions.
@@ -923,6 +973,25 @@ int kpref_image_grmhd_range(const kp_pass_a_params* params, const kp_grmhd_model
     auto grmhd = to_grmhd(*model, prims, derived);
     if (nfreq == 1 && freqs) grmhd.freq_cgs = freqs[0];
     run_metric(pa, grmhd, radiation_substeps, freqs, nfreq, fmks_metric(pa), pixel_begin, pixel_end, out);
+    return KP_OK;
+}
+
+// kpref_image_grmhd_range with a separate step-control frequency list.
+int kpref_image_grmhd_control_range(const kp_pass_a_params* params, const kp_grmhd_model* model, const double* prims,
+                                    const double* derived, int radiation_substeps, const double* freqs, int nfreq,
+                                    const double* ctl, int nctl, int threads, int pixel_begin, int pixel_end,
+                                    kp_image_out* out) {
+    if (!params || !model || !prims || !out || !freqs || !ctl) return fail("null argument");
+    if (nfreq < 1 || nfreq > KPOLARIS_MAX_FREQUENCIES) return fail("nfreq out of range");
+    if (nctl < 1) return fail("empty step-control list");
+    const int npix = params->camera.nx * params->camera.ny;
+    if (pixel_begin < 0 || pixel_end > npix || pixel_begin > pixel_end) return fail("pixel range out of bounds");
+    if (threads > 0) omp_set_num_threads(threads);
+    const auto pa = to_pass_a(*params);
+    if (pa.coordinate_system != kpolaris::CoordinateSystem::FMKS) return fail("GRMHD oracle is built for FMKS only");
+    auto grmhd = to_grmhd(*model, prims, derived);
+    run_metric(pa, grmhd, radiation_substeps, freqs, nfreq, fmks_metric(pa), pixel_begin, pixel_end, out, nullptr,
+               ctl, nctl);
     return KP_OK;
 }
 

@@ -22,6 +22,7 @@ libm conditioning measured on the reference's own templates
     python tests/golden/make_golden.py --sampling  # slow-light sampling fixture only
     python tests/golden/make_golden.py --bl        # Boyer-Lindquist RIAF fixtures only
     python tests/golden/make_golden.py --recommended  # riaf_recommended.par replay fixture only
+    python tests/golden/make_golden.py --control   # step-control (long frequency list) fixtures only
 
 Each Boyer-Lindquist fixture (riaf_bl_*.npz, BL_CASES) stores the case, every
 output array of the reference's image over KerrBoyerLindquistMetric, and the
@@ -33,6 +34,13 @@ dropped: the GPU box has no copy of the reference tree), the reference's
 image at a 32 x 32 lattice of its 256 x 256 pixels (golden_cases.
 recommended_pixels(8); arrays hold those pixels only) and that sample's
 +-2-ulp libm conditioning on the reference's own templates.
+
+Each step-control fixture (CONTROL_CASES: RIAF in Kerr-Schild and in
+Boyer-Lindquist, the GRMHD torus) stores the case and, for every chunk k of
+four frequencies of its list, the reference's image of that chunk with the
+pass-B step control over the whole list (the control variant,
+pass_b.hpp:1505-1895) as c<k>_<field>, with the chunk's +-2-ulp libm
+conditioning on the reference's templates (c<k>_cond_keys / c<k>_cond_vals).
 
 The slow-light sampling fixture (slow_sampling.npz) stores 16 distinct,
 unevenly spaced snapshot times, two observation times, seeded sample
@@ -71,7 +79,8 @@ sys.path.insert(0, str(ROOT / "tests"))
 import oracle  # noqa: E402
 from golden_cases import (BL_CASES, IMAGE_CASES, GRMHD_CASES, RECOMMENDED_PAR, SLOW_CASES,  # noqa: E402
                           bl_conditioning_of, build_bl_case, build_case, build_grmhd_case, conditioning_over,
-                          recommended_case, recommended_pixels,
+                          recommended_case, recommended_pixels, CONTROL_CASES, build_control_case,
+                          control_chunks,
                           build_slow_case, coefficient_points, grmhd_conditioning_of, prims_digest,
                           slow_conditioning_of, transfer_points)
 
@@ -221,6 +230,36 @@ def make_recommended():
           {cond_key(k): "%.1e" % cond[k] for k in keys if k[0] in ("flux", "image_i") or k in ("pass_a_steps", "steps")})
 
 
+def make_control():
+    for name, spec in CONTROL_CASES.items():
+        case = build_control_case(spec)
+        kind, params, model, freqs = case[:4]
+        derived = oracle.grmhd_derived(model, case[4]) if kind == "grmhd" else None
+        arrays = {"spec": json.dumps(spec)}
+        for k, chunk in enumerate(control_chunks(freqs)):
+            def run(lib_kind, chunk=chunk):
+                if kind == "grmhd":
+                    return oracle.image_grmhd_control(params, model, case[4], derived, chunk, freqs, threads=0,
+                                                      kind=lib_kind)
+                return oracle.image_riaf_control(params, model, chunk, freqs, kind=lib_kind, threads=0)
+
+            ref = run("reference")
+
+            def perturbed(seed, run=run):
+                oracle.set_libm_perturbation(seed, "reference_ulp")
+                return run("reference_ulp")
+
+            cond = conditioning_over(perturbed, ref.arrays, tuple(range(1, 9)))
+            keys = sorted(cond, key=cond_key)
+            arrays[f"c{k}_cond_keys"] = np.array([cond_key(x) for x in keys])
+            arrays[f"c{k}_cond_vals"] = np.array([cond[x] for x in keys])
+            for field, v in ref.arrays.items():
+                arrays[f"c{k}_{field}"] = v
+            print(name, "chunk", k, chunk, np.bincount(ref.reason, minlength=8)[:8],
+                  {cond_key(x): "%.1e" % cond[x] for x in keys if x[0] == "flux" or x in ("pass_a_steps", "steps")})
+        np.savez_compressed(OUT / f"{name}.npz", **arrays)
+
+
 def make_sampling():
     rng = np.random.default_rng(7001)
     times = np.cumsum(np.concatenate([[40.0], rng.uniform(4.0, 16.0, size=15)]))
@@ -249,6 +288,9 @@ def main():
         return
     if "--recommended" in sys.argv[1:]:
         make_recommended()
+        return
+    if "--control" in sys.argv[1:]:
+        make_control()
         return
     if "--steps" in sys.argv[1:]:
         make_steps()
@@ -284,6 +326,7 @@ def main():
     make_sampling()
     make_bl()
     make_recommended()
+    make_control()
 
 
 if __name__ == "__main__":

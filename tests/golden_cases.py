@@ -331,3 +331,38 @@ def recommended_pixels(step: int = 16):
     ix, iy = step/2 + step k."""
     c = np.arange(step // 2, 256, step)
     return (c[:, None] * 256 + c[None, :]).ravel().astype(np.int32)
+
+
+# Frequency lists longer than KP_MAX_FREQUENCIES, imaged in chunks of four as
+# the image tool does (tools/kpolaris_model_image.cpp:3432-3446): every
+# chunk's pass-B step control runs over the whole list, so all chunks follow
+# one geodesic per pixel.
+CONTROL_CASES = {
+    # config-2 controls (adaptive tol 1e-8, depth 1/1/4) at 8^2, 8 frequencies
+    "riaf_ctl8_cks_8": {"kind": "config2", "n": 8,
+                        "freqs": [86.0e9, 150.0e9, 230.0e9, 345.0e9, 450.0e9, 690.0e9, 1.0e12, 1.5e12]},
+    # Boyer-Lindquist, i = 60 deg, six frequencies (chunks of 4 and 2)
+    "riaf_ctl6_bl_9": {"kind": "custom", "nx": 9, "ny": 9, "spin": 0.9375, "inclination_deg": 60.0,
+                       "radius": 1000.0, "xspan": 40.0, "step": 0.025, "adaptive": 1, "max_steps": 100000,
+                       "tolerance": 1e-8, "min_step": 1e-10, "max_step": 2.0, "max_radiation_step": 2.0,
+                       "depths": [1.0, 1.0, 4.0], "coordinate": "bl",
+                       "freqs": [43.0e9, 86.0e9, 230.0e9, 345.0e9, 690.0e9, 1.0e12]},
+    # the GRMHD torus, five frequencies (chunks of 4 and 1)
+    "grmhd_ctl5_12": {"model": "grmhd", "grid": [48, 32, 16], "n": 12, "adaptive": 1, "step": 0.025,
+                      "max_steps": 400000, "freqs": [86.0e9, 230.0e9, 345.0e9, 690.0e9, 1.0e12]},
+}
+
+
+def control_chunks(freqs, size: int = 4):
+    return [list(freqs[i:i + size]) for i in range(0, len(freqs), size)]
+
+
+def build_control_case(spec: dict):
+    """('riaf', params, model, freqs) or ('grmhd', params, model, freqs, prims)."""
+    if spec.get("model") == "grmhd":
+        prims, model, params, _ = build_grmhd_case(dict(spec, freqs=spec["freqs"][:1]))
+        return "grmhd", params, model, list(spec["freqs"]), prims
+    params, model, _ = build_case(spec)
+    if spec.get("coordinate") == "bl":
+        params.coordinate_system = _abi.COORD_BOYER_LINDQUIST
+    return "riaf", params, model, list(spec["freqs"])

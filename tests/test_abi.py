@@ -102,3 +102,21 @@ def test_output_shape_mismatch_is_rejected():
     params, model, freqs = configs.config1(4, 4)
     with pytest.raises(kp.KPolarisInvalidArgument):
         kp.image_riaf(params, model, freqs, out=_abi.ImageHostData.allocate(15, 1))
+
+
+@pytest.mark.parametrize("control,msg", [
+    ([], "step-control frequency list must not be empty"),
+    ([230e9] * 65, "longer than KP_MAX_CONTROL_FREQUENCIES"),
+    ([230e9, float("nan")], "step-control frequency 1 must be finite and positive"),
+    ([230e9, -1.0], "step-control frequency 1 must be finite and positive"),
+])
+def test_step_control_lists_are_validated_before_launch(control, msg):
+    params, model, freqs = configs.config2(4, 4)
+    with pytest.raises(kp.KPolarisInvalidArgument, match=msg):
+        kp.image_riaf(params, model, freqs, control_frequencies=control)
+    lib = kp.library()
+    ca = (C.c_double * max(len(control), 1))(*control)
+    fa = (C.c_double * 4)(*freqs)
+    out = _abi.ImageHostData.allocate(16, 4).as_struct()
+    st = lib.kp_image_grmhd_step_control(C.byref(params), None, 1, fa, 4, ca, len(control), None, C.byref(out))
+    assert st == _abi.KP_ERR_INVALID
