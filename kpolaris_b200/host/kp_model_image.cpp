@@ -124,8 +124,12 @@ int run(const std::vector<std::string>& args) {
         HostImage img(npix, nf);
         kp_image_out out = img.view(npix, nf);
         const kp_riaf_model model = kpb::to_riaf_model(opt, freqs[c0]);
-        check(kp_image_riaf(&pass_a, &model, opt.radiation_substeps, freqs.data() + c0, nf, &ro, &out),
-              "kp_image_riaf");
+        // every chunk's step control runs over the whole frequency grid
+        // (tools/kpolaris_model_image.cpp:3432-3446), so all chunks follow
+        // one geodesic per pixel; a single chunk is the plain image
+        check(kp_image_riaf_step_control(&pass_a, &model, opt.radiation_substeps, freqs.data() + c0, nf,
+                                         freqs.data(), int(freqs.size()), &ro, &out),
+              "kp_image_riaf_step_control");
         for (int f = 0; f < nf; ++f) {
             PackedFrequency& pf = packed[c0 + size_t(f)];
             pf.frequency = freqs[c0 + size_t(f)];
