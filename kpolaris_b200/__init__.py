@@ -526,20 +526,18 @@ def run_riaf_multifrequency_image(pass_a: PassAParams, model: RIAFModel, radiati
     """Mirror of run_riaf_multifrequency_image (src/image/riaf.hpp:32-39):
     1..KP_MAX_FREQUENCIES channels on one shared geodesic.  A step-control
     list different from the frequency list selects the reference's separate
-    control variant (pass_b.hpp:1505-1895), which is not built here."""
+    control variant (pass_b.hpp:1505-1895): kp_image_riaf_step_control."""
     del split_transport
     freqs = [float(f) for f in frequencies]
     if not (1 <= len(freqs) <= _abi.KP_MAX_FREQUENCIES):
         raise KPolarisInvalidArgument(_abi.KP_ERR_INVALID,
                                       "multifrequency image chunk size must be between 1 and "
                                       "KP_MAX_FREQUENCIES")
+    ctl = None
     if step_control_frequencies is not None:
         ctl = [float(f) for f in step_control_frequencies]
         if not ctl:
             raise KPolarisInvalidArgument(_abi.KP_ERR_INVALID,
                                           "multifrequency step-control frequency list must not be empty")
-        if ctl != freqs:
-            raise KPolarisError(_abi.KP_ERR_UNSUPPORTED,
-                                "separate step-control frequency sets are not built")
     return image_riaf(pass_a, model, freqs, radiation_substeps=radiation_substeps, timing=timing,
-                      **options)
+                      control_frequencies=ctl, **options)

@@ -299,8 +299,6 @@ HostData run_riaf_multifrequency_image(const PassA& pass_a, Model model, int rad
     (void)split_transport;
     if (step_control_frequencies.empty())
         throw std::invalid_argument("multifrequency step-control frequency list must not be empty");
-    if (step_control_frequencies != frequencies)
-        throw std::runtime_error("separate step-control frequency sets are not built");
     const kp_pass_a_params p = to_c(pass_a);
     const kp_riaf_model m = to_c_riaf(model);
     HostData out;
@@ -310,7 +308,10 @@ HostData run_riaf_multifrequency_image(const PassA& pass_a, Model model, int rad
     kp_image_out o = bind_outputs(out, p.camera.nx * p.camera.ny, nfreq);
     kp_run_options opt = shim_options();
     opt.timing = timing;
-    throw_on_error(kp_image_riaf(&p, &m, radiation_substeps, frequencies.data(), nfreq, &opt, &o));
+    // a list equal to `frequencies` is the plain image inside the library
+    throw_on_error(kp_image_riaf_step_control(&p, &m, radiation_substeps, frequencies.data(), nfreq,
+                                              step_control_frequencies.data(),
+                                              int(step_control_frequencies.size()), &opt, &o));
     return out;
 }
 
@@ -411,8 +412,6 @@ HostData run_grmhd_multifrequency_image(const PassA& pass_a, Model model, int ra
                                         const std::vector<Real>& step_control_frequencies, int timing) {
     if (step_control_frequencies.empty())
         throw std::invalid_argument("multifrequency step-control frequency list must not be empty");
-    if (step_control_frequencies != frequencies)
-        throw std::runtime_error("separate step-control frequency sets are not built");
     const int nfreq = int(frequencies.size());
     if (nfreq < 1 || nfreq > KP_MAX_FREQUENCIES)
         throw std::invalid_argument("multifrequency image chunk size must be between 1 and KPOLARIS_MAX_FREQUENCIES");
@@ -423,7 +422,9 @@ HostData run_grmhd_multifrequency_image(const PassA& pass_a, Model model, int ra
     kp_run_options opt = shim_options();
     opt.timing = timing;
     std::vector<double> f(frequencies.begin(), frequencies.end());
-    throw_on_error(kp_image_grmhd(&p, g, radiation_substeps, f.data(), nfreq, &opt, &o));
+    std::vector<double> ctl(step_control_frequencies.begin(), step_control_frequencies.end());
+    throw_on_error(kp_image_grmhd_step_control(&p, g, radiation_substeps, f.data(), nfreq, ctl.data(), int(ctl.size()),
+                                               &opt, &o));
     return out;
 }
 
