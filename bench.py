@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--serve-requests", type=int, default=48, help="requests of the serving trace (0: skip)")
     ap.add_argument("--serve-rate", type=float, default=20.0, help="Poisson arrival rate of the trace, 1/s")
     ap.add_argument("--serve-plain", type=int, default=1, help="replay the trace on the plain FP64 kernel too")
+    ap.add_argument("--serve-rates", default="5,20,50,100,200",
+                    help="arrival rates of the serving curve, 1/s (the trace's arrival times rescaled)")
     ap.add_argument("--ref-row-stride", type=int, default=8,
                     help="reference arm: every N-th image row is traced per step")
     ap.add_argument("--fp64-batched-steps", type=int, default=2,
@@ -635,12 +637,10 @@ def serve_mixed(trace, grids, device):
             "max_inflight_jobs": st.max_inflight_jobs, "ticks": st.ticks - base.ticks}
 
 
-def serve_plain(trace, grids, device):
-    """The same trace through a FIFO of plain FP64 launches: each request
-    starts when it has arrived and the previous one has finished (RIAF: the
-    one-image-per-launch kernel; GRMHD: one FP64 image per call)."""
-    import numpy as np
-
+def plain_service_times(trace, grids, device):
+    """Service time of every request of the trace on the plain FP64 path
+    (RIAF: the one-image-per-launch kernel; GRMHD: one FP64 image per call),
+    each measured alone after a warm-up request of each kind."""
     import kpolaris_b200 as kp
 
     def run(kind, p, m, f):
@@ -653,18 +653,38 @@ def serve_plain(trace, grids, device):
         first = next((e for e in trace if e[1] == kind), None)
         if first:
             run(*first[1:])
-    finish = 0.0
-    lat = []
-    busy = 0.0
-    for (t, kind, p, m, f) in trace:
+    svc = []
+    for (_, kind, p, m, f) in trace:
         t_a = time.perf_counter()
         run(kind, p, m, f)
-        svc = time.perf_counter() - t_a
-        busy += svc
-        finish = max(finish, t) + svc
+        svc.append(time.perf_counter() - t_a)
+    return svc
+
+
+def fifo_latency(arrivals, svc):
+    """A FIFO of plain launches: each request starts when it has arrived and
+    the previous one has finished; a request's service time does not depend
+    on when it starts, so one measured set of service times serves every
+    arrival rate."""
+    import numpy as np
+
+    finish = 0.0
+    lat = []
+    for t, s in zip(arrivals, svc):
+        finish = max(finish, t) + s
         lat.append(finish - t)
-    return {"images_per_s": len(trace) / finish, "p50_s": float(np.percentile(lat, 50)),
-            "p99_s": float(np.percentile(lat, 99)), "max_s": float(max(lat)), "busy_s": busy}
+    return {"images_per_s": len(arrivals) / finish, "p50_s": float(np.percentile(lat, 50)),
+            "p99_s": float(np.percentile(lat, 99)), "max_s": float(max(lat)), "busy_s": float(sum(svc))}
+
+
+def rescale_trace(trace, factor):
+    """The trace with every arrival time multiplied by `factor`."""
+    return [(e[0] * factor,) + tuple(e[1:]) for e in trace]
+
+
+def serve_plain(trace, grids, device):
+    """The same trace through a FIFO of plain FP64 launches."""
+    return fifo_latency([e[0] for e in trace], plain_service_times(trace, grids, device))
 
 
 def progress(msg):
@@ -918,9 +938,23 @@ def ours_arm(args):
                        "requests": len(trace), "grmhd_requests": sum(1 for e in trace if e[1] == "grmhd"),
                        "rate_per_s": args.serve_rate,
                        "mixed_batched": serve_mixed(trace, grids, local)}
+            svc = None
             if args.serve_plain:
                 progress("serving trace on the plain FP64 path")
-                serving["plain_fp64"] = serve_plain(trace, grids, local)
+                svc = plain_service_times(trace, grids, local)
+                serving["plain_fp64"] = fifo_latency([e[0] for e in trace], svc)
+            # the serving curve: the same requests, arrival times rescaled
+            curve = []
+            for rate in [float(x) for x in args.serve_rates.split(",") if x.strip()]:
+                progress(f"serving curve at {rate:g}/s")
+                scaled = rescale_trace(trace, args.serve_rate / rate)
+                row = {"rate_per_s": rate,
+                       "mixed_batched": (serving["mixed_batched"] if rate == args.serve_rate
+                                         else serve_mixed(scaled, grids, local))}
+                if svc is not None:
+                    row["plain_fp64"] = fifo_latency([e[0] for e in scaled], svc)
+                curve.append(row)
+            serving["curve"] = curve
         finally:
             for g in grids:
                 g.release()

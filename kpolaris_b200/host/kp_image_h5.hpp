@@ -104,6 +104,33 @@ inline void h5_riaf_metadata(kph5::Group& g, const kp_riaf_model& m) {
     g.attr("dlambda_scale", l_unit / std::max(m.freq_cgs, 1.0));  // riaf.hpp:76-85
 }
 
+// A GRMHD model's metadata (write_model_metadata for GRMHDRadiationModel,
+// tools/kpolaris_model_image.cpp:739-787): the shared grmhd_* keys and the
+// same under the model's own prefix.  FMKS data, thermal fits.
+inline void h5_grmhd_metadata(kph5::Group& g, const kp_grmhd_model& m, const std::string& prefix, double freq) {
+    const double l_unit = 6.67430e-8 * m.mbh_solar * 1.98847e33 / (2.99792458e10 * 2.99792458e10);
+    const double dls = l_unit / std::max(freq, 1.0);  // grmhd_grid.hpp:159-161
+    for (const std::string& pre : {std::string("grmhd"), prefix}) {
+        g.attr(pre + "_n1", m.n1);
+        g.attr(pre + "_n2", m.n2);
+        g.attr(pre + "_n3", m.n3);
+        g.attr(pre + "_M_unit", m.M_unit);
+        g.attr(pre + "_mbh_solar", m.mbh_solar);
+        g.attr(pre + "_trat_small", m.trat_small);
+        g.attr(pre + "_trat_large", m.trat_large);
+        g.attr(pre + "_beta_crit", m.beta_crit);
+        g.attr(pre + "_sigma_cut", m.sigma_cut);
+        g.attr(pre + "_sigma_cut_high", m.sigma_cut_high);
+        g.attr(pre + "_interpolate_derived_scalars", m.has_derived_scalars);
+        g.attr(pre + "_precomputed_fluid_state", 0);
+        g.attr(pre + "_data_coordinate_system", int(KP_COORD_FMKS));
+        g.attr(pre + "_radial_coordinate_log", 1);
+        g.attr(pre + "_dlambda_scale", dls);
+    }
+    g.attr("emission_type", m.emission_type);
+    g.attr("emission_fit", emission_fit_name(m.emission_type));
+}
+
 inline void h5_provenance(kph5::Group& g) {
     g.attr("schema", "kpolaris_image");
     g.attr("schema_version", 1);
@@ -128,9 +155,11 @@ inline void h5_provenance(kph5::Group& g) {
     g.attr("image_backend", "KPolaris-B200 (sm_100a C ABI)");
 }
 
+// `grmhd`: the model of a GRMHD image (model=iharm), or null for RIAF.
 inline void write_image_h5(const std::string& path, const ImageOptions& opt, const std::string& params_path,
                            const kp_pass_a_params& pass_a, const std::vector<double>& freqs,
-                           const std::vector<H5Frequency>& images, const H5Diagnostics& dg, const FluxScale& fs) {
+                           const std::vector<H5Frequency>& images, const H5Diagnostics& dg, const FluxScale& fs,
+                           const kp_grmhd_model* grmhd = nullptr) {
     const int nx = opt.nx, ny = opt.ny, npix = nx * ny;
     const double nan = std::numeric_limits<double>::quiet_NaN();
     const double jy = fs.valid ? fs.jy_per_pixel : nan;
@@ -147,7 +176,14 @@ inline void write_image_h5(const std::string& path, const ImageOptions& opt, con
     for (int i = 0; i < nx; ++i) gx[size_t(i)] = (double(i) + 0.5) * dx - xh + pass_a.camera.x_offset;
     for (int j = 0; j < ny; ++j) gy[size_t(j)] = (double(j) + 0.5) * dy - yh + pass_a.camera.y_offset;
     const kp_riaf_model first_model = to_riaf_model(opt, freqs.front());
-    const double mbh = opt.riaf_mbh_solar;
+    const double mbh = model_mbh_solar(opt);
+    auto model_metadata = [&](kph5::Group& g, double freq) {
+        if (grmhd) {
+            h5_grmhd_metadata(g, *grmhd, opt.model, freq);
+        } else {
+            h5_riaf_metadata(g, freq == freqs.front() ? first_model : to_riaf_model(opt, freq));
+        }
+    };
     const int chunk = effective_chunk_size(opt, freqs.size());
     const std::string flist = h5_frequency_list(freqs);
     const std::string metric = metric_name_of(opt.coordinate);
@@ -243,7 +279,7 @@ inline void write_image_h5(const std::string& path, const ImageOptions& opt, con
     root.attr("max_steps", opt.max_steps);
     root.attr("inner_radius", opt.inner_radius);
     root.attr("outer_radius", opt.outer_radius);
-    h5_riaf_metadata(root, first_model);
+    model_metadata(root, freqs.front());
 
     kph5::Group& header = root.group("header");
     h5_provenance(header);
@@ -347,7 +383,7 @@ inline void write_image_h5(const std::string& path, const ImageOptions& opt, con
         g.attr("freq_spacing", opt.freq_spacing);
         g.attr("stokes_convention", "camera_frame");
         g.dataset("frequencies", {uint64_t(freqs.size())}, freqs.data());
-        h5_riaf_metadata(g, first_model);
+        model_metadata(g, freqs.front());
     }
     {
         kph5::Group& g = root.group("grid");
@@ -454,8 +490,7 @@ inline void write_image_h5(const std::string& path, const ImageOptions& opt, con
             g.attr("stokes_units", "cgs_specific_intensity");
             g.attr("intensity_to_flux_jy_per_pixel", jy);
             for (int k = 0; k < 4; ++k) g.attr(std::string("flux_") + nm[k] + "_Jy", im.flux_jy[k]);
-            kp_riaf_model fm = to_riaf_model(opt, im.frequency);
-            h5_riaf_metadata(g, fm);
+            model_metadata(g, im.frequency);
             for (int k = 0; k < 4; ++k) g.dataset(nm[k], dims, im.nu[k]);
             for (int k = 0; k < 4; ++k) g.dataset(std::string(nm[k]) + "_inv", dims, im.inv[k]);
         }

@@ -1,7 +1,9 @@
-// kp_model_image -- command-line image tool for the RIAF image path, the
-// counterpart of the reference's kpolaris_model_image for model=riaf
-// (tools/kpolaris_model_image.cpp:4908-4960 main, :3909-4260 run_model,
-// :2561-2800 output packing, :4136-4245 CSV output).
+// kp_model_image -- command-line image tool for the RIAF image path and
+// iharm GRMHD dumps, the counterpart of the reference's kpolaris_model_image
+// for model=riaf and model=iharm (tools/kpolaris_model_image.cpp:4908-5126
+// main, :3909-4260 run_model, :2561-2800 output packing, :4136-4245 CSV
+// output).  An iharm dump is read by kp_iharm_read / kp_grid_load_iharm
+// and imaged with kp_image_grmhd_step_control.
 //
 //   kp_model_image --parameter_file=run.par [--key=value ...]
 //
@@ -84,12 +86,23 @@ int run(const std::vector<std::string>& args) {
     const auto t_start = std::chrono::steady_clock::now();
     kpb::ImageOptions opt = kpb::parse_options(args);
     kpb::finalize_options(opt);
+    // model=iharm: the dump's header settles the spin, the radii and the
+    // coordinate map (read on the host; no device yet)
+    const bool grmhd = opt.model == "iharm";
+    kp_grmhd_model gm{};
+    kp_iharm_options io{};
+    if (grmhd) {
+        io = kpb::to_iharm_options(opt);
+        check(kp_iharm_read(opt.iharm_dump.c_str(), &io, &gm, nullptr, 0), "kp_iharm_read");
+        kpb::resolve_grmhd_geometry(opt, gm);
+    }
     if (opt.kp_print_resolved) {
         kpb::print_resolved(std::cout, opt);
         return 0;
     }
     const std::vector<double> freqs = kpb::build_frequency_grid(opt);
-    const kp_pass_a_params pass_a = kpb::to_pass_a(opt);
+    kp_pass_a_params pass_a = kpb::to_pass_a(opt);
+    if (grmhd) kpb::apply_fmks_map(pass_a, gm);
     const bool hdf5 = opt.output_format == "hdf5" ||
                       (opt.output_format == "auto" && opt.output.size() >= 3 &&
                        opt.output.compare(opt.output.size() - 3, 3, ".h5") == 0);
@@ -118,18 +131,36 @@ int run(const std::vector<std::string>& args) {
     const double jy = fs.valid ? fs.jy_per_pixel : -1.0;
     std::vector<PackedFrequency> packed(freqs.size());
     HostImage first_chunk(npix, 1);
+    kp_grid* grid = nullptr;
+    if (grmhd) {
+        const auto t_load = std::chrono::steady_clock::now();
+        check(kp_grid_load_iharm(opt.iharm_dump.c_str(), &io, opt.kp_device, &gm, &grid), "kp_grid_load_iharm");
+        report_timing(opt, "iharm_load_total", seconds_since(t_load));
+    }
+    struct GridGuard {
+        kp_grid* g;
+        ~GridGuard() {
+            if (g) kp_grid_release(g);
+        }
+    } guard{grid};
     const auto t_transport = std::chrono::steady_clock::now();
     for (size_t c0 = 0; c0 < freqs.size(); c0 += size_t(chunk)) {
         const int nf = int(std::min(freqs.size() - c0, size_t(chunk)));
         HostImage img(npix, nf);
         kp_image_out out = img.view(npix, nf);
-        const kp_riaf_model model = kpb::to_riaf_model(opt, freqs[c0]);
         // every chunk's step control runs over the whole frequency grid
         // (tools/kpolaris_model_image.cpp:3432-3446), so all chunks follow
         // one geodesic per pixel; a single chunk is the plain image
-        check(kp_image_riaf_step_control(&pass_a, &model, opt.radiation_substeps, freqs.data() + c0, nf,
-                                         freqs.data(), int(freqs.size()), &ro, &out),
-              "kp_image_riaf_step_control");
+        if (grmhd) {
+            check(kp_image_grmhd_step_control(&pass_a, grid, opt.radiation_substeps, freqs.data() + c0, nf,
+                                              freqs.data(), int(freqs.size()), &ro, &out),
+                  "kp_image_grmhd_step_control");
+        } else {
+            const kp_riaf_model model = kpb::to_riaf_model(opt, freqs[c0]);
+            check(kp_image_riaf_step_control(&pass_a, &model, opt.radiation_substeps, freqs.data() + c0, nf,
+                                             freqs.data(), int(freqs.size()), &ro, &out),
+                  "kp_image_riaf_step_control");
+        }
         for (int f = 0; f < nf; ++f) {
             PackedFrequency& pf = packed[c0 + size_t(f)];
             pf.frequency = freqs[c0 + size_t(f)];
@@ -180,7 +211,7 @@ int run(const std::vector<std::string>& args) {
         dg.steps = first_chunk.steps.data();
         dg.total_steps = packed.front().total_steps.data();
         for (int k = 0; k < 11; ++k) dg.diag[k] = first_chunk.diag[k].data();
-        kpb::write_image_h5(opt.output, opt, params_path, pass_a, freqs, h5f, dg, fs);
+        kpb::write_image_h5(opt.output, opt, params_path, pass_a, freqs, h5f, dg, fs, grmhd ? &gm : nullptr);
     } else {
         std::ofstream out(opt.output);
         if (!out) throw std::runtime_error("failed to open output: " + opt.output);
@@ -192,16 +223,34 @@ int run(const std::vector<std::string>& args) {
         out << "# coordinate," << opt.coordinate << "\n# metric," << kpb::metric_name_of(opt.coordinate) << "\n";
         out << "# stokes_convention,camera_frame\n# polarization_basis,camera_screen\n";
         out << "# inner_radius," << opt.inner_radius << "\n# outer_radius," << opt.outer_radius << "\n";
+        if (grmhd) {
+            // write_model_metadata for GRMHDRadiationModel (:739-787)
+            const double l_unit = 6.67430e-8 * gm.mbh_solar * 1.98847e33 / (2.99792458e10 * 2.99792458e10);
+            for (const std::string& pre : {std::string("grmhd"), opt.model}) {
+                out << "# " << pre << "_n1," << gm.n1 << "\n# " << pre << "_n2," << gm.n2 << "\n# " << pre << "_n3,"
+                    << gm.n3 << "\n# " << pre << "_M_unit," << gm.M_unit << "\n# " << pre << "_mbh_solar,"
+                    << gm.mbh_solar << "\n# " << pre << "_trat_small," << gm.trat_small << "\n# " << pre
+                    << "_trat_large," << gm.trat_large << "\n# " << pre << "_beta_crit," << gm.beta_crit << "\n# "
+                    << pre << "_sigma_cut," << gm.sigma_cut << "\n# " << pre << "_sigma_cut_high," << gm.sigma_cut_high
+                    << "\n";
+            }
+            out << "# emission_type," << gm.emission_type << "\n# emission_fit,"
+                << kpb::emission_fit_name(gm.emission_type) << "\n";
+            out << "# grmhd_interpolate_derived_scalars," << gm.has_derived_scalars << "\n# grmhd_dlambda_scale,"
+                << l_unit / std::max(freqs.front(), 1.0) << "\n";
+        }
         const kp_riaf_model m = kpb::to_riaf_model(opt, freqs.front());
-        out << "# riaf_r_min," << m.r_min << "\n# riaf_r_max," << m.r_max << "\n# riaf_nth0," << m.nth0
+        if (!grmhd) out << "# riaf_r_min," << m.r_min << "\n# riaf_r_max," << m.r_max << "\n# riaf_nth0," << m.nth0
             << "\n# riaf_Te0," << m.Te0 << "\n# riaf_disk_h," << m.disk_h << "\n# riaf_pow_nth," << m.pow_nth
             << "\n# riaf_pow_T," << m.pow_T << "\n# riaf_ne_unit," << m.ne_unit << "\n# riaf_te_unit," << m.te_unit
             << "\n# riaf_mbh_solar," << m.mbh_solar << "\n# riaf_keplerian_factor," << m.keplerian_factor
             << "\n# riaf_infall_factor," << m.infall_factor << "\n# emission_type," << m.emission_type
             << "\n# emission_fit," << kpb::emission_fit_name(m.emission_type) << "\n";
-        // riaf.hpp:76-85: length unit over the frequency
-        const double l_unit = 6.67430e-8 * m.mbh_solar * 1.98847e33 / (2.99792458e10 * 2.99792458e10);
-        out << "# dlambda_scale," << l_unit / std::max(m.freq_cgs, 1.0) << "\n";
+        if (!grmhd) {
+            // riaf.hpp:76-85: length unit over the frequency
+            const double l_unit = 6.67430e-8 * m.mbh_solar * 1.98847e33 / (2.99792458e10 * 2.99792458e10);
+            out << "# dlambda_scale," << l_unit / std::max(m.freq_cgs, 1.0) << "\n";
+        }
         if (multi) out << "freq_index,frequency_hz,";
         out << "ix,iy,I_inv,Q_inv,U_inv,V_inv,I_nu,Q_nu,U_nu,V_nu,reason,pass_a_steps,pass_b_steps,total_steps,"
                "closure_x,closure_k,final_null,frame_error,det_r,overlap_r11,overlap_r12,overlap_r21,overlap_r22,"
@@ -262,7 +311,8 @@ int main(int argc, char** argv) {
         const std::string a(argv[i]);
         if (a == "--help" || a == "-h") {
             std::cout << "usage: kp_model_image --parameter_file=FILE.par [--key=value ...]\n"
-                         "RIAF images through the KPolaris-B200 C ABI; CSV output and <output>.params.\n";
+                         "RIAF images and iharm GRMHD dumps through the KPolaris-B200 C ABI; HDF5 or CSV "
+                         "output and <output>.params.\n";
             return 0;
         }
         args.push_back(a);

@@ -117,6 +117,17 @@ struct ImageOptions {
     double riaf_keplerian_factor = 1.0;
     double riaf_infall_factor = 0.0;
     int emission_type = 0;
+    // model=iharm: the dump and the IHARMLoadOptions the tool passes
+    // (tools/kpolaris_model_image_options.hpp:190-201 defaults)
+    std::string iharm_dump;
+    double iharm_M_unit = 3.0e25;
+    double iharm_mbh_solar = 6.2e9;
+    double iharm_trat_small = 1.0;
+    double iharm_trat_large = 20.0;
+    double iharm_beta_crit = 1.0;
+    double iharm_sigma_cut = 1.0;
+    double iharm_sigma_cut_high = -1.0;
+    int iharm_interpolate_derived_scalars = 1;
     int timing = 0;
     int repeat_images = 1;
     // requests for subsystems that are not built (checked by validate_options)
@@ -355,6 +366,18 @@ inline const KeyTable& key_table() {
         t.add({"riaf_mbh_solar"}, real_field(&O::riaf_mbh_solar));
         t.add({"riaf_keplerian_factor"}, real_field(&O::riaf_keplerian_factor));
         t.add({"riaf_infall_factor"}, real_field(&O::riaf_infall_factor));
+        // iharm dump options (kpolaris_model_image_options.cpp:827-966); the
+        // unprefixed forms set every GRMHD loader's value, here the iharm one
+        t.add({"iharm_dump", "dump"}, text_field(&O::iharm_dump));
+        t.add({"iharm_M_unit", "iharm_m_unit", "M_unit"}, real_field(&O::iharm_M_unit));
+        t.add({"iharm_mbh_solar", "MBH"}, real_field(&O::iharm_mbh_solar));
+        t.add({"iharm_trat_small", "trat_small"}, real_field(&O::iharm_trat_small));
+        t.add({"iharm_trat_large", "trat_large"}, real_field(&O::iharm_trat_large));
+        t.add({"iharm_beta_crit", "beta_crit"}, real_field(&O::iharm_beta_crit));
+        t.add({"iharm_sigma_cut", "sigma_cut"}, real_field(&O::iharm_sigma_cut));
+        t.add({"iharm_sigma_cut_high", "sigma_cut_high"}, real_field(&O::iharm_sigma_cut_high));
+        t.add({"iharm_interpolate_derived_scalars", "interpolate_derived_scalars"},
+              int_field(&O::iharm_interpolate_derived_scalars));
         t.add({"emission_type"}, int_field(&O::emission_type));
         t.add({"emission_fit"}, [](O& o, const std::string& v) { o.emission_type = emission_type_from_name(v); });
         t.add({"timing", "profile"}, int_field(&O::timing));
@@ -480,6 +503,12 @@ inline ImageOptions parse_options(const std::vector<std::string>& args) {
     return opt;
 }
 
+// The black-hole mass of the model's length unit (camera_mbh_solar /
+// output_mbh_solar, kpolaris_model_image_options.cpp:126-134).
+inline double model_mbh_solar(const ImageOptions& o) {
+    return o.model == "iharm" ? o.iharm_mbh_solar : o.riaf_mbh_solar;
+}
+
 inline double length_unit_cm(double mbh_solar) {
     // the tool's constants (kpolaris_model_image_options.cpp:119-124)
     return 6.6742e-8 * mbh_solar * 1.989e33 / (2.99792458e10 * 2.99792458e10);
@@ -536,7 +565,7 @@ inline void resolve_camera_extents(ImageOptions& o) {
         if (o.dsource_pc <= 0.0) throw std::runtime_error("fovx_dsource/fovy_dsource require dsource in parsec");
         if (o.fovx_dsource <= 0.0) o.fovx_dsource = o.fovy_dsource;
         if (o.fovy_dsource <= 0.0) o.fovy_dsource = o.fovx_dsource;
-        const double m_per_muas = o.dsource_pc * pc_cm / length_unit_cm(o.riaf_mbh_solar) / muas_per_rad;
+        const double m_per_muas = o.dsource_pc * pc_cm / length_unit_cm(model_mbh_solar(o)) / muas_per_rad;
         o.image_width_x = o.fovx_dsource * m_per_muas;
         o.image_width_y = o.fovy_dsource * m_per_muas;
         o.effective_fovx_dsource = o.fovx_dsource;
@@ -561,7 +590,7 @@ inline void resolve_camera_extents(ImageOptions& o) {
         o.image_width_y = o.yspan > 0.0 ? 2.0 * o.yspan : o.fovy;
     }
     if (o.dsource_pc > 0.0 && o.image_width_x > 0.0 && o.image_width_y > 0.0) {
-        const double m_per_muas = o.dsource_pc * pc_cm / length_unit_cm(o.riaf_mbh_solar) / muas_per_rad;
+        const double m_per_muas = o.dsource_pc * pc_cm / length_unit_cm(model_mbh_solar(o)) / muas_per_rad;
         o.effective_fovx_dsource = o.image_width_x / m_per_muas;
         o.effective_fovy_dsource = o.image_width_y / m_per_muas;
     }
@@ -583,13 +612,63 @@ inline void finalize_options(ImageOptions& o) {
     validate_options(o);
     resolve_camera_extents(o);
     validate_resolved_camera(o);
+    if (o.model == "iharm") {
+        // the radii and the spin come from the dump (resolve_grmhd_geometry)
+        if (o.coordinate != "fmks")
+            throw std::runtime_error("iharm images are built for --coordinate=fmks (the dump's native grid)");
+        if (o.camera != "pinhole") throw std::runtime_error("iharm images are built for the pinhole camera");
+        return;
+    }
     const double horizon = 1.0 + std::sqrt(std::max(0.0, 1.0 - o.spin * o.spin));
     if (o.inner_radius <= 0.0) o.inner_radius = horizon * 1.05;
     if (o.model != "riaf")
         throw std::runtime_error("model '" + o.model +
-                                 "' is not built in this tool: the RIAF model only (GRMHD grids go through "
+                                 "' is not built in this tool: riaf and iharm only (other GRMHD grids go through "
                                  "kp_grid_upload / kp_image_grmhd)");
     if (o.outer_radius <= 0.0) o.outer_radius = o.riaf_r_max * 1.15;
+}
+
+// A GRMHD model's spin and radii once its dump header is read
+// (tools/kpolaris_model_image.cpp:5113-5125, safe_inner_radius :468-475):
+// the dump's spin; outer radius min(r_out, 0.9 camera radius) unless set;
+// inner radius the larger of the grid's r_in and 1.05 r_+, or an explicit
+// request no closer than 1.05 r_+.
+inline void resolve_grmhd_geometry(ImageOptions& o, const kp_grmhd_model& m) {
+    o.spin = m.spin;
+    if (o.outer_radius <= 0.0) o.outer_radius = std::min(m.r_out, o.radius * 0.9);
+    const double horizon = 1.0 + std::sqrt(std::max(0.0, 1.0 - m.spin * m.spin));
+    if (o.inner_radius_explicit && o.inner_radius > 0.0)
+        o.inner_radius = std::max(o.inner_radius, horizon * 1.05);
+    else
+        o.inner_radius = std::max(m.r_in, horizon * 1.05);
+}
+
+// The FMKS coordinate map of a GRMHD grid in the pass-A parameters.
+inline void apply_fmks_map(kp_pass_a_params& p, const kp_grmhd_model& m) {
+    p.fmks_startx1 = m.startx1;
+    p.fmks_hslope = m.hslope;
+    p.fmks_mks_smooth = m.mks_smooth;
+    p.fmks_poly_alpha = m.poly_alpha;
+    p.fmks_poly_xt = m.poly_xt;
+    p.fmks_poly_norm = m.poly_norm;
+}
+
+// IHARMLoadOptions of an iharm run (make_iharm_load_options,
+// tools/kpolaris_model_image.cpp:1734-1767); the fit defaults to Dexter.
+inline kp_iharm_options to_iharm_options(const ImageOptions& o) {
+    kp_iharm_options io;
+    kp_default_iharm_options(&io);
+    io.freq_cgs = o.freq;
+    io.M_unit = o.iharm_M_unit;
+    io.mbh_solar = o.iharm_mbh_solar;
+    io.trat_small = o.iharm_trat_small;
+    io.trat_large = o.iharm_trat_large;
+    io.beta_crit = o.iharm_beta_crit;
+    io.sigma_cut = o.iharm_sigma_cut;
+    io.sigma_cut_high = o.iharm_sigma_cut_high;
+    io.emission_type = o.emission_type > 0 ? o.emission_type : KP_FIT_DEXTER;
+    io.interpolate_derived_scalars = o.iharm_interpolate_derived_scalars;
+    return io;
 }
 
 inline std::vector<double> parse_frequency_list(const std::string& text) {
@@ -739,7 +818,7 @@ struct FluxScale {
 
 inline FluxScale flux_scale_of(const ImageOptions& o) {
     const double nan = std::numeric_limits<double>::quiet_NaN();
-    FluxScale s{length_unit_cm(o.riaf_mbh_solar), o.dsource_pc * 3.085678e18, nan, nan, false};
+    FluxScale s{length_unit_cm(model_mbh_solar(o)), o.dsource_pc * 3.085678e18, nan, nan, false};
     if (o.dsource_pc > 0.0 && o.image_width_x > 0.0 && o.image_width_y > 0.0 && o.nx > 0 && o.ny > 0) {
         const double px = o.image_width_x * s.l_unit_cm / double(o.nx);
         const double py = o.image_width_y * s.l_unit_cm / double(o.ny);
@@ -859,13 +938,23 @@ inline void write_effective_parameters(const std::string& path, const ImageOptio
     out << "# derived_nfreq=" << freqs.size() << "\n# effective_multifrequency_chunk_size="
         << effective_chunk_size(o, freqs.size()) << "\n# derived_freq_list=" << frequency_list_string(freqs) << "\n";
     out << "# compile_KP_MAX_FREQUENCIES=" << KP_MAX_FREQUENCIES << "\n";
-    out << "riaf_r_min=" << o.riaf_r_min << "\nriaf_r_max=" << o.riaf_r_max << "\nriaf_nth0=" << o.riaf_nth0
-        << "\nriaf_Te0=" << o.riaf_Te0 << "\nriaf_disk_h=" << o.riaf_disk_h << "\nriaf_pow_nth=" << o.riaf_pow_nth
-        << "\nriaf_pow_T=" << o.riaf_pow_T << "\nriaf_ne_unit=" << o.riaf_ne_unit << "\nriaf_te_unit="
-        << o.riaf_te_unit << "\nriaf_mbh_solar=" << o.riaf_mbh_solar << "\nriaf_keplerian_factor="
-        << o.riaf_keplerian_factor << "\nriaf_infall_factor=" << o.riaf_infall_factor << "\n";
-    out << "emission_type=" << effective_emission_type(o) << "\nemission_fit="
-        << emission_fit_name(effective_emission_type(o)) << "\n";
+    if (o.model == "iharm") {
+        out << "iharm_dump=" << o.iharm_dump << "\niharm_M_unit=" << o.iharm_M_unit
+            << "\niharm_mbh_solar=" << o.iharm_mbh_solar << "\niharm_trat_small=" << o.iharm_trat_small
+            << "\niharm_trat_large=" << o.iharm_trat_large << "\niharm_beta_crit=" << o.iharm_beta_crit
+            << "\niharm_sigma_cut=" << o.iharm_sigma_cut << "\niharm_sigma_cut_high=" << o.iharm_sigma_cut_high
+            << "\niharm_interpolate_derived_scalars=" << o.iharm_interpolate_derived_scalars << "\n";
+        const int fit = o.emission_type > 0 ? o.emission_type : KP_FIT_DEXTER;
+        out << "emission_type=" << fit << "\nemission_fit=" << emission_fit_name(fit) << "\n";
+    } else {
+        out << "riaf_r_min=" << o.riaf_r_min << "\nriaf_r_max=" << o.riaf_r_max << "\nriaf_nth0=" << o.riaf_nth0
+            << "\nriaf_Te0=" << o.riaf_Te0 << "\nriaf_disk_h=" << o.riaf_disk_h << "\nriaf_pow_nth=" << o.riaf_pow_nth
+            << "\nriaf_pow_T=" << o.riaf_pow_T << "\nriaf_ne_unit=" << o.riaf_ne_unit << "\nriaf_te_unit="
+            << o.riaf_te_unit << "\nriaf_mbh_solar=" << o.riaf_mbh_solar << "\nriaf_keplerian_factor="
+            << o.riaf_keplerian_factor << "\nriaf_infall_factor=" << o.riaf_infall_factor << "\n";
+        out << "emission_type=" << effective_emission_type(o) << "\nemission_fit="
+            << emission_fit_name(effective_emission_type(o)) << "\n";
+    }
     out << "# kp_precision=" << o.kp_precision << "\n# kp_schedule=" << o.kp_schedule << "\n";
 }
 

@@ -187,3 +187,77 @@ def test_tool_replays_riaf_recommended_par(tmp_path):
         key, _, fr = str(k).partition(":")
         cond[(key, int(fr)) if fr else key] = float(v)
     check_fp64(sample, fx, fixed=False, conditioning=cond)
+
+
+@pytest.mark.gpu
+def test_tool_images_an_iharm_dump(tmp_path):
+    """model=iharm through kp_model_image: a synthetic torus written as an
+    iharm dump (tests/iharm_dump.py), five frequencies in chunks whose step
+    control runs over all five, HDF5 output.  Every Stokes array equals the
+    library's image of the same dump (kp_grid_load_iharm +
+    kp_image_grmhd_step_control, packed with kp_pack_image), all chunks share
+    one geodesic per pixel, and the file carries the GRMHD metadata."""
+    import math
+
+    import hdf5_subset as h5
+    from iharm_dump import write_iharm_dump
+    from kpolaris_b200 import _abi, synthetic
+
+    assert TOOL.exists(), "kp_model_image not built"
+    prims, model = synthetic.fm_torus(48, 32, 16)
+    dump = tmp_path / "torus.h5"
+    write_iharm_dump(dump, prims, model, layout="chunked", chunks=(16, 16, 16, 8), filters=("shuffle", "deflate"))
+    inc = math.radians(163.0)
+    par = tmp_path / "iharm.par"
+    par.write_text(f"""
+model=iharm
+iharm_dump={dump}
+coordinate=fmks
+camera=pinhole
+nx=16
+ny=12
+radius=1000
+inclination_rad={inc!r}
+fov=0.04
+outer_radius=50
+step=0.025
+adaptive=1
+adaptive_tolerance=1e-8
+min_step=1e-10
+max_step=2
+max_steps=400000
+max_radiation_step=2
+max_radiation_depth=1
+max_absorption_depth=1
+max_faraday_depth=4
+freq_list=86e9,230e9,345e9,690e9,1e12
+M_unit=1e27
+iharm_mbh_solar=6.5e9
+trat_large=40
+emission_fit=dexter
+evpa_0=N
+""")
+    out = tmp_path / "img.h5"
+    r = subprocess.run([str(TOOL), f"--parameter_file={par}", f"--output={out}"], capture_output=True, text=True,
+                       timeout=900)
+    assert r.returncode == 0, r.stderr
+    f = h5.read(out)
+    assert f.attrs["model"] == "iharm" and f.attrs["nfreq"] == 5
+    assert f.attrs["grmhd_n1"] == 48 and f.attrs["iharm_trat_large"] == 40.0 and f.attrs["emission_type"] == 4
+
+    params = synthetic.fmks_pass_a_params(model, 16, 12, xspan=20.0, outer_radius=50.0)
+    opts = kp.default_iharm_options(M_unit=1e27, mbh_solar=6.5e9, trat_large=40.0, emission_type=_abi.FIT_DEXTER)
+    with kp.grid_load_iharm(dump, opts) as g:
+        fi = 0
+        for chunk in (FREQS[:4], FREQS[4:]):
+            res = kp.image_grmhd(params, g, chunk, control_frequencies=FREQS)
+            for k, freq in enumerate(chunk):
+                pk = kp.pack_image(res, k, freq, evpa_0="N")
+                grp = f[f"frame_0/freq_{fi}"]
+                for name, key in (("I_inv", "i_inv"), ("Q_inv", "q_inv"), ("U_inv", "u_inv"), ("V_inv", "v_inv")):
+                    assert np.array_equal(grp[name].value.ravel(), pk[key], equal_nan=True), (fi, name)
+                fi += 1
+            dg = f["frame_0/diagnostics"]
+            assert np.array_equal(dg["reason"].value.ravel(), res.reason)
+            assert np.array_equal(dg["steps"].value.ravel(), res.steps)
+    assert (np.asarray(f["frame_0/diagnostics/reason"].value) == 1).mean() > 0.9

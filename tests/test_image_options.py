@@ -206,7 +206,7 @@ def test_both_refuse(exes, tmp_path, name, args, par):
 
 def test_unbuilt_requests_are_refused(exes):
     tool, _ = exes
-    for extra in (["--analysis_mode=1"], ["--slow_light=1"], ["--model=iharm"], ["--repeat_images=2"]):
+    for extra in (["--analysis_mode=1"], ["--slow_light=1"], ["--model=kharma"], ["--repeat_images=2"]):
         r = _run(tool, extra, ["--kp_print_resolved=1"])
         assert r.returncode != 0 and "not built" in r.stderr, (extra, r.stderr)
 
@@ -284,3 +284,75 @@ def test_output_format_selection(exes, tmp_path):
     assert r.returncode == 0 and "format hdf5" in r.stdout, r.stderr
     r = _run(tool, [f"--output={tmp_path / 'x.out'}", "--format=fits"])
     assert r.returncode != 0 and "unknown output format" in r.stderr
+
+
+IHARM_PAR = """
+model=iharm
+coordinate=fmks
+camera=pinhole
+nx=32
+ny=24
+radius=1000
+inclination_deg=163
+dsource=16.9e6
+fovx_dsource=160
+fovy_dsource=120
+step=0.025
+adaptive=1
+adaptive_tolerance=1e-8
+min_step=1e-10
+max_step=1
+max_steps=800000
+freq=230e9
+M_unit=2e26
+iharm_mbh_solar=6.5e9
+trat_large=40
+emission_fit=dexter
+"""
+
+
+def test_iharm_runs_resolve_from_the_dump_header(exes, tmp_path):
+    """model=iharm: the dump's header sets the spin and the radii
+    (tools/kpolaris_model_image.cpp:5113-5125): outer radius min(r_out,
+    0.9 radius), inner radius max(r_in, 1.05 r_+); the field of view in
+    microarcseconds uses the iharm black-hole mass; the .params file names
+    the dump and the iharm options.  Header reading needs no GPU."""
+    from iharm_dump import write_iharm_dump
+    from kpolaris_b200 import synthetic
+
+    tool, _ = exes
+    prims, model = synthetic.fm_torus(12, 10, 6, spin=0.5, seed=5)
+    dump = tmp_path / "dump.h5"
+    write_iharm_dump(dump, prims, model)
+    par = tmp_path / "iharm.par"
+    par.write_text(IHARM_PAR + f"iharm_dump={dump}\n")
+    r = _run(tool, [f"--parameter_file={par}", "--kp_print_resolved=1"])
+    assert r.returncode == 0, r.stderr
+    res = _resolved(r.stdout)
+    horizon = 1.0 + math.sqrt(1.0 - 0.25)
+    assert float(res["spin"]) == 0.5
+    assert float(res["outer_radius"]) == min(model.r_out, 900.0)
+    assert float(res["inner_radius"]) == max(model.r_in, horizon * 1.05)
+    # 160 muas at 16.9 Mpc with 6.5e9 Msun (the tool's constants)
+    l_unit = 6.6742e-8 * 6.5e9 * 1.989e33 / 2.99792458e10 ** 2
+    m_per_muas = 16.9e6 * 3.085678e18 / l_unit / 2.06265e11
+    assert math.isclose(float(res["image_width_x"]), 160 * m_per_muas, rel_tol=1e-15)
+    out = tmp_path / "img.h5"
+    r = _run(tool, [f"--parameter_file={par}", f"--output={out}", "--kp_dry_run=1"])
+    assert r.returncode == 0 and "format hdf5" in r.stdout, r.stderr
+    text = Path(str(out) + ".params").read_text()
+    assert f"iharm_dump={dump}" in text and "iharm_M_unit=2.0000000000000001e+26" in text
+    assert "iharm_trat_large=40" in text
+    assert "emission_fit=dexter_thermal" in text and "spin=0.5" in text
+
+
+@pytest.mark.parametrize("extra,msg", [
+    ({"iharm_dump": "/nonexistent/dump.h5"}, "cannot open HDF5 file"),
+    ({"coordinate": "cartesian_ks"}, "iharm images are built for --coordinate=fmks"),
+])
+def test_iharm_runs_refuse_bad_input(exes, tmp_path, extra, msg):
+    tool, _ = exes
+    par = tmp_path / "iharm.par"
+    par.write_text(IHARM_PAR + "".join(f"{k}={v}\n" for k, v in extra.items()))
+    r = _run(tool, [f"--parameter_file={par}", "--kp_print_resolved=1"])
+    assert r.returncode != 0 and msg in r.stderr, r.stderr
