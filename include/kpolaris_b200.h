@@ -519,6 +519,24 @@ int kp_grid_load_iharm(const char* path, const kp_iharm_options* options, int de
 int kp_iharm_dump_time(const char* path, double* t);
 
 /*
+ * KHARMA GRMHD dumps (Parthenon .phdf: /Info NumMeshBlocks and
+ * MeshBlockSize, the run's parameter text in /Input File, Blocks/loc.lx123,
+ * prims.rho / prims.u [nblocks][nx3][nx2][nx1], prims.uvec / prims.B
+ * [nblocks][3][nx3][nx2][nx1]).  Replace read_kharma_staged_dump +
+ * materialize_kharma_model_from_staged and read_kharma_dump_time
+ * (src/grmhd/kharma_loader.cpp:556-823, 1066-1139, 726-749): the geometry
+ * from the parameter text (fmks and mmks transforms), the meshblocks
+ * assembled into the global grid, B negated with reverse_field; the
+ * options are KHARMALoadOptions' fields of kp_iharm_options (same defaults).
+ * The reference's checks and messages; file and format errors are KP_ERR_IO.
+ */
+int kp_kharma_read(const char* path, const kp_iharm_options* options, int reverse_field, kp_grmhd_model* model,
+                   float* prims, size_t capacity);
+int kp_grid_load_kharma(const char* path, const kp_iharm_options* options, int reverse_field, int device,
+                        kp_grmhd_model* model, kp_grid** out);
+int kp_kharma_dump_time(const char* path, double* t);
+
+/*
  * One GRMHD image in FMKS coordinates, 1..KP_MAX_FREQUENCIES frequencies on
  * one geodesic, through the wavefront engine (options->precision FP64, or
  * MIXED: FP64 geodesic and grid sample, FP32 fits and transfer).  Replaces

@@ -76,6 +76,11 @@ def library() -> C.CDLL:
     L.kp_grid_load_iharm.argtypes = [C.c_char_p, C.POINTER(_abi.IharmOptions), C.c_int,
                                      C.POINTER(_abi.GrmhdModel), C.POINTER(C.c_void_p)]
     L.kp_iharm_dump_time.argtypes = [C.c_char_p, C.POINTER(C.c_double)]
+    L.kp_kharma_read.argtypes = [C.c_char_p, C.POINTER(_abi.IharmOptions), C.c_int, C.POINTER(_abi.GrmhdModel),
+                                 C.POINTER(C.c_float), C.c_size_t]
+    L.kp_grid_load_kharma.argtypes = [C.c_char_p, C.POINTER(_abi.IharmOptions), C.c_int, C.c_int,
+                                      C.POINTER(_abi.GrmhdModel), C.POINTER(C.c_void_p)]
+    L.kp_kharma_dump_time.argtypes = [C.c_char_p, C.POINTER(C.c_double)]
     L.kp_image_grmhd.argtypes = [C.POINTER(PassAParams), C.c_void_p, C.c_int, C.POINTER(C.c_double), C.c_int,
                                  C.POINTER(RunOptions), C.POINTER(_abi.ImageOut)]
     L.kp_image_riaf_step_control.argtypes = [C.POINTER(PassAParams), C.POINTER(RIAFModel), C.c_int,
@@ -343,6 +348,43 @@ def grid_load_iharm(path, options: _abi.IharmOptions | None = None, device: int 
     m = _abi.GrmhdModel()
     h = C.c_void_p()
     check(L.kp_grid_load_iharm(str(path).encode(), C.byref(o), int(device), C.byref(m), C.byref(h)))
+    g = Grid.__new__(Grid)
+    g._h, g.model, g.device = h, m, device
+    return g
+
+
+def kharma_read(path, options: _abi.IharmOptions | None = None, *, reverse_field: bool = False,
+                header_only: bool = False):
+    """kp_kharma_read: (model, prims [8, n1, n2, n3] float32, or None with
+    header_only) from a KHARMA .phdf dump, on the host."""
+    L = library()
+    o = options if options is not None else default_iharm_options()
+    m = _abi.GrmhdModel()
+    check(L.kp_kharma_read(str(path).encode(), C.byref(o), int(reverse_field), C.byref(m), None, 0))
+    if header_only:
+        return m, None
+    prims = np.empty((8, m.n1, m.n2, m.n3), dtype=np.float32)
+    check(L.kp_kharma_read(str(path).encode(), C.byref(o), int(reverse_field), C.byref(m),
+                           prims.ctypes.data_as(C.POINTER(C.c_float)), prims.size))
+    return m, prims
+
+
+def kharma_dump_time(path) -> float:
+    """kp_kharma_dump_time: the /Info Time attribute."""
+    t = C.c_double()
+    check(library().kp_kharma_dump_time(str(path).encode(), C.byref(t)))
+    return t.value
+
+
+def grid_load_kharma(path, options: _abi.IharmOptions | None = None, *, reverse_field: bool = False,
+                     device: int = 0) -> "Grid":
+    """kp_grid_load_kharma: a KHARMA dump read and uploaded as a resident Grid."""
+    L = library()
+    o = options if options is not None else default_iharm_options()
+    m = _abi.GrmhdModel()
+    h = C.c_void_p()
+    check(L.kp_grid_load_kharma(str(path).encode(), C.byref(o), int(reverse_field), int(device), C.byref(m),
+                                C.byref(h)))
     g = Grid.__new__(Grid)
     g._h, g.model, g.device = h, m, device
     return g

@@ -1,11 +1,12 @@
-// kp_io.cu -- C ABI of the GRMHD dump readers (host code: the iharm HDF5
-// dump through kpolaris_b200/host/kp_iharm.hpp).  Exceptions never cross
+// kp_io.cu -- C ABI of the GRMHD dump readers (host code: iharm and KHARMA
+// HDF5 dumps through kpolaris_b200/host/kp_iharm.hpp and kp_kharma.hpp).  Exceptions never cross
 // the ABI: reader and format errors become KP_ERR_IO with their message.
 #include <exception>
 #include <stdexcept>
 #include <string>
 
 #include "kp_iharm.hpp"
+#include "kp_kharma.hpp"
 #include "kpolaris_b200.h"
 
 namespace kp {
@@ -79,6 +80,44 @@ int kp_iharm_dump_time(const char* path, double* t) {
     if (!path || !t) return kp::set_error(KP_ERR_INVALID, "kp_iharm_dump_time: null argument");
     return guarded([&] {
         *t = kpb::read_iharm_dump_time(path);
+        return int(KP_OK);
+    });
+}
+
+int kp_kharma_read(const char* path, const kp_iharm_options* options, int reverse_field, kp_grmhd_model* model,
+                   float* prims, size_t capacity) {
+    if (!path || !options || !model) return kp::set_error(KP_ERR_INVALID, "kp_kharma_read: null argument");
+    return guarded([&] {
+        kpb::IharmDump d = kpb::load_kharma_dump(path, *options, reverse_field, prims != nullptr);
+        if (prims) {
+            if (capacity < d.prims.size())
+                return kp::set_error(KP_ERR_INVALID, "kp_kharma_read: primitives need %zu floats, capacity %zu",
+                                     d.prims.size(), capacity);
+            std::copy(d.prims.begin(), d.prims.end(), prims);
+        }
+        *model = d.model;
+        return int(KP_OK);
+    });
+}
+
+int kp_grid_load_kharma(const char* path, const kp_iharm_options* options, int reverse_field, int device,
+                        kp_grmhd_model* model, kp_grid** out) {
+    if (!path || !options || !out) return kp::set_error(KP_ERR_INVALID, "kp_grid_load_kharma: null argument");
+    *out = nullptr;
+    kpb::IharmDump d;
+    const int rc = guarded([&] {
+        d = kpb::load_kharma_dump(path, *options, reverse_field, true);
+        return int(KP_OK);
+    });
+    if (rc != KP_OK) return rc;
+    if (model) *model = d.model;
+    return kp_grid_upload(&d.model, d.prims.data(), device, out);
+}
+
+int kp_kharma_dump_time(const char* path, double* t) {
+    if (!path || !t) return kp::set_error(KP_ERR_INVALID, "kp_kharma_dump_time: null argument");
+    return guarded([&] {
+        *t = kpb::read_kharma_dump_time(path);
         return int(KP_OK);
     });
 }

@@ -44,7 +44,7 @@ struct FormatError : std::runtime_error {
     using std::runtime_error::runtime_error;
 };
 
-enum class ElemType { Int, UInt, Float, String, Other };
+enum class ElemType { Int, UInt, Float, String, VarString, Other };
 
 struct DatasetInfo {
     std::vector<uint64_t> dims;  // empty: scalar
@@ -75,7 +75,7 @@ class Reader {
 public:
     explicit Reader(const std::string& path) : path_(path) {
         f_ = std::fopen(path.c_str(), "rb");
-        if (!f_) throw std::runtime_error("cannot open HDF5 file: " + path);
+        if (!f_) throw FormatError("cannot open HDF5 file: " + path);
         std::fseek(f_, 0, SEEK_END);
         file_size_ = uint64_t(std::ftell(f_));
         try {
@@ -99,7 +99,7 @@ public:
 
     DatasetInfo info(const std::string& path) {
         uint64_t addr = 0;
-        if (!resolve(path, addr)) throw std::runtime_error("HDF5 object not found: " + path);
+        if (!resolve(path, addr)) throw FormatError("HDF5 object not found: " + path);
         return dataset_info(addr, path);
     }
 
@@ -119,6 +119,52 @@ public:
         std::vector<T> out(static_cast<size_t>(n));
         for (uint64_t i = 0; i < n; ++i) out[size_t(i)] = convert<T>(raw.data() + i * d.elem, d);
         return out;
+    }
+
+    // An attribute of the object at `path` ("" or "/" for the root group):
+    // numeric values row-major in `raw`, or the text of a fixed-length or
+    // variable-length string in `text`.
+    struct AttrValue {
+        std::vector<uint64_t> dims;
+        DatasetInfo type;
+        std::vector<uint8_t> raw;
+        std::string text;
+        uint64_t count() const {
+            uint64_t n = 1;
+            for (uint64_t d : dims) n *= d;
+            return n;
+        }
+    };
+
+    bool has_attr(const std::string& path, const std::string& name) {
+        AttrValue v;
+        return find_attr(path, name, v, false);
+    }
+
+    AttrValue attr(const std::string& path, const std::string& name) {
+        AttrValue v;
+        if (!find_attr(path, name, v, true)) throw FormatError("HDF5 attribute not found: " + path + " " + name);
+        return v;
+    }
+
+    template <class T>
+    std::vector<T> attr_values(const std::string& path, const std::string& name) {
+        const AttrValue v = attr(path, name);
+        const DatasetInfo& d = v.type;
+        if (d.type != ElemType::Int && d.type != ElemType::UInt && d.type != ElemType::Float)
+            throw FormatError("HDF5 attribute " + name + " is not numeric");
+        const uint64_t n = v.count();
+        if (v.raw.size() < n * d.elem) throw FormatError("HDF5 attribute " + name + " truncated");
+        std::vector<T> out(static_cast<size_t>(n));
+        for (uint64_t i = 0; i < n; ++i) out[size_t(i)] = convert<T>(v.raw.data() + i * d.elem, d);
+        return out;
+    }
+
+    std::string attr_string(const std::string& path, const std::string& name) {
+        const AttrValue v = attr(path, name);
+        if (v.type.type != ElemType::String && v.type.type != ElemType::VarString)
+            throw FormatError("HDF5 attribute " + name + " is not a string");
+        return v.text;
     }
 
     template <class T>
@@ -395,6 +441,85 @@ private:
         return false;
     }
 
+    // -- attributes ----------------------------------------------------------
+    // Attribute messages versions 1-3; dense attribute storage (an
+    // Attribute Info message with a fractal heap) is refused.
+    bool find_attr(const std::string& path, const std::string& name, AttrValue& out, bool decode) {
+        uint64_t addr = 0;
+        if (!resolve(path, addr)) throw FormatError("HDF5 object not found: " + path);
+        const std::vector<Msg> msgs = header(addr);
+        for (const Msg& m : msgs) {
+            if (m.type == 0x15) {
+                Cursor c{m.data, 0};
+                c.u(1);
+                const int flags = int(c.u(1));
+                if (flags & 0x01) c.need(2);
+                if (offset(c.need(size_t(so_))) != kUndef)
+                    throw FormatError("HDF5 dense attribute storage (fractal heap) is not supported");
+            }
+            if (m.type != 0x0C) continue;
+            Cursor c{m.data, 0};
+            const int version = int(c.u(1));
+            const int flags = int(c.u(1));
+            const size_t nsz = size_t(c.u(2)), tsz = size_t(c.u(2)), ssz = size_t(c.u(2));
+            if (version < 1 || version > 3) throw FormatError("HDF5 attribute message version");
+            if (version >= 2 && (flags & 0x03)) throw FormatError("HDF5 shared attribute types are not supported");
+            if (version == 3) c.u(1);  // name character set
+            auto pad = [version](size_t n) { return version == 1 ? (n + 7) / 8 * 8 : n; };
+            const uint8_t* nm = c.need(pad(nsz));
+            std::string aname(reinterpret_cast<const char*>(nm), nsz);
+            while (!aname.empty() && aname.back() == '\0') aname.pop_back();
+            if (aname != name) continue;
+            if (!decode) return true;
+            const uint8_t* tp = c.need(pad(tsz));
+            const uint8_t* sp = c.need(pad(ssz));
+            const std::vector<uint8_t> tb(tp, tp + tsz), sb(sp, sp + ssz);
+            datatype(tb, out.type);
+            DatasetInfo space;
+            dataspace(sb, space);
+            out.dims = space.dims;
+            out.raw.assign(m.data.begin() + long(c.p), m.data.end());
+            const uint64_t n = out.count();
+            if (out.type.type == ElemType::String) {
+                if (n != 1) throw FormatError("HDF5 string attribute arrays are not supported");
+                const size_t len = std::min(out.raw.size(), out.type.elem);
+                out.text.assign(reinterpret_cast<const char*>(out.raw.data()), strnlen(
+                    reinterpret_cast<const char*>(out.raw.data()), len));
+            } else if (out.type.type == ElemType::VarString) {
+                if (n != 1) throw FormatError("HDF5 string attribute arrays are not supported");
+                if (out.raw.size() < 4 + size_t(so_) + 4) throw FormatError("HDF5 variable-length string truncated");
+                const uint64_t len = le(out.raw.data(), 4);
+                const uint64_t heap = offset(out.raw.data() + 4);
+                const uint64_t index = le(out.raw.data() + 4 + so_, 4);
+                out.text = global_heap_object(heap, index, len);
+            }
+            return true;
+        }
+        return false;
+    }
+
+    // One object of a global heap collection ("GCOL"), its first `len` bytes.
+    std::string global_heap_object(uint64_t addr, uint64_t index, uint64_t len) {
+        const std::vector<uint8_t> h = bytes(addr, 8 + size_t(sl_));
+        if (std::memcmp(h.data(), "GCOL", 4) != 0 || h[4] != 1) throw FormatError("HDF5 global heap collection");
+        const uint64_t size = length(&h[8]);
+        const std::vector<uint8_t> b = bytes(addr, size);
+        size_t p = 8 + size_t(sl_);
+        while (p + 8 + size_t(sl_) <= b.size()) {
+            const uint64_t idx = le(&b[p], 2);
+            const uint64_t osz = length(&b[p + 8]);
+            const size_t data = p + 8 + size_t(sl_);
+            if (idx == 0) break;  // free space: the rest of the collection
+            if (data + osz > b.size()) throw FormatError("HDF5 global heap object overruns its collection");
+            if (idx == index) {
+                if (len > osz) throw FormatError("HDF5 variable-length string longer than its heap object");
+                return std::string(reinterpret_cast<const char*>(&b[data]), size_t(len));
+            }
+            p = data + size_t((osz + 7) / 8 * 8);
+        }
+        throw FormatError("HDF5 global heap object not found");
+    }
+
     // -- datasets ------------------------------------------------------------
     DatasetInfo dataset_info(uint64_t addr, const std::string& path) {
         const std::vector<Msg> msgs = header(addr);
@@ -464,6 +589,9 @@ private:
             d.type = ElemType::Float;
         } else if (cls == 3) {
             d.type = ElemType::String;
+        } else if (cls == 9) {
+            // variable-length: bits 0-3 of the class bits are 1 for a string
+            d.type = (bits0 & 0x0F) == 1 ? ElemType::VarString : ElemType::Other;
         } else {
             d.type = ElemType::Other;
         }

@@ -40,17 +40,27 @@ def _pad8(b: bytes) -> bytes:
     return b + bytes((-len(b)) % 8)
 
 
-class Dataset:
+class _Attrs:
+    def attr(self, name, value):
+        """A numeric scalar or array, a str (variable-length UTF-8 string, as
+        h5py stores a Python str) or bytes (fixed-length string)."""
+        self.attrs[name] = value
+        return self
+
+
+class Dataset(_Attrs):
     def __init__(self, value, layout="contiguous", chunks=None, filters=(), index="btree", continuation=False):
         self.value = np.asarray(value)
         self.layout, self.chunks, self.filters = layout, chunks, tuple(filters)
         self.index, self.continuation = index, continuation
+        self.attrs = {}
 
 
-class Group:
+class Group(_Attrs):
     def __init__(self, fanout: int = 32, continuation: bool = False):
         self.children: dict[str, object] = {}
         self.fanout, self.continuation = fanout, continuation
+        self.attrs = {}
 
     def group(self, name, **kw) -> "Group":
         g = Group(**kw)
@@ -140,6 +150,16 @@ def _chunks_of(value: np.ndarray, chunks):
         yield o, block.tobytes()
 
 
+def _vlen_string_type(so: int = 8) -> bytes:
+    # class 9 version 1, string, null-terminated, UTF-8; base type one byte
+    base = struct.pack("<BBBBI", 0x10, 0, 0, 0, 1) + struct.pack("<HH", 0, 8)
+    return struct.pack("<BBBBI", 0x19, 0x01, 0x01, 0, 4 + so + 4) + base
+
+
+def _fixed_string_type(n: int) -> bytes:
+    return struct.pack("<BBBBI", 0x13, 0x00, 0, 0, n)
+
+
 class _Writer:
     def __init__(self, profile: str, userblock: int):
         self.profile = profile
@@ -185,6 +205,39 @@ class _Writer:
         whole = head + body
         return self.img.alloc(whole + struct.pack("<I", lookup3(whole)))
 
+    # -- attributes ------------------------------------------------------------
+    def _global_heap(self, data: bytes):
+        """(collection address, object index) of `data` in a new 4096-byte
+        global heap collection; the rest of it is the free-space object."""
+        obj = struct.pack("<HHIQ", 1, 0, 0, len(data)) + _pad8(data)
+        size = max(4096, 16 + len(obj) + 16)
+        free = size - 16 - len(obj)
+        body = b"GCOL" + struct.pack("<B3xQ", 1, size) + obj + struct.pack("<HHIQ", 0, 0, 0, free)
+        body += bytes(size - len(body))
+        return self.img.alloc(body), 1
+
+    def attr_messages(self, attrs):
+        msgs = []
+        for name, value in attrs.items():
+            if isinstance(value, str):
+                raw = value.encode()
+                addr, idx = self._global_heap(raw)
+                dtype, space, data = _vlen_string_type(), (), struct.pack("<IQI", len(raw), addr, idx)
+            elif isinstance(value, bytes):
+                dtype, space, data = _fixed_string_type(len(value) + 1), (), value + b"\0"
+            else:
+                v = np.asarray(value)
+                v = v.astype(v.dtype.newbyteorder("<"))
+                dtype, space, data = _datatype(v.dtype), v.shape, v.tobytes()
+            ds = _dataspace(space, 1 if self.profile == "earliest" else 2)
+            nm = name.encode() + b"\0"
+            if self.profile == "earliest":
+                body = struct.pack("<BBHHH", 1, 0, len(nm), len(dtype), len(ds)) + _pad8(nm) + _pad8(dtype) + _pad8(ds)
+            else:
+                body = struct.pack("<BBHHHB", 3, 0, len(nm), len(dtype), len(ds), 0) + nm + dtype + ds
+            msgs.append((0x0C, body + data))
+        return msgs
+
     # -- groups ----------------------------------------------------------------
     def group(self, g: Group) -> int:
         addrs = {name: (self.group(c) if isinstance(c, Group) else self.dataset(c))
@@ -194,7 +247,7 @@ class _Writer:
             for name, a in addrs.items():
                 nm = name.encode()
                 msgs.append((0x06, struct.pack("<BBB", 1, 0, len(nm)) + nm + struct.pack("<Q", a)))
-            return self.header(msgs, g.continuation)
+            return self.header(msgs + self.attr_messages(g.attrs), g.continuation)
         # local heap of names: offset 0 is the empty string
         names = sorted(addrs)
         heap = bytearray(8)
@@ -222,7 +275,8 @@ class _Writer:
         leaves = [snods[i:i + g.fanout] for i in range(0, len(snods), g.fanout)]
         level0 = [(node(0, kids), kids[-1][1]) for kids in leaves]
         root = level0[0][0] if len(level0) == 1 else node(1, level0)
-        return self.header([(0x11, struct.pack("<QQ", root, heap_addr))], g.continuation)
+        return self.header([(0x11, struct.pack("<QQ", root, heap_addr))] + self.attr_messages(g.attrs),
+                           g.continuation)
 
     # -- datasets --------------------------------------------------------------
     def dataset(self, d: Dataset) -> int:
@@ -264,7 +318,7 @@ class _Writer:
                     addr = self.img.alloc(b"".join(raw for _, raw in data))
                     msgs.append((0x08, head + struct.pack("<BQ", 2, addr)))
         msgs.append((0x12, struct.pack("<B3xI", 1, 1700000000)))  # modification time (skipped by readers)
-        return self.header(msgs, d.continuation)
+        return self.header(msgs + self.attr_messages(d.attrs), d.continuation)
 
     def _chunk_btree(self, entries, shape, fanout: int = 3) -> int:
         rank = len(shape)

@@ -194,3 +194,23 @@ def test_iharm_dump_images_like_the_reference(tmp_path, name):
     for key in res.arrays:
         assert np.array_equal(res.arrays[key], direct.arrays[key], equal_nan=True), key
     check_grmhd(res, fx, fixed=not params.adaptive, cond=cond)
+
+
+def test_kharma_dump_images_like_the_reference(tmp_path):
+    """The adaptive golden case's primitives written as a KHARMA .phdf dump
+    (3 x 2 x 2 meshblocks stored in shuffled order, chunked and compressed),
+    loaded with kp_grid_load_kharma and imaged: bit-identical to the directly
+    uploaded grid and within the bars above of the reference's image."""
+    from kharma_dump import write_kharma_dump
+
+    fx, prims, model, params, freqs, cond = load_case("grmhd_adaptive_16")
+    path = tmp_path / "dump.phdf"
+    write_kharma_dump(path, prims, model, blocks=(3, 2, 2), order_seed=11, layout="chunked",
+                      chunks=(1, 1, 4, 8, 16), filters=("shuffle", "deflate"))
+    opt = kp.default_iharm_options(freq_cgs=model.freq_cgs, M_unit=model.M_unit, mbh_solar=model.mbh_solar,
+                                   trat_large=model.trat_large, emission_type=model.emission_type)
+    with kp.grid_load_kharma(path, opt) as g:
+        for k in ("n1", "n2", "n3", "spin", "startx1", "hslope", "poly_alpha", "poly_xt", "r_in", "r_out"):
+            assert getattr(g.model, k) == pytest.approx(getattr(model, k), rel=1e-15), k
+        res = kp.image_grmhd(params, g, freqs)
+    check_grmhd(res, fx, fixed=not params.adaptive, cond=cond)

@@ -48,7 +48,11 @@ def run_probe(exe, path, paths, outdir):
         if ex == "exists 0":
             out[p] = None
             continue
-        rank = [int(x) for x in next(lines).split()[1:]]
+        kind = next(lines)
+        if kind == "text":
+            out[p] = (outdir / f"{i}.txt").read_bytes().decode()
+            continue
+        rank = [int(x) for x in kind.split()[1:]]
         shape = tuple(rank[1:])
         f64 = np.fromfile(outdir / f"{i}.f64", dtype=np.float64).reshape(shape)
         i64 = np.fromfile(outdir / f"{i}.i64", dtype=np.int64).reshape(shape)
@@ -69,7 +73,7 @@ def sample_tree(rng, profile):
     geom.dataset("r_in", arrays["header/geom/fmks/r_in"], continuation=True)
     prims = rng.standard_normal((9, 10, 11, 8)).astype(np.float32)
     arrays["prims"] = prims
-    root.dataset("prims", prims)
+    root.dataset("prims", prims).attr("units", np.array([1.5, 2.5], dtype=np.float32))
     arrays["prims_chunked"] = prims
     root.dataset("prims_chunked", prims, layout="chunked", chunks=(4, 3, 5, 8), filters=("shuffle", "deflate"))
     arrays["plain_chunked"] = rng.standard_normal((7, 13))
@@ -80,6 +84,14 @@ def sample_tree(rng, profile):
     ints = root.group("ints")
     for dt in (np.int8, np.uint16, np.int64, np.uint32):
         ints.dataset(np.dtype(dt).name, arrays[f"ints/{np.dtype(dt).name}"])
+    # attributes: numbers, arrays, a variable-length (h5py str) and a
+    # fixed-length string, on groups and datasets
+    attrs = {"@@Time": np.float64(1234.5), "@@NumBlocks": np.int64(6),
+             "@@Size": np.array([16, 8, 4], dtype=np.int64), "@@note": "<mesh>\nnx1 = 8\n# comment\n",
+             "@header@code": b"KHARMA", "@prims@units": np.array([1.5, 2.5], dtype=np.float32)}
+    root.attr("Time", attrs["@@Time"]).attr("NumBlocks", attrs["@@NumBlocks"])
+    root.attr("Size", attrs["@@Size"]).attr("note", attrs["@@note"])
+    hdr.attr("code", attrs["@header@code"])
     many = root.group("many", fanout=2)
     for k in range(20):
         arrays[f"many/d{k:02d}"] = np.float64(k * 1.5)
@@ -92,6 +104,7 @@ def sample_tree(rng, profile):
         root.dataset("single_raw", arrays["single_raw"], layout="chunked", chunks=(4, 4), index="single")
         arrays["implicit"] = rng.standard_normal((6, 9))
         root.dataset("implicit", arrays["implicit"], layout="chunked", chunks=(3, 4), index="implicit")
+    arrays.update(attrs)
     return root, arrays
 
 
@@ -101,10 +114,13 @@ def test_reads_every_value(probe, tmp_path, profile, userblock):
     root, arrays = sample_tree(rng, profile)
     path = tmp_path / "f.h5"
     h5w.write(path, root, profile=profile, userblock=userblock)
-    paths = sorted(arrays) + ["missing", "header/missing", "many/d20"]
+    paths = sorted(arrays) + ["missing", "header/missing", "many/d20", "@@missing", "@prims@missing"]
     out, log = run_probe(probe, path, paths, tmp_path / "out")
     assert out is not None, log
     for p, a in arrays.items():
+        if isinstance(a, (str, bytes)):
+            assert out[p] == (a if isinstance(a, str) else a.decode()), p
+            continue
         f64, i64 = out[p]
         assert f64.shape == np.shape(a), p
         assert np.array_equal(f64, np.asarray(a, dtype=np.float64)), p
