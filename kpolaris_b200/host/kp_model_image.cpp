@@ -1,9 +1,10 @@
 // kp_model_image -- command-line image tool for the RIAF image path and
-// iharm GRMHD dumps, the counterpart of the reference's kpolaris_model_image
-// for model=riaf and model=iharm (tools/kpolaris_model_image.cpp:4908-5126
-// main, :3909-4260 run_model, :2561-2800 output packing, :4136-4245 CSV
-// output).  An iharm dump is read by kp_iharm_read / kp_grid_load_iharm
-// and imaged with kp_image_grmhd_step_control.
+// iharm and KHARMA GRMHD dumps, the counterpart of the reference's
+// kpolaris_model_image for model=riaf, iharm and kharma
+// (tools/kpolaris_model_image.cpp:4908-5195 main, :3909-4260 run_model,
+// :2561-2800 output packing, :4136-4245 CSV output).  A dump is read by
+// kp_iharm_read / kp_kharma_read and kp_grid_load_iharm /
+// kp_grid_load_kharma and imaged with kp_image_grmhd_step_control.
 //
 //   kp_model_image --parameter_file=run.par [--key=value ...]
 //
@@ -88,12 +89,17 @@ int run(const std::vector<std::string>& args) {
     kpb::finalize_options(opt);
     // model=iharm: the dump's header settles the spin, the radii and the
     // coordinate map (read on the host; no device yet)
-    const bool grmhd = opt.model == "iharm";
+    const bool grmhd = kpb::grmhd_model(opt);
+    const bool kharma = opt.model == "kharma";
     kp_grmhd_model gm{};
     kp_iharm_options io{};
     if (grmhd) {
         io = kpb::to_iharm_options(opt);
-        check(kp_iharm_read(opt.iharm_dump.c_str(), &io, &gm, nullptr, 0), "kp_iharm_read");
+        if (kharma)
+            check(kp_kharma_read(opt.kharma_dump.c_str(), &io, opt.kharma_reverse_field, &gm, nullptr, 0),
+                  "kp_kharma_read");
+        else
+            check(kp_iharm_read(opt.iharm_dump.c_str(), &io, &gm, nullptr, 0), "kp_iharm_read");
         kpb::resolve_grmhd_geometry(opt, gm);
     }
     if (opt.kp_print_resolved) {
@@ -134,8 +140,13 @@ int run(const std::vector<std::string>& args) {
     kp_grid* grid = nullptr;
     if (grmhd) {
         const auto t_load = std::chrono::steady_clock::now();
-        check(kp_grid_load_iharm(opt.iharm_dump.c_str(), &io, opt.kp_device, &gm, &grid), "kp_grid_load_iharm");
-        report_timing(opt, "iharm_load_total", seconds_since(t_load));
+        if (kharma)
+            check(kp_grid_load_kharma(opt.kharma_dump.c_str(), &io, opt.kharma_reverse_field, opt.kp_device, &gm,
+                                      &grid),
+                  "kp_grid_load_kharma");
+        else
+            check(kp_grid_load_iharm(opt.iharm_dump.c_str(), &io, opt.kp_device, &gm, &grid), "kp_grid_load_iharm");
+        report_timing(opt, kharma ? "kharma_load_total" : "iharm_load_total", seconds_since(t_load));
     }
     struct GridGuard {
         kp_grid* g;
@@ -311,7 +322,7 @@ int main(int argc, char** argv) {
         const std::string a(argv[i]);
         if (a == "--help" || a == "-h") {
             std::cout << "usage: kp_model_image --parameter_file=FILE.par [--key=value ...]\n"
-                         "RIAF images and iharm GRMHD dumps through the KPolaris-B200 C ABI; HDF5 or CSV "
+                         "RIAF images and iharm / KHARMA GRMHD dumps through the KPolaris-B200 C ABI; HDF5 or CSV "
                          "output and <output>.params.\n";
             return 0;
         }

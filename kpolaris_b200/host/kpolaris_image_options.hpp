@@ -128,6 +128,17 @@ struct ImageOptions {
     double iharm_sigma_cut = 1.0;
     double iharm_sigma_cut_high = -1.0;
     int iharm_interpolate_derived_scalars = 1;
+    // model=kharma (tools/kpolaris_model_image_options.hpp:210-227 defaults)
+    std::string kharma_dump;
+    double kharma_M_unit = 3.0e25;
+    double kharma_mbh_solar = 6.2e9;
+    double kharma_trat_small = 1.0;
+    double kharma_trat_large = 20.0;
+    double kharma_beta_crit = 1.0;
+    double kharma_sigma_cut = 1.0;
+    double kharma_sigma_cut_high = -1.0;
+    int kharma_interpolate_derived_scalars = 1;
+    int kharma_reverse_field = 0;
     int timing = 0;
     int repeat_images = 1;
     // requests for subsystems that are not built (checked by validate_options)
@@ -366,18 +377,41 @@ inline const KeyTable& key_table() {
         t.add({"riaf_mbh_solar"}, real_field(&O::riaf_mbh_solar));
         t.add({"riaf_keplerian_factor"}, real_field(&O::riaf_keplerian_factor));
         t.add({"riaf_infall_factor"}, real_field(&O::riaf_infall_factor));
-        // iharm dump options (kpolaris_model_image_options.cpp:827-966); the
-        // unprefixed forms set every GRMHD loader's value, here the iharm one
-        t.add({"iharm_dump", "dump"}, text_field(&O::iharm_dump));
-        t.add({"iharm_M_unit", "iharm_m_unit", "M_unit"}, real_field(&O::iharm_M_unit));
-        t.add({"iharm_mbh_solar", "MBH"}, real_field(&O::iharm_mbh_solar));
-        t.add({"iharm_trat_small", "trat_small"}, real_field(&O::iharm_trat_small));
-        t.add({"iharm_trat_large", "trat_large"}, real_field(&O::iharm_trat_large));
-        t.add({"iharm_beta_crit", "beta_crit"}, real_field(&O::iharm_beta_crit));
-        t.add({"iharm_sigma_cut", "sigma_cut"}, real_field(&O::iharm_sigma_cut));
-        t.add({"iharm_sigma_cut_high", "sigma_cut_high"}, real_field(&O::iharm_sigma_cut_high));
-        t.add({"iharm_interpolate_derived_scalars", "interpolate_derived_scalars"},
-              int_field(&O::iharm_interpolate_derived_scalars));
+        // GRMHD dump options (kpolaris_model_image_options.cpp:827-970): the
+        // prefixed forms set one loader's value, the unprefixed forms both
+        auto both = [](double O::*a, double O::*b) {
+            return [a, b](O& o, const std::string& v) { o.*a = o.*b = to_real(v); };
+        };
+        t.add({"iharm_dump"}, text_field(&O::iharm_dump));
+        t.add({"kharma_dump", "phdf"}, text_field(&O::kharma_dump));
+        t.add({"dump"}, [](O& o, const std::string& v) { o.iharm_dump = o.kharma_dump = v; });
+        t.add({"iharm_M_unit", "iharm_m_unit"}, real_field(&O::iharm_M_unit));
+        t.add({"kharma_M_unit", "kharma_m_unit"}, real_field(&O::kharma_M_unit));
+        t.add({"M_unit"}, both(&O::iharm_M_unit, &O::kharma_M_unit));
+        t.add({"iharm_mbh_solar"}, real_field(&O::iharm_mbh_solar));
+        t.add({"kharma_mbh_solar"}, real_field(&O::kharma_mbh_solar));
+        t.add({"MBH"}, both(&O::iharm_mbh_solar, &O::kharma_mbh_solar));
+        t.add({"iharm_trat_small"}, real_field(&O::iharm_trat_small));
+        t.add({"kharma_trat_small"}, real_field(&O::kharma_trat_small));
+        t.add({"trat_small"}, both(&O::iharm_trat_small, &O::kharma_trat_small));
+        t.add({"iharm_trat_large"}, real_field(&O::iharm_trat_large));
+        t.add({"kharma_trat_large"}, real_field(&O::kharma_trat_large));
+        t.add({"trat_large"}, both(&O::iharm_trat_large, &O::kharma_trat_large));
+        t.add({"iharm_beta_crit"}, real_field(&O::iharm_beta_crit));
+        t.add({"kharma_beta_crit"}, real_field(&O::kharma_beta_crit));
+        t.add({"beta_crit"}, both(&O::iharm_beta_crit, &O::kharma_beta_crit));
+        t.add({"iharm_sigma_cut"}, real_field(&O::iharm_sigma_cut));
+        t.add({"kharma_sigma_cut"}, real_field(&O::kharma_sigma_cut));
+        t.add({"sigma_cut"}, both(&O::iharm_sigma_cut, &O::kharma_sigma_cut));
+        t.add({"iharm_sigma_cut_high"}, real_field(&O::iharm_sigma_cut_high));
+        t.add({"kharma_sigma_cut_high"}, real_field(&O::kharma_sigma_cut_high));
+        t.add({"sigma_cut_high"}, both(&O::iharm_sigma_cut_high, &O::kharma_sigma_cut_high));
+        t.add({"iharm_interpolate_derived_scalars"}, int_field(&O::iharm_interpolate_derived_scalars));
+        t.add({"kharma_interpolate_derived_scalars"}, int_field(&O::kharma_interpolate_derived_scalars));
+        t.add({"interpolate_derived_scalars"}, [](O& o, const std::string& v) {
+            o.iharm_interpolate_derived_scalars = o.kharma_interpolate_derived_scalars = to_int(v);
+        });
+        t.add({"kharma_reverse_field", "reverse_field"}, int_field(&O::kharma_reverse_field));
         t.add({"emission_type"}, int_field(&O::emission_type));
         t.add({"emission_fit"}, [](O& o, const std::string& v) { o.emission_type = emission_type_from_name(v); });
         t.add({"timing", "profile"}, int_field(&O::timing));
@@ -506,8 +540,11 @@ inline ImageOptions parse_options(const std::vector<std::string>& args) {
 // The black-hole mass of the model's length unit (camera_mbh_solar /
 // output_mbh_solar, kpolaris_model_image_options.cpp:126-134).
 inline double model_mbh_solar(const ImageOptions& o) {
-    return o.model == "iharm" ? o.iharm_mbh_solar : o.riaf_mbh_solar;
+    return o.model == "iharm" ? o.iharm_mbh_solar : o.model == "kharma" ? o.kharma_mbh_solar : o.riaf_mbh_solar;
 }
+
+// The GRMHD dump models the tool images.
+inline bool grmhd_model(const ImageOptions& o) { return o.model == "iharm" || o.model == "kharma"; }
 
 inline double length_unit_cm(double mbh_solar) {
     // the tool's constants (kpolaris_model_image_options.cpp:119-124)
@@ -612,18 +649,19 @@ inline void finalize_options(ImageOptions& o) {
     validate_options(o);
     resolve_camera_extents(o);
     validate_resolved_camera(o);
-    if (o.model == "iharm") {
+    if (grmhd_model(o)) {
         // the radii and the spin come from the dump (resolve_grmhd_geometry)
         if (o.coordinate != "fmks")
-            throw std::runtime_error("iharm images are built for --coordinate=fmks (the dump's native grid)");
-        if (o.camera != "pinhole") throw std::runtime_error("iharm images are built for the pinhole camera");
+            throw std::runtime_error(o.model + " images are built for --coordinate=fmks (the dump's native grid)");
+        if (o.camera != "pinhole") throw std::runtime_error(o.model + " images are built for the pinhole camera");
         return;
     }
     const double horizon = 1.0 + std::sqrt(std::max(0.0, 1.0 - o.spin * o.spin));
     if (o.inner_radius <= 0.0) o.inner_radius = horizon * 1.05;
     if (o.model != "riaf")
         throw std::runtime_error("model '" + o.model +
-                                 "' is not built in this tool: riaf and iharm only (other GRMHD grids go through "
+                                 "' is not built in this tool: riaf, iharm and kharma only (other GRMHD grids go "
+                                 "through "
                                  "kp_grid_upload / kp_image_grmhd)");
     if (o.outer_radius <= 0.0) o.outer_radius = o.riaf_r_max * 1.15;
 }
@@ -653,21 +691,24 @@ inline void apply_fmks_map(kp_pass_a_params& p, const kp_grmhd_model& m) {
     p.fmks_poly_norm = m.poly_norm;
 }
 
-// IHARMLoadOptions of an iharm run (make_iharm_load_options,
-// tools/kpolaris_model_image.cpp:1734-1767); the fit defaults to Dexter.
+// The load options of an iharm or KHARMA run (make_iharm_load_options,
+// tools/kpolaris_model_image.cpp:1734-1767, and the KHARMA block of main,
+// :5130-5175); the fit defaults to Dexter.
 inline kp_iharm_options to_iharm_options(const ImageOptions& o) {
     kp_iharm_options io;
     kp_default_iharm_options(&io);
+    const bool k = o.model == "kharma";
     io.freq_cgs = o.freq;
-    io.M_unit = o.iharm_M_unit;
-    io.mbh_solar = o.iharm_mbh_solar;
-    io.trat_small = o.iharm_trat_small;
-    io.trat_large = o.iharm_trat_large;
-    io.beta_crit = o.iharm_beta_crit;
-    io.sigma_cut = o.iharm_sigma_cut;
-    io.sigma_cut_high = o.iharm_sigma_cut_high;
+    io.M_unit = k ? o.kharma_M_unit : o.iharm_M_unit;
+    io.mbh_solar = k ? o.kharma_mbh_solar : o.iharm_mbh_solar;
+    io.trat_small = k ? o.kharma_trat_small : o.iharm_trat_small;
+    io.trat_large = k ? o.kharma_trat_large : o.iharm_trat_large;
+    io.beta_crit = k ? o.kharma_beta_crit : o.iharm_beta_crit;
+    io.sigma_cut = k ? o.kharma_sigma_cut : o.iharm_sigma_cut;
+    io.sigma_cut_high = k ? o.kharma_sigma_cut_high : o.iharm_sigma_cut_high;
     io.emission_type = o.emission_type > 0 ? o.emission_type : KP_FIT_DEXTER;
-    io.interpolate_derived_scalars = o.iharm_interpolate_derived_scalars;
+    io.interpolate_derived_scalars =
+        k ? o.kharma_interpolate_derived_scalars : o.iharm_interpolate_derived_scalars;
     return io;
 }
 
@@ -944,6 +985,15 @@ inline void write_effective_parameters(const std::string& path, const ImageOptio
             << "\niharm_trat_large=" << o.iharm_trat_large << "\niharm_beta_crit=" << o.iharm_beta_crit
             << "\niharm_sigma_cut=" << o.iharm_sigma_cut << "\niharm_sigma_cut_high=" << o.iharm_sigma_cut_high
             << "\niharm_interpolate_derived_scalars=" << o.iharm_interpolate_derived_scalars << "\n";
+    } else if (o.model == "kharma") {
+        out << "kharma_dump=" << o.kharma_dump << "\nkharma_M_unit=" << o.kharma_M_unit
+            << "\nkharma_mbh_solar=" << o.kharma_mbh_solar << "\nkharma_trat_small=" << o.kharma_trat_small
+            << "\nkharma_trat_large=" << o.kharma_trat_large << "\nkharma_beta_crit=" << o.kharma_beta_crit
+            << "\nkharma_sigma_cut=" << o.kharma_sigma_cut << "\nkharma_sigma_cut_high=" << o.kharma_sigma_cut_high
+            << "\nkharma_interpolate_derived_scalars=" << o.kharma_interpolate_derived_scalars
+            << "\nkharma_reverse_field=" << o.kharma_reverse_field << "\n";
+    }
+    if (grmhd_model(o)) {
         const int fit = o.emission_type > 0 ? o.emission_type : KP_FIT_DEXTER;
         out << "emission_type=" << fit << "\nemission_fit=" << emission_fit_name(fit) << "\n";
     } else {

@@ -206,7 +206,7 @@ def test_both_refuse(exes, tmp_path, name, args, par):
 
 def test_unbuilt_requests_are_refused(exes):
     tool, _ = exes
-    for extra in (["--analysis_mode=1"], ["--slow_light=1"], ["--model=kharma"], ["--repeat_images=2"]):
+    for extra in (["--analysis_mode=1"], ["--slow_light=1"], ["--model=athenak"], ["--repeat_images=2"]):
         r = _run(tool, extra, ["--kp_print_resolved=1"])
         assert r.returncode != 0 and "not built" in r.stderr, (extra, r.stderr)
 
@@ -356,3 +356,31 @@ def test_iharm_runs_refuse_bad_input(exes, tmp_path, extra, msg):
     par.write_text(IHARM_PAR + "".join(f"{k}={v}\n" for k, v in extra.items()))
     r = _run(tool, [f"--parameter_file={par}", "--kp_print_resolved=1"])
     assert r.returncode != 0 and msg in r.stderr, r.stderr
+
+
+def test_kharma_runs_resolve_from_the_dump(exes, tmp_path):
+    """model=kharma: the .phdf dump's parameter text sets the spin and radii;
+    unprefixed GRMHD keys set both loaders' values, prefixed ones one."""
+    from kharma_dump import write_kharma_dump
+    from kpolaris_b200 import synthetic
+
+    tool, _ = exes
+    prims, model = synthetic.fm_torus(12, 8, 6, spin=0.3, seed=9)
+    dump = tmp_path / "dump.phdf"
+    write_kharma_dump(dump, prims, model)
+    par = tmp_path / "k.par"
+    par.write_text(IHARM_PAR.replace("model=iharm", "model=kharma").replace("iharm_mbh_solar", "kharma_mbh_solar")
+                   + f"phdf={dump}\nreverse_field=1\niharm_trat_small=3\n")
+    r = _run(tool, [f"--parameter_file={par}", "--kp_print_resolved=1"])
+    assert r.returncode == 0, r.stderr
+    res = _resolved(r.stdout)
+    horizon = 1.0 + math.sqrt(1.0 - 0.09)
+    assert float(res["spin"]) == 0.3
+    assert float(res["inner_radius"]) == max(model.r_in, horizon * 1.05)
+    out = tmp_path / "k.h5"
+    r = _run(tool, [f"--parameter_file={par}", f"--output={out}", "--kp_dry_run=1"])
+    assert r.returncode == 0, r.stderr
+    text = Path(str(out) + ".params").read_text()
+    assert f"kharma_dump={dump}" in text and "kharma_reverse_field=1" in text
+    assert "kharma_M_unit=2.0000000000000001e+26" in text and "kharma_trat_large=40" in text
+    assert "kharma_trat_small=1\n" in text  # iharm_trat_small set only the iharm value
