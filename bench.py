@@ -445,8 +445,11 @@ def reference_arm(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": mean_s * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (analytic RIAF plasma)",
-        "config": {**config_dict(args.n, "reference CPU (OpenMP dynamic over pixels)", len(freqs), 1, 1),
-                   "images_per_step": frac, "l2": "n/a (CPU)"},
+        # the workload of the GPU arm (its config); each step is a bounded
+        # sample of it, described in cpu_baseline.sample and reference_step
+        "config": config_dict(args.n, args.path, len(freqs), world, args.batch),
+        "reference_step": {"path": "reference CPU (OpenMP dynamic over pixels)", "image_fraction": frac,
+                           "l2": "n/a (CPU)"},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": CPU["cores"], "kind": kind, "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "step_s": {"min": min(step_s), "max": max(step_s)},
