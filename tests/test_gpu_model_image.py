@@ -244,6 +244,9 @@ evpa_0=N
     f = h5.read(out)
     assert f.attrs["model"] == "iharm" and f.attrs["nfreq"] == 5
     assert f.attrs["grmhd_n1"] == 48 and f.attrs["iharm_trat_large"] == 40.0 and f.attrs["emission_type"] == 4
+    # an iharm product carries no kharma_* metadata (docs/hdf5_schema.md:104-109)
+    for g in (f, f["parameters/radiation"], f["frame_0/freq_0"], f["frame_0/freq_4"]):
+        assert not [k for k in g.attrs if k.startswith("kharma_")], g.name
 
     params = synthetic.fmks_pass_a_params(model, 16, 12, xspan=20.0, outer_radius=50.0)
     opts = kp.default_iharm_options(M_unit=1e27, mbh_solar=6.5e9, trat_large=40.0, emission_type=_abi.FIT_DEXTER)

@@ -83,6 +83,22 @@ def test_schema_and_values(written):
     for g in ("header", "parameters/camera", "parameters/spacetime", "parameters/integration",
               "parameters/radiation", "grid", "results", "frame_0", "frame_0/diagnostics"):
         assert g in f, g
+    # root conventions the schema requires (docs/hdf5_schema.md:141-150)
+    for key in ("stokes_definition", "electric_field_phase_convention", "screen_handedness", "evpa_definition",
+                "camera_azimuth_convention", "sky_orientation", "image_pixel_order", "image_axis_geometry",
+                "output_stokes_transform"):
+        assert isinstance(f.attrs[key], str) and f.attrs[key], key
+    assert f.attrs["polarization_conventions_version"] == "2"
+    assert (f.attrs["image_array_order"], f.attrs["image_display_origin"]) == ("y,x", "lower")
+    # the flux scale is repeated at the root, /parameters/camera, /results and
+    # every frequency group (docs/hdf5_schema.md:159-167)
+    jy = f.attrs["intensity_to_flux_jy_per_pixel"]
+    for g in ("parameters/camera", "results", "frame_0/freq_0", "frame_0/freq_1"):
+        assert f[g].attrs["intensity_to_flux_jy_per_pixel"] == jy, g
+    assert f.attrs["flux_scale_valid"] == 1 and jy > 0
+    for fi in range(2):
+        g = f[f"frame_0/freq_{fi}"]
+        assert (g.attrs["stokes_convention"], g.attrs["polarization_basis"]) == ("camera_frame", "camera_screen")
     assert f["header"].attrs["schema"] == "kpolaris_image"
     assert f["header"].attrs["image_layout"] == "/frame_0/freq_i"
     assert np.array_equal(f["grid/frequency_hz"].value, freqs)
