@@ -279,8 +279,11 @@ int kp_measure_fma_peak(int device, int fp64, double* tflops);
  * RIAF image, one or several frequencies sharing one geodesic per pixel.
  * Replaces run_riaf_image (src/image/riaf.hpp:12-16, nfreq == 1) and
  * run_riaf_multifrequency_image (src/image/riaf.hpp:32-39, 1..4 frequencies
- * with step-control list == frequency list).  `frequencies` may be NULL
- * when nfreq == 1, in which case model->freq_cgs is used.
+ * with step-control list == frequency list).  params->coordinate_system is
+ * KP_COORD_BOYER_LINDQUIST (the reference's RIAF backend,
+ * src/image/backends/riaf_bl.cpp) or KP_COORD_CARTESIAN_KS; other charts
+ * return KP_ERR_UNSUPPORTED.  `frequencies` may be NULL when nfreq == 1, in
+ * which case model->freq_cgs is used.
  * radiation_substeps is accepted for signature compatibility; the
  * reference's segment kernels ignore it (pass_b.hpp:526, :1003).
  */
