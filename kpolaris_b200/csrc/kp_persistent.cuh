@@ -387,20 +387,19 @@ __device__ __forceinline__ void persistent_body(const WaveDesc& W) {
         // ------------------------------------------------------------ RK job
         const bool run = !park && (st.mode == kAStep || st.mode == kACrossHi || st.mode == kACrossTrial ||
                                    st.mode == kBStep || st.mode == kBCamCross);
-        // Mixed policy: FP32 contraction in the far phase only.  Inside the
-        // radiating sphere FP32 noise in the RHS reaches the step-doubling
-        // error estimate at the tolerance level and reshapes the accepted-step
-        // sequence the Faraday-thick transfer is sensitive to.
+        // Mixed policy: FP32 stage chains in the far phase only.  Inside the
+        // radiating sphere FP32 rounding in dk and de reaches the
+        // step-doubling error estimate and reshapes the accepted-step
+        // sequence the Faraday-thick transfer is sensitive to.  One RK call
+        // site: the crossing search's job differs only in kind and step.
         constexpr bool fp32 = P::kMixed && kFar;
         Ray next, mid;
         double err = 0.0;
         if (run) {
-            if (kCross && (st.mode == kACrossHi || st.mode == kACrossTrial)) {
-                const double hh = st.mode == kACrossHi ? st.full_h : st.full_h * st.trial;
-                rk_job<P, fp32, SC>(J->c.adaptive ? kRkRK4x2 : kRkRK4, J->c, S, hh, next, mid, err);
-            } else {
-                rk_job<P, fp32, SC>(st.rk_kind, J->c, S, st.h_try, next, mid, err);
-            }
+            const bool crossing = kCross && (st.mode == kACrossHi || st.mode == kACrossTrial);
+            const int kind = crossing ? (J->c.adaptive ? kRkRK4x2 : kRkRK4) : st.rk_kind;
+            const double hj = crossing ? (st.mode == kACrossHi ? st.full_h : st.full_h * st.trial) : st.h_try;
+            rk_job<P, fp32, SC>(kind, J->c, S, hj, next, mid, err);
             if (++lane_jobs > (1LL << 30)) {
                 st.reason = kInvalidState;
                 st.mode = kDone;
