@@ -27,6 +27,7 @@ from __future__ import annotations
 
 import argparse
 import ctypes as C
+import hashlib
 import json
 import os
 import statistics
@@ -1033,6 +1034,8 @@ def ours_arm(args):
 
 def grmhd_only(args):
     """Profiling entry: GRMHD images of the seeded torus, nothing else."""
+    import numpy as np
+
     import kpolaris_b200 as kp
     from kpolaris_b200 import _abi, synthetic
 
@@ -1045,8 +1048,11 @@ def grmhd_only(args):
         for _ in range(max(1, args.grmhd_steps)):
             t0 = time.perf_counter()
             r = kp.image_grmhd(params, g, [230e9], precision=prec)
+            dt = time.perf_counter() - t0
+            digest = hashlib.sha256(b"".join(np.ascontiguousarray(r.arrays[k]).tobytes()
+                                             for k in sorted(r.arrays))).hexdigest()[:16]
             print(f"grmhd {n1}x{n2}x{n3} {args.grmhd_n}^2 {args.grmhd_precision}: "
-                  f"{time.perf_counter() - t0:.3f} s, steps A {int(r.pass_a_steps.sum())} B {int(r.steps.sum())}",
+                  f"{dt:.3f} s, steps A {int(r.pass_a_steps.sum())} B {int(r.steps.sum())}, image {digest}",
                   flush=True)
     return 0
 
