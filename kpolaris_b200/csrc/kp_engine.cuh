@@ -27,7 +27,7 @@
 
 namespace kp {
 
-// One image (job) of a launch.
+// Kinds of RK job.
 enum RkKind : int { kRkSD = 0, kRkRK4 = 1, kRkRK4x2 = 2, kRkCK = 3 };
 
 // Control modes: what the pending RK job's result is for.
@@ -315,98 +315,134 @@ __device__ __forceinline__ void chain_base_f(const Ray& B, ChainF& b) {
     }
 }
 
-// One RK4 chain of step hc from B.  k1 holds the RHS of B when use_k1 is set,
-// and receives it when save_k1 is set.
-__device__ __forceinline__ void far_chain_f(const ImageConsts& c, const Ray& B, double hc, bool use_k1,
-                                            bool save_k1, float (&k1)[3][4], Ray& end) {
-    const float M = float(c.mass), a = float(c.spin);
-    ChainF b;
-    chain_base_f(B, b);
-    ChainF X = b;
-    D4 Xk = B.k;   // k of the stage input, FP64: the position derivative
+// State of one RK4 chain between its stages: the next stage input (FP32,
+// with its k in FP64 as the position derivative) and the accumulators.
+struct ChainAcc {
+    ChainF X;      // stage input
+    D4 Xk;         // k of the stage input, FP64: the position derivative
     D4 Ax;         // position accumulator, FP64
     float Aq[3][4];
-    const double hh = 0.5 * hc;
-#pragma unroll 1
-    for (int st = 0; st < 4; ++st) {
-        float kq[3][4];
-        if (st == 0 && use_k1) {
+};
+
+// Folds stage st's derivative kq into the chain of step hc from B (base b):
+// acc = ((k1 + 2 k2) + 2 k3) + k4, then the next stage input
+// B + cc * (this stage's derivative).
+__device__ __forceinline__ void chain_stage_f(ChainAcc& C, const ChainF& b, const Ray& B, double hc, int st,
+                                              const float (&kq)[3][4]) {
+    if (st == 0) {
+        C.Ax = C.Xk;
 #pragma unroll
-            for (int w = 0; w < 3; ++w)
+        for (int w = 0; w < 3; ++w)
 #pragma unroll
-                for (int i = 0; i < 4; ++i) kq[w][i] = k1[w][i];
-        } else {
-            ks_transport_factored<float>(M, a, X.x[0], X.x[1], X.x[2], X.q, kq);
-        }
-        if (st == 0 && save_k1) {
+            for (int i = 0; i < 4; ++i) C.Aq[w][i] = kq[w][i];
+    } else {
+        const double wd = st == 3 ? 1.0 : 2.0;
+        const float wf = st == 3 ? 1.0f : 2.0f;
 #pragma unroll
-            for (int w = 0; w < 3; ++w)
+        for (int i = 0; i < 4; ++i) C.Ax.v[i] = C.Ax.v[i] + C.Xk.v[i] * wd;
 #pragma unroll
-                for (int i = 0; i < 4; ++i) k1[w][i] = kq[w][i];
-        }
-        // acc = ((k1 + 2 k2) + 2 k3) + k4
-        if (st == 0) {
-            Ax = Xk;
+        for (int w = 0; w < 3; ++w)
 #pragma unroll
-            for (int w = 0; w < 3; ++w)
-#pragma unroll
-                for (int i = 0; i < 4; ++i) Aq[w][i] = kq[w][i];
-        } else {
-            const double wd = st == 3 ? 1.0 : 2.0;
-            const float wf = st == 3 ? 1.0f : 2.0f;
-#pragma unroll
-            for (int i = 0; i < 4; ++i) Ax.v[i] = Ax.v[i] + Xk.v[i] * wd;
-#pragma unroll
-            for (int w = 0; w < 3; ++w)
-#pragma unroll
-                for (int i = 0; i < 4; ++i) Aq[w][i] = Aq[w][i] + kq[w][i] * wf;
-        }
-        if (st < 3) {
-            // next stage input B + cc * (this stage's derivative)
-            const double cc = st < 2 ? hh : hc;
-            const float cf = float(cc);
-#pragma unroll
-            for (int i = 0; i < 3; ++i) X.x[i] = b.x[i] + X.q[0][i + 1] * cf;
-#pragma unroll
-            for (int i = 0; i < 4; ++i) Xk.v[i] = B.k.v[i] + double(kq[0][i]) * cc;
-#pragma unroll
-            for (int w = 0; w < 3; ++w)
-#pragma unroll
-                for (int i = 0; i < 4; ++i) X.q[w][i] = b.q[w][i] + kq[w][i] * cf;
-        }
+            for (int i = 0; i < 4; ++i) C.Aq[w][i] = C.Aq[w][i] + kq[w][i] * wf;
     }
-    const double h6 = hc / 6.0;
+    if (st < 3) {
+        const double cc = st < 2 ? 0.5 * hc : hc;
+        const float cf = float(cc);
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        end.x.v[i] = B.x.v[i] + Ax.v[i] * h6;
-        end.k.v[i] = B.k.v[i] + double(Aq[0][i]) * h6;
-        end.e1.v[i] = B.e1.v[i] + double(Aq[1][i]) * h6;
-        end.e2.v[i] = B.e2.v[i] + double(Aq[2][i]) * h6;
+        for (int i = 0; i < 3; ++i) C.X.x[i] = b.x[i] + C.X.q[0][i + 1] * cf;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) C.Xk.v[i] = B.k.v[i] + double(kq[0][i]) * cc;
+#pragma unroll
+        for (int w = 0; w < 3; ++w)
+#pragma unroll
+            for (int i = 0; i < 4; ++i) C.X.q[w][i] = b.q[w][i] + kq[w][i] * cf;
     }
 }
 
-// Step-doubling attempt (half, half, full reusing k1), RK4 step or composed
-// RK4 pair from far_chain_f; outputs as rk_job's.
+__device__ __forceinline__ void chain_end_f(const ChainAcc& C, const Ray& B, double hc, Ray& end) {
+    const double h6 = hc / 6.0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        end.x.v[i] = B.x.v[i] + C.Ax.v[i] * h6;
+        end.k.v[i] = B.k.v[i] + double(C.Aq[0][i]) * h6;
+        end.e1.v[i] = B.e1.v[i] + double(C.Aq[1][i]) * h6;
+        end.e2.v[i] = B.e2.v[i] + double(C.Aq[2][i]) * h6;
+    }
+}
+
+// One RK4 chain of step hc from B.
+__device__ __forceinline__ void far_chain_f(const ImageConsts& c, const Ray& B, double hc, Ray& end) {
+    const float M = float(c.mass), a = float(c.spin);
+    ChainF b;
+    chain_base_f(B, b);
+    ChainAcc C;
+    C.X = b;
+    C.Xk = B.k;
+#pragma unroll 1
+    for (int st = 0; st < 4; ++st) {
+        float kq[3][4];
+        ks_transport_factored<float>(M, a, C.X.x[0], C.X.x[1], C.X.x[2], C.X.q, kq);
+        chain_stage_f(C, b, B, hc, st, kq);
+    }
+    chain_end_f(C, B, hc, end);
+}
+
+// Step-doubling attempt from far_chain_f pieces.  The full-step chain starts
+// from S like the first half chain and reuses its first derivative, so the
+// two run interleaved, stage by stage: their contractions are independent,
+// which gives the scheduler two dependency chains per lane.  Then the
+// second half chain from the half-step state.  Each chain's arithmetic is
+// the sequential chain's (same operations in the same order).
+__device__ __forceinline__ void far_sd_f(const ImageConsts& c, const Ray& S, double h, Ray& next, Ray& mid,
+                                         double& err) {
+    const float M = float(c.mass), a = float(c.spin);
+    ChainF b;
+    chain_base_f(S, b);
+    const double hh = 0.5 * h;
+    ChainAcc H, F;
+    H.X = b;
+    H.Xk = S.k;
+    F.X = b;
+    F.Xk = S.k;
+    Ray full;
+    {
+        float kq[3][4];
+        ks_transport_factored<float>(M, a, b.x[0], b.x[1], b.x[2], b.q, kq);
+        chain_stage_f(H, b, S, hh, 0, kq);
+        chain_stage_f(F, b, S, h, 0, kq);
+    }
+#pragma unroll 1
+    for (int st = 1; st < 4; ++st) {
+        float kh[3][4], kf[3][4];
+        ks_transport_factored<float>(M, a, H.X.x[0], H.X.x[1], H.X.x[2], H.X.q, kh);
+        ks_transport_factored<float>(M, a, F.X.x[0], F.X.x[1], F.X.x[2], F.X.q, kf);
+        chain_stage_f(H, b, S, hh, st, kh);
+        chain_stage_f(F, b, S, h, st, kf);
+    }
+    chain_end_f(H, S, hh, mid);
+    chain_end_f(F, S, h, full);
+    far_chain_f(c, mid, hh, next);
+    err = control_error(full, next, max_val(c.tolerance, kTolFloor));
+}
+
+// Step-doubling attempt, RK4 step or composed RK4 pair from the FP32
+// chains; outputs as rk_job's.
 __device__ __forceinline__ void far_job_f(int kind, const ImageConsts& c, const Ray& S, double h, Ray& next,
                                           Ray& mid, double& err) {
-    float k1[3][4];
-    Ray R2;
-    const int nchain = kind == kRkRK4 ? 1 : (kind == kRkRK4x2 ? 2 : 3);
     err = 0.0;
-#pragma unroll 1
-    for (int ch = 0; ch < nchain; ++ch) {
-        const double hc = (kind == kRkRK4 || ch == 2) ? h : 0.5 * h;
-        Ray E;
-        far_chain_f(c, ch == 1 ? R2 : S, hc, ch == 2, ch == 0 && kind == kRkSD, k1, E);
-        if (ch == 0 && kind != kRkRK4) {
-            R2 = E;
-        } else if (ch < 2) {
-            next = E;
-        } else {
-            err = control_error(E, next, max_val(c.tolerance, kTolFloor));
-        }
+    if (kind == kRkSD) {
+        far_sd_f(c, S, h, next, mid, err);
+        return;
     }
-    mid = kind == kRkSD ? R2 : next;
+    if (kind == kRkRK4) {
+        far_chain_f(c, S, h, next);
+        mid = next;
+        return;
+    }
+    Ray R2;
+    far_chain_f(c, S, 0.5 * h, R2);
+    far_chain_f(c, R2, 0.5 * h, next);
+    mid = next;
 }
 
 // Step-doubling attempt, RK4 step or composed RK4 pair as a stage loop around

@@ -438,9 +438,10 @@ inline const KeyTable& key_table() {
     return table;
 }
 
-// Options of subsystems this library does not build.  Their values do not
-// enter a RIAF image; the requests that would (analysis_mode, slow_light,
-// slow_light_time_probe, repeat_images) are table entries above.
+// Options this library does not use: loader settings beyond the table's
+// iharm/KHARMA entries, the other loaders, and subsystems not built here.
+// Their values enter no image; the requests that would (analysis_mode,
+// slow_light, slow_light_time_probe, repeat_images) are table entries above.
 inline bool inert_key(const std::string& key) {
     static const char* const prefixes[] = {"iharm_", "kharma_", "athenak_", "bhac_", "hamr_", "torus_",
                                            "binary_", "slow_light_", "slowlight_", "analysis_", "formation_",
