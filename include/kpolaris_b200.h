@@ -262,7 +262,7 @@ int kp_abi_version(void);
  * 0 kp_camera_params, 1 kp_emission_selection, 2 kp_pass_a_params,
  * 3 kp_riaf_model, 4 kp_image_out, 5 kp_run_options, 7 kp_riaf_job,
  * 8 kp_batch_stats, 9 kp_tuning, 10 kp_grmhd_model, 11 kp_grmhd_job, 12 kp_analysis_config,
- * 13 kp_analysis_out, 14 kp_iharm_options; 6 is the bytes of the per-image job descriptor an
+ * 13 kp_analysis_out, 14 kp_iharm_options, 15 kp_response_config; 6 is the bytes of the per-image job descriptor an
  * image uploads to the device; 0 for other ids. */
 size_t kp_abi_sizeof(int which);
 
@@ -404,6 +404,89 @@ typedef struct kp_analysis_out {
 int kp_image_riaf_analysis(const kp_pass_a_params* params, const kp_riaf_model* model, int radiation_substeps,
                            const kp_analysis_config* config, const kp_run_options* options, kp_image_out* out,
                            kp_analysis_out* analysis);
+
+/*
+ * Source-partition response channels of analysis mode (ResponseConfig,
+ * src/diagnostics/response_config.hpp:10-33; the accumulation of
+ * src/diagnostics/response.hpp).  `partition` tags every radiating sample
+ * with a source bin.  Each bin has a channel: the Stokes vector its own
+ * emission contributes at the camera.  With a response `parameter`, four
+ * derivative channels per bin follow (dS/dq through the emission,
+ * absorption, Faraday-rotation and Faraday-conversion coefficients of the
+ * samples in the bin: mechanism m, bin k is channel bins + m * bins + k),
+ * then four full-transfer reruns with the whole plasma at q = +h, -h,
+ * +h/2, -h/2 (channels 5 * bins + 0..3).  q is the logarithmic scale of the
+ * density (n_e, with B as sqrt(n_e)), the electron temperature, the
+ * magnetic field, or of every coefficient at once.
+ *
+ * Bins per partition, which the entry point checks: radial: `bins` bins
+ * between edges[0..bins] (edge_count = bins + 1, increasing), a sample
+ * below edges[1] in bin 0 and one at or above edges[bins - 1] in the last;
+ * region: 6 (funnel, disk, equatorial band by polar angle from the nearer
+ * spin axis, each split into the observer's near and far side); near_far:
+ * 2; plasma_region: 4 (sigma above its boundary, beta below its boundary,
+ * the rest, and samples without a magnetisation, always the last bin for
+ * the RIAF plasma); thetae / sigma / beta / ne_cgs / b_cgs: edge_count
+ * increasing positive edges and bins = edge_count + 2 (below the first
+ * edge, between edges, above the last, then unavailable).
+ */
+#define KP_MAX_PARTITION_EDGES 61
+
+typedef enum kp_response_parameter {
+    KP_RESPONSE_NONE = 0,
+    KP_RESPONSE_DENSITY_SCALE = 1,
+    KP_RESPONSE_TEMPERATURE_SCALE = 2,
+    KP_RESPONSE_MAGNETIC_SCALE = 3,
+    KP_RESPONSE_COEFFICIENTS = 4
+} kp_response_parameter;
+
+typedef enum kp_source_partition {
+    KP_PARTITION_NONE = 0,
+    KP_PARTITION_RADIAL = 1,
+    KP_PARTITION_REGION = 2,
+    KP_PARTITION_PLASMA_REGION = 3,
+    KP_PARTITION_NEAR_FAR = 4,
+    KP_PARTITION_THETAE = 5,
+    KP_PARTITION_SIGMA = 6,
+    KP_PARTITION_BETA = 7,
+    KP_PARTITION_NE_CGS = 8,
+    KP_PARTITION_B_CGS = 9
+} kp_source_partition;
+
+typedef struct kp_response_config {
+    int parameter;            /* kp_response_parameter */
+    int partition;            /* kp_source_partition; NONE with a parameter is refused */
+    double step;              /* h, in [1e-6, 0.1] when a parameter is set (1e-3) */
+    int bins;
+    int edge_count;
+    double edges[KP_MAX_PARTITION_EDGES];
+    double funnel_angle;      /* region: radians from either spin axis (20 deg) */
+    double disk_angle;        /* region: radians from either spin axis (60 deg) */
+    double sigma_boundary;    /* plasma_region (1) */
+    double beta_boundary;     /* plasma_region (1) */
+    double observer_theta;    /* region / near_far: the observer's direction, radians */
+    double observer_phi;
+} kp_response_config;
+
+/* The struct's default member initialisers (no partition, no parameter). */
+void kp_default_response_config(kp_response_config* config);
+
+/* Channels of a configuration: bins * (parameter ? 5 : 1) + (parameter ? 4 : 0),
+ * 0 without a partition; negative (and kp_last_error) when the configuration
+ * is invalid. */
+int kp_response_channels(const kp_response_config* config);
+
+/*
+ * kp_image_riaf_analysis with source-partition response channels.
+ * `response` takes 4 * channels * npix doubles, channel-major, then I, Q, U,
+ * V, then pixel: response[(4 * channel + s) * npix + pixel]; each channel in
+ * the observer basis, like the image.  Host or device memory as
+ * options->outputs_on_device says; NULL only when channels is 0.
+ */
+int kp_image_riaf_analysis_response(const kp_pass_a_params* params, const kp_riaf_model* model,
+                                    int radiation_substeps, const kp_analysis_config* config,
+                                    const kp_response_config* response_config, const kp_run_options* options,
+                                    kp_image_out* out, kp_analysis_out* analysis, double* response);
 
 /* One image of a batch: the arguments of one kp_image_riaf call. */
 typedef struct kp_riaf_job {

@@ -102,6 +102,12 @@ def library() -> C.CDLL:
     L.kp_image_riaf_analysis.argtypes = [C.POINTER(PassAParams), C.POINTER(RIAFModel), C.c_int,
                                          C.POINTER(_abi.AnalysisConfig), C.POINTER(RunOptions),
                                          C.POINTER(_abi.ImageOut), C.POINTER(_abi.AnalysisOut)]
+    L.kp_image_riaf_analysis_response.argtypes = [
+        C.POINTER(PassAParams), C.POINTER(RIAFModel), C.c_int, C.POINTER(_abi.AnalysisConfig),
+        C.POINTER(_abi.ResponseConfig), C.POINTER(RunOptions), C.POINTER(_abi.ImageOut), C.POINTER(_abi.AnalysisOut),
+        C.POINTER(C.c_double)]
+    L.kp_response_channels.argtypes = [C.POINTER(_abi.ResponseConfig)]
+    L.kp_default_response_config.argtypes = [C.POINTER(_abi.ResponseConfig)]
     L.kp_server_create.argtypes = [C.POINTER(_abi.ServerConfig), C.POINTER(C.c_void_p)]
     L.kp_server_submit.argtypes = [C.c_void_p, C.POINTER(_abi.RiafJob), C.POINTER(C.c_ulonglong)]
     L.kp_server_submit_grmhd.argtypes = [C.c_void_p, C.POINTER(_abi.GrmhdJob), C.POINTER(C.c_ulonglong)]
@@ -228,6 +234,31 @@ def image_riaf_analysis(params: PassAParams, model: RIAFModel, config: _abi.Anal
     check(L.kp_image_riaf_analysis(C.byref(params), C.byref(model), int(radiation_substeps), C.byref(config),
                                    C.byref(opt), C.byref(s), C.byref(a)))
     return out, an
+
+
+def image_riaf_analysis_response(params: PassAParams, model: RIAFModel, config: _abi.AnalysisConfig | None,
+                                 response: _abi.ResponseConfig, *, radiation_substeps=1, **options):
+    """kp_image_riaf_analysis_response: image_riaf_analysis with the
+    source-partition response channels of `response` (see
+    _abi.make_response_config).  Returns (ImageHostData, AnalysisHostData,
+    channels) with channels shaped [channel, 4 (I, Q, U, V), npix] in the
+    observer basis."""
+    L = library()
+    if config is None:
+        config = _abi.default_analysis_config()
+    nch = int(L.kp_response_channels(C.byref(response)))
+    if nch < 0:
+        check(nch)
+    npix = params.camera.nx * params.camera.ny
+    out = ImageHostData.allocate(npix, 1)
+    an = _abi.AnalysisHostData.allocate(npix, int(config.radial_bins))
+    channels = np.zeros((max(nch, 1), 4, npix), dtype=np.float64)
+    s, a = out.as_struct(), an.as_struct()
+    opt = _options(**options)
+    check(L.kp_image_riaf_analysis_response(C.byref(params), C.byref(model), int(radiation_substeps),
+                                            C.byref(config), C.byref(response), C.byref(opt), C.byref(s),
+                                            C.byref(a), channels.ctypes.data_as(C.POINTER(C.c_double))))
+    return out, an, channels[:nch]
 
 
 def flux_scale_jy_per_pixel(mbh_solar: float, dsource_pc: float, image_width_x: float, image_width_y: float,

@@ -305,6 +305,110 @@ def default_analysis_config(radial_bins: int = 16, radial_min: float = 2.0, radi
     return AnalysisConfig(int(radial_bins), float(radial_min), float(radial_max), float(formation_fraction))
 
 
+# Source-partition response channels (kp_response_config;
+# src/diagnostics/response_config.hpp:10-33)
+KP_MAX_PARTITION_EDGES = 61
+RESPONSE_PARAMETERS = {"none": 0, "density_scale": 1, "temperature_scale": 2, "magnetic_scale": 3,
+                       "coefficients": 4}
+SOURCE_PARTITIONS = {"none": 0, "radial": 1, "region": 2, "plasma_region": 3, "near_far": 4, "thetae": 5,
+                     "sigma": 6, "beta": 7, "ne_cgs": 8, "b_cgs": 9}
+
+
+class ResponseConfig(C.Structure):
+    _fields_ = [
+        ("parameter", C.c_int), ("partition", C.c_int), ("step", C.c_double), ("bins", C.c_int),
+        ("edge_count", C.c_int), ("edges", C.c_double * KP_MAX_PARTITION_EDGES),
+        ("funnel_angle", C.c_double), ("disk_angle", C.c_double),
+        ("sigma_boundary", C.c_double), ("beta_boundary", C.c_double),
+        ("observer_theta", C.c_double), ("observer_phi", C.c_double),
+    ]
+
+
+def default_response_config() -> ResponseConfig:
+    r = ResponseConfig()
+    r.step = 1e-3
+    r.funnel_angle = 0.3490658503988659
+    r.disk_angle = 1.0471975511965976
+    r.sigma_boundary = 1.0
+    r.beta_boundary = 1.0
+    return r
+
+
+def response_channels(r: ResponseConfig) -> int:
+    """ResponseConfig::channels (response_config.hpp:29)."""
+    if r.partition == 0:
+        return 0
+    resp = r.parameter != 0
+    return int(r.bins) * (5 if resp else 1) + (4 if resp else 0)
+
+
+_PARTITION_EDGES = {"thetae": "1,3,10,30,100", "sigma": "0.01,0.1,1,10,100", "beta": "0.01,0.1,1,10,100",
+                    "ne_cgs": "100,1000,10000,100000,1000000,10000000", "b_cgs": "0.1,1,10,100,1000"}
+
+
+def make_response_config(response: str = "none", partition: str = "none", *, step: float = 1e-3,
+                         radial_bins: int = 16, radial_min: float = 2.0, radial_max: float = 100.0,
+                         edges: str = "", funnel_angle_deg: float = 20.0, disk_angle_deg: float = 60.0,
+                         sigma_boundary: float = 1.0, beta_boundary: float = 1.0,
+                         inclination: float = 0.0) -> ResponseConfig:
+    """The response configuration the image tool builds from its
+    analysis_response / analysis_partition options and the analysis radial
+    bins (make_response_config, tools/kpolaris_response_options.hpp:10-82):
+    a response without a partition is radial; radial partitions take the
+    analysis bins' logarithmic edges; scalar partitions take `edges` (or the
+    tool's defaults) with underflow, overflow and unavailable bins;
+    `inclination` is the camera's, in radians."""
+    if response not in RESPONSE_PARAMETERS:
+        raise ValueError("analysis_response must be none, density_scale, temperature_scale, magnetic_scale, "
+                         "or coefficients")
+    if partition == "none" and response != "none":
+        partition = "radial"
+    if partition not in SOURCE_PARTITIONS:
+        raise ValueError("unknown analysis_partition")
+    r = default_response_config()
+    r.parameter = RESPONSE_PARAMETERS[response]
+    r.partition = SOURCE_PARTITIONS[partition]
+    r.step = float(step)
+    if not (math.isfinite(r.step) and 1e-6 <= r.step <= 0.1):
+        raise ValueError("analysis_response_step must be finite and in [1e-6,0.1]")
+    rad = math.pi / 180.0
+    r.funnel_angle = funnel_angle_deg * rad
+    r.disk_angle = disk_angle_deg * rad
+    if not (0.0 < r.funnel_angle < r.disk_angle < 0.5 * math.pi):
+        raise ValueError("analysis region angles must satisfy 0 < funnel < disk < 90 degrees")
+    r.sigma_boundary, r.beta_boundary = float(sigma_boundary), float(beta_boundary)
+    if not (sigma_boundary > 0 and beta_boundary > 0):
+        raise ValueError("analysis sigma/beta boundaries must be finite and positive")
+    r.observer_theta = float(inclination)
+    if partition == "radial":
+        if radial_bins + 1 > KP_MAX_PARTITION_EDGES:
+            raise ValueError("too many response radial bins")
+        r.bins, r.edge_count = int(radial_bins), int(radial_bins) + 1
+        for k in range(radial_bins + 1):
+            r.edges[k] = math.exp(math.log(radial_min) + k / radial_bins * math.log(radial_max / radial_min))
+    elif partition == "region":
+        r.bins = 6
+    elif partition == "plasma_region":
+        r.bins = 4
+    elif partition == "near_far":
+        r.bins = 2
+    elif partition != "none":
+        text = edges or _PARTITION_EDGES[partition]
+        values = [float(t) for t in text.split(",")]
+        if (not values or len(values) > KP_MAX_PARTITION_EDGES or
+                any(not (math.isfinite(v) and v > 0) for v in values) or
+                any(b <= a for a, b in zip(values, values[1:]))):
+            raise ValueError("analysis_partition_edges must be finite, positive, strictly increasing "
+                             "(at most 61 edges)")
+        for i, v in enumerate(values):
+            r.edges[i] = v
+        r.edge_count = len(values)
+        r.bins = len(values) + 2
+    if edges and r.partition < SOURCE_PARTITIONS["thetae"]:
+        raise ValueError("analysis_partition_edges applies only to scalar plasma partitions")
+    return r
+
+
 # kp_analysis_out, in order: per-pixel scalars, then the bin-major radial
 # arrays, then the observer-weighted results (src/image/result.hpp:35-92)
 ANALYSIS_SCALARS_A = ["radiating_path_length", "emission_weight", "emission_weighted_radius",

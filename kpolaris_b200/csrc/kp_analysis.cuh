@@ -17,8 +17,9 @@
 // (trace_pass_b_segment_model_endpoint_analysis_pixel_metric, :409-621),
 // single frequency; it differs from the imaging loop in two places: a
 // rejected attempt at the minimum step ends the ray as max_steps, and a
-// sample radiates when r >= inner_radius.  The source-partition response
-// channels (analysis_response) are not built.
+// sample radiates when r >= inner_radius.  With a kp_response_config, the
+// source-partition response channels (src/diagnostics/response.hpp) are
+// accumulated per radiating sample in global memory.
 #pragma once
 
 #include "kp_launch.h"
@@ -272,10 +273,191 @@ __device__ __forceinline__ ObserverAnalysis observer_analysis(const AnalysisAcc&
     return o;
 }
 
+// ------------------------------------------------ source-partition responses
+// Channel c of pixel p: four Stokes components at (4 c + s) npix + p
+// (response_read / response_write, response.hpp:12-24).
+__device__ __forceinline__ Stokes4<double> resp_read(const double* d, int pixel, int npix, int ch) {
+    const size_t base = size_t(4) * size_t(ch) * size_t(npix) + size_t(pixel);
+    return Stokes4<double>{d[base], d[base + npix], d[base + 2 * size_t(npix)], d[base + 3 * size_t(npix)]};
+}
+
+__device__ __forceinline__ void resp_write(double* d, int pixel, int npix, int ch, const Stokes4<double>& s) {
+    const size_t base = size_t(4) * size_t(ch) * size_t(npix) + size_t(pixel);
+    d[base] = s.I;
+    d[base + npix] = s.Q;
+    d[base + 2 * size_t(npix)] = s.U;
+    d[base + 3 * size_t(npix)] = s.V;
+}
+
+__device__ __forceinline__ Stokes4<double> resp_add(const Stokes4<double>& a, const Stokes4<double>& b) {
+    return Stokes4<double>{a.I + b.I, a.Q + b.Q, a.U + b.U, a.V + b.V};
+}
+
+// The transfer step as a linear map: its columns are the unit Stokes vectors
+// stepped without emission (ResponseStepMatrix, response.hpp:37-55).
+struct RespStepMatrix {
+    Stokes4<double> col[4];
+};
+
+__device__ __forceinline__ RespStepMatrix resp_step_matrix(Coeffs<double> co, double dl) {
+    co.jI = co.jQ = co.jU = co.jV = 0.0;
+    RespStepMatrix m;
+    for (int k = 0; k < 4; ++k) {
+        m.col[k] = Stokes4<double>{k == 0 ? 1.0 : 0.0, k == 1 ? 1.0 : 0.0, k == 2 ? 1.0 : 0.0, k == 3 ? 1.0 : 0.0};
+        stokes_step(m.col[k], co, dl);
+    }
+    return m;
+}
+
+__device__ __forceinline__ Stokes4<double> resp_apply(const RespStepMatrix& m, const Stokes4<double>& s) {
+    const Stokes4<double>* c = m.col;
+    return Stokes4<double>{c[0].I * s.I + c[1].I * s.Q + c[2].I * s.U + c[3].I * s.V,
+                           c[0].Q * s.I + c[1].Q * s.Q + c[2].Q * s.U + c[3].Q * s.V,
+                           c[0].U * s.I + c[1].U * s.Q + c[2].U * s.U + c[3].U * s.V,
+                           c[0].V * s.I + c[1].V * s.Q + c[2].V * s.U + c[3].V * s.V};
+}
+
+// response_replace_block (response.hpp:57-70): mechanism 0 emission, 1
+// absorption, 2 Faraday rotation, 3 Faraday conversion.
+__device__ __forceinline__ Coeffs<double> resp_replace(Coeffs<double> b, const Coeffs<double>& v, int m) {
+    if (m == 0) {
+        b.jI = v.jI; b.jQ = v.jQ; b.jU = v.jU; b.jV = v.jV;
+    } else if (m == 1) {
+        b.aI = v.aI; b.aQ = v.aQ; b.aU = v.aU; b.aV = v.aV;
+    } else if (m == 2) {
+        b.rV = v.rV;
+    } else {
+        b.rQ = v.rQ; b.rU = v.rU;
+    }
+    return b;
+}
+
+// Source bin of a sample (response_partition_bin, response.hpp:79-111) for
+// the RIAF plasma, whose magnetisation is undefined (src/diagnostics/
+// plasma.hpp:22-44).
+__device__ __forceinline__ int resp_partition_bin(const kp_response_config& R, const ImageConsts& c,
+                                                  const BlCoords& q) {
+    const double r = q.rc, theta = q.th;
+    if (R.partition == KP_PARTITION_RADIAL) {
+        int bin = 0;
+        while (bin < R.bins - 1 && r >= R.edges[bin + 1]) ++bin;
+        return bin;
+    }
+    if (R.partition == KP_PARTITION_REGION || R.partition == KP_PARTITION_NEAR_FAR) {
+        const double sight_dot =
+            sin(theta) * sin(R.observer_theta) * (q.cphi * cos(R.observer_phi) + q.sphi * sin(R.observer_phi)) +
+            cos(theta) * cos(R.observer_theta);
+        const int side = sight_dot >= 0.0 ? 0 : 1;
+        if (R.partition == KP_PARTITION_NEAR_FAR) return side;
+        const double polar = min_val(theta, 3.14159265358979323846 - theta);
+        const int region = polar < R.funnel_angle ? 0 : (polar < R.disk_angle ? 1 : 2);
+        return 2 * region + side;
+    }
+    if (R.partition == KP_PARTITION_PLASMA_REGION) return 3;
+    if (R.partition == KP_PARTITION_SIGMA || R.partition == KP_PARTITION_BETA) return R.bins - 1;
+    double r_bl, ne = 0.0, thetae = 0.0, b = 0.0;
+    const int valid = riaf_plasma(c, q, r_bl, ne, thetae, b) && ne > 0.0 && thetae > 0.0 && b > 0.0;
+    if (!valid) return R.bins - 1;
+    double value = thetae;
+    if (R.partition == KP_PARTITION_NE_CGS) value = ne;
+    if (R.partition == KP_PARTITION_B_CGS) value = b;
+    int bin = 0;
+    while (bin < R.edge_count && value >= R.edges[bin]) ++bin;
+    return bin;
+}
+
+// The coefficients at the sample with the plasma scaled by e^q
+// (PlasmaPerturbation::apply, src/radiation/plasma_perturbation.hpp:14-31,
+// inside RIAFAnalyticRadiationModel::coefficients, riaf.hpp:428-432), or
+// every coefficient scaled by e^q (response_scale_coefficients,
+// response.hpp:72-78).
+__device__ __forceinline__ Coeffs<double> resp_variant(const ImageConsts& c, const kp_response_config& R,
+                                                       const RiafSample& p, const Coeffs<double>& base, double q) {
+    if (R.parameter == KP_RESPONSE_COEFFICIENTS) {
+        const double f = exp(q);
+        Coeffs<double> o = base;
+        o.jI *= f; o.jQ *= f; o.jU *= f; o.jV *= f;
+        o.aI *= f; o.aQ *= f; o.aU *= f; o.aV *= f;
+        o.rQ *= f; o.rU *= f; o.rV *= f;
+        return o;
+    }
+    RiafSample v = p;
+    if (q != 0.0) {
+        const double f = exp(q);
+        if (R.parameter == KP_RESPONSE_DENSITY_SCALE) {
+            v.ne *= f;
+            v.b *= exp(q * 0.5);
+        } else if (R.parameter == KP_RESPONSE_TEMPERATURE_SCALE) {
+            v.thetae *= f;
+        } else if (R.parameter == KP_RESPONSE_MAGNETIC_SCALE) {
+            v.b *= f;
+        }
+    }
+    Coeffs<double> o = riaf_coefficients(c, v, c.freq[0]);
+    if (!c.faraday_rotation) o.rV = 0.0;
+    return o;
+}
+
+// accumulate_response_sample + response_transfer_step (response.hpp:117-
+// 184): `incoming` is the pixel's Stokes vector before this step, `base`
+// the step's coefficients, `p` the plasma sample they came from.
+__device__ __noinline__ void response_sample(const ImageConsts& c, const kp_response_config& R, const Ray& sample,
+                                             const RiafSample& p, const Stokes4<double>& incoming,
+                                             const Coeffs<double>& base, double dl, double* data, int pixel,
+                                             int npix) {
+    const BlCoords q = riaf_bl_coords(c.spin, sample.x);
+    const int bin = resp_partition_bin(R, c, q);
+    const bool responses = R.parameter != KP_RESPONSE_NONE;
+    Coeffs<double> variants[4];
+    if (responses) {
+        for (int v = 0; v < 4; ++v) {
+            const double qv = R.step * (v % 2 == 0 ? 1.0 : -1.0) * (v < 2 ? 1.0 : 0.5);
+            variants[v] = resp_variant(c, R, p, base, qv);
+        }
+    }
+    const RespStepMatrix m = resp_step_matrix(base, dl);
+    Stokes4<double> emitted{0.0, 0.0, 0.0, 0.0};
+    stokes_step(emitted, base, dl);
+    for (int k = 0; k < R.bins; ++k) {
+        Stokes4<double> s = resp_apply(m, resp_read(data, pixel, npix, k));
+        if (k == bin) s = resp_add(s, emitted);
+        resp_write(data, pixel, npix, k, s);
+    }
+    if (!responses) return;
+    const double denom = 2.0 * R.step;
+    for (int mech = 0; mech < 4; ++mech) {
+        Stokes4<double> plus = incoming, minus = incoming;
+        stokes_step(plus, resp_replace(base, variants[0], mech), dl);
+        stokes_step(minus, resp_replace(base, variants[1], mech), dl);
+        const Stokes4<double> forcing{(plus.I - minus.I) / denom, (plus.Q - minus.Q) / denom,
+                                      (plus.U - minus.U) / denom, (plus.V - minus.V) / denom};
+        for (int k = 0; k < R.bins; ++k) {
+            const int ch = R.bins + mech * R.bins + k;
+            Stokes4<double> s = resp_apply(m, resp_read(data, pixel, npix, ch));
+            if (k == bin) s = resp_add(s, forcing);
+            resp_write(data, pixel, npix, ch, s);
+        }
+    }
+    for (int v = 0; v < 4; ++v) {
+        const int ch = 5 * R.bins + v;
+        Stokes4<double> s = resp_read(data, pixel, npix, ch);
+        stokes_step(s, variants[v], dl);
+        resp_write(data, pixel, npix, ch, s);
+    }
+}
+
+// Channels of a configuration (ResponseConfig::channels, response_config.hpp:29).
+KP_HD int response_channel_count(const kp_response_config& R) {
+    if (R.partition == KP_PARTITION_NONE) return 0;
+    const bool responses = R.parameter != KP_RESPONSE_NONE;
+    return R.bins * (responses ? 5 : 1) + (responses ? 4 : 0);
+}
+
 // The analysis driver's pass B, one frequency (:444-611).
 __device__ __forceinline__ void trace_pass_b_analysis(const ImageConsts& c, const AnalysisConsts& k, Ray& state,
                                                       Stokes4<double>& stokes, int& steps, int& reason,
-                                                      AnalysisAcc& a) {
+                                                      AnalysisAcc& a, const kp_response_config* resp = nullptr,
+                                                      double* resp_data = nullptr, int pixel = 0, int npix = 0) {
     const double mass = c.mass, spin = c.spin;
     StepControl ctl;
     ctl.tolerance = c.tolerance;
@@ -351,8 +533,11 @@ __device__ __forceinline__ void trace_pass_b_analysis(const ImageConsts& c, cons
         const double next_r = ks_radius(spin, next.x);
         const int active = sample_r >= c.inner_radius && sample_r < c.outer_radius;
         Coeffs<double> co = {};
+        RiafSample ps;
+        ps.emitting = 0;
         if (active) {
-            co = riaf_coefficients(c, riaf_sample(c, sample), c.freq[0]);
+            ps = riaf_sample(c, sample);
+            co = riaf_coefficients(c, ps, c.freq[0]);
             if (!c.faraday_rotation) co.rV = 0.0;
         }
         const double local_max_rs =
@@ -383,6 +568,7 @@ __device__ __forceinline__ void trace_pass_b_analysis(const ImageConsts& c, cons
                 analysis_sample(c, sample, co, dlambda, r, bin, a);
                 Coeffs<double> propagation = co;
                 propagation.jI = propagation.jQ = propagation.jU = propagation.jV = 0.0;
+                if (resp) response_sample(c, *resp, sample, ps, stokes, co, dlambda, resp_data, pixel, npix);
 #pragma unroll 1
                 for (int b = 0; b < k.radial_bins; ++b) stokes_step(a.radial[b], b == bin ? co : propagation, dlambda);
                 a.substeps += 1;

@@ -818,6 +818,7 @@ size_t kp_abi_sizeof(int which) {
     case 12: return sizeof(kp_analysis_config);
     case 13: return sizeof(kp_analysis_out);
     case 14: return sizeof(kp_iharm_options);
+    case 15: return sizeof(kp_response_config);
     default: return 0;
     }
 }
@@ -1003,10 +1004,107 @@ void kp_default_analysis_config(kp_analysis_config* cfg) {
     cfg->formation_fraction = 0.9;
 }
 
+// Checks a response configuration against the bins each partition needs
+// (make_response_config, tools/kpolaris_response_options.hpp:10-82, whose
+// tool-level checks a caller of the C ABI bypasses); returns the channel
+// count or a negative status.
+static int validate_response(const kp_response_config* r) {
+    if (!r) return set_error(KP_ERR_INVALID, "null response configuration");
+    if (r->parameter < KP_RESPONSE_NONE || r->parameter > KP_RESPONSE_COEFFICIENTS)
+        return set_error(KP_ERR_INVALID, "unknown response parameter %d", r->parameter);
+    if (r->partition < KP_PARTITION_NONE || r->partition > KP_PARTITION_B_CGS)
+        return set_error(KP_ERR_INVALID, "unknown source partition %d", r->partition);
+    if (r->partition == KP_PARTITION_NONE) {
+        if (r->parameter != KP_RESPONSE_NONE)
+            return set_error(KP_ERR_INVALID, "a response parameter needs a source partition");
+        return 0;
+    }
+    if (r->parameter != KP_RESPONSE_NONE && !(std::isfinite(r->step) && r->step >= 1e-6 && r->step <= 0.1))
+        return set_error(KP_ERR_INVALID, "analysis_response_step must be finite and in [1e-6,0.1]");
+    const double half_pi = 0.5 * 3.14159265358979323846;
+    if (r->partition == KP_PARTITION_REGION &&
+        !(std::isfinite(r->funnel_angle) && std::isfinite(r->disk_angle) && r->funnel_angle > 0.0 &&
+          r->funnel_angle < r->disk_angle && r->disk_angle < half_pi))
+        return set_error(KP_ERR_INVALID, "analysis region angles must satisfy 0 < funnel < disk < 90 degrees");
+    if ((r->partition == KP_PARTITION_REGION || r->partition == KP_PARTITION_NEAR_FAR) &&
+        !(std::isfinite(r->observer_theta) && std::isfinite(r->observer_phi)))
+        return set_error(KP_ERR_INVALID, "the observer direction must be finite");
+    if (r->partition == KP_PARTITION_PLASMA_REGION &&
+        !(std::isfinite(r->sigma_boundary) && std::isfinite(r->beta_boundary) && r->sigma_boundary > 0.0 &&
+          r->beta_boundary > 0.0))
+        return set_error(KP_ERR_INVALID, "analysis sigma/beta boundaries must be finite and positive");
+    auto increasing = [&](int n) {
+        for (int i = 0; i < n; ++i) {
+            if (!(std::isfinite(r->edges[i]) && r->edges[i] > 0.0)) return false;
+            if (i > 0 && !(r->edges[i] > r->edges[i - 1])) return false;
+        }
+        return true;
+    };
+    int want = 0;
+    switch (r->partition) {
+    case KP_PARTITION_RADIAL:
+        if (r->bins < 1 || r->bins + 1 > KP_MAX_PARTITION_EDGES || r->edge_count != r->bins + 1 ||
+            !increasing(r->edge_count))
+            return set_error(KP_ERR_INVALID,
+                             "radial partition: bins in [1, %d], edge_count = bins + 1 increasing positive edges",
+                             KP_MAX_PARTITION_EDGES - 1);
+        want = r->bins;
+        break;
+    case KP_PARTITION_REGION: want = 6; break;
+    case KP_PARTITION_PLASMA_REGION: want = 4; break;
+    case KP_PARTITION_NEAR_FAR: want = 2; break;
+    default:
+        if (r->edge_count < 1 || r->edge_count > KP_MAX_PARTITION_EDGES || !increasing(r->edge_count))
+            return set_error(KP_ERR_INVALID,
+                             "analysis_partition_edges must be finite, positive, strictly increasing "
+                             "(at most %d edges)", KP_MAX_PARTITION_EDGES);
+        want = r->edge_count + 2;
+        break;
+    }
+    if (r->bins != want)
+        return set_error(KP_ERR_INVALID, "partition %d needs bins = %d, got %d", r->partition, want, r->bins);
+    const bool responses = r->parameter != KP_RESPONSE_NONE;
+    return r->bins * (responses ? 5 : 1) + (responses ? 4 : 0);
+}
+
+static int analysis_impl(const kp_pass_a_params* params, const kp_riaf_model* model,
+                         const kp_analysis_config* config, const kp_response_config* resp_cfg,
+                         const kp_run_options* options, kp_image_out* out, kp_analysis_out* analysis,
+                         double* response);
+
 int kp_image_riaf_analysis(const kp_pass_a_params* params, const kp_riaf_model* model, int radiation_substeps,
                            const kp_analysis_config* config, const kp_run_options* options, kp_image_out* out,
                            kp_analysis_out* analysis) {
     (void)radiation_substeps;
+    return analysis_impl(params, model, config, nullptr, options, out, analysis, nullptr);
+}
+
+void kp_default_response_config(kp_response_config* r) {
+    if (!r) return;
+    std::memset(r, 0, sizeof(*r));
+    r->parameter = KP_RESPONSE_NONE;
+    r->partition = KP_PARTITION_NONE;
+    r->step = 1e-3;
+    r->funnel_angle = 0.3490658503988659;
+    r->disk_angle = 1.0471975511965976;
+    r->sigma_boundary = 1.0;
+    r->beta_boundary = 1.0;
+}
+
+int kp_response_channels(const kp_response_config* r) { return validate_response(r); }
+
+int kp_image_riaf_analysis_response(const kp_pass_a_params* params, const kp_riaf_model* model,
+                                    int radiation_substeps, const kp_analysis_config* config,
+                                    const kp_response_config* response_config, const kp_run_options* options,
+                                    kp_image_out* out, kp_analysis_out* analysis, double* response) {
+    (void)radiation_substeps;
+    return analysis_impl(params, model, config, response_config, options, out, analysis, response);
+}
+
+static int analysis_impl(const kp_pass_a_params* params, const kp_riaf_model* model,
+                         const kp_analysis_config* config, const kp_response_config* resp_cfg,
+                         const kp_run_options* options, kp_image_out* out, kp_analysis_out* analysis,
+                         double* response) {
     kp_run_options opt;
     if (options) {
         opt = *options;
@@ -1037,6 +1135,10 @@ int kp_image_riaf_analysis(const kp_pass_a_params* params, const kp_riaf_model* 
     const int npix = params->camera.nx * params->camera.ny;
     st = check_outputs(out, npix, 1);
     if (st != KP_OK) return st;
+    const int channels = resp_cfg ? validate_response(resp_cfg) : 0;
+    if (channels < 0) return channels;
+    if (channels > 0 && !response) return set_error(KP_ERR_INVALID, "null response output with %d channels", channels);
+    const size_t response_bytes = size_t(4) * size_t(channels) * size_t(npix) * sizeof(double);
     // kp_analysis_out and AnalysisPtrs list the same arrays in the same order
     constexpr int kArrays = int(sizeof(kp_analysis_out) / sizeof(void*));
     static_assert(sizeof(kp_analysis_out) == sizeof(AnalysisPtrs), "analysis array lists differ");
@@ -1084,8 +1186,30 @@ int kp_image_riaf_analysis(const kp_pass_a_params* params, const kp_riaf_model* 
     }
     AnalysisPtrs an;
     std::memcpy(&an, dev_arrays, sizeof(an));
+    // response channels: the configuration and (host outputs) the channel
+    // array in one device buffer, the array zeroed before the launch
+    void* resp_buf = nullptr;
+    kp_response_config* d_resp = nullptr;
+    double* d_response = nullptr;
+    cudaError_t e = cudaSuccess;
+    if (channels > 0) {
+        const size_t cfg_bytes = (sizeof(kp_response_config) + 255) / 256 * 256;
+        const size_t bytes = cfg_bytes + (opt.outputs_on_device ? 0 : response_bytes);
+        e = cudaMalloc(&resp_buf, bytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            if (analysis_buf) cudaFree(analysis_buf);
+            return set_error(KP_ERR_OOM, "cudaMalloc(%zu bytes) for response channels: %s", bytes,
+                             cudaGetErrorString(e));
+        }
+        d_resp = static_cast<kp_response_config*>(resp_buf);
+        d_response = opt.outputs_on_device ? response
+                                           : reinterpret_cast<double*>(static_cast<char*>(resp_buf) + cfg_bytes);
+        e = cudaMemcpyAsync(d_resp, resp_cfg, sizeof(kp_response_config), cudaMemcpyHostToDevice, stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(d_response, 0, response_bytes, stream);
+    }
     const auto t0 = std::chrono::steady_clock::now();
-    cudaError_t e = launch_image_fp64_analysis(c, k, dptr, an, stream);
+    if (e == cudaSuccess) e = launch_image_fp64_analysis(c, k, dptr, an, d_resp, d_response, stream);
     if (e == cudaSuccess && opt.timing) {
         e = cudaStreamSynchronize(stream);
         if (e == cudaSuccess)
@@ -1096,10 +1220,14 @@ int kp_image_riaf_analysis(const kp_pass_a_params* params, const kp_riaf_model* 
         st = copy_outputs_to_host(dptr, out, npix, 1, stream);
         for (int i = 0; st == KP_OK && e == cudaSuccess && i < kArrays; ++i)
             e = cudaMemcpyAsync(host[i], dev_arrays[i], bytes_of(i), cudaMemcpyDeviceToHost, stream);
+        if (st == KP_OK && e == cudaSuccess && channels > 0)
+            e = cudaMemcpyAsync(response, d_response, response_bytes, cudaMemcpyDeviceToHost, stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
-    } else if (e == cudaSuccess && !opt.stream) {
+    } else if (e == cudaSuccess && (!opt.stream || resp_buf)) {
+        // the configuration buffer is freed below: the launch must be done
         e = cudaStreamSynchronize(stream);
     }
+    if (resp_buf) cudaFree(resp_buf);
     if (analysis_buf) cudaFree(analysis_buf);
     if (e != cudaSuccess) return cuda_error(e, "analysis image");
     return st;

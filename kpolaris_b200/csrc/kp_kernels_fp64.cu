@@ -56,7 +56,8 @@ __global__ void __launch_bounds__(128) image_fp64_per_pixel(const ImageConsts c,
 // ends without a valid endpoint returns zero diagnostics, as there.
 __global__ void __launch_bounds__(128) image_fp64_analysis(const ImageConsts c, const CameraFrame frame,
                                                            const AnalysisConsts k, const ImageOutPtrs out,
-                                                           const AnalysisPtrs an, int npix) {
+                                                           const AnalysisPtrs an, int npix,
+                                                           const kp_response_config* resp, double* resp_data) {
     const int pixel = blockIdx.x * blockDim.x + threadIdx.x;
     if (pixel >= npix) return;
     const Ray cam = camera_ray(c, frame, pixel);
@@ -70,9 +71,15 @@ __global__ void __launch_bounds__(128) image_fp64_analysis(const ImageConsts c, 
     o.reason = pa_reason;
     AnalysisAcc a;
     analysis_zero(a);
-    if (valid) trace_pass_b_analysis(c, k, state, stokes[0], o.steps, o.reason, a);
+    if (valid) trace_pass_b_analysis(c, k, state, stokes[0], o.steps, o.reason, a, resp, resp_data, pixel, npix);
     double obs[1][4];
     finish_ray<double, 1>(c, cam, state, valid, stokes, o, obs);
+    if (resp && valid) {
+        // finalize_response_basis (response.hpp:186-191)
+        const int channels = response_channel_count(*resp);
+        for (int ch = 0; ch < channels; ++ch)
+            resp_write(resp_data, pixel, npix, ch, observer_stokes(resp_read(resp_data, pixel, npix, ch), o));
+    }
     store_stokes<1>(out, pixel, npix, obs);
     store_diagnostics(out, pixel, o);
     ObserverAnalysis w = {};
@@ -138,13 +145,15 @@ __global__ void __launch_bounds__(128) image_fp64_analysis(const ImageConsts c, 
 }
 
 cudaError_t launch_image_fp64_analysis(const ImageConsts& c, const AnalysisConsts& k, const ImageOutPtrs& out,
-                                       const AnalysisPtrs& an, cudaStream_t stream) {
+                                       const AnalysisPtrs& an, const kp_response_config* resp, double* resp_data,
+                                       cudaStream_t stream) {
     if (c.nfreq != 1 || k.radial_bins < 1 || k.radial_bins > kMaxRadialBins) return cudaErrorInvalidValue;
+    if ((resp == nullptr) != (resp_data == nullptr)) return cudaErrorInvalidValue;
     const CameraFrame frame = camera_frame(c);
     const int npix = c.nx * c.ny;
     const int block = 128;
     const int grid = (npix + block - 1) / block;
-    image_fp64_analysis<<<grid, block, 0, stream>>>(c, frame, k, out, an, npix);
+    image_fp64_analysis<<<grid, block, 0, stream>>>(c, frame, k, out, an, npix, resp, resp_data);
     return cudaGetLastError();
 }
 

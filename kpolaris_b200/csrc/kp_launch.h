@@ -77,7 +77,8 @@ struct AnalysisPtrs {
 };
 
 cudaError_t launch_image_fp64_analysis(const ImageConsts& c, const AnalysisConsts& k, const ImageOutPtrs& out,
-                                       const AnalysisPtrs& an, cudaStream_t stream);
+                                       const AnalysisPtrs& an, const kp_response_config* resp, double* resp_data,
+                                       cudaStream_t stream);
 
 // Camera tetrad of an image, evaluated on the host (bit-identical to the
 // reference's CPU evaluation): Cartesian Kerr-Schild, or Boyer-Lindquist for

@@ -112,6 +112,10 @@ def lib(kind: str):
         L.kpref_image_riaf_analysis_range.argtypes = [
             C.POINTER(_abi.PassAParams), C.POINTER(_abi.RIAFModel), C.POINTER(_abi.AnalysisConfig), C.c_int,
             C.c_int, C.c_int, C.POINTER(_abi.ImageOut), C.POINTER(_abi.AnalysisOut)]
+        L.kpref_image_riaf_analysis_response_range.argtypes = [
+            C.POINTER(_abi.PassAParams), C.POINTER(_abi.RIAFModel), C.POINTER(_abi.AnalysisConfig),
+            C.POINTER(_abi.ResponseConfig), C.c_int, C.c_int, C.c_int, C.POINTER(_abi.ImageOut),
+            C.POINTER(_abi.AnalysisOut), C.POINTER(C.c_double)]
         _declare_common(L, "kpref_")
     else:
         raise ValueError(kind)
@@ -232,6 +236,30 @@ def image_riaf_analysis(params, model, config=None, *, kind="reference", threads
     if rc != 0:
         raise RuntimeError(L.kpref_last_error().decode())
     return out, analysis
+
+
+def image_riaf_analysis_response(params, model, config, response, *, kind="reference", threads=0):
+    """Analysis-mode RIAF image with source-partition response channels
+    through the reference's own per-pixel analysis function and its
+    response accumulation (src/diagnostics/response.hpp).  Returns
+    (ImageHostData, AnalysisHostData, channels [channel, 4, npix])."""
+    if kind not in ("reference", "reference_ulp"):
+        raise ValueError("the analysis oracle is the reference's own code")
+    L = lib(kind)
+    if config is None:
+        config = _abi.default_analysis_config()
+    npix = params.camera.nx * params.camera.ny
+    out = _abi.ImageHostData.allocate(npix, 1)
+    analysis = _abi.AnalysisHostData.allocate(npix, int(config.radial_bins))
+    nch = _abi.response_channels(response)
+    channels = np.zeros((max(nch, 1), 4, npix), dtype=np.float64)
+    s, a = out.as_struct(), analysis.as_struct()
+    rc = L.kpref_image_riaf_analysis_response_range(
+        C.byref(params), C.byref(model), C.byref(config), C.byref(response), int(threads), 0, npix, C.byref(s),
+        C.byref(a), channels.ctypes.data_as(C.POINTER(C.c_double)))
+    if rc != 0:
+        raise RuntimeError(L.kpref_last_error().decode())
+    return out, analysis, channels[:nch]
 
 
 def thermal_coefficients(fit, nu, ne, thetae, b, theta, sin_theta, cos_theta,

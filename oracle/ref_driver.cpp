@@ -645,6 +645,18 @@ int kpref_image_riaf_pixels(const kp_pass_a_params* params, const kp_riaf_model*
     return KP_OK;
 }
 
+// A caller-owned array as the response view the analysis function indexes
+// (response_read / response_write, src/diagnostics/response.hpp:12-24).
+struct RawResponseView {
+    double* p = nullptr;
+    double& operator()(size_t i) const { return p[i]; }
+};
+
+static int analysis_range(const kp_pass_a_params* params, const kp_riaf_model* model,
+                          const kp_analysis_config* config, const kp_response_config* resp, int threads,
+                          int pixel_begin, int pixel_end, kp_image_out* out, kp_analysis_out* an,
+                          double* response);
+
 // Analysis mode: pixels [pixel_begin, pixel_end) of a single-frequency RIAF
 // image through the reference's per-pixel analysis function
 // (trace_pass_b_segment_model_analysis_pixel_metric,
@@ -653,6 +665,27 @@ int kpref_image_riaf_pixels(const kp_pass_a_params* params, const kp_riaf_model*
 int kpref_image_riaf_analysis_range(const kp_pass_a_params* params, const kp_riaf_model* model,
                                     const kp_analysis_config* config, int threads, int pixel_begin,
                                     int pixel_end, kp_image_out* out, kp_analysis_out* an) {
+    return analysis_range(params, model, config, nullptr, threads, pixel_begin, pixel_end, out, an, nullptr);
+}
+
+// The same with source-partition response channels: the reference's
+// ResponseConfig (src/diagnostics/response_config.hpp:10-33) from
+// kp_response_config, and `response` (4 * channels * npix doubles, zeroed
+// by the caller, as the analysis image driver's view is) as its response
+// view.
+int kpref_image_riaf_analysis_response_range(const kp_pass_a_params* params, const kp_riaf_model* model,
+                                             const kp_analysis_config* config, const kp_response_config* resp,
+                                             int threads, int pixel_begin, int pixel_end, kp_image_out* out,
+                                             kp_analysis_out* an, double* response) {
+    if (!resp || !response) return fail("null response argument");
+    if (resp->edge_count < 0 || resp->edge_count > kpolaris::max_partition_edges) return fail("edge_count out of range");
+    return analysis_range(params, model, config, resp, threads, pixel_begin, pixel_end, out, an, response);
+}
+
+static int analysis_range(const kp_pass_a_params* params, const kp_riaf_model* model,
+                          const kp_analysis_config* config, const kp_response_config* resp, int threads,
+                          int pixel_begin, int pixel_end, kp_image_out* out, kp_analysis_out* an,
+                          double* response) {
     if (!params || !model || !config || !out || !an) return fail("null argument");
     const int npix = params->camera.nx * params->camera.ny;
     if (pixel_begin < 0 || pixel_end > npix || pixel_begin > pixel_end) return fail("pixel range out of bounds");
@@ -667,6 +700,22 @@ int kpref_image_riaf_analysis_range(const kp_pass_a_params* params, const kp_ria
     cfg.radial_min = config->radial_min;
     cfg.radial_max = config->radial_max;
     cfg.formation_fraction = config->formation_fraction;
+    if (resp) {
+        auto& rc = cfg.response;
+        rc.parameter = static_cast<kpolaris::PlasmaParameter>(resp->parameter);
+        rc.partition = static_cast<kpolaris::SourcePartition>(resp->partition);
+        rc.step = resp->step;
+        rc.bins = resp->bins;
+        rc.edge_count = resp->edge_count;
+        for (int i = 0; i < kpolaris::max_partition_edges; ++i) rc.edges[i] = resp->edges[i];
+        rc.funnel_angle = resp->funnel_angle;
+        rc.disk_angle = resp->disk_angle;
+        rc.sigma_boundary = resp->sigma_boundary;
+        rc.beta_boundary = resp->beta_boundary;
+        rc.observer_theta = resp->observer_theta;
+        rc.observer_phi = resp->observer_phi;
+    }
+    const RawResponseView view{response};
     const kpolaris::KerrSchildInMetric<Real> metric(pa.mass, pa.spin);
 #pragma omp parallel for schedule(dynamic)
     for (int pixel = pixel_begin; pixel < pixel_end; ++pixel) {
@@ -674,7 +723,8 @@ int kpref_image_riaf_analysis_range(const kp_pass_a_params* params, const kp_ria
         kpref_ulp::seed_pixel(pixel);
 #endif
         const kpolaris::PassBAnalysisResult<Real> r =
-            kpolaris::trace_pass_b_segment_model_analysis_pixel_metric(pixel, pa, cfg, riaf, 1, metric);
+            resp ? kpolaris::trace_pass_b_segment_model_analysis_pixel_metric(pixel, pa, cfg, riaf, 1, metric, view)
+                 : kpolaris::trace_pass_b_segment_model_analysis_pixel_metric(pixel, pa, cfg, riaf, 1, metric);
         const auto& t = r.transport;
         const auto& d = r.analysis;
         out->image_i[pixel] = t.observed_stokes.I;

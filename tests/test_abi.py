@@ -51,6 +51,7 @@ def test_struct_layouts_match_ctypes_mirror():
     assert lib.kp_abi_sizeof(12) == C.sizeof(_abi.AnalysisConfig)
     assert lib.kp_abi_sizeof(13) == C.sizeof(_abi.AnalysisOut)
     assert lib.kp_abi_sizeof(14) == C.sizeof(_abi.IharmOptions)
+    assert lib.kp_abi_sizeof(15) == C.sizeof(_abi.ResponseConfig)
     assert lib.kp_abi_sizeof(6) > 0
     assert lib.kp_abi_sizeof(99) == 0
 
@@ -120,3 +121,52 @@ def test_step_control_lists_are_validated_before_launch(control, msg):
     out = _abi.ImageHostData.allocate(16, 4).as_struct()
     st = lib.kp_image_grmhd_step_control(C.byref(params), None, 1, fa, 4, ca, len(control), None, C.byref(out))
     assert st == _abi.KP_ERR_INVALID
+
+
+def test_response_config_defaults_and_channels():
+    """kp_default_response_config holds ResponseConfig's member defaults
+    (src/diagnostics/response_config.hpp:12-24); kp_response_channels is
+    ResponseConfig::channels for valid configurations, the same as the
+    Python builder, which follows the tool's make_response_config."""
+    lib = kp.library()
+    r = _abi.ResponseConfig()
+    lib.kp_default_response_config(C.byref(r))
+    assert bytes(r) == bytes(_abi.default_response_config())
+    assert lib.kp_response_channels(C.byref(r)) == 0
+    cases = [("density_scale", "radial", 16 * 5 + 4), ("none", "radial", 16), ("none", "region", 6),
+             ("coefficients", "near_far", 2 * 5 + 4), ("magnetic_scale", "plasma_region", 4 * 5 + 4),
+             ("temperature_scale", "thetae", 7 * 5 + 4), ("none", "ne_cgs", 8), ("none", "b_cgs", 7)]
+    for resp, part, want in cases:
+        c = _abi.make_response_config(resp, part, inclination=0.3)
+        assert lib.kp_response_channels(C.byref(c)) == want == _abi.response_channels(c), (resp, part)
+    # a response without a partition is radial, as in the tool
+    assert _abi.make_response_config("density_scale").partition == _abi.SOURCE_PARTITIONS["radial"]
+
+
+def _bad_response(**fields):
+    c = _abi.make_response_config("density_scale", "radial", radial_bins=4)
+    for k, v in fields.items():
+        setattr(c, k, v)
+    return c
+
+
+@pytest.mark.parametrize("fields,msg", [
+    ({"parameter": 7}, "unknown response parameter"),
+    ({"partition": 12}, "unknown source partition"),
+    ({"partition": 0}, "needs a source partition"),
+    ({"step": 0.5}, r"analysis_response_step must be finite and in \[1e-6,0.1\]"),
+    ({"bins": 5}, "radial partition"),
+    ({"edge_count": 4}, "radial partition"),
+    ({"partition": 2, "bins": 5}, "needs bins = 6"),
+    ({"partition": 2, "bins": 6, "funnel_angle": 1.2}, "region angles"),
+    ({"partition": 3, "bins": 4, "sigma_boundary": 0.0}, "boundaries must be finite and positive"),
+    ({"partition": 5, "bins": 2, "edge_count": 0}, "analysis_partition_edges"),
+    ({"partition": 5, "bins": 5, "edge_count": 2}, "needs bins = 4"),
+])
+def test_response_config_is_validated_before_launch(fields, msg):
+    c = _bad_response(**fields)
+    lib = kp.library()
+    assert lib.kp_response_channels(C.byref(c)) == _abi.KP_ERR_INVALID
+    params, model, _ = configs.config2(4, 4)
+    with pytest.raises(kp.KPolarisInvalidArgument, match=msg):
+        kp.image_riaf_analysis_response(params, model, None, c)

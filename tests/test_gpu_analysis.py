@@ -82,3 +82,64 @@ def test_analysis_refuses_what_is_not_built():
         kp.image_riaf_analysis(p, m, _abi.default_analysis_config(radial_bins=25))
     with pytest.raises(kp.KPolarisError):
         kp.image_riaf_analysis(p, m, _abi.default_analysis_config(formation_fraction=1.0))
+
+
+# The derivative channels are central differences over q = +-h (h = 1e-3),
+# which scale rounding differences by 1/(2h): in Faraday-thick pixels their
+# libm conditioning has a longer tail than the image's.  Eight perturbed
+# reference runs and three times their largest deviation bound it.
+CHANNEL_LIBM_FACTOR = 3.0
+
+RESPONSE_CASES = [("density_scale", "radial"), ("none", "region"), ("coefficients", "near_far"),
+                  ("temperature_scale", "thetae"), ("magnetic_scale", "plasma_region"), ("none", "ne_cgs")]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("response,partition", RESPONSE_CASES)
+def test_analysis_response_channels_match_reference(response, partition):
+    """Source-partition response channels (src/diagnostics/response.hpp) on
+    the config-2 controls against the reference's own accumulation: step
+    counts and reasons bit-exact, every channel within max(1e-9 of its
+    largest magnitude, three times its libm conditioning), measured on the
+    reference with every libm result moved by up to +-2 ulp (eight seeds);
+    the bin channels close on the image (their sum is the pixel's Stokes
+    vector)."""
+    p, m, _ = configs.config2(16, 16)
+    cfg = _abi.default_analysis_config(radial_bins=6)
+    rc = _abi.make_response_config(response, partition, radial_bins=6, inclination=p.camera.inclination)
+    got, got_an, ch = kp.image_riaf_analysis_response(p, m, cfg, rc, device=0)
+    ref, ref_an, ref_ch = oracle.image_riaf_analysis_response(p, m, cfg, rc, threads=0)
+    assert ch.shape == ref_ch.shape == (_abi.response_channels(rc), 4, 256)
+    for k in INT_FIELDS:
+        assert np.array_equal(got.arrays[k], ref.arrays[k]), k
+    ch_cond = np.zeros(ch.shape[:2])
+    for seed in range(1, 9):
+        oracle.set_libm_perturbation(seed, "reference_ulp")
+        _, _, pert = oracle.image_riaf_analysis_response(p, m, cfg, rc, kind="reference_ulp", threads=0)
+        ch_cond = np.maximum(ch_cond, np.max(np.abs(pert - ref_ch), axis=2))
+    for c in range(ch.shape[0]):
+        for s in range(4):
+            scale = float(np.max(np.abs(ref_ch[c, s]), initial=0.0))
+            bar = max(1e-9 * scale, CHANNEL_LIBM_FACTOR * ch_cond[c, s])
+            assert float(np.max(np.abs(ch[c, s] - ref_ch[c, s]), initial=0.0)) <= bar, (c, s, bar, scale)
+    # the bin channels add up to the image (response.hpp:120-126: every
+    # sample's emission goes to exactly one bin, all bins propagate alike)
+    bins = rc.bins
+    for s, key in enumerate(("image_i", "image_q", "image_u", "image_v")):
+        total = ch[:bins, s].sum(axis=0)
+        img = got.arrays[key][0]
+        assert np.allclose(total, img, rtol=1e-9, atol=1e-9 * float(np.max(np.abs(img)))), key
+    assert np.count_nonzero(ch) > 0
+
+
+@pytest.mark.gpu
+def test_analysis_response_off_is_the_plain_analysis():
+    p, m, _ = configs.config2(12, 12)
+    cfg = _abi.default_analysis_config()
+    a, a_an = kp.image_riaf_analysis(p, m, cfg, device=0)
+    b, b_an, ch = kp.image_riaf_analysis_response(p, m, cfg, _abi.default_response_config(), device=0)
+    assert ch.shape[0] == 0
+    for k in a.arrays:
+        assert np.array_equal(a.arrays[k], b.arrays[k], equal_nan=True), k
+    for k in a_an.arrays:
+        assert np.array_equal(a_an.arrays[k], b_an.arrays[k], equal_nan=True), k
