@@ -1000,8 +1000,8 @@ def ours_arm(args):
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": launches[0],
             "roofline": roof, "cpu_baseline": cpu, "clocks": clocks,
-            # the secondary workloads (bulky) before the north-star numbers,
-            # which close the line
+            # the secondary workloads (bulky) before the headline comparison
+            # (plain FP64, speed-up, accuracy, latency), which closes the line
             "serving": serving,
             "grmhd": grmhd,
             "config4": config4,
