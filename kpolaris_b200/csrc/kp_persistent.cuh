@@ -2,7 +2,7 @@
 // phase queue (fresh camera rays, then ray ids handed over by other phases),
 // advance them one RK job per loop iteration through the pass-A / crossing /
 // pass-B control machine, and either finish the pixel or park the ray's
-// record in HBM for another phase (or for the next round when an iteration
+// record in HBM for another phase (or for its own next launch when an iteration
 // budget is set).  See kp_engine.cuh for the RK jobs.
 //
 // Three phases, one kernel each, so that the lanes of a warp run the same
@@ -283,7 +283,7 @@ __device__ __forceinline__ void persistent_body(const WaveDesc& W) {
         if (!__syncthreads_or(active || forward)) break;
 
         // ---------------------------------------------- control before the job
-        int dest = -1;  // phase the ray is handed to (PHASE itself: next round)
+        int dest = -1;  // phase the ray is handed to (PHASE itself: its next launch)
         if constexpr (kPassA) {
             if (active && st.mode == kAStep && st.rk_kind < 0) {
                 const ImageConsts& c = J->c;

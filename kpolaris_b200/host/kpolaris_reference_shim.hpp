@@ -182,14 +182,14 @@ HostData run_riaf_image(const PassA& pass_a, Model model, int radiation_substeps
 // run_riaf_analysis_image (src/image/riaf.hpp:22-28, src/image/riaf.cpp:48-75):
 // the image plus the analysis block of ImageHostData (src/image/result.hpp:
 // 35-92), with the radial-bin edges and centres the reference's analysis
-// driver records (src/image/analysis_driver.hpp:1060-1076).  The response
-// channels (analysis_config.response) are not built.
+// driver records (src/image/analysis_driver.hpp:1060-1076).  With
+// analysis_config.response enabled, the source-partition response channels
+// come back in response_data (4 * channels * npix, the driver's view layout,
+// :729-730, 1016-1017) through kp_image_riaf_analysis_response.
 template<class HostData, class PassA, class AnalysisCfg, class Model>
 HostData run_riaf_analysis_image(const PassA& pass_a, const AnalysisCfg& analysis_config, Model model,
                                  int radiation_substeps, int timing, int split_transport) {
     (void)split_transport;
-    if (analysis_config.response.enabled())
-        throw std::runtime_error("analysis response channels (analysis_partition) are not built");
     const kp_pass_a_params p = to_c(pass_a);
     const kp_riaf_model m = to_c_riaf(model);
     const int npix = p.camera.nx * p.camera.ny;
@@ -268,7 +268,30 @@ HostData run_riaf_analysis_image(const PassA& pass_a, const AnalysisCfg& analysi
     c.formation_fraction = analysis_config.formation_fraction;
     kp_run_options opt = shim_options();
     opt.timing = timing;
-    throw_on_error(kp_image_riaf_analysis(&p, &m, radiation_substeps, &c, &opt, &o, &a));
+    const auto& rc = analysis_config.response;
+    if (rc.enabled()) {
+        kp_response_config r;
+        kp_default_response_config(&r);
+        r.parameter = static_cast<int>(rc.parameter);
+        r.partition = static_cast<int>(rc.partition);
+        r.step = rc.step;
+        r.bins = rc.bins;
+        r.edge_count = rc.edge_count;
+        for (int i = 0; i < KP_MAX_PARTITION_EDGES; ++i) r.edges[i] = rc.edges[i];
+        r.funnel_angle = rc.funnel_angle;
+        r.disk_angle = rc.disk_angle;
+        r.sigma_boundary = rc.sigma_boundary;
+        r.beta_boundary = rc.beta_boundary;
+        r.observer_theta = rc.observer_theta;
+        r.observer_phi = rc.observer_phi;
+        const int channels = kp_response_channels(&r);
+        throw_on_error(channels < 0 ? channels : KP_OK);
+        out.response_data.assign(size_t(4) * size_t(channels) * size_t(npix), 0.0);
+        throw_on_error(kp_image_riaf_analysis_response(&p, &m, radiation_substeps, &c, &r, &opt, &o, &a,
+                                                       out.response_data.data()));
+    } else {
+        throw_on_error(kp_image_riaf_analysis(&p, &m, radiation_substeps, &c, &opt, &o, &a));
+    }
     out.has_analysis = 1;
     out.response_config = analysis_config.response;
     out.analysis_radial_bins = bins;

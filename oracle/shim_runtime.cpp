@@ -138,5 +138,32 @@ int main() {
     check(std::fabs(an.analysis_radial_bin_edges.front() - e0) <= 1e-12 &&
               std::fabs(an.analysis_radial_bin_edges.back() - e10) <= 1e-9,
           "analysis bin edges", an.analysis_radial_bin_edges.back(), e10);
+
+    // response channels through the same signature: a density response on
+    // four radial bins, against the reference's own accumulation into a
+    // zeroed view of the driver's layout (analysis_driver.hpp:729-730)
+    kpolaris::AnalysisConfig<Real> rcfg = cfg;
+    auto& rc = rcfg.response;
+    rc.parameter = kpolaris::PlasmaParameter::density_scale;
+    rc.partition = kpolaris::SourcePartition::radial;
+    rc.bins = 4;
+    rc.edge_count = 5;
+    for (int k = 0; k <= 4; ++k) rc.edges[k] = std::exp(std::log(2.0) + Real(k) / 4 * std::log(110.0 / 2.0));
+    const ImageHostData rs = kpolaris_b200::run_riaf_analysis_image<ImageHostData>(pa, rcfg, model, 1, 0, 1);
+    const size_t nresp = size_t(4) * size_t(rc.channels()) * size_t(npix);
+    std::vector<Real> want(nresp, 0.0);
+    struct View {
+        Real* q;
+        Real& operator()(size_t i) const { return q[i]; }
+    } view{want.data()};
+    for (int p = 0; p < npix; ++p)
+        (void)kpolaris::trace_pass_b_segment_model_analysis_pixel_metric(p, pa, rcfg, model, 1, metric, view);
+    check(rs.response_data.size() == nresp, "response channel count", double(rs.response_data.size()),
+          double(nresp));
+    // the emission channels (4 bins) and the derivative and rerun channels
+    std::vector<Real> g_emit(rs.response_data.begin(), rs.response_data.begin() + size_t(16) * npix);
+    std::vector<Real> w_emit(want.begin(), want.begin() + size_t(16) * npix);
+    close("response emission channels", g_emit, w_emit, 1e-6);
+    close("response all channels", rs.response_data, want, 1e-5);
     return g_fail;
 }

@@ -4,7 +4,9 @@ reference's own headers by `make -C oracle ref`) calls the shim's
 run_riaf_image and run_riaf_analysis_image on the GPU and the reference's own
 per-pixel functions on the CPU for the same 12 x 10 image, and checks every
 block the shim fills: reasons and step counts exact, Stokes and analysis
-values within their parity bars, bin metadata."""
+values within their parity bars, bin metadata, and the source-partition
+response channels (a density response on four radial bins) against the
+reference's own accumulation."""
 from __future__ import annotations
 
 import subprocess
