@@ -18,34 +18,50 @@
 // how rays are distributed over launches, lanes or warps.
 #pragma once
 
+#include <cstddef>
+
 #include "kp_engine.cuh"
 
 namespace kp {
 
 enum : int { kEndA = 7 };
 
-// Control state of one ray (doubles first: 17 doubles + 17 ints, 208 bytes).
+// Control state of one ray (17 doubles + 17 ints, 208 bytes), in three
+// parts: what every phase uses; what only the pass-A phases (far and
+// near-A) use; the surface-crossing search (near-A).  A phase kernel moves
+// only the parts it uses between its registers and the record, so the
+// others hold no registers there; the record keeps them as the last phase
+// that used them left them.
 struct LaneState {
     // adaptive attempt sequence (rk4.hpp:108-161)
     double h_try, req_h, ctl_min, ctl_max;
-    // pass A (pass_b.hpp:786-938)
-    double h_current, old_r;
-    // surface-crossing search (pass_a_core.hpp:94-197)
-    double lo, hi, flo, fhi, full_h, surf, trial;
+    double h_current;
     // pass B (pass_b.hpp:940-1114)
     double cap, hB, start_r;
+    int job, pixel, mode, in_b;
+    int attempt, rk_kind;
+    int pa_steps, reason;
+    int steps, reached;
+    // pass A (pass_b.hpp:786-938)
+    double old_r;
     // far-phase chart scenes: the FMKS azimuth the ray entered the far
     // phase with, and whether S (here and in a record parked for the far
     // phase itself) holds the far phase's chart
     double x3_ref;
-    int job, pixel, mode, in_b;
-    int attempt, rk_kind;
-    int n, entered, inside, pa_steps, reason;
-    int cross_reason, iter, use_secant;
-    int steps, reached;
+    int n, entered, inside;
     int chart;
+    // surface-crossing search (pass_a_core.hpp:94-197)
+    double lo, hi, flo, fhi, full_h, surf, trial;
+    int cross_reason, iter, use_secant;
 };
 static_assert(sizeof(LaneState) <= sizeof(((RayRecord*)nullptr)->st), "LaneState must fit its record slot");
+static_assert(offsetof(LaneState, old_r) % 8 == 0 && offsetof(LaneState, lo) % 8 == 0, "parts are whole doubles");
+
+// Bytes of LaneState a phase kernel moves: near-B runs no pass-A step and
+// never holds a far chart, far runs no crossing search.
+template<int PHASE>
+constexpr size_t kLaneStateBytes = PHASE == kPhaseNearB ? offsetof(LaneState, old_r)
+                                   : (PHASE == kPhaseFar ? offsetof(LaneState, lo) : sizeof(LaneState));
 
 template<class LS>
 __device__ __forceinline__ void begin_adaptive(LS& L, double requested, double min_step, double max_step) {
@@ -260,7 +276,7 @@ __device__ __forceinline__ void persistent_body(const WaveDesc& W) {
                     my_id = W.in_ids[k - nfresh];
                     const RayRecord& rec = W.pool[my_id];
                     S = rec.S;
-                    memcpy(&st, rec.st, sizeof(LaneState));
+                    memcpy(&st, rec.st, kLaneStateBytes<PHASE>);
                     J = &W.jobs[st.job];
                     if constexpr (SC::kFarChart) {
                         // a record parked for this phase already holds its chart
@@ -375,7 +391,7 @@ __device__ __forceinline__ void persistent_body(const WaveDesc& W) {
             } else {
                 rec.S = S;
             }
-            memcpy(rec.st, &st, sizeof(LaneState));
+            memcpy(rec.st, &st, kLaneStateBytes<PHASE>);
             if constexpr (kRad) memcpy(rec.stokes, &stokes[0], sizeof(stokes));
         }
         // A lane past its budget keeps claiming and parks each claimed ray at
