@@ -225,9 +225,13 @@ __device__ __forceinline__ void persistent_body(const WaveDesc& W) {
     st.job = -1;
     st.rk_kind = -1;
     Ray S;
-    Ray best;
     typename RT::Stokes stokes[NF];
     unsigned my_id = 0;
+    // the crossing search's best state (near-A) lives in the record's Stokes
+    // slot, which pass A leaves unused: it holds no registers between the
+    // search's iterations
+    auto best = [&]() -> Ray& { return *reinterpret_cast<Ray*>(W.pool[my_id].stokes); };
+    static_assert(sizeof(((RayRecord*)nullptr)->stokes) >= sizeof(Ray), "the Stokes slot holds a ray");
     int exhausted = 0;
     long long lane_jobs = 0;
     const JobDesc* J = nullptr;
@@ -477,7 +481,7 @@ __device__ __forceinline__ void persistent_body(const WaveDesc& W) {
                             st.cross_reason = crossing;
                             st.surf = crossing == kReachedInner ? c.inner_radius : c.outer_radius;
                             st.full_h = used_h;
-                            best = S;
+                            best() = S;
                             st.lo = 0.0;
                             st.hi = 1.0;
                             st.flo = SC::radius(c, S.x) - st.surf;
@@ -512,7 +516,7 @@ __device__ __forceinline__ void persistent_body(const WaveDesc& W) {
                     if (!(fhi == fhi) || abs_val(fhi) >= kLarge) {
                         finish = true;
                     } else if (fhi == 0.0) {
-                        best = next;
+                        best() = next;
                         finish = true;
                     } else if ((st.flo > 0.0) == (fhi > 0.0)) {
                         finish = true;
@@ -528,12 +532,12 @@ __device__ __forceinline__ void persistent_body(const WaveDesc& W) {
                     st.hi = st.trial;
                     st.use_secant = 0;
                 } else if (ft == 0.0) {
-                    best = next;
+                    best() = next;
                     finish = true;
                 } else if ((st.flo > 0.0) == (ft > 0.0)) {
                     st.lo = st.trial;
                     st.flo = ft;
-                    best = next;
+                    best() = next;
                 } else {
                     st.hi = st.trial;
                     st.fhi = ft;
@@ -542,7 +546,7 @@ __device__ __forceinline__ void persistent_body(const WaveDesc& W) {
             }
             if (!finish && st.iter >= 12) finish = true;
             if (finish) {
-                S = best;
+                S = best();
                 st.pa_steps += 1;
                 st.reason = st.cross_reason;
                 st.mode = kEndA;
