@@ -58,10 +58,11 @@ static_assert(sizeof(LaneState) <= sizeof(((RayRecord*)nullptr)->st), "LaneState
 static_assert(offsetof(LaneState, old_r) % 8 == 0 && offsetof(LaneState, lo) % 8 == 0, "parts are whole doubles");
 
 // Bytes of LaneState a phase kernel moves: near-B runs no pass-A step and
-// never holds a far chart, far runs no crossing search.
+// never holds a far chart, far runs no crossing search, and near-A's
+// crossing search works on the crossing part in the record itself (one
+// search per ray, a few iterations).
 template<int PHASE>
-constexpr size_t kLaneStateBytes = PHASE == kPhaseNearB ? offsetof(LaneState, old_r)
-                                   : (PHASE == kPhaseFar ? offsetof(LaneState, lo) : sizeof(LaneState));
+constexpr size_t kLaneStateBytes = PHASE == kPhaseNearB ? offsetof(LaneState, old_r) : offsetof(LaneState, lo);
 
 template<class LS>
 __device__ __forceinline__ void begin_adaptive(LS& L, double requested, double min_step, double max_step) {
@@ -231,6 +232,8 @@ __device__ __forceinline__ void persistent_body(const WaveDesc& W) {
     // slot, which pass A leaves unused: it holds no registers between the
     // search's iterations
     auto best = [&]() -> Ray& { return *reinterpret_cast<Ray*>(W.pool[my_id].stokes); };
+    // ... and its bracket, the crossing part of the control state, in the record
+    auto cs = [&]() -> LaneState& { return *reinterpret_cast<LaneState*>(W.pool[my_id].st); };
     static_assert(sizeof(((RayRecord*)nullptr)->stokes) >= sizeof(Ray), "the Stokes slot holds a ray");
     int exhausted = 0;
     long long lane_jobs = 0;
@@ -418,7 +421,7 @@ __device__ __forceinline__ void persistent_body(const WaveDesc& W) {
         if (run) {
             const bool crossing = kCross && (st.mode == kACrossHi || st.mode == kACrossTrial);
             const int kind = crossing ? (J->c.adaptive ? kRkRK4x2 : kRkRK4) : st.rk_kind;
-            const double hj = crossing ? (st.mode == kACrossHi ? st.full_h : st.full_h * st.trial) : st.h_try;
+            const double hj = crossing ? (st.mode == kACrossHi ? cs().full_h : cs().full_h * cs().trial) : st.h_try;
             rk_job<P, fp32, SC>(kind, J->c, S, hj, next, mid, err);
             if (++lane_jobs > (1LL << 30)) {
                 st.reason = kInvalidState;
@@ -478,14 +481,14 @@ __device__ __forceinline__ void persistent_body(const WaveDesc& W) {
                     }
                     if (crossing != kNone) {
                         if constexpr (kCross) {
-                            st.cross_reason = crossing;
-                            st.surf = crossing == kReachedInner ? c.inner_radius : c.outer_radius;
-                            st.full_h = used_h;
+                            cs().cross_reason = crossing;
+                            cs().surf = crossing == kReachedInner ? c.inner_radius : c.outer_radius;
+                            cs().full_h = used_h;
                             best() = S;
-                            st.lo = 0.0;
-                            st.hi = 1.0;
-                            st.flo = SC::radius(c, S.x) - st.surf;
-                            if (st.flo == 0.0 || !finite_ray(next)) {
+                            cs().lo = 0.0;
+                            cs().hi = 1.0;
+                            cs().flo = SC::radius(c, S.x) - cs().surf;
+                            if (cs().flo == 0.0 || !finite_ray(next)) {
                                 st.pa_steps += 1;  // the event keeps the first state
                                 st.reason = crossing;
                                 st.mode = kEndA;
@@ -512,54 +515,54 @@ __device__ __forceinline__ void persistent_body(const WaveDesc& W) {
                 if (!finite_ray(next)) {
                     finish = true;
                 } else {
-                    const double fhi = SC::radius(c, next.x) - st.surf;
+                    const double fhi = SC::radius(c, next.x) - cs().surf;
                     if (!(fhi == fhi) || abs_val(fhi) >= kLarge) {
                         finish = true;
                     } else if (fhi == 0.0) {
                         best() = next;
                         finish = true;
-                    } else if ((st.flo > 0.0) == (fhi > 0.0)) {
+                    } else if ((cs().flo > 0.0) == (fhi > 0.0)) {
                         finish = true;
                     } else {
-                        st.fhi = fhi;
-                        st.iter = 0;
-                        st.use_secant = 1;
+                        cs().fhi = fhi;
+                        cs().iter = 0;
+                        cs().use_secant = 1;
                     }
                 }
             } else {
-                const double ft = finite_ray(next) ? SC::radius(c, next.x) - st.surf : 0.0;
+                const double ft = finite_ray(next) ? SC::radius(c, next.x) - cs().surf : 0.0;
                 if (!finite_ray(next) || !(ft == ft) || abs_val(ft) >= kLarge) {
-                    st.hi = st.trial;
-                    st.use_secant = 0;
+                    cs().hi = cs().trial;
+                    cs().use_secant = 0;
                 } else if (ft == 0.0) {
                     best() = next;
                     finish = true;
-                } else if ((st.flo > 0.0) == (ft > 0.0)) {
-                    st.lo = st.trial;
-                    st.flo = ft;
+                } else if ((cs().flo > 0.0) == (ft > 0.0)) {
+                    cs().lo = cs().trial;
+                    cs().flo = ft;
                     best() = next;
                 } else {
-                    st.hi = st.trial;
-                    st.fhi = ft;
+                    cs().hi = cs().trial;
+                    cs().fhi = ft;
                 }
-                st.iter += 1;
+                cs().iter += 1;
             }
-            if (!finish && st.iter >= 12) finish = true;
+            if (!finish && cs().iter >= 12) finish = true;
             if (finish) {
                 S = best();
                 st.pa_steps += 1;
-                st.reason = st.cross_reason;
+                st.reason = cs().cross_reason;
                 st.mode = kEndA;
             } else {
-                const double width = st.hi - st.lo;
-                double trial = (st.lo + st.hi) * 0.5;
-                const double denom = st.flo - st.fhi;
-                if (st.use_secant && abs_val(denom) > kTiny) {
-                    const double secant = st.lo + width * st.flo / denom;
+                const double width = cs().hi - cs().lo;
+                double trial = (cs().lo + cs().hi) * 0.5;
+                const double denom = cs().flo - cs().fhi;
+                if (cs().use_secant && abs_val(denom) > kTiny) {
+                    const double secant = cs().lo + width * cs().flo / denom;
                     const double g = width * 0.1;
-                    if (secant > st.lo + g && secant < st.hi - g) trial = secant;
+                    if (secant > cs().lo + g && secant < cs().hi - g) trial = secant;
                 }
-                st.trial = trial;
+                cs().trial = trial;
                 st.mode = kACrossTrial;
             }
         } else if (kPassB && run && (st.mode == kBStep || st.mode == kBCamCross)) {
